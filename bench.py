@@ -1,0 +1,356 @@
+#!/usr/bin/env python
+"""Benchmark: forward+adjoint tile-iterations/s of the imaging-and-gradient hot path.
+
+One step = one CTM objective evaluation on one 2048 x 2048 float32 tile with
+24 SOCS kernels of 35 x 35 (theta -> mask -> SOCS aerial image -> sigmoid
+resist -> PE loss -> adjoint dPE/dM -> dPE/dtheta and its norm), i.e. one
+tile-iteration of CTM_Optimizer::_evaluate_theta_objective
+(source/optimizer/CTM_Optimizer.cpp:175-187 of the reference).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Multi-GPU (torchrun, one rank per GPU): tiles are independent, so every rank
+solves its own tile with no data-path collective (weak scaling); the timed
+region is bracketed by barriers and the max over ranks is reported.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "forward+adjoint tile-iters/s (2048^2, 24 SOCS kernels)"
+UNIT = "tile-iters/s"
+THRESHOLD, ALPHA = 0.225, 50.0
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--size", type=int, default=2048)
+    p.add_argument("--kernels", type=int, default=24)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--cpu-seconds", type=float, default=12.0)
+    return p.parse_args()
+
+
+def workload(N, K, seed):
+    wl = importlib.import_module("c-version-lithography_b200.workloads")
+    band, r0, c0, w, wss = wl.synthetic_socs_band(K=K)
+    rng = np.random.default_rng(seed)
+    target = wl.manhattan_target(N, int(rng.integers(80, 151)), seed=seed, n_lt=10)
+    theta = wl.theta_init_reference(target)
+    return band, r0, c0, w, wss, target, theta
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = float(parts[1])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[3:7]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def stage_bytes(N, Nc, ks):
+    """Algorithmic DRAM bytes per launch of each stage of one CTM evaluation (float32)."""
+    px = 4 * N * N
+    part = 4 * ks * N * 2 * Nc
+    return {"row_analysis": px + part, "row_synthesis_resist": 2 * px,
+            "adjoint_row_analysis": px + part, "adjoint_row_synthesis_theta": 2 * px}
+
+
+def cpu_baseline(N, K, band, r0, c0, w, wss, target, theta, seconds):
+    """The FP64 restatement of the reference CPU path on the host cores (oracle)."""
+    from oracle import imaging_oracle as io
+    wl = importlib.import_module("c-version-lithography_b200.workloads")
+    cores = os.cpu_count() or 1
+    io.set_fft_workers(cores)
+    oc = io.OracleCache(N=N, kernels=list(wl.band_to_dense(band, r0, c0, N)),
+                        source_ws=np.array([wss]), eigenvalues=tuple(w))
+    io.ctm_evaluate(theta, target, oc, THRESHOLD, ALPHA)  # FFT plan / page-in warm-up
+    times = []
+    t_end = time.perf_counter() + seconds
+    while not times or (time.perf_counter() < t_end and len(times) < 8):
+        t0 = time.perf_counter()
+        io.ctm_evaluate(theta, target, oc, THRESHOLD, ALPHA)
+        times.append(time.perf_counter() - t0)
+    return {"value": len(times) / sum(times), "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{len(times)} CTM evaluations at {N}^2, K={K}: FP64 NumPy/SciPy "
+                      f"restatement of the reference CPU path (1 + 3K full FFTs), "
+                      f"scipy.fft workers={cores}"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if rank != 0:
+        return
+    from oracle import imaging_oracle as io
+    wl = importlib.import_module("c-version-lithography_b200.workloads")
+    N, K = args.size, args.kernels
+    band, r0, c0, w, wss, target, theta = workload(N, K, seed=1)
+    cores = os.cpu_count() or 1
+    io.set_fft_workers(cores)
+    oc = io.OracleCache(N=N, kernels=list(wl.band_to_dense(band, r0, c0, N)),
+                        source_ws=np.array([wss]), eigenvalues=tuple(w))
+    t0 = time.perf_counter()
+    io.ctm_evaluate(theta, target, oc, THRESHOLD, ALPHA)
+    est = time.perf_counter() - t0
+    budget = 240.0
+    warm = max(0, min(args.warmup - 1, int(budget * 0.2 / max(est, 1e-3))))
+    for _ in range(warm):
+        io.ctm_evaluate(theta, target, oc, THRESHOLD, ALPHA)
+    steps = max(2, min(args.steps, int(budget * 0.8 / max(est, 1e-3))))
+    times = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        io.ctm_evaluate(theta, target, oc, THRESHOLD, ALPHA)
+        times.append(time.perf_counter() - t0)
+    value = len(times) / sum(times)
+    sample = (f"{steps} of the requested {args.steps} steps timed (each one CTM evaluation at "
+              f"{N}^2, K={K}); FP64 NumPy/SciPy restatement of the reference CPU path, the "
+              f"reference itself does not build here (Eigen/FFTW/OpenCV-C++ absent)")
+    out = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+           "steps": steps, "warmup": warm + 1, "ms_per_step": 1e3 * sum(times) / len(times),
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+           "data": "synthetic", "config": config_dict(N, K, "fp64-cpu"),
+           "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                            "sample": sample},
+           "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+           "latency_ms": {"p50": 1e3 * float(np.percentile(times, 50)),
+                          "p99": 1e3 * float(np.percentile(times, 99))}}
+    print(json.dumps(out), flush=True)
+
+
+def config_dict(N, K, precision):
+    return {"workload": f"CTM objective evaluation (forward + adjoint) on one {N}^2 tile, "
+                        f"{K} SOCS kernels of 35x35, 2 nm pixels, sigmoid resist alpha 50 "
+                        f"thr 0.225, L2 pattern error, dPE/dtheta",
+            "tile": N, "kernels": K, "kernel_support": [35, 35], "tiles_per_gpu": 1,
+            "precision": precision, "theta_init": "0.3pi on target / 0.7pi off target",
+            "l2": "flushed between timed steps (256 MiB write)", "parallelism": "tile-sharded"}
+
+
+def run_ours(args):
+    import torch
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    L = importlib.import_module("c-version-lithography_b200")
+    N, K = args.size, args.kernels
+    band, r0, c0, w, wss, target, theta = workload(N, K, seed=1 + rank)
+    stream = torch.cuda.Stream()
+    ctx = L.Context(local, stream=stream)
+    cache = L.ImagingCache.from_band(N, band, r0, c0, w, wss, ctx=ctx)
+    with torch.cuda.stream(stream):
+        opt = L.CTMOptimizer(cache, target, THRESHOLD, ALPHA, iterations=1)
+        th = torch.tensor(theta, dtype=torch.float32, device="cuda")
+        flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    torch.cuda.synchronize()
+    for _ in range(max(3, args.warmup)):
+        opt.evaluate(th)
+    ctx.enable_stage_timing(True)
+    launches0 = ctx.launch_count
+    times = []
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            loss, _, _ = opt.evaluate(th)
+            e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+    torch.cuda.synchronize()
+    launches = ctx.launch_count - launches0
+    stages = ctx.stage_times()
+    ctx.enable_stage_timing(False)
+    total_ms = sum(times)
+    if dist:
+        t = torch.tensor([total_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+        dist.barrier()
+    value = world * args.steps / (total_ms / 1e3)
+
+    # End to end through the host-buffer entry point (H2D + compute + D2H per step).
+    h_theta = torch.tensor(theta, dtype=torch.float32).pin_memory()
+    h_target = torch.tensor(target, dtype=torch.float32).pin_memory()
+    h_grad = torch.empty((N, N), dtype=torch.float32).pin_memory()
+    import ctypes
+    lossd, normd = ctypes.c_double(), ctypes.c_double()
+
+    def host_call():
+        ctx._check(ctx.lib.litho_ctm_evaluate_host(
+            ctx.handle, cache.handle, opt.field.handle, h_theta.data_ptr(), h_target.data_ptr(),
+            THRESHOLD, ALPHA, h_grad.data_ptr(), ctypes.byref(lossd), ctypes.byref(normd)))
+
+    for _ in range(3):
+        host_call()
+    e2e_times = []
+    if dist:
+        dist.barrier()
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        stream.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        host_call()
+        e1.record(stream)
+        e1.synchronize()
+        e2e_times.append(e0.elapsed_time(e1))
+    e2e_total = sum(e2e_times)
+    if dist:
+        t = torch.tensor([e2e_total], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_total = float(t.item())
+    e2e_value = world * args.steps / (e2e_total / 1e3)
+
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return
+    # Roofline of the dominant stage (HBM-bound DFT passes), live CUDA-event timing.
+    hbm, src = peaks()
+    ks = _row_splits(N)
+    sb = stage_bytes(N, cache.Nc, ks)
+    dom = max(sb, key=lambda s: stages[s][0] / max(stages[s][1], 1))
+    avg_ms = stages[dom][0] / max(stages[dom][1], 1)
+    achieved = sb[dom] / (avg_ms / 1e3) / 1e9
+    traffic = _ncu_traffic(dom, N)
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": max(3, args.warmup), "ms_per_step": total_ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic", "config": config_dict(N, K, "fp32"),
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm,
+                     "peak_source": src, "unit": "GB/s", "frac": achieved / hbm,
+                     "traffic": traffic, "algorithmic_bytes": sb[dom], "avg_launch_ms": avg_ms},
+        "stages_ms_per_step": {k: v[0] / max(v[1], 1) for k, v in stages.items() if v[1]},
+        "latency_ms": {"p50": float(np.percentile(times, 50)), "p99": float(np.percentile(times, 99))},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * 4 * N * N,
+                "d2h_bytes_per_step": 4 * N * N + 8 * 3},
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(N, K, band, r0, c0, w, wss, target, theta,
+                                           args.cpu_seconds)
+    print(json.dumps(out), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
+def _row_splits(N):
+    rowblocks = (N + 127) // 128
+    req = max(1, min((296 + rowblocks - 1) // rowblocks, max(1, N // 64)))
+    kps = ((N + req - 1) // req + 15) // 16 * 16
+    return (N + kps - 1) // kps
+
+
+def _ncu_traffic(stage, N):
+    """DRAM bytes per launch from the committed ncu summary, when one exists."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            t = json.load(f)
+        v = t.get(f"{stage}@{N}")
+        return None if v is None else float(v)
+    except Exception:
+        return None
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,566 @@
+"""B200 imaging-and-gradient hot path of wyhcoder/C-version-Lithography.
+
+Host layer over the C ABI of ``liblitho_b200.so`` (declared in
+``include/litho_b200.h``). It mirrors the reference's C++ classes so code and
+tests read like the reference's:
+
+===========================  =================================================
+reference (C++)              here
+===========================  =================================================
+``ImagingCache``             :class:`ImagingCache` (device band kernels)
+``Imaging::compute``         :meth:`Imaging.compute` -> :class:`ImagingResult`
+``get_electric_field()``     :meth:`Imaging.get_electric_field` (band field)
+``Gradient::pe_gradient*``   :meth:`Gradient.pe_gradient`,
+                             :meth:`Gradient.pe_gradient_with_penalty`
+``Gradient::_backpropagate`` :meth:`Gradient.backpropagate`
+``Loss::pe_loss*``           :class:`Loss`
+``LevelSetUtils::*``         :class:`LevelSetUtils`
+``CTM_Optimizer``            :class:`CTMOptimizer`
+``LSM_Optimizer``            :class:`LSMOptimizer`
+===========================  =================================================
+
+Images are float32 CUDA tensors (row = y, col = x). PyTorch provides device
+memory and the stream; every computation runs in the library's CUDA kernels.
+There is no CPU fallback: without the built library or a GPU the calls raise.
+Errors raise :class:`LithoError` (``ValueError`` subclass, as the reference
+throws ``std::invalid_argument``).
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import os
+from dataclasses import dataclass
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liblitho_b200.so")
+
+# Status codes (include/litho_b200.h).
+LITHO_OK = 0
+STATUS_NAMES = {0: "ok", 1: "invalid argument", 2: "shape mismatch", 3: "non-finite input",
+                4: "out of device memory", 5: "CUDA error", 6: "field not computed",
+                7: "unsupported"}
+
+# Every exported symbol and its ctypes signature (restype, argtypes).
+_P = ctypes.c_void_p
+_I = ctypes.c_int
+_D = ctypes.c_double
+_PP = ctypes.POINTER(ctypes.c_void_p)
+_PD = ctypes.POINTER(ctypes.c_double)
+_PI = ctypes.POINTER(ctypes.c_int)
+
+
+class PeOptions(ctypes.Structure):
+    """litho_pe_options (include/litho_b200.h)."""
+    _fields_ = [("pe_window", _P), ("penalty_window", _P), ("pe_weight", _D),
+                ("penalty", _D), ("penalty_threshold", _D)]
+
+
+SIGNATURES = {
+    "litho_version": (_I, []),
+    "litho_status_string": (ctypes.c_char_p, [_I]),
+    "litho_ctx_last_error": (ctypes.c_char_p, [_P]),
+    "litho_ctx_create": (_I, [_I, _P, _PP]),
+    "litho_ctx_destroy": (_I, [_P]),
+    "litho_ctx_synchronize": (_I, [_P]),
+    "litho_ctx_set_precision": (_I, [_P, _I]),
+    "litho_ctx_launch_count": (ctypes.c_longlong, [_P]),
+    "litho_ctx_enable_stage_timing": (_I, [_P, _I]),
+    "litho_ctx_stage_times": (_I, [_P, _PD, ctypes.POINTER(ctypes.c_longlong)]),
+    "litho_cache_create_dense": (_I, [_P, _I, _I, _PD, _PD, _D, _PP]),
+    "litho_cache_create_band": (_I, [_P, _I, _I, _I, _I, _I, _I, _PD, _PD, _D, _PP]),
+    "litho_cache_info": (_I, [_P, _PI, _PI, _PI, _PI, _PI, _PI]),
+    "litho_cache_destroy": (_I, [_P]),
+    "litho_field_create": (_I, [_P, _P, _PP]),
+    "litho_field_destroy": (_I, [_P]),
+    "litho_field_export": (_I, [_P, _P, _I, _P]),
+    "litho_imaging_compute": (_I, [_P, _P, _P, _D, _D, _P, _P, _P]),
+    "litho_backpropagate": (_I, [_P, _P, _P, _D, _P]),
+    "litho_pe_gradient": (_I, [_P, _P, _P, _P, ctypes.POINTER(PeOptions), _D, _P, _PD]),
+    "litho_pe_loss": (_I, [_P, _P, _P, _I, _I, ctypes.POINTER(PeOptions), _PD]),
+    "litho_ctm_evaluate": (_I, [_P, _P, _P, _P, _P, _D, _D, _P, _P, _P, _P, _P, _PD, _PD]),
+    "litho_ctm_evaluate_host": (_I, [_P, _P, _P, _P, _P, _D, _D, _P, _PD, _PD]),
+    "litho_weno_godunov": (_I, [_P, _I, _I, _P, _P, _D, _D, _P, _P]),
+    "litho_kappa": (_I, [_P, _I, _I, _P, _D, _D, _D, _P]),
+    "litho_evolution_term": (_I, [_P, _I, _I, _P, _P, _D, _D, _D, _D, _P, _PD]),
+    "litho_lsm_rk2_update": (_I, [_P, _I, _I, _P, _P, _D, _D, _D, _D, _P, _P, _PD]),
+}
+
+
+class LithoError(ValueError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+_lib = None
+
+
+def library_path() -> str:
+    return LIB_PATH
+
+
+def load_library(path: Optional[str] = None):
+    """Load the C ABI library (no GPU needed to load it)."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise LithoError(7, f"{p} is not built; run c-version-lithography_b200/build.py")
+    lib = ctypes.CDLL(p)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    if path is None:
+        _lib = lib
+    return lib
+
+
+def _torch():
+    import torch
+    if not torch.cuda.is_available():
+        raise LithoError(5, "no CUDA device: the B200 library has no CPU path")
+    return torch
+
+
+def _ptr(t) -> Optional[int]:
+    return None if t is None else t.data_ptr()
+
+
+def _f32(t, torch, shape=None, name="array"):
+    """Contiguous float32 CUDA tensor view of t (copies host data to the device)."""
+    if t is None:
+        return None
+    if not isinstance(t, torch.Tensor):
+        t = torch.as_tensor(np.asarray(t))
+    if t.device.type != "cuda":
+        t = t.to("cuda")
+    t = t.to(torch.float32).contiguous()
+    if shape is not None and tuple(t.shape) != tuple(shape):
+        raise LithoError(2, f"{name} has shape {tuple(t.shape)}, expected {tuple(shape)}")
+    return t
+
+
+class Context:
+    """One CUDA stream plus scratch memory; used by one host thread at a time."""
+
+    def __init__(self, device: int = 0, stream=None):
+        torch = _torch()
+        self.lib = load_library()
+        self.torch = torch
+        self.device = device
+        torch.cuda.set_device(device)
+        if stream is None:
+            stream = torch.cuda.current_stream(device)
+        self.stream = stream
+        h = ctypes.c_void_p()
+        self._check(self.lib.litho_ctx_create(device, ctypes.c_void_p(stream.cuda_stream),
+                                              ctypes.byref(h)), None)
+        self.handle = h
+
+    def _check(self, status, handle="self"):
+        if status != LITHO_OK:
+            h = self.handle if handle == "self" else handle
+            msg = self.lib.litho_ctx_last_error(h).decode() if h else ""
+            raise LithoError(status, msg)
+
+    def synchronize(self):
+        self._check(self.lib.litho_ctx_synchronize(self.handle))
+
+    @property
+    def launch_count(self) -> int:
+        return int(self.lib.litho_ctx_launch_count(self.handle))
+
+    STAGES = ("row_analysis", "column_contraction", "band_forward", "row_synthesis_resist",
+              "adjoint_row_analysis", "adjoint_column_contraction", "band_adjoint",
+              "adjoint_row_synthesis_theta", "levelset_rk2")
+
+    def enable_stage_timing(self, on: bool = True):
+        self._check(self.lib.litho_ctx_enable_stage_timing(self.handle, 1 if on else 0))
+
+    def stage_times(self):
+        """{stage: (total ms, launches)} since timing was enabled."""
+        ms = (ctypes.c_double * 9)()
+        cnt = (ctypes.c_longlong * 9)()
+        self._check(self.lib.litho_ctx_stage_times(self.handle, ms, cnt))
+        return {name: (ms[i], cnt[i]) for i, name in enumerate(self.STAGES)}
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.litho_ctx_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_default_ctx: Optional[Context] = None
+
+
+def default_context() -> Context:
+    global _default_ctx
+    if _default_ctx is None:
+        _default_ctx = Context()
+    return _default_ctx
+
+
+class ImagingCache:
+    """Device copy of the optical kernels (ImagingCache, litho_prepare.h:18-47).
+
+    ``kernels`` are K full N x N complex frequency kernels with DC at [0, 0]
+    (the reference's ``optical_kernels_frequency``), ``eigenvalues`` the SOCS
+    weights (empty for Abbe) and ``source_ws`` the source weights.
+    """
+
+    def __init__(self, handle, ctx: Context):
+        self.handle = handle
+        self.ctx = ctx
+        vals = [ctypes.c_int() for _ in range(6)]
+        ctx.lib.litho_cache_info(handle, *[ctypes.byref(v) for v in vals])
+        self.N, self.K, self.Nr, self.Nc, self.row0, self.col0 = [v.value for v in vals]
+
+    @classmethod
+    def from_kernels(cls, kernels, source_ws, eigenvalues=(), ctx: Optional[Context] = None):
+        ctx = ctx or default_context()
+        ker = np.ascontiguousarray(np.asarray(kernels, dtype=np.complex128))
+        if ker.ndim != 3 or ker.shape[1] != ker.shape[2]:
+            raise LithoError(2, "kernels must be K x N x N")
+        K, N = ker.shape[0], ker.shape[1]
+        w = np.asarray(eigenvalues if len(eigenvalues) else source_ws, dtype=np.float64)
+        if w.size != K:
+            raise LithoError(1, "Imaging: SOCS kernel/value counts do not match" if len(eigenvalues)
+                             else "Imaging: Abbe kernel/source counts do not match")
+        ws = np.asarray(source_ws, dtype=np.float64)
+        if not (np.all(np.isfinite(ws)) and np.all(ws >= 0)):
+            raise LithoError(1, "Imaging: source weights must be finite, nonnegative, and have a positive sum")
+        flat = ker.view(np.float64).reshape(-1)
+        h = ctypes.c_void_p()
+        ctx._check(ctx.lib.litho_cache_create_dense(
+            ctx.handle, N, K, flat.ctypes.data_as(_PD), np.ascontiguousarray(w).ctypes.data_as(_PD),
+            float(ws.sum()), ctypes.byref(h)))
+        return cls(h, ctx)
+
+    @classmethod
+    def from_band(cls, N, band_kernels, row0, col0, weights, ws_sum, ctx: Optional[Context] = None):
+        ctx = ctx or default_context()
+        kb = np.ascontiguousarray(np.asarray(band_kernels, dtype=np.complex128))
+        K, Nr, Nc = kb.shape
+        w = np.ascontiguousarray(np.asarray(weights, dtype=np.float64))
+        h = ctypes.c_void_p()
+        ctx._check(ctx.lib.litho_cache_create_band(
+            ctx.handle, N, K, Nr, Nc, row0, col0, kb.view(np.float64).reshape(-1).ctypes.data_as(_PD),
+            w.ctypes.data_as(_PD), float(ws_sum), ctypes.byref(h)))
+        return cls(h, ctx)
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.ctx.lib.litho_cache_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Field:
+    """Band-domain electric-field state of one imaging call (get_electric_field())."""
+
+    def __init__(self, cache: ImagingCache):
+        self.cache = cache
+        self.ctx = cache.ctx
+        h = ctypes.c_void_p()
+        self.ctx._check(self.ctx.lib.litho_field_create(self.ctx.handle, cache.handle, ctypes.byref(h)))
+        self.handle = h
+
+    def export(self, k: int):
+        """E_k at full resolution (complex64 N x N), centred like the reference's."""
+        torch = self.ctx.torch
+        N = self.cache.N
+        out = torch.empty((N, N, 2), dtype=torch.float32, device="cuda")
+        self.ctx._check(self.ctx.lib.litho_field_export(self.ctx.handle, self.handle, k, _ptr(out)))
+        return torch.view_as_complex(out)
+
+    def fields(self) -> List:
+        return [self.export(k) for k in range(self.cache.K)]
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.ctx.lib.litho_field_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+@dataclass
+class ImagingResult:
+    aerial_image: object
+    wafer_image: object
+
+
+class Imaging:
+    """Imaging (include/litho_model/imaging.h:16-53)."""
+
+    def __init__(self, cache: ImagingCache):
+        self.cache = cache
+        self.ctx = cache.ctx
+        self.field = Field(cache)
+
+    def compute(self, mask, threshold: float = 0.25, alpha: float = 50.0) -> ImagingResult:
+        """Imaging::compute (source/litho_model/imaging.cpp:60-171)."""
+        torch = self.ctx.torch
+        N = self.cache.N
+        m = _f32(mask, torch, (N, N), "Imaging: mask")
+        aerial = torch.empty((N, N), dtype=torch.float32, device="cuda")
+        wafer = torch.empty_like(aerial)
+        self.ctx._check(self.ctx.lib.litho_imaging_compute(
+            self.ctx.handle, self.cache.handle, _ptr(m), float(threshold), float(alpha),
+            _ptr(aerial), _ptr(wafer), self.field.handle))
+        return ImagingResult(aerial, wafer)
+
+    def get_electric_field(self) -> Field:
+        return self.field
+
+
+class Gradient:
+    """Gradient (include/utils/gradient.h:10-89)."""
+
+    def __init__(self, cache: ImagingCache, threshold: float, alpha: float):
+        self.cache = cache
+        self.ctx = cache.ctx
+        self.threshold = threshold
+        self.alpha = alpha
+        self.last_loss = None
+
+    def backpropagate(self, dLdI, field: Field, output_scale: float):
+        """Gradient::_backpropagate (source/utils/gradient.cpp:34-109)."""
+        torch = self.ctx.torch
+        N = self.cache.N
+        g = _f32(dLdI, torch, (N, N), "Gradient: dLdI")
+        out = torch.empty((N, N), dtype=torch.float32, device="cuda")
+        self.ctx._check(self.ctx.lib.litho_backpropagate(self.ctx.handle, field.handle, _ptr(g),
+                                                         float(output_scale), _ptr(out)))
+        return out
+
+    def _pe(self, wafer, target, field, pe_window=None, penalty_window=None, pe_weight=1.0,
+            penalty=0.0, penalty_threshold=0.01):
+        torch = self.ctx.torch
+        N = self.cache.N
+        w = _f32(wafer, torch, (N, N), "wafer_image")
+        t = _f32(target, torch, (N, N), "target_image")
+        pw = _f32(pe_window, torch, (N, N), "loss_window")
+        qw = _f32(penalty_window, torch, (N, N), "penalty_window")
+        opt = PeOptions(_ptr(pw), _ptr(qw), float(pe_weight), float(penalty), float(penalty_threshold))
+        out = torch.empty((N, N), dtype=torch.float32, device="cuda")
+        loss = ctypes.c_double()
+        self.ctx._check(self.ctx.lib.litho_pe_gradient(
+            self.ctx.handle, field.handle, _ptr(w), _ptr(t), ctypes.byref(opt), float(self.alpha),
+            _ptr(out), ctypes.byref(loss)))
+        self.last_loss = loss.value
+        return out
+
+    def pe_gradient(self, wafer_image, target_image, electric_field: Field, loss_window=None):
+        """Gradient::pe_gradient (gradient.cpp:121-141)."""
+        return self._pe(wafer_image, target_image, electric_field, pe_window=loss_window)
+
+    def pe_gradient_with_penalty(self, wafer_image, target_image, electric_field: Field, penalty,
+                                 penalty_threshold=0.01, loss_window=None, pe_weight=1.0,
+                                 penalty_window=None):
+        """Gradient::pe_gradient_with_penalty overloads (gradient.cpp:143-196)."""
+        return self._pe(wafer_image, target_image, electric_field, pe_window=loss_window,
+                        penalty_window=penalty_window, pe_weight=pe_weight, penalty=penalty,
+                        penalty_threshold=penalty_threshold)
+
+
+class Loss:
+    """Loss statics (include/utils/loss.h:38-113) evaluated on the device."""
+
+    @staticmethod
+    def _run(wafer, target, window=None, penalty=0.0, penalty_threshold=0.01, ctx=None):
+        ctx = ctx or default_context()
+        torch = ctx.torch
+        w = _f32(wafer, torch)
+        t = _f32(target, torch, tuple(w.shape), "target")
+        win = _f32(window, torch, tuple(w.shape), "loss_window")
+        opt = PeOptions(_ptr(win), None, 1.0, float(penalty), float(penalty_threshold))
+        out = ctypes.c_double()
+        ctx._check(ctx.lib.litho_pe_loss(ctx.handle, _ptr(w), _ptr(t), w.shape[0], w.shape[1],
+                                         ctypes.byref(opt), ctypes.byref(out)))
+        return out.value
+
+    @staticmethod
+    def pe_loss(wafer, target, loss_window=None, ctx=None) -> float:
+        return Loss._run(wafer, target, loss_window, ctx=ctx)
+
+    @staticmethod
+    def pe_loss_with_penalty(wafer, target, penalty, penalty_threshold, loss_window=None,
+                             ctx=None) -> float:
+        return Loss._run(wafer, target, loss_window, penalty, penalty_threshold, ctx=ctx)
+
+
+@dataclass
+class EvolveParams:
+    delta: object
+    H1_abs: object
+    H2_abs: object
+
+
+class LevelSetUtils:
+    """LevelSetUtils statics (include/utils/level_set_utils.h:14-33) on the device."""
+
+    @staticmethod
+    def evolve_normal_WENO_godunov(phi, Vn, dy, dx, ctx=None) -> EvolveParams:
+        ctx = ctx or default_context()
+        torch = ctx.torch
+        p = _f32(phi, torch)
+        v = _f32(Vn, torch)
+        if p.shape != v.shape:
+            raise LithoError(1, "evolve_normal_WENO_godunov: phi and Vn sizes must match")
+        if p.dim() != 2:
+            raise LithoError(2, "phi must be 2-D")
+        rows, cols = p.shape
+        delta = torch.empty_like(p)
+        h = torch.empty_like(p)
+        ctx._check(ctx.lib.litho_weno_godunov(ctx.handle, rows, cols, _ptr(p), _ptr(v), float(dy),
+                                              float(dx), _ptr(delta), _ptr(h)))
+        return EvolveParams(delta, h, h.clone())
+
+    @staticmethod
+    def evolve_kappa(phi, dx, dy, b, ctx=None):
+        ctx = ctx or default_context()
+        torch = ctx.torch
+        p = _f32(phi, torch)
+        out = torch.empty_like(p)
+        ctx._check(ctx.lib.litho_kappa(ctx.handle, p.shape[0], p.shape[1], _ptr(p), float(dx),
+                                       float(dy), float(b), _ptr(out)))
+        return out
+
+    @staticmethod
+    def evolution_term(phi, Vn, dx, dy, cfl, b, ctx=None):
+        """LSM_Optimizer::_caculate_evolution_term -> (normal, dt)."""
+        ctx = ctx or default_context()
+        torch = ctx.torch
+        p = _f32(phi, torch)
+        v = _f32(Vn, torch, tuple(p.shape), "Vn")
+        out = torch.empty_like(p)
+        dt = ctypes.c_double()
+        ctx._check(ctx.lib.litho_evolution_term(ctx.handle, p.shape[0], p.shape[1], _ptr(p), _ptr(v),
+                                                float(dx), float(dy), float(cfl), float(b),
+                                                _ptr(out), ctypes.byref(dt)))
+        return out, dt.value
+
+    @staticmethod
+    def rk2_update(phi, Vn, dx, dy, cfl, b, ctx=None):
+        """One RK2 update (LSM_Optimizer.cpp:109-115) -> (phi_next, mask, dt)."""
+        ctx = ctx or default_context()
+        torch = ctx.torch
+        p = _f32(phi, torch)
+        v = _f32(Vn, torch, tuple(p.shape), "Vn")
+        out = torch.empty_like(p)
+        mask = torch.empty_like(p)
+        dt = ctypes.c_double()
+        ctx._check(ctx.lib.litho_lsm_rk2_update(ctx.handle, p.shape[0], p.shape[1], _ptr(p), _ptr(v),
+                                                float(dx), float(dy), float(cfl), float(b),
+                                                _ptr(out), _ptr(mask), ctypes.byref(dt)))
+        return out, mask, dt.value
+
+
+class CTMOptimizer:
+    """CTM_Optimizer (source/optimizer/CTM_Optimizer.cpp) over the fused evaluation."""
+
+    def __init__(self, cache: ImagingCache, target, threshold, alpha, iterations, learning_rate=0.9,
+                 optimizer_method="lbfgs", lbfgs_history_size=10, gradient_tolerance=0.0):
+        if optimizer_method not in ("gradient_descent", "lbfgs"):
+            raise LithoError(1, "CTM optimizer must be gradient_descent or lbfgs")
+        if iterations <= 0:
+            raise LithoError(1, "CTM max_iteration must be positive")
+        if not (math.isfinite(learning_rate) and learning_rate > 0):
+            raise LithoError(1, "CTM learning_rate must be finite and positive")
+        if lbfgs_history_size <= 0:
+            raise LithoError(1, "CTM lbfgs_history_size must be positive")
+        if not (math.isfinite(gradient_tolerance) and gradient_tolerance >= 0):
+            raise LithoError(1, "CTM gradient_tolerance must be finite and non-negative")
+        self.cache = cache
+        self.ctx = cache.ctx
+        torch = self.ctx.torch
+        N = cache.N
+        self.target = _f32(target, torch, (N, N), "target")
+        self.threshold, self.alpha = float(threshold), float(alpha)
+        self.iterations = iterations
+        self.learning_rate = learning_rate
+        self.method = optimizer_method
+        self.m = lbfgs_history_size
+        self.tol = gradient_tolerance
+        self.field = Field(cache)
+        self.error_history: List[float] = []
+        self.grad_theta = torch.empty((N, N), dtype=torch.float32, device="cuda")
+        self.mask = torch.empty_like(self.grad_theta)
+
+    def initialize_theta(self):
+        """CTM_Optimizer::_initialize_theta (CTM_Optimizer.cpp:55-64)."""
+        torch = self.ctx.torch
+        pi = 3.14159265358979323846
+        return torch.where(self.target > 0, torch.full_like(self.target, 0.3 * pi),
+                           torch.full_like(self.target, 0.7 * pi))
+
+    def evaluate(self, theta, want_mask=False):
+        """CTM_Optimizer::_evaluate_theta_objective (CTM_Optimizer.cpp:175-187)."""
+        loss = ctypes.c_double()
+        norm = ctypes.c_double()
+        self.ctx._check(self.ctx.lib.litho_ctm_evaluate(
+            self.ctx.handle, self.cache.handle, self.field.handle, _ptr(theta), _ptr(self.target),
+            self.threshold, self.alpha, _ptr(self.mask) if want_mask else None, None, None, None,
+            _ptr(self.grad_theta), ctypes.byref(loss), ctypes.byref(norm)))
+        return loss.value, self.grad_theta, norm.value
+
+    def optimize(self):
+        return self._lbfgs() if self.method == "lbfgs" else self._gd()
+
+    def _gd(self):
+        """_optimize_gradient_descent (CTM_Optimizer.cpp:109-173)."""
+        torch = self.ctx.torch
+        self.error_history = []
+        theta = self.initialize_theta()
+        best_mask = 0.5 * (1.0 + torch.cos(theta))
+        min_pe = float("inf")
+        for _ in range(self.iterations):
+            pe, gt, norm = self.evaluate(theta, want_mask=True)
+            self.error_history.append(pe)
+            if pe < min_pe:
+                min_pe = pe
+                best_mask = self.mask.clone()
+            if norm <= self.tol:
+                break
+            theta = theta - self.learning_rate * gt
+        self.theta = theta
+        return best_mask
+
+    def _lbfgs(self):
+        """optimize_lbfgs (CTM_Optimizer.cpp:189-227): L-BFGS with FP64 two-loop scalars."""
+        from .lbfgs import minimize_lbfgs
+        torch = self.ctx.torch
+        self.error_history = []
+        theta = self.initialize_theta()
+
+        def fg(x):
+            pe, gt, norm = self.evaluate(x)
+            self.error_history.append(pe)
+            return pe, gt.clone(), norm
+
+        theta, self.lbfgs_info = minimize_lbfgs(fg, theta, m=self.m, epsilon=self.tol,
+                                                max_iterations=self.iterations)
+        self.theta = theta
+        return 0.5 * (1.0 + torch.cos(theta))

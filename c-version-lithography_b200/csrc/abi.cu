@@ -1,0 +1,973 @@
+// C ABI of the imaging-and-gradient library: contexts, optical caches, fields
+// and the entry points declared in include/litho_b200.h. Host-side
+// orchestration of the band-DFT kernels (band_dft.cu) and the level-set
+// kernels (levelset.cu).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "litho_internal.cuh"
+
+using namespace litho_b200;
+
+struct litho_ctx : public Context {};
+struct litho_cache : public Cache {};
+struct litho_field : public Field {};
+
+namespace {
+
+constexpr double kTwoPi = 6.283185307179586476925286766559;
+
+size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+int round16(int v) { return (v + 15) / 16 * 16; }
+
+// e^{sign 2 pi i (f * j mod P) / P}, exact integer phase reduction in FP64.
+void twiddle(long long f, long long j, long long P, double sign, double* re, double* im) {
+  long long p = ((f % P) + P) % P;
+  p = (p * (j % P)) % P;
+  const double a = sign * kTwoPi * (double)p / (double)P;
+  *re = std::cos(a);
+  *im = std::sin(a);
+}
+
+template <class T>
+int upload(Context* ctx, T** dst, const std::vector<T>& src) {
+  if (cudaMalloc(reinterpret_cast<void**>(dst), src.size() * sizeof(T)) != cudaSuccess) {
+    cudaGetLastError();
+    return ctx->fail(LITHO_ERR_OOM, "device allocation of an optical table failed");
+  }
+  if (cudaMemcpy(*dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice) !=
+      cudaSuccess)
+    return ctx->fail(LITHO_ERR_CUDA, "upload of an optical table failed");
+  return LITHO_OK;
+}
+
+void free_cache(Cache* c) {
+  void* ptrs[] = {c->H,    c->w,    c->TXS,  c->TXD,   c->TYS,   c->TYD,   c->AYS,
+                  c->AYD,  c->TXSc, c->TXDc, c->ESr_t, c->ESc_t, c->ESc,   c->EDr_t,
+                  c->EDc_t};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+}
+
+// Scratch layout of one imaging + adjoint evaluation.
+struct Layout {
+  size_t R, mpart, gpart, T, ik, Q, chat, Ut, Vt, dldi, Gam, gam, Z1, Zk, X, phi1, rows_tmp,
+      total;
+  int ks, ys;
+};
+
+Layout make_layout(const BandGeom& g) {
+  Layout L{};
+  const int N = g.N;
+  // Split of the row analyses over x and of the column contractions over y,
+  // sized for about two waves of the 148 SMs.
+  const int rowblocks = (N + 127) / 128;
+  const int ks_req = std::max(1, std::min((296 + rowblocks - 1) / rowblocks, std::max(1, N / 64)));
+  int kps = 0;
+  row_split(N, ks_req, &kps, &L.ks);  // L.ks: the chunk count the row analysis produces
+  L.ys = std::max(1, std::min(32, N / 32));
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    const size_t o = off;
+    off = align_up(off + bytes, 256);
+    return o;
+  };
+  L.R = take((size_t)L.ks * N * 2 * g.Nc * sizeof(float));
+  L.mpart = take((size_t)L.ys * g.Nr * g.Nc * sizeof(float2));
+  L.gpart = take((size_t)L.ys * (2 * g.Nr - 1) * g.Nc * sizeof(float2));
+  L.T = take((size_t)g.K * g.Nr * g.Pc * sizeof(float2));
+  L.ik = take((size_t)g.K * g.Pr * g.Pc * sizeof(float));
+  L.Q = take((size_t)g.Pr * (2 * g.Nc - 1) * sizeof(float2));
+  L.chat = take((size_t)g.Nr * (2 * g.Nc - 1) * sizeof(float2));
+  L.Ut = take((size_t)N * g.kp_rows * sizeof(float));
+  L.Vt = take((size_t)N * g.kp_rows * sizeof(float));
+  L.dldi = take((size_t)N * N * sizeof(float));
+  L.Gam = take((size_t)(2 * g.Nr - 1) * g.Pc * sizeof(float2));
+  L.gam = take((size_t)g.Pr * g.Pc * sizeof(float));
+  L.Z1 = take((size_t)g.K * g.Pr * g.Nc * sizeof(float2));
+  L.Zk = take((size_t)g.K * g.Nr * g.Nc * sizeof(float2));
+  L.X = take((size_t)g.Nr * g.Nc * sizeof(float2));
+  L.phi1 = 0;
+  L.rows_tmp = take((size_t)g.Nr * N * sizeof(float2));
+  L.total = off;
+  return L;
+}
+
+template <class T>
+T* at(const Context* ctx, size_t off) {
+  return reinterpret_cast<T*>(static_cast<char*>(ctx->scratch.base) + off);
+}
+
+bool finite_all(const double* p, size_t n) {
+  for (size_t i = 0; i < n; ++i)
+    if (!std::isfinite(p[i])) return false;
+  return true;
+}
+
+// Reduction slots in ctx->d_red: [0] flag (as int), partial sums after 8.
+constexpr int RED_FLAG = 0;
+constexpr int RED_SUM = 2;    // summed results (up to 4 doubles)
+constexpr int RED_PART = 8;   // per-block partials
+
+}  // namespace
+
+int Context::ensure_scratch(size_t bytes) {
+  if (scratch.bytes >= bytes) return LITHO_OK;
+  if (scratch.base) {
+    cudaStreamSynchronize(stream);
+    cudaFree(scratch.base);
+    scratch.base = nullptr;
+    scratch.bytes = 0;
+  }
+  if (cudaMalloc(&scratch.base, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(LITHO_ERR_OOM, "scratch allocation of " + std::to_string(bytes) + " bytes failed");
+  }
+  scratch.bytes = bytes;
+  return LITHO_OK;
+}
+
+int Context::ensure_red(size_t n) {
+  if (red_cap >= n) return LITHO_OK;
+  if (d_red) {
+    cudaStreamSynchronize(stream);
+    cudaFree(d_red);
+    d_red = nullptr;
+  }
+  if (cudaMalloc(&d_red, n * sizeof(double)) != cudaSuccess) {
+    cudaGetLastError();
+    red_cap = 0;
+    return fail(LITHO_ERR_OOM, "reduction buffer allocation failed");
+  }
+  red_cap = n;
+  return LITHO_OK;
+}
+
+void Context::collect_stages() {
+  for (int i = 0; i < LITHO_NUM_STAGES; ++i) {
+    if (!ev_pending[i]) continue;
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, ev[i][0], ev[i][1]) == cudaSuccess) {
+      stage_ms[i] += ms;
+      stage_count[i] += 1;
+    } else {
+      cudaGetLastError();
+    }
+    ev_pending[i] = false;
+  }
+}
+
+// ============================================================== ABI
+extern "C" {
+
+int litho_version(void) { return 1; }
+
+const char* litho_status_string(int s) {
+  switch (s) {
+    case LITHO_OK: return "ok";
+    case LITHO_ERR_INVALID_ARGUMENT: return "invalid argument";
+    case LITHO_ERR_SHAPE: return "shape mismatch";
+    case LITHO_ERR_NONFINITE: return "non-finite input";
+    case LITHO_ERR_OOM: return "out of device memory";
+    case LITHO_ERR_CUDA: return "CUDA error";
+    case LITHO_ERR_NOT_READY: return "field not computed";
+    case LITHO_ERR_UNSUPPORTED: return "unsupported";
+    default: return "unknown status";
+  }
+}
+
+const char* litho_ctx_last_error(const litho_ctx* ctx) {
+  return ctx ? ctx->last_error.c_str() : "null context";
+}
+
+int litho_ctx_create(int device, void* stream, litho_ctx** out) {
+  if (!out) return LITHO_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+    cudaGetLastError();
+    return LITHO_ERR_CUDA;
+  }
+  if (cudaSetDevice(device) != cudaSuccess) return LITHO_ERR_CUDA;
+  litho_ctx* c = new (std::nothrow) litho_ctx();
+  if (!c) return LITHO_ERR_OOM;
+  c->device = device;
+  if (stream) {
+    c->stream = static_cast<cudaStream_t>(stream);
+  } else {
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+      delete c;
+      return LITHO_ERR_CUDA;
+    }
+    c->own_stream = true;
+  }
+  if (cudaMallocHost(reinterpret_cast<void**>(&c->h_red), 64 * sizeof(double)) != cudaSuccess) {
+    if (c->own_stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return LITHO_ERR_OOM;
+  }
+  *out = c;
+  return LITHO_OK;
+}
+
+int litho_ctx_destroy(litho_ctx* ctx) {
+  if (!ctx) return LITHO_OK;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  if (ctx->scratch.base) cudaFree(ctx->scratch.base);
+  if (ctx->d_red) cudaFree(ctx->d_red);
+  if (ctx->h_red) cudaFreeHost(ctx->h_red);
+  for (int i = 0; i < LITHO_NUM_STAGES; ++i)
+    for (int j = 0; j < 2; ++j)
+      if (ctx->ev[i][j]) cudaEventDestroy(ctx->ev[i][j]);
+  if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return LITHO_OK;
+}
+
+int litho_ctx_synchronize(litho_ctx* ctx) {
+  if (!ctx) return LITHO_ERR_INVALID_ARGUMENT;
+  LITHO_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  return LITHO_OK;
+}
+
+int litho_ctx_set_precision(litho_ctx* ctx, int precision) {
+  if (!ctx) return LITHO_ERR_INVALID_ARGUMENT;
+  if (precision != LITHO_PRECISION_FP32)
+    return ctx->fail(LITHO_ERR_UNSUPPORTED, "precision mode not built");
+  ctx->precision = precision;
+  return LITHO_OK;
+}
+
+long long litho_ctx_launch_count(const litho_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+int litho_ctx_enable_stage_timing(litho_ctx* ctx, int on) {
+  if (!ctx) return LITHO_ERR_INVALID_ARGUMENT;
+  if (cudaSetDevice(ctx->device) != cudaSuccess) return LITHO_ERR_CUDA;
+  if (on && !ctx->ev[0][0]) {
+    for (int i = 0; i < LITHO_NUM_STAGES; ++i)
+      for (int j = 0; j < 2; ++j)
+        if (cudaEventCreate(&ctx->ev[i][j]) != cudaSuccess)
+          return ctx->fail(LITHO_ERR_CUDA, "cudaEventCreate failed");
+  }
+  ctx->timing = on != 0;
+  for (int i = 0; i < LITHO_NUM_STAGES; ++i) {
+    ctx->stage_ms[i] = 0.0;
+    ctx->stage_count[i] = 0;
+    ctx->ev_pending[i] = false;
+  }
+  return LITHO_OK;
+}
+
+int litho_ctx_stage_times(const litho_ctx* ctx, double* ms, long long* counts) {
+  if (!ctx) return LITHO_ERR_INVALID_ARGUMENT;
+  for (int i = 0; i < LITHO_NUM_STAGES; ++i) {
+    if (ms) ms[i] = ctx->stage_ms[i];
+    if (counts) counts[i] = ctx->stage_count[i];
+  }
+  return LITHO_OK;
+}
+
+// ---------------------------------------------------------------- cache
+int litho_cache_create_band(litho_ctx* ctx, int N, int K, int Nr, int Nc, int row0, int col0,
+                            const double* kb, const double* weights, double ws_sum,
+                            litho_cache** out) {
+  if (!ctx || !out) return LITHO_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  if (N <= 0) return ctx->fail(LITHO_ERR_INVALID_ARGUMENT, "Imaging: cache.N must be positive");
+  if (K <= 0 || !kb || !weights)
+    return ctx->fail(LITHO_ERR_INVALID_ARGUMENT, "Imaging: no optical kernels available");
+  if (Nr <= 0 || Nc <= 0 || Nr > N || Nc > N)
+    return ctx->fail(LITHO_ERR_SHAPE, "band size must be within 1..N");
+  if (!std::isfinite(ws_sum) || ws_sum <= 0.0)
+    return ctx->fail(LITHO_ERR_INVALID_ARGUMENT,
+                     "Imaging: source weights must be finite, nonnegative, and have a positive sum");
+  for (int k = 0; k < K; ++k)
+    if (!std::isfinite(weights[k]) || weights[k] < 0.0)
+      return ctx->fail(LITHO_ERR_INVALID_ARGUMENT,
+                       "Imaging: SOCS values must be finite and nonnegative");
+  if (!finite_all(kb, (size_t)K * Nr * Nc * 2))
+    return ctx->fail(LITHO_ERR_NONFINITE, "optical kernels must be finite");
+  if (cudaSetDevice(ctx->device) != cudaSuccess) return LITHO_ERR_CUDA;
+
+  litho_cache* c = new (std::nothrow) litho_cache();
+  if (!c) return LITHO_ERR_OOM;
+  c->device = ctx->device;
+  BandGeom& g = c->g;
+  g.N = N; g.K = K; g.Nr = Nr; g.Nc = Nc; g.row0 = row0; g.col0 = col0;
+  g.Pr = 2 * Nr; g.Pc = 2 * Nc;
+  g.kp_rows = round16(2 * Nr);
+  g.kp_cols = 2 * Nc;
+
+  std::vector<float2> H((size_t)K * Nr * Nc);
+  for (size_t i = 0; i < H.size(); ++i) H[i] = make_float2((float)kb[2 * i], (float)kb[2 * i + 1]);
+  c->w_host.resize(K);
+  std::vector<float> w(K);
+  for (int k = 0; k < K; ++k) {
+    c->w_host[k] = weights[k] / ws_sum;
+    w[k] = (float)c->w_host[k];
+  }
+  double re, im;
+  std::vector<float> TXS((size_t)2 * Nc * N), TXD((size_t)2 * Nc * N);
+  std::vector<float2> TXSc((size_t)Nc * N), TXDc((size_t)Nc * N);
+  for (int cidx = 0; cidx < Nc; ++cidx)
+    for (int x = 0; x < N; ++x) {
+      twiddle(col0 + cidx, x, N, -1.0, &re, &im);
+      TXS[(size_t)(2 * cidx) * N + x] = (float)re;
+      TXS[(size_t)(2 * cidx + 1) * N + x] = (float)im;
+      TXSc[(size_t)cidx * N + x] = make_float2((float)re, (float)im);
+      twiddle(cidx, x, N, -1.0, &re, &im);
+      TXD[(size_t)(2 * cidx) * N + x] = (float)re;
+      TXD[(size_t)(2 * cidx + 1) * N + x] = (float)im;
+      TXDc[(size_t)cidx * N + x] = make_float2((float)re, (float)im);
+    }
+  std::vector<float2> TYS((size_t)Nr * N), TYD((size_t)Nr * N);
+  std::vector<float> AYS((size_t)N * g.kp_rows, 0.f), AYD((size_t)N * g.kp_rows, 0.f);
+  for (int r = 0; r < Nr; ++r)
+    for (int y = 0; y < N; ++y) {
+      twiddle(row0 + r, y, N, -1.0, &re, &im);
+      TYS[(size_t)r * N + y] = make_float2((float)re, (float)im);
+      AYS[(size_t)y * g.kp_rows + 2 * r] = (float)re;
+      AYS[(size_t)y * g.kp_rows + 2 * r + 1] = (float)im;
+      twiddle(r, y, N, -1.0, &re, &im);
+      TYD[(size_t)r * N + y] = make_float2((float)re, (float)im);
+      AYD[(size_t)y * g.kp_rows + 2 * r] = (float)re;
+      AYD[(size_t)y * g.kp_rows + 2 * r + 1] = (float)im;
+    }
+  std::vector<float2> ESr_t((size_t)Nr * g.Pr), ESc_t((size_t)Nc * g.Pc), ESc((size_t)g.Pc * Nc);
+  std::vector<float2> EDr_t((size_t)(2 * Nr - 1) * g.Pr), EDc_t((size_t)(2 * Nc - 1) * g.Pc);
+  for (int r = 0; r < Nr; ++r)
+    for (int j = 0; j < g.Pr; ++j) {
+      twiddle(row0 + r, j, g.Pr, 1.0, &re, &im);
+      ESr_t[(size_t)r * g.Pr + j] = make_float2((float)re, (float)im);
+    }
+  for (int cidx = 0; cidx < Nc; ++cidx)
+    for (int j = 0; j < g.Pc; ++j) {
+      twiddle(col0 + cidx, j, g.Pc, 1.0, &re, &im);
+      ESc_t[(size_t)cidx * g.Pc + j] = make_float2((float)re, (float)im);
+      ESc[(size_t)j * Nc + cidx] = make_float2((float)re, (float)im);
+    }
+  for (int a = 0; a < 2 * Nr - 1; ++a)
+    for (int j = 0; j < g.Pr; ++j) {
+      twiddle(a - (Nr - 1), j, g.Pr, 1.0, &re, &im);
+      EDr_t[(size_t)a * g.Pr + j] = make_float2((float)re, (float)im);
+    }
+  for (int a = 0; a < 2 * Nc - 1; ++a)
+    for (int j = 0; j < g.Pc; ++j) {
+      twiddle(a - (Nc - 1), j, g.Pc, 1.0, &re, &im);
+      EDc_t[(size_t)a * g.Pc + j] = make_float2((float)re, (float)im);
+    }
+  int st = LITHO_OK;
+  if (st == LITHO_OK) st = upload(ctx, &c->H, H);
+  if (st == LITHO_OK) st = upload(ctx, &c->w, w);
+  if (st == LITHO_OK) st = upload(ctx, &c->TXS, TXS);
+  if (st == LITHO_OK) st = upload(ctx, &c->TXD, TXD);
+  if (st == LITHO_OK) st = upload(ctx, &c->TXSc, TXSc);
+  if (st == LITHO_OK) st = upload(ctx, &c->TXDc, TXDc);
+  if (st == LITHO_OK) st = upload(ctx, &c->TYS, TYS);
+  if (st == LITHO_OK) st = upload(ctx, &c->TYD, TYD);
+  if (st == LITHO_OK) st = upload(ctx, &c->AYS, AYS);
+  if (st == LITHO_OK) st = upload(ctx, &c->AYD, AYD);
+  if (st == LITHO_OK) st = upload(ctx, &c->ESr_t, ESr_t);
+  if (st == LITHO_OK) st = upload(ctx, &c->ESc_t, ESc_t);
+  if (st == LITHO_OK) st = upload(ctx, &c->ESc, ESc);
+  if (st == LITHO_OK) st = upload(ctx, &c->EDr_t, EDr_t);
+  if (st == LITHO_OK) st = upload(ctx, &c->EDc_t, EDc_t);
+  if (st != LITHO_OK) {
+    free_cache(c);
+    delete c;
+    return st;
+  }
+  *out = c;
+  return LITHO_OK;
+}
+
+// Smallest wrapped range of indices holding every flagged entry: the
+// complement of the longest circular run of unflagged entries.
+static void wrapped_range(const std::vector<char>& nz, int N, int* start, int* len) {
+  int best = 0, best_end = -1, run = 0;
+  for (int j = 0; j < 2 * N; ++j) {
+    if (!nz[j % N]) {
+      ++run;
+      if (run > best && run < N) { best = run; best_end = j; }
+    } else {
+      run = 0;
+    }
+  }
+  if (best == 0) {  // every index used
+    *start = -(N / 2);
+    *len = N;
+    return;
+  }
+  int s = (best_end + 1) % N;
+  *len = N - best;
+  *start = s <= N / 2 ? s : s - N;
+}
+
+int litho_cache_create_dense(litho_ctx* ctx, int N, int K, const double* kernels,
+                             const double* weights, double ws_sum, litho_cache** out) {
+  if (!ctx || !out) return LITHO_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  if (N <= 0) return ctx->fail(LITHO_ERR_INVALID_ARGUMENT, "Imaging: cache.N must be positive");
+  if (K <= 0 || !kernels)
+    return ctx->fail(LITHO_ERR_INVALID_ARGUMENT, "Imaging: no optical kernels available");
+  const size_t nn = (size_t)N * N;
+  if (!finite_all(kernels, (size_t)K * nn * 2))
+    return ctx->fail(LITHO_ERR_NONFINITE, "optical kernels must be finite");
+  // Coefficients below 1e-12 of the largest magnitude (SVD round-off outside the
+  // pupil support) are treated as zero; float32 cannot resolve them anyway.
+  double amax = 0.0;
+  for (size_t i = 0; i < (size_t)K * nn; ++i)
+    amax = std::max(amax, std::hypot(kernels[2 * i], kernels[2 * i + 1]));
+  const double tol = amax * 1e-12;
+  std::vector<char> nzr(N, 0), nzc(N, 0);
+  for (int k = 0; k < K; ++k)
+    for (int r = 0; r < N; ++r)
+      for (int cc = 0; cc < N; ++cc) {
+        const size_t i = ((size_t)k * N + r) * N + cc;
+        if (std::hypot(kernels[2 * i], kernels[2 * i + 1]) > tol) { nzr[r] = 1; nzc[cc] = 1; }
+      }
+  int row0, Nr, col0, Nc;
+  wrapped_range(nzr, N, &row0, &Nr);
+  wrapped_range(nzc, N, &col0, &Nc);
+  if (Nr == 0 || Nc == 0) { row0 = 0; Nr = 1; col0 = 0; Nc = 1; }
+  std::vector<double> band((size_t)K * Nr * Nc * 2);
+  for (int k = 0; k < K; ++k)
+    for (int r = 0; r < Nr; ++r)
+      for (int cc = 0; cc < Nc; ++cc) {
+        const int R = ((row0 + r) % N + N) % N, C = ((col0 + cc) % N + N) % N;
+        const size_t src = ((size_t)k * N + R) * N + C;
+        const size_t dst = ((size_t)k * Nr + r) * Nc + cc;
+        band[2 * dst] = kernels[2 * src];
+        band[2 * dst + 1] = kernels[2 * src + 1];
+      }
+  return litho_cache_create_band(ctx, N, K, Nr, Nc, row0, col0, band.data(), weights, ws_sum,
+                                 out);
+}
+
+int litho_cache_info(const litho_cache* c, int* N, int* K, int* Nr, int* Nc, int* row0,
+                     int* col0) {
+  if (!c) return LITHO_ERR_INVALID_ARGUMENT;
+  if (N) *N = c->g.N;
+  if (K) *K = c->g.K;
+  if (Nr) *Nr = c->g.Nr;
+  if (Nc) *Nc = c->g.Nc;
+  if (row0) *row0 = c->g.row0;
+  if (col0) *col0 = c->g.col0;
+  return LITHO_OK;
+}
+
+int litho_cache_destroy(litho_cache* c) {
+  if (!c) return LITHO_OK;
+  cudaSetDevice(c->device);
+  cudaDeviceSynchronize();
+  free_cache(c);
+  delete c;
+  return LITHO_OK;
+}
+
+// ---------------------------------------------------------------- field
+int litho_field_create(litho_ctx* ctx, const litho_cache* cache, litho_field** out) {
+  if (!ctx || !cache || !out) return LITHO_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  litho_field* f = new (std::nothrow) litho_field();
+  if (!f) return LITHO_ERR_OOM;
+  f->cache = cache;
+  const BandGeom& g = cache->g;
+  if (cudaMalloc(&f->mband, (size_t)g.Nr * g.Nc * sizeof(float2)) != cudaSuccess ||
+      cudaMalloc(&f->e, (size_t)g.K * g.Pr * g.Pc * sizeof(float2)) != cudaSuccess) {
+    cudaGetLastError();
+    if (f->mband) cudaFree(f->mband);
+    delete f;
+    return ctx->fail(LITHO_ERR_OOM, "field allocation failed");
+  }
+  *out = f;
+  return LITHO_OK;
+}
+
+int litho_field_destroy(litho_field* f) {
+  if (!f) return LITHO_OK;
+  cudaDeviceSynchronize();
+  if (f->mband) cudaFree(f->mband);
+  if (f->e) cudaFree(f->e);
+  delete f;
+  return LITHO_OK;
+}
+
+}  // extern "C"
+
+// ============================================================== orchestration
+namespace {
+
+int check_launch(Context* ctx, cudaError_t e, const char* what) {
+  if (e != cudaSuccess) return ctx->fail(LITHO_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+  return LITHO_OK;
+}
+
+// Forward: row analysis -> column contraction -> small-grid band stage -> row
+// synthesis with the fused resist epilogue. input_mode 1 reads theta.
+int run_forward(Context* ctx, const Cache& c, Field& f, const Layout& L, int input_mode,
+                const float* input, float* mask_out, ResistEpilogue ep, int* nblocks) {
+  const BandGeom& g = c.g;
+  cudaStream_t s = ctx->stream;
+  int* flag = reinterpret_cast<int*>(ctx->d_red + RED_FLAG);
+  int st;
+  ctx->stage_begin(0);
+  st = check_launch(ctx, launch_analysis_rows(s, input_mode, input, mask_out, flag, c.TXS, g.N,
+                                              g.Nc, L.ks, at<float>(ctx, L.R)),
+                    "row analysis");
+  ctx->stage_end(0);
+  if (st) return st;
+  ctx->stage_begin(1);
+  st = check_launch(ctx, launch_analysis_cols(s, at<float>(ctx, L.R), L.ks, g.N, g.Nc, c.TYS,
+                                              g.Nr, g.Nr, 0, L.ys, 1.f / ((float)g.N * g.N),
+                                              at<float2>(ctx, L.mpart)),
+                    "column contraction");
+  ctx->stage_end(1);
+  if (st) return st;
+  ctx->stage_begin(2);
+  st = check_launch(ctx, launch_band_forward(s, c, at<float2>(ctx, L.mpart), L.ys, f,
+                                             at<float>(ctx, L.ik), at<float2>(ctx, L.T),
+                                             at<float2>(ctx, L.Q), at<float2>(ctx, L.chat),
+                                             at<float>(ctx, L.Ut)),
+                    "band forward");
+  ctx->stage_end(2);
+  if (st) return st;
+  ctx->stage_begin(3);
+  st = check_launch(ctx, launch_synth_resist(s, c.AYD, at<float>(ctx, L.Ut), g.N, g.kp_rows, ep,
+                                             nblocks),
+                    "row synthesis");
+  ctx->stage_end(3);
+  ctx->launches += 8;
+  f.valid = (st == LITHO_OK);
+  return st;
+}
+
+int run_adjoint(Context* ctx, const Cache& c, const Field& f, const Layout& L, const float* dldi,
+                double scale, GradEpilogue ep, int* nblocks) {
+  const BandGeom& g = c.g;
+  cudaStream_t s = ctx->stream;
+  int* flag = reinterpret_cast<int*>(ctx->d_red + RED_FLAG);
+  int st;
+  ctx->stage_begin(4);
+  st = check_launch(ctx, launch_analysis_rows(s, 0, dldi, nullptr, flag, c.TXD, g.N, g.Nc, L.ks,
+                                              at<float>(ctx, L.R)),
+                    "adjoint row analysis");
+  ctx->stage_end(4);
+  if (st) return st;
+  ctx->stage_begin(5);
+  st = check_launch(ctx, launch_analysis_cols(s, at<float>(ctx, L.R), L.ks, g.N, g.Nc, c.TYD,
+                                              2 * g.Nr - 1, g.Nr, 1, L.ys,
+                                              1.f / ((float)g.N * g.N), at<float2>(ctx, L.gpart)),
+                    "adjoint column contraction");
+  ctx->stage_end(5);
+  if (st) return st;
+  ctx->stage_begin(6);
+  st = check_launch(ctx, launch_band_adjoint(s, c, f, at<float2>(ctx, L.gpart), L.ys, scale,
+                                             at<float2>(ctx, L.Gam), at<float>(ctx, L.gam),
+                                             at<float2>(ctx, L.Z1), at<float2>(ctx, L.Zk),
+                                             at<float2>(ctx, L.X), at<float>(ctx, L.Vt)),
+                    "band adjoint");
+  ctx->stage_end(6);
+  if (st) return st;
+  ctx->stage_begin(7);
+  st = check_launch(ctx, launch_synth_grad(s, c.AYS, at<float>(ctx, L.Vt), g.N, g.kp_rows, ep,
+                                           nblocks),
+                    "adjoint row synthesis");
+  ctx->stage_end(7);
+  ctx->launches += 9;
+  return st;
+}
+
+int prepare(Context* ctx, const Cache& c, Layout* L) {
+  if (cudaSetDevice(ctx->device) != cudaSuccess) return ctx->fail(LITHO_ERR_CUDA, "cudaSetDevice");
+  *L = make_layout(c.g);
+  int st = ctx->ensure_scratch(L->total);
+  if (st) return st;
+  const int blocks = ((c.g.N + 127) / 128) * ((c.g.N + 127) / 128);
+  st = ctx->ensure_red(RED_PART + 3 * (size_t)blocks + 1200);
+  if (st) return st;
+  LITHO_CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_red, 0, RED_PART * sizeof(double), ctx->stream));
+  return LITHO_OK;
+}
+
+// Copies n summed doubles (and the flag) back to the host and waits.
+int fetch(Context* ctx, int n) {
+  LITHO_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->h_red, ctx->d_red, (RED_SUM + n) * sizeof(double),
+                                      cudaMemcpyDeviceToHost, ctx->stream));
+  LITHO_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  ctx->collect_stages();
+  return LITHO_OK;
+}
+
+bool flag_set(const Context* ctx) {
+  int v;
+  std::memcpy(&v, ctx->h_red + RED_FLAG, sizeof(int));
+  return v != 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int litho_imaging_compute(litho_ctx* ctx, const litho_cache* cache, const float* d_mask,
+                          double threshold, double alpha, float* d_aerial, float* d_wafer,
+                          litho_field* field) {
+  if (!ctx || !cache || !d_mask) return LITHO_ERR_INVALID_ARGUMENT;
+  if (!std::isfinite(threshold) || !std::isfinite(alpha))
+    return ctx->fail(LITHO_ERR_NONFINITE, "Imaging: mask, threshold, and alpha must be finite");
+  if (field && field->cache != cache)
+    return ctx->fail(LITHO_ERR_INVALID_ARGUMENT, "field belongs to another cache");
+  Layout L;
+  int st = prepare(ctx, *cache, &L);
+  if (st) return st;
+  Field tmp;
+  Field* f = field;
+  float2* tmp_e = nullptr;
+  float2* tmp_m = nullptr;
+  if (!f) {  // a throw-away field lives in the adjoint part of the scratch
+    const BandGeom& g = cache->g;
+    if (cudaMalloc(&tmp_e, (size_t)g.K * g.Pr * g.Pc * sizeof(float2)) != cudaSuccess ||
+        cudaMalloc(&tmp_m, (size_t)g.Nr * g.Nc * sizeof(float2)) != cudaSuccess) {
+      cudaGetLastError();
+      if (tmp_e) cudaFree(tmp_e);
+      return ctx->fail(LITHO_ERR_OOM, "temporary field allocation failed");
+    }
+    tmp.cache = cache; tmp.e = tmp_e; tmp.mband = tmp_m;
+    f = &tmp;
+  }
+  f->valid = false;
+  ResistEpilogue ep{};
+  ep.mode = 0;
+  ep.thr = (float)threshold;
+  ep.alpha = (float)alpha;
+  ep.aerial = d_aerial;
+  ep.wafer = d_wafer;
+  int nb = 0;
+  st = run_forward(ctx, *cache, *f, L, 0, d_mask, nullptr, ep, &nb);
+  if (!st) st = fetch(ctx, 0);
+  if (tmp_e) { cudaFree(tmp_e); cudaFree(tmp_m); }
+  if (st) return st;
+  if (flag_set(ctx)) {
+    f->valid = false;
+    return ctx->fail(LITHO_ERR_NONFINITE, "Imaging: mask, threshold, and alpha must be finite");
+  }
+  return LITHO_OK;
+}
+
+int litho_backpropagate(litho_ctx* ctx, const litho_field* field, const float* d_dLdI,
+                        double output_scale, float* d_grad) {
+  if (!ctx || !field || !d_dLdI || !d_grad) return LITHO_ERR_INVALID_ARGUMENT;
+  if (!field->valid) return ctx->fail(LITHO_ERR_NOT_READY, "Gradient: field not computed");
+  const Cache& c = *field->cache;
+  Layout L;
+  int st = prepare(ctx, c, &L);
+  if (st) return st;
+  GradEpilogue ep{};
+  ep.grad_mask = d_grad;
+  int nb = 0;
+  st = run_adjoint(ctx, c, *field, L, d_dLdI, output_scale, ep, &nb);
+  if (!st) st = fetch(ctx, 0);
+  if (st) return st;
+  if (flag_set(ctx)) return ctx->fail(LITHO_ERR_NONFINITE, "Gradient: dLdI must be finite");
+  return LITHO_OK;
+}
+
+int litho_pe_loss(litho_ctx* ctx, const float* d_wafer, const float* d_target, int rows,
+                  int cols, const litho_pe_options* opt, double* loss) {
+  if (!ctx || !d_wafer || !d_target || !loss || rows <= 0 || cols <= 0)
+    return LITHO_ERR_INVALID_ARGUMENT;
+  if (cudaSetDevice(ctx->device) != cudaSuccess) return LITHO_ERR_CUDA;
+  int st = ctx->ensure_red(RED_PART + 2 * 600);
+  if (st) return st;
+  litho_pe_options o{nullptr, nullptr, 1.0, 0.0, 0.01};
+  if (opt) o = *opt;
+  int nb = 0;
+  st = check_launch(ctx,
+                    launch_pe_loss(ctx->stream, d_wafer, d_target, o.pe_window, o.penalty_window,
+                                   (float)o.penalty, (float)o.penalty_threshold,
+                                   (size_t)rows * cols, ctx->d_red + RED_PART, &nb),
+                    "pe loss");
+  if (st) return st;
+  st = check_launch(ctx, launch_sum_partials(ctx->stream, ctx->d_red + RED_PART, nb, 2,
+                                             ctx->d_red + RED_SUM),
+                    "sum");
+  if (st) return st;
+  ctx->launches += 2;
+  st = fetch(ctx, 2);
+  if (st) return st;
+  // pe_weight * Loss::pe_loss + penalty * Loss::background_penalty_loss; with
+  // pe_weight 1 this is Loss::pe_loss_with_penalty (loss.cpp:25-51).
+  *loss = o.pe_weight * ctx->h_red[RED_SUM] + o.penalty * ctx->h_red[RED_SUM + 1];
+  return LITHO_OK;
+}
+
+int litho_pe_gradient(litho_ctx* ctx, const litho_field* field, const float* d_wafer,
+                      const float* d_target, const litho_pe_options* opt, double alpha,
+                      float* d_grad, double* loss) {
+  if (!ctx || !field || !d_wafer || !d_target || !d_grad) return LITHO_ERR_INVALID_ARGUMENT;
+  if (!field->valid) return ctx->fail(LITHO_ERR_NOT_READY, "Gradient: field not computed");
+  const Cache& c = *field->cache;
+  Layout L;
+  int st = prepare(ctx, c, &L);
+  if (st) return st;
+  litho_pe_options o{nullptr, nullptr, 1.0, 0.0, 0.01};
+  if (opt) o = *opt;
+  const int N = c.g.N;
+  int nb = 0;
+  st = check_launch(ctx,
+                    launch_pe_dldi(ctx->stream, d_wafer, d_target, o.pe_window, o.penalty_window,
+                                   (float)o.pe_weight, (float)o.penalty,
+                                   (float)o.penalty_threshold, (size_t)N * N,
+                                   at<float>(ctx, L.dldi), ctx->d_red + RED_PART, &nb),
+                    "dL/dI");
+  if (st) return st;
+  st = check_launch(ctx, launch_sum_partials(ctx->stream, ctx->d_red + RED_PART, nb, 2,
+                                             ctx->d_red + RED_SUM),
+                    "sum");
+  if (st) return st;
+  ctx->launches += 2;
+  GradEpilogue ep{};
+  ep.grad_mask = d_grad;
+  int nb2 = 0;
+  st = run_adjoint(ctx, c, *field, L, at<float>(ctx, L.dldi), 4.0 * alpha, ep, &nb2);
+  if (!st) st = fetch(ctx, 2);
+  if (st) return st;
+  if (loss) *loss = o.pe_weight * ctx->h_red[RED_SUM] + o.penalty * ctx->h_red[RED_SUM + 1];
+  return LITHO_OK;
+}
+
+int litho_ctm_evaluate(litho_ctx* ctx, const litho_cache* cache, litho_field* field,
+                       const float* d_theta, const float* d_target, double threshold,
+                       double alpha, float* d_mask, float* d_aerial, float* d_wafer,
+                       float* d_grad_mask, float* d_grad_theta, double* loss,
+                       double* grad_norm) {
+  if (!ctx || !cache || !d_theta || !d_target || !d_grad_theta) return LITHO_ERR_INVALID_ARGUMENT;
+  if (!std::isfinite(threshold) || !std::isfinite(alpha))
+    return ctx->fail(LITHO_ERR_NONFINITE, "Imaging: mask, threshold, and alpha must be finite");
+  if (field && field->cache != cache)
+    return ctx->fail(LITHO_ERR_INVALID_ARGUMENT, "field belongs to another cache");
+  Layout L;
+  int st = prepare(ctx, *cache, &L);
+  if (st) return st;
+  Field tmp;
+  Field* f = field;
+  float2* tmp_e = nullptr;
+  float2* tmp_m = nullptr;
+  if (!f) {
+    const BandGeom& g = cache->g;
+    if (cudaMalloc(&tmp_e, (size_t)g.K * g.Pr * g.Pc * sizeof(float2)) != cudaSuccess ||
+        cudaMalloc(&tmp_m, (size_t)g.Nr * g.Nc * sizeof(float2)) != cudaSuccess) {
+      cudaGetLastError();
+      if (tmp_e) cudaFree(tmp_e);
+      return ctx->fail(LITHO_ERR_OOM, "temporary field allocation failed");
+    }
+    tmp.cache = cache; tmp.e = tmp_e; tmp.mband = tmp_m;
+    f = &tmp;
+  }
+  const int N = cache->g.N;
+  ResistEpilogue ep{};
+  ep.mode = 1;
+  ep.thr = (float)threshold;
+  ep.alpha = (float)alpha;
+  ep.aerial = d_aerial;
+  ep.wafer = d_wafer;
+  ep.target = d_target;
+  ep.pe_weight = 1.f;
+  ep.penalty = 0.f;
+  ep.pen_thr = 0.01f;
+  ep.dldi = at<float>(ctx, L.dldi);
+  ep.loss_partial = ctx->d_red + RED_PART;
+  int nb = 0;
+  st = run_forward(ctx, *cache, *f, L, 1, d_theta, d_mask, ep, &nb);
+  if (!st)
+    st = check_launch(ctx, launch_sum_partials(ctx->stream, ctx->d_red + RED_PART, nb, 2,
+                                               ctx->d_red + RED_SUM),
+                      "sum");
+  GradEpilogue gp{};
+  gp.grad_mask = d_grad_mask;
+  gp.theta = d_theta;
+  gp.grad_theta = d_grad_theta;
+  gp.norm_partial = ctx->d_red + RED_PART + 2 * (size_t)nb;
+  int nb2 = 0;
+  if (!st) st = run_adjoint(ctx, *cache, *f, L, at<float>(ctx, L.dldi), 4.0 * alpha, gp, &nb2);
+  if (!st)
+    st = check_launch(ctx, launch_sum_partials(ctx->stream, gp.norm_partial, nb2, 1,
+                                               ctx->d_red + RED_SUM + 2),
+                      "sum");
+  ctx->launches += 2;
+  if (!st) st = fetch(ctx, 3);
+  if (tmp_e) { cudaFree(tmp_e); cudaFree(tmp_m); }
+  if (st) return st;
+  if (flag_set(ctx)) {
+    f->valid = false;
+    return ctx->fail(LITHO_ERR_NONFINITE, "theta must be finite");
+  }
+  (void)N;
+  if (loss) *loss = ctx->h_red[RED_SUM];
+  if (grad_norm) *grad_norm = std::sqrt(ctx->h_red[RED_SUM + 2]);
+  return LITHO_OK;
+}
+
+int litho_ctm_evaluate_host(litho_ctx* ctx, const litho_cache* cache, litho_field* field,
+                            const float* h_theta, const float* h_target, double threshold,
+                            double alpha, float* h_grad_theta, double* loss,
+                            double* grad_norm) {
+  if (!ctx || !cache || !h_theta || !h_target || !h_grad_theta) return LITHO_ERR_INVALID_ARGUMENT;
+  const size_t n = (size_t)cache->g.N * cache->g.N;
+  float *d = nullptr;
+  if (cudaSetDevice(ctx->device) != cudaSuccess) return LITHO_ERR_CUDA;
+  if (cudaMallocAsync(reinterpret_cast<void**>(&d), 3 * n * sizeof(float), ctx->stream) !=
+      cudaSuccess) {
+    cudaGetLastError();
+    return ctx->fail(LITHO_ERR_OOM, "host-call staging allocation failed");
+  }
+  int st = LITHO_OK;
+  if (cudaMemcpyAsync(d, h_theta, n * sizeof(float), cudaMemcpyHostToDevice, ctx->stream) !=
+          cudaSuccess ||
+      cudaMemcpyAsync(d + n, h_target, n * sizeof(float), cudaMemcpyHostToDevice, ctx->stream) !=
+          cudaSuccess)
+    st = ctx->fail(LITHO_ERR_CUDA, "host to device copy failed");
+  if (!st)
+    st = litho_ctm_evaluate(ctx, cache, field, d, d + n, threshold, alpha, nullptr, nullptr,
+                            nullptr, nullptr, d + 2 * n, loss, grad_norm);
+  if (!st && cudaMemcpyAsync(h_grad_theta, d + 2 * n, n * sizeof(float), cudaMemcpyDeviceToHost,
+                             ctx->stream) != cudaSuccess)
+    st = ctx->fail(LITHO_ERR_CUDA, "device to host copy failed");
+  cudaFreeAsync(d, ctx->stream);
+  if (cudaStreamSynchronize(ctx->stream) != cudaSuccess && !st)
+    st = ctx->fail(LITHO_ERR_CUDA, "stream synchronize failed");
+  return st;
+}
+
+int litho_field_export(litho_ctx* ctx, const litho_field* field, int k, float* d_E) {
+  if (!ctx || !field || !d_E) return LITHO_ERR_INVALID_ARGUMENT;
+  if (!field->valid) return ctx->fail(LITHO_ERR_NOT_READY, "field not computed");
+  const Cache& c = *field->cache;
+  if (k < 0 || k >= c.g.K) return ctx->fail(LITHO_ERR_INVALID_ARGUMENT, "kernel index out of range");
+  Layout L;
+  int st = prepare(ctx, c, &L);
+  if (st) return st;
+  st = check_launch(ctx, launch_export_field(ctx->stream, c, *field, k, at<float2>(ctx, L.rows_tmp),
+                                             reinterpret_cast<float2*>(d_E)),
+                    "field export");
+  ctx->launches += 2;
+  if (!st) LITHO_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  return st;
+}
+
+// ---------------------------------------------------------------- level set
+static int ls_check(litho_ctx* ctx, int rows, int cols, double dx, double dy, int minsz) {
+  if (rows <= 0 || cols <= 0 || !(dx > 0.0) || !(dy > 0.0))
+    return ctx->fail(LITHO_ERR_INVALID_ARGUMENT,
+                     "evolve_normal_WENO_godunov: grid must be non-empty and dx/dy must be positive");
+  if (rows < minsz || cols < minsz)
+    return ctx->fail(LITHO_ERR_SHAPE, "curvature needs at least 3 rows and 3 columns");
+  if (cudaSetDevice(ctx->device) != cudaSuccess) return ctx->fail(LITHO_ERR_CUDA, "cudaSetDevice");
+  return LITHO_OK;
+}
+
+int litho_weno_godunov(litho_ctx* ctx, int rows, int cols, const float* d_phi, const float* d_vn,
+                       double dy, double dx, float* d_delta, float* d_habs) {
+  if (!ctx || !d_phi || !d_vn || !d_delta) return LITHO_ERR_INVALID_ARGUMENT;
+  int st = ls_check(ctx, rows, cols, dx, dy, 1);
+  if (st) return st;
+  st = check_launch(ctx, launch_levelset(ctx->stream, 0, rows, cols, d_phi, nullptr, d_vn,
+                                         (float)dx, (float)dy, 0.f, nullptr, d_delta, d_habs),
+                    "weno godunov");
+  ctx->launches += 1;
+  if (!st) LITHO_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  return st;
+}
+
+int litho_kappa(litho_ctx* ctx, int rows, int cols, const float* d_phi, double dx, double dy,
+                double b, float* d_out) {
+  if (!ctx || !d_phi || !d_out) return LITHO_ERR_INVALID_ARGUMENT;
+  int st = ls_check(ctx, rows, cols, dx, dy, 3);
+  if (st) return st;
+  st = check_launch(ctx, launch_levelset(ctx->stream, 1, rows, cols, d_phi, nullptr, nullptr,
+                                         (float)dx, (float)dy, (float)b, nullptr, d_out, nullptr),
+                    "kappa");
+  ctx->launches += 1;
+  if (!st) LITHO_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  return st;
+}
+
+static int ls_dt(litho_ctx* ctx, int rows, int cols, const float* d_vn, double dx, double dy,
+                 double cfl, double b, float** dt_dev) {
+  int st = ctx->ensure_red(RED_PART + 2 * 600);
+  if (st) return st;
+  LITHO_CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_red, 0, RED_PART * sizeof(double), ctx->stream));
+  float* part = reinterpret_cast<float*>(ctx->d_red + RED_PART);
+  float* vmax = reinterpret_cast<float*>(ctx->d_red + RED_SUM);
+  float* dt = vmax + 1;
+  st = check_launch(ctx, launch_dt(ctx->stream, d_vn, (size_t)rows * cols, (float)dx, (float)dy,
+                                   (float)cfl, (float)b, part, vmax, dt,
+                                   reinterpret_cast<int*>(ctx->d_red + RED_FLAG)),
+                    "dt");
+  ctx->launches += 2;
+  *dt_dev = dt;
+  return st;
+}
+
+int litho_evolution_term(litho_ctx* ctx, int rows, int cols, const float* d_phi,
+                         const float* d_vn, double dx, double dy, double cfl, double b,
+                         float* d_normal, double* dt) {
+  if (!ctx || !d_phi || !d_vn || !d_normal) return LITHO_ERR_INVALID_ARGUMENT;
+  int st = ls_check(ctx, rows, cols, dx, dy, 3);
+  if (st) return st;
+  float* dtd = nullptr;
+  st = ls_dt(ctx, rows, cols, d_vn, dx, dy, cfl, b, &dtd);
+  if (st) return st;
+  st = check_launch(ctx, launch_levelset(ctx->stream, 2, rows, cols, d_phi, nullptr, d_vn,
+                                         (float)dx, (float)dy, (float)b, dtd, d_normal, nullptr),
+                    "evolution");
+  ctx->launches += 1;
+  if (!st) st = fetch(ctx, 1);
+  if (st) return st;
+  if (flag_set(ctx)) return ctx->fail(LITHO_ERR_NONFINITE, "normal speed must be finite");
+  float h[2];
+  std::memcpy(h, ctx->h_red + RED_SUM, sizeof(h));
+  if (dt) *dt = h[1];
+  return LITHO_OK;
+}
+
+int litho_lsm_rk2_update(litho_ctx* ctx, int rows, int cols, const float* d_phi,
+                         const float* d_vn, double dx, double dy, double cfl, double b,
+                         float* d_phi_out, float* d_mask, double* dt) {
+  if (!ctx || !d_phi || !d_vn || !d_phi_out) return LITHO_ERR_INVALID_ARGUMENT;
+  int st = ls_check(ctx, rows, cols, dx, dy, 3);
+  if (st) return st;
+  const size_t n = (size_t)rows * cols;
+  st = ctx->ensure_scratch(n * sizeof(float));
+  if (st) return st;
+  float* phi1 = static_cast<float*>(ctx->scratch.base);
+  float* dtd = nullptr;
+  st = ls_dt(ctx, rows, cols, d_vn, dx, dy, cfl, b, &dtd);
+  if (st) return st;
+  ctx->stage_begin(8);
+  st = check_launch(ctx, launch_levelset(ctx->stream, 3, rows, cols, d_phi, nullptr, d_vn,
+                                         (float)dx, (float)dy, (float)b, dtd, phi1, nullptr),
+                    "rk2 stage 1");
+  if (!st)
+    st = check_launch(ctx, launch_levelset(ctx->stream, 4, rows, cols, phi1, d_phi, d_vn,
+                                           (float)dx, (float)dy, (float)b, dtd, d_phi_out, d_mask),
+                      "rk2 stage 2");
+  ctx->stage_end(8);
+  ctx->launches += 2;
+  if (!st) st = fetch(ctx, 1);
+  if (st) return st;
+  if (flag_set(ctx)) return ctx->fail(LITHO_ERR_NONFINITE, "normal speed must be finite");
+  float h[2];
+  std::memcpy(h, ctx->h_red + RED_SUM, sizeof(h));
+  if (dt) *dt = h[1];
+  return LITHO_OK;
+}
+
+}  // extern "C"

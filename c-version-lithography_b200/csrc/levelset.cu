@@ -1,0 +1,244 @@
+// WENO5-Godunov level-set kernels (source/utils/level_set_utils.cpp of the
+// reference) as shared-memory-tiled stencils.
+//
+// Boundary handling: the reference edge-pads phi by 3 on both axes and
+// der_weno5 pads by 3 more along the derivative axis; edge padding twice is
+// edge padding once by 6, and after cropping the output pixel (i, j) reads
+// phi[i][clamp(j-3 .. j+3)] and phi[clamp(i-3 .. i+3)][j]. The tile loader
+// therefore clamps every halo index into the image.
+#include <cuda_runtime.h>
+#include <cfloat>
+
+#include "litho_internal.cuh"
+
+namespace litho_b200 {
+
+constexpr int LS_TX = 32;      // tile width (x, columns)
+constexpr int LS_TY = 8;       // tile height (y, rows); each thread computes 2 rows
+constexpr int LS_RPT = 2;
+constexpr int LS_H = 3;        // halo
+constexpr int LS_SW = LS_TX + 2 * LS_H;
+constexpr int LS_SH = LS_TY * LS_RPT + 2 * LS_H;
+constexpr int LS_NT = LS_TX * LS_TY;
+
+// WENO5-JS one-sided derivative from the five differences v1..v5 (already
+// divided by the spacing), level_set_utils.cpp:45-113. The smoothness
+// indicators are scaled by 1/max(v^2) before forming the weights: the weights
+// are invariant under that scaling (eps = 1e-6 max v^2 scales the same way) and
+// the scaled values stay inside FP32 range.
+__device__ __forceinline__ float weno5(float v1, float v2, float v3, float v4, float v5) {
+  const float d1 = (1.f / 3.f) * v1 - (7.f / 6.f) * v2 + (11.f / 6.f) * v3;
+  const float d2 = -(1.f / 6.f) * v2 + (5.f / 6.f) * v3 + (1.f / 3.f) * v4;
+  const float d3 = (1.f / 3.f) * v3 + (5.f / 6.f) * v4 - (1.f / 6.f) * v5;
+  const float vmax2 = fmaxf(fmaxf(fmaxf(v1 * v1, v2 * v2), fmaxf(v3 * v3, v4 * v4)), v5 * v5);
+  if (!(vmax2 > 0.f)) return 0.f;  // all differences zero: every candidate is zero
+  const float t1 = v1 - 2.f * v2 + v3;
+  const float t2 = v2 - 2.f * v3 + v4;
+  const float t3 = v3 - 2.f * v4 + v5;
+  const float q1 = v1 - 4.f * v2 + 3.f * v3;
+  const float q2 = v2 - v4;
+  const float q3 = 3.f * v3 - 4.f * v4 + v5;
+  const float inv = 1.f / vmax2;
+  const float S1 = ((13.f / 12.f) * t1 * t1 + 0.25f * q1 * q1) * inv + 1e-6f;
+  const float S2 = ((13.f / 12.f) * t2 * t2 + 0.25f * q2 * q2) * inv + 1e-6f;
+  const float S3 = ((13.f / 12.f) * t3 * t3 + 0.25f * q3 * q3) * inv + 1e-6f;
+  const float a1 = 0.1f / (S1 * S1);
+  const float a2 = 0.6f / (S2 * S2);
+  const float a3 = 0.3f / (S3 * S3);
+  return (a1 * d1 + a2 * d2 + a3 * d3) / (a1 + a2 + a3);
+}
+
+// Godunov |grad phi| for the sign of the normal speed (level_set_utils.cpp:180-213).
+__device__ __forceinline__ float godunov(float speed, float xm, float xp, float ym, float yp) {
+  float gx2 = 0.f, gy2 = 0.f;
+  if (speed > 0.f) {
+    const float a = fmaxf(xm, 0.f), b = fminf(xp, 0.f);
+    const float c = fmaxf(ym, 0.f), d = fminf(yp, 0.f);
+    gx2 = fmaxf(a * a, b * b);
+    gy2 = fmaxf(c * c, d * d);
+  } else if (speed < 0.f) {
+    const float a = fminf(xm, 0.f), b = fmaxf(xp, 0.f);
+    const float c = fminf(ym, 0.f), d = fmaxf(yp, 0.f);
+    gx2 = fmaxf(a * a, b * b);
+    gy2 = fmaxf(c * c, d * d);
+  }
+  return sqrtf(gx2 + gy2);
+}
+
+__device__ __forceinline__ void load_tile(float (*t)[LS_SW], const float* __restrict__ phi,
+                                          int rows, int cols, int y0, int x0) {
+  for (int e = threadIdx.x; e < LS_SH * LS_SW; e += LS_NT) {
+    const int ty = e / LS_SW, tx = e % LS_SW;
+    const int y = min(max(y0 - LS_H + ty, 0), rows - 1);
+    const int x = min(max(x0 - LS_H + tx, 0), cols - 1);
+    t[ty][tx] = __ldg(phi + (size_t)y * cols + x);
+  }
+}
+
+// delta = Vn |grad phi|_G at tile pixel (ly, lx) (tile coordinates include the halo).
+__device__ __forceinline__ float weno_delta(const float (*t)[LS_SW], int ly, int lx, float speed,
+                                            float idx, float idy) {
+  float d[6];
+#pragma unroll
+  for (int q = 0; q < 6; ++q) d[q] = (t[ly][lx - 2 + q] - t[ly][lx - 3 + q]) * idx;
+  // minus: D(j-3..j+1) = d[0..4]; plus: mirrored d[5..1]
+  const float xm = weno5(d[0], d[1], d[2], d[3], d[4]);
+  const float xp = weno5(d[5], d[4], d[3], d[2], d[1]);
+#pragma unroll
+  for (int q = 0; q < 6; ++q) d[q] = (t[ly - 2 + q][lx] - t[ly - 3 + q][lx]) * idy;
+  const float ym = weno5(d[0], d[1], d[2], d[3], d[4]);
+  const float yp = weno5(d[5], d[4], d[3], d[2], d[1]);
+  return speed * godunov(speed, xm, xp, ym, yp);
+}
+
+// _gradient_1d along x (level_set_utils.cpp:228-255) at global column x of row ly.
+__device__ __forceinline__ float grad_x(const float (*t)[LS_SW], int ly, int lx, int x, int cols,
+                                        float inv2d) {
+  if (x == 0) return (-3.f * t[ly][lx] + 4.f * t[ly][lx + 1] - t[ly][lx + 2]) * inv2d;
+  if (x == cols - 1) return (3.f * t[ly][lx] - 4.f * t[ly][lx - 1] + t[ly][lx - 2]) * inv2d;
+  return (t[ly][lx + 1] - t[ly][lx - 1]) * inv2d;
+}
+__device__ __forceinline__ float grad_y(const float (*t)[LS_SW], int ly, int lx, int y, int rows,
+                                        float inv2d) {
+  if (y == 0) return (-3.f * t[ly][lx] + 4.f * t[ly + 1][lx] - t[ly + 2][lx]) * inv2d;
+  if (y == rows - 1) return (3.f * t[ly][lx] - 4.f * t[ly - 1][lx] + t[ly - 2][lx]) * inv2d;
+  return (t[ly + 1][lx] - t[ly - 1][lx]) * inv2d;
+}
+
+// b * kappa |grad phi| (level_set_utils.cpp:257-278) at global (y, x).
+__device__ float kappa_term(const float (*t)[LS_SW], int ly, int lx, int y, int x, int rows,
+                            int cols, float dx, float dy, float b) {
+  const float ix = 1.f / (2.f * dx), iy = 1.f / (2.f * dy);
+  // phi_x at (y, x) and its row/column neighbours used by the second derivatives.
+  auto px_at = [&](int oy, int ox) { return grad_x(t, ly + oy, lx + ox, x + ox, cols, ix); };
+  auto py_at = [&](int oy) { return grad_y(t, ly + oy, lx, y + oy, rows, iy); };
+  const float px = px_at(0, 0);
+  const float py = py_at(0);
+  float pxy, pxx, pyy;
+  if (y == 0) pxy = (-3.f * px + 4.f * px_at(1, 0) - px_at(2, 0)) * iy;
+  else if (y == rows - 1) pxy = (3.f * px - 4.f * px_at(-1, 0) + px_at(-2, 0)) * iy;
+  else pxy = (px_at(1, 0) - px_at(-1, 0)) * iy;
+  if (x == 0) pxx = (-3.f * px + 4.f * px_at(0, 1) - px_at(0, 2)) * ix;
+  else if (x == cols - 1) pxx = (3.f * px - 4.f * px_at(0, -1) + px_at(0, -2)) * ix;
+  else pxx = (px_at(0, 1) - px_at(0, -1)) * ix;
+  if (y == 0) pyy = (-3.f * py + 4.f * py_at(1) - py_at(2)) * iy;
+  else if (y == rows - 1) pyy = (3.f * py - 4.f * py_at(-1) + py_at(-2)) * iy;
+  else pyy = (py_at(1) - py_at(-1)) * iy;
+  const float g2 = px * px + py * py;
+  const float num = pxx * py * py - 2.f * px * py * pxy + pyy * px * px;
+  return g2 > (float)DBL_EPSILON ? b * (num / g2) : 0.f;
+}
+
+__device__ float block_max(float v, float* sh) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+  __syncthreads();
+  float r = 0.f;
+  if (threadIdx.x == 0)
+    for (int w = 0; w < LS_NT / 32; ++w) r = fmaxf(r, sh[w]);
+  __syncthreads();
+  return r;
+}
+
+// what: 0 = delta (+ habs), 1 = kappa term, 2 = normal = kappa - delta,
+// 3 = RK2 stage 1: out = phi0 + dt N(phi0), 4 = RK2 stage 2:
+// out = 0.5 phi0 + 0.5 (phi1 + dt N(phi1)), mask_out = out >= 0.
+struct LsArgs {
+  int rows, cols, what;
+  const float* phi;   // field whose stencil is evaluated
+  const float* phi0;  // stage 2: the step's starting phi
+  const float* vn;
+  float dx, dy, b;
+  const float* dt;    // device scalar (stages)
+  float* out;
+  float* out2;        // habs (what 0) or mask (what 4)
+};
+
+__global__ void __launch_bounds__(LS_NT) levelset_kernel(LsArgs a) {
+  __shared__ float t[LS_SH][LS_SW];
+  const int x0 = blockIdx.x * LS_TX;
+  const int y0 = blockIdx.y * LS_TY * LS_RPT;
+  load_tile(t, a.phi, a.rows, a.cols, y0, x0);
+  __syncthreads();
+  const float idx = 1.f / a.dx, idy = 1.f / a.dy;
+  const float dt = (a.what >= 3) ? *a.dt : 0.f;
+  const int lx = threadIdx.x % LS_TX;
+  for (int r = 0; r < LS_RPT; ++r) {
+    const int ly = threadIdx.x / LS_TX + r * LS_TY;
+    const int y = y0 + ly, x = x0 + lx;
+    if (y >= a.rows || x >= a.cols) continue;
+    const size_t i = (size_t)y * a.cols + x;
+    const float speed = a.what == 1 ? 0.f : __ldg(a.vn + i);
+    float v;
+    if (a.what == 0) {
+      v = weno_delta(t, ly + LS_H, lx + LS_H, speed, idx, idy);
+      if (a.out2) a.out2[i] = fabsf(speed);
+    } else if (a.what == 1) {
+      v = kappa_term(t, ly + LS_H, lx + LS_H, y, x, a.rows, a.cols, a.dx, a.dy, a.b);
+    } else {
+      const float n = kappa_term(t, ly + LS_H, lx + LS_H, y, x, a.rows, a.cols, a.dx, a.dy, a.b) -
+                      weno_delta(t, ly + LS_H, lx + LS_H, speed, idx, idy);
+      if (a.what == 2) {
+        v = n;
+      } else if (a.what == 3) {
+        v = t[ly + LS_H][lx + LS_H] + dt * n;
+      } else {
+        v = 0.5f * __ldg(a.phi0 + i) + 0.5f * (t[ly + LS_H][lx + LS_H] + dt * n);
+        if (a.out2) a.out2[i] = v >= 0.f ? 1.f : 0.f;
+      }
+    }
+    a.out[i] = v;
+  }
+}
+
+static dim3 ls_grid(int rows, int cols) {
+  return dim3((cols + LS_TX - 1) / LS_TX, (rows + LS_TY * LS_RPT - 1) / (LS_TY * LS_RPT));
+}
+
+cudaError_t launch_levelset(cudaStream_t s, int what, int rows, int cols, const float* phi,
+                            const float* phi0, const float* vn, float dx, float dy, float b,
+                            const float* dt, float* out, float* out2) {
+  LsArgs a{rows, cols, what, phi, phi0, vn, dx, dy, b, dt, out, out2};
+  levelset_kernel<<<ls_grid(rows, cols), LS_NT, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+// max |Vn| partials then dt = get_dt_normal_kappa (level_set_utils.cpp:280-288).
+__global__ void __launch_bounds__(LS_NT) absmax_kernel(const float* __restrict__ v, size_t n,
+                                                       float* __restrict__ part, int* bad) {
+  __shared__ float sh[LS_NT / 32];
+  float m = 0.f;
+  bool nonfinite = false;
+  for (size_t i = (size_t)blockIdx.x * LS_NT + threadIdx.x; i < n; i += (size_t)gridDim.x * LS_NT) {
+    const float a = v[i];
+    nonfinite |= !isfinite(a);
+    m = fmaxf(m, fabsf(a));
+  }
+  if (nonfinite && bad) atomicOr(bad, 1);
+  const float r = block_max(m, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = r;
+}
+
+__global__ void dt_kernel(const float* __restrict__ part, int n, float dx, float dy, float cfl,
+                          float b, float* __restrict__ vmax, float* __restrict__ dt) {
+  if (threadIdx.x != 0) return;
+  float m = 0.f;
+  for (int i = 0; i < n; ++i) m = fmaxf(m, part[i]);
+  const double normal = (double)m / dx + (double)m / dy;
+  const double kap = (double)b * (1.0 / ((double)dx * dx) + 1.0 / ((double)dy * dy)) * 2.0;
+  const double den = normal + kap;
+  *vmax = m;
+  *dt = den < 1e-9 ? 1e-3f : (float)(cfl / den);
+}
+
+cudaError_t launch_dt(cudaStream_t s, const float* vn, size_t n, float dx, float dy, float cfl,
+                      float b, float* part, float* vmax, float* dt, int* bad) {
+  int nb = (int)((n + LS_NT - 1) / LS_NT);
+  if (nb > 296) nb = 296;
+  absmax_kernel<<<nb, LS_NT, 0, s>>>(vn, n, part, bad);
+  dt_kernel<<<1, 32, 0, s>>>(part, nb, dx, dy, cfl, b, vmax, dt);
+  return cudaGetLastError();
+}
+
+}  // namespace litho_b200

@@ -1,0 +1,195 @@
+/*
+ * litho_b200.h - C ABI of the B200 imaging-and-gradient library.
+ *
+ * Drop-in boundary for the hot path of wyhcoder/C-version-Lithography:
+ *   SOCS/Abbe aerial image  I = sum_k w_k |IFFT(H_k . FFT(M))|^2 / sum(ws),
+ *   sigmoid resist          W = 1 / (1 + exp(-alpha (I - thr))),
+ *   pattern-error loss      PE = sum (W - T)^2 (+ background penalty),
+ *   its adjoint             dPE/dM and dPE/dtheta through M = (1 + cos theta)/2,
+ *   WENO5-Godunov level-set update (RK2) used by LSM and full-chip LSM.
+ *
+ * Conventions
+ *   - Every entry point returns an int status (LITHO_OK == 0) and never throws.
+ *     litho_ctx_last_error() gives a message for the last failure on a context.
+ *   - Images are float32, row-major (row = y, col = x), N x N, in DEVICE memory
+ *     unless the name ends in _host. Eigen's default column-major matrices map
+ *     onto these by transposition (Eigen::Map<Matrix<float,-1,-1,RowMajor>>).
+ *   - Kernels and weights cross the boundary in float64, as the reference's
+ *     ImagingCache holds them; the library keeps them in float32 on the device.
+ *   - A context owns one CUDA stream and its scratch memory and is used by one
+ *     host thread at a time (the reference uses one Imaging/Gradient object per
+ *     thread, include/utils/micro_gradient_exchange.h:131-138).
+ *   - Caches must outlive the fields created from them (the reference's
+ *     Imaging holds a const reference to its ImagingCache, imaging.h:42).
+ */
+#ifndef LITHO_B200_H
+#define LITHO_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------ status codes */
+#define LITHO_OK 0
+#define LITHO_ERR_INVALID_ARGUMENT 1 /* std::invalid_argument in the reference */
+#define LITHO_ERR_SHAPE 2            /* dimension mismatch */
+#define LITHO_ERR_NONFINITE 3        /* NaN/Inf in an input that must be finite */
+#define LITHO_ERR_OOM 4              /* device allocation failed */
+#define LITHO_ERR_CUDA 5             /* CUDA runtime error */
+#define LITHO_ERR_NOT_READY 6        /* a field used before imaging filled it */
+#define LITHO_ERR_UNSUPPORTED 7      /* size or option outside what is built */
+
+#define LITHO_PRECISION_FP32 0       /* plain FP32 DFT passes (SIMT) */
+
+typedef struct litho_ctx litho_ctx;
+typedef struct litho_cache litho_cache;
+typedef struct litho_field litho_field;
+
+int litho_version(void);
+const char* litho_status_string(int status);
+const char* litho_ctx_last_error(const litho_ctx* ctx);
+
+/* ------------------------------------------------------------ context
+ * stream: a cudaStream_t to run on, or NULL for a stream the context creates.
+ */
+int litho_ctx_create(int device, void* stream, litho_ctx** out);
+int litho_ctx_destroy(litho_ctx* ctx);
+int litho_ctx_synchronize(litho_ctx* ctx);
+int litho_ctx_set_precision(litho_ctx* ctx, int precision);
+/* Kernels this context has launched so far (a counter, for benchmarks). */
+long long litho_ctx_launch_count(const litho_ctx* ctx);
+
+/* Per-stage device timing with CUDA events on the context's stream. Stages:
+ * 0 row analysis (mask), 1 column contraction, 2 band forward (small grid),
+ * 3 row synthesis + resist/loss epilogue, 4 row analysis (dL/dI),
+ * 5 column contraction (adjoint), 6 band adjoint, 7 row synthesis + theta chain,
+ * 8 level-set stencil. ms[i] accumulates milliseconds, counts[i] launches of
+ * stage i since timing was enabled (enabling resets both). */
+#define LITHO_NUM_STAGES 9
+int litho_ctx_enable_stage_timing(litho_ctx* ctx, int on);
+int litho_ctx_stage_times(const litho_ctx* ctx, double* ms, long long* counts);
+
+/* ------------------------------------------------------------ optical cache
+ * Replaces ImagingCache (include/litho_model/litho_prepare.h:18-47) as consumed
+ * by Imaging (source/litho_model/imaging.cpp:60-107) and Gradient
+ * (source/utils/gradient.cpp:34-55).
+ *
+ * litho_cache_create_dense: the reference's own layout. kernels = K full N x N
+ *   complex frequency kernels with DC at index (0,0) (the layout of
+ *   ImagingCache::optical_kernels_frequency), interleaved (re, im) float64,
+ *   row-major [k][row][col][2]. weights = socs_eigenvalues (SOCS) or source_ws
+ *   (Abbe), ws_sum = source_ws.sum(). The band support (the smallest wrapped
+ *   row and column ranges holding every nonzero coefficient) is detected here.
+ * litho_cache_create_band: the same kernels given only on their support, K x Nr
+ *   x Nc, where band row r holds integer frequency row0 + r (mod N) and band
+ *   column c holds col0 + c (mod N); row0/col0 may be negative.
+ * Errors mirror imaging.cpp:68-107: K == 0, non-finite or negative weights,
+ * ws_sum <= 0 give LITHO_ERR_INVALID_ARGUMENT.
+ */
+int litho_cache_create_dense(litho_ctx* ctx, int N, int K, const double* kernels,
+                             const double* weights, double ws_sum, litho_cache** out);
+int litho_cache_create_band(litho_ctx* ctx, int N, int K, int Nr, int Nc, int row0, int col0,
+                            const double* kernels_band, const double* weights, double ws_sum,
+                            litho_cache** out);
+int litho_cache_info(const litho_cache* cache, int* N, int* K, int* Nr, int* Nc, int* row0,
+                     int* col0);
+int litho_cache_destroy(litho_cache* cache);
+
+/* ------------------------------------------------------------ field
+ * The band-domain electric-field state of one imaging call. It replaces
+ * Imaging::get_electric_field() (include/litho_model/imaging.h:34-36): the
+ * reference hands K full N x N complex fields to Gradient::pe_gradient; here
+ * the exact band representation is kept and litho_field_export rebuilds E_k
+ * (centred exactly like the reference's fields) when a caller needs it.
+ */
+int litho_field_create(litho_ctx* ctx, const litho_cache* cache, litho_field** out);
+int litho_field_destroy(litho_field* field);
+/* E_k as interleaved (re, im) float32, N x N row-major, device memory. */
+int litho_field_export(litho_ctx* ctx, const litho_field* field, int k, float* d_E);
+
+/* ------------------------------------------------------------ imaging
+ * Imaging::compute (source/litho_model/imaging.cpp:60-171). aerial / wafer may
+ * be NULL. field (may be NULL) receives the state Gradient needs.
+ */
+int litho_imaging_compute(litho_ctx* ctx, const litho_cache* cache, const float* d_mask,
+                          double threshold, double alpha, float* d_aerial, float* d_wafer,
+                          litho_field* field);
+
+/* ------------------------------------------------------------ adjoint
+ * Gradient::_backpropagate (source/utils/gradient.cpp:34-109):
+ *   grad = output_scale / sum(ws) * sum_k w_k Re IFFT(conj(H_k) FFT(E_k dLdI)).
+ */
+int litho_backpropagate(litho_ctx* ctx, const litho_field* field, const float* d_dLdI,
+                        double output_scale, float* d_grad);
+
+/* Options shared by the pe_gradient* and pe_loss* variants
+ * (source/utils/gradient.cpp:121-196, source/utils/loss.cpp:16-64):
+ *   dL/dI = [pe_weight (W-T) pe_window + penalty [T<0.5] max(W - pen_thr, 0)
+ *            penalty_window] W (1-W),  output_scale = 4 alpha.
+ * A NULL window is all ones; a NULL penalty_window uses pe_window, as the
+ * reference's single-window overloads do.
+ */
+typedef struct litho_pe_options {
+  const float* pe_window;
+  const float* penalty_window;
+  double pe_weight;         /* 1.0 for Gradient::pe_gradient */
+  double penalty;           /* 0.0 disables the background penalty */
+  double penalty_threshold; /* 0.01 is the reference's default */
+} litho_pe_options;
+
+/* pe_gradient / pe_gradient_with_penalty (gradient.cpp:121-196). opt may be
+ * NULL (plain PE). loss (host, nullable) receives the matching
+ * Loss::pe_loss / pe_loss_with_penalty value. */
+int litho_pe_gradient(litho_ctx* ctx, const litho_field* field, const float* d_wafer,
+                      const float* d_target, const litho_pe_options* opt, double alpha,
+                      float* d_grad, double* loss);
+
+/* Loss::pe_loss / pe_loss_with_penalty (source/utils/loss.cpp:16-51). */
+int litho_pe_loss(litho_ctx* ctx, const float* d_wafer, const float* d_target, int rows,
+                  int cols, const litho_pe_options* opt, double* loss);
+
+/* One CTM objective evaluation, fused (CTM_Optimizer::_evaluate_theta_objective,
+ * source/optimizer/CTM_Optimizer.cpp:175-187): M = (1 + cos theta)/2, imaging,
+ * PE, dPE/dM, dPE/dtheta = -1/2 dPE/dM sin theta and ||dPE/dtheta||_2.
+ * Every output pointer except d_grad_theta may be NULL. */
+int litho_ctm_evaluate(litho_ctx* ctx, const litho_cache* cache, litho_field* field,
+                       const float* d_theta, const float* d_target, double threshold,
+                       double alpha, float* d_mask, float* d_aerial, float* d_wafer,
+                       float* d_grad_mask, float* d_grad_theta, double* loss,
+                       double* grad_norm);
+
+/* Same, through host buffers (copies inside): the call a CPU caller makes. */
+int litho_ctm_evaluate_host(litho_ctx* ctx, const litho_cache* cache, litho_field* field,
+                            const float* h_theta, const float* h_target, double threshold,
+                            double alpha, float* h_grad_theta, double* loss,
+                            double* grad_norm);
+
+/* ------------------------------------------------------------ level set
+ * LevelSetUtils::evolve_normal_WENO_godunov (source/utils/level_set_utils.cpp:150-225):
+ * delta = Vn |grad phi|_Godunov with WENO5-JS one-sided derivatives and edge
+ * replication. h_abs (nullable) = |Vn| (the reference's H1_abs == H2_abs).
+ */
+int litho_weno_godunov(litho_ctx* ctx, int rows, int cols, const float* d_phi,
+                       const float* d_vn, double dy, double dx, float* d_delta, float* d_habs);
+/* LevelSetUtils::evolve_kappa (level_set_utils.cpp:257-278). */
+int litho_kappa(litho_ctx* ctx, int rows, int cols, const float* d_phi, double dx, double dy,
+                double b, float* d_out);
+/* LSM_Optimizer::_caculate_evolution_term (source/optimizer/LSM_Optimizer.cpp:47-58):
+ * normal = kappa term - delta, dt = get_dt_normal_kappa (level_set_utils.cpp:280-288). */
+int litho_evolution_term(litho_ctx* ctx, int rows, int cols, const float* d_phi,
+                         const float* d_vn, double dx, double dy, double cfl, double b,
+                         float* d_normal, double* dt);
+/* One RK2 level-set update (LSM_Optimizer.cpp:109-115, the second stage reuses
+ * the first stage's dt) and the printed mask (phi >= 0) (LSM_Optimizer.cpp:128).
+ * d_phi_out may alias nothing else; d_mask (nullable) receives 1/0 floats. */
+int litho_lsm_rk2_update(litho_ctx* ctx, int rows, int cols, const float* d_phi,
+                         const float* d_vn, double dx, double dy, double cfl, double b,
+                         float* d_phi_out, float* d_mask, double* dt);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LITHO_B200_H */
