@@ -87,6 +87,7 @@ SIGNATURES = {
     "litho_kappa": (_I, [_P, _I, _I, _P, _D, _D, _D, _P]),
     "litho_evolution_term": (_I, [_P, _I, _I, _P, _P, _D, _D, _D, _D, _P, _PD]),
     "litho_lsm_rk2_update": (_I, [_P, _I, _I, _P, _P, _D, _D, _D, _D, _P, _P, _PD]),
+    "litho_reinit_sdf": (_I, [_P, _I, _I, _P, _D, _D, _P, _P]),
 }
 
 
@@ -176,9 +177,9 @@ class Context:
     def launch_count(self) -> int:
         return int(self.lib.litho_ctx_launch_count(self.handle))
 
-    STAGES = ("row_analysis", "column_contraction", "band_forward", "row_synthesis_resist",
-              "adjoint_row_analysis", "adjoint_column_contraction", "band_adjoint",
-              "adjoint_row_synthesis_theta", "levelset_rk2")
+    STAGES = ("tile_analysis", "tile_reduction", "band_forward", "row_synthesis_resist",
+              "adjoint_tile_analysis", "adjoint_tile_reduction", "band_adjoint",
+              "adjoint_row_synthesis_theta", "levelset")
 
     def enable_stage_timing(self, on: bool = True):
         self._check(self.lib.litho_ctx_enable_stage_timing(self.handle, 1 if on else 0))
@@ -463,6 +464,26 @@ class LevelSetUtils:
         return out, dt.value
 
     @staticmethod
+    def get_dt_normal_kappa(cfl, dx, dy, H1_abs, H2_abs, b) -> float:
+        """LevelSetUtils::get_dt_normal_kappa (level_set_utils.cpp:280-288), host scalar."""
+        h1 = float(H1_abs.max()) if hasattr(H1_abs, "max") else float(H1_abs)
+        h2 = float(H2_abs.max()) if hasattr(H2_abs, "max") else float(H2_abs)
+        den = h1 / dx + h2 / dy + b * (1.0 / (dx * dx) + 1.0 / (dy * dy)) * 2
+        return 1e-3 if den < 1e-9 else cfl / den
+
+    @staticmethod
+    def reinit_sdf(phi, dx, dy, ctx=None, with_mask=False):
+        """LevelSetUtils::reinit_sdf (level_set_utils.cpp:290-319) on the device."""
+        ctx = ctx or default_context()
+        torch = ctx.torch
+        p = _f32(phi, torch)
+        out = torch.empty_like(p)
+        mask = torch.empty_like(p) if with_mask else None
+        ctx._check(ctx.lib.litho_reinit_sdf(ctx.handle, p.shape[0], p.shape[1], _ptr(p), float(dx),
+                                            float(dy), _ptr(out), _ptr(mask)))
+        return (out, mask) if with_mask else out
+
+    @staticmethod
     def rk2_update(phi, Vn, dx, dy, cfl, b, ctx=None):
         """One RK2 update (LSM_Optimizer.cpp:109-115) -> (phi_next, mask, dt)."""
         ctx = ctx or default_context()
@@ -564,3 +585,77 @@ class CTMOptimizer:
                                                 max_iterations=self.iterations)
         self.theta = theta
         return 0.5 * (1.0 + torch.cos(theta))
+
+
+@dataclass
+class LevelSetResult:
+    """Level_set_result of LSM_Optimizer::optimize: (best_sdf, best_mask, initial_sdf)."""
+    best_sdf: object
+    best_mask: object
+    initial_sdf: object
+
+
+class LSMOptimizer:
+    """LSM_Optimizer (source/optimizer/LSM_Optimizer.cpp:60-149) over the device kernels.
+
+    Per iteration: imaging of the current binary mask, PE (+ penalty) loss, the
+    PE gradient as the normal speed, one RK2 WENO5-Godunov update with the
+    first stage's dt, a chamfer re-initialisation every 20 iterations and the
+    printed mask phi >= 0. Best-state bookkeeping follows the reference,
+    including that best_sdf records the previous iteration's phi.
+    """
+
+    def __init__(self, cache: ImagingCache, target, threshold, alpha, dx, dy, cfl=0.5, b=0.01,
+                 iterations=200, penalty=0.0, penalty_threshold=0.01):
+        self.cache = cache
+        self.ctx = cache.ctx
+        torch = self.ctx.torch
+        N = cache.N
+        self.target = _f32(target, torch, (N, N), "target")
+        self.threshold, self.alpha = float(threshold), float(alpha)
+        self.dx, self.dy, self.cfl, self.b = float(dx), float(dy), float(cfl), float(b)
+        self.iterations = int(iterations)
+        self.penalty, self.penalty_threshold = float(penalty), float(penalty_threshold)
+        self.imaging = Imaging(cache)
+        self.gradient = Gradient(cache, threshold, alpha)
+        self.error_history: List[float] = []
+
+    def optimize(self, mask) -> LevelSetResult:
+        torch = self.ctx.torch
+        N = self.cache.N
+        m0 = _f32(mask, torch, (N, N), "mask")
+        phi_n = LevelSetUtils.reinit_sdf(m0 - 0.5, self.dx, self.dy, ctx=self.ctx)
+        initial_sdf = phi_n.clone()
+        phi_M = torch.zeros_like(phi_n)
+        best_sdf = torch.zeros_like(phi_n)
+        best_mask = m0.clone()
+        temp = m0.clone()
+        min_error = float("inf")
+        self.error_history = []
+        for i in range(self.iterations):
+            r = self.imaging.compute(temp, self.threshold, self.alpha)
+            if self.penalty > 0.0:
+                pe = Loss.pe_loss_with_penalty(r.wafer_image, self.target, self.penalty,
+                                               self.penalty_threshold, ctx=self.ctx)
+            else:
+                pe = Loss.pe_loss_with_penalty(r.wafer_image, self.target, 1.0, 0.01, ctx=self.ctx)
+            if pe < min_error:
+                min_error = pe
+                best_mask = temp.clone()
+                best_sdf = phi_M.clone()
+            self.error_history.append(pe)
+            field = self.imaging.get_electric_field()
+            if self.penalty > 0.0:
+                gm = self.gradient.pe_gradient_with_penalty(r.wafer_image, self.target, field,
+                                                            self.penalty, self.penalty_threshold)
+            else:
+                gm = self.gradient.pe_gradient(r.wafer_image, self.target, field)
+            phi_next, mask_next, _ = LevelSetUtils.rk2_update(phi_n, gm, self.dx, self.dy, self.cfl,
+                                                              self.b, ctx=self.ctx)
+            phi_M = phi_next
+            if i % 20 == 0 and i > 0:
+                phi_M, mask_next = LevelSetUtils.reinit_sdf(phi_M, self.dx, self.dy, ctx=self.ctx,
+                                                            with_mask=True)
+            phi_n = phi_M
+            temp = mask_next
+        return LevelSetResult(best_sdf, best_mask, initial_sdf)

@@ -50,50 +50,36 @@ int upload(Context* ctx, T** dst, const std::vector<T>& src) {
 void free_cache(Cache* c) {
   void* ptrs[] = {c->H,    c->w,    c->TXS,  c->TXD,   c->TYS,   c->TYD,   c->AYS,
                   c->AYD,  c->TXSc, c->TXDc, c->ESr_t, c->ESc_t, c->ESc,   c->EDr_t,
-                  c->EDc_t};
+                  c->EDc_t, c->EDc};
   for (void* p : ptrs)
     if (p) cudaFree(p);
 }
 
 // Scratch layout of one imaging + adjoint evaluation.
 struct Layout {
-  size_t R, mpart, gpart, T, ik, Q, chat, Ut, Vt, dldi, Gam, gam, Z1, Zk, X, phi1, rows_tmp,
-      total;
-  int ks, ys;
+  size_t part, gh, ik, iP, Ut, Vt, dldi, gam, Zk, rows_tmp, total;
+  int tiles;
 };
 
 Layout make_layout(const BandGeom& g) {
   Layout L{};
   const int N = g.N;
-  // Split of the row analyses over x and of the column contractions over y,
-  // sized for about two waves of the 148 SMs.
-  const int rowblocks = (N + 127) / 128;
-  const int ks_req = std::max(1, std::min((296 + rowblocks - 1) / rowblocks, std::max(1, N / 64)));
-  int kps = 0;
-  row_split(N, ks_req, &kps, &L.ks);  // L.ks: the chunk count the row analysis produces
-  L.ys = std::max(1, std::min(32, N / 32));
+  L.tiles = analysis_tiles(N);
   size_t off = 0;
   auto take = [&](size_t bytes) {
     const size_t o = off;
     off = align_up(off + bytes, 256);
     return o;
   };
-  L.R = take((size_t)L.ks * N * 2 * g.Nc * sizeof(float));
-  L.mpart = take((size_t)L.ys * g.Nr * g.Nc * sizeof(float2));
-  L.gpart = take((size_t)L.ys * (2 * g.Nr - 1) * g.Nc * sizeof(float2));
-  L.T = take((size_t)g.K * g.Nr * g.Pc * sizeof(float2));
+  L.part = take((size_t)L.tiles * (2 * g.Nr - 1) * g.Nc * sizeof(float2));
+  L.gh = take((size_t)(2 * g.Nr - 1) * g.Nc * sizeof(float2));
   L.ik = take((size_t)g.K * g.Pr * g.Pc * sizeof(float));
-  L.Q = take((size_t)g.Pr * (2 * g.Nc - 1) * sizeof(float2));
-  L.chat = take((size_t)g.Nr * (2 * g.Nc - 1) * sizeof(float2));
+  L.iP = take((size_t)g.Pr * g.Pc * sizeof(float));
   L.Ut = take((size_t)N * g.kp_rows * sizeof(float));
   L.Vt = take((size_t)N * g.kp_rows * sizeof(float));
   L.dldi = take((size_t)N * N * sizeof(float));
-  L.Gam = take((size_t)(2 * g.Nr - 1) * g.Pc * sizeof(float2));
   L.gam = take((size_t)g.Pr * g.Pc * sizeof(float));
-  L.Z1 = take((size_t)g.K * g.Pr * g.Nc * sizeof(float2));
   L.Zk = take((size_t)g.K * g.Nr * g.Nc * sizeof(float2));
-  L.X = take((size_t)g.Nr * g.Nc * sizeof(float2));
-  L.phi1 = 0;
   L.rows_tmp = take((size_t)g.Nr * N * sizeof(float2));
   L.total = off;
   return L;
@@ -342,6 +328,7 @@ int litho_cache_create_band(litho_ctx* ctx, int N, int K, int Nr, int Nc, int ro
     }
   std::vector<float2> ESr_t((size_t)Nr * g.Pr), ESc_t((size_t)Nc * g.Pc), ESc((size_t)g.Pc * Nc);
   std::vector<float2> EDr_t((size_t)(2 * Nr - 1) * g.Pr), EDc_t((size_t)(2 * Nc - 1) * g.Pc);
+  std::vector<float2> EDc((size_t)g.Pc * (2 * Nc - 1));
   for (int r = 0; r < Nr; ++r)
     for (int j = 0; j < g.Pr; ++j) {
       twiddle(row0 + r, j, g.Pr, 1.0, &re, &im);
@@ -362,7 +349,15 @@ int litho_cache_create_band(litho_ctx* ctx, int N, int K, int Nr, int Nc, int ro
     for (int j = 0; j < g.Pc; ++j) {
       twiddle(a - (Nc - 1), j, g.Pc, 1.0, &re, &im);
       EDc_t[(size_t)a * g.Pc + j] = make_float2((float)re, (float)im);
+      EDc[(size_t)j * (2 * Nc - 1) + a] = make_float2((float)re, (float)im);
     }
+  // The per-kernel CTAs of the small-grid stage keep a band (and a band-by-grid
+  // product) in shared memory; larger bands are not built.
+  if (band_fields_smem(g) > 200 * 1024 || (size_t)g.Pr * Nc * sizeof(float2) > 200 * 1024) {
+    delete c;
+    return ctx->fail(LITHO_ERR_UNSUPPORTED,
+                     "kernel band too large: needs (Nr*Nc + 2*Nr*Nc) * 8 bytes <= 200 KiB");
+  }
   int st = LITHO_OK;
   if (st == LITHO_OK) st = upload(ctx, &c->H, H);
   if (st == LITHO_OK) st = upload(ctx, &c->w, w);
@@ -379,6 +374,7 @@ int litho_cache_create_band(litho_ctx* ctx, int N, int K, int Nr, int Nc, int ro
   if (st == LITHO_OK) st = upload(ctx, &c->ESc, ESc);
   if (st == LITHO_OK) st = upload(ctx, &c->EDr_t, EDr_t);
   if (st == LITHO_OK) st = upload(ctx, &c->EDc_t, EDc_t);
+  if (st == LITHO_OK) st = upload(ctx, &c->EDc, EDc);
   if (st != LITHO_OK) {
     free_cache(c);
     delete c;
@@ -510,7 +506,7 @@ int check_launch(Context* ctx, cudaError_t e, const char* what) {
   return LITHO_OK;
 }
 
-// Forward: row analysis -> column contraction -> small-grid band stage -> row
+// Forward: tile analysis -> tile reduction -> small-grid band stage -> row
 // synthesis with the fused resist epilogue. input_mode 1 reads theta.
 int run_forward(Context* ctx, const Cache& c, Field& f, const Layout& L, int input_mode,
                 const float* input, float* mask_out, ResistEpilogue ep, int* nblocks) {
@@ -519,22 +515,19 @@ int run_forward(Context* ctx, const Cache& c, Field& f, const Layout& L, int inp
   int* flag = reinterpret_cast<int*>(ctx->d_red + RED_FLAG);
   int st;
   ctx->stage_begin(0);
-  st = check_launch(ctx, launch_analysis_rows(s, input_mode, input, mask_out, flag, c.TXS, g.N,
-                                              g.Nc, L.ks, at<float>(ctx, L.R)),
-                    "row analysis");
+  st = check_launch(ctx, launch_analysis(s, input_mode, input, mask_out, flag, c.TXS, g.N, g.Nc,
+                                         c.TYS, g.Nr, g.Nr, 0, at<float2>(ctx, L.part)),
+                    "tile analysis");
   ctx->stage_end(0);
   if (st) return st;
   ctx->stage_begin(1);
-  st = check_launch(ctx, launch_analysis_cols(s, at<float>(ctx, L.R), L.ks, g.N, g.Nc, c.TYS,
-                                              g.Nr, g.Nr, 0, L.ys, 1.f / ((float)g.N * g.N),
-                                              at<float2>(ctx, L.mpart)),
-                    "column contraction");
+  st = check_launch(ctx, launch_reduce_tiles(s, at<float2>(ctx, L.part), L.tiles, g.Nr * g.Nc,
+                                             1.f / ((float)g.N * g.N), f.mband),
+                    "tile reduction");
   ctx->stage_end(1);
   if (st) return st;
   ctx->stage_begin(2);
-  st = check_launch(ctx, launch_band_forward(s, c, at<float2>(ctx, L.mpart), L.ys, f,
-                                             at<float>(ctx, L.ik), at<float2>(ctx, L.T),
-                                             at<float2>(ctx, L.Q), at<float2>(ctx, L.chat),
+  st = check_launch(ctx, launch_band_forward(s, c, f, at<float>(ctx, L.ik), at<float>(ctx, L.iP),
                                              at<float>(ctx, L.Ut)),
                     "band forward");
   ctx->stage_end(2);
@@ -544,7 +537,7 @@ int run_forward(Context* ctx, const Cache& c, Field& f, const Layout& L, int inp
                                              nblocks),
                     "row synthesis");
   ctx->stage_end(3);
-  ctx->launches += 8;
+  ctx->launches += 6;
   f.valid = (st == LITHO_OK);
   return st;
 }
@@ -554,25 +547,24 @@ int run_adjoint(Context* ctx, const Cache& c, const Field& f, const Layout& L, c
   const BandGeom& g = c.g;
   cudaStream_t s = ctx->stream;
   int* flag = reinterpret_cast<int*>(ctx->d_red + RED_FLAG);
+  const int na = 2 * g.Nr - 1;
   int st;
   ctx->stage_begin(4);
-  st = check_launch(ctx, launch_analysis_rows(s, 0, dldi, nullptr, flag, c.TXD, g.N, g.Nc, L.ks,
-                                              at<float>(ctx, L.R)),
-                    "adjoint row analysis");
+  st = check_launch(ctx, launch_analysis(s, 0, dldi, nullptr, flag, c.TXD, g.N, g.Nc, c.TYD, na,
+                                         g.Nr, 1, at<float2>(ctx, L.part)),
+                    "adjoint tile analysis");
   ctx->stage_end(4);
   if (st) return st;
   ctx->stage_begin(5);
-  st = check_launch(ctx, launch_analysis_cols(s, at<float>(ctx, L.R), L.ks, g.N, g.Nc, c.TYD,
-                                              2 * g.Nr - 1, g.Nr, 1, L.ys,
-                                              1.f / ((float)g.N * g.N), at<float2>(ctx, L.gpart)),
-                    "adjoint column contraction");
+  st = check_launch(ctx, launch_reduce_tiles(s, at<float2>(ctx, L.part), L.tiles, na * g.Nc,
+                                             1.f / ((float)g.N * g.N), at<float2>(ctx, L.gh)),
+                    "adjoint tile reduction");
   ctx->stage_end(5);
   if (st) return st;
   ctx->stage_begin(6);
-  st = check_launch(ctx, launch_band_adjoint(s, c, f, at<float2>(ctx, L.gpart), L.ys, scale,
-                                             at<float2>(ctx, L.Gam), at<float>(ctx, L.gam),
-                                             at<float2>(ctx, L.Z1), at<float2>(ctx, L.Zk),
-                                             at<float2>(ctx, L.X), at<float>(ctx, L.Vt)),
+  st = check_launch(ctx, launch_band_adjoint(s, c, f, at<float2>(ctx, L.gh), scale,
+                                             at<float>(ctx, L.gam), at<float2>(ctx, L.Zk),
+                                             at<float>(ctx, L.Vt)),
                     "band adjoint");
   ctx->stage_end(6);
   if (st) return st;
@@ -581,7 +573,7 @@ int run_adjoint(Context* ctx, const Cache& c, const Field& f, const Layout& L, c
                                            nblocks),
                     "adjoint row synthesis");
   ctx->stage_end(7);
-  ctx->launches += 9;
+  ctx->launches += 6;
   return st;
 }
 
@@ -936,6 +928,31 @@ int litho_evolution_term(litho_ctx* ctx, int rows, int cols, const float* d_phi,
   std::memcpy(h, ctx->h_red + RED_SUM, sizeof(h));
   if (dt) *dt = h[1];
   return LITHO_OK;
+}
+
+int litho_reinit_sdf(litho_ctx* ctx, int rows, int cols, const float* d_phi, double dx,
+                     double dy, float* d_sdf, float* d_mask) {
+  if (!ctx || !d_phi || !d_sdf) return LITHO_ERR_INVALID_ARGUMENT;
+  int st = ls_check(ctx, rows, cols, dx, dy, 1);
+  if (st) return st;
+  if ((size_t)3 * cols * sizeof(float) > 200 * 1024)
+    return ctx->fail(LITHO_ERR_UNSUPPORTED, "reinit_sdf supports at most 17066 columns");
+  const size_t n = (size_t)rows * cols;
+  st = ctx->ensure_scratch(2 * n * sizeof(float));
+  if (st) return st;
+  ctx->stage_begin(8);
+  st = check_launch(ctx, launch_reinit_sdf(ctx->stream, rows, cols, d_phi, (float)dx,
+                                           static_cast<float*>(ctx->scratch.base), d_sdf),
+                    "reinit_sdf");
+  if (!st && d_mask)
+    st = check_launch(ctx, launch_levelset(ctx->stream, 5, rows, cols, d_sdf, nullptr, nullptr,
+                                           (float)dx, (float)dy, 0.f, nullptr, d_mask, nullptr),
+                      "mask");
+  ctx->stage_end(8);
+  ctx->launches += d_mask ? 2 : 1;
+  if (!st) LITHO_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  if (!st) ctx->collect_stages();
+  return st;
 }
 
 int litho_lsm_rk2_update(litho_ctx* ctx, int rows, int cols, const float* d_phi,

@@ -10,22 +10,18 @@
 //   g'(d)    = DFT_N(dL/dI)|_D / N^2,   gamma(j) = sum_{d in D} g'(d) e^{2 pi i d.j/P}
 //   Z_k(u)   = DFT_P(e_k gamma)(u)/(Pr Pc) = sum_v H_k(v) m(v) g'(u - v)
 //   X(u)     = scale sum_k w'_k conj(H_k(u)) Z_k(u),  grad(y) = Re sum_{u in S} X(u) e^{2 pi i u.y/N}.
-// So the full-resolution work is four K-independent separable passes (row
-// analysis / column contraction / column expansion / row synthesis); the
-// K-dependent work lives on the small grid.
+// So the full-resolution work is two K-independent separable passes per
+// direction: a tile analysis (row DFT of a 128 x 128 tile, then its column
+// contraction, giving one band partial per tile) and a row synthesis GEMM with
+// a fused elementwise epilogue. The K-dependent work lives on the small grid.
 #include <cuda_runtime.h>
-#include <math_constants.h>
 
-#include "gemm_nt.cuh"
 #include "litho_internal.cuh"
 
 namespace litho_b200 {
 
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
   return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
-}
-__device__ __forceinline__ float2 cmulc(float2 a, float2 b) {  // a * conj(b)
-  return make_float2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
 }
 __device__ __forceinline__ float2 conjf2(float2 a) { return make_float2(a.x, -a.y); }
 __device__ __forceinline__ void cfma(float2& acc, float2 a, float2 b) {
@@ -49,7 +45,53 @@ __device__ double block_sum(double v, double* sh) {
   return r;
 }
 
-// ---------------------------------------------------------------- row analysis
+// ---------------------------------------------------------------- GEMM main loop
+// acc[i][j] += sum_{k in [kbeg, kend)} A(m0 + ty*TM + i, k) * B[(n0 + tx + j*BNT) * ldb + k]
+// with 256 threads (BMT x BNT), A produced by a functor (load4 of 4 consecutive k),
+// shared tiles As[BK][BM + 4] (transposed, float4 reads) and Bs[BK][BN + 1].
+template <int BMT, int BNT, int TM, int TN, int BK, class ALoad>
+__device__ __forceinline__ void gemm_mainloop(ALoad& aload, const float* __restrict__ B, int ldb,
+                                              int Nn, int m0, int n0, int kbeg, int kend,
+                                              float* As, float* Bs, float (&acc)[TM][TN]) {
+  constexpr int BM = BMT * TM, BN = BNT * TN, NT = BMT * BNT;
+  constexpr int AS = BM + 4, BS = BN + 1;
+  const int tid = threadIdx.x, tx = tid % BNT, ty = tid / BNT;
+  for (int kt = kbeg; kt < kend; kt += BK) {
+    for (int e = tid; e < BM * (BK / 4); e += NT) {
+      const int mm = e / (BK / 4);
+      const int kq = (e % (BK / 4)) * 4;
+      float v[4];
+      aload.load4(m0 + mm, kt + kq, kend, v);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) As[(kq + q) * AS + mm] = v[q];
+    }
+    for (int e = tid; e < BN * BK; e += NT) {
+      const int nn = e / BK, kk = e % BK;
+      const int gn = n0 + nn, gk = kt + kk;
+      Bs[kk * BS + nn] = (gn < Nn && gk < kend) ? __ldg(B + (size_t)gn * ldb + gk) : 0.f;
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int kk = 0; kk < BK; ++kk) {
+      float a[TM];
+#pragma unroll
+      for (int i = 0; i < TM; i += 4) {
+        const float4 t = *reinterpret_cast<const float4*>(&As[kk * AS + ty * TM + i]);
+        a[i] = t.x; a[i + 1] = t.y; a[i + 2] = t.z; a[i + 3] = t.w;
+      }
+      float b[TN];
+#pragma unroll
+      for (int j = 0; j < TN; ++j) b[j] = Bs[kk * BS + tx + j * BNT];
+#pragma unroll
+      for (int i = 0; i < TM; ++i)
+#pragma unroll
+        for (int j = 0; j < TN; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------- tile analysis
 // mode 0: A = in;  mode 1: A = (1 + cos(in))/2 (theta -> mask), optional mask_out.
 // Non-finite inputs raise flag[0].
 struct ImageLoad {
@@ -61,7 +103,7 @@ struct ImageLoad {
   int vec4;  // rows are 16-byte aligned (N % 4 == 0 and an aligned base pointer)
   __device__ __forceinline__ void load4(int m, int k, int kend, float* v) {
     if (vec4 && m < N && k + 3 < kend) {
-      float4 t = __ldg(reinterpret_cast<const float4*>(in + (size_t)m * N + k));
+      const float4 t = __ldg(reinterpret_cast<const float4*>(in + (size_t)m * N + k));
       v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
     } else {
 #pragma unroll
@@ -70,186 +112,185 @@ struct ImageLoad {
     }
     bool bad = false;
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
+    for (int q = 0; q < 4; ++q)
       if (m < N && k + q < kend) bad |= !isfinite(v[q]);
-    }
     if (bad) atomicOr(flag, 1);
     if (mode == 1) {
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
-        v[q] = 0.5f * (1.f + cosf(v[q]));
-        if (mask_out && m < N && k + q < kend) mask_out[(size_t)m * N + k + q] = v[q];
+        const bool in_range = m < N && k + q < kend;
+        v[q] = in_range ? 0.5f * (1.f + cosf(v[q])) : 0.f;
+        if (mask_out && in_range) mask_out[(size_t)m * N + k + q] = v[q];
       }
     }
   }
 };
 
-struct PartialStore {
-  float* out;  // [gridDim.z][M][ld]
-  int M, ld;
-  __device__ __forceinline__ void store(int m, int n, float v) {
-    out[((size_t)blockIdx.z * M + m) * ld + n] = v;
-  }
-  __device__ __forceinline__ void finish() {}
+constexpr int AT_BMT = 16, AT_BNT = 16, AT_TM = 8, AT_BK = 32, AT_NT = 256;
+constexpr int AT_TILE = AT_BMT * AT_TM;  // 128 rows, and 128 columns of x per tile
+constexpr int AT_RC = 16;                // band rows staged per chunk in phase 2
+
+struct AnalysisArgs {
+  ImageLoad ld;
+  const float* tw;     // [2 * ncols][N] real rows (Re, Im of the column twiddles)
+  int N, ncols;
+  const float2* TY;    // [nr][N] row twiddles
+  int nrows_out, nr, sym;
+  float2* part;        // [tiles][nrows_out][ncols]
 };
 
 template <int TN>
-static cudaError_t analysis_rows_t(cudaStream_t s, const ImageLoad& ld, const float* tw, int N,
-                                   int ncols2, int ksplit, float* out) {
-  constexpr int BMT = 32, BNT = 8, TM = 4, BK = 16;
-  int kps, zs;
-  row_split(N, ksplit, &kps, &zs);
-  dim3 grid((N + BMT * TM - 1) / (BMT * TM), (ncols2 + BNT * TN - 1) / (BNT * TN), zs);
-  PartialStore st{out, N, ncols2};
-  gemm_nt_kernel<BMT, BNT, TM, TN, BK><<<grid, BMT * BNT, 0, s>>>(N, ncols2, N, kps, ld, tw,
-                                                                 N, st);
+__global__ void __launch_bounds__(AT_NT)
+analysis_tile_kernel(AnalysisArgs a) {
+  extern __shared__ __align__(16) float smem[];
+  constexpr int BN = AT_BNT * TN;   // real columns (2 per complex frequency)
+  constexpr int BNC = BN / 2;       // complex columns
+  float* As = smem;
+  float* Bs = smem + AT_BK * (AT_TILE + 4);
+  const int tid = threadIdx.x, tx = tid % AT_BNT, ty = tid / AT_BNT;
+  const int x0 = blockIdx.x * AT_TILE, y0 = blockIdx.y * AT_TILE;
+  const int f0 = blockIdx.z * BN;
+  const int Nn = 2 * a.ncols;
+  ImageLoad ld = a.ld;
+
+  // Phase 1: R[y][f] = sum_{x in tile} A[y][x] tw[f][x]  (128 rows x BN real columns).
+  float acc[AT_TM][TN];
+#pragma unroll
+  for (int i = 0; i < AT_TM; ++i)
+#pragma unroll
+    for (int j = 0; j < TN; ++j) acc[i][j] = 0.f;
+  gemm_mainloop<AT_BMT, AT_BNT, AT_TM, TN, AT_BK>(ld, a.tw, a.N, Nn, y0, f0, x0,
+                                                  min(a.N, x0 + AT_TILE), As, Bs, acc);
+  // Phase 2: P[r][c] = sum_{y in tile} T(r, y) R[y][c] for the tile's rows.
+  constexpr int RS = BN + 1;
+  float* Rs = smem;                                  // [128][RS]
+  float2* TYs = reinterpret_cast<float2*>(smem + ((AT_TILE * RS + 3) & ~3));  // [RC][128]
+#pragma unroll
+  for (int i = 0; i < AT_TM; ++i)
+#pragma unroll
+    for (int j = 0; j < TN; ++j) Rs[(ty * AT_TM + i) * RS + tx + j * AT_BNT] = acc[i][j];
+  const int cl = tid % BNC, ag = tid / BNC, AG = AT_NT / BNC;
+  const int cg = f0 / 2 + cl;
+  const bool col_active = ag < AG && cg < a.ncols;
+  const int tile = blockIdx.y * gridDim.x + blockIdx.x;
+  for (int r0 = 0; r0 < a.nrows_out; r0 += AT_RC) {
+    __syncthreads();
+    for (int e = tid; e < AT_RC * AT_TILE; e += AT_NT) {
+      const int r = e / AT_TILE, yy = e % AT_TILE;
+      const int row = r0 + r, y = y0 + yy;
+      float2 t = make_float2(0.f, 0.f);
+      if (row < a.nrows_out && y < a.N) {
+        if (!a.sym) {
+          t = a.TY[(size_t)row * a.N + y];
+        } else {
+          const int d = row - (a.nr - 1);
+          t = d >= 0 ? a.TY[(size_t)d * a.N + y] : conjf2(a.TY[(size_t)(-d) * a.N + y]);
+        }
+      }
+      TYs[r * AT_TILE + yy] = t;
+    }
+    __syncthreads();
+    if (col_active) {
+      for (int r = ag; r < AT_RC; r += AG) {
+        const int row = r0 + r;
+        if (row >= a.nrows_out) break;
+        float2 p0 = make_float2(0.f, 0.f), p1 = p0;
+        const float2* tyr = TYs + r * AT_TILE;
+#pragma unroll 4
+        for (int yy = 0; yy < AT_TILE; yy += 2) {
+          cfma(p0, tyr[yy], make_float2(Rs[yy * RS + 2 * cl], Rs[yy * RS + 2 * cl + 1]));
+          cfma(p1, tyr[yy + 1],
+               make_float2(Rs[(yy + 1) * RS + 2 * cl], Rs[(yy + 1) * RS + 2 * cl + 1]));
+        }
+        a.part[((size_t)tile * a.nrows_out + row) * a.ncols + cg] =
+            make_float2(p0.x + p1.x, p0.y + p1.y);
+      }
+    }
+  }
+}
+
+template <int TN>
+static cudaError_t analysis_tile_t(cudaStream_t s, const AnalysisArgs& a) {
+  constexpr int BN = AT_BNT * TN;
+  const size_t p1 = (size_t)(AT_BK * (AT_TILE + 4) + AT_BK * (BN + 1)) * sizeof(float);
+  const size_t p2 = (size_t)((AT_TILE * (BN + 1) + 3) & ~3) * sizeof(float) +
+                    (size_t)AT_RC * AT_TILE * sizeof(float2);
+  const size_t smem = p1 > p2 ? p1 : p2;
+  cudaError_t e = cudaFuncSetAttribute(analysis_tile_kernel<TN>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  const int t = (a.N + AT_TILE - 1) / AT_TILE;
+  dim3 grid(t, t, (2 * a.ncols + BN - 1) / BN);
+  analysis_tile_kernel<TN><<<grid, AT_NT, smem, s>>>(a);
   return cudaGetLastError();
 }
 
-// in: N x N image (mode 0) or theta (mode 1). tw: [2*ncols][N] real rows
-// (Re, Im interleaved by row). out: [zs][N][2*ncols] partial sums, where
-// row_split(N, ksplit) gives zs (the number of x chunks actually used).
-cudaError_t launch_analysis_rows(cudaStream_t s, int mode, const float* in, float* mask_out,
-                                 int* flag, const float* tw, int N, int ncols, int ksplit,
-                                 float* out) {
+int analysis_tiles(int N) {
+  const int t = (N + AT_TILE - 1) / AT_TILE;
+  return t * t;
+}
+
+// Tile partials of sum_{y, x} T(a, y) A[y][x] tw(c, x) for every 128 x 128 tile:
+// part[tile][a][c], tiles in row-major order of the tile grid.
+cudaError_t launch_analysis(cudaStream_t s, int mode, const float* in, float* mask_out,
+                            int* flag, const float* tw, int N, int ncols, const float2* TY,
+                            int nrows_out, int nr, int sym, float2* part) {
   const int vec4 = (N % 4 == 0) && (reinterpret_cast<uintptr_t>(in) % 16 == 0);
-  ImageLoad ld{in, mask_out, flag, N, mode, vec4};
+  AnalysisArgs a{ImageLoad{in, mask_out, flag, N, mode, vec4}, tw, N, ncols, TY, nrows_out,
+                 nr, sym, part};
   const int n2 = 2 * ncols;
-  if (n2 <= 16) return analysis_rows_t<2>(s, ld, tw, N, n2, ksplit, out);
-  if (n2 <= 32) return analysis_rows_t<4>(s, ld, tw, N, n2, ksplit, out);
-  if (n2 <= 48) return analysis_rows_t<6>(s, ld, tw, N, n2, ksplit, out);
-  if (n2 <= 64) return analysis_rows_t<8>(s, ld, tw, N, n2, ksplit, out);
-  if (n2 <= 72) return analysis_rows_t<9>(s, ld, tw, N, n2, ksplit, out);
-  if (n2 <= 80) return analysis_rows_t<10>(s, ld, tw, N, n2, ksplit, out);
-  if (n2 <= 96) return analysis_rows_t<12>(s, ld, tw, N, n2, ksplit, out);
-  return analysis_rows_t<16>(s, ld, tw, N, n2, ksplit, out);
+  if (n2 <= 32) return analysis_tile_t<2>(s, a);
+  if (n2 <= 48) return analysis_tile_t<3>(s, a);
+  if (n2 <= 64) return analysis_tile_t<4>(s, a);
+  if (n2 <= 80) return analysis_tile_t<5>(s, a);
+  if (n2 <= 96) return analysis_tile_t<6>(s, a);
+  return analysis_tile_t<8>(s, a);
 }
 
-// ---------------------------------------------------------------- column contraction
-// out[ys][a][c] = scale * sum_{y in chunk ys} T(a, y) * sum_z R[z][y][c]
-// sym == 0: a in [0, nrows), T(a, y) = TY[a][y].
-// sym == 1: a in [0, 2*nr - 1), d = a - (nr - 1), T = d >= 0 ? TY[d][y] : conj(TY[-d][y]).
-constexpr int AC_RB = 8;    // rows a per block
-constexpr int AC_YT = 32;   // y tile staged in shared memory
-__global__ void __launch_bounds__(128)
-analysis_cols_kernel(const float2* __restrict__ R, int ksplit, int N, int ncols,
-                     const float2* __restrict__ TY, int nrows_out, int nr, int sym, int ychunk,
-                     float scale, float2* __restrict__ out) {
-  __shared__ float2 tys[AC_RB][AC_YT];
-  const int a0 = blockIdx.x * AC_RB;
-  const int ys = blockIdx.y;
-  const int y0 = ys * ychunk;
-  const int y1 = min(N, y0 + ychunk);
-  for (int c0 = 0; c0 < ncols; c0 += blockDim.x) {
-    const int c = c0 + threadIdx.x;
-    float2 acc[AC_RB];
-#pragma unroll
-    for (int r = 0; r < AC_RB; ++r) acc[r] = make_float2(0.f, 0.f);
-    for (int yt = y0; yt < y1; yt += AC_YT) {
-      __syncthreads();
-      for (int e = threadIdx.x; e < AC_RB * AC_YT; e += blockDim.x) {
-        const int r = e / AC_YT, yy = e % AC_YT;
-        const int a = a0 + r, y = yt + yy;
-        float2 t = make_float2(0.f, 0.f);
-        if (a < nrows_out && y < y1) {
-          if (!sym) {
-            t = TY[(size_t)a * N + y];
-          } else {
-            const int d = a - (nr - 1);
-            t = d >= 0 ? TY[(size_t)d * N + y] : conjf2(TY[(size_t)(-d) * N + y]);
-          }
-        }
-        tys[r][yy] = t;
-      }
-      __syncthreads();
-      if (c < ncols) {
-        const int ye = min(AC_YT, y1 - yt);
-        for (int yy = 0; yy < ye; ++yy) {
-          const int y = yt + yy;
-          float2 v = make_float2(0.f, 0.f);
-          for (int z = 0; z < ksplit; ++z) {
-            const float2 p = R[((size_t)z * N + y) * ncols + c];
-            v.x += p.x; v.y += p.y;
-          }
-#pragma unroll
-          for (int r = 0; r < AC_RB; ++r) cfma(acc[r], tys[r][yy], v);
-        }
-      }
-    }
-    if (c < ncols) {
-#pragma unroll
-      for (int r = 0; r < AC_RB; ++r) {
-        const int a = a0 + r;
-        if (a < nrows_out)
-          out[((size_t)ys * nrows_out + a) * ncols + c] =
-              make_float2(acc[r].x * scale, acc[r].y * scale);
-      }
-    }
+// out[o] = scale * sum_t part[t][o] in a fixed tree order (one warp per output).
+__global__ void __launch_bounds__(256)
+reduce_tiles_kernel(const float2* __restrict__ part, int tiles, int count, float scale,
+                    float2* __restrict__ out) {
+  const int o = blockIdx.x * 8 + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (o >= count) return;
+  float2 v0 = make_float2(0.f, 0.f), v1 = v0;
+  int t = lane;
+  for (; t + 32 < tiles; t += 64) {
+    const float2 p = part[(size_t)t * count + o];
+    const float2 q = part[(size_t)(t + 32) * count + o];
+    v0.x += p.x; v0.y += p.y;
+    v1.x += q.x; v1.y += q.y;
   }
-}
-
-cudaError_t launch_analysis_cols(cudaStream_t s, const float* R, int ksplit, int N, int ncols,
-                                 const float2* TY, int nrows_out, int nr, int sym, int ysplit,
-                                 float scale, float2* out_partial) {
-  const int ychunk = (N + ysplit - 1) / ysplit;
-  dim3 grid((nrows_out + AC_RB - 1) / AC_RB, ysplit);
-  const int threads = ncols <= 64 ? 64 : 128;
-  analysis_cols_kernel<<<grid, threads, 0, s>>>(reinterpret_cast<const float2*>(R), ksplit, N,
-                                                ncols, TY, nrows_out, nr, sym, ychunk, scale,
-                                                out_partial);
-  return cudaGetLastError();
-}
-
-// ---------------------------------------------------------------- column expansion
-// Ut[x][2a + {0,1}] = kappa(a) * sum_c coef[a][c] * phase(c, x), ld = kp (columns
-// 2*nrows..kp-1 are zero-filled by the a == 0 blocks).
-// mode 0 (band S): phase = conj(TX[c][x]) (TX = e^{-2 pi i s_c x/N}), kappa = 1.
-// mode 1 (difference set D): c in [0, 2*nc-1), d = c - (nc-1),
-//   phase = d >= 0 ? conj(TX[d][x]) : TX[-d][x], kappa(a) = a > 0 ? 2 : 1.
-__global__ void __launch_bounds__(128)
-expand_cols_kernel(const float2* __restrict__ coef, int ncoef, int coef_ld,
-                   const float2* __restrict__ TX, int N, int nrows, int mode, int nc, int kp,
-                   float* __restrict__ Ut) {
-  extern __shared__ float2 crow[];
-  const int a = blockIdx.y;
-  for (int c = threadIdx.x; c < ncoef; c += blockDim.x) crow[c] = coef[(size_t)a * coef_ld + c];
-  __syncthreads();
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
-  if (x >= N) return;
-  float2 acc = make_float2(0.f, 0.f);
-  if (mode == 0) {
-    for (int c = 0; c < ncoef; ++c) cfma(acc, crow[c], conjf2(TX[(size_t)c * N + x]));
-  } else {
-    for (int c = 0; c < ncoef; ++c) {
-      const int d = c - (nc - 1);
-      const float2 t = d >= 0 ? conjf2(TX[(size_t)d * N + x]) : TX[(size_t)(-d) * N + x];
-      cfma(acc, crow[c], t);
-    }
-    if (a > 0) { acc.x *= 2.f; acc.y *= 2.f; }
+  if (t < tiles) {
+    const float2 p = part[(size_t)t * count + o];
+    v0.x += p.x; v0.y += p.y;
   }
-  Ut[(size_t)x * kp + 2 * a] = acc.x;
-  Ut[(size_t)x * kp + 2 * a + 1] = acc.y;
-  if (a == 0)
-    for (int f = 2 * nrows; f < kp; ++f) Ut[(size_t)x * kp + f] = 0.f;
+  float vx = v0.x + v1.x, vy = v0.y + v1.y;
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    vx += __shfl_xor_sync(0xffffffffu, vx, off);
+    vy += __shfl_xor_sync(0xffffffffu, vy, off);
+  }
+  if (lane == 0) out[o] = make_float2(vx * scale, vy * scale);
 }
 
-cudaError_t launch_expand_cols(cudaStream_t s, const float2* coef, int nrows, int ncoef,
-                               int coef_ld, const float2* TX, int N, int mode, int nc, int kp,
-                               float* Ut) {
-  dim3 grid((N + 127) / 128, nrows);
-  expand_cols_kernel<<<grid, 128, ncoef * sizeof(float2), s>>>(coef, ncoef, coef_ld, TX, N,
-                                                               nrows, mode, nc, kp, Ut);
+cudaError_t launch_reduce_tiles(cudaStream_t s, const float2* part, int tiles, int count,
+                                float scale, float2* out) {
+  reduce_tiles_kernel<<<(count + 7) / 8, 256, 0, s>>>(part, tiles, count, scale, out);
   return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------- row synthesis
-// out[y][x] = sum_f AY[y][f] * Bt[x][f]; the functor is the fused epilogue.
+// out[y][x] = sum_f AY[y][f] * Bt[x][f] (K = kp) with the epilogue applied to the
+// tile through shared memory in two halves, so that every global access of the
+// epilogue is a coalesced float4 (or scalar at ragged edges).
 struct AYLoad {
   const float* AY;
   int N, kp;
   __device__ __forceinline__ void load4(int m, int k, int kend, float* v) {
     if (m < N && k + 3 < kend) {
-      float4 t = __ldg(reinterpret_cast<const float4*>(AY + (size_t)m * kp + k));
+      const float4 t = __ldg(reinterpret_cast<const float4*>(AY + (size_t)m * kp + k));
       v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
     } else {
 #pragma unroll
@@ -260,30 +301,71 @@ struct AYLoad {
 
 constexpr int SY_BMT = 16, SY_BNT = 16, SY_TM = 8, SY_TN = 8, SY_BK = 16;
 constexpr int SY_NT = SY_BMT * SY_BNT;
+constexpr int SY_TILE = 128;
+constexpr int SY_SS = SY_TILE + 4;  // staging row stride
+
+template <class T>
+__device__ __forceinline__ float4 ld4(const T* p, size_t i, int vec, int nvalid) {
+  if (vec && nvalid == 4) return __ldg(reinterpret_cast<const float4*>(p + i));
+  float4 r = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (nvalid > 0) r.x = p[i];
+  if (nvalid > 1) r.y = p[i + 1];
+  if (nvalid > 2) r.z = p[i + 2];
+  if (nvalid > 3) r.w = p[i + 3];
+  return r;
+}
+__device__ __forceinline__ void st4(float* p, size_t i, float4 v, int vec, int nvalid) {
+  if (vec && nvalid == 4) {
+    *reinterpret_cast<float4*>(p + i) = v;
+    return;
+  }
+  if (nvalid > 0) p[i] = v.x;
+  if (nvalid > 1) p[i + 1] = v.y;
+  if (nvalid > 2) p[i + 2] = v.z;
+  if (nvalid > 3) p[i + 3] = v.w;
+}
 
 struct ResistEpi {
   ResistEpilogue p;
-  int N;
+  int N, vec;
   double pe, pen;
-  __device__ __forceinline__ void store(int m, int n, float I) {
-    const size_t i = (size_t)m * N + n;
-    const float W = 1.f / (1.f + expf(-p.alpha * (I - p.thr)));
-    if (p.aerial) p.aerial[i] = I;
-    if (p.wafer) p.wafer[i] = W;
-    if (p.mode == 1) {
-      const float T = p.target[i];
-      const float pw = p.pe_window ? p.pe_window[i] : 1.f;
-      const float r = W - T;
-      pe += (double)r * (double)r * (double)pw;
-      float s = p.pe_weight * r * pw;
-      if (p.penalty != 0.f && T < 0.5f) {
-        const float qw = p.pen_window ? p.pen_window[i] : pw;
-        const float ex = fmaxf(W - p.pen_thr, 0.f);
-        pen += (double)ex * (double)ex * (double)qw;
-        s += p.penalty * ex * qw;
-      }
-      p.dldi[i] = s * W * (1.f - W);
+  __device__ __forceinline__ void one(float I, float T, float pw, float qw, float& W, float& g) {
+    W = 1.f / (1.f + expf(-p.alpha * (I - p.thr)));
+    const float r = W - T;
+    pe += (double)r * (double)r * (double)pw;
+    float s = p.pe_weight * r * pw;
+    if (p.penalty != 0.f && T < 0.5f) {
+      const float ex = fmaxf(W - p.pen_thr, 0.f);
+      pen += (double)ex * (double)ex * (double)qw;
+      s += p.penalty * ex * qw;
     }
+    g = s * W * (1.f - W);
+  }
+  __device__ __forceinline__ void store4(int m, int n, float4 I, int nvalid) {
+    const size_t i = (size_t)m * N + n;
+    if (p.aerial) st4(p.aerial, i, I, vec, nvalid);
+    if (p.mode == 0) {
+      if (p.wafer) {
+        float4 W;
+        W.x = 1.f / (1.f + expf(-p.alpha * (I.x - p.thr)));
+        W.y = 1.f / (1.f + expf(-p.alpha * (I.y - p.thr)));
+        W.z = 1.f / (1.f + expf(-p.alpha * (I.z - p.thr)));
+        W.w = 1.f / (1.f + expf(-p.alpha * (I.w - p.thr)));
+        st4(p.wafer, i, W, vec, nvalid);
+      }
+      return;
+    }
+    const float4 T = ld4(p.target, i, vec, nvalid);
+    const float4 one4 = make_float4(1.f, 1.f, 1.f, 1.f);
+    const float4 pw = p.pe_window ? ld4(p.pe_window, i, vec, nvalid) : one4;
+    const float4 qw = p.pen_window ? ld4(p.pen_window, i, vec, nvalid) : pw;
+    float4 W, g;
+    if (nvalid > 0) one(I.x, T.x, pw.x, qw.x, W.x, g.x);
+    if (nvalid > 1) one(I.y, T.y, pw.y, qw.y, W.y, g.y);
+    if (nvalid > 2) one(I.z, T.z, pw.z, qw.z, W.z, g.z);
+    if (nvalid > 3) one(I.w, T.w, pw.w, qw.w, W.w, g.w);
+    if (p.wafer) st4(p.wafer, i, W, vec, nvalid);
+    st4(p.dldi, i, g, vec, nvalid);
   }
   __device__ __forceinline__ void finish() {
     if (p.mode != 1) return;
@@ -300,16 +382,23 @@ struct ResistEpi {
 
 struct GradEpi {
   GradEpilogue p;
-  int N;
+  int N, vec;
   double nrm;
-  __device__ __forceinline__ void store(int m, int n, float G) {
+  __device__ __forceinline__ void store4(int m, int n, float4 G, int nvalid) {
     const size_t i = (size_t)m * N + n;
-    if (p.grad_mask) p.grad_mask[i] = G;
-    if (p.theta) {
-      const float gt = -0.5f * G * sinf(p.theta[i]);
-      p.grad_theta[i] = gt;
-      nrm += (double)gt * (double)gt;
-    }
+    if (p.grad_mask) st4(p.grad_mask, i, G, vec, nvalid);
+    if (!p.theta) return;
+    const float4 th = ld4(p.theta, i, vec, nvalid);
+    float4 gt;
+    gt.x = -0.5f * G.x * sinf(th.x);
+    gt.y = -0.5f * G.y * sinf(th.y);
+    gt.z = -0.5f * G.z * sinf(th.z);
+    gt.w = -0.5f * G.w * sinf(th.w);
+    if (nvalid > 0) nrm += (double)gt.x * gt.x;
+    if (nvalid > 1) nrm += (double)gt.y * gt.y;
+    if (nvalid > 2) nrm += (double)gt.z * gt.z;
+    if (nvalid > 3) nrm += (double)gt.w * gt.w;
+    st4(p.grad_theta, i, gt, vec, nvalid);
   }
   __device__ __forceinline__ void finish() {
     if (!p.theta) return;
@@ -319,254 +408,332 @@ struct GradEpi {
   }
 };
 
-static dim3 synth_grid(int N) {
-  return dim3((N + SY_BMT * SY_TM - 1) / (SY_BMT * SY_TM),
-              (N + SY_BNT * SY_TN - 1) / (SY_BNT * SY_TN), 1);
+template <class Epi>
+__global__ void __launch_bounds__(SY_NT)
+synth_kernel(const float* __restrict__ AY, const float* __restrict__ Bt, int N, int kp, Epi epi) {
+  __shared__ __align__(16) float As[SY_BK * (SY_TILE + 4)];
+  __shared__ float Bs[SY_BK * (SY_TILE + 1)];
+  extern __shared__ __align__(16) float stage[];  // [64][SY_SS]
+  const int tid = threadIdx.x, tx = tid % SY_BNT, ty = tid / SY_BNT;
+  const int m0 = blockIdx.y * SY_TILE, n0 = blockIdx.x * SY_TILE;
+  float acc[SY_TM][SY_TN];
+#pragma unroll
+  for (int i = 0; i < SY_TM; ++i)
+#pragma unroll
+    for (int j = 0; j < SY_TN; ++j) acc[i][j] = 0.f;
+  AYLoad ld{AY, N, kp};
+  gemm_mainloop<SY_BMT, SY_BNT, SY_TM, SY_TN, SY_BK>(ld, Bt, kp, N, m0, n0, 0, kp, As, Bs, acc);
+  for (int h = 0; h < 2; ++h) {
+    __syncthreads();
+    if (ty / 8 == h) {
+#pragma unroll
+      for (int i = 0; i < SY_TM; ++i)
+#pragma unroll
+        for (int j = 0; j < SY_TN; ++j)
+          stage[(ty * SY_TM + i - 64 * h) * SY_SS + tx + j * SY_BNT] = acc[i][j];
+    }
+    __syncthreads();
+    for (int e = tid; e < 64 * (SY_TILE / 4); e += SY_NT) {
+      const int r = e / (SY_TILE / 4), c4 = (e % (SY_TILE / 4)) * 4;
+      const int m = m0 + 64 * h + r, n = n0 + c4;
+      if (m >= N || n >= N) continue;
+      const float4 v = *reinterpret_cast<const float4*>(&stage[r * SY_SS + c4]);
+      epi.store4(m, n, v, min(4, N - n));
+    }
+  }
+  epi.finish();
 }
+
+static dim3 synth_grid(int N) {
+  const int t = (N + SY_TILE - 1) / SY_TILE;
+  return dim3(t, t, 1);
+}
+
+template <class Epi>
+static cudaError_t launch_synth(cudaStream_t s, const float* AY, const float* Bt, int N, int kp,
+                                const Epi& e) {
+  const int smem = 64 * SY_SS * sizeof(float);
+  cudaError_t err = cudaFuncSetAttribute(synth_kernel<Epi>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (err != cudaSuccess) return err;
+  synth_kernel<Epi><<<synth_grid(N), SY_NT, smem, s>>>(AY, Bt, N, kp, e);
+  return cudaGetLastError();
+}
+
+static int aligned16(const void* p) { return p == nullptr || reinterpret_cast<uintptr_t>(p) % 16 == 0; }
 
 cudaError_t launch_synth_resist(cudaStream_t s, const float* AY, const float* Bt, int N, int kp,
                                 const ResistEpilogue& ep, int* nblocks) {
   const dim3 grid = synth_grid(N);
   *nblocks = grid.x * grid.y;
-  ResistEpi e{ep, N, 0.0, 0.0};
-  AYLoad ld{AY, N, kp};
-  gemm_nt_kernel<SY_BMT, SY_BNT, SY_TM, SY_TN, SY_BK>
-      <<<grid, SY_NT, 0, s>>>(N, N, kp, kp, ld, Bt, kp, e);
-  return cudaGetLastError();
+  const int vec = N % 4 == 0 && aligned16(ep.aerial) && aligned16(ep.wafer) &&
+                  aligned16(ep.target) && aligned16(ep.pe_window) && aligned16(ep.pen_window) &&
+                  aligned16(ep.dldi);
+  return launch_synth(s, AY, Bt, N, kp, ResistEpi{ep, N, vec, 0.0, 0.0});
 }
 
 cudaError_t launch_synth_grad(cudaStream_t s, const float* AY, const float* Bt, int N, int kp,
                               const GradEpilogue& ep, int* nblocks) {
   const dim3 grid = synth_grid(N);
   *nblocks = grid.x * grid.y;
-  GradEpi e{ep, N, 0.0};
-  AYLoad ld{AY, N, kp};
-  gemm_nt_kernel<SY_BMT, SY_BNT, SY_TM, SY_TN, SY_BK>
-      <<<grid, SY_NT, 0, s>>>(N, N, kp, kp, ld, Bt, kp, e);
-  return cudaGetLastError();
+  const int vec = N % 4 == 0 && aligned16(ep.grad_mask) && aligned16(ep.theta) &&
+                  aligned16(ep.grad_theta);
+  return launch_synth(s, AY, Bt, N, kp, GradEpi{ep, N, vec, 0.0});
 }
 
 // ---------------------------------------------------------------- small-grid band stage
-// Forward 1: T[k][r][jc] = sum_c H[k][r][c] m[r][c] ESc_t[c][jc],  m = sum_ys mpart[ys][r][c].
-__global__ void band_fwd1_kernel(const float2* __restrict__ H, const float2* __restrict__ mpart,
-                                 int ysplit, int Nr, int Nc, int Pc,
-                                 const float2* __restrict__ ESc_t, float2* __restrict__ mband,
-                                 float2* __restrict__ T) {
-  extern __shared__ float2 ah[];
-  const int r = blockIdx.x, k = blockIdx.y;
-  for (int c = threadIdx.x; c < Nc; c += blockDim.x) {
-    float2 m = make_float2(0.f, 0.f);
-    for (int ys = 0; ys < ysplit; ++ys) {
-      const float2 p = mpart[((size_t)ys * Nr + r) * Nc + c];
-      m.x += p.x; m.y += p.y;
-    }
-    if (k == 0 && mband) mband[(size_t)r * Nc + c] = m;
-    ah[c] = cmul(H[((size_t)k * Nr + r) * Nc + c], m);
-  }
+// Forward 1 (one CTA per kernel k): A = H_k m on the band, T = A ESc^T (Nr x Pc,
+// shared memory), e_k = ESr T (Pr x Pc) and ik = w_k |e_k|^2.
+constexpr int BF_NT = 512;
+__global__ void __launch_bounds__(BF_NT)
+band_fields_kernel(const float2* __restrict__ H, const float2* __restrict__ mband,
+                   const float* __restrict__ w, int Nr, int Nc, int Pr, int Pc,
+                   const float2* __restrict__ ESc_t, const float2* __restrict__ ESr_t,
+                   float2* __restrict__ e, float* __restrict__ ik) {
+  extern __shared__ float2 sm2[];
+  float2* A = sm2;              // [Nr][Nc]
+  float2* T = sm2 + Nr * Nc;    // [Nr][Pc]
+  const int k = blockIdx.x;
+  for (int i = threadIdx.x; i < Nr * Nc; i += BF_NT) A[i] = cmul(H[(size_t)k * Nr * Nc + i], mband[i]);
   __syncthreads();
-  for (int jc = threadIdx.x; jc < Pc; jc += blockDim.x) {
-    float2 acc = make_float2(0.f, 0.f);
-    for (int c = 0; c < Nc; ++c) cfma(acc, ah[c], ESc_t[(size_t)c * Pc + jc]);
-    T[((size_t)k * Nr + r) * Pc + jc] = acc;
+  for (int i = threadIdx.x; i < Nr * Pc; i += BF_NT) {
+    const int r = i / Pc, jc = i % Pc;
+    float2 a0 = make_float2(0.f, 0.f), a1 = a0;
+    int c = 0;
+    for (; c + 1 < Nc; c += 2) {
+      cfma(a0, A[r * Nc + c], ESc_t[(size_t)c * Pc + jc]);
+      cfma(a1, A[r * Nc + c + 1], ESc_t[(size_t)(c + 1) * Pc + jc]);
+    }
+    if (c < Nc) cfma(a0, A[r * Nc + c], ESc_t[(size_t)c * Pc + jc]);
+    T[i] = make_float2(a0.x + a1.x, a0.y + a1.y);
   }
-}
-
-// Forward 2: e[k][jr][jc] = sum_r ESr_t[r][jr] T[k][r][jc]; ik[k][jr][jc] = w_k |e|^2.
-__global__ void band_fwd2_kernel(const float2* __restrict__ T, const float2* __restrict__ ESr_t,
-                                 const float* __restrict__ w, int Nr, int Pr, int Pc,
-                                 float2* __restrict__ e, float* __restrict__ ik) {
-  extern __shared__ float2 er[];
-  const int jr = blockIdx.x, k = blockIdx.y;
-  for (int r = threadIdx.x; r < Nr; r += blockDim.x) er[r] = ESr_t[(size_t)r * Pr + jr];
   __syncthreads();
   const float wk = w[k];
-  for (int jc = threadIdx.x; jc < Pc; jc += blockDim.x) {
-    float2 acc = make_float2(0.f, 0.f);
-    for (int r = 0; r < Nr; ++r) cfma(acc, er[r], T[((size_t)k * Nr + r) * Pc + jc]);
-    const size_t o = ((size_t)k * Pr + jr) * Pc + jc;
-    e[o] = acc;
-    ik[o] = wk * (acc.x * acc.x + acc.y * acc.y);
-  }
-}
-
-// Forward 3: Q[jr][dc] = sum_jc i[jr][jc] conj(EDc_t[dc][jc]),  i = sum_k ik[k] (k order).
-__global__ void band_fwd3_kernel(const float* __restrict__ ik, int K, int Pr, int Pc, int nd,
-                                 const float2* __restrict__ EDc_t, float2* __restrict__ Q) {
-  extern __shared__ float irow[];
-  const int jr = blockIdx.x;
-  for (int jc = threadIdx.x; jc < Pc; jc += blockDim.x) {
-    float s = 0.f;
-    for (int k = 0; k < K; ++k) s += ik[((size_t)k * Pr + jr) * Pc + jc];
-    irow[jc] = s;
-  }
-  __syncthreads();
-  for (int dc = threadIdx.x; dc < nd; dc += blockDim.x) {
-    float2 acc = make_float2(0.f, 0.f);
-    for (int jc = 0; jc < Pc; ++jc) {
-      const float2 t = EDc_t[(size_t)dc * Pc + jc];
-      acc.x = fmaf(irow[jc], t.x, acc.x);
-      acc.y = fmaf(-irow[jc], t.y, acc.y);
+  for (int i = threadIdx.x; i < Pr * Pc; i += BF_NT) {
+    const int jr = i / Pc, jc = i % Pc;
+    float2 a0 = make_float2(0.f, 0.f), a1 = a0;
+    int r = 0;
+    for (; r + 1 < Nr; r += 2) {
+      cfma(a0, ESr_t[(size_t)r * Pr + jr], T[r * Pc + jc]);
+      cfma(a1, ESr_t[(size_t)(r + 1) * Pr + jr], T[(r + 1) * Pc + jc]);
     }
-    Q[(size_t)jr * nd + dc] = acc;
+    if (r < Nr) cfma(a0, ESr_t[(size_t)r * Pr + jr], T[r * Pc + jc]);
+    const float2 v = make_float2(a0.x + a1.x, a0.y + a1.y);
+    const size_t o = (size_t)k * Pr * Pc + i;
+    e[o] = v;
+    ik[o] = wk * (v.x * v.x + v.y * v.y);
   }
 }
 
-// Forward 4: chat[dr][dc] = sum_jr conj(EDr_t[dr + Nr - 1][jr]) Q[jr][dc] / (Pr Pc), dr >= 0.
-__global__ void band_fwd4_kernel(const float2* __restrict__ Q, int Nr, int Pr, int nd,
-                                 const float2* __restrict__ EDr_t, float inv,
-                                 float2* __restrict__ chat) {
+// Forward 2: i[j] = sum_k ik[k][j] in k order.
+__global__ void sum_k_kernel(const float* __restrict__ ik, int K, int n, float* __restrict__ iP) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  float s = 0.f;
+  for (int k = 0; k < K; ++k) s += ik[(size_t)k * n + j];
+  iP[j] = s;
+}
+
+// Forward 3 (one CTA per band row dr >= 0): chat[dr][dc] = DFT_P(i)(dr, dc) / (Pr Pc)
+// over dc in [-(Nc-1), Nc-1], then U[dr][x] = kappa(dr) sum_dc chat[dr][dc] e^{2 pi i dc x/N}
+// written as Ut[x][2 dr + {0,1}] for the row synthesis (kappa = 2 for dr > 0: the
+// Hermitian half of the spectrum of a real image).
+constexpr int BI_NT = 256;
+__global__ void __launch_bounds__(BI_NT)
+band_image_kernel(const float* __restrict__ iP, int Nr, int Nc, int Pr, int Pc,
+                  const float2* __restrict__ EDr_t, const float2* __restrict__ EDc,
+                  const float2* __restrict__ TXDc, int N, int kp, float inv,
+                  float* __restrict__ Ut) {
+  extern __shared__ float2 sb[];
+  float2* v = sb;             // [Pc]
+  float2* ch = sb + Pc;       // [2Nc - 1]
   const int dr = blockIdx.x;
+  const int nd = 2 * Nc - 1;
   const float2* ed = EDr_t + (size_t)(dr + Nr - 1) * Pr;
-  for (int dc = threadIdx.x; dc < nd; dc += blockDim.x) {
-    float2 acc = make_float2(0.f, 0.f);
-    for (int jr = 0; jr < Pr; ++jr) cfma(acc, conjf2(ed[jr]), Q[(size_t)jr * nd + dc]);
-    chat[(size_t)dr * nd + dc] = make_float2(acc.x * inv, acc.y * inv);
-  }
-}
-
-static int pick_threads(int n) {
-  int t = 32;
-  while (t < n && t < 256) t <<= 1;
-  return t;
-}
-
-cudaError_t launch_band_forward(cudaStream_t s, const Cache& c, const float2* mpart,
-                                int ysplit, Field& f, float* ik, float2* T, float2* Q,
-                                float2* chat, float* Ut) {
-  const BandGeom& g = c.g;
-  band_fwd1_kernel<<<dim3(g.Nr, g.K), pick_threads(g.Pc), g.Nc * sizeof(float2), s>>>(
-      c.H, mpart, ysplit, g.Nr, g.Nc, g.Pc, c.ESc_t, f.mband, T);
-  band_fwd2_kernel<<<dim3(g.Pr, g.K), pick_threads(g.Pc), g.Nr * sizeof(float2), s>>>(
-      T, c.ESr_t, c.w, g.Nr, g.Pr, g.Pc, f.e, ik);
-  const int nd = 2 * g.Nc - 1;
-  band_fwd3_kernel<<<g.Pr, pick_threads(nd), g.Pc * sizeof(float), s>>>(ik, g.K, g.Pr, g.Pc,
-                                                                         nd, c.EDc_t, Q);
-  band_fwd4_kernel<<<g.Nr, pick_threads(nd), 0, s>>>(Q, g.Nr, g.Pr, nd, c.EDr_t,
-                                                     1.f / ((float)g.Pr * (float)g.Pc), chat);
-  // U[dr][x] (dr = 0..Nr-1, Hermitian half with kappa) for the row synthesis.
-  return launch_expand_cols(s, chat, g.Nr, nd, nd, c.TXDc, g.N, 1, g.Nc, g.kp_rows, Ut);
-}
-
-// Adjoint 1: Gam[a][jc] = sum_{c < Nc} kappa(c) g'[a][c] EDc_t[c + Nc - 1][jc],
-//            g' = sum_ys gpart[ys][a][c], a = dr + Nr - 1 in [0, 2Nr - 1).
-__global__ void band_adj1_kernel(const float2* __restrict__ gpart, int ysplit, int na, int Nc,
-                                 int Pc, const float2* __restrict__ EDc_t,
-                                 float2* __restrict__ Gam) {
-  extern __shared__ float2 grow[];
-  const int a = blockIdx.x;
-  for (int c = threadIdx.x; c < Nc; c += blockDim.x) {
-    float2 v = make_float2(0.f, 0.f);
-    for (int ys = 0; ys < ysplit; ++ys) {
-      const float2 p = gpart[((size_t)ys * na + a) * Nc + c];
-      v.x += p.x; v.y += p.y;
+  for (int jc = threadIdx.x; jc < Pc; jc += BI_NT) {
+    float2 a = make_float2(0.f, 0.f);
+    for (int jr = 0; jr < Pr; ++jr) {
+      const float iv = iP[(size_t)jr * Pc + jc];
+      const float2 t = ed[jr];
+      a.x = fmaf(t.x, iv, a.x);
+      a.y = fmaf(-t.y, iv, a.y);
     }
-    const float kc = c > 0 ? 2.f : 1.f;
-    grow[c] = make_float2(v.x * kc, v.y * kc);
+    v[jc] = a;
   }
   __syncthreads();
-  for (int jc = threadIdx.x; jc < Pc; jc += blockDim.x) {
-    float2 acc = make_float2(0.f, 0.f);
-    for (int c = 0; c < Nc; ++c) cfma(acc, grow[c], EDc_t[(size_t)(c + Nc - 1) * Pc + jc]);
-    Gam[(size_t)a * Pc + jc] = acc;
+  for (int dc = threadIdx.x; dc < nd; dc += BI_NT) {
+    float2 a = make_float2(0.f, 0.f);
+    for (int jc = 0; jc < Pc; ++jc) cfma(a, v[jc], conjf2(EDc[(size_t)jc * nd + dc]));
+    ch[dc] = make_float2(a.x * inv, a.y * inv);
+  }
+  __syncthreads();
+  const float kap = dr > 0 ? 2.f : 1.f;
+  for (int x = threadIdx.x; x < N; x += BI_NT) {
+    float2 a = make_float2(0.f, 0.f);
+    for (int c = 0; c < nd; ++c) {
+      const int d = c - (Nc - 1);
+      const float2 t = d >= 0 ? conjf2(TXDc[(size_t)d * N + x]) : TXDc[(size_t)(-d) * N + x];
+      cfma(a, ch[c], t);
+    }
+    Ut[(size_t)x * kp + 2 * dr] = kap * a.x;
+    Ut[(size_t)x * kp + 2 * dr + 1] = kap * a.y;
+    if (dr == 0)
+      for (int f = 2 * Nr; f < kp; ++f) Ut[(size_t)x * kp + f] = 0.f;
   }
 }
 
-// Adjoint 2: gam[jr][jc] = Re sum_a EDr_t[a][jr] Gam[a][jc]   (gamma is real).
-__global__ void band_adj2_kernel(const float2* __restrict__ Gam, int na, int Pr, int Pc,
-                                 const float2* __restrict__ EDr_t, float* __restrict__ gam) {
-  extern __shared__ float2 ed[];
+cudaError_t launch_band_forward(cudaStream_t s, const Cache& c, Field& f, float* ik, float* iP,
+                                float* Ut) {
+  const BandGeom& g = c.g;
+  const size_t sm1 = (size_t)(g.Nr * g.Nc + g.Nr * g.Pc) * sizeof(float2);
+  cudaError_t err = cudaFuncSetAttribute(band_fields_kernel,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1);
+  if (err != cudaSuccess) return err;
+  band_fields_kernel<<<g.K, BF_NT, sm1, s>>>(c.H, f.mband, c.w, g.Nr, g.Nc, g.Pr, g.Pc, c.ESc_t,
+                                             c.ESr_t, f.e, ik);
+  const int n = g.Pr * g.Pc;
+  sum_k_kernel<<<(n + 255) / 256, 256, 0, s>>>(ik, g.K, n, iP);
+  const size_t sm3 = (size_t)(g.Pc + 2 * g.Nc - 1) * sizeof(float2);
+  band_image_kernel<<<g.Nr, BI_NT, sm3, s>>>(iP, g.Nr, g.Nc, g.Pr, g.Pc, c.EDr_t, c.EDc, c.TXDc,
+                                             g.N, g.kp_rows, 1.f / ((float)g.Pr * (float)g.Pc),
+                                             Ut);
+  return cudaGetLastError();
+}
+
+size_t band_fields_smem(const BandGeom& g) {
+  return (size_t)(g.Nr * g.Nc + g.Nr * g.Pc) * sizeof(float2);
+}
+
+// Adjoint 1 (one CTA per small-grid row jr):
+//   wv[c] = sum_a EDr_t[a][jr] kappa(c) g'[a][c]   (a = dr + Nr - 1, c = dc >= 0)
+//   gamma[jr][jc] = Re sum_c wv[c] EDc_t[c + Nc - 1][jc]   (gamma is real)
+__global__ void __launch_bounds__(256)
+band_gamma_kernel(const float2* __restrict__ gh, int Nr, int Nc, int Pr, int Pc,
+                  const float2* __restrict__ EDr_t, const float2* __restrict__ EDc_t,
+                  float* __restrict__ gam) {
+  extern __shared__ float2 sg[];  // [Nc]
   const int jr = blockIdx.x;
-  for (int a = threadIdx.x; a < na; a += blockDim.x) ed[a] = EDr_t[(size_t)a * Pr + jr];
+  const int na = 2 * Nr - 1;
+  for (int c = threadIdx.x; c < Nc; c += blockDim.x) {
+    float2 a = make_float2(0.f, 0.f);
+    for (int r = 0; r < na; ++r) cfma(a, EDr_t[(size_t)r * Pr + jr], gh[(size_t)r * Nc + c]);
+    const float kc = c > 0 ? 2.f : 1.f;
+    sg[c] = make_float2(kc * a.x, kc * a.y);
+  }
   __syncthreads();
   for (int jc = threadIdx.x; jc < Pc; jc += blockDim.x) {
     float acc = 0.f;
-    for (int a = 0; a < na; ++a) {
-      const float2 t = Gam[(size_t)a * Pc + jc];
-      acc = fmaf(ed[a].x, t.x, fmaf(-ed[a].y, t.y, acc));
+    for (int c = 0; c < Nc; ++c) {
+      const float2 t = EDc_t[(size_t)(c + Nc - 1) * Pc + jc];
+      acc = fmaf(sg[c].x, t.x, fmaf(-sg[c].y, t.y, acc));
     }
     gam[(size_t)jr * Pc + jc] = acc;
   }
 }
 
-// Adjoint 3: Z1[k][jr][uc] = sum_jc e[k][jr][jc] gam[jr][jc] conj(ESc[jc][uc]).
-__global__ void band_adj3_kernel(const float2* __restrict__ e, const float* __restrict__ gam,
-                                 int Pr, int Pc, int Nc, const float2* __restrict__ ESc,
-                                 float2* __restrict__ Z1) {
-  extern __shared__ float2 q[];
-  const int jr = blockIdx.x, k = blockIdx.y;
-  for (int jc = threadIdx.x; jc < Pc; jc += blockDim.x) {
-    const float2 v = e[((size_t)k * Pr + jr) * Pc + jc];
-    const float gv = gam[(size_t)jr * Pc + jc];
-    q[jc] = make_float2(v.x * gv, v.y * gv);
+// Adjoint 2 (one CTA per kernel k): Z1[jr][uc] = sum_jc e_k[jr][jc] gamma[jr][jc] conj(ESc[jc][uc])
+// (shared memory), Zk[ur][uc] = sum_jr conj(ESr_t[ur][jr]) Z1[jr][uc] / (Pr Pc).
+__global__ void __launch_bounds__(BF_NT)
+band_z_kernel(const float2* __restrict__ e, const float* __restrict__ gam, int Nr, int Nc, int Pr,
+              int Pc, const float2* __restrict__ ESc, const float2* __restrict__ ESr_t, float inv,
+              float2* __restrict__ Zk) {
+  extern __shared__ float2 sz[];  // [Pr][Nc]
+  const int k = blockIdx.x;
+  const float2* ek = e + (size_t)k * Pr * Pc;
+  for (int i = threadIdx.x; i < Pr * Nc; i += BF_NT) {
+    const int jr = i / Nc, uc = i % Nc;
+    float2 a0 = make_float2(0.f, 0.f), a1 = a0;
+    int jc = 0;
+    for (; jc + 1 < Pc; jc += 2) {
+      const float2 v0 = ek[(size_t)jr * Pc + jc];
+      const float g0 = gam[(size_t)jr * Pc + jc];
+      const float2 v1 = ek[(size_t)jr * Pc + jc + 1];
+      const float g1 = gam[(size_t)jr * Pc + jc + 1];
+      cfma(a0, make_float2(v0.x * g0, v0.y * g0), conjf2(ESc[(size_t)jc * Nc + uc]));
+      cfma(a1, make_float2(v1.x * g1, v1.y * g1), conjf2(ESc[(size_t)(jc + 1) * Nc + uc]));
+    }
+    if (jc < Pc) {
+      const float2 v0 = ek[(size_t)jr * Pc + jc];
+      const float g0 = gam[(size_t)jr * Pc + jc];
+      cfma(a0, make_float2(v0.x * g0, v0.y * g0), conjf2(ESc[(size_t)jc * Nc + uc]));
+    }
+    sz[i] = make_float2(a0.x + a1.x, a0.y + a1.y);
   }
   __syncthreads();
+  for (int i = threadIdx.x; i < Nr * Nc; i += BF_NT) {
+    const int ur = i / Nc, uc = i % Nc;
+    float2 a0 = make_float2(0.f, 0.f), a1 = a0;
+    int jr = 0;
+    for (; jr + 1 < Pr; jr += 2) {
+      cfma(a0, conjf2(ESr_t[(size_t)ur * Pr + jr]), sz[jr * Nc + uc]);
+      cfma(a1, conjf2(ESr_t[(size_t)ur * Pr + jr + 1]), sz[(jr + 1) * Nc + uc]);
+    }
+    if (jr < Pr) cfma(a0, conjf2(ESr_t[(size_t)ur * Pr + jr]), sz[jr * Nc + uc]);
+    Zk[(size_t)k * Nr * Nc + i] = make_float2((a0.x + a1.x) * inv, (a0.y + a1.y) * inv);
+  }
+}
+
+// Adjoint 3 (one CTA per band row ur): X[ur][uc] = scale sum_k w_k conj(H_k) Z_k (k order),
+// V[ur][x] = sum_uc X[ur][uc] e^{2 pi i s_uc x/N}, written as Vt[x][2 ur + {0,1}].
+__global__ void __launch_bounds__(256)
+band_x_kernel(const float2* __restrict__ Zk, const float2* __restrict__ H,
+              const float* __restrict__ w, int K, int Nr, int Nc, float scale,
+              const float2* __restrict__ TXSc, int N, int kp, float* __restrict__ Vt) {
+  extern __shared__ float2 sx[];  // [Nc]
+  const int ur = blockIdx.x;
+  const int nb = Nr * Nc;
   for (int uc = threadIdx.x; uc < Nc; uc += blockDim.x) {
+    const int u = ur * Nc + uc;
     float2 acc = make_float2(0.f, 0.f);
-    for (int jc = 0; jc < Pc; ++jc) cfma(acc, q[jc], conjf2(ESc[(size_t)jc * Nc + uc]));
-    Z1[((size_t)k * Pr + jr) * Nc + uc] = acc;
+    for (int k = 0; k < K; ++k) {
+      const float2 t = cmul(conjf2(H[(size_t)k * nb + u]), Zk[(size_t)k * nb + u]);
+      acc.x = fmaf(w[k], t.x, acc.x);
+      acc.y = fmaf(w[k], t.y, acc.y);
+    }
+    sx[uc] = make_float2(acc.x * scale, acc.y * scale);
+  }
+  __syncthreads();
+  for (int x = threadIdx.x; x < N; x += blockDim.x) {
+    float2 a = make_float2(0.f, 0.f);
+    for (int uc = 0; uc < Nc; ++uc) cfma(a, sx[uc], conjf2(TXSc[(size_t)uc * N + x]));
+    Vt[(size_t)x * kp + 2 * ur] = a.x;
+    Vt[(size_t)x * kp + 2 * ur + 1] = a.y;
+    if (ur == 0)
+      for (int f = 2 * Nr; f < kp; ++f) Vt[(size_t)x * kp + f] = 0.f;
   }
 }
 
-// Adjoint 4: Zk[k][ur][uc] = sum_jr conj(ESr_t[ur][jr]) Z1[k][jr][uc] / (Pr Pc).
-__global__ void band_adj4_kernel(const float2* __restrict__ Z1, int Pr, int Nc,
-                                 const float2* __restrict__ ESr_t, float inv,
-                                 float2* __restrict__ Zk, int Nr) {
-  const int ur = blockIdx.x, k = blockIdx.y;
-  const float2* es = ESr_t + (size_t)ur * Pr;
-  for (int uc = threadIdx.x; uc < Nc; uc += blockDim.x) {
-    float2 acc = make_float2(0.f, 0.f);
-    for (int jr = 0; jr < Pr; ++jr) cfma(acc, conjf2(es[jr]), Z1[((size_t)k * Pr + jr) * Nc + uc]);
-    Zk[((size_t)k * Nr + ur) * Nc + uc] = make_float2(acc.x * inv, acc.y * inv);
-  }
-}
-
-// Adjoint 5: X[u] = scale * sum_k w_k conj(H[k][u]) Zk[k][u]  (k order).
-__global__ void band_adj5_kernel(const float2* __restrict__ Zk, const float2* __restrict__ H,
-                                 const float* __restrict__ w, int K, int nb, float scale,
-                                 float2* __restrict__ X) {
-  const int u = blockIdx.x * blockDim.x + threadIdx.x;
-  if (u >= nb) return;
-  float2 acc = make_float2(0.f, 0.f);
-  for (int k = 0; k < K; ++k) {
-    const float2 t = cmul(conjf2(H[(size_t)k * nb + u]), Zk[(size_t)k * nb + u]);
-    acc.x = fmaf(w[k], t.x, acc.x);
-    acc.y = fmaf(w[k], t.y, acc.y);
-  }
-  X[u] = make_float2(acc.x * scale, acc.y * scale);
-}
-
-cudaError_t launch_band_adjoint(cudaStream_t s, const Cache& c, const Field& f,
-                                const float2* gpart, int ysplit, double scale, float2* Gam,
-                                float* gam, float2* Z1, float2* Zk, float2* X, float* Vt) {
+cudaError_t launch_band_adjoint(cudaStream_t s, const Cache& c, const Field& f, const float2* gh,
+                                double scale, float* gam, float2* Zk, float* Vt) {
   const BandGeom& g = c.g;
-  const int na = 2 * g.Nr - 1;
-  band_adj1_kernel<<<na, pick_threads(g.Pc), g.Nc * sizeof(float2), s>>>(gpart, ysplit, na, g.Nc,
-                                                                         g.Pc, c.EDc_t, Gam);
-  band_adj2_kernel<<<g.Pr, pick_threads(g.Pc), na * sizeof(float2), s>>>(Gam, na, g.Pr, g.Pc,
-                                                                         c.EDr_t, gam);
-  band_adj3_kernel<<<dim3(g.Pr, g.K), pick_threads(g.Nc), g.Pc * sizeof(float2), s>>>(
-      f.e, gam, g.Pr, g.Pc, g.Nc, c.ESc, Z1);
-  band_adj4_kernel<<<dim3(g.Nr, g.K), pick_threads(g.Nc), 0, s>>>(
-      Z1, g.Pr, g.Nc, c.ESr_t, 1.f / ((float)g.Pr * (float)g.Pc), Zk, g.Nr);
-  const int nb = g.Nr * g.Nc;
-  band_adj5_kernel<<<(nb + 127) / 128, 128, 0, s>>>(Zk, c.H, c.w, g.K, nb, (float)scale, X);
-  return launch_expand_cols(s, X, g.Nr, g.Nc, g.Nc, c.TXSc, g.N, 0, g.Nc, g.kp_rows, Vt);
+  band_gamma_kernel<<<g.Pr, 256, g.Nc * sizeof(float2), s>>>(gh, g.Nr, g.Nc, g.Pr, g.Pc, c.EDr_t,
+                                                             c.EDc_t, gam);
+  const size_t smz = (size_t)g.Pr * g.Nc * sizeof(float2);
+  cudaError_t err = cudaFuncSetAttribute(band_z_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smz);
+  if (err != cudaSuccess) return err;
+  band_z_kernel<<<g.K, BF_NT, smz, s>>>(f.e, gam, g.Nr, g.Nc, g.Pr, g.Pc, c.ESc, c.ESr_t,
+                                        1.f / ((float)g.Pr * (float)g.Pc), Zk);
+  band_x_kernel<<<g.Nr, 256, g.Nc * sizeof(float2), s>>>(Zk, c.H, c.w, g.K, g.Nr, g.Nc,
+                                                         (float)scale, c.TXSc, g.N, g.kp_rows, Vt);
+  return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------- FP64 partial sums
 __global__ void sum_partials_kernel(const double* __restrict__ part, int n, int stride,
                                     double* __restrict__ out) {
-  // One thread per component, fixed order (deterministic).
-  const int comp = threadIdx.x;
-  if (comp >= stride) return;
+  // One warp per component; lanes stride over blocks, then a fixed shuffle tree.
+  const int comp = blockIdx.x;
   double s = 0.0;
-  for (int i = 0; i < n; ++i) s += part[(size_t)i * stride + comp];
-  out[comp] = s;
+  for (int i = threadIdx.x; i < n; i += 32) s += part[(size_t)i * stride + comp];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (threadIdx.x == 0) out[comp] = s;
 }
 
 cudaError_t launch_sum_partials(cudaStream_t s, const double* part, int n, int stride,
                                 double* out) {
-  sum_partials_kernel<<<1, 32, 0, s>>>(part, n, stride, out);
+  sum_partials_kernel<<<stride, 32, 0, s>>>(part, n, stride, out);
   return cudaGetLastError();
 }
 

@@ -156,6 +156,17 @@ struct LsArgs {
 };
 
 __global__ void __launch_bounds__(LS_NT) levelset_kernel(LsArgs a) {
+  if (a.what == 5) {  // printed mask: phi >= 0 (LSM_Optimizer.cpp:128)
+    const int x = blockIdx.x * LS_TX + threadIdx.x % LS_TX;
+    for (int r = 0; r < LS_RPT; ++r) {
+      const int y = blockIdx.y * LS_TY * LS_RPT + threadIdx.x / LS_TX + r * LS_TY;
+      if (y < a.rows && x < a.cols) {
+        const size_t i = (size_t)y * a.cols + x;
+        a.out[i] = a.phi[i] >= 0.f ? 1.f : 0.f;
+      }
+    }
+    return;
+  }
   __shared__ float t[LS_SH][LS_SW];
   const int x0 = blockIdx.x * LS_TX;
   const int y0 = blockIdx.y * LS_TY * LS_RPT;
@@ -230,6 +241,181 @@ __global__ void dt_kernel(const float* __restrict__ part, int n, float dx, float
   const double den = normal + kap;
   *vmax = m;
   *dt = den < 1e-9 ? 1e-3f : (float)(cfl / den);
+}
+
+// ---------------------------------------------------------------- reinit_sdf
+// LevelSetUtils::reinit_sdf (level_set_utils.cpp:290-319): two OpenCV
+// distanceTransform(DIST_L2, 5) calls, i.e. the 5x5 chamfer distance with
+// weights a = 1, b = 1.4, c = 2.1969 (float32) to the nearest feature pixel,
+// computed by a forward raster pass (rows top to bottom, left to right) and a
+// backward pass. Within a row the only dependency is d(j) = min(g(j), d(j-1) + a),
+// which is evaluated exactly as a min-plus prefix scan
+//   d(j) = j + min_{k <= j} (g(k) - k)     (double precision, then float),
+// g being the minimum over the already final rows above (below) plus the
+// pixel's own value. One CTA runs one transform; blockIdx.x = 0 measures
+// inside pixels (phi > 0) to the outside and writes +d dx to sdf there,
+// blockIdx.x = 1 measures outside pixels to the inside and writes -d dx. Each
+// pixel of sdf is written by exactly one of the two CTAs. With no feature
+// pixel at all the distance stays FLT_MAX, as OpenCV returns.
+constexpr int DT_NT = 1024;
+constexpr float DT_A = 1.0f, DT_B = 1.4f, DT_C = 2.1969f;
+
+__device__ __forceinline__ double dt_block_min_scan(double v, double* wsum, bool reverse) {
+  // inclusive prefix (reverse: suffix) minimum over the block in thread order
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const double u = reverse ? __shfl_down_sync(0xffffffffu, v, o) : __shfl_up_sync(0xffffffffu, v, o);
+    if (reverse ? (lane + o < 32) : (lane >= o)) v = fmin(v, u);
+  }
+  if (lane == (reverse ? 0 : 31)) wsum[warp] = v;
+  __syncthreads();
+  if (warp == 0) {
+    double t = wsum[lane];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const double u = reverse ? __shfl_down_sync(0xffffffffu, t, o) : __shfl_up_sync(0xffffffffu, t, o);
+      if (reverse ? (lane + o < 32) : (lane >= o)) t = fmin(t, u);
+    }
+    wsum[32 + lane] = t;  // inclusive scan of warp totals
+  }
+  __syncthreads();
+  double carry = 1e300;
+  if (!reverse && warp > 0) carry = wsum[32 + warp - 1];
+  if (reverse && warp < 31) carry = wsum[32 + warp + 1];
+  __syncthreads();
+  return fmin(v, carry);
+}
+
+__global__ void __launch_bounds__(DT_NT)
+chamfer_sdf_kernel(const float* __restrict__ phi, int rows, int cols, float dx,
+                   float* __restrict__ work, float* __restrict__ sdf) {
+  extern __shared__ float rowbuf[];  // 3 rows of cols floats: ring of the last rows
+  __shared__ double wsum[64];
+  const bool inside_pass = blockIdx.x == 0;
+  float* d = work + (size_t)blockIdx.x * rows * cols;
+  const int per = (cols + DT_NT - 1) / DT_NT;  // contiguous columns per thread
+  const int j0 = threadIdx.x * per;
+  const float FMAX = 3.402823466e38f;
+  auto feature = [&](int i, int j) {
+    const float p = phi[(size_t)i * cols + j];
+    return inside_pass ? !(p > 0.f) : (p > 0.f);
+  };
+  // ---- forward pass
+  for (int i = 0; i < rows; ++i) {
+    float* r0 = rowbuf + (i % 3) * cols;
+    const float* r1 = rowbuf + ((i + 2) % 3) * cols;  // row i-1
+    const float* r2 = rowbuf + ((i + 1) % 3) * cols;  // row i-2
+    double local = 1e300;
+    for (int q = 0; q < per; ++q) {
+      const int j = j0 + q;
+      if (j >= cols) break;
+      float g = FMAX;
+      if (feature(i, j)) {
+        g = 0.f;
+      } else {
+        if (i >= 1) {
+          g = fminf(g, r1[j] + DT_A);
+          if (j >= 1) g = fminf(g, r1[j - 1] + DT_B);
+          if (j + 1 < cols) g = fminf(g, r1[j + 1] + DT_B);
+          if (j >= 2) g = fminf(g, r1[j - 2] + DT_C);
+          if (j + 2 < cols) g = fminf(g, r1[j + 2] + DT_C);
+        }
+        if (i >= 2) {
+          if (j >= 1) g = fminf(g, r2[j - 1] + DT_C);
+          if (j + 1 < cols) g = fminf(g, r2[j + 1] + DT_C);
+        }
+      }
+      const double u = (g >= FMAX ? 1e300 : (double)g - (double)j);
+      local = fmin(local, u);
+      r0[j] = g;  // provisional
+    }
+    // exclusive carry from the threads on the left
+    const double incl = dt_block_min_scan(local, wsum, false);
+    double run = 1e300;
+    {
+      // recover the exclusive prefix of this thread: scan again within the thread
+      const double left = __shfl_up_sync(0xffffffffu, incl, 1);
+      const int lane = threadIdx.x & 31;
+      if (lane > 0) run = left;
+      else if (threadIdx.x > 0) run = wsum[32 + (threadIdx.x >> 5) - 1];
+    }
+    for (int q = 0; q < per; ++q) {
+      const int j = j0 + q;
+      if (j >= cols) break;
+      const float g = r0[j];
+      const double u = (g >= FMAX ? 1e300 : (double)g - (double)j);
+      run = fmin(run, u);
+      const double v = run + (double)j;
+      r0[j] = v >= 1e299 ? FMAX : fminf(g, (float)v);
+      d[(size_t)i * cols + j] = r0[j];
+    }
+    __syncthreads();
+  }
+  // ---- backward pass
+  for (int i = rows - 1; i >= 0; --i) {
+    const int slot = (rows - 1 - i);
+    float* r0 = rowbuf + (slot % 3) * cols;
+    const float* r1 = rowbuf + ((slot + 2) % 3) * cols;  // row i+1 (final)
+    const float* r2 = rowbuf + ((slot + 1) % 3) * cols;  // row i+2 (final)
+    double local = 1e300;
+    for (int q = 0; q < per; ++q) {
+      const int j = j0 + q;
+      if (j >= cols) break;
+      float g = d[(size_t)i * cols + j];
+      if (g > DT_A) {
+        if (i + 1 < rows) {
+          g = fminf(g, r1[j] + DT_A);
+          if (j + 1 < cols) g = fminf(g, r1[j + 1] + DT_B);
+          if (j >= 1) g = fminf(g, r1[j - 1] + DT_B);
+          if (j + 2 < cols) g = fminf(g, r1[j + 2] + DT_C);
+          if (j >= 2) g = fminf(g, r1[j - 2] + DT_C);
+        }
+        if (i + 2 < rows) {
+          if (j + 1 < cols) g = fminf(g, r2[j + 1] + DT_C);
+          if (j >= 1) g = fminf(g, r2[j - 1] + DT_C);
+        }
+      }
+      const double u = (g >= FMAX ? 1e300 : (double)g + (double)j);
+      local = fmin(local, u);
+      r0[j] = g;
+    }
+    const double incl = dt_block_min_scan(local, wsum, true);
+    double run = 1e300;
+    {
+      const double right = __shfl_down_sync(0xffffffffu, incl, 1);
+      const int lane = threadIdx.x & 31;
+      if (lane < 31) run = right;
+      else if ((threadIdx.x >> 5) < 31) run = wsum[32 + (threadIdx.x >> 5) + 1];
+    }
+    for (int q = per - 1; q >= 0; --q) {
+      const int j = j0 + q;
+      if (j >= cols) continue;
+      const float g = r0[j];
+      const double u = (g >= FMAX ? 1e300 : (double)g + (double)j);
+      run = fmin(run, u);
+      const double v = run - (double)j;
+      const float out = v >= 1e299 ? FMAX : fminf(g, (float)v);
+      r0[j] = out;
+      const float p = phi[(size_t)i * cols + j];
+      const bool in = p > 0.f;
+      if (inside_pass && in) sdf[(size_t)i * cols + j] = out >= FMAX ? FMAX : out * dx;
+      if (!inside_pass && !in) sdf[(size_t)i * cols + j] = out >= FMAX ? -FMAX : -out * dx;
+    }
+    __syncthreads();
+  }
+}
+
+cudaError_t launch_reinit_sdf(cudaStream_t s, int rows, int cols, const float* phi, float dx,
+                              float* work, float* sdf) {
+  const size_t smem = (size_t)3 * cols * sizeof(float);
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(chamfer_sdf_kernel,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+  }
+  chamfer_sdf_kernel<<<2, DT_NT, smem, s>>>(phi, rows, cols, dx, work, sdf);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_dt(cudaStream_t s, const float* vn, size_t n, float dx, float dy, float cfl,

@@ -63,6 +63,7 @@ struct Cache {
   float2* ESc = nullptr;    // [Pc][Nc]: the same, transposed
   float2* EDr_t = nullptr;  // [2Nr-1][Pr]: e^{+2 pi i d j / Pr}, d = -(Nr-1)..Nr-1
   float2* EDc_t = nullptr;  // [2Nc-1][Pc]: e^{+2 pi i d j / Pc}, d = -(Nc-1)..Nc-1
+  float2* EDc = nullptr;    // [Pc][2Nc-1]: the same, transposed
   int device = 0;
 };
 
@@ -114,34 +115,28 @@ struct Context {
   int ensure_red(size_t n);
 };
 
-// Split of a length-N contraction into chunks of kps (a multiple of 16) for a
-// requested number of splits; zs is the number of chunks actually produced.
-inline void row_split(int N, int ksplit, int* kps, int* zs) {
-  if (ksplit < 1) ksplit = 1;
-  *kps = ((N + ksplit - 1) / ksplit + 15) / 16 * 16;
-  *zs = (N + *kps - 1) / *kps;
-}
-
 // ---------------------------------------------------------------- kernels
 // All launchers return cudaGetLastError() of their launches.
-// Row analysis: out[z][y][2c+{0,1}] = sum_{x in split z} A[y][x] tw[2c+{0,1}][x],
-// A = in (mode 0) or (1 + cos in)/2 (mode 1, optionally stored to mask_out).
-cudaError_t launch_analysis_rows(cudaStream_t s, int mode, const float* in, float* mask_out,
-                                 int* flag, const float* tw, int N, int ncols, int ksplit,
-                                 float* out);
-// Column contraction over y of the row-analysis partials (see band_dft.cu).
-cudaError_t launch_analysis_cols(cudaStream_t s, const float* R, int ksplit, int N, int ncols,
-                                 const float2* TY, int nrows_out, int nr, int sym, int ysplit,
-                                 float scale, float2* out_partial);
-cudaError_t launch_band_forward(cudaStream_t s, const Cache& c, const float2* mpart, int ysplit,
-                                Field& f, float* ik, float2* T, float2* Q, float2* chat,
+// Tile analysis: for every 128 x 128 tile t of the image A (A = in for mode 0,
+// (1 + cos in)/2 for mode 1, optionally stored to mask_out)
+//   part[t][a][c] = sum_{(y, x) in t} T(a, y) A[y][x] tw(c, x)
+// with tw = [2 ncols][N] real rows (Re, Im) and T(a, y) = TY[a][y] (sym 0,
+// a < nrows_out) or, for sym 1, d = a - (nr - 1), TY[d][y] / conj(TY[-d][y]).
+int analysis_tiles(int N);
+cudaError_t launch_analysis(cudaStream_t s, int mode, const float* in, float* mask_out,
+                            int* flag, const float* tw, int N, int ncols, const float2* TY,
+                            int nrows_out, int nr, int sym, float2* part);
+// out[o] = scale * sum_t part[t][o] (fixed order).
+cudaError_t launch_reduce_tiles(cudaStream_t s, const float2* part, int tiles, int count,
+                                float scale, float2* out);
+// Small-grid stage of the forward: f.mband -> f.e, ik, iP and Ut (the row
+// synthesis operand). Shared memory of its per-kernel CTA: band_fields_smem.
+size_t band_fields_smem(const BandGeom& g);
+cudaError_t launch_band_forward(cudaStream_t s, const Cache& c, Field& f, float* ik, float* iP,
                                 float* Ut);
-cudaError_t launch_band_adjoint(cudaStream_t s, const Cache& c, const Field& f,
-                                const float2* gpart, int ysplit, double scale, float2* Gam,
-                                float* gam, float2* Z1, float2* Zk, float2* X, float* Vt);
-cudaError_t launch_expand_cols(cudaStream_t s, const float2* coef, int nrows, int ncoef,
-                               int coef_ld, const float2* TX, int N, int mode, int nc, int kp,
-                               float* Ut);
+// Small-grid stage of the adjoint: gh (the D-band DFT of dL/dI) -> gam, Zk and Vt.
+cudaError_t launch_band_adjoint(cudaStream_t s, const Cache& c, const Field& f, const float2* gh,
+                                double scale, float* gam, float2* Zk, float* Vt);
 
 // Row synthesis: out[y][x] = sum_f AY[y][f] * Bt[x][f] with a fused epilogue.
 struct ResistEpilogue {
@@ -184,5 +179,8 @@ cudaError_t launch_levelset(cudaStream_t s, int what, int rows, int cols, const 
                             const float* dt, float* out, float* out2);
 cudaError_t launch_dt(cudaStream_t s, const float* vn, size_t n, float dx, float dy, float cfl,
                       float b, float* part, float* vmax, float* dt, int* bad);
+// Chamfer signed distance of reinit_sdf; work holds 2 * rows * cols floats.
+cudaError_t launch_reinit_sdf(cudaStream_t s, int rows, int cols, const float* phi, float dx,
+                              float* work, float* sdf);
 
 }  // namespace litho_b200

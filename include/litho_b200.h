@@ -62,11 +62,12 @@ int litho_ctx_set_precision(litho_ctx* ctx, int precision);
 long long litho_ctx_launch_count(const litho_ctx* ctx);
 
 /* Per-stage device timing with CUDA events on the context's stream. Stages:
- * 0 row analysis (mask), 1 column contraction, 2 band forward (small grid),
- * 3 row synthesis + resist/loss epilogue, 4 row analysis (dL/dI),
- * 5 column contraction (adjoint), 6 band adjoint, 7 row synthesis + theta chain,
- * 8 level-set stencil. ms[i] accumulates milliseconds, counts[i] launches of
- * stage i since timing was enabled (enabling resets both). */
+ * 0 tile analysis of the mask (row DFT + column contraction per 128 x 128 tile),
+ * 1 tile reduction, 2 band forward (small grid), 3 row synthesis + resist/loss
+ * epilogue, 4 tile analysis of dL/dI, 5 its tile reduction, 6 band adjoint,
+ * 7 row synthesis + theta chain, 8 level-set kernels (RK2 update, reinit).
+ * ms[i] accumulates milliseconds, counts[i] calls of stage i since timing was
+ * enabled (enabling resets both). */
 #define LITHO_NUM_STAGES 9
 int litho_ctx_enable_stage_timing(litho_ctx* ctx, int on);
 int litho_ctx_stage_times(const litho_ctx* ctx, double* ms, long long* counts);
@@ -181,6 +182,13 @@ int litho_kappa(litho_ctx* ctx, int rows, int cols, const float* d_phi, double d
 int litho_evolution_term(litho_ctx* ctx, int rows, int cols, const float* d_phi,
                          const float* d_vn, double dx, double dy, double cfl, double b,
                          float* d_normal, double* dt);
+/* LevelSetUtils::reinit_sdf (level_set_utils.cpp:290-319): signed distance
+ * dist_in * dx - dist_out * dx with the 5x5 chamfer metric of OpenCV's
+ * distanceTransform(DIST_L2, 5) (weights 1, 1.4, 2.1969), inside = phi > 0.
+ * With no boundary in the tile the magnitude is FLT_MAX (OpenCV's no-feature
+ * value). d_mask (nullable) receives the printed mask sdf >= 0 as 1/0 floats. */
+int litho_reinit_sdf(litho_ctx* ctx, int rows, int cols, const float* d_phi, double dx,
+                     double dy, float* d_sdf, float* d_mask);
 /* One RK2 level-set update (LSM_Optimizer.cpp:109-115, the second stage reuses
  * the first stage's dt) and the printed mask (phi >= 0) (LSM_Optimizer.cpp:128).
  * d_phi_out may alias nothing else; d_mask (nullable) receives 1/0 floats. */

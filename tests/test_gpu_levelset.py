@@ -124,3 +124,69 @@ def test_flat_field_is_zero(L):
     phi = np.full((16, 16), 3.0)
     d = cpu(L.LevelSetUtils.evolve_normal_WENO_godunov(phi, np.ones_like(phi), 1.0, 1.0).delta)
     assert np.all(d == 0.0)
+
+
+@pytest.mark.parametrize("shape", [(7, 9), (64, 64), (65, 200), (517, 300), (2048, 2048)])
+def test_reinit_sdf_matches_opencv(L, shape):
+    """reinit_sdf (level_set_utils.cpp:290-319) against cv2.distanceTransform(DIST_L2, 5).
+
+    OpenCV accumulates the chamfer sums in float32 along its raster order; the
+    device evaluates the same minimum exactly, so values agree to float
+    rounding: 1e-5 relative (plus 1e-6 absolute) per pixel.
+    """
+    rows, cols = shape
+    rng = np.random.default_rng(rows + cols)
+    yy, xx = np.mgrid[0:rows, 0:cols].astype(np.float64)
+    phi = np.sin(0.07 * xx + 0.3) * np.cos(0.05 * yy) + 0.3 * rng.standard_normal((rows, cols))
+    phi[rows // 3, :] = 0.0  # exact zeros count as outside (phi > 0 is inside)
+    ref = lo.reinit_sdf(phi, 2.0, 2.0)
+    got, mask = L.LevelSetUtils.reinit_sdf(phi, 2.0, 2.0, with_mask=True)
+    got = cpu(got)
+    assert np.all(np.abs(got - ref) <= 1e-5 * np.abs(ref) + 1e-6)
+    assert np.array_equal(cpu(mask), (got >= 0).astype(np.float64))
+
+
+def test_reinit_sdf_of_binary_mask(L):
+    """The LSM initialisation reinit_sdf(mask - 0.5) (LSM_Optimizer.cpp:62) on a target."""
+    wl = importlib.import_module("c-version-lithography_b200.workloads")
+    target = wl.manhattan_target(512, 10, seed=4)
+    ref = lo.reinit_sdf(target - 0.5, 2.0, 2.0)
+    got = cpu(L.LevelSetUtils.reinit_sdf(target - 0.5, 2.0, 2.0))
+    assert np.all(np.abs(got - ref) <= 1e-5 * np.abs(ref) + 1e-6)
+
+
+def test_reinit_without_boundary(L):
+    """No feature pixel: OpenCV returns FLT_MAX; the sign follows inside/outside."""
+    got = cpu(L.LevelSetUtils.reinit_sdf(np.full((8, 8), 2.0), 1.0, 1.0))
+    assert np.all(got == np.float32(3.4028235e38))
+    got = cpu(L.LevelSetUtils.reinit_sdf(np.full((8, 8), -2.0), 1.0, 1.0))
+    assert np.all(got == -np.float32(3.4028235e38))
+
+
+def test_lsm_optimizer_tracks_oracle(L):
+    """LSM_Optimizer::optimize (LSM_Optimizer.cpp:60-149) for 6 iterations on real optics,
+    against the FP64 oracle loop: PE history within 1e-3 relative, printed masks
+    equal except pixels whose oracle phi is within 1e-3 of zero."""
+    from oracle import imaging_oracle as io
+    from oracle import optics_oracle as oo
+    n, dx = 64, 4.0
+    oc = oo.prepare(n, dx, 193.0, 1.35, 0.6, 0.9, use_socs=True)
+    target = np.zeros((n, n)); target[23:42, 23:42] = 1.0
+    mask0 = target.copy(); mask0[20:45, 26:38] = 1.0
+    thr, alpha, cfl, b = 0.25, 85.0, 0.5, 0.01
+    # Oracle loop (LSM_Optimizer.cpp:60-128), penalty off.
+    phi = lo.reinit_sdf(mask0 - 0.5, dx, dx)
+    temp = mask0.copy(); hist = []; phis = []
+    for i in range(6):
+        _, w, E = io.imaging_compute(temp, oc, thr, alpha)
+        hist.append(io.pe_loss_with_penalty(w, target, 1.0, 0.01))
+        gm = io.pe_gradient(w, target, E, oc, alpha)
+        phi, _ = lo.lsm_rk2_update(phi, gm, dx, dx, cfl, b)
+        phis.append(phi.copy())
+        temp = (phi >= 0).astype(np.float64)
+    cache = L.ImagingCache.from_kernels(np.stack(oc.kernels), oc.source_ws, oc.eigenvalues)
+    lsm = L.LSMOptimizer(cache, target, thr, alpha, dx, dx, cfl, b, iterations=6)
+    res = lsm.optimize(mask0)
+    for a, r in zip(lsm.error_history, hist):
+        assert abs(a - r) <= 1e-3 * r, (lsm.error_history, hist)
+    assert np.allclose(cpu(res.initial_sdf), lo.reinit_sdf(mask0 - 0.5, dx, dx), rtol=1e-5, atol=1e-5)
