@@ -57,7 +57,7 @@ void free_cache(Cache* c) {
 
 // Scratch layout of one imaging + adjoint evaluation.
 struct Layout {
-  size_t part, gh, ik, iP, Ut, Vt, dldi, gam, Zk, rows_tmp, total;
+  size_t part, gh, ik, iP, chat, X, Ut, Vt, dldi, gam, Zk, rows_tmp, total;
   int tiles;
 };
 
@@ -80,6 +80,8 @@ Layout make_layout(const BandGeom& g) {
   L.dldi = take((size_t)N * N * sizeof(float));
   L.gam = take((size_t)g.Pr * g.Pc * sizeof(float));
   L.Zk = take((size_t)g.K * g.Nr * g.Nc * sizeof(float2));
+  L.chat = take((size_t)g.Nr * (2 * g.Nc - 1) * sizeof(float2));
+  L.X = take((size_t)g.Nr * g.Nc * sizeof(float2));
   L.rows_tmp = take((size_t)g.Nr * N * sizeof(float2));
   L.total = off;
   return L;
@@ -353,7 +355,8 @@ int litho_cache_create_band(litho_ctx* ctx, int N, int K, int Nr, int Nc, int ro
     }
   // The per-kernel CTAs of the small-grid stage keep a band (and a band-by-grid
   // product) in shared memory; larger bands are not built.
-  if (band_fields_smem(g) > 200 * 1024 || (size_t)g.Pr * Nc * sizeof(float2) > 200 * 1024) {
+  if (band_fields_smem(g) > 200 * 1024 || (size_t)g.Pr * Nc * sizeof(float2) > 200 * 1024 ||
+      (size_t)72 * (2 * Nc - 1) * sizeof(float2) > 200 * 1024) {
     delete c;
     return ctx->fail(LITHO_ERR_UNSUPPORTED,
                      "kernel band too large: needs (Nr*Nc + 2*Nr*Nc) * 8 bytes <= 200 KiB");
@@ -528,7 +531,7 @@ int run_forward(Context* ctx, const Cache& c, Field& f, const Layout& L, int inp
   if (st) return st;
   ctx->stage_begin(2);
   st = check_launch(ctx, launch_band_forward(s, c, f, at<float>(ctx, L.ik), at<float>(ctx, L.iP),
-                                             at<float>(ctx, L.Ut)),
+                                             at<float2>(ctx, L.chat), at<float>(ctx, L.Ut)),
                     "band forward");
   ctx->stage_end(2);
   if (st) return st;
@@ -537,7 +540,7 @@ int run_forward(Context* ctx, const Cache& c, Field& f, const Layout& L, int inp
                                              nblocks),
                     "row synthesis");
   ctx->stage_end(3);
-  ctx->launches += 6;
+  ctx->launches += 7;
   f.valid = (st == LITHO_OK);
   return st;
 }
@@ -564,7 +567,7 @@ int run_adjoint(Context* ctx, const Cache& c, const Field& f, const Layout& L, c
   ctx->stage_begin(6);
   st = check_launch(ctx, launch_band_adjoint(s, c, f, at<float2>(ctx, L.gh), scale,
                                              at<float>(ctx, L.gam), at<float2>(ctx, L.Zk),
-                                             at<float>(ctx, L.Vt)),
+                                             at<float2>(ctx, L.X), at<float>(ctx, L.Vt)),
                     "band adjoint");
   ctx->stage_end(6);
   if (st) return st;
@@ -573,7 +576,7 @@ int run_adjoint(Context* ctx, const Cache& c, const Field& f, const Layout& L, c
                                            nblocks),
                     "adjoint row synthesis");
   ctx->stage_end(7);
-  ctx->launches += 6;
+  ctx->launches += 7;
   return st;
 }
 

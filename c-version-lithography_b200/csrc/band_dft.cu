@@ -161,17 +161,19 @@ analysis_tile_kernel(AnalysisArgs a) {
     for (int j = 0; j < TN; ++j) acc[i][j] = 0.f;
   gemm_mainloop<AT_BMT, AT_BNT, AT_TM, TN, AT_BK>(ld, a.tw, a.N, Nn, y0, f0, x0,
                                                   min(a.N, x0 + AT_TILE), As, Bs, acc);
-  // Phase 2: P[r][c] = sum_{y in tile} T(r, y) R[y][c] for the tile's rows.
-  constexpr int RS = BN + 1;
+  // Phase 2: P[r][c] = sum_{y in tile} T(r, y) R[y][c] for the tile's rows, as a
+  // register-tiled complex product: each thread owns 2 band rows x 2 columns.
+  constexpr int RS = BN + 4;                         // keeps float4 alignment of R rows
   float* Rs = smem;                                  // [128][RS]
-  float2* TYs = reinterpret_cast<float2*>(smem + ((AT_TILE * RS + 3) & ~3));  // [RC][128]
+  float2* TYs = reinterpret_cast<float2*>(smem + AT_TILE * RS);  // [RC][128]
 #pragma unroll
   for (int i = 0; i < AT_TM; ++i)
 #pragma unroll
     for (int j = 0; j < TN; ++j) Rs[(ty * AT_TM + i) * RS + tx + j * AT_BNT] = acc[i][j];
-  const int cl = tid % BNC, ag = tid / BNC, AG = AT_NT / BNC;
-  const int cg = f0 / 2 + cl;
-  const bool col_active = ag < AG && cg < a.ncols;
+  constexpr int CP = BNC / 2;                        // column pairs
+  const int cp = tid % CP, rp = tid / CP;            // rows 2rp, 2rp+1 of each chunk
+  const bool active = rp < AT_RC / 2;
+  const int c0g = f0 / 2 + 2 * cp;                   // first of the two global columns
   const int tile = blockIdx.y * gridDim.x + blockIdx.x;
   for (int r0 = 0; r0 < a.nrows_out; r0 += AT_RC) {
     __syncthreads();
@@ -190,20 +192,28 @@ analysis_tile_kernel(AnalysisArgs a) {
       TYs[r * AT_TILE + yy] = t;
     }
     __syncthreads();
-    if (col_active) {
-      for (int r = ag; r < AT_RC; r += AG) {
-        const int row = r0 + r;
-        if (row >= a.nrows_out) break;
-        float2 p0 = make_float2(0.f, 0.f), p1 = p0;
-        const float2* tyr = TYs + r * AT_TILE;
+    if (active && r0 + 2 * rp < a.nrows_out) {
+      float2 p00 = make_float2(0.f, 0.f), p01 = p00, p10 = p00, p11 = p00;
+      const float2* t0 = TYs + (2 * rp) * AT_TILE;
+      const float2* t1 = t0 + AT_TILE;
 #pragma unroll 4
-        for (int yy = 0; yy < AT_TILE; yy += 2) {
-          cfma(p0, tyr[yy], make_float2(Rs[yy * RS + 2 * cl], Rs[yy * RS + 2 * cl + 1]));
-          cfma(p1, tyr[yy + 1],
-               make_float2(Rs[(yy + 1) * RS + 2 * cl], Rs[(yy + 1) * RS + 2 * cl + 1]));
-        }
-        a.part[((size_t)tile * a.nrows_out + row) * a.ncols + cg] =
-            make_float2(p0.x + p1.x, p0.y + p1.y);
+      for (int yy = 0; yy < AT_TILE; ++yy) {
+        const float4 rv = *reinterpret_cast<const float4*>(&Rs[yy * RS + 4 * cp]);
+        const float2 ra = make_float2(rv.x, rv.y), rb = make_float2(rv.z, rv.w);
+        const float2 ta = t0[yy], tb = t1[yy];
+        cfma(p00, ta, ra);
+        cfma(p01, ta, rb);
+        cfma(p10, tb, ra);
+        cfma(p11, tb, rb);
+      }
+      const int row0 = r0 + 2 * rp;
+      float2* out0 = a.part + ((size_t)tile * a.nrows_out + row0) * a.ncols;
+      if (c0g < a.ncols) out0[c0g] = p00;
+      if (c0g + 1 < a.ncols) out0[c0g + 1] = p01;
+      if (row0 + 1 < a.nrows_out) {
+        float2* out1 = out0 + a.ncols;
+        if (c0g < a.ncols) out1[c0g] = p10;
+        if (c0g + 1 < a.ncols) out1[c0g + 1] = p11;
       }
     }
   }
@@ -213,7 +223,7 @@ template <int TN>
 static cudaError_t analysis_tile_t(cudaStream_t s, const AnalysisArgs& a) {
   constexpr int BN = AT_BNT * TN;
   const size_t p1 = (size_t)(AT_BK * (AT_TILE + 4) + AT_BK * (BN + 1)) * sizeof(float);
-  const size_t p2 = (size_t)((AT_TILE * (BN + 1) + 3) & ~3) * sizeof(float) +
+  const size_t p2 = (size_t)AT_TILE * (BN + 4) * sizeof(float) +
                     (size_t)AT_RC * AT_TILE * sizeof(float2);
   const size_t smem = p1 > p2 ? p1 : p2;
   cudaError_t e = cudaFuncSetAttribute(analysis_tile_kernel<TN>,
@@ -482,29 +492,45 @@ cudaError_t launch_synth_grad(cudaStream_t s, const float* AY, const float* Bt, 
 }
 
 // ---------------------------------------------------------------- small-grid band stage
-// Forward 1 (one CTA per kernel k): A = H_k m on the band, T = A ESc^T (Nr x Pc,
-// shared memory), e_k = ESr T (Pr x Pc) and ik = w_k |e_k|^2.
-constexpr int BF_NT = 512;
+// Small tables (a few tens of KB for a 35 x 35 band) are staged in shared
+// memory when they fit in SMEM_STAGE bytes; otherwise the kernels read them
+// from global memory (L2-resident), with the same arithmetic.
+constexpr size_t SMEM_STAGE = 200 * 1024;
+constexpr int BF_NT = 1024;
+
+template <class T>
+__device__ __forceinline__ const T* stage_copy(T* dst, const T* src, int n, bool use) {
+  if (!use) return src;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
+  return dst;
+}
+
+// Forward 1 (one CTA per kernel k): A = H_k m on the band, T = A ESc^T (Nr x Pc),
+// e_k = ESr T (Pr x Pc) and ik = w_k |e_k|^2.
 __global__ void __launch_bounds__(BF_NT)
 band_fields_kernel(const float2* __restrict__ H, const float2* __restrict__ mband,
                    const float* __restrict__ w, int Nr, int Nc, int Pr, int Pc,
                    const float2* __restrict__ ESc_t, const float2* __restrict__ ESr_t,
-                   float2* __restrict__ e, float* __restrict__ ik) {
+                   int stage_tables, float2* __restrict__ e, float* __restrict__ ik) {
   extern __shared__ float2 sm2[];
-  float2* A = sm2;              // [Nr][Nc]
-  float2* T = sm2 + Nr * Nc;    // [Nr][Pc]
+  float2* A = sm2;                  // [Nr][Nc]
+  float2* T = A + Nr * Nc;          // [Nr][Pc]
+  float2* esc = T + Nr * Pc;        // [Nc][Pc] (staged)
+  float2* esr = esc + Nc * Pc;      // [Nr][Pr] (staged)
   const int k = blockIdx.x;
   for (int i = threadIdx.x; i < Nr * Nc; i += BF_NT) A[i] = cmul(H[(size_t)k * Nr * Nc + i], mband[i]);
+  const float2* ESC = stage_copy(esc, ESc_t, Nc * Pc, stage_tables);
+  const float2* ESR = stage_copy(esr, ESr_t, Nr * Pr, stage_tables);
   __syncthreads();
   for (int i = threadIdx.x; i < Nr * Pc; i += BF_NT) {
     const int r = i / Pc, jc = i % Pc;
     float2 a0 = make_float2(0.f, 0.f), a1 = a0;
     int c = 0;
     for (; c + 1 < Nc; c += 2) {
-      cfma(a0, A[r * Nc + c], ESc_t[(size_t)c * Pc + jc]);
-      cfma(a1, A[r * Nc + c + 1], ESc_t[(size_t)(c + 1) * Pc + jc]);
+      cfma(a0, A[r * Nc + c], ESC[c * Pc + jc]);
+      cfma(a1, A[r * Nc + c + 1], ESC[(c + 1) * Pc + jc]);
     }
-    if (c < Nc) cfma(a0, A[r * Nc + c], ESc_t[(size_t)c * Pc + jc]);
+    if (c < Nc) cfma(a0, A[r * Nc + c], ESC[c * Pc + jc]);
     T[i] = make_float2(a0.x + a1.x, a0.y + a1.y);
   }
   __syncthreads();
@@ -514,15 +540,22 @@ band_fields_kernel(const float2* __restrict__ H, const float2* __restrict__ mban
     float2 a0 = make_float2(0.f, 0.f), a1 = a0;
     int r = 0;
     for (; r + 1 < Nr; r += 2) {
-      cfma(a0, ESr_t[(size_t)r * Pr + jr], T[r * Pc + jc]);
-      cfma(a1, ESr_t[(size_t)(r + 1) * Pr + jr], T[(r + 1) * Pc + jc]);
+      cfma(a0, ESR[r * Pr + jr], T[r * Pc + jc]);
+      cfma(a1, ESR[(r + 1) * Pr + jr], T[(r + 1) * Pc + jc]);
     }
-    if (r < Nr) cfma(a0, ESr_t[(size_t)r * Pr + jr], T[r * Pc + jc]);
+    if (r < Nr) cfma(a0, ESR[r * Pr + jr], T[r * Pc + jc]);
     const float2 v = make_float2(a0.x + a1.x, a0.y + a1.y);
     const size_t o = (size_t)k * Pr * Pc + i;
     e[o] = v;
     ik[o] = wk * (v.x * v.x + v.y * v.y);
   }
+}
+
+static size_t fields_smem_full(const BandGeom& g) {
+  return (size_t)(g.Nr * g.Nc + g.Nr * g.Pc + g.Nc * g.Pc + g.Nr * g.Pr) * sizeof(float2);
+}
+size_t band_fields_smem(const BandGeom& g) {
+  return (size_t)(g.Nr * g.Nc + g.Nr * g.Pc) * sizeof(float2);
 }
 
 // Forward 2: i[j] = sum_k ik[k][j] in k order.
@@ -535,73 +568,128 @@ __global__ void sum_k_kernel(const float* __restrict__ ik, int K, int n, float* 
 }
 
 // Forward 3 (one CTA per band row dr >= 0): chat[dr][dc] = DFT_P(i)(dr, dc) / (Pr Pc)
-// over dc in [-(Nc-1), Nc-1], then U[dr][x] = kappa(dr) sum_dc chat[dr][dc] e^{2 pi i dc x/N}
-// written as Ut[x][2 dr + {0,1}] for the row synthesis (kappa = 2 for dr > 0: the
-// Hermitian half of the spectrum of a real image).
+// for dc in [-(Nc-1), Nc-1].
 constexpr int BI_NT = 256;
 __global__ void __launch_bounds__(BI_NT)
-band_image_kernel(const float* __restrict__ iP, int Nr, int Nc, int Pr, int Pc,
-                  const float2* __restrict__ EDr_t, const float2* __restrict__ EDc,
-                  const float2* __restrict__ TXDc, int N, int kp, float inv,
-                  float* __restrict__ Ut) {
+band_chat_kernel(const float* __restrict__ iP, int Nr, int Nc, int Pr, int Pc,
+                 const float2* __restrict__ EDr_t, const float2* __restrict__ EDc, float inv,
+                 float2* __restrict__ chat) {
   extern __shared__ float2 sb[];
   float2* v = sb;             // [Pc]
-  float2* ch = sb + Pc;       // [2Nc - 1]
+  float2* ed = sb + Pc;       // [Pr]
   const int dr = blockIdx.x;
   const int nd = 2 * Nc - 1;
-  const float2* ed = EDr_t + (size_t)(dr + Nr - 1) * Pr;
+  for (int jr = threadIdx.x; jr < Pr; jr += BI_NT) ed[jr] = EDr_t[(size_t)(dr + Nr - 1) * Pr + jr];
+  __syncthreads();
   for (int jc = threadIdx.x; jc < Pc; jc += BI_NT) {
-    float2 a = make_float2(0.f, 0.f);
-    for (int jr = 0; jr < Pr; ++jr) {
-      const float iv = iP[(size_t)jr * Pc + jc];
-      const float2 t = ed[jr];
-      a.x = fmaf(t.x, iv, a.x);
-      a.y = fmaf(-t.y, iv, a.y);
+    float2 a = make_float2(0.f, 0.f), b = a;
+    int jr = 0;
+    for (; jr + 1 < Pr; jr += 2) {
+      const float i0 = iP[(size_t)jr * Pc + jc], i1 = iP[(size_t)(jr + 1) * Pc + jc];
+      a.x = fmaf(ed[jr].x, i0, a.x); a.y = fmaf(-ed[jr].y, i0, a.y);
+      b.x = fmaf(ed[jr + 1].x, i1, b.x); b.y = fmaf(-ed[jr + 1].y, i1, b.y);
     }
-    v[jc] = a;
+    if (jr < Pr) {
+      const float i0 = iP[(size_t)jr * Pc + jc];
+      a.x = fmaf(ed[jr].x, i0, a.x); a.y = fmaf(-ed[jr].y, i0, a.y);
+    }
+    v[jc] = make_float2(a.x + b.x, a.y + b.y);
   }
   __syncthreads();
   for (int dc = threadIdx.x; dc < nd; dc += BI_NT) {
     float2 a = make_float2(0.f, 0.f);
     for (int jc = 0; jc < Pc; ++jc) cfma(a, v[jc], conjf2(EDc[(size_t)jc * nd + dc]));
-    ch[dc] = make_float2(a.x * inv, a.y * inv);
-  }
-  __syncthreads();
-  const float kap = dr > 0 ? 2.f : 1.f;
-  for (int x = threadIdx.x; x < N; x += BI_NT) {
-    float2 a = make_float2(0.f, 0.f);
-    for (int c = 0; c < nd; ++c) {
-      const int d = c - (Nc - 1);
-      const float2 t = d >= 0 ? conjf2(TXDc[(size_t)d * N + x]) : TXDc[(size_t)(-d) * N + x];
-      cfma(a, ch[c], t);
-    }
-    Ut[(size_t)x * kp + 2 * dr] = kap * a.x;
-    Ut[(size_t)x * kp + 2 * dr + 1] = kap * a.y;
-    if (dr == 0)
-      for (int f = 2 * Nr; f < kp; ++f) Ut[(size_t)x * kp + f] = 0.f;
+    chat[(size_t)dr * nd + dc] = make_float2(a.x * inv, a.y * inv);
   }
 }
 
+// Band -> image columns: Ut[x][2a + {0,1}] = kappa(a) sum_c coef[a][c] phase(c, x) for
+// a 64-column x strip and 8 band rows per CTA (coefficients and phases staged).
+// mode 0 (band S): phase = conj(TX[c][x]) (TX = e^{-2 pi i s_c x/N}), kappa = 1.
+// mode 1 (difference set D, c in [0, 2nc-1), d = c - (nc-1)):
+//   phase = d >= 0 ? conj(TX[d][x]) : TX[-d][x], kappa(a) = a > 0 ? 2 : 1 (Hermitian half).
+// Columns 2*nrows .. kp-1 of Ut are zero-filled by the first row block.
+constexpr int EX_X = 64, EX_R = 8, EX_NT = 256;
+__global__ void __launch_bounds__(EX_NT)
+expand_kernel(const float2* __restrict__ coef, int nrows, int ncoef, int ld,
+              const float2* __restrict__ TX, int N, int mode, int nc, int kp,
+              float* __restrict__ Ut) {
+  extern __shared__ float2 se[];
+  float2* cf = se;                    // [EX_R][ncoef]
+  float2* ph = se + EX_R * ncoef;     // [ncoef][EX_X]
+  const int x0 = blockIdx.x * EX_X, a0 = blockIdx.y * EX_R;
+  for (int i = threadIdx.x; i < EX_R * ncoef; i += EX_NT) {
+    const int r = i / ncoef, c = i % ncoef;
+    cf[i] = (a0 + r < nrows) ? coef[(size_t)(a0 + r) * ld + c] : make_float2(0.f, 0.f);
+  }
+  for (int i = threadIdx.x; i < ncoef * EX_X; i += EX_NT) {
+    const int c = i / EX_X, xx = i % EX_X, x = x0 + xx;
+    float2 t = make_float2(0.f, 0.f);
+    if (x < N) {
+      if (mode == 0) {
+        t = conjf2(TX[(size_t)c * N + x]);
+      } else {
+        const int d = c - (nc - 1);
+        t = d >= 0 ? conjf2(TX[(size_t)d * N + x]) : TX[(size_t)(-d) * N + x];
+      }
+    }
+    ph[i] = t;
+  }
+  __syncthreads();
+  const int xx = threadIdx.x % EX_X, rq = threadIdx.x / EX_X;  // rq in [0, 4): rows rq, rq + 4
+  const int x = x0 + xx;
+  float2 acc0 = make_float2(0.f, 0.f), acc1 = acc0;
+  for (int c = 0; c < ncoef; ++c) {
+    const float2 p = ph[c * EX_X + xx];
+    cfma(acc0, cf[rq * ncoef + c], p);
+    cfma(acc1, cf[(rq + 4) * ncoef + c], p);
+  }
+  if (x >= N) return;
+  const int ra = a0 + rq, rb = a0 + rq + 4;
+  if (ra < nrows) {
+    const float k = (mode == 1 && ra > 0) ? 2.f : 1.f;
+    Ut[(size_t)x * kp + 2 * ra] = k * acc0.x;
+    Ut[(size_t)x * kp + 2 * ra + 1] = k * acc0.y;
+  }
+  if (rb < nrows) {
+    const float k = (mode == 1 && rb > 0) ? 2.f : 1.f;
+    Ut[(size_t)x * kp + 2 * rb] = k * acc1.x;
+    Ut[(size_t)x * kp + 2 * rb + 1] = k * acc1.y;
+  }
+  if (blockIdx.y == 0 && rq == 0)
+    for (int f = 2 * nrows; f < kp; ++f) Ut[(size_t)x * kp + f] = 0.f;
+}
+
+static cudaError_t launch_expand(cudaStream_t s, const float2* coef, int nrows, int ncoef, int ld,
+                                 const float2* TX, int N, int mode, int nc, int kp, float* Ut) {
+  const size_t smem = (size_t)(EX_R * ncoef + ncoef * EX_X) * sizeof(float2);
+  cudaError_t e = cudaFuncSetAttribute(expand_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem);
+  if (e != cudaSuccess) return e;
+  dim3 grid((N + EX_X - 1) / EX_X, (nrows + EX_R - 1) / EX_R);
+  expand_kernel<<<grid, EX_NT, smem, s>>>(coef, nrows, ncoef, ld, TX, N, mode, nc, kp, Ut);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_band_forward(cudaStream_t s, const Cache& c, Field& f, float* ik, float* iP,
-                                float* Ut) {
+                                float2* chat, float* Ut) {
   const BandGeom& g = c.g;
-  const size_t sm1 = (size_t)(g.Nr * g.Nc + g.Nr * g.Pc) * sizeof(float2);
+  const size_t full = fields_smem_full(g);
+  const int stage = full <= SMEM_STAGE;
+  const size_t sm1 = stage ? full : band_fields_smem(g);
   cudaError_t err = cudaFuncSetAttribute(band_fields_kernel,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1);
   if (err != cudaSuccess) return err;
   band_fields_kernel<<<g.K, BF_NT, sm1, s>>>(c.H, f.mband, c.w, g.Nr, g.Nc, g.Pr, g.Pc, c.ESc_t,
-                                             c.ESr_t, f.e, ik);
+                                             c.ESr_t, stage, f.e, ik);
   const int n = g.Pr * g.Pc;
   sum_k_kernel<<<(n + 255) / 256, 256, 0, s>>>(ik, g.K, n, iP);
-  const size_t sm3 = (size_t)(g.Pc + 2 * g.Nc - 1) * sizeof(float2);
-  band_image_kernel<<<g.Nr, BI_NT, sm3, s>>>(iP, g.Nr, g.Nc, g.Pr, g.Pc, c.EDr_t, c.EDc, c.TXDc,
-                                             g.N, g.kp_rows, 1.f / ((float)g.Pr * (float)g.Pc),
-                                             Ut);
-  return cudaGetLastError();
-}
-
-size_t band_fields_smem(const BandGeom& g) {
-  return (size_t)(g.Nr * g.Nc + g.Nr * g.Pc) * sizeof(float2);
+  const int nd = 2 * g.Nc - 1;
+  band_chat_kernel<<<g.Nr, BI_NT, (size_t)(g.Pc + g.Pr) * sizeof(float2), s>>>(
+      iP, g.Nr, g.Nc, g.Pr, g.Pc, c.EDr_t, c.EDc, 1.f / ((float)g.Pr * (float)g.Pc), chat);
+  err = cudaGetLastError();
+  if (err != cudaSuccess) return err;
+  return launch_expand(s, chat, g.Nr, nd, nd, c.TXDc, g.N, 1, g.Nc, g.kp_rows, Ut);
 }
 
 // Adjoint 1 (one CTA per small-grid row jr):
@@ -631,33 +719,45 @@ band_gamma_kernel(const float2* __restrict__ gh, int Nr, int Nc, int Pr, int Pc,
   }
 }
 
-// Adjoint 2 (one CTA per kernel k): Z1[jr][uc] = sum_jc e_k[jr][jc] gamma[jr][jc] conj(ESc[jc][uc])
-// (shared memory), Zk[ur][uc] = sum_jr conj(ESr_t[ur][jr]) Z1[jr][uc] / (Pr Pc).
+// Adjoint 2 (one CTA per kernel k): q = e_k gamma (Pr x Pc), Z1 = q conj(ESc) (Pr x Nc),
+// Zk = conj(ESr_t) Z1 / (Pr Pc) (Nr x Nc).
 __global__ void __launch_bounds__(BF_NT)
 band_z_kernel(const float2* __restrict__ e, const float* __restrict__ gam, int Nr, int Nc, int Pr,
-              int Pc, const float2* __restrict__ ESc, const float2* __restrict__ ESr_t, float inv,
-              float2* __restrict__ Zk) {
-  extern __shared__ float2 sz[];  // [Pr][Nc]
+              int Pc, const float2* __restrict__ ESc, const float2* __restrict__ ESr_t,
+              int stage_tables, float inv, float2* __restrict__ Zk) {
+  extern __shared__ float2 sz[];
+  float2* Z1 = sz;                  // [Pr][Nc]
+  float2* q = Z1 + Pr * Nc;         // [Pr][Pc]   (staged)
+  float2* esc = q + Pr * Pc;        // [Pc][Nc]   (staged)
+  float2* esr = esc + Pc * Nc;      // [Nr][Pr]   (staged)
   const int k = blockIdx.x;
   const float2* ek = e + (size_t)k * Pr * Pc;
+  const float2* ESC = stage_copy(esc, ESc, Pc * Nc, stage_tables);
+  const float2* ESR = stage_copy(esr, ESr_t, Nr * Pr, stage_tables);
+  if (stage_tables) {
+    for (int i = threadIdx.x; i < Pr * Pc; i += BF_NT) {
+      const float2 v = ek[i];
+      const float gv = gam[i];
+      q[i] = make_float2(v.x * gv, v.y * gv);
+    }
+  }
+  __syncthreads();
   for (int i = threadIdx.x; i < Pr * Nc; i += BF_NT) {
     const int jr = i / Nc, uc = i % Nc;
     float2 a0 = make_float2(0.f, 0.f), a1 = a0;
-    int jc = 0;
-    for (; jc + 1 < Pc; jc += 2) {
-      const float2 v0 = ek[(size_t)jr * Pc + jc];
-      const float g0 = gam[(size_t)jr * Pc + jc];
-      const float2 v1 = ek[(size_t)jr * Pc + jc + 1];
-      const float g1 = gam[(size_t)jr * Pc + jc + 1];
-      cfma(a0, make_float2(v0.x * g0, v0.y * g0), conjf2(ESc[(size_t)jc * Nc + uc]));
-      cfma(a1, make_float2(v1.x * g1, v1.y * g1), conjf2(ESc[(size_t)(jc + 1) * Nc + uc]));
+    for (int jc = 0; jc < Pc; ++jc) {
+      float2 v;
+      if (stage_tables) {
+        v = q[jr * Pc + jc];
+      } else {
+        const float2 t = ek[(size_t)jr * Pc + jc];
+        const float gv = gam[(size_t)jr * Pc + jc];
+        v = make_float2(t.x * gv, t.y * gv);
+      }
+      if (jc & 1) cfma(a1, v, conjf2(ESC[jc * Nc + uc]));
+      else cfma(a0, v, conjf2(ESC[jc * Nc + uc]));
     }
-    if (jc < Pc) {
-      const float2 v0 = ek[(size_t)jr * Pc + jc];
-      const float g0 = gam[(size_t)jr * Pc + jc];
-      cfma(a0, make_float2(v0.x * g0, v0.y * g0), conjf2(ESc[(size_t)jc * Nc + uc]));
-    }
-    sz[i] = make_float2(a0.x + a1.x, a0.y + a1.y);
+    Z1[i] = make_float2(a0.x + a1.x, a0.y + a1.y);
   }
   __syncthreads();
   for (int i = threadIdx.x; i < Nr * Nc; i += BF_NT) {
@@ -665,58 +765,48 @@ band_z_kernel(const float2* __restrict__ e, const float* __restrict__ gam, int N
     float2 a0 = make_float2(0.f, 0.f), a1 = a0;
     int jr = 0;
     for (; jr + 1 < Pr; jr += 2) {
-      cfma(a0, conjf2(ESr_t[(size_t)ur * Pr + jr]), sz[jr * Nc + uc]);
-      cfma(a1, conjf2(ESr_t[(size_t)ur * Pr + jr + 1]), sz[(jr + 1) * Nc + uc]);
+      cfma(a0, conjf2(ESR[ur * Pr + jr]), Z1[jr * Nc + uc]);
+      cfma(a1, conjf2(ESR[ur * Pr + jr + 1]), Z1[(jr + 1) * Nc + uc]);
     }
-    if (jr < Pr) cfma(a0, conjf2(ESr_t[(size_t)ur * Pr + jr]), sz[jr * Nc + uc]);
+    if (jr < Pr) cfma(a0, conjf2(ESR[ur * Pr + jr]), Z1[jr * Nc + uc]);
     Zk[(size_t)k * Nr * Nc + i] = make_float2((a0.x + a1.x) * inv, (a0.y + a1.y) * inv);
   }
 }
 
-// Adjoint 3 (one CTA per band row ur): X[ur][uc] = scale sum_k w_k conj(H_k) Z_k (k order),
-// V[ur][x] = sum_uc X[ur][uc] e^{2 pi i s_uc x/N}, written as Vt[x][2 ur + {0,1}].
-__global__ void __launch_bounds__(256)
-band_x_kernel(const float2* __restrict__ Zk, const float2* __restrict__ H,
-              const float* __restrict__ w, int K, int Nr, int Nc, float scale,
-              const float2* __restrict__ TXSc, int N, int kp, float* __restrict__ Vt) {
-  extern __shared__ float2 sx[];  // [Nc]
-  const int ur = blockIdx.x;
-  const int nb = Nr * Nc;
-  for (int uc = threadIdx.x; uc < Nc; uc += blockDim.x) {
-    const int u = ur * Nc + uc;
-    float2 acc = make_float2(0.f, 0.f);
-    for (int k = 0; k < K; ++k) {
-      const float2 t = cmul(conjf2(H[(size_t)k * nb + u]), Zk[(size_t)k * nb + u]);
-      acc.x = fmaf(w[k], t.x, acc.x);
-      acc.y = fmaf(w[k], t.y, acc.y);
-    }
-    sx[uc] = make_float2(acc.x * scale, acc.y * scale);
+// Adjoint 3: X[u] = scale sum_k w_k conj(H_k(u)) Z_k(u) (k order), one thread per u.
+__global__ void band_x_kernel(const float2* __restrict__ Zk, const float2* __restrict__ H,
+                              const float* __restrict__ w, int K, int nb, float scale,
+                              float2* __restrict__ X) {
+  const int u = blockIdx.x * blockDim.x + threadIdx.x;
+  if (u >= nb) return;
+  float2 acc = make_float2(0.f, 0.f);
+  for (int k = 0; k < K; ++k) {
+    const float2 t = cmul(conjf2(H[(size_t)k * nb + u]), Zk[(size_t)k * nb + u]);
+    acc.x = fmaf(w[k], t.x, acc.x);
+    acc.y = fmaf(w[k], t.y, acc.y);
   }
-  __syncthreads();
-  for (int x = threadIdx.x; x < N; x += blockDim.x) {
-    float2 a = make_float2(0.f, 0.f);
-    for (int uc = 0; uc < Nc; ++uc) cfma(a, sx[uc], conjf2(TXSc[(size_t)uc * N + x]));
-    Vt[(size_t)x * kp + 2 * ur] = a.x;
-    Vt[(size_t)x * kp + 2 * ur + 1] = a.y;
-    if (ur == 0)
-      for (int f = 2 * Nr; f < kp; ++f) Vt[(size_t)x * kp + f] = 0.f;
-  }
+  X[u] = make_float2(acc.x * scale, acc.y * scale);
 }
 
 cudaError_t launch_band_adjoint(cudaStream_t s, const Cache& c, const Field& f, const float2* gh,
-                                double scale, float* gam, float2* Zk, float* Vt) {
+                                double scale, float* gam, float2* Zk, float2* X, float* Vt) {
   const BandGeom& g = c.g;
   band_gamma_kernel<<<g.Pr, 256, g.Nc * sizeof(float2), s>>>(gh, g.Nr, g.Nc, g.Pr, g.Pc, c.EDr_t,
                                                              c.EDc_t, gam);
-  const size_t smz = (size_t)g.Pr * g.Nc * sizeof(float2);
+  const size_t base = (size_t)g.Pr * g.Nc * sizeof(float2);
+  const size_t full = base + (size_t)(g.Pr * g.Pc + g.Pc * g.Nc + g.Nr * g.Pr) * sizeof(float2);
+  const int stage = full <= SMEM_STAGE;
+  const size_t smz = stage ? full : base;
   cudaError_t err = cudaFuncSetAttribute(band_z_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smz);
   if (err != cudaSuccess) return err;
-  band_z_kernel<<<g.K, BF_NT, smz, s>>>(f.e, gam, g.Nr, g.Nc, g.Pr, g.Pc, c.ESc, c.ESr_t,
+  band_z_kernel<<<g.K, BF_NT, smz, s>>>(f.e, gam, g.Nr, g.Nc, g.Pr, g.Pc, c.ESc, c.ESr_t, stage,
                                         1.f / ((float)g.Pr * (float)g.Pc), Zk);
-  band_x_kernel<<<g.Nr, 256, g.Nc * sizeof(float2), s>>>(Zk, c.H, c.w, g.K, g.Nr, g.Nc,
-                                                         (float)scale, c.TXSc, g.N, g.kp_rows, Vt);
-  return cudaGetLastError();
+  const int nb = g.Nr * g.Nc;
+  band_x_kernel<<<(nb + 127) / 128, 128, 0, s>>>(Zk, c.H, c.w, g.K, nb, (float)scale, X);
+  err = cudaGetLastError();
+  if (err != cudaSuccess) return err;
+  return launch_expand(s, X, g.Nr, g.Nc, g.Nc, c.TXSc, g.N, 0, g.Nc, g.kp_rows, Vt);
 }
 
 // ---------------------------------------------------------------- FP64 partial sums

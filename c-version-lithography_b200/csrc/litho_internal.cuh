@@ -133,10 +133,10 @@ cudaError_t launch_reduce_tiles(cudaStream_t s, const float2* part, int tiles, i
 // synthesis operand). Shared memory of its per-kernel CTA: band_fields_smem.
 size_t band_fields_smem(const BandGeom& g);
 cudaError_t launch_band_forward(cudaStream_t s, const Cache& c, Field& f, float* ik, float* iP,
-                                float* Ut);
-// Small-grid stage of the adjoint: gh (the D-band DFT of dL/dI) -> gam, Zk and Vt.
+                                float2* chat, float* Ut);
+// Small-grid stage of the adjoint: gh (the D-band DFT of dL/dI) -> gam, Zk, X and Vt.
 cudaError_t launch_band_adjoint(cudaStream_t s, const Cache& c, const Field& f, const float2* gh,
-                                double scale, float* gam, float2* Zk, float* Vt);
+                                double scale, float* gam, float2* Zk, float2* X, float* Vt);
 
 // Row synthesis: out[y][x] = sum_f AY[y][f] * Bt[x][f] with a fused epilogue.
 struct ResistEpilogue {
