@@ -45,6 +45,8 @@ def parse():
     p.add_argument("--kernels", type=int, default=24)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=12.0)
+    p.add_argument("--precision", default="auto", choices=["auto", "fp32", "bf16x3"],
+                   help="auto: time both, report the split-BF16 tensor-core path")
     return p.parse_args()
 
 
@@ -205,7 +207,46 @@ def config_dict(N, K, precision):
             "l2": "flushed between timed steps (256 MiB write)", "parallelism": "tile-sharded"}
 
 
+def _measure(L, torch, ctx, stream, cache, target, th, flush, steps, warmup, dist):
+    """Times `steps` device-resident CTM evaluations (L2 flushed before each)."""
+    with torch.cuda.stream(stream):
+        opt = L.CTMOptimizer(cache, target, THRESHOLD, ALPHA, iterations=1)
+    t_warm = time.perf_counter()
+    nwarm = 0
+    while nwarm < max(3, warmup) or time.perf_counter() - t_warm < 0.5:
+        opt.evaluate(th)
+        nwarm += 1
+    ctx.enable_stage_timing(True)
+    launches0 = ctx.launch_count
+    times = []
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    for _ in range(steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        opt.evaluate(th)
+        e1.record(stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+    torch.cuda.synchronize()
+    launches = ctx.launch_count - launches0
+    stages = ctx.stage_times()
+    ctx.enable_stage_timing(False)
+    total_ms = sum(times)
+    if dist:
+        t = torch.tensor([total_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+        dist.barrier()
+    return dict(opt=opt, times=times, total_ms=total_ms, stages=stages, launches=launches)
+
+
 def run_ours(args):
+    import ctypes
     import torch
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -221,55 +262,31 @@ def run_ours(args):
     N, K = args.size, args.kernels
     band, r0, c0, w, wss, target, theta = workload(N, K, seed=1 + rank)
     stream = torch.cuda.Stream()
-    ctx = L.Context(local, stream=stream)
-    cache = L.ImagingCache.from_band(N, band, r0, c0, w, wss, ctx=ctx)
     with torch.cuda.stream(stream):
-        opt = L.CTMOptimizer(cache, target, THRESHOLD, ALPHA, iterations=1)
         th = torch.tensor(theta, dtype=torch.float32, device="cuda")
         flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
     torch.cuda.synchronize()
+    modes = ["fp32", "bf16x3"] if args.precision == "auto" else [args.precision]
     clk = ClockSampler(local).__enter__()
     time.sleep(0.3)  # let the sampler start before the GPU work
-    t_warm = time.perf_counter()
-    nwarm = 0
-    while nwarm < max(3, args.warmup) or time.perf_counter() - t_warm < 0.5:
-        opt.evaluate(th)
-        nwarm += 1
-    ctx.enable_stage_timing(True)
-    launches0 = ctx.launch_count
-    times = []
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    if True:
-        for _ in range(args.steps):
-            with torch.cuda.stream(stream):
-                flush.zero_()
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            loss, _, _ = opt.evaluate(th)
-            e1.record(stream)
-            e1.synchronize()
-            times.append(e0.elapsed_time(e1))
-    torch.cuda.synchronize()
+    runs = {}
+    for mode in modes:
+        ctx = L.Context(local, stream=stream)
+        ctx.set_precision(mode)
+        cache = L.ImagingCache.from_band(N, band, r0, c0, w, wss, ctx=ctx)
+        r = _measure(L, torch, ctx, stream, cache, target, th, flush, args.steps, args.warmup, dist)
+        r.update(ctx=ctx, cache=cache)
+        runs[mode] = r
     clk.__exit__(None, None, None)
-    launches = ctx.launch_count - launches0
-    stages = ctx.stage_times()
-    ctx.enable_stage_timing(False)
-    total_ms = sum(times)
-    if dist:
-        t = torch.tensor([total_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-        dist.barrier()
-    value = world * args.steps / (total_ms / 1e3)
+    head = modes[-1]          # the tensor-core path when both ran
+    R = runs[head]
+    ctx, cache, opt = R["ctx"], R["cache"], R["opt"]
+    value = world * args.steps / (R["total_ms"] / 1e3)
 
     # End to end through the host-buffer entry point (H2D + compute + D2H per step).
     h_theta = torch.tensor(theta, dtype=torch.float32).pin_memory()
     h_target = torch.tensor(target, dtype=torch.float32).pin_memory()
     h_grad = torch.empty((N, N), dtype=torch.float32).pin_memory()
-    import ctypes
     lossd, normd = ctypes.c_double(), ctypes.c_double()
 
     def host_call():
@@ -304,28 +321,36 @@ def run_ours(args):
         if dist:
             dist.destroy_process_group()
         return
-    # Roofline of the dominant stage (HBM-bound DFT passes), live CUDA-event timing.
+    # Roofline of the dominant full-resolution stage, live CUDA-event timing.
     hbm, src = peaks()
+    stages = R["stages"]
     sb = stage_bytes(N, cache.Nr, cache.Nc)
     dom = max(sb, key=lambda s: stages[s][0] / max(stages[s][1], 1))
     avg_ms = stages[dom][0] / max(stages[dom][1], 1)
     achieved = sb[dom] / (avg_ms / 1e3) / 1e9
-    traffic = _ncu_traffic(dom, N)
+    traffic = _ncu_traffic(dom, N, head)
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": max(3, args.warmup), "ms_per_step": total_ms / args.steps,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic", "config": config_dict(N, K, "fp32"),
+        "warmup": max(3, args.warmup), "ms_per_step": R["total_ms"] / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "bf16x3" if head == "bf16x3" else "f32",
+        "data": "synthetic", "config": config_dict(N, K, head),
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm,
                      "peak_source": src, "unit": "GB/s", "frac": achieved / hbm,
                      "traffic": traffic, "algorithmic_bytes": sb[dom], "avg_launch_ms": avg_ms},
         "stages_ms_per_step": {k: v[0] / max(v[1], 1) for k, v in stages.items() if v[1]},
-        "latency_ms": {"p50": float(np.percentile(times, 50)), "p99": float(np.percentile(times, 99))},
+        "latency_ms": {"p50": float(np.percentile(R["times"], 50)),
+                       "p99": float(np.percentile(R["times"], 99))},
+        "precision_modes": {m: {"value": world * args.steps / (runs[m]["total_ms"] / 1e3),
+                                "ms_per_step": runs[m]["total_ms"] / args.steps}
+                            for m in runs},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * 4 * N * N,
                 "d2h_bytes_per_step": 4 * N * N + 8 * 3},
-        "gpu_launches": launches,
+        "gpu_launches": R["launches"],
         "clocks": clk.summary(),
     }
+    if "fp32" in runs and "bf16x3" in runs:
+        out["precision_modes"]["bf16x3_over_fp32"] = runs["fp32"]["total_ms"] / runs["bf16x3"]["total_ms"]
     if world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(N, K, band, r0, c0, w, wss, target, theta,
                                            args.cpu_seconds)
@@ -334,12 +359,12 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
-def _ncu_traffic(stage, N):
+def _ncu_traffic(stage, N, precision):
     """DRAM bytes per launch from the committed ncu summary, when one exists."""
     try:
         with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
             t = json.load(f)
-        v = t.get(f"{stage}@{N}")
+        v = t.get(f"{stage}@{N}@{precision}")
         return None if v is None else float(v)
     except Exception:
         return None

@@ -173,6 +173,13 @@ class Context:
     def synchronize(self):
         self._check(self.lib.litho_ctx_synchronize(self.handle))
 
+    PRECISIONS = {"fp32": 0, "bf16x3": 1}
+
+    def set_precision(self, mode: str):
+        """'fp32' (SIMT FP32 DFT passes) or 'bf16x3' (row syntheses on tcgen05 in split-BF16)."""
+        self._check(self.lib.litho_ctx_set_precision(self.handle, self.PRECISIONS[mode]))
+        self.precision = mode
+
     @property
     def launch_count(self) -> int:
         return int(self.lib.litho_ctx_launch_count(self.handle))

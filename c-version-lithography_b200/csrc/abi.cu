@@ -50,14 +50,14 @@ int upload(Context* ctx, T** dst, const std::vector<T>& src) {
 void free_cache(Cache* c) {
   void* ptrs[] = {c->H,    c->w,    c->TXS,  c->TXD,   c->TYS,   c->TYD,   c->AYS,
                   c->AYD,  c->TXSc, c->TXDc, c->ESr_t, c->ESc_t, c->ESc,   c->EDr_t,
-                  c->EDc_t, c->EDc};
+                  c->EDc_t, c->EDc,  c->AYS_img, c->AYD_img};
   for (void* p : ptrs)
     if (p) cudaFree(p);
 }
 
 // Scratch layout of one imaging + adjoint evaluation.
 struct Layout {
-  size_t part, gh, ik, iP, chat, X, Ut, Vt, dldi, gam, Zk, rows_tmp, total;
+  size_t part, gh, ik, iP, chat, X, Ut, Vt, dldi, gam, Zk, rows_tmp, img, total;
   int tiles;
 };
 
@@ -83,6 +83,7 @@ Layout make_layout(const BandGeom& g) {
   L.chat = take((size_t)g.Nr * (2 * g.Nc - 1) * sizeof(float2));
   L.X = take((size_t)g.Nr * g.Nc * sizeof(float2));
   L.rows_tmp = take((size_t)g.Nr * N * sizeof(float2));
+  L.img = take(tc_image_bytes(N, g.kp_rows, 256));  // band operand image (tensor-core path)
   L.total = off;
   return L;
 }
@@ -227,7 +228,7 @@ int litho_ctx_synchronize(litho_ctx* ctx) {
 
 int litho_ctx_set_precision(litho_ctx* ctx, int precision) {
   if (!ctx) return LITHO_ERR_INVALID_ARGUMENT;
-  if (precision != LITHO_PRECISION_FP32)
+  if (precision != LITHO_PRECISION_FP32 && precision != LITHO_PRECISION_BF16X3)
     return ctx->fail(LITHO_ERR_UNSUPPORTED, "precision mode not built");
   ctx->precision = precision;
   return LITHO_OK;
@@ -378,6 +379,18 @@ int litho_cache_create_band(litho_ctx* ctx, int N, int K, int Nr, int Nc, int ro
   if (st == LITHO_OK) st = upload(ctx, &c->EDr_t, EDr_t);
   if (st == LITHO_OK) st = upload(ctx, &c->EDc_t, EDc_t);
   if (st == LITHO_OK) st = upload(ctx, &c->EDc, EDc);
+  // Split-BF16 images of the two row-synthesis twiddle tables for the tensor cores.
+  for (int t = 0; t < 2 && st == LITHO_OK; ++t) {
+    void** img = t == 0 ? &c->AYS_img : &c->AYD_img;
+    const float* src = t == 0 ? c->AYS : c->AYD;
+    if (cudaMalloc(img, tc_image_bytes(N, g.kp_rows, 128)) != cudaSuccess) {
+      cudaGetLastError();
+      st = ctx->fail(LITHO_ERR_OOM, "tensor-core operand image allocation failed");
+    } else if (launch_pack_split(ctx->stream, src, N, g.kp_rows, 128, 0, *img) != cudaSuccess ||
+               cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
+      st = ctx->fail(LITHO_ERR_CUDA, "tensor-core operand packing failed");
+    }
+  }
   if (st != LITHO_OK) {
     free_cache(c);
     delete c;
@@ -536,9 +549,21 @@ int run_forward(Context* ctx, const Cache& c, Field& f, const Layout& L, int inp
   ctx->stage_end(2);
   if (st) return st;
   ctx->stage_begin(3);
-  st = check_launch(ctx, launch_synth_resist(s, c.AYD, at<float>(ctx, L.Ut), g.N, g.kp_rows, ep,
-                                             nblocks),
-                    "row synthesis");
+  if (ctx->precision == LITHO_PRECISION_BF16X3) {
+    int* err = reinterpret_cast<int*>(ctx->d_red + RED_FLAG) + 1;
+    st = check_launch(ctx, launch_pack_split(s, at<float>(ctx, L.Ut), g.N, g.kp_rows, 256, 1,
+                                             at<void>(ctx, L.img)),
+                      "band operand packing");
+    if (!st)
+      st = check_launch(ctx, launch_synth_resist_tc(s, c.AYD_img, at<void>(ctx, L.img), g.N,
+                                                    g.kp_rows, ep, err, nblocks),
+                        "tensor-core row synthesis");
+    ctx->launches += 1;
+  } else {
+    st = check_launch(ctx, launch_synth_resist(s, c.AYD, at<float>(ctx, L.Ut), g.N, g.kp_rows, ep,
+                                               nblocks),
+                      "row synthesis");
+  }
   ctx->stage_end(3);
   ctx->launches += 7;
   f.valid = (st == LITHO_OK);
@@ -572,9 +597,21 @@ int run_adjoint(Context* ctx, const Cache& c, const Field& f, const Layout& L, c
   ctx->stage_end(6);
   if (st) return st;
   ctx->stage_begin(7);
-  st = check_launch(ctx, launch_synth_grad(s, c.AYS, at<float>(ctx, L.Vt), g.N, g.kp_rows, ep,
-                                           nblocks),
-                    "adjoint row synthesis");
+  if (ctx->precision == LITHO_PRECISION_BF16X3) {
+    int* err = reinterpret_cast<int*>(ctx->d_red + RED_FLAG) + 1;
+    st = check_launch(ctx, launch_pack_split(s, at<float>(ctx, L.Vt), g.N, g.kp_rows, 256, 1,
+                                             at<void>(ctx, L.img)),
+                      "band operand packing");
+    if (!st)
+      st = check_launch(ctx, launch_synth_grad_tc(s, c.AYS_img, at<void>(ctx, L.img), g.N,
+                                                  g.kp_rows, ep, err, nblocks),
+                        "tensor-core adjoint row synthesis");
+    ctx->launches += 1;
+  } else {
+    st = check_launch(ctx, launch_synth_grad(s, c.AYS, at<float>(ctx, L.Vt), g.N, g.kp_rows, ep,
+                                             nblocks),
+                      "adjoint row synthesis");
+  }
   ctx->stage_end(7);
   ctx->launches += 7;
   return st;
@@ -598,6 +635,12 @@ int fetch(Context* ctx, int n) {
                                       cudaMemcpyDeviceToHost, ctx->stream));
   LITHO_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
   ctx->collect_stages();
+  int tc_err;
+  std::memcpy(&tc_err, reinterpret_cast<const char*>(ctx->h_red + RED_FLAG) + sizeof(int),
+              sizeof(int));
+  if (tc_err)
+    return ctx->fail(LITHO_ERR_CUDA, "tensor-core synthesis: a bounded wait expired (code " +
+                                         std::to_string(tc_err) + ")");
   return LITHO_OK;
 }
 

@@ -64,6 +64,9 @@ struct Cache {
   float2* EDr_t = nullptr;  // [2Nr-1][Pr]: e^{+2 pi i d j / Pr}, d = -(Nr-1)..Nr-1
   float2* EDc_t = nullptr;  // [2Nc-1][Pc]: e^{+2 pi i d j / Pc}, d = -(Nc-1)..Nc-1
   float2* EDc = nullptr;    // [Pc][2Nc-1]: the same, transposed
+  // Split-BF16 tensor-core operand images of AYS / AYD (see synth_tc.cu).
+  void* AYS_img = nullptr;
+  void* AYD_img = nullptr;
   int device = 0;
 };
 
@@ -171,6 +174,17 @@ cudaError_t launch_pe_loss(cudaStream_t s, const float* w, const float* t, const
 cudaError_t launch_pe_dldi(cudaStream_t s, const float* w, const float* t, const float* pe_win,
                            const float* pen_win, float pe_weight, float penalty, float pen_thr,
                            size_t n, float* dldi, double* partial, int* nblocks);
+
+// Tensor-core row synthesis (synth_tc.cu). Images: split-BF16 K-major SW128
+// tiles of an FP32 [rows][kp] matrix (tile_rows 128 for the twiddle operand,
+// 256 for the band operand; order 0 = [hi, hi, lo], 1 = [hi, lo, hi]).
+size_t tc_image_bytes(int rows, int kp, int tile_rows);
+cudaError_t launch_pack_split(cudaStream_t s, const float* src, int rows, int kp, int tile_rows,
+                              int order, void* dst);
+cudaError_t launch_synth_resist_tc(cudaStream_t s, const void* Aimg, const void* Bimg, int N,
+                                   int kp, const ResistEpilogue& ep, int* err, int* nblocks);
+cudaError_t launch_synth_grad_tc(cudaStream_t s, const void* Aimg, const void* Bimg, int N, int kp,
+                                 const GradEpilogue& ep, int* err, int* nblocks);
 
 // Level set (levelset.cu). what: 0 delta (+|Vn|), 1 kappa term, 2 normal,
 // 3 RK2 stage 1, 4 RK2 stage 2 (+ mask).

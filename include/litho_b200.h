@@ -42,6 +42,8 @@ extern "C" {
 #define LITHO_ERR_UNSUPPORTED 7      /* size or option outside what is built */
 
 #define LITHO_PRECISION_FP32 0       /* plain FP32 DFT passes (SIMT) */
+#define LITHO_PRECISION_BF16X3 1     /* row syntheses on tcgen05 tensor cores in split-BF16
+                                        (hi*hi + hi*lo + lo*hi, FP32 accumulation) */
 
 typedef struct litho_ctx litho_ctx;
 typedef struct litho_cache litho_cache;

@@ -1,0 +1,102 @@
+"""Split-BF16 tensor-core (tcgen05) row syntheses against the FP64 oracle.
+
+Tolerances for the split-BF16 path: aerial image max|dI| <= 1e-4 of peak (the
+north star allows 1e-3 for split-BF16), gradients relative L2 <= 1e-3, PE
+relative 1e-4. Results must also agree with the FP32 path of the same library.
+"""
+import importlib
+
+import numpy as np
+import pytest
+
+from oracle import imaging_oracle as io
+from oracle import optics_oracle as oo
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def L():
+    p = importlib.import_module("c-version-lithography_b200")
+    assert torch.cuda.is_available()
+    p.load_library()
+    return p
+
+
+@pytest.fixture(scope="module")
+def wl():
+    return importlib.import_module("c-version-lithography_b200.workloads")
+
+
+def cpu(t):
+    return t.detach().cpu().numpy().astype(np.float64)
+
+
+def rel_l2(a, b):
+    return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / np.linalg.norm(b))
+
+
+def peak_err(a, b):
+    return float(np.max(np.abs(np.asarray(a) - np.asarray(b))) / np.max(np.abs(b)))
+
+
+@pytest.fixture()
+def tc_ctx(L):
+    ctx = L.Context()
+    ctx.set_precision("bf16x3")
+    yield ctx
+    ctx.close()
+
+
+@pytest.mark.parametrize("N", [128, 300, 2048])
+def test_bf16x3_ctm_matches_oracle(L, wl, tc_ctx, N):
+    band, r0, c0, w, wss = wl.synthetic_socs_band()
+    target = wl.manhattan_target(N, max(4, N // 20), seed=N)
+    theta = wl.theta_init_reference(target)
+    oc = io.OracleCache(N=N, kernels=list(wl.band_to_dense(band, r0, c0, N)),
+                        source_ws=np.array([wss]), eigenvalues=tuple(w))
+    ref = io.ctm_evaluate(theta, target, oc, 0.225, 50.0)
+    cache = L.ImagingCache.from_band(N, band, r0, c0, w, wss, ctx=tc_ctx)
+    imaging = L.Imaging(cache)
+    r = imaging.compute(io.theta_to_mask(theta), 0.225, 50.0)
+    assert peak_err(cpu(r.aerial_image), ref["aerial"]) <= 1e-4
+    opt = L.CTMOptimizer(cache, target, 0.225, 50.0, iterations=1)
+    loss, gt, norm = opt.evaluate(torch.tensor(theta, dtype=torch.float32, device="cuda"))
+    assert abs(loss - ref["loss"]) <= 1e-4 * ref["loss"]
+    assert rel_l2(cpu(gt), ref["grad_theta"]) <= 1e-3
+
+
+def test_bf16x3_real_optics_and_penalty(L, tc_ctx):
+    n = 64
+    oc = oo.prepare(n, 4.0, 193.0, 1.35, 0.6, 0.9, use_socs=True)
+    target = np.zeros((n, n)); target[23:42, 23:42] = 1.0
+    theta = io.initialize_theta(target)
+    mask = io.theta_to_mask(theta)
+    a, w, E = io.imaging_compute(mask, oc, 0.25, 85.0)
+    gp_ref = io.pe_gradient(w, target, E, oc, 85.0, penalty=2.0, penalty_threshold=0.01)
+    cache = L.ImagingCache.from_kernels(np.stack(oc.kernels), oc.source_ws, oc.eigenvalues, ctx=tc_ctx)
+    imaging = L.Imaging(cache)
+    r = imaging.compute(mask, 0.25, 85.0)
+    assert peak_err(cpu(r.aerial_image), a) <= 1e-4
+    gp = L.Gradient(cache, 0.25, 85.0).pe_gradient_with_penalty(w, target, imaging.get_electric_field(),
+                                                               2.0, 0.01)
+    assert rel_l2(cpu(gp), gp_ref) <= 1e-3
+
+
+def test_bf16x3_agrees_with_fp32_path(L, wl, tc_ctx):
+    N = 1024
+    band, r0, c0, w, wss = wl.synthetic_socs_band(K=48)
+    target = wl.manhattan_target(N, 40, seed=2)
+    rng = np.random.default_rng(8)
+    theta = torch.tensor(rng.uniform(0.0, np.pi, (N, N)), dtype=torch.float32, device="cuda")
+    outs = {}
+    for mode, ctx in (("fp32", L.Context()), ("bf16x3", tc_ctx)):
+        if mode == "fp32":
+            ctx.set_precision("fp32")
+        cache = L.ImagingCache.from_band(N, band, r0, c0, w, wss, ctx=ctx)
+        opt = L.CTMOptimizer(cache, target, 0.225, 50.0, iterations=1)
+        loss, gt, _ = opt.evaluate(theta)
+        outs[mode] = (loss, cpu(gt))
+    assert abs(outs["fp32"][0] - outs["bf16x3"][0]) <= 1e-4 * outs["fp32"][0]
+    assert rel_l2(outs["bf16x3"][1], outs["fp32"][1]) <= 1e-3
