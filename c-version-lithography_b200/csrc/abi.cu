@@ -50,7 +50,7 @@ int upload(Context* ctx, T** dst, const std::vector<T>& src) {
 void free_cache(Cache* c) {
   void* ptrs[] = {c->H,    c->w,    c->TXS,  c->TXD,   c->TYS,   c->TYD,   c->AYS,
                   c->AYD,  c->TXSc, c->TXDc, c->ESr_t, c->ESc_t, c->ESc,   c->EDr_t,
-                  c->EDc_t, c->EDc,  c->AYS_img, c->AYD_img};
+                  c->EDc_t, c->EDc,  c->AYS_img, c->AYD_img, c->TXS_img, c->TXD_img};
   for (void* p : ptrs)
     if (p) cudaFree(p);
 }
@@ -356,11 +356,11 @@ int litho_cache_create_band(litho_ctx* ctx, int N, int K, int Nr, int Nc, int ro
     }
   // The per-kernel CTAs of the small-grid stage keep a band (and a band-by-grid
   // product) in shared memory; larger bands are not built.
-  if (band_fields_smem(g) > 200 * 1024 || (size_t)g.Pr * Nc * sizeof(float2) > 200 * 1024 ||
-      (size_t)72 * (2 * Nc - 1) * sizeof(float2) > 200 * 1024) {
+  if (band_max_smem(g) > 220 * 1024) {
     delete c;
     return ctx->fail(LITHO_ERR_UNSUPPORTED,
-                     "kernel band too large: needs (Nr*Nc + 2*Nr*Nc) * 8 bytes <= 200 KiB");
+                     "kernel band too large for the small-grid kernels' shared memory "
+                     "(supported up to about 70 x 70 frequencies)");
   }
   int st = LITHO_OK;
   if (st == LITHO_OK) st = upload(ctx, &c->H, H);
@@ -379,6 +379,18 @@ int litho_cache_create_band(litho_ctx* ctx, int N, int K, int Nr, int Nc, int ro
   if (st == LITHO_OK) st = upload(ctx, &c->EDr_t, EDr_t);
   if (st == LITHO_OK) st = upload(ctx, &c->EDc_t, EDc_t);
   if (st == LITHO_OK) st = upload(ctx, &c->EDc, EDc);
+  // Split-BF16 images of the two row-analysis twiddle tables for the tensor cores.
+  for (int t = 0; t < 2 && st == LITHO_OK; ++t) {
+    void** img = t == 0 ? &c->TXS_img : &c->TXD_img;
+    const float* src = t == 0 ? c->TXS : c->TXD;
+    if (cudaMalloc(img, tw_image_bytes(N, Nc)) != cudaSuccess) {
+      cudaGetLastError();
+      st = ctx->fail(LITHO_ERR_OOM, "tensor-core operand image allocation failed");
+    } else if (launch_pack_tw(ctx->stream, src, Nc, N, *img) != cudaSuccess ||
+               cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
+      st = ctx->fail(LITHO_ERR_CUDA, "tensor-core operand packing failed");
+    }
+  }
   // Split-BF16 images of the two row-synthesis twiddle tables for the tensor cores.
   for (int t = 0; t < 2 && st == LITHO_OK; ++t) {
     void** img = t == 0 ? &c->AYS_img : &c->AYD_img;
@@ -531,8 +543,10 @@ int run_forward(Context* ctx, const Cache& c, Field& f, const Layout& L, int inp
   int* flag = reinterpret_cast<int*>(ctx->d_red + RED_FLAG);
   int st;
   ctx->stage_begin(0);
+  const bool tc = ctx->precision == LITHO_PRECISION_BF16X3;
   st = check_launch(ctx, launch_analysis(s, input_mode, input, mask_out, flag, c.TXS, g.N, g.Nc,
-                                         c.TYS, g.Nr, g.Nr, 0, at<float2>(ctx, L.part)),
+                                         c.TYS, g.Nr, g.Nr, 0, at<float2>(ctx, L.part),
+                                         tc ? c.TXS_img : nullptr, flag + 1),
                     "tile analysis");
   ctx->stage_end(0);
   if (st) return st;
@@ -578,8 +592,10 @@ int run_adjoint(Context* ctx, const Cache& c, const Field& f, const Layout& L, c
   const int na = 2 * g.Nr - 1;
   int st;
   ctx->stage_begin(4);
+  const bool tc = ctx->precision == LITHO_PRECISION_BF16X3;
   st = check_launch(ctx, launch_analysis(s, 0, dldi, nullptr, flag, c.TXD, g.N, g.Nc, c.TYD, na,
-                                         g.Nr, 1, at<float2>(ctx, L.part)),
+                                         g.Nr, 1, at<float2>(ctx, L.part),
+                                         tc ? c.TXD_img : nullptr, flag + 1),
                     "adjoint tile analysis");
   ctx->stage_end(4);
   if (st) return st;

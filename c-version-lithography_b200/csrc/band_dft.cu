@@ -16,7 +16,12 @@
 // a fused elementwise epilogue. The K-dependent work lives on the small grid.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
+#include <cuda_bf16.h>
+
 #include "device_common.cuh"
+#include "tc_ptx.cuh"
 
 namespace litho_b200 {
 
@@ -114,12 +119,14 @@ struct AnalysisArgs {
   float2* part;        // [tiles][nrows_out][ncols]
 };
 
+template <int BN>
+__device__ void analysis_phase2(float* smem, const AnalysisArgs& a, int y0, int f0, int tile);
+
 template <int TN>
 __global__ void __launch_bounds__(AT_NT)
 analysis_tile_kernel(AnalysisArgs a) {
   extern __shared__ __align__(16) float smem[];
   constexpr int BN = AT_BNT * TN;   // real columns (2 per complex frequency)
-  constexpr int BNC = BN / 2;       // complex columns
   float* As = smem;
   float* Bs = smem + AT_BK * (AT_TILE + 4);
   const int tid = threadIdx.x, tx = tid % AT_BNT, ty = tid / AT_BNT;
@@ -136,20 +143,31 @@ analysis_tile_kernel(AnalysisArgs a) {
     for (int j = 0; j < TN; ++j) acc[i][j] = 0.f;
   gemm_mainloop<AT_BMT, AT_BNT, AT_TM, TN, AT_BK>(ld, a.tw, a.N, Nn, y0, f0, x0,
                                                   min(a.N, x0 + AT_TILE), As, Bs, acc);
-  // Phase 2: P[r][c] = sum_{y in tile} T(r, y) R[y][c] for the tile's rows, as a
-  // register-tiled complex product: each thread owns 2 band rows x 2 columns.
-  constexpr int RS = BN + 4;                         // keeps float4 alignment of R rows
-  float* Rs = smem;                                  // [128][RS]
-  float2* TYs = reinterpret_cast<float2*>(smem + AT_TILE * RS);  // [RC][128]
+  // Phase 2 input: R staged as [128][BN + 4] floats.
+  constexpr int RS = BN + 4;
 #pragma unroll
   for (int i = 0; i < AT_TM; ++i)
 #pragma unroll
-    for (int j = 0; j < TN; ++j) Rs[(ty * AT_TM + i) * RS + tx + j * AT_BNT] = acc[i][j];
+    for (int j = 0; j < TN; ++j) smem[(ty * AT_TM + i) * RS + tx + j * AT_BNT] = acc[i][j];
+  analysis_phase2<BN>(smem, a, y0, f0, blockIdx.y * gridDim.x + blockIdx.x);
+}
+
+// Phase 2 of a tile analysis: P[r][c] = sum_{y in tile} T(r, y) R[y][c] for the
+// tile's rows, R given in smem as [128][BN + 4] floats (complex column c at
+// floats 2c, 2c + 1), as a register-tiled complex product: each thread owns 2
+// band rows x 2 columns. Every thread of the CTA (AT_NT) must call it; it
+// begins with a barrier, so the caller's writes of R need no extra one.
+template <int BN>
+__device__ void analysis_phase2(float* smem, const AnalysisArgs& a, int y0, int f0, int tile) {
+  constexpr int BNC = BN / 2;
+  constexpr int RS = BN + 4;                         // keeps float4 alignment of R rows
+  const float* Rs = smem;                            // [128][RS]
+  float2* TYs = reinterpret_cast<float2*>(smem + AT_TILE * RS);  // [RC][128]
+  const int tid = threadIdx.x;
   constexpr int CP = BNC / 2;                        // column pairs
   const int cp = tid % CP, rp = tid / CP;            // rows 2rp, 2rp+1 of each chunk
   const bool active = rp < AT_RC / 2;
   const int c0g = f0 / 2 + 2 * cp;                   // first of the two global columns
-  const int tile = blockIdx.y * gridDim.x + blockIdx.x;
   for (int r0 = 0; r0 < a.nrows_out; r0 += AT_RC) {
     __syncthreads();
     for (int e = tid; e < AT_RC * AT_TILE; e += AT_NT) {
@@ -215,15 +233,229 @@ int analysis_tiles(int N) {
   return t * t;
 }
 
+// ---------------------------------------------------------------- tile analysis, tcgen05
+// Phase 1 of the tile analysis on the tensor cores in split-BF16:
+//   R[y][f] = sum_{x in tile} A[y][x] tw[f][x]
+// as one BF16 GEMM with M = 128 (rows y), N = rowsP (2 ncols rounded to 16),
+// K = 3 x 128: A3[y] = [A_hi | A_hi | A_lo] is built by the CTA's threads from
+// the FP32 tile (theta -> mask fused), B3[f] = [tw_hi | tw_lo | tw_hi] is a
+// per-cache image bulk-copied from global memory. The accumulator lives in
+// tensor memory; phase 2 (the column contraction) then runs on the CUDA cores
+// from shared memory, exactly as in the SIMT kernel.
+constexpr int AQ_K3 = 3 * AT_TILE;                       // 384
+constexpr uint32_t AQ_A_BYTES = AT_TILE * AQ_K3 * 2;     // 96 KiB
+
+// Image of the row-analysis twiddles tw [nrow][N] for the tensor cores: per
+// 128-column x tile t, a K-major SW128 tile of rowsP rows and 384 K
+// ([hi | lo | hi] of the 128 columns); rows >= nrow and columns >= N are zero.
+__global__ void pack_tw_kernel(const float* __restrict__ tw, int nrow, int rowsP, int N,
+                               uint4* __restrict__ dst, size_t n16) {
+  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= n16) return;
+  const int c = (int)(idx % 8);
+  size_t rest = idx / 8;
+  const int r = (int)(rest % rowsP);
+  rest /= rowsP;
+  const int kb = (int)(rest % (AQ_K3 / 64));
+  const int t = (int)(rest / (AQ_K3 / 64));
+  __nv_bfloat16 out[8];
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    const int k = kb * 64 + c * 8 + q;
+    const int sec = k / AT_TILE, x = t * AT_TILE + k % AT_TILE;
+    const float v = (r < nrow && x < N) ? tw[(size_t)r * N + x] : 0.f;
+    const __nv_bfloat16 hi = __float2bfloat16_rn(v);
+    out[q] = sec == 1 ? __float2bfloat16_rn(v - __bfloat162float(hi)) : hi;
+  }
+  const size_t off16 = ((size_t)t * (AQ_K3 / 64) + kb) * (size_t)rowsP * 8 +
+                       (size_t)(r / 8) * 64 + (size_t)(r % 8) * 8 + (size_t)(c ^ (r % 8));
+  dst[off16] = *reinterpret_cast<const uint4*>(out);
+}
+
+int tw_rows_padded(int ncols) { return (2 * ncols + 15) / 16 * 16; }
+
+size_t tw_image_bytes(int N, int ncols) {
+  const size_t tiles = (size_t)(N + AT_TILE - 1) / AT_TILE;
+  return tiles * (size_t)tw_rows_padded(ncols) * AQ_K3 * 2;
+}
+
+cudaError_t launch_pack_tw(cudaStream_t s, const float* tw, int ncols, int N, void* dst) {
+  const int rowsP = tw_rows_padded(ncols);
+  const size_t tiles = (size_t)(N + AT_TILE - 1) / AT_TILE;
+  const size_t n16 = tiles * (AQ_K3 / 64) * (size_t)rowsP * 8;
+  pack_tw_kernel<<<(unsigned)((n16 + 255) / 256), 256, 0, s>>>(
+      tw, 2 * ncols, rowsP, N, reinterpret_cast<uint4*>(dst), n16);
+  return cudaGetLastError();
+}
+
+// 16 consecutive FP32 columns of this thread's TMEM lane.
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+      "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+template <int BN>   // BN = rowsP: real columns of the accumulator
+__global__ void __launch_bounds__(AT_NT, 1)
+analysis_tc_kernel(AnalysisArgs a, const uint8_t* __restrict__ Bimg, int* __restrict__ err) {
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  __shared__ __align__(8) uint64_t bars[2];
+  __shared__ uint32_t tmem_slot;
+  __shared__ int fail;
+  constexpr uint32_t B_BYTES = (uint32_t)BN * AQ_K3 * 2;
+  constexpr uint32_t TM_COLS = BN <= 32 ? 32 : (BN <= 64 ? 64 : 128);
+  uint8_t* smem = reinterpret_cast<uint8_t*>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
+  uint8_t* sA = smem;
+  uint8_t* sB = smem + AQ_A_BYTES;
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int xt = blockIdx.x, yt = blockIdx.y;
+  const int x0 = xt * AT_TILE, y0 = yt * AT_TILE;
+  const uint32_t barL = tc::smem_u32(&bars[0]), barM = tc::smem_u32(&bars[1]);
+  if (tid == 0) {
+    tc::mbar_init(barL, 1);
+    tc::mbar_init(barM, 1);
+    fail = 0;
+    tc::fence_mbar_init();
+  }
+  if (warp == 0) tc::tmem_alloc(tc::smem_u32(&tmem_slot), TM_COLS);
+  tc::fence_before();
+  __syncthreads();
+  tc::fence_after();
+  const uint32_t tmem = tmem_slot;
+  // Twiddle operand: bulk copy of this x tile's image.
+  if (tid == 0) {
+    tc::mbar_expect_tx(barL, B_BYTES);
+    const uint8_t* gb = Bimg + (size_t)xt * B_BYTES;
+    for (uint32_t q = 0; q < B_BYTES; q += 16384) {
+      const uint32_t n = B_BYTES - q < 16384u ? B_BYTES - q : 16384u;
+      tc::bulk_g2s(tc::smem_u32(sB) + q, gb + q, n, barL);
+    }
+  }
+  // Image operand: 128 rows x 16 chunks of 8 columns, split into [hi | hi | lo].
+  const ImageLoad& ld = a.ld;
+  bool bad = false;
+  for (int j = tid; j < AT_TILE * (AT_TILE / 8); j += AT_NT) {
+    const int r = j / (AT_TILE / 8), c8 = (j % (AT_TILE / 8)) * 8;
+    const int m = y0 + r, x = x0 + c8;
+    float v[8];
+    if (ld.vec4 && m < ld.N && x + 7 < ld.N) {
+      const float4 p = __ldg(reinterpret_cast<const float4*>(ld.in + (size_t)m * ld.N + x));
+      const float4 q = __ldg(reinterpret_cast<const float4*>(ld.in + (size_t)m * ld.N + x + 4));
+      v[0] = p.x; v[1] = p.y; v[2] = p.z; v[3] = p.w; v[4] = q.x; v[5] = q.y; v[6] = q.z; v[7] = q.w;
+    } else {
+#pragma unroll
+      for (int e = 0; e < 8; ++e)
+        v[e] = (m < ld.N && x + e < ld.N) ? __ldg(ld.in + (size_t)m * ld.N + x + e) : 0.f;
+    }
+    __nv_bfloat16 hi[8], lo[8];
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+      const bool in_range = m < ld.N && x + e < ld.N;
+      if (in_range) bad |= !isfinite(v[e]);
+      float u = v[e];
+      if (ld.mode == 1) {
+        u = in_range ? 0.5f * (1.f + cosf(v[e])) : 0.f;
+        if (ld.mask_out && in_range) ld.mask_out[(size_t)m * ld.N + x + e] = u;
+      }
+      hi[e] = __float2bfloat16_rn(u);
+      lo[e] = __float2bfloat16_rn(u - __bfloat162float(hi[e]));
+    }
+    const uint4 h4 = *reinterpret_cast<const uint4*>(hi);
+    const uint4 l4 = *reinterpret_cast<const uint4*>(lo);
+    *reinterpret_cast<uint4*>(sA + sw128_offset(AT_TILE, r, c8)) = h4;
+    *reinterpret_cast<uint4*>(sA + sw128_offset(AT_TILE, r, AT_TILE + c8)) = h4;
+    *reinterpret_cast<uint4*>(sA + sw128_offset(AT_TILE, r, 2 * AT_TILE + c8)) = l4;
+  }
+  if (bad) atomicOr(ld.flag, 1);
+  // Generic-proxy writes of the operand must be visible to the tensor cores.
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  __syncthreads();
+  if (tid == 0) {
+    if (!tc::mbar_wait(barL, 0)) {
+      fail = 1;
+      atomicExch(err, 3);
+    } else {
+      tc::fence_after();
+      constexpr uint32_t idesc = tc::idesc_bf16(AT_TILE, BN);
+      for (int st = 0; st < AQ_K3 / 16; ++st) {
+        const int kb = st >> 2;
+        const uint32_t ko = (uint32_t)(st & 3) * 32;
+        const uint64_t ad = tc::desc_sw128(tc::smem_u32(sA) + kb * (AT_TILE * 128) + ko);
+        const uint64_t bd = tc::desc_sw128(tc::smem_u32(sB) + kb * (BN * 128) + ko);
+        tc::mma_bf16(tmem, ad, bd, idesc, st > 0 ? 1u : 0u);
+      }
+      tc::mma_commit(barM);
+      if (!tc::mbar_wait(barM, 0)) {
+        fail = 2;
+        atomicExch(err, 4);
+        tc::mbar_wait(barM, 0);
+      }
+    }
+  }
+  __syncthreads();
+  tc::fence_after();
+  const bool ok = !fail;
+  if (ok) {
+    // Accumulator -> R staged as [128][BN + 4] floats (the operand tiles are dead).
+    float* Rs = reinterpret_cast<float*>(smem);
+    const int lane_base = (warp & 3) * 32;
+    const int row = lane_base + (tid & 31);
+    for (int cc = (warp >> 2) * 16; cc < BN; cc += 32) {
+      float v[16];
+      tmem_ld16(tmem + ((uint32_t)lane_base << 16) + (uint32_t)cc, v);
+#pragma unroll
+      for (int i = 0; i < 16; ++i) Rs[row * (BN + 4) + cc + i] = v[i];
+    }
+  }
+  tc::fence_before();
+  __syncthreads();
+  if (warp == 0) tc::tmem_dealloc(tmem, TM_COLS);
+  if (ok) analysis_phase2<BN>(reinterpret_cast<float*>(smem), a, y0, 0, yt * gridDim.x + xt);
+}
+
+template <int BN>
+static cudaError_t analysis_tc_t(cudaStream_t s, const AnalysisArgs& a, const void* Bimg, int* err) {
+  const size_t smem = AQ_A_BYTES + (size_t)BN * AQ_K3 * 2 + 1024;
+  cudaError_t e = cudaFuncSetAttribute(analysis_tc_kernel<BN>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  const int t = (a.N + AT_TILE - 1) / AT_TILE;
+  analysis_tc_kernel<BN><<<dim3(t, t), AT_NT, smem, s>>>(a, static_cast<const uint8_t*>(Bimg), err);
+  return cudaGetLastError();
+}
+
 // Tile partials of sum_{y, x} T(a, y) A[y][x] tw(c, x) for every 128 x 128 tile:
 // part[tile][a][c], tiles in row-major order of the tile grid.
 cudaError_t launch_analysis(cudaStream_t s, int mode, const float* in, float* mask_out,
                             int* flag, const float* tw, int N, int ncols, const float2* TY,
-                            int nrows_out, int nr, int sym, float2* part) {
+                            int nrows_out, int nr, int sym, float2* part, const void* tw_img,
+                            int* err) {
   const int vec4 = (N % 4 == 0) && (reinterpret_cast<uintptr_t>(in) % 16 == 0);
   AnalysisArgs a{ImageLoad{in, mask_out, flag, N, mode, vec4}, tw, N, ncols, TY, nrows_out,
                  nr, sym, part};
   const int n2 = 2 * ncols;
+  if (tw_img) {  // split-BF16 tensor-core phase 1 (rowsP <= 128)
+    switch (tw_rows_padded(ncols)) {
+      case 16: return analysis_tc_t<16>(s, a, tw_img, err);
+      case 32: return analysis_tc_t<32>(s, a, tw_img, err);
+      case 48: return analysis_tc_t<48>(s, a, tw_img, err);
+      case 64: return analysis_tc_t<64>(s, a, tw_img, err);
+      case 80: return analysis_tc_t<80>(s, a, tw_img, err);
+      case 96: return analysis_tc_t<96>(s, a, tw_img, err);
+      case 112: return analysis_tc_t<112>(s, a, tw_img, err);
+      case 128: return analysis_tc_t<128>(s, a, tw_img, err);
+      default: break;  // wider bands keep the SIMT phase 1
+    }
+  }
   if (n2 <= 32) return analysis_tile_t<2>(s, a);
   if (n2 <= 48) return analysis_tile_t<3>(s, a);
   if (n2 <= 64) return analysis_tile_t<4>(s, a);
@@ -366,7 +598,6 @@ cudaError_t launch_synth_grad(cudaStream_t s, const float* AY, const float* Bt, 
 // memory when they fit in SMEM_STAGE bytes; otherwise the kernels read them
 // from global memory (L2-resident), with the same arithmetic.
 constexpr size_t SMEM_STAGE = 200 * 1024;
-constexpr int BF_NT = 1024;
 
 template <class T>
 __device__ __forceinline__ const T* stage_copy(T* dst, const T* src, int n, bool use) {
@@ -375,57 +606,71 @@ __device__ __forceinline__ const T* stage_copy(T* dst, const T* src, int n, bool
   return dst;
 }
 
-// Forward 1 (one CTA per kernel k): A = H_k m on the band, T = A ESc^T (Nr x Pc),
-// e_k = ESr T (Pr x Pc) and ik = w_k |e_k|^2.
+// Forward 1: grid (K, column chunks of the small grid). CTA (k, q) owns small-grid
+// columns jc in [q CW, q CW + CW): A = H_k m on the band, T = A ESc^T restricted
+// to those columns (Nr x CW) and e_k = ESr T (Pr x CW); ik = w_k |e_k|^2. Columns
+// are independent, so the split costs no recomputation.
+constexpr int BF_NT = 256;
+constexpr int BF_CW = 10;   // small-grid columns per CTA (forward fields)
+constexpr int BZ_UW = 7;    // band columns per CTA (adjoint Z)
 __global__ void __launch_bounds__(BF_NT)
 band_fields_kernel(const float2* __restrict__ H, const float2* __restrict__ mband,
                    const float* __restrict__ w, int Nr, int Nc, int Pr, int Pc,
                    const float2* __restrict__ ESc_t, const float2* __restrict__ ESr_t,
                    int stage_tables, float2* __restrict__ e, float* __restrict__ ik) {
   extern __shared__ float2 sm2[];
-  float2* A = sm2;                  // [Nr][Nc]
-  float2* T = A + Nr * Nc;          // [Nr][Pc]
-  float2* esc = T + Nr * Pc;        // [Nc][Pc] (staged)
-  float2* esr = esc + Nc * Pc;      // [Nr][Pr] (staged)
   const int k = blockIdx.x;
+  const int j0 = blockIdx.y * BF_CW;
+  const int cw = min(BF_CW, Pc - j0);
+  float2* A = sm2;                  // [Nr][Nc]
+  float2* T = A + Nr * Nc;          // [Nr][BF_CW]
+  float2* esc = T + Nr * BF_CW;     // [Nc][BF_CW]
+  float2* esr = esc + Nc * BF_CW;   // [Nr][Pr] (staged when stage_tables)
   for (int i = threadIdx.x; i < Nr * Nc; i += BF_NT) A[i] = cmul(H[(size_t)k * Nr * Nc + i], mband[i]);
-  const float2* ESC = stage_copy(esc, ESc_t, Nc * Pc, stage_tables);
-  const float2* ESR = stage_copy(esr, ESr_t, Nr * Pr, stage_tables);
+  for (int i = threadIdx.x; i < Nc * BF_CW; i += BF_NT) {
+    const int c = i / BF_CW, jj = i % BF_CW;
+    esc[i] = jj < cw ? ESc_t[(size_t)c * Pc + j0 + jj] : make_float2(0.f, 0.f);
+  }
+  const float2* ESR = ESr_t;
+  if (stage_tables) {
+    for (int i = threadIdx.x; i < Nr * Pr; i += BF_NT) esr[i] = ESr_t[i];
+    ESR = esr;
+  }
   __syncthreads();
-  for (int i = threadIdx.x; i < Nr * Pc; i += BF_NT) {
-    const int r = i / Pc, jc = i % Pc;
+  for (int i = threadIdx.x; i < Nr * BF_CW; i += BF_NT) {
+    const int r = i / BF_CW, jj = i % BF_CW;
     float2 a0 = make_float2(0.f, 0.f), a1 = a0;
     int c = 0;
     for (; c + 1 < Nc; c += 2) {
-      cfma(a0, A[r * Nc + c], ESC[c * Pc + jc]);
-      cfma(a1, A[r * Nc + c + 1], ESC[(c + 1) * Pc + jc]);
+      cfma(a0, A[r * Nc + c], esc[c * BF_CW + jj]);
+      cfma(a1, A[r * Nc + c + 1], esc[(c + 1) * BF_CW + jj]);
     }
-    if (c < Nc) cfma(a0, A[r * Nc + c], ESC[c * Pc + jc]);
+    if (c < Nc) cfma(a0, A[r * Nc + c], esc[c * BF_CW + jj]);
     T[i] = make_float2(a0.x + a1.x, a0.y + a1.y);
   }
   __syncthreads();
   const float wk = w[k];
-  for (int i = threadIdx.x; i < Pr * Pc; i += BF_NT) {
-    const int jr = i / Pc, jc = i % Pc;
+  for (int i = threadIdx.x; i < Pr * cw; i += BF_NT) {
+    const int jr = i / cw, jj = i % cw;
     float2 a0 = make_float2(0.f, 0.f), a1 = a0;
     int r = 0;
     for (; r + 1 < Nr; r += 2) {
-      cfma(a0, ESR[r * Pr + jr], T[r * Pc + jc]);
-      cfma(a1, ESR[(r + 1) * Pr + jr], T[(r + 1) * Pc + jc]);
+      cfma(a0, ESR[r * Pr + jr], T[r * BF_CW + jj]);
+      cfma(a1, ESR[(r + 1) * Pr + jr], T[(r + 1) * BF_CW + jj]);
     }
-    if (r < Nr) cfma(a0, ESR[r * Pr + jr], T[r * Pc + jc]);
+    if (r < Nr) cfma(a0, ESR[r * Pr + jr], T[r * BF_CW + jj]);
     const float2 v = make_float2(a0.x + a1.x, a0.y + a1.y);
-    const size_t o = (size_t)k * Pr * Pc + i;
+    const size_t o = ((size_t)k * Pr + jr) * Pc + j0 + jj;
     e[o] = v;
     ik[o] = wk * (v.x * v.x + v.y * v.y);
   }
 }
 
 static size_t fields_smem_full(const BandGeom& g) {
-  return (size_t)(g.Nr * g.Nc + g.Nr * g.Pc + g.Nc * g.Pc + g.Nr * g.Pr) * sizeof(float2);
+  return (size_t)(g.Nr * g.Nc + g.Nr * BF_CW + g.Nc * BF_CW + g.Nr * g.Pr) * sizeof(float2);
 }
 size_t band_fields_smem(const BandGeom& g) {
-  return (size_t)(g.Nr * g.Nc + g.Nr * g.Pc) * sizeof(float2);
+  return (size_t)(g.Nr * g.Nc + g.Nr * BF_CW + g.Nc * BF_CW) * sizeof(float2);
 }
 
 // Forward 2: i[j] = sum_k ik[k][j] in k order.
@@ -444,33 +689,49 @@ __global__ void __launch_bounds__(BI_NT)
 band_chat_kernel(const float* __restrict__ iP, int Nr, int Nc, int Pr, int Pc,
                  const float2* __restrict__ EDr_t, const float2* __restrict__ EDc, float inv,
                  float2* __restrict__ chat) {
+  // Operands are staged with one parallel round trip; the products then run
+  // from shared memory (the L2 latency chains of a per-thread loop dominated).
   extern __shared__ float2 sb[];
-  float2* v = sb;             // [Pc]
-  float2* ed = sb + Pc;       // [Pr]
-  const int dr = blockIdx.x;
   const int nd = 2 * Nc - 1;
+  float2* v = sb;                                    // [Pc]
+  float2* ed = v + Pc;                               // [Pr]
+  float2* edc = ed + Pr;                             // [Pc][nd]
+  float* ip = reinterpret_cast<float*>(edc + Pc * nd);  // [Pr][Pc]
+  const int dr = blockIdx.x;
   for (int jr = threadIdx.x; jr < Pr; jr += BI_NT) ed[jr] = EDr_t[(size_t)(dr + Nr - 1) * Pr + jr];
+  for (int i = threadIdx.x; i < Pc * nd; i += BI_NT) edc[i] = EDc[i];
+  for (int i = threadIdx.x; i < Pr * Pc; i += BI_NT) ip[i] = iP[i];
   __syncthreads();
   for (int jc = threadIdx.x; jc < Pc; jc += BI_NT) {
     float2 a = make_float2(0.f, 0.f), b = a;
     int jr = 0;
     for (; jr + 1 < Pr; jr += 2) {
-      const float i0 = iP[(size_t)jr * Pc + jc], i1 = iP[(size_t)(jr + 1) * Pc + jc];
+      const float i0 = ip[jr * Pc + jc], i1 = ip[(jr + 1) * Pc + jc];
       a.x = fmaf(ed[jr].x, i0, a.x); a.y = fmaf(-ed[jr].y, i0, a.y);
       b.x = fmaf(ed[jr + 1].x, i1, b.x); b.y = fmaf(-ed[jr + 1].y, i1, b.y);
     }
     if (jr < Pr) {
-      const float i0 = iP[(size_t)jr * Pc + jc];
+      const float i0 = ip[jr * Pc + jc];
       a.x = fmaf(ed[jr].x, i0, a.x); a.y = fmaf(-ed[jr].y, i0, a.y);
     }
     v[jc] = make_float2(a.x + b.x, a.y + b.y);
   }
   __syncthreads();
   for (int dc = threadIdx.x; dc < nd; dc += BI_NT) {
-    float2 a = make_float2(0.f, 0.f);
-    for (int jc = 0; jc < Pc; ++jc) cfma(a, v[jc], conjf2(EDc[(size_t)jc * nd + dc]));
-    chat[(size_t)dr * nd + dc] = make_float2(a.x * inv, a.y * inv);
+    float2 a = make_float2(0.f, 0.f), b = a;
+    int jc = 0;
+    for (; jc + 1 < Pc; jc += 2) {
+      cfma(a, v[jc], conjf2(edc[jc * nd + dc]));
+      cfma(b, v[jc + 1], conjf2(edc[(jc + 1) * nd + dc]));
+    }
+    if (jc < Pc) cfma(a, v[jc], conjf2(edc[jc * nd + dc]));
+    chat[(size_t)dr * nd + dc] = make_float2((a.x + b.x) * inv, (a.y + b.y) * inv);
   }
+}
+
+static size_t chat_smem(const BandGeom& g) {
+  const int nd = 2 * g.Nc - 1;
+  return (size_t)(g.Pc + g.Pr + g.Pc * nd) * sizeof(float2) + (size_t)g.Pr * g.Pc * sizeof(float);
 }
 
 // Band -> image columns: Ut[x][2a + {0,1}] = kappa(a) sum_c coef[a][c] phase(c, x) for
@@ -550,13 +811,17 @@ cudaError_t launch_band_forward(cudaStream_t s, const Cache& c, Field& f, float*
   cudaError_t err = cudaFuncSetAttribute(band_fields_kernel,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1);
   if (err != cudaSuccess) return err;
-  band_fields_kernel<<<g.K, BF_NT, sm1, s>>>(c.H, f.mband, c.w, g.Nr, g.Nc, g.Pr, g.Pc, c.ESc_t,
-                                             c.ESr_t, stage, f.e, ik);
+  band_fields_kernel<<<dim3(g.K, (g.Pc + BF_CW - 1) / BF_CW), BF_NT, sm1, s>>>(
+      c.H, f.mband, c.w, g.Nr, g.Nc, g.Pr, g.Pc, c.ESc_t, c.ESr_t, stage, f.e, ik);
   const int n = g.Pr * g.Pc;
   sum_k_kernel<<<(n + 255) / 256, 256, 0, s>>>(ik, g.K, n, iP);
   const int nd = 2 * g.Nc - 1;
-  band_chat_kernel<<<g.Nr, BI_NT, (size_t)(g.Pc + g.Pr) * sizeof(float2), s>>>(
-      iP, g.Nr, g.Nc, g.Pr, g.Pc, c.EDr_t, c.EDc, 1.f / ((float)g.Pr * (float)g.Pc), chat);
+  const size_t smc = chat_smem(g);
+  err = cudaFuncSetAttribute(band_chat_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smc);
+  if (err != cudaSuccess) return err;
+  band_chat_kernel<<<g.Nr, BI_NT, smc, s>>>(iP, g.Nr, g.Nc, g.Pr, g.Pc, c.EDr_t, c.EDc,
+                                            1.f / ((float)g.Pr * (float)g.Pc), chat);
   err = cudaGetLastError();
   if (err != cudaSuccess) return err;
   return launch_expand(s, chat, g.Nr, nd, nd, c.TXDc, g.N, 1, g.Nc, g.kp_rows, Ut);
@@ -569,51 +834,83 @@ __global__ void __launch_bounds__(256)
 band_gamma_kernel(const float2* __restrict__ gh, int Nr, int Nc, int Pr, int Pc,
                   const float2* __restrict__ EDr_t, const float2* __restrict__ EDc_t,
                   float* __restrict__ gam) {
-  extern __shared__ float2 sg[];  // [Nc]
+  extern __shared__ float2 sg[];
   const int jr = blockIdx.x;
   const int na = 2 * Nr - 1;
+  float2* wv = sg;               // [Nc]
+  float2* edr = wv + Nc;         // [na]   column jr of EDr_t
+  float2* ghs = edr + na;        // [na][Nc]
+  float2* edc = ghs + na * Nc;   // [Nc][Pc] rows Nc-1 .. 2Nc-2 of EDc_t
+  for (int r = threadIdx.x; r < na; r += blockDim.x) edr[r] = EDr_t[(size_t)r * Pr + jr];
+  for (int i = threadIdx.x; i < na * Nc; i += blockDim.x) ghs[i] = gh[i];
+  for (int i = threadIdx.x; i < Nc * Pc; i += blockDim.x) edc[i] = EDc_t[(size_t)(Nc - 1) * Pc + i];
+  __syncthreads();
   for (int c = threadIdx.x; c < Nc; c += blockDim.x) {
     float2 a = make_float2(0.f, 0.f);
-    for (int r = 0; r < na; ++r) cfma(a, EDr_t[(size_t)r * Pr + jr], gh[(size_t)r * Nc + c]);
+    for (int r = 0; r < na; ++r) cfma(a, edr[r], ghs[r * Nc + c]);
     const float kc = c > 0 ? 2.f : 1.f;
-    sg[c] = make_float2(kc * a.x, kc * a.y);
+    wv[c] = make_float2(kc * a.x, kc * a.y);
   }
   __syncthreads();
   for (int jc = threadIdx.x; jc < Pc; jc += blockDim.x) {
     float acc = 0.f;
     for (int c = 0; c < Nc; ++c) {
-      const float2 t = EDc_t[(size_t)(c + Nc - 1) * Pc + jc];
-      acc = fmaf(sg[c].x, t.x, fmaf(-sg[c].y, t.y, acc));
+      const float2 t = edc[c * Pc + jc];
+      acc = fmaf(wv[c].x, t.x, fmaf(-wv[c].y, t.y, acc));
     }
     gam[(size_t)jr * Pc + jc] = acc;
   }
 }
 
-// Adjoint 2 (one CTA per kernel k): q = e_k gamma (Pr x Pc), Z1 = q conj(ESc) (Pr x Nc),
-// Zk = conj(ESr_t) Z1 / (Pr Pc) (Nr x Nc).
+static size_t gamma_smem(const BandGeom& g) {
+  const int na = 2 * g.Nr - 1;
+  return (size_t)(g.Nc + na + na * g.Nc + g.Nc * g.Pc) * sizeof(float2);
+}
+
+// Largest dynamic shared memory any small-grid kernel needs for this band
+// (the per-kernel CTAs fall back to unstaged tables above their staging limit).
+size_t band_max_smem(const BandGeom& g) {
+  size_t m = band_fields_smem(g);
+  m = std::max(m, (size_t)(g.Pr * BZ_UW + g.Pc * BZ_UW) * sizeof(float2));
+  m = std::max(m, chat_smem(g));
+  m = std::max(m, gamma_smem(g));
+  m = std::max(m, (size_t)72 * (2 * g.Nc - 1) * sizeof(float2));
+  return m;
+}
+
+// Adjoint 2: grid (K, band column chunks). CTA (k, q) owns band columns uc in
+// [q UW, q UW + UW): q_k = e_k gamma (Pr x Pc, staged), Z1 = q_k conj(ESc)
+// restricted to those columns (Pr x UW), Zk = conj(ESr_t) Z1 / (Pr Pc) (Nr x UW).
 __global__ void __launch_bounds__(BF_NT)
 band_z_kernel(const float2* __restrict__ e, const float* __restrict__ gam, int Nr, int Nc, int Pr,
               int Pc, const float2* __restrict__ ESc, const float2* __restrict__ ESr_t,
               int stage_tables, float inv, float2* __restrict__ Zk) {
   extern __shared__ float2 sz[];
-  float2* Z1 = sz;                  // [Pr][Nc]
-  float2* q = Z1 + Pr * Nc;         // [Pr][Pc]   (staged)
-  float2* esc = q + Pr * Pc;        // [Pc][Nc]   (staged)
-  float2* esr = esc + Pc * Nc;      // [Nr][Pr]   (staged)
   const int k = blockIdx.x;
+  const int u0 = blockIdx.y * BZ_UW;
+  const int uw = min(BZ_UW, Nc - u0);
+  float2* Z1 = sz;                  // [Pr][BZ_UW]
+  float2* esc = Z1 + Pr * BZ_UW;    // [Pc][BZ_UW]
+  float2* q = esc + Pc * BZ_UW;     // [Pr][Pc]   (staged)
+  float2* esr = q + Pr * Pc;        // [Nr][Pr]   (staged)
   const float2* ek = e + (size_t)k * Pr * Pc;
-  const float2* ESC = stage_copy(esc, ESc, Pc * Nc, stage_tables);
-  const float2* ESR = stage_copy(esr, ESr_t, Nr * Pr, stage_tables);
+  for (int i = threadIdx.x; i < Pc * BZ_UW; i += BF_NT) {
+    const int jc = i / BZ_UW, uu = i % BZ_UW;
+    esc[i] = uu < uw ? conjf2(ESc[(size_t)jc * Nc + u0 + uu]) : make_float2(0.f, 0.f);
+  }
+  const float2* ESR = ESr_t;
   if (stage_tables) {
     for (int i = threadIdx.x; i < Pr * Pc; i += BF_NT) {
       const float2 v = ek[i];
       const float gv = gam[i];
       q[i] = make_float2(v.x * gv, v.y * gv);
     }
+    for (int i = threadIdx.x; i < Nr * Pr; i += BF_NT) esr[i] = ESr_t[i];
+    ESR = esr;
   }
   __syncthreads();
-  for (int i = threadIdx.x; i < Pr * Nc; i += BF_NT) {
-    const int jr = i / Nc, uc = i % Nc;
+  for (int i = threadIdx.x; i < Pr * BZ_UW; i += BF_NT) {
+    const int jr = i / BZ_UW, uu = i % BZ_UW;
     float2 a0 = make_float2(0.f, 0.f), a1 = a0;
     for (int jc = 0; jc < Pc; ++jc) {
       float2 v;
@@ -624,22 +921,23 @@ band_z_kernel(const float2* __restrict__ e, const float* __restrict__ gam, int N
         const float gv = gam[(size_t)jr * Pc + jc];
         v = make_float2(t.x * gv, t.y * gv);
       }
-      if (jc & 1) cfma(a1, v, conjf2(ESC[jc * Nc + uc]));
-      else cfma(a0, v, conjf2(ESC[jc * Nc + uc]));
+      if (jc & 1) cfma(a1, v, esc[jc * BZ_UW + uu]);
+      else cfma(a0, v, esc[jc * BZ_UW + uu]);
     }
     Z1[i] = make_float2(a0.x + a1.x, a0.y + a1.y);
   }
   __syncthreads();
-  for (int i = threadIdx.x; i < Nr * Nc; i += BF_NT) {
-    const int ur = i / Nc, uc = i % Nc;
+  for (int i = threadIdx.x; i < Nr * uw; i += BF_NT) {
+    const int ur = i / uw, uu = i % uw;
     float2 a0 = make_float2(0.f, 0.f), a1 = a0;
     int jr = 0;
     for (; jr + 1 < Pr; jr += 2) {
-      cfma(a0, conjf2(ESR[ur * Pr + jr]), Z1[jr * Nc + uc]);
-      cfma(a1, conjf2(ESR[ur * Pr + jr + 1]), Z1[(jr + 1) * Nc + uc]);
+      cfma(a0, conjf2(ESR[ur * Pr + jr]), Z1[jr * BZ_UW + uu]);
+      cfma(a1, conjf2(ESR[ur * Pr + jr + 1]), Z1[(jr + 1) * BZ_UW + uu]);
     }
-    if (jr < Pr) cfma(a0, conjf2(ESR[ur * Pr + jr]), Z1[jr * Nc + uc]);
-    Zk[(size_t)k * Nr * Nc + i] = make_float2((a0.x + a1.x) * inv, (a0.y + a1.y) * inv);
+    if (jr < Pr) cfma(a0, conjf2(ESR[ur * Pr + jr]), Z1[jr * BZ_UW + uu]);
+    Zk[((size_t)k * Nr + ur) * Nc + u0 + uu] =
+        make_float2((a0.x + a1.x) * inv, (a0.y + a1.y) * inv);
   }
 }
 
@@ -661,17 +959,21 @@ __global__ void band_x_kernel(const float2* __restrict__ Zk, const float2* __res
 cudaError_t launch_band_adjoint(cudaStream_t s, const Cache& c, const Field& f, const float2* gh,
                                 double scale, float* gam, float2* Zk, float2* X, float* Vt) {
   const BandGeom& g = c.g;
-  band_gamma_kernel<<<g.Pr, 256, g.Nc * sizeof(float2), s>>>(gh, g.Nr, g.Nc, g.Pr, g.Pc, c.EDr_t,
-                                                             c.EDc_t, gam);
-  const size_t base = (size_t)g.Pr * g.Nc * sizeof(float2);
-  const size_t full = base + (size_t)(g.Pr * g.Pc + g.Pc * g.Nc + g.Nr * g.Pr) * sizeof(float2);
+  const size_t smg = gamma_smem(g);
+  cudaError_t e0 = cudaFuncSetAttribute(band_gamma_kernel,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smg);
+  if (e0 != cudaSuccess) return e0;
+  band_gamma_kernel<<<g.Pr, 256, smg, s>>>(gh, g.Nr, g.Nc, g.Pr, g.Pc, c.EDr_t, c.EDc_t, gam);
+  const size_t base = (size_t)(g.Pr * BZ_UW + g.Pc * BZ_UW) * sizeof(float2);
+  const size_t full = base + (size_t)(g.Pr * g.Pc + g.Nr * g.Pr) * sizeof(float2);
   const int stage = full <= SMEM_STAGE;
   const size_t smz = stage ? full : base;
   cudaError_t err = cudaFuncSetAttribute(band_z_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smz);
   if (err != cudaSuccess) return err;
-  band_z_kernel<<<g.K, BF_NT, smz, s>>>(f.e, gam, g.Nr, g.Nc, g.Pr, g.Pc, c.ESc, c.ESr_t, stage,
-                                        1.f / ((float)g.Pr * (float)g.Pc), Zk);
+  band_z_kernel<<<dim3(g.K, (g.Nc + BZ_UW - 1) / BZ_UW), BF_NT, smz, s>>>(
+      f.e, gam, g.Nr, g.Nc, g.Pr, g.Pc, c.ESc, c.ESr_t, stage, 1.f / ((float)g.Pr * (float)g.Pc),
+      Zk);
   const int nb = g.Nr * g.Nc;
   band_x_kernel<<<(nb + 127) / 128, 128, 0, s>>>(Zk, c.H, c.w, g.K, nb, (float)scale, X);
   err = cudaGetLastError();

@@ -113,6 +113,40 @@ struct ResistEpi {
     if (p.wafer) st4(p.wafer, i, W, vec, nvalid);
     st4(p.dldi, i, g, vec, nvalid);
   }
+  // V float4 chunks at once: every input load is issued before any store, so
+  // the loads of the batch overlap instead of waiting on one another.
+  template <int V>
+  __device__ __forceinline__ void store4v(const int (&m)[V], const int (&n)[V],
+                                          const float4 (&I)[V], const int (&nv)[V]) {
+    if (p.mode == 0) {
+#pragma unroll
+      for (int q = 0; q < V; ++q)
+        if (nv[q] > 0) store4(m[q], n[q], I[q], nv[q]);
+      return;
+    }
+    float4 T[V], pw[V], qw[V];
+    const float4 one4 = make_float4(1.f, 1.f, 1.f, 1.f);
+#pragma unroll
+    for (int q = 0; q < V; ++q) {
+      const size_t i = (size_t)m[q] * N + n[q];
+      T[q] = nv[q] > 0 ? ld4(p.target, i, vec, nv[q]) : one4;
+      pw[q] = (p.pe_window && nv[q] > 0) ? ld4(p.pe_window, i, vec, nv[q]) : one4;
+      qw[q] = (p.pen_window && nv[q] > 0) ? ld4(p.pen_window, i, vec, nv[q]) : pw[q];
+    }
+#pragma unroll
+    for (int q = 0; q < V; ++q) {
+      if (nv[q] <= 0) continue;
+      const size_t i = (size_t)m[q] * N + n[q];
+      float4 W = make_float4(0.f, 0.f, 0.f, 0.f), g = W;
+      if (nv[q] > 0) one(I[q].x, T[q].x, pw[q].x, qw[q].x, W.x, g.x);
+      if (nv[q] > 1) one(I[q].y, T[q].y, pw[q].y, qw[q].y, W.y, g.y);
+      if (nv[q] > 2) one(I[q].z, T[q].z, pw[q].z, qw[q].z, W.z, g.z);
+      if (nv[q] > 3) one(I[q].w, T[q].w, pw[q].w, qw[q].w, W.w, g.w);
+      if (p.aerial) st4(p.aerial, i, I[q], vec, nv[q]);
+      if (p.wafer) st4(p.wafer, i, W, vec, nv[q]);
+      st4(p.dldi, i, g, vec, nv[q]);
+    }
+  }
   // All EPI_NT threads of the CTA must call finish.
   __device__ __forceinline__ void finish() {
     if (p.mode != 1) return;
@@ -156,6 +190,32 @@ struct GradEpi {
     if (nvalid > 2) nrm += (double)gt.z * gt.z;
     if (nvalid > 3) nrm += (double)gt.w * gt.w;
     st4(p.grad_theta, i, gt, vec, nvalid);
+  }
+  template <int V>
+  __device__ __forceinline__ void store4v(const int (&m)[V], const int (&n)[V],
+                                          const float4 (&G)[V], const int (&nv)[V]) {
+    float4 th[V];
+#pragma unroll
+    for (int q = 0; q < V; ++q)
+      th[q] = (p.theta && nv[q] > 0) ? ld4(p.theta, (size_t)m[q] * N + n[q], vec, nv[q])
+                                     : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+    for (int q = 0; q < V; ++q) {
+      if (nv[q] <= 0) continue;
+      const size_t i = (size_t)m[q] * N + n[q];
+      if (p.grad_mask) st4(p.grad_mask, i, G[q], vec, nv[q]);
+      if (!p.theta) continue;
+      float4 gt;
+      gt.x = -0.5f * G[q].x * sinf(th[q].x);
+      gt.y = -0.5f * G[q].y * sinf(th[q].y);
+      gt.z = -0.5f * G[q].z * sinf(th[q].z);
+      gt.w = -0.5f * G[q].w * sinf(th[q].w);
+      if (nv[q] > 0) nrm += (double)gt.x * gt.x;
+      if (nv[q] > 1) nrm += (double)gt.y * gt.y;
+      if (nv[q] > 2) nrm += (double)gt.z * gt.z;
+      if (nv[q] > 3) nrm += (double)gt.w * gt.w;
+      st4(p.grad_theta, i, gt, vec, nv[q]);
+    }
   }
   __device__ __forceinline__ void finish() {
     if (!p.theta) return;

@@ -67,6 +67,9 @@ struct Cache {
   // Split-BF16 tensor-core operand images of AYS / AYD (see synth_tc.cu).
   void* AYS_img = nullptr;
   void* AYD_img = nullptr;
+  // Split-BF16 tensor-core images of the row-analysis twiddles TXS / TXD.
+  void* TXS_img = nullptr;
+  void* TXD_img = nullptr;
   int device = 0;
 };
 
@@ -126,15 +129,22 @@ struct Context {
 // with tw = [2 ncols][N] real rows (Re, Im) and T(a, y) = TY[a][y] (sym 0,
 // a < nrows_out) or, for sym 1, d = a - (nr - 1), TY[d][y] / conj(TY[-d][y]).
 int analysis_tiles(int N);
+// tw_img (nullable): the split-BF16 tensor-core image of tw (launch_pack_tw);
+// when set, phase 1 runs on tcgen05 and err receives a code if a bounded wait
+// of the kernel expires.
 cudaError_t launch_analysis(cudaStream_t s, int mode, const float* in, float* mask_out,
                             int* flag, const float* tw, int N, int ncols, const float2* TY,
-                            int nrows_out, int nr, int sym, float2* part);
+                            int nrows_out, int nr, int sym, float2* part, const void* tw_img,
+                            int* err);
+size_t tw_image_bytes(int N, int ncols);
+cudaError_t launch_pack_tw(cudaStream_t s, const float* tw, int ncols, int N, void* dst);
 // out[o] = scale * sum_t part[t][o] (fixed order).
 cudaError_t launch_reduce_tiles(cudaStream_t s, const float2* part, int tiles, int count,
                                 float scale, float2* out);
 // Small-grid stage of the forward: f.mband -> f.e, ik, iP and Ut (the row
 // synthesis operand). Shared memory of its per-kernel CTA: band_fields_smem.
 size_t band_fields_smem(const BandGeom& g);
+size_t band_max_smem(const BandGeom& g);
 cudaError_t launch_band_forward(cudaStream_t s, const Cache& c, Field& f, float* ik, float* iP,
                                 float2* chat, float* Ut);
 // Small-grid stage of the adjoint: gh (the D-band DFT of dL/dI) -> gam, Zk, X and Vt.

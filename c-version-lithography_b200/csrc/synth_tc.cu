@@ -31,7 +31,7 @@ constexpr int TC_M = 128, TC_N = 256, TC_KC = 256;  // tile rows, tile columns, 
 constexpr int TC_NT = 256;
 constexpr uint32_t TC_A_BYTES = TC_M * TC_KC * 2;   // 64 KiB
 constexpr uint32_t TC_B_BYTES = TC_N * TC_KC * 2;   // 128 KiB
-constexpr int TC_SS = 33;                           // staging row stride (floats)
+constexpr int TC_SS = TC_N + 4;                     // staging row stride (floats)
 
 // ---------------------------------------------------------------- operand images
 // Image of a [rows][kp] FP32 matrix as split-BF16 K-major SW128 tiles:
@@ -157,9 +157,12 @@ synth_tc_kernel(const uint8_t* __restrict__ Aimg, const uint8_t* __restrict__ Bi
   tc::fence_after();
 
   if (!fail) {
-    // Epilogue. Warps w and w + 4 read TMEM lanes 32 (w % 4) .. + 31 (tile rows);
-    // warps 0-3 take accumulator columns [0, 128), warps 4-7 [128, 256), in four
-    // rounds of 32 columns, staged as [2][128][TC_SS] floats.
+    // Epilogue. The whole 128 x 256 FP32 accumulator is staged in shared memory
+    // (the operand tiles are dead): warps w and w + 4 read TMEM lanes 32 (w % 4)
+    // .. + 31, warps 0-3 columns [0, 128), warps 4-7 [128, 256), and store rows
+    // with 16-byte writes (row stride TC_SS, conflict-free per quarter warp).
+    // Then all threads run the fused epilogue over 16-byte column chunks, four
+    // chunks per batch so that their global loads overlap.
     float* stg = reinterpret_cast<float*>(smem);
     const int lane_base = (warp & 3) * 32;
     const int half = warp >> 2;
@@ -168,17 +171,28 @@ synth_tc_kernel(const uint8_t* __restrict__ Aimg, const uint8_t* __restrict__ Bi
       const int col = half * 128 + rd * 32;
       float v[32];
       tc::tmem_ld32(tmem + ((uint32_t)lane_base << 16) + (uint32_t)col, v);
-      float* row = stg + ((size_t)half * TC_M + lane_base + lane) * TC_SS;
+      float* row = stg + (size_t)(lane_base + lane) * TC_SS + col;
 #pragma unroll
-      for (int i = 0; i < 32; ++i) row[i] = v[i];
-      __syncthreads();
-      // 2 halves x 128 rows x 32 columns; warp w handles rows w, w + 8, ... of both halves.
-      for (int rr = warp; rr < 2 * TC_M; rr += TC_NT / 32) {
-        const int h = rr / TC_M, r = rr % TC_M;
-        const int m = y0 + r, n = x0 + h * 128 + rd * 32 + lane;
-        if (m < N && n < N) epi.store1(m, n, stg[((size_t)h * TC_M + r) * TC_SS + lane]);
+      for (int i = 0; i < 32; i += 4)
+        *reinterpret_cast<float4*>(row + i) = make_float4(v[i], v[i + 1], v[i + 2], v[i + 3]);
+    }
+    __syncthreads();
+    constexpr int CH = TC_N / 4;                 // float4 chunks per row
+    constexpr int V = 4;
+    for (int base = tid; base < TC_M * CH; base += TC_NT * V) {
+      int m[V], n[V], nv[V];
+      float4 val[V];
+#pragma unroll
+      for (int q = 0; q < V; ++q) {
+        const int idx = base + q * TC_NT;
+        const int r = idx / CH, c4 = (idx % CH) * 4;
+        m[q] = y0 + r;
+        n[q] = x0 + c4;
+        nv[q] = (idx < TC_M * CH && m[q] < N && n[q] < N) ? min(4, N - n[q]) : 0;
+        val[q] = nv[q] > 0 ? *reinterpret_cast<const float4*>(stg + (size_t)r * TC_SS + c4)
+                           : make_float4(0.f, 0.f, 0.f, 0.f);
       }
-      __syncthreads();
+      epi.template store4v<V>(m, n, val, nv);
     }
   }
   epi.finish();
@@ -208,12 +222,17 @@ static cudaError_t launch_tc(cudaStream_t s, const void* Aimg, const void* Bimg,
 
 cudaError_t launch_synth_resist_tc(cudaStream_t s, const void* Aimg, const void* Bimg, int N,
                                    int kp, const ResistEpilogue& ep, int* err, int* nblocks) {
-  return launch_tc(s, Aimg, Bimg, N, kp, ResistEpi{ep, N, 0, 0.0, 0.0}, err, nblocks);
+  const int vec = N % 4 == 0 && aligned16(ep.aerial) && aligned16(ep.wafer) &&
+                  aligned16(ep.target) && aligned16(ep.pe_window) && aligned16(ep.pen_window) &&
+                  aligned16(ep.dldi);
+  return launch_tc(s, Aimg, Bimg, N, kp, ResistEpi{ep, N, vec, 0.0, 0.0}, err, nblocks);
 }
 
 cudaError_t launch_synth_grad_tc(cudaStream_t s, const void* Aimg, const void* Bimg, int N, int kp,
                                  const GradEpilogue& ep, int* err, int* nblocks) {
-  return launch_tc(s, Aimg, Bimg, N, kp, GradEpi{ep, N, 0, 0.0}, err, nblocks);
+  const int vec = N % 4 == 0 && aligned16(ep.grad_mask) && aligned16(ep.theta) &&
+                  aligned16(ep.grad_theta);
+  return launch_tc(s, Aimg, Bimg, N, kp, GradEpi{ep, N, vec, 0.0}, err, nblocks);
 }
 
 }  // namespace litho_b200

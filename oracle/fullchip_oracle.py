@@ -1,0 +1,266 @@
+"""FP64 restatement of the reference full-chip partition, micro-gradient exchange and
+full-chip CTM (test infrastructure only, see ``oracle/__init__.py``).
+
+Follows source/utils/partition.cpp:21-120, source/utils/micro_gradient_exchange.cpp:65-334
+(PE and PEPenalty loss types, Core or Core+Guard loss region, guard-only or
+two-sided CEPT, Average or Linear guard-gradient fusion) and
+source/optimizer/full_chip_ctm.cpp:25-152. EPE loss types need EP selection
+(ep_select.cpp), which is outside the restated path.
+"""
+from __future__ import annotations
+
+import dataclasses
+from typing import List, Optional
+
+import numpy as np
+
+from . import imaging_oracle as io
+
+
+@dataclasses.dataclass(frozen=True)
+class Rect:
+    """PartitionRect (include/utils/partition.h): half-open [y0, y1) x [x0, x1)."""
+    y0: int
+    y1: int
+    x0: int
+    x1: int
+
+    @property
+    def rows(self):
+        return self.y1 - self.y0
+
+    @property
+    def cols(self):
+        return self.x1 - self.x0
+
+    def shifted(self, dy, dx):
+        return Rect(self.y0 + dy, self.y1 + dy, self.x0 + dx, self.x1 + dx)
+
+    def expanded(self, w):
+        return Rect(self.y0 - w, self.y1 + w, self.x0 - w, self.x1 + w)
+
+    @staticmethod
+    def intersection(a, b):
+        return Rect(max(a.y0, b.y0), min(a.y1, b.y1), max(a.x0, b.x0), min(a.x1, b.x1))
+
+
+LEFT, RIGHT, TOP, BOTTOM = 0, 1, 2, 3
+
+
+@dataclasses.dataclass
+class Neighbor:
+    id: int
+    direction: int
+    guard_global: Rect
+    my_guard_local: Rect
+    neighbor_overlap_local: Rect
+    overlap_global: Rect
+    my_overlap_local: Rect
+    neighbor_guard_local: Rect
+
+
+@dataclasses.dataclass
+class Tile:
+    id: int
+    row: int
+    col: int
+    halo: int
+    guard: int
+    core_global: Rect
+    tile_global: Rect
+    core_local: Rect
+    update_local: Rect
+    neighbors: List[Neighbor]
+
+
+@dataclasses.dataclass
+class Meta:
+    height: int
+    width: int
+    grid_rows: int
+    grid_cols: int
+    halo: int
+    guard: int
+    tile_size: int
+    tiles: List[Tile]
+
+
+def build(height, width, grid_rows, grid_cols, halo, guard) -> Meta:
+    """Partition::build (source/utils/partition.cpp:21-80)."""
+    max_r = (height + grid_rows - 1) // grid_rows
+    max_c = (width + grid_cols - 1) // grid_cols
+    ts = max(max_r, max_c) + 2 * halo
+    ts += ts % 2
+    tiles = []
+    for row in range(grid_rows):
+        for col in range(grid_cols):
+            core = Rect(row * height // grid_rows, (row + 1) * height // grid_rows,
+                        col * width // grid_cols, (col + 1) * width // grid_cols)
+            oy, ox = core.y0 - halo, core.x0 - halo
+            tg = Rect(oy, oy + ts, ox, ox + ts)
+            cl = core.shifted(-oy, -ox)
+            tiles.append(Tile(row * grid_cols + col, row, col, halo, guard, core, tg, cl,
+                              cl.expanded(guard), []))
+    dirs = [(0, -1, LEFT), (0, 1, RIGHT), (-1, 0, TOP), (1, 0, BOTTOM)]
+    for t in tiles:
+        for dr, dc, d in dirs:
+            r, c = t.row + dr, t.col + dc
+            if r < 0 or r >= grid_rows or c < 0 or c >= grid_cols:
+                continue
+            nb = tiles[r * grid_cols + c]
+            gg = Rect.intersection(t.core_global.expanded(guard), nb.core_global)
+            og = Rect.intersection(t.core_global, nb.core_global.expanded(guard))
+            t.neighbors.append(Neighbor(
+                nb.id, d, gg, gg.shifted(-t.tile_global.y0, -t.tile_global.x0),
+                gg.shifted(-nb.tile_global.y0, -nb.tile_global.x0), og,
+                og.shifted(-t.tile_global.y0, -t.tile_global.x0),
+                og.shifted(-nb.tile_global.y0, -nb.tile_global.x0)))
+    return Meta(height, width, grid_rows, grid_cols, halo, guard, ts, tiles)
+
+
+def extract_local_tile(g, tile):
+    """Partition::extract_local_tile (partition.cpp:83-95): periodic wrap."""
+    H, W = g.shape
+    ys = (tile.tile_global.y0 + np.arange(tile.tile_global.rows)) % H
+    xs = (tile.tile_global.x0 + np.arange(tile.tile_global.cols)) % W
+    return g[np.ix_(ys, xs)].copy()
+
+
+def assemble_global(locals_, meta):
+    """Partition::assemble_global (partition.cpp:105-113): Core only."""
+    out = np.zeros((meta.height, meta.width))
+    for t in meta.tiles:
+        d, s = t.core_global, t.core_local
+        out[d.y0:d.y1, d.x0:d.x1] = locals_[t.id][s.y0:s.y1, s.x0:s.x1]
+    return out
+
+
+def _blk(m, r):
+    return m[r.y0:r.y1, r.x0:r.x1]
+
+
+def linear_strength(direction, y, x, rows, cols):
+    """micro_gradient_exchange.cpp:56-64."""
+    if direction == LEFT:
+        return 1.0 if cols == 1 else 1.0 - x / (cols - 1)
+    if direction == RIGHT:
+        return 1.0 if cols == 1 else x / (cols - 1)
+    if direction == TOP:
+        return 1.0 if rows == 1 else 1.0 - y / (rows - 1)
+    return 1.0 if rows == 1 else y / (rows - 1)
+
+
+@dataclasses.dataclass
+class ExchangeOptions:
+    """MicroGradientOptions (include/utils/micro_gradient_exchange.h:19-40), PE types."""
+    loss_type: str = "PE"            # "PE" or "PEPenalty"
+    loss_region: str = "Core"        # "Core" or "CoreGuard"
+    pe_weight: float = 1.0
+    penalty_weight: float = 2.0
+    penalty_threshold: float = 0.01
+    enable_cept: bool = False
+    cept_guard_only: bool = False
+    cept_weight: float = 1.1
+    enable_grad_fusion: bool = False
+    fusion_mode: str = "Average"     # "Average" or "Linear"
+    fusion_weight_owner: float = 0.5
+    fusion_weight_neighbor: float = 0.5
+
+
+def loss_windows(local_target, region, opt):
+    """build_micro_loss_windows (micro_gradient_exchange.cpp:65-93), PE / PEPenalty."""
+    pe = np.zeros_like(local_target)
+    pen = np.zeros_like(local_target)
+    sl = (slice(region.y0, region.y1), slice(region.x0, region.x1))
+    pen[sl] = (local_target[sl] < 0.5)
+    pe[sl] = (local_target[sl] > 0.5) if opt.loss_type == "PEPenalty" else 1.0
+    return pe, pen
+
+
+def exchange(local_masks, global_target, meta, cache, thr, alpha, opt: ExchangeOptions):
+    """MicroGradientExchange::compute (micro_gradient_exchange.cpp:134-334) for PE types."""
+    wpe = opt.pe_weight
+    wpen = opt.penalty_weight if opt.loss_type == "PEPenalty" else 0.0
+    locals_ = []
+    for t in meta.tiles:
+        m = local_masks[t.id]
+        tgt = extract_local_tile(global_target, t)
+        _, wafer, E = io.imaging_compute(m, cache, thr, alpha)
+        region = t.update_local if opt.loss_region == "CoreGuard" else t.core_local
+        pe_w, pen_w = loss_windows(tgt, region, opt)
+        pe_loss = io.pe_loss(_blk(wafer, region), _blk(tgt, region), _blk(pe_w, region))
+        bg = io.background_penalty_loss(_blk(wafer, region), _blk(tgt, region),
+                                        opt.penalty_threshold, _blk(pen_w, region)) \
+            if opt.loss_type == "PEPenalty" else 0.0
+        if wpen != 0.0:
+            raw = io.pe_gradient(wafer, tgt, E, cache, alpha, pe_window=pe_w, pe_weight=wpe,
+                                 penalty=wpen, penalty_threshold=opt.penalty_threshold,
+                                 penalty_window=pen_w)
+        elif wpe != 0.0:
+            raw = wpe * io.pe_gradient(wafer, tgt, E, cache, alpha, pe_window=pe_w)
+        else:
+            raw = np.zeros_like(m)
+        data = wpe * pe_loss + wpen * bg
+        locals_.append(dict(pe_loss=pe_loss, bg_penalty_raw=bg, data_loss=data, loss=data,
+                            raw=raw, grad=raw.copy(), cept_loss=0.0,
+                            cept_grad=np.zeros_like(m)))
+    for t in meta.tiles:
+        L = locals_[t.id]
+        for nb in t.neighbors:
+            B = locals_[nb.id]
+            g_src = nb.neighbor_overlap_local
+            recv_guard = _blk(B["raw"], g_src)
+            guard = nb.my_guard_local
+            if opt.enable_cept:
+                diff = _blk(local_masks[t.id], guard) - _blk(local_masks[nb.id], g_src)
+                L["cept_loss"] += float(np.sum(diff * diff))
+                L["cept_grad"][guard.y0:guard.y1, guard.x0:guard.x1] += 2.0 * diff
+                if not opt.cept_guard_only:
+                    ov = nb.my_overlap_local
+                    d2 = _blk(local_masks[t.id], ov) - _blk(local_masks[nb.id], nb.neighbor_guard_local)
+                    L["cept_grad"][ov.y0:ov.y1, ov.x0:ov.x1] += 2.0 * d2
+            if opt.enable_grad_fusion:
+                for y in range(guard.rows):
+                    for x in range(guard.cols):
+                        s = 1.0 if opt.fusion_mode == "Average" else \
+                            linear_strength(nb.direction, y, x, guard.rows, guard.cols)
+                        wn = opt.fusion_weight_neighbor * s
+                        if wn == 0.0:
+                            continue
+                        lv = L["raw"][guard.y0 + y, guard.x0 + x]
+                        L["grad"][guard.y0 + y, guard.x0 + x] = \
+                            (opt.fusion_weight_owner * lv + wn * recv_guard[y, x]) / \
+                            (opt.fusion_weight_owner + wn)
+        if opt.enable_cept:
+            L["grad"] = L["grad"] + opt.cept_weight * L["cept_grad"]
+            L["loss"] = L["loss"] + opt.cept_weight * L["cept_loss"]
+    total = sum(l["loss"] for l in locals_)
+    data = sum(l["data_loss"] for l in locals_)
+    cept = sum(l["cept_loss"] for l in locals_)
+    return dict(locals=locals_, loss=total, data_loss=data, cept_loss=cept)
+
+
+def full_chip_ctm(initial_pattern, global_target, meta, cache, thr, alpha, opt, iterations,
+                  learning_rate):
+    """FullChipCTMOptimizer::optimize (source/optimizer/full_chip_ctm.cpp:25-152), CEPT guard-only."""
+    opt = dataclasses.replace(opt, cept_guard_only=True)
+    theta_g = io.initialize_theta(initial_pattern)
+    thetas = [extract_local_tile(theta_g, t) for t in meta.tiles]
+    masks = [io.theta_to_mask(th) for th in thetas]
+    ev = exchange(masks, global_target, meta, cache, thr, alpha, opt)
+    history = [ev["loss"]]
+    best = dict(loss=ev["loss"], iteration=0, masks=[m.copy() for m in masks])
+    for it in range(1, iterations + 1):
+        for t in meta.tiles:
+            w = t.update_local
+            th = thetas[t.id]
+            g = ev["locals"][t.id]["grad"][w.y0:w.y1, w.x0:w.x1]
+            gt = -0.5 * g * np.sin(th[w.y0:w.y1, w.x0:w.x1])
+            th[w.y0:w.y1, w.x0:w.x1] -= learning_rate * gt
+            masks[t.id] = io.theta_to_mask(th)
+        ev = exchange(masks, global_target, meta, cache, thr, alpha, opt)
+        history.append(ev["loss"])
+        if ev["loss"] < best["loss"]:
+            best = dict(loss=ev["loss"], iteration=it, masks=[m.copy() for m in masks])
+    return dict(history=history, best=best, global_mask=assemble_global(best["masks"], meta),
+                thetas=thetas)
