@@ -17,6 +17,9 @@ reference (C++)              here
 ``LevelSetUtils::*``         :class:`LevelSetUtils`
 ``CTM_Optimizer``            :class:`CTMOptimizer`
 ``LSM_Optimizer``            :class:`LSMOptimizer`
+``Partition``                :class:`fullchip.Partition`
+``MicroGradientExchange``    :class:`fullchip.MicroGradientExchange`
+``FullChipCTMOptimizer``     :class:`fullchip.FullChipCTMOptimizer`
 ===========================  =================================================
 
 Images are float32 CUDA tensors (row = y, col = x). PyTorch provides device
@@ -59,6 +62,15 @@ class PeOptions(ctypes.Structure):
                 ("penalty", _D), ("penalty_threshold", _D)]
 
 
+class ExchangeOptionsC(ctypes.Structure):
+    """litho_exchange_options (include/litho_b200.h)."""
+    _fields_ = [("loss_type", _I), ("loss_region", _I), ("pe_weight", _D),
+                ("penalty_weight", _D), ("penalty_threshold", _D), ("enable_cept", _I),
+                ("cept_guard_only", _I), ("cept_weight", _D), ("enable_grad_fusion", _I),
+                ("fusion_mode", _I), ("fusion_weight_owner", _D),
+                ("fusion_weight_neighbor", _D)]
+
+
 SIGNATURES = {
     "litho_version": (_I, []),
     "litho_status_string": (ctypes.c_char_p, [_I]),
@@ -88,6 +100,15 @@ SIGNATURES = {
     "litho_evolution_term": (_I, [_P, _I, _I, _P, _P, _D, _D, _D, _D, _P, _PD]),
     "litho_lsm_rk2_update": (_I, [_P, _I, _I, _P, _P, _D, _D, _D, _D, _P, _P, _PD]),
     "litho_reinit_sdf": (_I, [_P, _I, _I, _P, _D, _D, _P, _P]),
+    "litho_partition_create": (_I, [_P, _I, _I, _I, _I, _I, _I, _PP]),
+    "litho_partition_destroy": (_I, [_P]),
+    "litho_partition_info": (_I, [_P, _PI, _PI]),
+    "litho_partition_tile_rects": (_I, [_P, _I, _PI]),
+    "litho_partition_extract": (_I, [_P, _P, _P, _P]),
+    "litho_partition_assemble": (_I, [_P, _P, _P, _P]),
+    "litho_exchange_compute": (_I, [_P, _P, _P, _P, _P, _D, _D,
+                                    ctypes.POINTER(ExchangeOptionsC), _P, _P, _PD, _PD]),
+    "litho_fullchip_theta_step": (_I, [_P, _P, _P, _P, _D, _P]),
 }
 
 

@@ -1050,3 +1050,323 @@ int litho_lsm_rk2_update(litho_ctx* ctx, int rows, int cols, const float* d_phi,
 }
 
 }  // extern "C"
+
+// ============================================================== full chip
+struct litho_partition {
+  int device = 0;
+  int height = 0, width = 0, grid_rows = 0, grid_cols = 0, halo = 0, guard = 0;
+  int ts = 0, ntiles = 0;
+  static constexpr int kMaxRel = 4;
+  std::vector<int> rects;  // 16 per tile: core_global, tile_global, core_local, update_local
+  // Device metadata: origins (2/tile) | core_global | core_local | update_local (4/tile
+  // each) | neighbour count (1/tile) | relations (kMaxRel * FC_REL_INTS per tile).
+  int* d_meta = nullptr;
+  size_t off_origin = 0, off_core_g = 0, off_core_l = 0, off_update = 0, off_nrel = 0, off_rel = 0;
+  // Exchange work, allocated on first use: targets | pe windows | penalty windows |
+  // raw gradients (ntiles * ts * ts floats each), the imaging field, loss sums.
+  float* d_work = nullptr;
+  float2* fe = nullptr;
+  float2* fm = nullptr;
+  size_t fe_n = 0, fm_n = 0;
+  double* d_loss = nullptr;  // 2 per tile (PE, background penalty) then 1 per tile (CEPT)
+  std::vector<double> h_loss;
+};
+
+namespace {
+
+struct IRect {
+  int y0, y1, x0, x1;
+};
+IRect irect_intersect(IRect a, IRect b) {
+  return {std::max(a.y0, b.y0), std::min(a.y1, b.y1), std::max(a.x0, b.x0), std::min(a.x1, b.x1)};
+}
+IRect irect_grow(IRect a, int w) { return {a.y0 - w, a.y1 + w, a.x0 - w, a.x1 + w}; }
+IRect irect_shift(IRect a, int dy, int dx) { return {a.y0 + dy, a.y1 + dy, a.x0 + dx, a.x1 + dx}; }
+void put(std::vector<int>& v, size_t at, IRect r) {
+  v[at] = r.y0; v[at + 1] = r.y1; v[at + 2] = r.x0; v[at + 3] = r.x1;
+}
+
+void free_partition(litho_partition* p) {
+  cudaSetDevice(p->device);
+  if (p->d_meta) cudaFree(p->d_meta);
+  if (p->d_work) cudaFree(p->d_work);
+  if (p->fe) cudaFree(p->fe);
+  if (p->fm) cudaFree(p->fm);
+  if (p->d_loss) cudaFree(p->d_loss);
+}
+
+}  // namespace
+
+extern "C" {
+
+int litho_partition_create(litho_ctx* ctx, int height, int width, int grid_rows, int grid_cols,
+                           int halo, int guard, litho_partition** out) {
+  if (!ctx || !out) return LITHO_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  if (height <= 0 || width <= 0 || grid_rows <= 0 || grid_cols <= 0 || grid_rows > height ||
+      grid_cols > width || halo < 0 || guard < 0)
+    return ctx->fail(LITHO_ERR_INVALID_ARGUMENT, "Partition: invalid layout or grid size");
+  if (guard > halo)
+    return ctx->fail(LITHO_ERR_INVALID_ARGUMENT, "Partition: guard must not exceed halo");
+  auto* p = new (std::nothrow) litho_partition();
+  if (!p) return ctx->fail(LITHO_ERR_OOM, "host allocation failed");
+  p->device = ctx->device;
+  p->height = height; p->width = width; p->grid_rows = grid_rows; p->grid_cols = grid_cols;
+  p->halo = halo; p->guard = guard;
+  // Partition::build (partition.cpp:21-80): Core boundaries at i * extent / count, one
+  // square tile size = largest Core side + 2 halo, rounded up to even.
+  const int max_r = (height + grid_rows - 1) / grid_rows;
+  const int max_c = (width + grid_cols - 1) / grid_cols;
+  int ts = std::max(max_r, max_c) + 2 * halo;
+  ts += ts % 2;
+  p->ts = ts;
+  const int n = grid_rows * grid_cols;
+  p->ntiles = n;
+  std::vector<IRect> core(n), tile(n);
+  for (int r = 0; r < grid_rows; ++r)
+    for (int c = 0; c < grid_cols; ++c) {
+      const int id = r * grid_cols + c;
+      core[id] = {(int)((long long)r * height / grid_rows), (int)((long long)(r + 1) * height / grid_rows),
+                  (int)((long long)c * width / grid_cols), (int)((long long)(c + 1) * width / grid_cols)};
+      tile[id] = {core[id].y0 - halo, core[id].y0 - halo + ts, core[id].x0 - halo,
+                  core[id].x0 - halo + ts};
+    }
+  const int R = litho_partition::kMaxRel;
+  p->off_origin = 0;
+  p->off_core_g = 2 * (size_t)n;
+  p->off_core_l = p->off_core_g + 4 * (size_t)n;
+  p->off_update = p->off_core_l + 4 * (size_t)n;
+  p->off_nrel = p->off_update + 4 * (size_t)n;
+  p->off_rel = p->off_nrel + (size_t)n;
+  std::vector<int> meta(p->off_rel + (size_t)n * R * FC_REL_INTS, 0);
+  p->rects.assign(16 * (size_t)n, 0);
+  const int dirs[4][3] = {{0, -1, 0}, {0, 1, 1}, {-1, 0, 2}, {1, 0, 3}};  // left, right, top, bottom
+  for (int id = 0; id < n; ++id) {
+    const int r = id / grid_cols, c = id % grid_cols;
+    const IRect cl = irect_shift(core[id], -tile[id].y0, -tile[id].x0);
+    const IRect up = irect_grow(cl, guard);
+    put(p->rects, 16 * (size_t)id, core[id]);
+    put(p->rects, 16 * (size_t)id + 4, tile[id]);
+    put(p->rects, 16 * (size_t)id + 8, cl);
+    put(p->rects, 16 * (size_t)id + 12, up);
+    meta[p->off_origin + 2 * id] = tile[id].y0;
+    meta[p->off_origin + 2 * id + 1] = tile[id].x0;
+    put(meta, p->off_core_g + 4 * (size_t)id, core[id]);
+    put(meta, p->off_core_l + 4 * (size_t)id, cl);
+    put(meta, p->off_update + 4 * (size_t)id, up);
+    int k = 0;
+    for (const auto& d : dirs) {
+      const int rr = r + d[0], cc = c + d[1];
+      if (rr < 0 || rr >= grid_rows || cc < 0 || cc >= grid_cols) continue;
+      const int nb = rr * grid_cols + cc;
+      const IRect gg = irect_intersect(irect_grow(core[id], guard), core[nb]);
+      const IRect og = irect_intersect(core[id], irect_grow(core[nb], guard));
+      const size_t at = p->off_rel + ((size_t)id * R + k) * FC_REL_INTS;
+      meta[at] = nb;
+      meta[at + 1] = d[2];
+      put(meta, at + 2, irect_shift(gg, -tile[id].y0, -tile[id].x0));
+      put(meta, at + 6, irect_shift(gg, -tile[nb].y0, -tile[nb].x0));
+      put(meta, at + 10, irect_shift(og, -tile[id].y0, -tile[id].x0));
+      put(meta, at + 14, irect_shift(og, -tile[nb].y0, -tile[nb].x0));
+      ++k;
+    }
+    meta[p->off_nrel + id] = k;
+  }
+  if (cudaSetDevice(ctx->device) != cudaSuccess) {
+    delete p;
+    return ctx->fail(LITHO_ERR_CUDA, "cudaSetDevice");
+  }
+  int st = upload(ctx, &p->d_meta, meta);
+  if (st) {
+    free_partition(p);
+    delete p;
+    return st;
+  }
+  *out = p;
+  return LITHO_OK;
+}
+
+int litho_partition_destroy(litho_partition* p) {
+  if (!p) return LITHO_OK;
+  free_partition(p);
+  delete p;
+  return LITHO_OK;
+}
+
+int litho_partition_info(const litho_partition* p, int* num_tiles, int* tile_size) {
+  if (!p) return LITHO_ERR_INVALID_ARGUMENT;
+  if (num_tiles) *num_tiles = p->ntiles;
+  if (tile_size) *tile_size = p->ts;
+  return LITHO_OK;
+}
+
+int litho_partition_tile_rects(const litho_partition* p, int tile, int* rects) {
+  if (!p || !rects || tile < 0 || tile >= p->ntiles) return LITHO_ERR_INVALID_ARGUMENT;
+  std::memcpy(rects, p->rects.data() + 16 * (size_t)tile, 16 * sizeof(int));
+  return LITHO_OK;
+}
+
+int litho_partition_extract(litho_ctx* ctx, const litho_partition* p, const float* d_global,
+                            float* d_tiles) {
+  if (!ctx || !p || !d_global || !d_tiles) return LITHO_ERR_INVALID_ARGUMENT;
+  if (cudaSetDevice(ctx->device) != cudaSuccess) return ctx->fail(LITHO_ERR_CUDA, "cudaSetDevice");
+  ctx->launches += 1;
+  return check_launch(ctx, launch_tiles_extract(ctx->stream, d_global, p->height, p->width,
+                                                p->ntiles, p->d_meta + p->off_origin, p->ts,
+                                                d_tiles),
+                      "tile extraction");
+}
+
+int litho_partition_assemble(litho_ctx* ctx, const litho_partition* p, const float* d_tiles,
+                             float* d_global) {
+  if (!ctx || !p || !d_global || !d_tiles) return LITHO_ERR_INVALID_ARGUMENT;
+  if (cudaSetDevice(ctx->device) != cudaSuccess) return ctx->fail(LITHO_ERR_CUDA, "cudaSetDevice");
+  ctx->launches += 1;
+  return check_launch(ctx, launch_tiles_assemble(ctx->stream, d_tiles, p->ntiles, p->ts,
+                                                 p->d_meta + p->off_core_g,
+                                                 p->d_meta + p->off_core_l, p->width, d_global),
+                      "tile assembly");
+}
+
+int litho_exchange_compute(litho_ctx* ctx, const litho_partition* cp, const litho_cache* cache,
+                           const float* d_masks, const float* d_global_target, double threshold,
+                           double alpha, const litho_exchange_options* opt, float* d_raw,
+                           float* d_grad, double* tile_losses, double* totals) {
+  if (!ctx || !cp || !cache || !d_masks || !d_global_target || !d_grad)
+    return LITHO_ERR_INVALID_ARGUMENT;
+  auto* p = const_cast<litho_partition*>(cp);  // owns mutable work buffers only
+  litho_exchange_options o{LITHO_MICRO_LOSS_PE, LITHO_MICRO_REGION_CORE, 1.0, 2.0, 0.01, 0, 0,
+                           1.1, 0, LITHO_FUSION_AVERAGE, 0.5, 0.5};
+  if (opt) o = *opt;
+  if ((o.loss_type != LITHO_MICRO_LOSS_PE && o.loss_type != LITHO_MICRO_LOSS_PE_PENALTY) ||
+      (o.loss_region != LITHO_MICRO_REGION_CORE && o.loss_region != LITHO_MICRO_REGION_CORE_GUARD) ||
+      (o.fusion_mode != LITHO_FUSION_AVERAGE && o.fusion_mode != LITHO_FUSION_LINEAR))
+    return ctx->fail(LITHO_ERR_UNSUPPORTED, "MicroGradientOptions: unsupported loss type, region or fusion mode");
+  const double w8[] = {o.pe_weight, o.penalty_weight, o.penalty_threshold, o.cept_weight,
+                       o.fusion_weight_owner, o.fusion_weight_neighbor, threshold, alpha};
+  if (!finite_all(w8, 8))
+    return ctx->fail(LITHO_ERR_NONFINITE, "MicroGradientOptions: weights must be finite");
+  if (o.enable_grad_fusion && (o.fusion_weight_owner < 0.0 || o.fusion_weight_neighbor < 0.0 ||
+                               o.fusion_weight_owner + o.fusion_weight_neighbor <= 0.0))
+    return ctx->fail(LITHO_ERR_INVALID_ARGUMENT,
+                     "MicroGradientOptions: fusion weights must be non-negative with a positive sum");
+  if (cache->g.N != p->ts)
+    return ctx->fail(LITHO_ERR_SHAPE, "MicroGradientExchange: cache N must equal the tile size");
+  if (d_raw && d_raw == d_grad)
+    return ctx->fail(LITHO_ERR_INVALID_ARGUMENT, "raw and exchanged gradients must not alias");
+  Layout L;
+  int st = prepare(ctx, *cache, &L);
+  if (st) return st;
+  const int n = p->ntiles;
+  const size_t tt = (size_t)p->ts * p->ts;
+  if (!p->d_work) {
+    if (cudaMalloc(&p->d_work, 4 * n * tt * sizeof(float)) != cudaSuccess ||
+        cudaMalloc(&p->d_loss, 3 * (size_t)n * sizeof(double)) != cudaSuccess) {
+      cudaGetLastError();
+      return ctx->fail(LITHO_ERR_OOM, "full-chip work allocation failed");
+    }
+    p->h_loss.assign(3 * (size_t)n, 0.0);
+  }
+  const BandGeom& g = cache->g;
+  const size_t fe_n = (size_t)g.K * g.Pr * g.Pc, fm_n = (size_t)g.Nr * g.Nc;
+  if (p->fe_n < fe_n || p->fm_n < fm_n) {
+    LITHO_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    if (p->fe) cudaFree(p->fe);
+    if (p->fm) cudaFree(p->fm);
+    p->fe = nullptr; p->fm = nullptr; p->fe_n = p->fm_n = 0;
+    if (cudaMalloc(&p->fe, fe_n * sizeof(float2)) != cudaSuccess ||
+        cudaMalloc(&p->fm, fm_n * sizeof(float2)) != cudaSuccess) {
+      cudaGetLastError();
+      return ctx->fail(LITHO_ERR_OOM, "full-chip field allocation failed");
+    }
+    p->fe_n = fe_n; p->fm_n = fm_n;
+  }
+  float* targets = p->d_work;
+  float* pe_w = targets + n * tt;
+  float* pen_w = pe_w + n * tt;
+  float* raw = d_raw ? d_raw : pen_w + n * tt;
+  Field f;
+  f.cache = cache; f.e = p->fe; f.mband = p->fm;
+  cudaStream_t s = ctx->stream;
+  st = check_launch(ctx, launch_tiles_extract(s, d_global_target, p->height, p->width, n,
+                                              p->d_meta + p->off_origin, p->ts, targets),
+                    "target extraction");
+  if (!st)
+    st = check_launch(ctx, launch_loss_windows(
+                               s, targets, n, p->ts,
+                               p->d_meta + (o.loss_region == LITHO_MICRO_REGION_CORE_GUARD
+                                                ? p->off_update : p->off_core_l),
+                               o.loss_type == LITHO_MICRO_LOSS_PE_PENALTY, pe_w, pen_w),
+                      "loss windows");
+  ctx->launches += 2;
+  // micro_loss_weights (micro_gradient_exchange.cpp:95-99): the penalty term only for PEPenalty.
+  const double wpe = o.pe_weight;
+  const double wpen = o.loss_type == LITHO_MICRO_LOSS_PE_PENALTY ? o.penalty_weight : 0.0;
+  for (int t = 0; t < n && !st; ++t) {
+    ResistEpilogue ep{};
+    ep.mode = 1;
+    ep.thr = (float)threshold;
+    ep.alpha = (float)alpha;
+    ep.target = targets + t * tt;
+    ep.pe_window = pe_w + t * tt;
+    ep.pen_window = pen_w + t * tt;
+    ep.pe_weight = (float)wpe;
+    ep.penalty = (float)wpen;
+    ep.pen_thr = (float)o.penalty_threshold;
+    ep.dldi = at<float>(ctx, L.dldi);
+    ep.loss_partial = ctx->d_red + RED_PART;
+    int nb = 0;
+    st = run_forward(ctx, *cache, f, L, 0, d_masks + t * tt, nullptr, ep, &nb);
+    if (!st)
+      st = check_launch(ctx, launch_sum_partials(s, ctx->d_red + RED_PART, nb, 2, p->d_loss + 2 * t),
+                        "sum");
+    ctx->launches += 1;
+    GradEpilogue gp{};
+    gp.grad_mask = raw + t * tt;
+    int nb2 = 0;
+    if (!st) st = run_adjoint(ctx, *cache, f, L, at<float>(ctx, L.dldi), 4.0 * alpha, gp, &nb2);
+  }
+  if (!st)
+    LITHO_CUDA_TRY(ctx, cudaMemcpyAsync(d_grad, raw, n * tt * sizeof(float),
+                                        cudaMemcpyDeviceToDevice, s));
+  if (!st)
+    st = check_launch(ctx, launch_exchange(s, d_masks, raw, n, p->ts, p->d_meta + p->off_nrel,
+                                           p->d_meta + p->off_rel, litho_partition::kMaxRel, o,
+                                           d_grad, p->d_loss + 2 * n),
+                      "micro-gradient exchange");
+  ctx->launches += 1;
+  if (!st)
+    LITHO_CUDA_TRY(ctx, cudaMemcpyAsync(p->h_loss.data(), p->d_loss, 3 * n * sizeof(double),
+                                        cudaMemcpyDeviceToHost, s));
+  if (!st) st = fetch(ctx, 0);
+  if (st) return st;
+  if (flag_set(ctx)) return ctx->fail(LITHO_ERR_NONFINITE, "Imaging: mask, threshold, and alpha must be finite");
+  double tot[3] = {0.0, 0.0, 0.0};
+  for (int t = 0; t < n; ++t) {
+    const double pe = p->h_loss[2 * t], bg = p->h_loss[2 * t + 1], cept = p->h_loss[2 * n + t];
+    const double data = wpe * pe + wpen * bg;
+    const double loss = data + (o.enable_cept ? o.cept_weight * cept : 0.0);
+    if (tile_losses) {
+      double* r = tile_losses + 5 * (size_t)t;
+      r[0] = pe; r[1] = wpen != 0.0 ? bg : 0.0; r[2] = data; r[3] = cept; r[4] = loss;
+    }
+    tot[0] += loss; tot[1] += data; tot[2] += cept;
+  }
+  if (totals) std::memcpy(totals, tot, sizeof(tot));
+  return LITHO_OK;
+}
+
+int litho_fullchip_theta_step(litho_ctx* ctx, const litho_partition* p, float* d_theta,
+                              const float* d_grad, double learning_rate, float* d_masks) {
+  if (!ctx || !p || !d_theta || !d_masks) return LITHO_ERR_INVALID_ARGUMENT;
+  if (!std::isfinite(learning_rate))
+    return ctx->fail(LITHO_ERR_NONFINITE, "learning rate must be finite");
+  if (cudaSetDevice(ctx->device) != cudaSuccess) return ctx->fail(LITHO_ERR_CUDA, "cudaSetDevice");
+  ctx->launches += 1;
+  return check_launch(ctx, launch_theta_update(ctx->stream, d_theta, d_grad, p->ntiles, p->ts,
+                                               p->d_meta + p->off_update, (float)learning_rate,
+                                               d_masks),
+                      "theta update");
+}
+
+}  // extern "C"

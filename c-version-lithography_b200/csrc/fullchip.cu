@@ -1,0 +1,198 @@
+// Full-chip micro-tile kernels: periodic Halo extraction and Core assembly
+// (source/utils/partition.cpp:83-113), the neighbour exchange of
+// MicroGradientExchange::compute phase two (source/utils/micro_gradient_exchange.cpp:253-326:
+// CEPT against the frozen neighbour Core, optional two-sided CEPT, Average or
+// Linear guard-gradient fusion) and the windowed CTM theta update of
+// FullChipCTMOptimizer (source/optimizer/full_chip_ctm.cpp:127-147).
+//
+// All tiles of a partition share one tile size ts and live contiguously as
+// [tile][ts][ts] float32 arrays.
+#include <cuda_runtime.h>
+
+#include "device_common.cuh"
+
+namespace litho_b200 {
+
+// out[t][y][x] = global[(oy_t + y) mod H][(ox_t + x) mod W]
+__global__ void tiles_extract_kernel(const float* __restrict__ g, int H, int W,
+                                     const int* __restrict__ origins, int ts,
+                                     float* __restrict__ out) {
+  const int t = blockIdx.y;
+  const int oy = origins[2 * t], ox = origins[2 * t + 1];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ts * ts; i += gridDim.x * blockDim.x) {
+    const int y = i / ts, x = i % ts;
+    const int gy = ((oy + y) % H + H) % H, gx = ((ox + x) % W + W) % W;
+    out[(size_t)t * ts * ts + i] = g[(size_t)gy * W + gx];
+  }
+}
+
+cudaError_t launch_tiles_extract(cudaStream_t s, const float* g, int H, int W, int ntiles,
+                                 const int* origins, int ts, float* out) {
+  dim3 grid((ts * ts + 255) / 256 < 64 ? (ts * ts + 255) / 256 : 64, ntiles);
+  tiles_extract_kernel<<<grid, 256, 0, s>>>(g, H, W, origins, ts, out);
+  return cudaGetLastError();
+}
+
+// global[core_global] = local[core_local]; rects as (y0, y1, x0, x1).
+__global__ void tiles_assemble_kernel(const float* __restrict__ loc, int ts,
+                                      const int* __restrict__ core_g,
+                                      const int* __restrict__ core_l, int W,
+                                      float* __restrict__ g) {
+  const int t = blockIdx.y;
+  const int gy0 = core_g[4 * t], gx0 = core_g[4 * t + 2];
+  const int rows = core_g[4 * t + 1] - gy0, cols = core_g[4 * t + 3] - gx0;
+  const int ly0 = core_l[4 * t], lx0 = core_l[4 * t + 2];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < rows * cols; i += gridDim.x * blockDim.x) {
+    const int y = i / cols, x = i % cols;
+    g[(size_t)(gy0 + y) * W + gx0 + x] = loc[((size_t)t * ts + ly0 + y) * ts + lx0 + x];
+  }
+}
+
+cudaError_t launch_tiles_assemble(cudaStream_t s, const float* loc, int ntiles, int ts,
+                                  const int* core_g, const int* core_l, int W, float* g) {
+  dim3 grid(64, ntiles);
+  tiles_assemble_kernel<<<grid, 256, 0, s>>>(loc, ts, core_g, core_l, W, g);
+  return cudaGetLastError();
+}
+
+// build_micro_loss_windows (micro_gradient_exchange.cpp:65-93) for the PE types, every
+// tile at once: inside the tile's loss region pe = 1 (PE) or [T > 0.5] (PEPenalty) and
+// pen = [T < 0.5]; both are 0 outside it.
+__global__ void loss_windows_kernel(const float* __restrict__ target, int ts,
+                                    const int* __restrict__ region, int pe_from_target,
+                                    float* __restrict__ pe_w, float* __restrict__ pen_w) {
+  const int t = blockIdx.y;
+  const int y0 = region[4 * t], y1 = region[4 * t + 1], x0 = region[4 * t + 2],
+            x1 = region[4 * t + 3];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ts * ts; i += gridDim.x * blockDim.x) {
+    const int y = i / ts, x = i % ts;
+    const size_t k = (size_t)t * ts * ts + i;
+    const bool in = y >= y0 && y < y1 && x >= x0 && x < x1;
+    const float T = target[k];
+    pe_w[k] = in ? (pe_from_target ? (T > 0.5f ? 1.f : 0.f) : 1.f) : 0.f;
+    pen_w[k] = in && T < 0.5f ? 1.f : 0.f;
+  }
+}
+
+cudaError_t launch_loss_windows(cudaStream_t s, const float* target, int ntiles, int ts,
+                                const int* region, int pe_from_target, float* pe_w,
+                                float* pen_w) {
+  dim3 grid((ts * ts + 255) / 256 < 128 ? (ts * ts + 255) / 256 : 128, ntiles);
+  loss_windows_kernel<<<grid, 256, 0, s>>>(target, ts, region, pe_from_target, pe_w, pen_w);
+  return cudaGetLastError();
+}
+
+// Neighbour relations of one tile come in the reference's order (left, right,
+// top, bottom; absent neighbours omitted).
+constexpr int REL_INTS = FC_REL_INTS;
+constexpr int EX_NT = 256;
+
+__device__ __forceinline__ float linear_strength(int dir, int y, int x, int rows, int cols) {
+  switch (dir) {
+    case 0: return cols == 1 ? 1.f : 1.f - (float)x / (float)(cols - 1);   // left
+    case 1: return cols == 1 ? 1.f : (float)x / (float)(cols - 1);         // right
+    case 2: return rows == 1 ? 1.f : 1.f - (float)y / (float)(rows - 1);   // top
+    default: return rows == 1 ? 1.f : (float)y / (float)(rows - 1);        // bottom
+  }
+}
+
+// One CTA per tile, over the guard strips only: grad holds a copy of raw on entry
+// and leaves as raw (fused on guards) + cept_weight * cept_grad; cept_loss[t] = sum
+// over neighbours of sum (A guard mask - B core mask)^2. Guard strips of different
+// neighbours are disjoint; the two-sided overlaps can share corner pixels, so the
+// neighbours are taken one after another.
+__global__ void __launch_bounds__(EX_NT)
+exchange_kernel(const float* __restrict__ masks, const float* __restrict__ raw, int ts,
+                const int* __restrict__ nrel, const int* __restrict__ rel, int max_rel,
+                litho_exchange_options o, float* __restrict__ grad, double* __restrict__ cept_loss) {
+  __shared__ double sh[EX_NT / 32];
+  const int t = blockIdx.x;
+  const size_t tt = (size_t)ts * ts;
+  const float* mA = masks + t * tt;
+  const float* rA = raw + t * tt;
+  float* gA = grad + t * tt;
+  double loss = 0.0;
+  for (int j = 0; j < nrel[t]; ++j) {
+    const int* R = rel + ((size_t)t * max_rel + j) * REL_INTS;
+    const int nb = R[0], dir = R[1];
+    const int gy0 = R[2], gy1 = R[3], gx0 = R[4], gx1 = R[5];       // my guard (local A)
+    const int sy0 = R[6], sx0 = R[8];                                // neighbour overlap (local B)
+    const float* mB = masks + (size_t)nb * tt;
+    const float* rB = raw + (size_t)nb * tt;
+    const int rows = gy1 - gy0, cols = gx1 - gx0;
+    double part = 0.0;
+    for (int i = threadIdx.x; i < rows * cols; i += EX_NT) {
+      const int y = i / cols, x = i % cols;
+      const size_t ia = (size_t)(gy0 + y) * ts + gx0 + x;
+      const size_t ib = (size_t)(sy0 + y) * ts + sx0 + x;
+      float g = gA[ia];
+      if (o.enable_grad_fusion) {
+        const float s = o.fusion_mode == 0 ? 1.f : linear_strength(dir, y, x, rows, cols);
+        const float wn = (float)o.fusion_weight_neighbor * s;
+        if (wn != 0.f)
+          g = ((float)o.fusion_weight_owner * rA[ia] + wn * rB[ib]) /
+              ((float)o.fusion_weight_owner + wn);
+      }
+      if (o.enable_cept) {
+        const float d = mA[ia] - mB[ib];
+        part += (double)d * (double)d;
+        g += (float)o.cept_weight * 2.f * d;
+      }
+      gA[ia] = g;
+    }
+    loss += part;
+    __syncthreads();
+    if (o.enable_cept && !o.cept_guard_only) {
+      // The neighbour's guard over this tile's Core edge drives the Core side too.
+      const int oy0 = R[10], oy1 = R[11], ox0 = R[12], ox1 = R[13];   // my overlap (local A)
+      const int ny0 = R[14], nx0 = R[16];                              // neighbour guard (local B)
+      const int orows = oy1 - oy0, ocols = ox1 - ox0;
+      for (int i = threadIdx.x; i < orows * ocols; i += EX_NT) {
+        const int y = i / ocols, x = i % ocols;
+        const size_t ia = (size_t)(oy0 + y) * ts + ox0 + x;
+        const size_t ib = (size_t)(ny0 + y) * ts + nx0 + x;
+        gA[ia] += (float)o.cept_weight * 2.f * (mA[ia] - mB[ib]);
+      }
+      __syncthreads();
+    }
+  }
+  const double total = block_sum<EX_NT>(loss, sh);
+  if (threadIdx.x == 0) cept_loss[t] = total;
+}
+
+cudaError_t launch_exchange(cudaStream_t s, const float* masks, const float* raw, int ntiles,
+                            int ts, const int* nrel, const int* rel, int max_rel,
+                            const litho_exchange_options& o, float* grad, double* cept_loss) {
+  exchange_kernel<<<ntiles, EX_NT, 0, s>>>(masks, raw, ts, nrel, rel, max_rel, o, grad,
+                                           cept_loss);
+  return cudaGetLastError();
+}
+
+// theta -= lr * (-1/2 G sin theta) inside the update window (y0, y1, x0, x1) of each
+// tile; mask = (1 + cos theta) / 2 over the whole tile. grad == nullptr only
+// refreshes the masks.
+__global__ void theta_update_kernel(float* __restrict__ theta, const float* __restrict__ grad,
+                                    int ts, const int* __restrict__ win, float lr,
+                                    float* __restrict__ mask) {
+  const int t = blockIdx.y;
+  const int y0 = win[4 * t], y1 = win[4 * t + 1], x0 = win[4 * t + 2], x1 = win[4 * t + 3];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ts * ts; i += gridDim.x * blockDim.x) {
+    const int y = i / ts, x = i % ts;
+    const size_t k = (size_t)t * ts * ts + i;
+    float th = theta[k];
+    if (grad && y >= y0 && y < y1 && x >= x0 && x < x1) {
+      th -= lr * (-0.5f * grad[k] * sinf(th));
+      theta[k] = th;
+    }
+    mask[k] = 0.5f * (1.f + cosf(th));
+  }
+}
+
+cudaError_t launch_theta_update(cudaStream_t s, float* theta, const float* grad, int ntiles,
+                                int ts, const int* win, float lr, float* mask) {
+  dim3 grid((ts * ts + 255) / 256 < 64 ? (ts * ts + 255) / 256 : 64, ntiles);
+  theta_update_kernel<<<grid, 256, 0, s>>>(theta, grad, ts, win, lr, mask);
+  return cudaGetLastError();
+}
+
+}  // namespace litho_b200

@@ -207,4 +207,22 @@ cudaError_t launch_dt(cudaStream_t s, const float* vn, size_t n, float dx, float
 cudaError_t launch_reinit_sdf(cudaStream_t s, int rows, int cols, const float* phi, float dx,
                               float* work, float* sdf);
 
+// Full-chip micro tiles (fullchip.cu). Rects are 4 ints (y0, y1, x0, x1) per tile;
+// origins 2 ints (y, x) per tile; rel holds max_rel entries of FC_REL_INTS ints
+// per tile: {neighbour, direction, my_guard[4], neighbour_overlap[4],
+// my_overlap[4], neighbour_guard[4]}.
+constexpr int FC_REL_INTS = 18;
+cudaError_t launch_tiles_extract(cudaStream_t s, const float* g, int H, int W, int ntiles,
+                                 const int* origins, int ts, float* out);
+cudaError_t launch_tiles_assemble(cudaStream_t s, const float* loc, int ntiles, int ts,
+                                  const int* core_g, const int* core_l, int W, float* g);
+cudaError_t launch_loss_windows(cudaStream_t s, const float* target, int ntiles, int ts,
+                                const int* region, int pe_from_target, float* pe_w,
+                                float* pen_w);
+cudaError_t launch_exchange(cudaStream_t s, const float* masks, const float* raw, int ntiles,
+                            int ts, const int* nrel, const int* rel, int max_rel,
+                            const litho_exchange_options& o, float* grad, double* cept_loss);
+cudaError_t launch_theta_update(cudaStream_t s, float* theta, const float* grad, int ntiles,
+                                int ts, const int* win, float lr, float* mask);
+
 }  // namespace litho_b200

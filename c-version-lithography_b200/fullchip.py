@@ -1,0 +1,309 @@
+"""Full-chip micro-tile optimisation over the C ABI.
+
+Mirrors the reference's full-chip classes:
+
+* :class:`Partition` - ``Partition`` / ``PartitionMeta`` (include/utils/partition.h,
+  source/utils/partition.cpp:21-120): Cores, Halo tiles with periodic wrap,
+  Core + Guard update windows, four-neighbour relations.
+* :class:`MicroGradientExchange` - ``MicroGradientExchange::compute``
+  (source/utils/micro_gradient_exchange.cpp:134-334) for the PE and PEPenalty
+  loss types: per-tile imaging and windowed data loss, raw mask gradients,
+  CEPT against the neighbours' Cores and Average / Linear guard fusion.
+* :class:`FullChipCTMOptimizer` - ``FullChipCTMOptimizer::optimize``
+  (source/optimizer/full_chip_ctm.cpp:25-152): fixed-step theta descent inside
+  each tile's Core + Guard window, best state over all evaluations.
+
+Local tiles are one float32 CUDA tensor of shape (num_tiles, tile_size,
+tile_size), tile id = row * grid_cols + col. Every computation runs in the
+library's kernels; there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+from dataclasses import dataclass, field
+from typing import List, Optional
+
+import numpy as np
+
+from . import (ExchangeOptionsC, ImagingCache, LithoError, _f32, _ptr, default_context)
+
+LOSS_TYPES = {"PE": 0, "PEPenalty": 1}
+LOSS_REGIONS = {"Core": 0, "CoreGuard": 1}
+FUSION_MODES = {"Average": 0, "Linear": 1}
+
+
+@dataclass
+class MicroGradientOptions:
+    """MicroGradientOptions (include/utils/micro_gradient_exchange.h:19-40), PE types."""
+    loss_type: str = "PE"
+    loss_region: str = "Core"
+    pe_weight: float = 1.0
+    penalty_weight: float = 2.0
+    penalty_threshold: float = 0.01
+    enable_cept: bool = False
+    cept_guard_only: bool = False
+    cept_weight: float = 1.1
+    enable_grad_fusion: bool = False
+    fusion_mode: str = "Average"
+    fusion_weight_owner: float = 0.5
+    fusion_weight_neighbor: float = 0.5
+
+    def to_c(self) -> ExchangeOptionsC:
+        for name, table in (("loss_type", LOSS_TYPES), ("loss_region", LOSS_REGIONS),
+                            ("fusion_mode", FUSION_MODES)):
+            if getattr(self, name) not in table:
+                raise LithoError(7, f"MicroGradientOptions.{name}={getattr(self, name)!r} is not "
+                                    f"one of {sorted(table)}")
+        return ExchangeOptionsC(
+            LOSS_TYPES[self.loss_type], LOSS_REGIONS[self.loss_region], self.pe_weight,
+            self.penalty_weight, self.penalty_threshold, int(self.enable_cept),
+            int(self.cept_guard_only), self.cept_weight, int(self.enable_grad_fusion),
+            FUSION_MODES[self.fusion_mode], self.fusion_weight_owner, self.fusion_weight_neighbor)
+
+    def weights(self):
+        """micro_loss_weights (micro_gradient_exchange.cpp:95-99): (pe, penalty)."""
+        return self.pe_weight, (self.penalty_weight if self.loss_type == "PEPenalty" else 0.0)
+
+
+@dataclass(frozen=True)
+class PartitionRect:
+    """PartitionRect: half-open [y0, y1) x [x0, x1)."""
+    y0: int
+    y1: int
+    x0: int
+    x1: int
+
+    def rows(self) -> int:
+        return self.y1 - self.y0
+
+    def cols(self) -> int:
+        return self.x1 - self.x0
+
+
+@dataclass(frozen=True)
+class PartitionTile:
+    id: int
+    row: int
+    col: int
+    core_global: PartitionRect
+    tile_global: PartitionRect
+    core_local: PartitionRect
+    update_local: PartitionRect
+
+
+class Partition:
+    """Partition::build (partition.cpp:21-80) on the device: geometry + tile copies."""
+
+    def __init__(self, height: int, width: int, grid_rows: int, grid_cols: int, halo: int,
+                 guard: int, ctx=None):
+        self.ctx = ctx or default_context()
+        lib = self.ctx.lib
+        h = ctypes.c_void_p()
+        self.ctx._check(lib.litho_partition_create(self.ctx.handle, height, width, grid_rows,
+                                                   grid_cols, halo, guard, ctypes.byref(h)))
+        self.handle = h
+        self.height, self.width = height, width
+        self.grid_rows, self.grid_cols = grid_rows, grid_cols
+        self.halo, self.guard = halo, guard
+        n, ts = ctypes.c_int(), ctypes.c_int()
+        lib.litho_partition_info(h, ctypes.byref(n), ctypes.byref(ts))
+        self.num_tiles, self.tile_size = n.value, ts.value
+        self.tiles: List[PartitionTile] = []
+        buf = (ctypes.c_int * 16)()
+        for t in range(self.num_tiles):
+            self.ctx._check(lib.litho_partition_tile_rects(h, t, buf))
+            r = [PartitionRect(*buf[4 * i:4 * i + 4]) for i in range(4)]
+            self.tiles.append(PartitionTile(t, t // grid_cols, t % grid_cols, *r))
+
+    def empty_tiles(self):
+        torch = self.ctx.torch
+        ts = self.tile_size
+        return torch.empty((self.num_tiles, ts, ts), dtype=torch.float32, device="cuda")
+
+    def extract_all(self, global_image):
+        """Partition::extract_all (partition.cpp:97-103): periodic Halo tiles."""
+        g = _f32(global_image, self.ctx.torch, (self.height, self.width), "global image")
+        out = self.empty_tiles()
+        self.ctx._check(self.ctx.lib.litho_partition_extract(self.ctx.handle, self.handle,
+                                                             _ptr(g), _ptr(out)))
+        return out
+
+    def assemble_global(self, local_tiles):
+        """Partition::assemble_global (partition.cpp:105-113): Cores only."""
+        ts = self.tile_size
+        loc = _f32(local_tiles, self.ctx.torch, (self.num_tiles, ts, ts), "local tiles")
+        out = self.ctx.torch.zeros((self.height, self.width), dtype=self.ctx.torch.float32,
+                                   device="cuda")
+        self.ctx._check(self.ctx.lib.litho_partition_assemble(self.ctx.handle, self.handle,
+                                                              _ptr(loc), _ptr(out)))
+        return out
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.ctx.lib.litho_partition_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+@dataclass
+class MicroLocalLoss:
+    pe_loss: float
+    bg_penalty_raw: float
+    penalty_loss: float
+    data_loss: float
+    cept_loss: float
+    loss: float
+
+
+@dataclass
+class MicroGradientExchangeResult:
+    """MicroGradientExchangeResult: totals, per-tile losses, gradients (device)."""
+    loss: float
+    data_loss: float
+    cept_loss: float
+    locals: List[MicroLocalLoss]
+    mask_gradients: object     # (num_tiles, ts, ts) exchanged gradients
+    raw_gradients: object      # (num_tiles, ts, ts) before CEPT and fusion
+
+
+class MicroGradientExchange:
+    """MicroGradientExchange (include/utils/micro_gradient_exchange.h:119-139)."""
+
+    def __init__(self, partition: Partition, cache: ImagingCache, threshold: float = 0.25,
+                 alpha: float = 85.0):
+        if cache.N != partition.tile_size:
+            raise LithoError(2, f"cache N {cache.N} != tile size {partition.tile_size}")
+        self.partition = partition
+        self.cache = cache
+        self.ctx = partition.ctx
+        self.threshold, self.alpha = float(threshold), float(alpha)
+        self.grad = partition.empty_tiles()
+        self.raw = partition.empty_tiles()
+
+    def compute(self, local_masks, global_target, options: Optional[MicroGradientOptions] = None):
+        """compute(local_masks, global_target, options) (micro_gradient_exchange.cpp:134-334).
+
+        The returned gradient tensors are reused by the next call."""
+        p = self.partition
+        torch = self.ctx.torch
+        opt = options or MicroGradientOptions()
+        copt = opt.to_c()
+        ts = p.tile_size
+        masks = _f32(local_masks, torch, (p.num_tiles, ts, ts), "local masks")
+        tgt = _f32(global_target, torch, (p.height, p.width), "global target")
+        per = (ctypes.c_double * (5 * p.num_tiles))()
+        tot = (ctypes.c_double * 3)()
+        self.ctx._check(self.ctx.lib.litho_exchange_compute(
+            self.ctx.handle, p.handle, self.cache.handle, _ptr(masks), _ptr(tgt),
+            self.threshold, self.alpha, ctypes.byref(copt), _ptr(self.raw), _ptr(self.grad),
+            per, tot))
+        _, wpen = opt.weights()
+        locs = [MicroLocalLoss(per[5 * t], per[5 * t + 1], wpen * per[5 * t + 1], per[5 * t + 2],
+                               per[5 * t + 3], per[5 * t + 4]) for t in range(p.num_tiles)]
+        return MicroGradientExchangeResult(tot[0], tot[1], tot[2], locs, self.grad, self.raw)
+
+
+@dataclass
+class FullChipCTMOptions:
+    """FullChipCTMOptions (include/optimizer/full_chip_ctm.h:10-17)."""
+    iterations: int = 50
+    learning_rate: float = 0.9
+    gradient_options: MicroGradientOptions = field(
+        default_factory=lambda: MicroGradientOptions(cept_guard_only=True))
+    verbose: bool = False
+    retain_final_masks: bool = False
+
+
+@dataclass
+class FullChipCTMIteration:
+    iteration: int
+    loss: float
+    data_loss: float
+    cept_loss: float
+    pe_contribution: float
+    penalty_contribution: float
+    cept_contribution: float
+    pe_loss_raw: float
+    bg_penalty_raw: float
+
+
+@dataclass
+class FullChipCTMResult:
+    best_iteration: int
+    best_loss: float
+    global_mask: object
+    local_masks: object
+    local_theta: object
+    final_local_masks: object
+    history: List[FullChipCTMIteration]
+
+
+class FullChipCTMOptimizer:
+    """FullChipCTMOptimizer (include/optimizer/full_chip_ctm.h:38-58)."""
+
+    def __init__(self, partition: Partition, cache: ImagingCache, threshold: float = 0.25,
+                 alpha: float = 85.0):
+        self.partition = partition
+        self.exchange = MicroGradientExchange(partition, cache, threshold, alpha)
+        self.ctx = partition.ctx
+
+    @staticmethod
+    def initialize_theta(pattern, torch):
+        """CTM_Optimizer::_initialize_theta (CTM_Optimizer.cpp:55-64): > 0 -> 0.3 pi, else 0.7 pi."""
+        pi = 3.14159265358979323846
+        return torch.where(pattern > 0, torch.full_like(pattern, 0.3 * pi),
+                           torch.full_like(pattern, 0.7 * pi))
+
+    def optimize(self, global_target, options: Optional[FullChipCTMOptions] = None,
+                 initial_pattern=None) -> FullChipCTMResult:
+        """optimize([initial_pattern,] global_target, options) (full_chip_ctm.cpp:25-152)."""
+        opt = options or FullChipCTMOptions()
+        if opt.iterations < 0:
+            raise LithoError(1, "FullChipCTM iterations must be non-negative")
+        if not math.isfinite(opt.learning_rate):
+            raise LithoError(3, "FullChipCTM learning_rate must be finite")
+        go = MicroGradientOptions(**{**opt.gradient_options.__dict__, "cept_guard_only": True})
+        wpe, wpen = go.weights()
+        p = self.partition
+        torch = self.ctx.torch
+        tgt = _f32(global_target, torch, (p.height, p.width), "global target")
+        init = tgt if initial_pattern is None else _f32(initial_pattern, torch,
+                                                        (p.height, p.width), "initial pattern")
+        theta = p.extract_all(self.initialize_theta(init, torch))
+        masks = p.empty_tiles()
+        lib, h = self.ctx.lib, self.ctx.handle
+        self.ctx._check(lib.litho_fullchip_theta_step(h, p.handle, _ptr(theta), None, 0.0,
+                                                      _ptr(masks)))
+        history: List[FullChipCTMIteration] = []
+        best = dict(loss=math.inf, iteration=0, masks=None, theta=None)
+
+        def record(it, ev):
+            pe = sum(wpe * l.pe_loss for l in ev.locals)
+            pen = sum(l.penalty_loss for l in ev.locals)
+            cept = go.cept_weight * ev.cept_loss if go.enable_cept else 0.0
+            history.append(FullChipCTMIteration(
+                it, ev.loss, ev.data_loss, ev.cept_loss, pe, pen, cept,
+                sum(l.pe_loss for l in ev.locals), sum(l.bg_penalty_raw for l in ev.locals)))
+            if ev.loss < best["loss"]:
+                best.update(loss=ev.loss, iteration=it, masks=masks.clone(), theta=theta.clone())
+            if opt.verbose:
+                print(f"CTM {it:>3}/{opt.iterations} data={ev.data_loss:.3f} "
+                      f"cept={ev.cept_loss:.3f} total={ev.loss:.3f}")
+
+        ev = self.exchange.compute(masks, tgt, go)
+        record(0, ev)
+        for it in range(1, opt.iterations + 1):
+            self.ctx._check(lib.litho_fullchip_theta_step(h, p.handle, _ptr(theta),
+                                                          _ptr(ev.mask_gradients),
+                                                          opt.learning_rate, _ptr(masks)))
+            ev = self.exchange.compute(masks, tgt, go)
+            record(it, ev)
+        return FullChipCTMResult(best["iteration"], best["loss"],
+                                 p.assemble_global(best["masks"]), best["masks"], best["theta"],
+                                 masks.clone() if opt.retain_final_masks else None, history)

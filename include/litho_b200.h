@@ -198,6 +198,79 @@ int litho_lsm_rk2_update(litho_ctx* ctx, int rows, int cols, const float* d_phi,
                          const float* d_vn, double dx, double dy, double cfl, double b,
                          float* d_phi_out, float* d_mask, double* dt);
 
+/* ------------------------------------------------------------ full chip
+ * Partition (include/utils/partition.h, source/utils/partition.cpp:21-120): the
+ * height x width layout is split into grid_rows x grid_cols Cores (boundaries
+ * at i * height / grid_rows); each Core grows by halo pixels into a square
+ * local tile of tile_size = max Core side + 2 halo, rounded up to even, read
+ * with periodic wrap at the layout edge. Core + guard pixels is the update
+ * window; the guard strips over the left/right/top/bottom neighbours' Cores are
+ * what the micro-gradient exchange compares and fuses.
+ * Local tiles live contiguously in device memory as [tile][tile_size][tile_size]
+ * float32, tile id = row * grid_cols + col (PartitionMeta::tiles order).
+ */
+typedef struct litho_partition litho_partition;
+int litho_partition_create(litho_ctx* ctx, int height, int width, int grid_rows, int grid_cols,
+                           int halo, int guard, litho_partition** out);
+int litho_partition_destroy(litho_partition* partition);
+int litho_partition_info(const litho_partition* partition, int* num_tiles, int* tile_size);
+/* Rectangles of one tile, each (y0, y1, x0, x1) half-open: rects[0..3]
+ * core_global, [4..7] tile_global, [8..11] core_local, [12..15] update_local
+ * (PartitionTile, include/utils/partition.h). */
+int litho_partition_tile_rects(const litho_partition* partition, int tile, int* rects);
+/* Partition::extract_all (partition.cpp:83-103): global (height x width) -> tiles. */
+int litho_partition_extract(litho_ctx* ctx, const litho_partition* partition,
+                            const float* d_global, float* d_tiles);
+/* Partition::assemble_global (partition.cpp:105-113): every tile's Core -> global. */
+int litho_partition_assemble(litho_ctx* ctx, const litho_partition* partition,
+                             const float* d_tiles, float* d_global);
+
+/* MicroGradientOptions (include/utils/micro_gradient_exchange.h:19-40) for the
+ * PE loss types; the reference's defaults are given beside each field. */
+#define LITHO_MICRO_LOSS_PE 0
+#define LITHO_MICRO_LOSS_PE_PENALTY 1
+#define LITHO_MICRO_REGION_CORE 0
+#define LITHO_MICRO_REGION_CORE_GUARD 1
+#define LITHO_FUSION_AVERAGE 0
+#define LITHO_FUSION_LINEAR 1
+typedef struct litho_exchange_options {
+  int loss_type;                 /* LITHO_MICRO_LOSS_PE */
+  int loss_region;               /* LITHO_MICRO_REGION_CORE */
+  double pe_weight;              /* 1.0 */
+  double penalty_weight;         /* 2.0 (PEPenalty only) */
+  double penalty_threshold;      /* 0.01 */
+  int enable_cept;               /* 0 */
+  int cept_guard_only;           /* 0 */
+  double cept_weight;            /* 1.1 */
+  int enable_grad_fusion;        /* 0 */
+  int fusion_mode;               /* LITHO_FUSION_AVERAGE */
+  double fusion_weight_owner;    /* 0.5; fusion weights must be >= 0 with a positive sum */
+  double fusion_weight_neighbor; /* 0.5 */
+} litho_exchange_options;
+
+/* MicroGradientExchange::compute (source/utils/micro_gradient_exchange.cpp:134-334)
+ * for the PE loss types: per tile imaging, the windowed data loss over the loss
+ * region and its raw mask gradient (phase one, tiles in sequence on the
+ * context's stream), then one launch for every tile's neighbour exchange: CEPT
+ * against the neighbours' Cores and Average/Linear guard-gradient fusion.
+ * cache N must equal tile_size. d_masks: local masks [tile][ts][ts];
+ * d_global_target: height x width; d_raw (nullable): raw per-tile gradients;
+ * d_grad: exchanged gradients. tile_losses (host, nullable): 5 doubles per tile
+ * {pe_loss_raw, bg_penalty_raw, data_loss, cept_loss, loss}; totals (host,
+ * nullable): {loss, data_loss, cept_loss} (MicroGradientExchangeResult). */
+int litho_exchange_compute(litho_ctx* ctx, const litho_partition* partition,
+                           const litho_cache* cache, const float* d_masks,
+                           const float* d_global_target, double threshold, double alpha,
+                           const litho_exchange_options* opt, float* d_raw, float* d_grad,
+                           double* tile_losses, double* totals);
+/* One fixed-step theta update of FullChipCTMOptimizer (source/optimizer/full_chip_ctm.cpp:127-147):
+ * inside each tile's update window theta -= lr * (-1/2 grad sin theta); the
+ * whole tile's mask = (1 + cos theta) / 2. d_grad == NULL only refreshes the
+ * masks from theta. */
+int litho_fullchip_theta_step(litho_ctx* ctx, const litho_partition* partition,
+                              float* d_theta, const float* d_grad, double learning_rate,
+                              float* d_masks);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,189 @@
+"""GPU parity of the full-chip micro-tile path (Partition, MicroGradientExchange,
+FullChipCTMOptimizer) against the FP64 full-chip oracle, through the C ABI.
+
+Tolerances (FP32 path): tile copies bit-exact; raw and exchanged gradients
+relative L2 <= 1e-4 per tile; data and CEPT losses relative 1e-5; full-chip CTM
+loss history relative 1e-4 and best global mask max|d| <= 1e-4.
+"""
+import importlib
+
+import numpy as np
+import pytest
+
+from oracle import fullchip_oracle as fc
+from oracle import imaging_oracle as io
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+THR, ALPHA = 0.225, 50.0
+
+
+@pytest.fixture(scope="module")
+def L():
+    p = importlib.import_module("c-version-lithography_b200")
+    assert torch.cuda.is_available(), "GPU tests need a CUDA device"
+    p.load_library()
+    return p
+
+
+@pytest.fixture(scope="module")
+def FC():
+    return importlib.import_module("c-version-lithography_b200.fullchip")
+
+
+@pytest.fixture(scope="module")
+def band128():
+    wl = importlib.import_module("c-version-lithography_b200.workloads")
+    band, r0, c0, w, wss = wl.synthetic_socs_band()
+    oc = io.OracleCache(N=128, kernels=list(wl.band_to_dense(band, r0, c0, 128)),
+                        source_ws=np.array([wss]), eigenvalues=tuple(w))
+    return oc, wl
+
+
+def rel_l2(a, b):
+    a = np.asarray(a, dtype=np.float64); b = np.asarray(b, dtype=np.float64)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def cpu(t):
+    return t.detach().cpu().numpy().astype(np.float64)
+
+
+def rect(r):
+    return (r.y0, r.y1, r.x0, r.x1)
+
+
+@pytest.mark.parametrize("cfg", [(24, 24, 2, 2, 4, 2), (25, 31, 2, 3, 3, 1), (280, 190, 3, 2, 16, 6),
+                                 (40, 40, 1, 1, 0, 0)])
+def test_partition_matches_oracle(L, FC, cfg):
+    meta = fc.build(*cfg)
+    part = FC.Partition(*cfg)
+    assert part.tile_size == meta.tile_size and part.num_tiles == len(meta.tiles)
+    for a, b in zip(part.tiles, meta.tiles):
+        assert (a.row, a.col) == (b.row, b.col)
+        assert rect(a.core_global) == rect(b.core_global)
+        assert rect(a.tile_global) == rect(b.tile_global)
+        assert rect(a.core_local) == rect(b.core_local)
+        assert rect(a.update_local) == rect(b.update_local)
+    g = np.random.default_rng(3).random((cfg[0], cfg[1])).astype(np.float32)
+    tiles = part.extract_all(torch.from_numpy(g).cuda())
+    ref = [fc.extract_local_tile(g, t) for t in meta.tiles]
+    assert np.array_equal(tiles.cpu().numpy(), np.stack(ref))
+    back = part.assemble_global(tiles).cpu().numpy()
+    assert np.array_equal(back, g)
+
+
+def make_target(H, W, seed):
+    rng = np.random.default_rng(seed)
+    t = np.zeros((H, W))
+    for _ in range(10):
+        y, x = rng.integers(0, H - 20), rng.integers(0, W - 20)
+        t[y:y + rng.integers(6, 20), x:x + rng.integers(6, 20)] = 1.0
+    return t
+
+
+OPTION_SETS = [
+    dict(),
+    dict(loss_type="PEPenalty", loss_region="CoreGuard", pe_weight=0.7, penalty_weight=2.0,
+         enable_cept=True, cept_guard_only=False, cept_weight=1.1, enable_grad_fusion=True,
+         fusion_mode="Linear", fusion_weight_owner=0.5, fusion_weight_neighbor=0.5),
+    dict(enable_cept=True, cept_guard_only=True, enable_grad_fusion=True, fusion_mode="Average",
+         fusion_weight_owner=0.25, fusion_weight_neighbor=0.75),
+]
+
+
+@pytest.mark.parametrize("oi", range(len(OPTION_SETS)))
+def test_exchange_matches_oracle(L, FC, band128, oi):
+    oc, _ = band128
+    cfg = (280, 190, 3, 2, 16, 6)
+    meta = fc.build(*cfg)
+    assert meta.tile_size == oc.N
+    part = FC.Partition(*cfg)
+    cache = L.ImagingCache.from_kernels(np.stack(oc.kernels), oc.source_ws, oc.eigenvalues)
+    target = make_target(cfg[0], cfg[1], oi)
+    rng = np.random.default_rng(10 + oi)
+    theta_g = io.initialize_theta(target) + 0.3 * rng.standard_normal(target.shape)
+    masks32 = [io.theta_to_mask(fc.extract_local_tile(theta_g, t)).astype(np.float32)
+               for t in meta.tiles]
+    masks = [m.astype(np.float64) for m in masks32]
+    opts = OPTION_SETS[oi]
+    ev = fc.exchange(masks, target, meta, oc, THR, ALPHA, fc.ExchangeOptions(**opts))
+    ex = FC.MicroGradientExchange(part, cache, THR, ALPHA)
+    res = ex.compute(torch.from_numpy(np.stack(masks32)).cuda(),
+                     torch.from_numpy(target.astype(np.float32)).cuda(),
+                     FC.MicroGradientOptions(**opts))
+    raw, grad = cpu(res.raw_gradients), cpu(res.mask_gradients)
+    for t in meta.tiles:
+        o = ev["locals"][t.id]
+        assert rel_l2(raw[t.id], o["raw"]) < 1e-4, t.id
+        assert rel_l2(grad[t.id], o["grad"]) < 1e-4, t.id
+        g = res.locals[t.id]
+        assert abs(g.pe_loss - o["pe_loss"]) <= 1e-5 * max(o["pe_loss"], 1e-12)
+        assert abs(g.bg_penalty_raw - o["bg_penalty_raw"]) <= 1e-5 * max(o["bg_penalty_raw"], 1e-9)
+        assert abs(g.cept_loss - o["cept_loss"]) <= 1e-6 * max(o["cept_loss"], 1e-9)
+    assert abs(res.loss - ev["loss"]) <= 1e-5 * ev["loss"]
+    assert abs(res.data_loss - ev["data_loss"]) <= 1e-5 * ev["data_loss"]
+    assert abs(res.cept_loss - ev["cept_loss"]) <= 1e-5 * max(ev["cept_loss"], 1e-9)
+    if opts.get("enable_cept"):
+        assert res.cept_loss > 0.0
+
+
+def test_fullchip_ctm_matches_oracle(L, FC, band128):
+    oc, _ = band128
+    cfg = (192, 192, 2, 2, 16, 6)
+    meta = fc.build(*cfg)
+    part = FC.Partition(*cfg)
+    cache = L.ImagingCache.from_kernels(np.stack(oc.kernels), oc.source_ws, oc.eigenvalues)
+    target = make_target(192, 192, 7)
+    opts = dict(enable_cept=True, enable_grad_fusion=True)
+    ref = fc.full_chip_ctm(target, target, meta, oc, THR, ALPHA, fc.ExchangeOptions(**opts), 3, 0.9)
+    optz = FC.FullChipCTMOptimizer(part, cache, THR, ALPHA)
+    res = optz.optimize(torch.from_numpy(target.astype(np.float32)).cuda(),
+                        FC.FullChipCTMOptions(iterations=3, learning_rate=0.9,
+                                              gradient_options=FC.MicroGradientOptions(**opts)))
+    hist = [h.loss for h in res.history]
+    assert len(hist) == 4
+    for a, b in zip(hist, ref["history"]):
+        assert abs(a - b) <= 1e-4 * b
+    assert res.best_iteration == ref["best"]["iteration"]
+    assert np.max(np.abs(cpu(res.global_mask) - ref["global_mask"])) < 1e-4
+    # theta outside each tile's update window keeps its initial value
+    init = part.extract_all(optz.initialize_theta(torch.from_numpy(target.astype(np.float32)).cuda(),
+                                                  torch))
+    th, th0 = cpu(res.local_theta), cpu(init)
+    for t in part.tiles:
+        w = t.update_local
+        out = np.ones((part.tile_size, part.tile_size), bool)
+        out[w.y0:w.y1, w.x0:w.x1] = False
+        assert np.array_equal(th[t.id][out], th0[t.id][out])
+
+
+def test_fullchip_errors(L, FC, band128):
+    oc, _ = band128
+    with pytest.raises(L.LithoError) as e:
+        FC.Partition(24, 24, 2, 2, 2, 4)          # guard > halo
+    assert e.value.status == 1
+    with pytest.raises(L.LithoError):
+        FC.Partition(4, 24, 5, 2, 2, 1)           # more grid rows than layout rows
+    part = FC.Partition(24, 24, 2, 2, 4, 2)       # tile 20 != cache 128
+    cache = L.ImagingCache.from_kernels(np.stack(oc.kernels), oc.source_ws, oc.eigenvalues)
+    with pytest.raises(L.LithoError) as e:
+        FC.MicroGradientExchange(part, cache)
+    assert e.value.status == 2
+    cfg = (192, 192, 2, 2, 16, 6)
+    part = FC.Partition(*cfg)
+    ex = FC.MicroGradientExchange(part, cache, THR, ALPHA)
+    masks = torch.full((4, 128, 128), 0.5, device="cuda")
+    tgt = torch.zeros((192, 192), device="cuda")
+    with pytest.raises(L.LithoError) as e:
+        ex.compute(masks, tgt, FC.MicroGradientOptions(enable_grad_fusion=True,
+                                                       fusion_weight_owner=-1.0))
+    assert e.value.status == 1
+    with pytest.raises(L.LithoError) as e:
+        ex.compute(masks, tgt, FC.MicroGradientOptions(loss_type="EPE"))
+    assert e.value.status == 7
+    masks[1, 5, 7] = float("nan")
+    with pytest.raises(L.LithoError) as e:
+        ex.compute(masks, tgt)
+    assert e.value.status == 3
