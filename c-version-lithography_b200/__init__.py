@@ -109,6 +109,7 @@ SIGNATURES = {
     "litho_exchange_compute": (_I, [_P, _P, _P, _P, _P, _D, _D,
                                     ctypes.POINTER(ExchangeOptionsC), _P, _P, _PD, _PD]),
     "litho_fullchip_theta_step": (_I, [_P, _P, _P, _P, _D, _P]),
+    "litho_lsm_rk2_update_noalloc": (_I, [_P, _I, _I, _P, _P, _D, _D, _D, _D, _P, _P, _PD]),
 }
 
 

@@ -271,6 +271,33 @@ int litho_fullchip_theta_step(litho_ctx* ctx, const litho_partition* partition,
                               float* d_theta, const float* d_grad, double learning_rate,
                               float* d_masks);
 
+/* ------------------------------------------------------------ no-allocation variant
+ * litho_lsm_rk2_update_noalloc: the RK2 level-set update of litho_lsm_rk2_update
+ * (same kernels, same results) for callers that must not allocate device
+ * memory at call time, e.g. a service whose device memory budget is fully
+ * reserved up front, or code interleaved with other streams' work where a
+ * cudaMalloc would implicitly synchronise the device. It takes a plain
+ * cudaStream_t (NULL = default stream) instead of a litho_ctx and never calls
+ * cudaMalloc/cudaFree: its scratch (the first RK2 stage and the dt reduction)
+ * is one static device array of 2048 * 2048 + 512 floats (about 16 MiB) per
+ * device, so rows * cols must not exceed LITHO_RK2_NOALLOC_MAX_PIXELS; larger
+ * grids return LITHO_ERR_UNSUPPORTED without launching anything (use
+ * litho_lsm_rk2_update for them). Nothing has to be zero beforehand: each call
+ * clears the non-finite flag it uses. The first call on each device looks up
+ * the scratch address (cudaGetSymbolAddress) and loads the module; make that
+ * call before any stream capture begins. The calling thread's current device
+ * must be the stream's device. Calls share the one scratch array per device,
+ * so two calls that overlap in time (different host threads or streams) race:
+ * serialise them. The call waits for its stream to return dt (host, nullable).
+ * Status as litho_lsm_rk2_update; LITHO_ERR_NONFINITE for non-finite Vn.
+ * This entry point has no counterpart in the reference (its LSM_Optimizer
+ * allocates Eigen matrices on every step, source/optimizer/LSM_Optimizer.cpp:109-115).
+ */
+#define LITHO_RK2_NOALLOC_MAX_PIXELS (2048 * 2048)
+int litho_lsm_rk2_update_noalloc(void* stream, int rows, int cols, const float* d_phi,
+                                 const float* d_vn, double dx, double dy, double cfl, double b,
+                                 float* d_phi_out, float* d_mask, double* dt);
+
 #ifdef __cplusplus
 }
 #endif

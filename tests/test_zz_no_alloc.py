@@ -1,0 +1,100 @@
+"""litho_lsm_rk2_update_noalloc (static device scratch, no allocation) against
+the context-based litho_lsm_rk2_update, through the C ABI. Collected last on
+purpose: it must pass alone and after every other test in the process.
+
+Tolerance: both entry points run the same kernels, so phi, mask and dt must agree
+to max|d| <= 1e-6 (in practice bit-identical).
+"""
+import ctypes
+import importlib
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-6
+
+
+@pytest.fixture(scope="module")
+def L():
+    p = importlib.import_module("c-version-lithography_b200")
+    assert torch.cuda.is_available(), "GPU tests need a CUDA device"
+    p.load_library()
+    return p
+
+
+def noalloc(L, phi, vn, dx, dy, cfl, b, out, mask):
+    dt = ctypes.c_double()
+    st = L.load_library().litho_lsm_rk2_update_noalloc(
+        ctypes.c_void_p(torch.cuda.current_stream().cuda_stream), phi.shape[0], phi.shape[1],
+        phi.data_ptr(), vn.data_ptr(), dx, dy, cfl, b, out.data_ptr(),
+        None if mask is None else mask.data_ptr(), ctypes.byref(dt))
+    return st, dt.value
+
+
+def reference(L, ctx, phi, vn, dx, dy, cfl, b):
+    out = torch.empty_like(phi)
+    mask = torch.empty_like(phi)
+    dt = ctypes.c_double()
+    ctx._check(ctx.lib.litho_lsm_rk2_update(ctx.handle, phi.shape[0], phi.shape[1], phi.data_ptr(),
+                                            vn.data_ptr(), dx, dy, cfl, b, out.data_ptr(),
+                                            mask.data_ptr(), ctypes.byref(dt)))
+    ctx.synchronize()
+    return out, mask, dt.value
+
+
+def test_noalloc_matches_context_entry_point_twice(L):
+    rows, cols, dx, dy, cfl, b = 300, 257, 1.0, 1.0, 0.5, 0.01
+    yy, xx = np.mgrid[0:rows, 0:cols].astype(np.float64)
+    phi0 = 40.0 - np.hypot(yy - 150.0, xx - 120.0) + 3.0 * np.sin(xx / 7.0)
+    rng = np.random.default_rng(0)
+    phi = torch.from_numpy(phi0.astype(np.float32)).cuda()
+    vn = torch.from_numpy(rng.standard_normal((rows, cols)).astype(np.float32)).cuda()
+    ctx = L.Context()
+    for _ in range(2):  # two calls in a row, the second starting from the first's output
+        ref_out, ref_mask, ref_dt = reference(L, ctx, phi, vn, dx, dy, cfl, b)
+        out = torch.empty_like(phi)
+        mask = torch.empty_like(phi)
+        st, dt = noalloc(L, phi, vn, dx, dy, cfl, b, out, mask)
+        assert st == 0
+        assert abs(dt - ref_dt) <= TOL * abs(ref_dt)
+        assert torch.max(torch.abs(out - ref_out)).item() <= TOL * torch.max(torch.abs(ref_out)).item()
+        assert torch.equal(mask, ref_mask)
+        phi = out
+    ctx.close()
+
+
+def test_noalloc_limits_and_flag(L):
+    rows, cols = 64, 64
+    phi = torch.randn(rows, cols, device="cuda")
+    vn = torch.randn(rows, cols, device="cuda")
+    out = torch.empty_like(phi)
+    # beyond the static scratch: rejected before any launch (pointers are never read)
+    n_max = 2048 * 2048
+    st, _ = noalloc_shape(L, n_max // 1024 + 1, 1024, phi, vn, out)
+    assert st == 7
+    st, _ = noalloc_shape(L, 2, 64, phi, vn, out)
+    assert st == 2
+    # non-finite speed raises the flag; the next call clears it and succeeds
+    bad = vn.clone()
+    bad[3, 4] = float("inf")
+    st, _ = noalloc(L, phi, bad, 1.0, 1.0, 0.5, 0.01, out, None)
+    assert st == 3
+    st, dt = noalloc(L, phi, vn, 1.0, 1.0, 0.5, 0.01, out, None)
+    assert st == 0 and dt > 0.0
+    # no device memory is taken by repeated calls
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    for _ in range(3):
+        assert noalloc(L, phi, vn, 1.0, 1.0, 0.5, 0.01, out, None)[0] == 0
+    assert torch.cuda.mem_get_info()[0] == free0
+
+
+def noalloc_shape(L, rows, cols, phi, vn, out):
+    dt = ctypes.c_double()
+    st = L.load_library().litho_lsm_rk2_update_noalloc(
+        ctypes.c_void_p(torch.cuda.current_stream().cuda_stream), rows, cols, phi.data_ptr(),
+        vn.data_ptr(), 1.0, 1.0, 0.5, 0.01, out.data_ptr(), None, ctypes.byref(dt))
+    return st, dt.value
