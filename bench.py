@@ -216,7 +216,6 @@ def _measure(L, torch, ctx, stream, cache, target, th, flush, steps, warmup, dis
     while nwarm < max(3, warmup) or time.perf_counter() - t_warm < 0.5:
         opt.evaluate(th)
         nwarm += 1
-    ctx.enable_stage_timing(True)
     launches0 = ctx.launch_count
     times = []
     if dist:
@@ -234,6 +233,14 @@ def _measure(L, torch, ctx, stream, cache, target, th, flush, steps, warmup, dis
         times.append(e0.elapsed_time(e1))
     torch.cuda.synchronize()
     launches = ctx.launch_count - launches0
+    # Per-stage breakdown from separate steps: the stage events sit between kernels
+    # and would otherwise perturb the timed steps above.
+    ctx.enable_stage_timing(True)
+    for _ in range(min(steps, 5)):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        opt.evaluate(th)
+    torch.cuda.synchronize()
     stages = ctx.stage_times()
     ctx.enable_stage_timing(False)
     total_ms = sum(times)

@@ -48,16 +48,17 @@ int upload(Context* ctx, T** dst, const std::vector<T>& src) {
 }
 
 void free_cache(Cache* c) {
-  void* ptrs[] = {c->H,    c->w,    c->TXS,  c->TXD,   c->TYS,   c->TYD,   c->AYS,
-                  c->AYD,  c->TXSc, c->TXDc, c->ESr_t, c->ESc_t, c->ESc,   c->EDr_t,
-                  c->EDc_t, c->EDc,  c->AYS_img, c->AYD_img, c->TXS_img, c->TXD_img};
+  void* ptrs[] = {c->H,     c->w,       c->TXS,     c->TXD,     c->TYS,     c->TYD,
+                  c->AYS,   c->AYD,     c->TXSc,    c->TXDc,    c->ESr_t,   c->ESc_t,
+                  c->ESc,   c->EDr_t,   c->EDc_t,   c->EDc,     c->AYS_img, c->AYD_img,
+                  c->TXS_img, c->TXD_img, c->TYS_img, c->TYD_img};
   for (void* p : ptrs)
     if (p) cudaFree(p);
 }
 
 // Scratch layout of one imaging + adjoint evaluation.
 struct Layout {
-  size_t part, gh, ik, iP, chat, X, Ut, Vt, dldi, gam, Zk, rows_tmp, img, total;
+  size_t part, gh, ik, iP, chat, Ut, Vt, dldi, gam, Zk, rows_tmp, img, total;
   int tiles;
 };
 
@@ -81,9 +82,8 @@ Layout make_layout(const BandGeom& g) {
   L.gam = take((size_t)g.Pr * g.Pc * sizeof(float));
   L.Zk = take((size_t)g.K * g.Nr * g.Nc * sizeof(float2));
   L.chat = take((size_t)g.Nr * (2 * g.Nc - 1) * sizeof(float2));
-  L.X = take((size_t)g.Nr * g.Nc * sizeof(float2));
   L.rows_tmp = take((size_t)g.Nr * N * sizeof(float2));
-  L.img = take(tc_image_bytes(N, g.kp_rows, 256));  // band operand image (tensor-core path)
+  L.img = take(tc2_supported(g) ? tc2_rows_image_bytes(N, g.kp_rows) : 16);  // band operand image
   L.total = off;
   return L;
 }
@@ -212,6 +212,10 @@ int litho_ctx_destroy(litho_ctx* ctx) {
   if (ctx->scratch.base) cudaFree(ctx->scratch.base);
   if (ctx->d_red) cudaFree(ctx->d_red);
   if (ctx->h_red) cudaFreeHost(ctx->h_red);
+  if (ctx->host_stage.base) cudaFree(ctx->host_stage.base);
+  for (cudaEvent_t e : ctx->ev_aux)
+    if (e) cudaEventDestroy(e);
+  if (ctx->aux) cudaStreamDestroy(ctx->aux);
   for (int i = 0; i < LITHO_NUM_STAGES; ++i)
     for (int j = 0; j < 2; ++j)
       if (ctx->ev[i][j]) cudaEventDestroy(ctx->ev[i][j]);
@@ -379,28 +383,34 @@ int litho_cache_create_band(litho_ctx* ctx, int N, int K, int Nr, int Nc, int ro
   if (st == LITHO_OK) st = upload(ctx, &c->EDr_t, EDr_t);
   if (st == LITHO_OK) st = upload(ctx, &c->EDc_t, EDc_t);
   if (st == LITHO_OK) st = upload(ctx, &c->EDc, EDc);
-  // Split-BF16 images of the two row-analysis twiddle tables for the tensor cores.
-  for (int t = 0; t < 2 && st == LITHO_OK; ++t) {
-    void** img = t == 0 ? &c->TXS_img : &c->TXD_img;
-    const float* src = t == 0 ? c->TXS : c->TXD;
-    if (cudaMalloc(img, tw_image_bytes(N, Nc)) != cudaSuccess) {
-      cudaGetLastError();
-      st = ctx->fail(LITHO_ERR_OOM, "tensor-core operand image allocation failed");
-    } else if (launch_pack_tw(ctx->stream, src, Nc, N, *img) != cudaSuccess ||
-               cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
-      st = ctx->fail(LITHO_ERR_CUDA, "tensor-core operand packing failed");
-    }
-  }
-  // Split-BF16 images of the two row-synthesis twiddle tables for the tensor cores.
-  for (int t = 0; t < 2 && st == LITHO_OK; ++t) {
-    void** img = t == 0 ? &c->AYS_img : &c->AYD_img;
-    const float* src = t == 0 ? c->AYS : c->AYD;
-    if (cudaMalloc(img, tc_image_bytes(N, g.kp_rows, 128)) != cudaSuccess) {
-      cudaGetLastError();
-      st = ctx->fail(LITHO_ERR_OOM, "tensor-core operand image allocation failed");
-    } else if (launch_pack_split(ctx->stream, src, N, g.kp_rows, 128, 0, *img) != cudaSuccess ||
-               cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
-      st = ctx->fail(LITHO_ERR_CUDA, "tensor-core operand packing failed");
+  // Split-BF16 images of the twiddle tables for the tensor-core passes.
+  if (tc2_supported(g)) {
+    struct ImageJob {
+      void** dst;
+      size_t bytes;
+      int what;
+    } jobs[] = {{&c->TXS_img, tc2_tx_image_bytes(N, Nc), 0}, {&c->TXD_img, tc2_tx_image_bytes(N, Nc), 1},
+                {&c->TYS_img, tc2_ty_image_bytes(N), 2},     {&c->TYD_img, tc2_ty_image_bytes(N), 3},
+                {&c->AYS_img, tc2_rows_image_bytes(N, g.kp_rows), 4},
+                {&c->AYD_img, tc2_rows_image_bytes(N, g.kp_rows), 5}};
+    for (const ImageJob& j : jobs) {
+      if (st != LITHO_OK) break;
+      if (cudaMalloc(j.dst, j.bytes) != cudaSuccess) {
+        cudaGetLastError();
+        st = ctx->fail(LITHO_ERR_OOM, "tensor-core operand image allocation failed");
+        break;
+      }
+      cudaError_t e;
+      switch (j.what) {
+        case 0: e = launch_pack_tc2_tx(ctx->stream, c->TXS, Nc, N, *j.dst); break;
+        case 1: e = launch_pack_tc2_tx(ctx->stream, c->TXD, Nc, N, *j.dst); break;
+        case 2: e = launch_pack_tc2_ty(ctx->stream, c->TYS, Nr, N, *j.dst); break;
+        case 3: e = launch_pack_tc2_ty(ctx->stream, c->TYD, Nr, N, *j.dst); break;
+        case 4: e = launch_pack_tc2_rows(ctx->stream, c->AYS, N, g.kp_rows, *j.dst); break;
+        default: e = launch_pack_tc2_rows(ctx->stream, c->AYD, N, g.kp_rows, *j.dst); break;
+      }
+      if (e != cudaSuccess || cudaStreamSynchronize(ctx->stream) != cudaSuccess)
+        st = ctx->fail(LITHO_ERR_CUDA, "tensor-core operand packing failed");
     }
   }
   if (st != LITHO_OK) {
@@ -537,17 +547,23 @@ int check_launch(Context* ctx, cudaError_t e, const char* what) {
 // Forward: tile analysis -> tile reduction -> small-grid band stage -> row
 // synthesis with the fused resist epilogue. input_mode 1 reads theta.
 int run_forward(Context* ctx, const Cache& c, Field& f, const Layout& L, int input_mode,
-                const float* input, float* mask_out, ResistEpilogue ep, int* nblocks) {
+                const float* input, float* mask_out, ResistEpilogue ep, int* nblocks,
+                cudaEvent_t before_synthesis = nullptr) {
   const BandGeom& g = c.g;
   cudaStream_t s = ctx->stream;
   int* flag = reinterpret_cast<int*>(ctx->d_red + RED_FLAG);
   int st;
   ctx->stage_begin(0);
-  const bool tc = ctx->precision == LITHO_PRECISION_BF16X3;
-  st = check_launch(ctx, launch_analysis(s, input_mode, input, mask_out, flag, c.TXS, g.N, g.Nc,
-                                         c.TYS, g.Nr, g.Nr, 0, at<float2>(ctx, L.part),
-                                         tc ? c.TXS_img : nullptr, flag + 1),
-                    "tile analysis");
+  const bool tc = ctx->precision == LITHO_PRECISION_BF16X3 && c.TXS_img;
+  if (tc)
+    st = check_launch(ctx, launch_analysis_tc2(s, input_mode, input, mask_out, flag, g.N, g.Nc,
+                                               g.Nr, g.Nr, 0, at<float2>(ctx, L.part), c.TXS_img,
+                                               c.TYS_img, flag + 1),
+                      "tensor-core tile analysis");
+  else
+    st = check_launch(ctx, launch_analysis(s, input_mode, input, mask_out, flag, c.TXS, g.N, g.Nc,
+                                           c.TYS, g.Nr, g.Nr, 0, at<float2>(ctx, L.part)),
+                      "tile analysis");
   ctx->stage_end(0);
   if (st) return st;
   ctx->stage_begin(1);
@@ -562,15 +578,17 @@ int run_forward(Context* ctx, const Cache& c, Field& f, const Layout& L, int inp
                     "band forward");
   ctx->stage_end(2);
   if (st) return st;
+  // The epilogue's inputs may still be arriving on another stream.
+  if (before_synthesis) LITHO_CUDA_TRY(ctx, cudaStreamWaitEvent(s, before_synthesis, 0));
   ctx->stage_begin(3);
-  if (ctx->precision == LITHO_PRECISION_BF16X3) {
+  if (tc) {
     int* err = reinterpret_cast<int*>(ctx->d_red + RED_FLAG) + 1;
-    st = check_launch(ctx, launch_pack_split(s, at<float>(ctx, L.Ut), g.N, g.kp_rows, 256, 1,
-                                             at<void>(ctx, L.img)),
+    st = check_launch(ctx, launch_pack_tc2_rows(s, at<float>(ctx, L.Ut), g.N, g.kp_rows,
+                                                at<void>(ctx, L.img)),
                       "band operand packing");
     if (!st)
-      st = check_launch(ctx, launch_synth_resist_tc(s, c.AYD_img, at<void>(ctx, L.img), g.N,
-                                                    g.kp_rows, ep, err, nblocks),
+      st = check_launch(ctx, launch_synth_resist_tc2(s, c.AYD_img, at<void>(ctx, L.img), g.N,
+                                                     g.kp_rows, ep, err, nblocks),
                         "tensor-core row synthesis");
     ctx->launches += 1;
   } else {
@@ -592,11 +610,16 @@ int run_adjoint(Context* ctx, const Cache& c, const Field& f, const Layout& L, c
   const int na = 2 * g.Nr - 1;
   int st;
   ctx->stage_begin(4);
-  const bool tc = ctx->precision == LITHO_PRECISION_BF16X3;
-  st = check_launch(ctx, launch_analysis(s, 0, dldi, nullptr, flag, c.TXD, g.N, g.Nc, c.TYD, na,
-                                         g.Nr, 1, at<float2>(ctx, L.part),
-                                         tc ? c.TXD_img : nullptr, flag + 1),
-                    "adjoint tile analysis");
+  const bool tc = ctx->precision == LITHO_PRECISION_BF16X3 && c.TXD_img;
+  if (tc)
+    st = check_launch(ctx, launch_analysis_tc2(s, 0, dldi, nullptr, flag, g.N, g.Nc, na, g.Nr, 1,
+                                               at<float2>(ctx, L.part), c.TXD_img, c.TYD_img,
+                                               flag + 1),
+                      "tensor-core adjoint tile analysis");
+  else
+    st = check_launch(ctx, launch_analysis(s, 0, dldi, nullptr, flag, c.TXD, g.N, g.Nc, c.TYD, na,
+                                           g.Nr, 1, at<float2>(ctx, L.part)),
+                      "adjoint tile analysis");
   ctx->stage_end(4);
   if (st) return st;
   ctx->stage_begin(5);
@@ -608,19 +631,19 @@ int run_adjoint(Context* ctx, const Cache& c, const Field& f, const Layout& L, c
   ctx->stage_begin(6);
   st = check_launch(ctx, launch_band_adjoint(s, c, f, at<float2>(ctx, L.gh), scale,
                                              at<float>(ctx, L.gam), at<float2>(ctx, L.Zk),
-                                             at<float2>(ctx, L.X), at<float>(ctx, L.Vt)),
+                                             at<float>(ctx, L.Vt)),
                     "band adjoint");
   ctx->stage_end(6);
   if (st) return st;
   ctx->stage_begin(7);
-  if (ctx->precision == LITHO_PRECISION_BF16X3) {
+  if (tc) {
     int* err = reinterpret_cast<int*>(ctx->d_red + RED_FLAG) + 1;
-    st = check_launch(ctx, launch_pack_split(s, at<float>(ctx, L.Vt), g.N, g.kp_rows, 256, 1,
-                                             at<void>(ctx, L.img)),
+    st = check_launch(ctx, launch_pack_tc2_rows(s, at<float>(ctx, L.Vt), g.N, g.kp_rows,
+                                                at<void>(ctx, L.img)),
                       "band operand packing");
     if (!st)
-      st = check_launch(ctx, launch_synth_grad_tc(s, c.AYS_img, at<void>(ctx, L.img), g.N,
-                                                  g.kp_rows, ep, err, nblocks),
+      st = check_launch(ctx, launch_synth_grad_tc2(s, c.AYS_img, at<void>(ctx, L.img), g.N,
+                                                   g.kp_rows, ep, err, nblocks),
                         "tensor-core adjoint row synthesis");
     ctx->launches += 1;
   } else {
@@ -797,11 +820,11 @@ int litho_pe_gradient(litho_ctx* ctx, const litho_field* field, const float* d_w
   return LITHO_OK;
 }
 
-int litho_ctm_evaluate(litho_ctx* ctx, const litho_cache* cache, litho_field* field,
-                       const float* d_theta, const float* d_target, double threshold,
-                       double alpha, float* d_mask, float* d_aerial, float* d_wafer,
-                       float* d_grad_mask, float* d_grad_theta, double* loss,
-                       double* grad_norm) {
+static int ctm_evaluate_impl(litho_ctx* ctx, const litho_cache* cache, litho_field* field,
+                             const float* d_theta, const float* d_target, double threshold,
+                             double alpha, float* d_mask, float* d_aerial, float* d_wafer,
+                             float* d_grad_mask, float* d_grad_theta, double* loss,
+                             double* grad_norm, cudaEvent_t target_ready) {
   if (!ctx || !cache || !d_theta || !d_target || !d_grad_theta) return LITHO_ERR_INVALID_ARGUMENT;
   if (!std::isfinite(threshold) || !std::isfinite(alpha))
     return ctx->fail(LITHO_ERR_NONFINITE, "Imaging: mask, threshold, and alpha must be finite");
@@ -839,7 +862,7 @@ int litho_ctm_evaluate(litho_ctx* ctx, const litho_cache* cache, litho_field* fi
   ep.dldi = at<float>(ctx, L.dldi);
   ep.loss_partial = ctx->d_red + RED_PART;
   int nb = 0;
-  st = run_forward(ctx, *cache, *f, L, 1, d_theta, d_mask, ep, &nb);
+  st = run_forward(ctx, *cache, *f, L, 1, d_theta, d_mask, ep, &nb, target_ready);
   if (!st)
     st = check_launch(ctx, launch_sum_partials(ctx->stream, ctx->d_red + RED_PART, nb, 2,
                                                ctx->d_red + RED_SUM),
@@ -869,34 +892,66 @@ int litho_ctm_evaluate(litho_ctx* ctx, const litho_cache* cache, litho_field* fi
   return LITHO_OK;
 }
 
+int litho_ctm_evaluate(litho_ctx* ctx, const litho_cache* cache, litho_field* field,
+                       const float* d_theta, const float* d_target, double threshold,
+                       double alpha, float* d_mask, float* d_aerial, float* d_wafer,
+                       float* d_grad_mask, float* d_grad_theta, double* loss,
+                       double* grad_norm) {
+  return ctm_evaluate_impl(ctx, cache, field, d_theta, d_target, threshold, alpha, d_mask,
+                           d_aerial, d_wafer, d_grad_mask, d_grad_theta, loss, grad_norm,
+                           nullptr);
+}
+
+// Host buffers: theta goes up first on the context's stream; the target follows on
+// an upload stream while the analysis and the small-grid stage run, and the
+// resist epilogue waits for it. The staging buffer and the upload stream persist
+// in the context.
 int litho_ctm_evaluate_host(litho_ctx* ctx, const litho_cache* cache, litho_field* field,
                             const float* h_theta, const float* h_target, double threshold,
                             double alpha, float* h_grad_theta, double* loss,
                             double* grad_norm) {
   if (!ctx || !cache || !h_theta || !h_target || !h_grad_theta) return LITHO_ERR_INVALID_ARGUMENT;
   const size_t n = (size_t)cache->g.N * cache->g.N;
-  float *d = nullptr;
   if (cudaSetDevice(ctx->device) != cudaSuccess) return LITHO_ERR_CUDA;
-  if (cudaMallocAsync(reinterpret_cast<void**>(&d), 3 * n * sizeof(float), ctx->stream) !=
-      cudaSuccess) {
-    cudaGetLastError();
-    return ctx->fail(LITHO_ERR_OOM, "host-call staging allocation failed");
+  if (ctx->host_stage.bytes < 3 * n * sizeof(float)) {
+    cudaStreamSynchronize(ctx->stream);
+    if (ctx->host_stage.base) cudaFree(ctx->host_stage.base);
+    ctx->host_stage.base = nullptr;
+    ctx->host_stage.bytes = 0;
+    if (cudaMalloc(&ctx->host_stage.base, 3 * n * sizeof(float)) != cudaSuccess) {
+      cudaGetLastError();
+      return ctx->fail(LITHO_ERR_OOM, "host-call staging allocation failed");
+    }
+    ctx->host_stage.bytes = 3 * n * sizeof(float);
   }
+  if (!ctx->aux) {
+    if (cudaStreamCreateWithFlags(&ctx->aux, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ctx->ev_aux[0], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ctx->ev_aux[1], cudaEventDisableTiming) != cudaSuccess) {
+      cudaGetLastError();
+      return ctx->fail(LITHO_ERR_CUDA, "upload stream creation failed");
+    }
+  }
+  float* d = static_cast<float*>(ctx->host_stage.base);
   int st = LITHO_OK;
   if (cudaMemcpyAsync(d, h_theta, n * sizeof(float), cudaMemcpyHostToDevice, ctx->stream) !=
           cudaSuccess ||
-      cudaMemcpyAsync(d + n, h_target, n * sizeof(float), cudaMemcpyHostToDevice, ctx->stream) !=
-          cudaSuccess)
+      cudaEventRecord(ctx->ev_aux[0], ctx->stream) != cudaSuccess ||
+      cudaStreamWaitEvent(ctx->aux, ctx->ev_aux[0], 0) != cudaSuccess ||
+      cudaMemcpyAsync(d + n, h_target, n * sizeof(float), cudaMemcpyHostToDevice, ctx->aux) !=
+          cudaSuccess ||
+      cudaEventRecord(ctx->ev_aux[1], ctx->aux) != cudaSuccess)
     st = ctx->fail(LITHO_ERR_CUDA, "host to device copy failed");
   if (!st)
-    st = litho_ctm_evaluate(ctx, cache, field, d, d + n, threshold, alpha, nullptr, nullptr,
-                            nullptr, nullptr, d + 2 * n, loss, grad_norm);
+    st = ctm_evaluate_impl(ctx, cache, field, d, d + n, threshold, alpha, nullptr, nullptr,
+                           nullptr, nullptr, d + 2 * n, loss, grad_norm, ctx->ev_aux[1]);
   if (!st && cudaMemcpyAsync(h_grad_theta, d + 2 * n, n * sizeof(float), cudaMemcpyDeviceToHost,
                              ctx->stream) != cudaSuccess)
     st = ctx->fail(LITHO_ERR_CUDA, "device to host copy failed");
-  cudaFreeAsync(d, ctx->stream);
   if (cudaStreamSynchronize(ctx->stream) != cudaSuccess && !st)
     st = ctx->fail(LITHO_ERR_CUDA, "stream synchronize failed");
+  if (cudaStreamSynchronize(ctx->aux) != cudaSuccess && !st)
+    st = ctx->fail(LITHO_ERR_CUDA, "upload stream synchronize failed");
   return st;
 }
 

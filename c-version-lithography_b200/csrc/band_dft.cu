@@ -18,10 +18,7 @@
 
 #include <algorithm>
 
-#include <cuda_bf16.h>
-
 #include "device_common.cuh"
-#include "tc_ptx.cuh"
 
 namespace litho_b200 {
 
@@ -134,6 +131,8 @@ analysis_tile_kernel(AnalysisArgs a) {
   const int f0 = blockIdx.z * BN;
   const int Nn = 2 * a.ncols;
   ImageLoad ld = a.ld;
+  pdl_trigger();
+  pdl_wait();
 
   // Phase 1: R[y][f] = sum_{x in tile} A[y][x] tw[f][x]  (128 rows x BN real columns).
   float acc[AT_TM][TN];
@@ -224,8 +223,7 @@ static cudaError_t analysis_tile_t(cudaStream_t s, const AnalysisArgs& a) {
   if (e != cudaSuccess) return e;
   const int t = (a.N + AT_TILE - 1) / AT_TILE;
   dim3 grid(t, t, (2 * a.ncols + BN - 1) / BN);
-  analysis_tile_kernel<TN><<<grid, AT_NT, smem, s>>>(a);
-  return cudaGetLastError();
+  return launch_pdl(analysis_tile_kernel<TN>, grid, dim3(AT_NT), smem, s, a);
 }
 
 int analysis_tiles(int N) {
@@ -233,229 +231,15 @@ int analysis_tiles(int N) {
   return t * t;
 }
 
-// ---------------------------------------------------------------- tile analysis, tcgen05
-// Phase 1 of the tile analysis on the tensor cores in split-BF16:
-//   R[y][f] = sum_{x in tile} A[y][x] tw[f][x]
-// as one BF16 GEMM with M = 128 (rows y), N = rowsP (2 ncols rounded to 16),
-// K = 3 x 128: A3[y] = [A_hi | A_hi | A_lo] is built by the CTA's threads from
-// the FP32 tile (theta -> mask fused), B3[f] = [tw_hi | tw_lo | tw_hi] is a
-// per-cache image bulk-copied from global memory. The accumulator lives in
-// tensor memory; phase 2 (the column contraction) then runs on the CUDA cores
-// from shared memory, exactly as in the SIMT kernel.
-constexpr int AQ_K3 = 3 * AT_TILE;                       // 384
-constexpr uint32_t AQ_A_BYTES = AT_TILE * AQ_K3 * 2;     // 96 KiB
-
-// Image of the row-analysis twiddles tw [nrow][N] for the tensor cores: per
-// 128-column x tile t, a K-major SW128 tile of rowsP rows and 384 K
-// ([hi | lo | hi] of the 128 columns); rows >= nrow and columns >= N are zero.
-__global__ void pack_tw_kernel(const float* __restrict__ tw, int nrow, int rowsP, int N,
-                               uint4* __restrict__ dst, size_t n16) {
-  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= n16) return;
-  const int c = (int)(idx % 8);
-  size_t rest = idx / 8;
-  const int r = (int)(rest % rowsP);
-  rest /= rowsP;
-  const int kb = (int)(rest % (AQ_K3 / 64));
-  const int t = (int)(rest / (AQ_K3 / 64));
-  __nv_bfloat16 out[8];
-#pragma unroll
-  for (int q = 0; q < 8; ++q) {
-    const int k = kb * 64 + c * 8 + q;
-    const int sec = k / AT_TILE, x = t * AT_TILE + k % AT_TILE;
-    const float v = (r < nrow && x < N) ? tw[(size_t)r * N + x] : 0.f;
-    const __nv_bfloat16 hi = __float2bfloat16_rn(v);
-    out[q] = sec == 1 ? __float2bfloat16_rn(v - __bfloat162float(hi)) : hi;
-  }
-  const size_t off16 = ((size_t)t * (AQ_K3 / 64) + kb) * (size_t)rowsP * 8 +
-                       (size_t)(r / 8) * 64 + (size_t)(r % 8) * 8 + (size_t)(c ^ (r % 8));
-  dst[off16] = *reinterpret_cast<const uint4*>(out);
-}
-
-int tw_rows_padded(int ncols) { return (2 * ncols + 15) / 16 * 16; }
-
-size_t tw_image_bytes(int N, int ncols) {
-  const size_t tiles = (size_t)(N + AT_TILE - 1) / AT_TILE;
-  return tiles * (size_t)tw_rows_padded(ncols) * AQ_K3 * 2;
-}
-
-cudaError_t launch_pack_tw(cudaStream_t s, const float* tw, int ncols, int N, void* dst) {
-  const int rowsP = tw_rows_padded(ncols);
-  const size_t tiles = (size_t)(N + AT_TILE - 1) / AT_TILE;
-  const size_t n16 = tiles * (AQ_K3 / 64) * (size_t)rowsP * 8;
-  pack_tw_kernel<<<(unsigned)((n16 + 255) / 256), 256, 0, s>>>(
-      tw, 2 * ncols, rowsP, N, reinterpret_cast<uint4*>(dst), n16);
-  return cudaGetLastError();
-}
-
-// 16 consecutive FP32 columns of this thread's TMEM lane.
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
-  uint32_t r[16];
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
-      "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
-        "=r"(r[14]), "=r"(r[15])
-      : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
-}
-
-template <int BN>   // BN = rowsP: real columns of the accumulator
-__global__ void __launch_bounds__(AT_NT, 1)
-analysis_tc_kernel(AnalysisArgs a, const uint8_t* __restrict__ Bimg, int* __restrict__ err) {
-  extern __shared__ __align__(1024) uint8_t smem_raw[];
-  __shared__ __align__(8) uint64_t bars[2];
-  __shared__ uint32_t tmem_slot;
-  __shared__ int fail;
-  constexpr uint32_t B_BYTES = (uint32_t)BN * AQ_K3 * 2;
-  constexpr uint32_t TM_COLS = BN <= 32 ? 32 : (BN <= 64 ? 64 : 128);
-  uint8_t* smem = reinterpret_cast<uint8_t*>(
-      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
-  uint8_t* sA = smem;
-  uint8_t* sB = smem + AQ_A_BYTES;
-  const int tid = threadIdx.x, warp = tid >> 5;
-  const int xt = blockIdx.x, yt = blockIdx.y;
-  const int x0 = xt * AT_TILE, y0 = yt * AT_TILE;
-  const uint32_t barL = tc::smem_u32(&bars[0]), barM = tc::smem_u32(&bars[1]);
-  if (tid == 0) {
-    tc::mbar_init(barL, 1);
-    tc::mbar_init(barM, 1);
-    fail = 0;
-    tc::fence_mbar_init();
-  }
-  if (warp == 0) tc::tmem_alloc(tc::smem_u32(&tmem_slot), TM_COLS);
-  tc::fence_before();
-  __syncthreads();
-  tc::fence_after();
-  const uint32_t tmem = tmem_slot;
-  // Twiddle operand: bulk copy of this x tile's image.
-  if (tid == 0) {
-    tc::mbar_expect_tx(barL, B_BYTES);
-    const uint8_t* gb = Bimg + (size_t)xt * B_BYTES;
-    for (uint32_t q = 0; q < B_BYTES; q += 16384) {
-      const uint32_t n = B_BYTES - q < 16384u ? B_BYTES - q : 16384u;
-      tc::bulk_g2s(tc::smem_u32(sB) + q, gb + q, n, barL);
-    }
-  }
-  // Image operand: 128 rows x 16 chunks of 8 columns, split into [hi | hi | lo].
-  const ImageLoad& ld = a.ld;
-  bool bad = false;
-  for (int j = tid; j < AT_TILE * (AT_TILE / 8); j += AT_NT) {
-    const int r = j / (AT_TILE / 8), c8 = (j % (AT_TILE / 8)) * 8;
-    const int m = y0 + r, x = x0 + c8;
-    float v[8];
-    if (ld.vec4 && m < ld.N && x + 7 < ld.N) {
-      const float4 p = __ldg(reinterpret_cast<const float4*>(ld.in + (size_t)m * ld.N + x));
-      const float4 q = __ldg(reinterpret_cast<const float4*>(ld.in + (size_t)m * ld.N + x + 4));
-      v[0] = p.x; v[1] = p.y; v[2] = p.z; v[3] = p.w; v[4] = q.x; v[5] = q.y; v[6] = q.z; v[7] = q.w;
-    } else {
-#pragma unroll
-      for (int e = 0; e < 8; ++e)
-        v[e] = (m < ld.N && x + e < ld.N) ? __ldg(ld.in + (size_t)m * ld.N + x + e) : 0.f;
-    }
-    __nv_bfloat16 hi[8], lo[8];
-#pragma unroll
-    for (int e = 0; e < 8; ++e) {
-      const bool in_range = m < ld.N && x + e < ld.N;
-      if (in_range) bad |= !isfinite(v[e]);
-      float u = v[e];
-      if (ld.mode == 1) {
-        u = in_range ? 0.5f * (1.f + cosf(v[e])) : 0.f;
-        if (ld.mask_out && in_range) ld.mask_out[(size_t)m * ld.N + x + e] = u;
-      }
-      hi[e] = __float2bfloat16_rn(u);
-      lo[e] = __float2bfloat16_rn(u - __bfloat162float(hi[e]));
-    }
-    const uint4 h4 = *reinterpret_cast<const uint4*>(hi);
-    const uint4 l4 = *reinterpret_cast<const uint4*>(lo);
-    *reinterpret_cast<uint4*>(sA + sw128_offset(AT_TILE, r, c8)) = h4;
-    *reinterpret_cast<uint4*>(sA + sw128_offset(AT_TILE, r, AT_TILE + c8)) = h4;
-    *reinterpret_cast<uint4*>(sA + sw128_offset(AT_TILE, r, 2 * AT_TILE + c8)) = l4;
-  }
-  if (bad) atomicOr(ld.flag, 1);
-  // Generic-proxy writes of the operand must be visible to the tensor cores.
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-  __syncthreads();
-  if (tid == 0) {
-    if (!tc::mbar_wait(barL, 0)) {
-      fail = 1;
-      atomicExch(err, 3);
-    } else {
-      tc::fence_after();
-      constexpr uint32_t idesc = tc::idesc_bf16(AT_TILE, BN);
-      for (int st = 0; st < AQ_K3 / 16; ++st) {
-        const int kb = st >> 2;
-        const uint32_t ko = (uint32_t)(st & 3) * 32;
-        const uint64_t ad = tc::desc_sw128(tc::smem_u32(sA) + kb * (AT_TILE * 128) + ko);
-        const uint64_t bd = tc::desc_sw128(tc::smem_u32(sB) + kb * (BN * 128) + ko);
-        tc::mma_bf16(tmem, ad, bd, idesc, st > 0 ? 1u : 0u);
-      }
-      tc::mma_commit(barM);
-      if (!tc::mbar_wait(barM, 0)) {
-        fail = 2;
-        atomicExch(err, 4);
-        tc::mbar_wait(barM, 0);
-      }
-    }
-  }
-  __syncthreads();
-  tc::fence_after();
-  const bool ok = !fail;
-  if (ok) {
-    // Accumulator -> R staged as [128][BN + 4] floats (the operand tiles are dead).
-    float* Rs = reinterpret_cast<float*>(smem);
-    const int lane_base = (warp & 3) * 32;
-    const int row = lane_base + (tid & 31);
-    for (int cc = (warp >> 2) * 16; cc < BN; cc += 32) {
-      float v[16];
-      tmem_ld16(tmem + ((uint32_t)lane_base << 16) + (uint32_t)cc, v);
-#pragma unroll
-      for (int i = 0; i < 16; ++i) Rs[row * (BN + 4) + cc + i] = v[i];
-    }
-  }
-  tc::fence_before();
-  __syncthreads();
-  if (warp == 0) tc::tmem_dealloc(tmem, TM_COLS);
-  if (ok) analysis_phase2<BN>(reinterpret_cast<float*>(smem), a, y0, 0, yt * gridDim.x + xt);
-}
-
-template <int BN>
-static cudaError_t analysis_tc_t(cudaStream_t s, const AnalysisArgs& a, const void* Bimg, int* err) {
-  const size_t smem = AQ_A_BYTES + (size_t)BN * AQ_K3 * 2 + 1024;
-  cudaError_t e = cudaFuncSetAttribute(analysis_tc_kernel<BN>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
-  const int t = (a.N + AT_TILE - 1) / AT_TILE;
-  analysis_tc_kernel<BN><<<dim3(t, t), AT_NT, smem, s>>>(a, static_cast<const uint8_t*>(Bimg), err);
-  return cudaGetLastError();
-}
-
 // Tile partials of sum_{y, x} T(a, y) A[y][x] tw(c, x) for every 128 x 128 tile:
 // part[tile][a][c], tiles in row-major order of the tile grid.
 cudaError_t launch_analysis(cudaStream_t s, int mode, const float* in, float* mask_out,
                             int* flag, const float* tw, int N, int ncols, const float2* TY,
-                            int nrows_out, int nr, int sym, float2* part, const void* tw_img,
-                            int* err) {
+                            int nrows_out, int nr, int sym, float2* part) {
   const int vec4 = (N % 4 == 0) && (reinterpret_cast<uintptr_t>(in) % 16 == 0);
   AnalysisArgs a{ImageLoad{in, mask_out, flag, N, mode, vec4}, tw, N, ncols, TY, nrows_out,
                  nr, sym, part};
   const int n2 = 2 * ncols;
-  if (tw_img) {  // split-BF16 tensor-core phase 1 (rowsP <= 128)
-    switch (tw_rows_padded(ncols)) {
-      case 16: return analysis_tc_t<16>(s, a, tw_img, err);
-      case 32: return analysis_tc_t<32>(s, a, tw_img, err);
-      case 48: return analysis_tc_t<48>(s, a, tw_img, err);
-      case 64: return analysis_tc_t<64>(s, a, tw_img, err);
-      case 80: return analysis_tc_t<80>(s, a, tw_img, err);
-      case 96: return analysis_tc_t<96>(s, a, tw_img, err);
-      case 112: return analysis_tc_t<112>(s, a, tw_img, err);
-      case 128: return analysis_tc_t<128>(s, a, tw_img, err);
-      default: break;  // wider bands keep the SIMT phase 1
-    }
-  }
   if (n2 <= 32) return analysis_tile_t<2>(s, a);
   if (n2 <= 48) return analysis_tile_t<3>(s, a);
   if (n2 <= 64) return analysis_tile_t<4>(s, a);
@@ -468,6 +252,8 @@ cudaError_t launch_analysis(cudaStream_t s, int mode, const float* in, float* ma
 __global__ void __launch_bounds__(256)
 reduce_tiles_kernel(const float2* __restrict__ part, int tiles, int count, float scale,
                     float2* __restrict__ out) {
+  pdl_trigger();
+  pdl_wait();
   const int o = blockIdx.x * 8 + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
   if (o >= count) return;
@@ -494,8 +280,8 @@ reduce_tiles_kernel(const float2* __restrict__ part, int tiles, int count, float
 
 cudaError_t launch_reduce_tiles(cudaStream_t s, const float2* part, int tiles, int count,
                                 float scale, float2* out) {
-  reduce_tiles_kernel<<<(count + 7) / 8, 256, 0, s>>>(part, tiles, count, scale, out);
-  return cudaGetLastError();
+  return launch_pdl(reduce_tiles_kernel, dim3((count + 7) / 8), dim3(256), 0, s, part, tiles, count,
+                    scale, out);
 }
 
 // ---------------------------------------------------------------- row synthesis
@@ -529,6 +315,8 @@ synth_kernel(const float* __restrict__ AY, const float* __restrict__ Bt, int N, 
   extern __shared__ __align__(16) float stage[];  // [64][SY_SS]
   const int tid = threadIdx.x, tx = tid % SY_BNT, ty = tid / SY_BNT;
   const int m0 = blockIdx.y * SY_TILE, n0 = blockIdx.x * SY_TILE;
+  pdl_trigger();
+  pdl_wait();
   float acc[SY_TM][SY_TN];
 #pragma unroll
   for (int i = 0; i < SY_TM; ++i)
@@ -569,8 +357,7 @@ static cudaError_t launch_synth(cudaStream_t s, const float* AY, const float* Bt
   cudaError_t err = cudaFuncSetAttribute(synth_kernel<Epi>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (err != cudaSuccess) return err;
-  synth_kernel<Epi><<<synth_grid(N), SY_NT, smem, s>>>(AY, Bt, N, kp, e);
-  return cudaGetLastError();
+  return launch_pdl(synth_kernel<Epi>, synth_grid(N), dim3(SY_NT), smem, s, AY, Bt, N, kp, e);
 }
 
 
@@ -626,7 +413,7 @@ band_fields_kernel(const float2* __restrict__ H, const float2* __restrict__ mban
   float2* T = A + Nr * Nc;          // [Nr][BF_CW]
   float2* esc = T + Nr * BF_CW;     // [Nc][BF_CW]
   float2* esr = esc + Nc * BF_CW;   // [Nr][Pr] (staged when stage_tables)
-  for (int i = threadIdx.x; i < Nr * Nc; i += BF_NT) A[i] = cmul(H[(size_t)k * Nr * Nc + i], mband[i]);
+  pdl_trigger();
   for (int i = threadIdx.x; i < Nc * BF_CW; i += BF_NT) {
     const int c = i / BF_CW, jj = i % BF_CW;
     esc[i] = jj < cw ? ESc_t[(size_t)c * Pc + j0 + jj] : make_float2(0.f, 0.f);
@@ -636,6 +423,8 @@ band_fields_kernel(const float2* __restrict__ H, const float2* __restrict__ mban
     for (int i = threadIdx.x; i < Nr * Pr; i += BF_NT) esr[i] = ESr_t[i];
     ESR = esr;
   }
+  pdl_wait();
+  for (int i = threadIdx.x; i < Nr * Nc; i += BF_NT) A[i] = cmul(H[(size_t)k * Nr * Nc + i], mband[i]);
   __syncthreads();
   for (int i = threadIdx.x; i < Nr * BF_CW; i += BF_NT) {
     const int r = i / BF_CW, jj = i % BF_CW;
@@ -675,6 +464,8 @@ size_t band_fields_smem(const BandGeom& g) {
 
 // Forward 2: i[j] = sum_k ik[k][j] in k order.
 __global__ void sum_k_kernel(const float* __restrict__ ik, int K, int n, float* __restrict__ iP) {
+  pdl_trigger();
+  pdl_wait();
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= n) return;
   float s = 0.f;
@@ -698,8 +489,10 @@ band_chat_kernel(const float* __restrict__ iP, int Nr, int Nc, int Pr, int Pc,
   float2* edc = ed + Pr;                             // [Pc][nd]
   float* ip = reinterpret_cast<float*>(edc + Pc * nd);  // [Pr][Pc]
   const int dr = blockIdx.x;
+  pdl_trigger();
   for (int jr = threadIdx.x; jr < Pr; jr += BI_NT) ed[jr] = EDr_t[(size_t)(dr + Nr - 1) * Pr + jr];
   for (int i = threadIdx.x; i < Pc * nd; i += BI_NT) edc[i] = EDc[i];
+  pdl_wait();
   for (int i = threadIdx.x; i < Pr * Pc; i += BI_NT) ip[i] = iP[i];
   __syncthreads();
   for (int jc = threadIdx.x; jc < Pc; jc += BI_NT) {
@@ -740,19 +533,20 @@ static size_t chat_smem(const BandGeom& g) {
 // mode 1 (difference set D, c in [0, 2nc-1), d = c - (nc-1)):
 //   phase = d >= 0 ? conj(TX[d][x]) : TX[-d][x], kappa(a) = a > 0 ? 2 : 1 (Hermitian half).
 // Columns 2*nrows .. kp-1 of Ut are zero-filled by the first row block.
+// With Zk set (adjoint, mode 0) the coefficients are formed here instead of read:
+//   coef[a][c] = scale sum_k w_k conj(H_k[a][c]) Z_k[a][c]   (k in order),
+// each CTA for its own rows.
 constexpr int EX_X = 64, EX_R = 8, EX_NT = 256;
 __global__ void __launch_bounds__(EX_NT)
 expand_kernel(const float2* __restrict__ coef, int nrows, int ncoef, int ld,
               const float2* __restrict__ TX, int N, int mode, int nc, int kp,
-              float* __restrict__ Ut) {
+              float* __restrict__ Ut, const float2* __restrict__ Zk,
+              const float2* __restrict__ H, const float* __restrict__ w, int K, float scale) {
   extern __shared__ float2 se[];
   float2* cf = se;                    // [EX_R][ncoef]
   float2* ph = se + EX_R * ncoef;     // [ncoef][EX_X]
   const int x0 = blockIdx.x * EX_X, a0 = blockIdx.y * EX_R;
-  for (int i = threadIdx.x; i < EX_R * ncoef; i += EX_NT) {
-    const int r = i / ncoef, c = i % ncoef;
-    cf[i] = (a0 + r < nrows) ? coef[(size_t)(a0 + r) * ld + c] : make_float2(0.f, 0.f);
-  }
+  pdl_trigger();
   for (int i = threadIdx.x; i < ncoef * EX_X; i += EX_NT) {
     const int c = i / EX_X, xx = i % EX_X, x = x0 + xx;
     float2 t = make_float2(0.f, 0.f);
@@ -765,6 +559,41 @@ expand_kernel(const float2* __restrict__ coef, int nrows, int ncoef, int ld,
       }
     }
     ph[i] = t;
+  }
+  pdl_wait();
+  if (Zk) {
+    const size_t nb = (size_t)nrows * ncoef;
+    for (int i = threadIdx.x; i < EX_R * ncoef; i += EX_NT) {
+      const int r = i / ncoef, c = i % ncoef;
+      float2 x = make_float2(0.f, 0.f);
+      if (a0 + r < nrows) {
+        const size_t u = (size_t)(a0 + r) * ncoef + c;
+        float2 acc = make_float2(0.f, 0.f);
+        for (int k0 = 0; k0 < K; k0 += 8) {
+          float2 hv[8], zv[8];
+#pragma unroll
+          for (int q = 0; q < 8; ++q)
+            if (k0 + q < K) {
+              hv[q] = H[(size_t)(k0 + q) * nb + u];
+              zv[q] = Zk[(size_t)(k0 + q) * nb + u];
+            }
+#pragma unroll
+          for (int q = 0; q < 8; ++q)
+            if (k0 + q < K) {
+              const float2 t = cmul(conjf2(hv[q]), zv[q]);
+              acc.x = fmaf(w[k0 + q], t.x, acc.x);
+              acc.y = fmaf(w[k0 + q], t.y, acc.y);
+            }
+        }
+        x = make_float2(acc.x * scale, acc.y * scale);
+      }
+      cf[i] = x;
+    }
+  } else {
+    for (int i = threadIdx.x; i < EX_R * ncoef; i += EX_NT) {
+      const int r = i / ncoef, c = i % ncoef;
+      cf[i] = (a0 + r < nrows) ? coef[(size_t)(a0 + r) * ld + c] : make_float2(0.f, 0.f);
+    }
   }
   __syncthreads();
   const int xx = threadIdx.x % EX_X, rq = threadIdx.x / EX_X;  // rq in [0, 4): rows rq, rq + 4
@@ -792,14 +621,16 @@ expand_kernel(const float2* __restrict__ coef, int nrows, int ncoef, int ld,
 }
 
 static cudaError_t launch_expand(cudaStream_t s, const float2* coef, int nrows, int ncoef, int ld,
-                                 const float2* TX, int N, int mode, int nc, int kp, float* Ut) {
+                                 const float2* TX, int N, int mode, int nc, int kp, float* Ut,
+                                 const float2* Zk = nullptr, const float2* H = nullptr,
+                                 const float* w = nullptr, int K = 0, float scale = 0.f) {
   const size_t smem = (size_t)(EX_R * ncoef + ncoef * EX_X) * sizeof(float2);
   cudaError_t e = cudaFuncSetAttribute(expand_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
   if (e != cudaSuccess) return e;
   dim3 grid((N + EX_X - 1) / EX_X, (nrows + EX_R - 1) / EX_R);
-  expand_kernel<<<grid, EX_NT, smem, s>>>(coef, nrows, ncoef, ld, TX, N, mode, nc, kp, Ut);
-  return cudaGetLastError();
+  return launch_pdl(expand_kernel, grid, dim3(EX_NT), smem, s, coef, nrows, ncoef, ld, TX, N, mode,
+                    nc, kp, Ut, Zk, H, w, K, scale);
 }
 
 cudaError_t launch_band_forward(cudaStream_t s, const Cache& c, Field& f, float* ik, float* iP,
@@ -811,18 +642,22 @@ cudaError_t launch_band_forward(cudaStream_t s, const Cache& c, Field& f, float*
   cudaError_t err = cudaFuncSetAttribute(band_fields_kernel,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1);
   if (err != cudaSuccess) return err;
-  band_fields_kernel<<<dim3(g.K, (g.Pc + BF_CW - 1) / BF_CW), BF_NT, sm1, s>>>(
-      c.H, f.mband, c.w, g.Nr, g.Nc, g.Pr, g.Pc, c.ESc_t, c.ESr_t, stage, f.e, ik);
+  err = launch_pdl(band_fields_kernel, dim3(g.K, (g.Pc + BF_CW - 1) / BF_CW), dim3(BF_NT), sm1, s,
+                   c.H, static_cast<const float2*>(f.mband), c.w, g.Nr, g.Nc, g.Pr, g.Pc, c.ESc_t,
+                   c.ESr_t, stage, f.e, ik);
+  if (err != cudaSuccess) return err;
   const int n = g.Pr * g.Pc;
-  sum_k_kernel<<<(n + 255) / 256, 256, 0, s>>>(ik, g.K, n, iP);
+  err = launch_pdl(sum_k_kernel, dim3((n + 255) / 256), dim3(256), 0, s,
+                   static_cast<const float*>(ik), g.K, n, iP);
+  if (err != cudaSuccess) return err;
   const int nd = 2 * g.Nc - 1;
   const size_t smc = chat_smem(g);
   err = cudaFuncSetAttribute(band_chat_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)smc);
   if (err != cudaSuccess) return err;
-  band_chat_kernel<<<g.Nr, BI_NT, smc, s>>>(iP, g.Nr, g.Nc, g.Pr, g.Pc, c.EDr_t, c.EDc,
-                                            1.f / ((float)g.Pr * (float)g.Pc), chat);
-  err = cudaGetLastError();
+  err = launch_pdl(band_chat_kernel, dim3(g.Nr), dim3(BI_NT), smc, s,
+                   static_cast<const float*>(iP), g.Nr, g.Nc, g.Pr, g.Pc, c.EDr_t, c.EDc,
+                   1.f / ((float)g.Pr * (float)g.Pc), chat);
   if (err != cudaSuccess) return err;
   return launch_expand(s, chat, g.Nr, nd, nd, c.TXDc, g.N, 1, g.Nc, g.kp_rows, Ut);
 }
@@ -841,9 +676,11 @@ band_gamma_kernel(const float2* __restrict__ gh, int Nr, int Nc, int Pr, int Pc,
   float2* edr = wv + Nc;         // [na]   column jr of EDr_t
   float2* ghs = edr + na;        // [na][Nc]
   float2* edc = ghs + na * Nc;   // [Nc][Pc] rows Nc-1 .. 2Nc-2 of EDc_t
+  pdl_trigger();
   for (int r = threadIdx.x; r < na; r += blockDim.x) edr[r] = EDr_t[(size_t)r * Pr + jr];
-  for (int i = threadIdx.x; i < na * Nc; i += blockDim.x) ghs[i] = gh[i];
   for (int i = threadIdx.x; i < Nc * Pc; i += blockDim.x) edc[i] = EDc_t[(size_t)(Nc - 1) * Pc + i];
+  pdl_wait();
+  for (int i = threadIdx.x; i < na * Nc; i += blockDim.x) ghs[i] = gh[i];
   __syncthreads();
   for (int c = threadIdx.x; c < Nc; c += blockDim.x) {
     float2 a = make_float2(0.f, 0.f);
@@ -894,19 +731,23 @@ band_z_kernel(const float2* __restrict__ e, const float* __restrict__ gam, int N
   float2* q = esc + Pc * BZ_UW;     // [Pr][Pc]   (staged)
   float2* esr = q + Pr * Pc;        // [Nr][Pr]   (staged)
   const float2* ek = e + (size_t)k * Pr * Pc;
+  pdl_trigger();
   for (int i = threadIdx.x; i < Pc * BZ_UW; i += BF_NT) {
     const int jc = i / BZ_UW, uu = i % BZ_UW;
     esc[i] = uu < uw ? conjf2(ESc[(size_t)jc * Nc + u0 + uu]) : make_float2(0.f, 0.f);
   }
   const float2* ESR = ESr_t;
   if (stage_tables) {
+    for (int i = threadIdx.x; i < Nr * Pr; i += BF_NT) esr[i] = ESr_t[i];
+    ESR = esr;
+  }
+  pdl_wait();
+  if (stage_tables) {
     for (int i = threadIdx.x; i < Pr * Pc; i += BF_NT) {
       const float2 v = ek[i];
       const float gv = gam[i];
       q[i] = make_float2(v.x * gv, v.y * gv);
     }
-    for (int i = threadIdx.x; i < Nr * Pr; i += BF_NT) esr[i] = ESr_t[i];
-    ESR = esr;
   }
   __syncthreads();
   for (int i = threadIdx.x; i < Pr * BZ_UW; i += BF_NT) {
@@ -941,29 +782,16 @@ band_z_kernel(const float2* __restrict__ e, const float* __restrict__ gam, int N
   }
 }
 
-// Adjoint 3: X[u] = scale sum_k w_k conj(H_k(u)) Z_k(u) (k order), one thread per u.
-__global__ void band_x_kernel(const float2* __restrict__ Zk, const float2* __restrict__ H,
-                              const float* __restrict__ w, int K, int nb, float scale,
-                              float2* __restrict__ X) {
-  const int u = blockIdx.x * blockDim.x + threadIdx.x;
-  if (u >= nb) return;
-  float2 acc = make_float2(0.f, 0.f);
-  for (int k = 0; k < K; ++k) {
-    const float2 t = cmul(conjf2(H[(size_t)k * nb + u]), Zk[(size_t)k * nb + u]);
-    acc.x = fmaf(w[k], t.x, acc.x);
-    acc.y = fmaf(w[k], t.y, acc.y);
-  }
-  X[u] = make_float2(acc.x * scale, acc.y * scale);
-}
-
 cudaError_t launch_band_adjoint(cudaStream_t s, const Cache& c, const Field& f, const float2* gh,
-                                double scale, float* gam, float2* Zk, float2* X, float* Vt) {
+                                double scale, float* gam, float2* Zk, float* Vt) {
   const BandGeom& g = c.g;
   const size_t smg = gamma_smem(g);
   cudaError_t e0 = cudaFuncSetAttribute(band_gamma_kernel,
                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smg);
   if (e0 != cudaSuccess) return e0;
-  band_gamma_kernel<<<g.Pr, 256, smg, s>>>(gh, g.Nr, g.Nc, g.Pr, g.Pc, c.EDr_t, c.EDc_t, gam);
+  e0 = launch_pdl(band_gamma_kernel, dim3(g.Pr), dim3(256), smg, s, gh, g.Nr, g.Nc, g.Pr, g.Pc,
+                  c.EDr_t, c.EDc_t, gam);
+  if (e0 != cudaSuccess) return e0;
   const size_t base = (size_t)(g.Pr * BZ_UW + g.Pc * BZ_UW) * sizeof(float2);
   const size_t full = base + (size_t)(g.Pr * g.Pc + g.Nr * g.Pr) * sizeof(float2);
   const int stage = full <= SMEM_STAGE;
@@ -971,20 +799,21 @@ cudaError_t launch_band_adjoint(cudaStream_t s, const Cache& c, const Field& f, 
   cudaError_t err = cudaFuncSetAttribute(band_z_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smz);
   if (err != cudaSuccess) return err;
-  band_z_kernel<<<dim3(g.K, (g.Nc + BZ_UW - 1) / BZ_UW), BF_NT, smz, s>>>(
-      f.e, gam, g.Nr, g.Nc, g.Pr, g.Pc, c.ESc, c.ESr_t, stage, 1.f / ((float)g.Pr * (float)g.Pc),
-      Zk);
-  const int nb = g.Nr * g.Nc;
-  band_x_kernel<<<(nb + 127) / 128, 128, 0, s>>>(Zk, c.H, c.w, g.K, nb, (float)scale, X);
-  err = cudaGetLastError();
+  err = launch_pdl(band_z_kernel, dim3(g.K, (g.Nc + BZ_UW - 1) / BZ_UW), dim3(BF_NT), smz, s,
+                   static_cast<const float2*>(f.e), static_cast<const float*>(gam), g.Nr, g.Nc,
+                   g.Pr, g.Pc, c.ESc, c.ESr_t, stage, 1.f / ((float)g.Pr * (float)g.Pc), Zk);
   if (err != cudaSuccess) return err;
-  return launch_expand(s, X, g.Nr, g.Nc, g.Nc, c.TXSc, g.N, 0, g.Nc, g.kp_rows, Vt);
+  // X = scale sum_k w_k conj(H_k) Z_k is formed inside the expansion.
+  return launch_expand(s, nullptr, g.Nr, g.Nc, g.Nc, c.TXSc, g.N, 0, g.Nc, g.kp_rows, Vt, Zk, c.H,
+                       c.w, g.K, (float)scale);
 }
 
 // ---------------------------------------------------------------- FP64 partial sums
 __global__ void sum_partials_kernel(const double* __restrict__ part, int n, int stride,
                                     double* __restrict__ out) {
   // One warp per component; lanes stride over blocks, then a fixed shuffle tree.
+  pdl_trigger();
+  pdl_wait();
   const int comp = blockIdx.x;
   double s = 0.0;
   for (int i = threadIdx.x; i < n; i += 32) s += part[(size_t)i * stride + comp];
@@ -995,8 +824,7 @@ __global__ void sum_partials_kernel(const double* __restrict__ part, int n, int 
 
 cudaError_t launch_sum_partials(cudaStream_t s, const double* part, int n, int stride,
                                 double* out) {
-  sum_partials_kernel<<<stride, 32, 0, s>>>(part, n, stride, out);
-  return cudaGetLastError();
+  return launch_pdl(sum_partials_kernel, dim3(stride), dim3(32), 0, s, part, n, stride, out);
 }
 
 // ---------------------------------------------------------------- field export

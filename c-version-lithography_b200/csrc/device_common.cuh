@@ -8,6 +8,18 @@
 
 namespace litho_b200 {
 
+// Programmatic dependent launch. Every kernel of an imaging / adjoint chain calls
+// pdl_trigger() first, so that its stream successor may be scheduled while it runs,
+// and pdl_wait() before its first access to global data that an earlier kernel of
+// the stream writes or reads (only the optical cache's constant tables may be
+// touched before it), and before its first global write. pdl_wait returns once the
+// predecessor grid has completed and its memory is visible; both are no-ops for a
+// kernel launched without the programmatic-serialization attribute.
+__device__ __forceinline__ void pdl_trigger() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
   return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
@@ -56,42 +68,53 @@ __device__ __forceinline__ void st4(float* p, size_t i, float4 v, int vec, int n
 
 constexpr int EPI_NT = 256;  // threads of every CTA that runs a synthesis epilogue
 
+// sin / cos for the split-BF16 tensor-core path: Cody-Waite reduction of x by
+// 2 pi with a two-term constant (6.28125, exact in 9 bits so that k * 6.28125 is
+// exact for |k| < 2^15, plus the remainder 2 pi - 6.28125), then the SFU sine
+// or cosine on [-pi, pi]. Absolute error below about 1e-6 for |x| < 1e3: far
+// inside the 1e-3 budget of that path, and a few instructions instead of the
+// full-range library routine, which keeps the unrolled epilogues compact.
+__device__ __forceinline__ float reduce_2pi(float x) {
+  const float k = rintf(x * 0.15915494309189535f);
+  return fmaf(-k, 1.9353071795864769e-3f, fmaf(-k, 6.28125f, x));
+}
+__device__ __forceinline__ float fast_cos(float x) { return __cosf(reduce_2pi(x)); }
+__device__ __forceinline__ float fast_sin(float x) { return __sinf(reduce_2pi(x)); }
+
 // Resist + PE + dL/dI (imaging.cpp:165-168, loss.cpp:16-64, gradient.cpp:121-196).
-struct ResistEpi {
+// FAST (tensor-core path) uses the SFU exponential and reciprocal and rounds each
+// pixel's loss term to FP32 before the FP64 accumulation.
+template <bool FAST>
+struct ResistEpiT {
   ResistEpilogue p;
   int N, vec;
   double pe, pen;
   __device__ __forceinline__ float sigmoid(float I) const {
-    return 1.f / (1.f + expf(-p.alpha * (I - p.thr)));
+    const float z = -p.alpha * (I - p.thr);
+    return FAST ? __fdividef(1.f, 1.f + __expf(z)) : 1.f / (1.f + expf(z));
   }
   __device__ __forceinline__ void one(float I, float T, float pw, float qw, float& W, float& g) {
     W = sigmoid(I);
     const float r = W - T;
-    pe += (double)r * (double)r * (double)pw;
+    pe += FAST ? (double)(r * r * pw) : (double)r * (double)r * (double)pw;
     float s = p.pe_weight * r * pw;
     if (p.penalty != 0.f && T < 0.5f) {
       const float ex = fmaxf(W - p.pen_thr, 0.f);
-      pen += (double)ex * (double)ex * (double)qw;
+      pen += FAST ? (double)(ex * ex * qw) : (double)ex * (double)ex * (double)qw;
       s += p.penalty * ex * qw;
     }
     g = s * W * (1.f - W);
   }
-  __device__ __forceinline__ void store1(int m, int n, float I) {
-    const size_t i = (size_t)m * N + n;
-    if (p.aerial) p.aerial[i] = I;
-    if (p.mode == 0) {
-      if (p.wafer) p.wafer[i] = sigmoid(I);
-      return;
-    }
-    const float T = __ldg(p.target + i);
-    const float pw = p.pe_window ? __ldg(p.pe_window + i) : 1.f;
-    const float qw = p.pen_window ? __ldg(p.pen_window + i) : pw;
-    float W, g;
-    one(I, T, pw, qw, W, g);
-    if (p.wafer) p.wafer[i] = W;
-    p.dldi[i] = g;
-  }
   __device__ __forceinline__ void store4(int m, int n, float4 I, int nvalid) {
+    store4p(m, n, I, pre4(m, n, nvalid), nvalid);
+  }
+  // The per-pixel input (target) fetched before the accumulator is ready, and the
+  // store that consumes it.
+  __device__ __forceinline__ float4 pre4(int m, int n, int nvalid) const {
+    if (p.mode == 0 || nvalid <= 0) return make_float4(0.f, 0.f, 0.f, 0.f);
+    return ld4(p.target, (size_t)m * N + n, vec, nvalid);
+  }
+  __device__ __forceinline__ void store4p(int m, int n, float4 I, float4 T, int nvalid) {
     const size_t i = (size_t)m * N + n;
     if (p.aerial) st4(p.aerial, i, I, vec, nvalid);
     if (p.mode == 0) {
@@ -101,7 +124,6 @@ struct ResistEpi {
       }
       return;
     }
-    const float4 T = ld4(p.target, i, vec, nvalid);
     const float4 one4 = make_float4(1.f, 1.f, 1.f, 1.f);
     const float4 pw = p.pe_window ? ld4(p.pe_window, i, vec, nvalid) : one4;
     const float4 qw = p.pen_window ? ld4(p.pen_window, i, vec, nvalid) : pw;
@@ -112,40 +134,6 @@ struct ResistEpi {
     if (nvalid > 3) one(I.w, T.w, pw.w, qw.w, W.w, g.w);
     if (p.wafer) st4(p.wafer, i, W, vec, nvalid);
     st4(p.dldi, i, g, vec, nvalid);
-  }
-  // V float4 chunks at once: every input load is issued before any store, so
-  // the loads of the batch overlap instead of waiting on one another.
-  template <int V>
-  __device__ __forceinline__ void store4v(const int (&m)[V], const int (&n)[V],
-                                          const float4 (&I)[V], const int (&nv)[V]) {
-    if (p.mode == 0) {
-#pragma unroll
-      for (int q = 0; q < V; ++q)
-        if (nv[q] > 0) store4(m[q], n[q], I[q], nv[q]);
-      return;
-    }
-    float4 T[V], pw[V], qw[V];
-    const float4 one4 = make_float4(1.f, 1.f, 1.f, 1.f);
-#pragma unroll
-    for (int q = 0; q < V; ++q) {
-      const size_t i = (size_t)m[q] * N + n[q];
-      T[q] = nv[q] > 0 ? ld4(p.target, i, vec, nv[q]) : one4;
-      pw[q] = (p.pe_window && nv[q] > 0) ? ld4(p.pe_window, i, vec, nv[q]) : one4;
-      qw[q] = (p.pen_window && nv[q] > 0) ? ld4(p.pen_window, i, vec, nv[q]) : pw[q];
-    }
-#pragma unroll
-    for (int q = 0; q < V; ++q) {
-      if (nv[q] <= 0) continue;
-      const size_t i = (size_t)m[q] * N + n[q];
-      float4 W = make_float4(0.f, 0.f, 0.f, 0.f), g = W;
-      if (nv[q] > 0) one(I[q].x, T[q].x, pw[q].x, qw[q].x, W.x, g.x);
-      if (nv[q] > 1) one(I[q].y, T[q].y, pw[q].y, qw[q].y, W.y, g.y);
-      if (nv[q] > 2) one(I[q].z, T[q].z, pw[q].z, qw[q].z, W.z, g.z);
-      if (nv[q] > 3) one(I[q].w, T[q].w, pw[q].w, qw[q].w, W.w, g.w);
-      if (p.aerial) st4(p.aerial, i, I[q], vec, nv[q]);
-      if (p.wafer) st4(p.wafer, i, W, vec, nv[q]);
-      st4(p.dldi, i, g, vec, nv[q]);
-    }
   }
   // All EPI_NT threads of the CTA must call finish.
   __device__ __forceinline__ void finish() {
@@ -162,60 +150,40 @@ struct ResistEpi {
 };
 
 // dPE/dM, the theta chain -1/2 G sin(theta) and its FP64 squared norm
-// (CTM_Optimizer.cpp:151-152).
-struct GradEpi {
+// (CTM_Optimizer.cpp:151-152). FAST selects fast_sin and per-chunk FP32 norms
+// (tensor-core path).
+template <bool FAST>
+struct GradEpiT {
   GradEpilogue p;
   int N, vec;
   double nrm;
-  __device__ __forceinline__ void store1(int m, int n, float G) {
-    const size_t i = (size_t)m * N + n;
-    if (p.grad_mask) p.grad_mask[i] = G;
-    if (!p.theta) return;
-    const float gt = -0.5f * G * sinf(__ldg(p.theta + i));
-    nrm += (double)gt * gt;
-    p.grad_theta[i] = gt;
-  }
+  __device__ __forceinline__ float sn(float t) const { return FAST ? fast_sin(t) : sinf(t); }
   __device__ __forceinline__ void store4(int m, int n, float4 G, int nvalid) {
+    store4p(m, n, G, pre4(m, n, nvalid), nvalid);
+  }
+  __device__ __forceinline__ float4 pre4(int m, int n, int nvalid) const {
+    if (!p.theta || nvalid <= 0) return make_float4(0.f, 0.f, 0.f, 0.f);
+    return ld4(p.theta, (size_t)m * N + n, vec, nvalid);
+  }
+  __device__ __forceinline__ void store4p(int m, int n, float4 G, float4 th, int nvalid) {
     const size_t i = (size_t)m * N + n;
     if (p.grad_mask) st4(p.grad_mask, i, G, vec, nvalid);
     if (!p.theta) return;
-    const float4 th = ld4(p.theta, i, vec, nvalid);
     float4 gt;
-    gt.x = -0.5f * G.x * sinf(th.x);
-    gt.y = -0.5f * G.y * sinf(th.y);
-    gt.z = -0.5f * G.z * sinf(th.z);
-    gt.w = -0.5f * G.w * sinf(th.w);
-    if (nvalid > 0) nrm += (double)gt.x * gt.x;
-    if (nvalid > 1) nrm += (double)gt.y * gt.y;
-    if (nvalid > 2) nrm += (double)gt.z * gt.z;
-    if (nvalid > 3) nrm += (double)gt.w * gt.w;
-    st4(p.grad_theta, i, gt, vec, nvalid);
-  }
-  template <int V>
-  __device__ __forceinline__ void store4v(const int (&m)[V], const int (&n)[V],
-                                          const float4 (&G)[V], const int (&nv)[V]) {
-    float4 th[V];
-#pragma unroll
-    for (int q = 0; q < V; ++q)
-      th[q] = (p.theta && nv[q] > 0) ? ld4(p.theta, (size_t)m[q] * N + n[q], vec, nv[q])
-                                     : make_float4(0.f, 0.f, 0.f, 0.f);
-#pragma unroll
-    for (int q = 0; q < V; ++q) {
-      if (nv[q] <= 0) continue;
-      const size_t i = (size_t)m[q] * N + n[q];
-      if (p.grad_mask) st4(p.grad_mask, i, G[q], vec, nv[q]);
-      if (!p.theta) continue;
-      float4 gt;
-      gt.x = -0.5f * G[q].x * sinf(th[q].x);
-      gt.y = -0.5f * G[q].y * sinf(th[q].y);
-      gt.z = -0.5f * G[q].z * sinf(th[q].z);
-      gt.w = -0.5f * G[q].w * sinf(th[q].w);
-      if (nv[q] > 0) nrm += (double)gt.x * gt.x;
-      if (nv[q] > 1) nrm += (double)gt.y * gt.y;
-      if (nv[q] > 2) nrm += (double)gt.z * gt.z;
-      if (nv[q] > 3) nrm += (double)gt.w * gt.w;
-      st4(p.grad_theta, i, gt, vec, nv[q]);
+    gt.x = -0.5f * G.x * sn(th.x);
+    gt.y = -0.5f * G.y * sn(th.y);
+    gt.z = -0.5f * G.z * sn(th.z);
+    gt.w = -0.5f * G.w * sn(th.w);
+    if (FAST) {
+      // lanes past the edge hold theta = 0 and G = 0, so they add nothing
+      nrm += (double)(gt.x * gt.x + gt.y * gt.y + gt.z * gt.z + gt.w * gt.w);
+    } else {
+      if (nvalid > 0) nrm += (double)gt.x * gt.x;
+      if (nvalid > 1) nrm += (double)gt.y * gt.y;
+      if (nvalid > 2) nrm += (double)gt.z * gt.z;
+      if (nvalid > 3) nrm += (double)gt.w * gt.w;
     }
+    st4(p.grad_theta, i, gt, vec, nvalid);
   }
   __device__ __forceinline__ void finish() {
     if (!p.theta) return;
@@ -224,6 +192,9 @@ struct GradEpi {
     if (threadIdx.x == 0) p.norm_partial[blockIdx.y * gridDim.x + blockIdx.x] = a;
   }
 };
+
+using ResistEpi = ResistEpiT<false>;
+using GradEpi = GradEpiT<false>;
 
 inline int aligned16(const void* p) {
   return p == nullptr || reinterpret_cast<uintptr_t>(p) % 16 == 0;

@@ -64,12 +64,16 @@ struct Cache {
   float2* EDr_t = nullptr;  // [2Nr-1][Pr]: e^{+2 pi i d j / Pr}, d = -(Nr-1)..Nr-1
   float2* EDc_t = nullptr;  // [2Nc-1][Pc]: e^{+2 pi i d j / Pc}, d = -(Nc-1)..Nc-1
   float2* EDc = nullptr;    // [Pc][2Nc-1]: the same, transposed
-  // Split-BF16 tensor-core operand images of AYS / AYD (see synth_tc.cu).
+  // Split-BF16 tensor-core operand images (tc2.cu), built when tc2_supported:
+  // the row-synthesis twiddles AYS / AYD (rows y), the row-analysis column
+  // twiddles TXS / TXD (rows f, K tiles of x) and the row twiddles TYS / TYD
+  // (rows 2r / 2r + 1 = Re / Im, K tiles of y).
   void* AYS_img = nullptr;
   void* AYD_img = nullptr;
-  // Split-BF16 tensor-core images of the row-analysis twiddles TXS / TXD.
   void* TXS_img = nullptr;
   void* TXD_img = nullptr;
+  void* TYS_img = nullptr;
+  void* TYD_img = nullptr;
   int device = 0;
 };
 
@@ -94,6 +98,9 @@ struct Context {
   bool own_stream = false;
   int precision = LITHO_PRECISION_FP32;
   Scratch scratch;
+  Scratch host_stage;            // device staging of the host-buffer entry points
+  cudaStream_t aux = nullptr;    // upload stream of the host-buffer entry points
+  cudaEvent_t ev_aux[2] = {};    // [0] theta uploaded (main stream), [1] target uploaded (aux)
   double* d_red = nullptr;       // FP64 reduction partials
   size_t red_cap = 0;
   double* h_red = nullptr;       // pinned host mirror for results
@@ -121,6 +128,25 @@ struct Context {
   int ensure_red(size_t n);
 };
 
+// ---------------------------------------------------------------- launch helper
+// Launch with programmatic stream serialization (the kernel must follow the
+// pdl_trigger / pdl_wait protocol of device_common.cuh).
+template <typename... KArgs, typename... Args>
+cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                       cudaStream_t s, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
+
 // ---------------------------------------------------------------- kernels
 // All launchers return cudaGetLastError() of their launches.
 // Tile analysis: for every 128 x 128 tile t of the image A (A = in for mode 0,
@@ -129,15 +155,9 @@ struct Context {
 // with tw = [2 ncols][N] real rows (Re, Im) and T(a, y) = TY[a][y] (sym 0,
 // a < nrows_out) or, for sym 1, d = a - (nr - 1), TY[d][y] / conj(TY[-d][y]).
 int analysis_tiles(int N);
-// tw_img (nullable): the split-BF16 tensor-core image of tw (launch_pack_tw);
-// when set, phase 1 runs on tcgen05 and err receives a code if a bounded wait
-// of the kernel expires.
 cudaError_t launch_analysis(cudaStream_t s, int mode, const float* in, float* mask_out,
                             int* flag, const float* tw, int N, int ncols, const float2* TY,
-                            int nrows_out, int nr, int sym, float2* part, const void* tw_img,
-                            int* err);
-size_t tw_image_bytes(int N, int ncols);
-cudaError_t launch_pack_tw(cudaStream_t s, const float* tw, int ncols, int N, void* dst);
+                            int nrows_out, int nr, int sym, float2* part);
 // out[o] = scale * sum_t part[t][o] (fixed order).
 cudaError_t launch_reduce_tiles(cudaStream_t s, const float2* part, int tiles, int count,
                                 float scale, float2* out);
@@ -147,9 +167,9 @@ size_t band_fields_smem(const BandGeom& g);
 size_t band_max_smem(const BandGeom& g);
 cudaError_t launch_band_forward(cudaStream_t s, const Cache& c, Field& f, float* ik, float* iP,
                                 float2* chat, float* Ut);
-// Small-grid stage of the adjoint: gh (the D-band DFT of dL/dI) -> gam, Zk, X and Vt.
+// Small-grid stage of the adjoint: gh (the D-band DFT of dL/dI) -> gam, Zk and Vt.
 cudaError_t launch_band_adjoint(cudaStream_t s, const Cache& c, const Field& f, const float2* gh,
-                                double scale, float* gam, float2* Zk, float2* X, float* Vt);
+                                double scale, float* gam, float2* Zk, float* Vt);
 
 // Row synthesis: out[y][x] = sum_f AY[y][f] * Bt[x][f] with a fused epilogue.
 struct ResistEpilogue {
@@ -185,16 +205,30 @@ cudaError_t launch_pe_dldi(cudaStream_t s, const float* w, const float* t, const
                            const float* pen_win, float pe_weight, float penalty, float pen_thr,
                            size_t n, float* dldi, double* partial, int* nblocks);
 
-// Tensor-core row synthesis (synth_tc.cu). Images: split-BF16 K-major SW128
-// tiles of an FP32 [rows][kp] matrix (tile_rows 128 for the twiddle operand,
-// 256 for the band operand; order 0 = [hi, hi, lo], 1 = [hi, lo, hi]).
-size_t tc_image_bytes(int rows, int kp, int tile_rows);
-cudaError_t launch_pack_split(cudaStream_t s, const float* src, int rows, int kp, int tile_rows,
-                              int order, void* dst);
-cudaError_t launch_synth_resist_tc(cudaStream_t s, const void* Aimg, const void* Bimg, int N,
-                                   int kp, const ResistEpilogue& ep, int* err, int* nblocks);
-cudaError_t launch_synth_grad_tc(cudaStream_t s, const void* Aimg, const void* Bimg, int N, int kp,
-                                 const GradEpilogue& ep, int* err, int* nblocks);
+// Split-BF16 tensor-core passes (tc2.cu). err receives a code (1..6) when a
+// bounded wait of a kernel expires.
+// Tile analysis, same partials as launch_analysis: tx_img / ty_img are the
+// images of tw and TY (launch_pack_tc2_tx / _ty); needs tc2_analysis_supported.
+bool tc2_analysis_supported(int ncols, int nr);
+size_t tc2_tx_image_bytes(int N, int ncols);
+size_t tc2_ty_image_bytes(int N);
+cudaError_t launch_pack_tc2_tx(cudaStream_t s, const float* tw, int ncols, int N, void* dst);
+cudaError_t launch_pack_tc2_ty(cudaStream_t s, const float2* T, int nr, int N, void* dst);
+cudaError_t launch_analysis_tc2(cudaStream_t s, int mode, const float* in, float* mask_out,
+                                int* flag, int N, int ncols, int nrows_out, int nr, int sym,
+                                float2* part, const void* tx_img, const void* ty_img, int* err);
+// Row synthesis: Aimg = image of AY ([N][kp], launch_pack_tc2_rows), Bimg = image
+// of the band operand Bt ([N][kp]); kp % 16 == 0 and kp <= 128.
+size_t tc2_rows_image_bytes(int N, int kp);
+cudaError_t launch_pack_tc2_rows(cudaStream_t s, const float* src, int N, int kp, void* dst);
+cudaError_t launch_synth_resist_tc2(cudaStream_t s, const void* Aimg, const void* Bimg, int N,
+                                    int kp, const ResistEpilogue& ep, int* err, int* nblocks);
+cudaError_t launch_synth_grad_tc2(cudaStream_t s, const void* Aimg, const void* Bimg, int N,
+                                  int kp, const GradEpilogue& ep, int* err, int* nblocks);
+// The tensor-core path needs kp <= 128 and 2 Nc <= 128 (bands up to 64 x 64).
+inline bool tc2_supported(const BandGeom& g) {
+  return g.kp_rows <= 128 && tc2_analysis_supported(g.Nc, g.Nr);
+}
 
 // Level set (levelset.cu). what: 0 delta (+|Vn|), 1 kappa term, 2 normal,
 // 3 RK2 stage 1, 4 RK2 stage 2 (+ mask).

@@ -3,7 +3,9 @@ FullChipCTMOptimizer) against the FP64 full-chip oracle, through the C ABI.
 
 Tolerances (FP32 path): tile copies bit-exact; raw and exchanged gradients
 relative L2 <= 1e-4 per tile; data and CEPT losses relative 1e-5; full-chip CTM
-loss history relative 1e-4 and best global mask max|d| <= 1e-4.
+loss history relative 1e-5 at the start and 1e-3 after three fixed steps, best
+global mask max|d| <= 1e-3. Optics: the 193 nm / NA 1.35 annular SOCS cache
+(36 kernels) on 128 x 128 tiles of 4 nm pixels.
 """
 import importlib
 
@@ -12,11 +14,12 @@ import pytest
 
 from oracle import fullchip_oracle as fc
 from oracle import imaging_oracle as io
+from oracle import optics_oracle as oo
 
 torch = pytest.importorskip("torch")
 pytestmark = pytest.mark.gpu
 
-THR, ALPHA = 0.225, 50.0
+THR, ALPHA = 0.1, 50.0
 
 
 @pytest.fixture(scope="module")
@@ -34,11 +37,7 @@ def FC():
 
 @pytest.fixture(scope="module")
 def band128():
-    wl = importlib.import_module("c-version-lithography_b200.workloads")
-    band, r0, c0, w, wss = wl.synthetic_socs_band()
-    oc = io.OracleCache(N=128, kernels=list(wl.band_to_dense(band, r0, c0, 128)),
-                        source_ws=np.array([wss]), eigenvalues=tuple(w))
-    return oc, wl
+    return oo.prepare(128, 4.0, 193.0, 1.35, 0.6, 0.9, use_socs=True), None
 
 
 def rel_l2(a, b):
@@ -104,7 +103,9 @@ def test_exchange_matches_oracle(L, FC, band128, oi):
     target = make_target(cfg[0], cfg[1], oi)
     rng = np.random.default_rng(10 + oi)
     theta_g = io.initialize_theta(target) + 0.3 * rng.standard_normal(target.shape)
-    masks32 = [io.theta_to_mask(fc.extract_local_tile(theta_g, t)).astype(np.float32)
+    # independent per-tile perturbations, so guards and neighbour Cores disagree
+    masks32 = [io.theta_to_mask(fc.extract_local_tile(theta_g, t)
+                                + 0.05 * rng.standard_normal((meta.tile_size,) * 2)).astype(np.float32)
                for t in meta.tiles]
     masks = [m.astype(np.float64) for m in masks32]
     opts = OPTION_SETS[oi]
@@ -144,10 +145,11 @@ def test_fullchip_ctm_matches_oracle(L, FC, band128):
                                               gradient_options=FC.MicroGradientOptions(**opts)))
     hist = [h.loss for h in res.history]
     assert len(hist) == 4
+    assert abs(hist[0] - ref["history"][0]) <= 1e-5 * ref["history"][0]
     for a, b in zip(hist, ref["history"]):
-        assert abs(a - b) <= 1e-4 * b
+        assert abs(a - b) <= 1e-3 * b
     assert res.best_iteration == ref["best"]["iteration"]
-    assert np.max(np.abs(cpu(res.global_mask) - ref["global_mask"])) < 1e-4
+    assert np.max(np.abs(cpu(res.global_mask) - ref["global_mask"])) < 1e-3
     # theta outside each tile's update window keeps its initial value
     init = part.extract_all(optz.initialize_theta(torch.from_numpy(target.astype(np.float32)).cuda(),
                                                   torch))

@@ -302,3 +302,31 @@ def test_ctm_gd_and_lbfgs_stopping(L):
     _, hist, _ = io.ctm_gradient_descent(target, oc, 0.25, 85.0, 3, 0.9, 0.0)
     for a, b in zip(gd3.error_history, hist):
         assert abs(a - b) <= 1e-4 * b
+
+
+@pytest.mark.parametrize("precision", ["fp32", "bf16x3"])
+def test_ctm_evaluate_host_buffers(L, wl, precision):
+    """litho_ctm_evaluate_host (host buffers, overlapped uploads) equals the device-buffer call."""
+    import ctypes
+    N = 256
+    band, r0, c0, w, wss = wl.synthetic_socs_band()
+    ctx = L.Context()
+    ctx.set_precision(precision)
+    cache = L.ImagingCache.from_band(N, band, r0, c0, w, wss, ctx=ctx)
+    rng = np.random.default_rng(5)
+    theta = (rng.random((N, N)) * 3.0).astype(np.float32)
+    target = (rng.random((N, N)) > 0.5).astype(np.float32)
+    opt = L.CTMOptimizer(cache, target, 0.02, 50.0, iterations=1)
+    loss_d, g_d, norm_d = opt.evaluate(torch.from_numpy(theta).cuda())
+    g_d = g_d.cpu().numpy()
+    field = L.Field(cache)
+    for _ in range(2):
+        h_theta = torch.from_numpy(theta).pin_memory()
+        h_target = torch.from_numpy(target).pin_memory()
+        h_grad = torch.empty((N, N), dtype=torch.float32).pin_memory()
+        loss, norm = ctypes.c_double(), ctypes.c_double()
+        ctx._check(ctx.lib.litho_ctm_evaluate_host(
+            ctx.handle, cache.handle, field.handle, h_theta.data_ptr(), h_target.data_ptr(),
+            0.02, 50.0, h_grad.data_ptr(), ctypes.byref(loss), ctypes.byref(norm)))
+        assert loss.value == loss_d and norm.value == norm_d
+        assert np.array_equal(h_grad.numpy(), g_d)
