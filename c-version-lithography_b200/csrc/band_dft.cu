@@ -386,11 +386,24 @@ cudaError_t launch_synth_grad(cudaStream_t s, const float* AY, const float* Bt, 
 // from global memory (L2-resident), with the same arithmetic.
 constexpr size_t SMEM_STAGE = 200 * 1024;
 
-template <class T>
-__device__ __forceinline__ const T* stage_copy(T* dst, const T* src, int n, bool use) {
-  if (!use) return src;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
-  return dst;
+// dst[i] = load(i) for i < n, the NT threads of the CTA striding through i: every
+// thread issues B loads before its B shared-memory stores, so the global (L2)
+// latencies of a staging pass overlap instead of adding up.
+template <int NT, int B = 8, class T, class Load>
+__device__ __forceinline__ void fill_batched(T* dst, int n, Load load) {
+  for (int base = threadIdx.x; base < n; base += NT * B) {
+    T v[B];
+#pragma unroll
+    for (int q = 0; q < B; ++q) {
+      const int i = base + q * NT;
+      if (i < n) v[q] = load(i);
+    }
+#pragma unroll
+    for (int q = 0; q < B; ++q) {
+      const int i = base + q * NT;
+      if (i < n) dst[i] = v[q];
+    }
+  }
 }
 
 // Forward 1: grid (K, column chunks of the small grid). CTA (k, q) owns small-grid
@@ -414,17 +427,17 @@ band_fields_kernel(const float2* __restrict__ H, const float2* __restrict__ mban
   float2* esc = T + Nr * BF_CW;     // [Nc][BF_CW]
   float2* esr = esc + Nc * BF_CW;   // [Nr][Pr] (staged when stage_tables)
   pdl_trigger();
-  for (int i = threadIdx.x; i < Nc * BF_CW; i += BF_NT) {
+  fill_batched<BF_NT>(esc, Nc * BF_CW, [&](int i) {
     const int c = i / BF_CW, jj = i % BF_CW;
-    esc[i] = jj < cw ? ESc_t[(size_t)c * Pc + j0 + jj] : make_float2(0.f, 0.f);
-  }
+    return jj < cw ? ESc_t[(size_t)c * Pc + j0 + jj] : make_float2(0.f, 0.f);
+  });
   const float2* ESR = ESr_t;
   if (stage_tables) {
-    for (int i = threadIdx.x; i < Nr * Pr; i += BF_NT) esr[i] = ESr_t[i];
+    fill_batched<BF_NT>(esr, Nr * Pr, [&](int i) { return ESr_t[i]; });
     ESR = esr;
   }
   pdl_wait();
-  for (int i = threadIdx.x; i < Nr * Nc; i += BF_NT) A[i] = cmul(H[(size_t)k * Nr * Nc + i], mband[i]);
+  fill_batched<BF_NT>(A, Nr * Nc, [&](int i) { return cmul(H[(size_t)k * Nr * Nc + i], mband[i]); });
   __syncthreads();
   for (int i = threadIdx.x; i < Nr * BF_CW; i += BF_NT) {
     const int r = i / BF_CW, jj = i % BF_CW;
@@ -490,10 +503,10 @@ band_chat_kernel(const float* __restrict__ iP, int Nr, int Nc, int Pr, int Pc,
   float* ip = reinterpret_cast<float*>(edc + Pc * nd);  // [Pr][Pc]
   const int dr = blockIdx.x;
   pdl_trigger();
-  for (int jr = threadIdx.x; jr < Pr; jr += BI_NT) ed[jr] = EDr_t[(size_t)(dr + Nr - 1) * Pr + jr];
-  for (int i = threadIdx.x; i < Pc * nd; i += BI_NT) edc[i] = EDc[i];
+  fill_batched<BI_NT>(ed, Pr, [&](int jr) { return EDr_t[(size_t)(dr + Nr - 1) * Pr + jr]; });
+  fill_batched<BI_NT>(edc, Pc * nd, [&](int i) { return EDc[i]; });
   pdl_wait();
-  for (int i = threadIdx.x; i < Pr * Pc; i += BI_NT) ip[i] = iP[i];
+  fill_batched<BI_NT>(ip, Pr * Pc, [&](int i) { return iP[i]; });
   __syncthreads();
   for (int jc = threadIdx.x; jc < Pc; jc += BI_NT) {
     float2 a = make_float2(0.f, 0.f), b = a;
@@ -547,7 +560,7 @@ expand_kernel(const float2* __restrict__ coef, int nrows, int ncoef, int ld,
   float2* ph = se + EX_R * ncoef;     // [ncoef][EX_X]
   const int x0 = blockIdx.x * EX_X, a0 = blockIdx.y * EX_R;
   pdl_trigger();
-  for (int i = threadIdx.x; i < ncoef * EX_X; i += EX_NT) {
+  fill_batched<EX_NT>(ph, ncoef * EX_X, [&](int i) {
     const int c = i / EX_X, xx = i % EX_X, x = x0 + xx;
     float2 t = make_float2(0.f, 0.f);
     if (x < N) {
@@ -558,8 +571,8 @@ expand_kernel(const float2* __restrict__ coef, int nrows, int ncoef, int ld,
         t = d >= 0 ? conjf2(TX[(size_t)d * N + x]) : TX[(size_t)(-d) * N + x];
       }
     }
-    ph[i] = t;
-  }
+    return t;
+  });
   pdl_wait();
   if (Zk) {
     const size_t nb = (size_t)nrows * ncoef;
@@ -590,10 +603,10 @@ expand_kernel(const float2* __restrict__ coef, int nrows, int ncoef, int ld,
       cf[i] = x;
     }
   } else {
-    for (int i = threadIdx.x; i < EX_R * ncoef; i += EX_NT) {
+    fill_batched<EX_NT>(cf, EX_R * ncoef, [&](int i) {
       const int r = i / ncoef, c = i % ncoef;
-      cf[i] = (a0 + r < nrows) ? coef[(size_t)(a0 + r) * ld + c] : make_float2(0.f, 0.f);
-    }
+      return (a0 + r < nrows) ? coef[(size_t)(a0 + r) * ld + c] : make_float2(0.f, 0.f);
+    });
   }
   __syncthreads();
   const int xx = threadIdx.x % EX_X, rq = threadIdx.x / EX_X;  // rq in [0, 4): rows rq, rq + 4
@@ -677,10 +690,10 @@ band_gamma_kernel(const float2* __restrict__ gh, int Nr, int Nc, int Pr, int Pc,
   float2* ghs = edr + na;        // [na][Nc]
   float2* edc = ghs + na * Nc;   // [Nc][Pc] rows Nc-1 .. 2Nc-2 of EDc_t
   pdl_trigger();
-  for (int r = threadIdx.x; r < na; r += blockDim.x) edr[r] = EDr_t[(size_t)r * Pr + jr];
-  for (int i = threadIdx.x; i < Nc * Pc; i += blockDim.x) edc[i] = EDc_t[(size_t)(Nc - 1) * Pc + i];
+  fill_batched<256>(edr, na, [&](int r) { return EDr_t[(size_t)r * Pr + jr]; });
+  fill_batched<256>(edc, Nc * Pc, [&](int i) { return EDc_t[(size_t)(Nc - 1) * Pc + i]; });
   pdl_wait();
-  for (int i = threadIdx.x; i < na * Nc; i += blockDim.x) ghs[i] = gh[i];
+  fill_batched<256>(ghs, na * Nc, [&](int i) { return gh[i]; });
   __syncthreads();
   for (int c = threadIdx.x; c < Nc; c += blockDim.x) {
     float2 a = make_float2(0.f, 0.f);
@@ -732,22 +745,22 @@ band_z_kernel(const float2* __restrict__ e, const float* __restrict__ gam, int N
   float2* esr = q + Pr * Pc;        // [Nr][Pr]   (staged)
   const float2* ek = e + (size_t)k * Pr * Pc;
   pdl_trigger();
-  for (int i = threadIdx.x; i < Pc * BZ_UW; i += BF_NT) {
+  fill_batched<BF_NT>(esc, Pc * BZ_UW, [&](int i) {
     const int jc = i / BZ_UW, uu = i % BZ_UW;
-    esc[i] = uu < uw ? conjf2(ESc[(size_t)jc * Nc + u0 + uu]) : make_float2(0.f, 0.f);
-  }
+    return uu < uw ? conjf2(ESc[(size_t)jc * Nc + u0 + uu]) : make_float2(0.f, 0.f);
+  });
   const float2* ESR = ESr_t;
   if (stage_tables) {
-    for (int i = threadIdx.x; i < Nr * Pr; i += BF_NT) esr[i] = ESr_t[i];
+    fill_batched<BF_NT>(esr, Nr * Pr, [&](int i) { return ESr_t[i]; });
     ESR = esr;
   }
   pdl_wait();
   if (stage_tables) {
-    for (int i = threadIdx.x; i < Pr * Pc; i += BF_NT) {
+    fill_batched<BF_NT>(q, Pr * Pc, [&](int i) {
       const float2 v = ek[i];
       const float gv = gam[i];
-      q[i] = make_float2(v.x * gv, v.y * gv);
-    }
+      return make_float2(v.x * gv, v.y * gv);
+    });
   }
   __syncthreads();
   for (int i = threadIdx.x; i < Pr * BZ_UW; i += BF_NT) {
