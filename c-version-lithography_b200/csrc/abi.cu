@@ -58,7 +58,7 @@ void free_cache(Cache* c) {
 
 // Scratch layout of one imaging + adjoint evaluation.
 struct Layout {
-  size_t part, gh, ik, iP, chat, Ut, Vt, dldi, gam, Zk, rows_tmp, img, total;
+  size_t part, gh, ik, iP, chat, X, Ut, Vt, dldi, gam, Zk, rows_tmp, img, total;
   int tiles;
 };
 
@@ -82,6 +82,7 @@ Layout make_layout(const BandGeom& g) {
   L.gam = take((size_t)g.Pr * g.Pc * sizeof(float));
   L.Zk = take((size_t)g.K * g.Nr * g.Nc * sizeof(float2));
   L.chat = take((size_t)g.Nr * (2 * g.Nc - 1) * sizeof(float2));
+  L.X = take((size_t)g.Nr * g.Nc * sizeof(float2));
   L.rows_tmp = take((size_t)g.Nr * N * sizeof(float2));
   L.img = take(tc2_supported(g) ? tc2_rows_image_bytes(N, g.kp_rows) : 16);  // band operand image
   L.total = off;
@@ -545,10 +546,13 @@ int check_launch(Context* ctx, cudaError_t e, const char* what) {
 }
 
 // Forward: tile analysis -> tile reduction -> small-grid band stage -> row
-// synthesis with the fused resist epilogue. input_mode 1 reads theta.
+// synthesis with the fused resist epilogue. input_mode 1 reads theta. With
+// fuse_adjoint (tensor-core path, ep.mode 1) the synthesis also runs the adjoint
+// tile analysis of dL/dI, leaving its tile partials in L.part for run_adjoint
+// with analysed set; dL/dI is then not stored.
 int run_forward(Context* ctx, const Cache& c, Field& f, const Layout& L, int input_mode,
                 const float* input, float* mask_out, ResistEpilogue ep, int* nblocks,
-                cudaEvent_t before_synthesis = nullptr) {
+                cudaEvent_t before_synthesis = nullptr, bool fuse_adjoint = false) {
   const BandGeom& g = c.g;
   cudaStream_t s = ctx->stream;
   int* flag = reinterpret_cast<int*>(ctx->d_red + RED_FLAG);
@@ -574,7 +578,8 @@ int run_forward(Context* ctx, const Cache& c, Field& f, const Layout& L, int inp
   if (st) return st;
   ctx->stage_begin(2);
   st = check_launch(ctx, launch_band_forward(s, c, f, at<float>(ctx, L.ik), at<float>(ctx, L.iP),
-                                             at<float2>(ctx, L.chat), at<float>(ctx, L.Ut)),
+                                             at<float2>(ctx, L.chat), at<float>(ctx, L.Ut),
+                                             tc ? at<void>(ctx, L.img) : nullptr),
                     "band forward");
   ctx->stage_end(2);
   if (st) return st;
@@ -583,14 +588,16 @@ int run_forward(Context* ctx, const Cache& c, Field& f, const Layout& L, int inp
   ctx->stage_begin(3);
   if (tc) {
     int* err = reinterpret_cast<int*>(ctx->d_red + RED_FLAG) + 1;
-    st = check_launch(ctx, launch_pack_tc2_rows(s, at<float>(ctx, L.Ut), g.N, g.kp_rows,
-                                                at<void>(ctx, L.img)),
-                      "band operand packing");
-    if (!st)
+    if (fuse_adjoint)
+      st = check_launch(ctx, launch_synth_resist_analysis_tc2(
+                                 s, c.AYD_img, at<void>(ctx, L.img), g.N, g.kp_rows, ep, g.Nc,
+                                 g.Nr, at<float2>(ctx, L.part), flag, c.TXD_img, c.TYD_img, err,
+                                 nblocks),
+                        "tensor-core row synthesis with adjoint tile analysis");
+    else
       st = check_launch(ctx, launch_synth_resist_tc2(s, c.AYD_img, at<void>(ctx, L.img), g.N,
                                                      g.kp_rows, ep, err, nblocks),
                         "tensor-core row synthesis");
-    ctx->launches += 1;
   } else {
     st = check_launch(ctx, launch_synth_resist(s, c.AYD, at<float>(ctx, L.Ut), g.N, g.kp_rows, ep,
                                                nblocks),
@@ -603,7 +610,7 @@ int run_forward(Context* ctx, const Cache& c, Field& f, const Layout& L, int inp
 }
 
 int run_adjoint(Context* ctx, const Cache& c, const Field& f, const Layout& L, const float* dldi,
-                double scale, GradEpilogue ep, int* nblocks) {
+                double scale, GradEpilogue ep, int* nblocks, bool analysed = false) {
   const BandGeom& g = c.g;
   cudaStream_t s = ctx->stream;
   int* flag = reinterpret_cast<int*>(ctx->d_red + RED_FLAG);
@@ -611,7 +618,9 @@ int run_adjoint(Context* ctx, const Cache& c, const Field& f, const Layout& L, c
   int st;
   ctx->stage_begin(4);
   const bool tc = ctx->precision == LITHO_PRECISION_BF16X3 && c.TXD_img;
-  if (tc)
+  if (analysed)
+    st = LITHO_OK;  // the partials are already in L.part
+  else if (tc)
     st = check_launch(ctx, launch_analysis_tc2(s, 0, dldi, nullptr, flag, g.N, g.Nc, na, g.Nr, 1,
                                                at<float2>(ctx, L.part), c.TXD_img, c.TYD_img,
                                                flag + 1),
@@ -631,28 +640,24 @@ int run_adjoint(Context* ctx, const Cache& c, const Field& f, const Layout& L, c
   ctx->stage_begin(6);
   st = check_launch(ctx, launch_band_adjoint(s, c, f, at<float2>(ctx, L.gh), scale,
                                              at<float>(ctx, L.gam), at<float2>(ctx, L.Zk),
-                                             at<float>(ctx, L.Vt)),
+                                             at<float2>(ctx, L.X), at<float>(ctx, L.Vt),
+                                             tc ? at<void>(ctx, L.img) : nullptr),
                     "band adjoint");
   ctx->stage_end(6);
   if (st) return st;
   ctx->stage_begin(7);
   if (tc) {
     int* err = reinterpret_cast<int*>(ctx->d_red + RED_FLAG) + 1;
-    st = check_launch(ctx, launch_pack_tc2_rows(s, at<float>(ctx, L.Vt), g.N, g.kp_rows,
-                                                at<void>(ctx, L.img)),
-                      "band operand packing");
-    if (!st)
-      st = check_launch(ctx, launch_synth_grad_tc2(s, c.AYS_img, at<void>(ctx, L.img), g.N,
-                                                   g.kp_rows, ep, err, nblocks),
-                        "tensor-core adjoint row synthesis");
-    ctx->launches += 1;
+    st = check_launch(ctx, launch_synth_grad_tc2(s, c.AYS_img, at<void>(ctx, L.img), g.N,
+                                                 g.kp_rows, ep, err, nblocks),
+                      "tensor-core adjoint row synthesis");
   } else {
     st = check_launch(ctx, launch_synth_grad(s, c.AYS, at<float>(ctx, L.Vt), g.N, g.kp_rows, ep,
                                              nblocks),
                       "adjoint row synthesis");
   }
   ctx->stage_end(7);
-  ctx->launches += 7;
+  ctx->launches += analysed ? 6 : 7;  // analysis, reduction, gamma, Z, X, expansion, synthesis
   return st;
 }
 
@@ -862,7 +867,9 @@ static int ctm_evaluate_impl(litho_ctx* ctx, const litho_cache* cache, litho_fie
   ep.dldi = at<float>(ctx, L.dldi);
   ep.loss_partial = ctx->d_red + RED_PART;
   int nb = 0;
-  st = run_forward(ctx, *cache, *f, L, 1, d_theta, d_mask, ep, &nb, target_ready);
+  // Tensor-core path: the resist synthesis also runs the adjoint tile analysis.
+  const bool fuse = ctx->precision == LITHO_PRECISION_BF16X3 && cache->TXD_img != nullptr;
+  st = run_forward(ctx, *cache, *f, L, 1, d_theta, d_mask, ep, &nb, target_ready, fuse);
   if (!st)
     st = check_launch(ctx, launch_sum_partials(ctx->stream, ctx->d_red + RED_PART, nb, 2,
                                                ctx->d_red + RED_SUM),
@@ -873,7 +880,8 @@ static int ctm_evaluate_impl(litho_ctx* ctx, const litho_cache* cache, litho_fie
   gp.grad_theta = d_grad_theta;
   gp.norm_partial = ctx->d_red + RED_PART + 2 * (size_t)nb;
   int nb2 = 0;
-  if (!st) st = run_adjoint(ctx, *cache, *f, L, at<float>(ctx, L.dldi), 4.0 * alpha, gp, &nb2);
+  if (!st)
+    st = run_adjoint(ctx, *cache, *f, L, at<float>(ctx, L.dldi), 4.0 * alpha, gp, &nb2, fuse);
   if (!st)
     st = check_launch(ctx, launch_sum_partials(ctx->stream, gp.norm_partial, nb2, 1,
                                                ctx->d_red + RED_SUM + 2),

@@ -18,7 +18,10 @@
 
 #include <algorithm>
 
+#include <cuda_bf16.h>
+
 #include "device_common.cuh"
+#include "tc_ptx.cuh"
 
 namespace litho_b200 {
 
@@ -546,15 +549,15 @@ static size_t chat_smem(const BandGeom& g) {
 // mode 1 (difference set D, c in [0, 2nc-1), d = c - (nc-1)):
 //   phase = d >= 0 ? conj(TX[d][x]) : TX[-d][x], kappa(a) = a > 0 ? 2 : 1 (Hermitian half).
 // Columns 2*nrows .. kp-1 of Ut are zero-filled by the first row block.
-// With Zk set (adjoint, mode 0) the coefficients are formed here instead of read:
-//   coef[a][c] = scale sum_k w_k conj(H_k[a][c]) Z_k[a][c]   (k in order),
-// each CTA for its own rows.
+// With img set (tensor-core path) the result goes
+// straight into the split-BF16 operand image of the row synthesis instead of Ut:
+// x tile x / 128 at img + (x / 128) * img_tile_bytes, hi of column f at
+// sw128_offset(128, x % 128, f) and lo at sw128_offset(128, x % 128, kp + f).
 constexpr int EX_X = 64, EX_R = 8, EX_NT = 256;
 __global__ void __launch_bounds__(EX_NT)
 expand_kernel(const float2* __restrict__ coef, int nrows, int ncoef, int ld,
               const float2* __restrict__ TX, int N, int mode, int nc, int kp,
-              float* __restrict__ Ut, const float2* __restrict__ Zk,
-              const float2* __restrict__ H, const float* __restrict__ w, int K, float scale) {
+              float* __restrict__ Ut, uint8_t* __restrict__ img, uint32_t img_tile_bytes) {
   extern __shared__ float2 se[];
   float2* cf = se;                    // [EX_R][ncoef]
   float2* ph = se + EX_R * ncoef;     // [ncoef][EX_X]
@@ -574,40 +577,10 @@ expand_kernel(const float2* __restrict__ coef, int nrows, int ncoef, int ld,
     return t;
   });
   pdl_wait();
-  if (Zk) {
-    const size_t nb = (size_t)nrows * ncoef;
-    for (int i = threadIdx.x; i < EX_R * ncoef; i += EX_NT) {
-      const int r = i / ncoef, c = i % ncoef;
-      float2 x = make_float2(0.f, 0.f);
-      if (a0 + r < nrows) {
-        const size_t u = (size_t)(a0 + r) * ncoef + c;
-        float2 acc = make_float2(0.f, 0.f);
-        for (int k0 = 0; k0 < K; k0 += 8) {
-          float2 hv[8], zv[8];
-#pragma unroll
-          for (int q = 0; q < 8; ++q)
-            if (k0 + q < K) {
-              hv[q] = H[(size_t)(k0 + q) * nb + u];
-              zv[q] = Zk[(size_t)(k0 + q) * nb + u];
-            }
-#pragma unroll
-          for (int q = 0; q < 8; ++q)
-            if (k0 + q < K) {
-              const float2 t = cmul(conjf2(hv[q]), zv[q]);
-              acc.x = fmaf(w[k0 + q], t.x, acc.x);
-              acc.y = fmaf(w[k0 + q], t.y, acc.y);
-            }
-        }
-        x = make_float2(acc.x * scale, acc.y * scale);
-      }
-      cf[i] = x;
-    }
-  } else {
-    fill_batched<EX_NT>(cf, EX_R * ncoef, [&](int i) {
-      const int r = i / ncoef, c = i % ncoef;
-      return (a0 + r < nrows) ? coef[(size_t)(a0 + r) * ld + c] : make_float2(0.f, 0.f);
-    });
-  }
+  fill_batched<EX_NT>(cf, EX_R * ncoef, [&](int i) {
+    const int r = i / ncoef, c = i % ncoef;
+    return (a0 + r < nrows) ? coef[(size_t)(a0 + r) * ld + c] : make_float2(0.f, 0.f);
+  });
   __syncthreads();
   const int xx = threadIdx.x % EX_X, rq = threadIdx.x / EX_X;  // rq in [0, 4): rows rq, rq + 4
   const int x = x0 + xx;
@@ -618,36 +591,48 @@ expand_kernel(const float2* __restrict__ coef, int nrows, int ncoef, int ld,
     cfma(acc1, cf[(rq + 4) * ncoef + c], p);
   }
   if (x >= N) return;
+  uint8_t* tile = img ? img + (size_t)(x / 128) * img_tile_bytes : nullptr;
+  auto put = [&](int f, float v) {
+    if (tile) {
+      const __nv_bfloat16 hi = __float2bfloat16_rn(v);
+      const __nv_bfloat16 lo = __float2bfloat16_rn(v - __bfloat162float(hi));
+      *reinterpret_cast<__nv_bfloat16*>(tile + sw128_offset(128, x % 128, f)) = hi;
+      *reinterpret_cast<__nv_bfloat16*>(tile + sw128_offset(128, x % 128, kp + f)) = lo;
+    } else {
+      Ut[(size_t)x * kp + f] = v;
+    }
+  };
   const int ra = a0 + rq, rb = a0 + rq + 4;
   if (ra < nrows) {
     const float k = (mode == 1 && ra > 0) ? 2.f : 1.f;
-    Ut[(size_t)x * kp + 2 * ra] = k * acc0.x;
-    Ut[(size_t)x * kp + 2 * ra + 1] = k * acc0.y;
+    put(2 * ra, k * acc0.x);
+    put(2 * ra + 1, k * acc0.y);
   }
   if (rb < nrows) {
     const float k = (mode == 1 && rb > 0) ? 2.f : 1.f;
-    Ut[(size_t)x * kp + 2 * rb] = k * acc1.x;
-    Ut[(size_t)x * kp + 2 * rb + 1] = k * acc1.y;
+    put(2 * rb, k * acc1.x);
+    put(2 * rb + 1, k * acc1.y);
   }
   if (blockIdx.y == 0 && rq == 0)
-    for (int f = 2 * nrows; f < kp; ++f) Ut[(size_t)x * kp + f] = 0.f;
+    for (int f = 2 * nrows; f < kp; ++f) put(f, 0.f);
 }
 
 static cudaError_t launch_expand(cudaStream_t s, const float2* coef, int nrows, int ncoef, int ld,
                                  const float2* TX, int N, int mode, int nc, int kp, float* Ut,
-                                 const float2* Zk = nullptr, const float2* H = nullptr,
-                                 const float* w = nullptr, int K = 0, float scale = 0.f) {
+                                 void* img) {
+  // Split-BF16 image tile: 128 rows x [hi | lo] of kp columns, in 64-column atoms.
+  const uint32_t img_tile_bytes = (uint32_t)((2 * kp + 63) / 64) * 128u * 128u;
   const size_t smem = (size_t)(EX_R * ncoef + ncoef * EX_X) * sizeof(float2);
   cudaError_t e = cudaFuncSetAttribute(expand_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
   if (e != cudaSuccess) return e;
   dim3 grid((N + EX_X - 1) / EX_X, (nrows + EX_R - 1) / EX_R);
   return launch_pdl(expand_kernel, grid, dim3(EX_NT), smem, s, coef, nrows, ncoef, ld, TX, N, mode,
-                    nc, kp, Ut, Zk, H, w, K, scale);
+                    nc, kp, Ut, static_cast<uint8_t*>(img), img_tile_bytes);
 }
 
 cudaError_t launch_band_forward(cudaStream_t s, const Cache& c, Field& f, float* ik, float* iP,
-                                float2* chat, float* Ut) {
+                                float2* chat, float* Ut, void* img) {
   const BandGeom& g = c.g;
   const size_t full = fields_smem_full(g);
   const int stage = full <= SMEM_STAGE;
@@ -672,7 +657,7 @@ cudaError_t launch_band_forward(cudaStream_t s, const Cache& c, Field& f, float*
                    static_cast<const float*>(iP), g.Nr, g.Nc, g.Pr, g.Pc, c.EDr_t, c.EDc,
                    1.f / ((float)g.Pr * (float)g.Pc), chat);
   if (err != cudaSuccess) return err;
-  return launch_expand(s, chat, g.Nr, nd, nd, c.TXDc, g.N, 1, g.Nc, g.kp_rows, Ut);
+  return launch_expand(s, chat, g.Nr, nd, nd, c.TXDc, g.N, 1, g.Nc, g.kp_rows, Ut, img);
 }
 
 // Adjoint 1 (one CTA per small-grid row jr):
@@ -795,8 +780,38 @@ band_z_kernel(const float2* __restrict__ e, const float* __restrict__ gam, int N
   }
 }
 
+// Adjoint 3: X[u] = scale sum_k w_k conj(H_k(u)) Z_k(u), k in order, one thread per
+// u; the loads of 8 consecutive k are issued together.
+__global__ void band_x_kernel(const float2* __restrict__ Zk, const float2* __restrict__ H,
+                              const float* __restrict__ w, int K, int nb, float scale,
+                              float2* __restrict__ X) {
+  pdl_trigger();
+  pdl_wait();
+  const int u = blockIdx.x * blockDim.x + threadIdx.x;
+  if (u >= nb) return;
+  float2 acc = make_float2(0.f, 0.f);
+  for (int k0 = 0; k0 < K; k0 += 8) {
+    float2 hv[8], zv[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q)
+      if (k0 + q < K) {
+        hv[q] = H[(size_t)(k0 + q) * nb + u];
+        zv[q] = Zk[(size_t)(k0 + q) * nb + u];
+      }
+#pragma unroll
+    for (int q = 0; q < 8; ++q)
+      if (k0 + q < K) {
+        const float2 t = cmul(conjf2(hv[q]), zv[q]);
+        acc.x = fmaf(w[k0 + q], t.x, acc.x);
+        acc.y = fmaf(w[k0 + q], t.y, acc.y);
+      }
+  }
+  X[u] = make_float2(acc.x * scale, acc.y * scale);
+}
+
 cudaError_t launch_band_adjoint(cudaStream_t s, const Cache& c, const Field& f, const float2* gh,
-                                double scale, float* gam, float2* Zk, float* Vt) {
+                                double scale, float* gam, float2* Zk, float2* X, float* Vt,
+                                void* img) {
   const BandGeom& g = c.g;
   const size_t smg = gamma_smem(g);
   cudaError_t e0 = cudaFuncSetAttribute(band_gamma_kernel,
@@ -816,9 +831,11 @@ cudaError_t launch_band_adjoint(cudaStream_t s, const Cache& c, const Field& f, 
                    static_cast<const float2*>(f.e), static_cast<const float*>(gam), g.Nr, g.Nc,
                    g.Pr, g.Pc, c.ESc, c.ESr_t, stage, 1.f / ((float)g.Pr * (float)g.Pc), Zk);
   if (err != cudaSuccess) return err;
-  // X = scale sum_k w_k conj(H_k) Z_k is formed inside the expansion.
-  return launch_expand(s, nullptr, g.Nr, g.Nc, g.Nc, c.TXSc, g.N, 0, g.Nc, g.kp_rows, Vt, Zk, c.H,
-                       c.w, g.K, (float)scale);
+  const int nb = g.Nr * g.Nc;
+  err = launch_pdl(band_x_kernel, dim3((nb + 127) / 128), dim3(128), 0, s,
+                   static_cast<const float2*>(Zk), c.H, c.w, g.K, nb, (float)scale, X);
+  if (err != cudaSuccess) return err;
+  return launch_expand(s, X, g.Nr, g.Nc, g.Nc, c.TXSc, g.N, 0, g.Nc, g.kp_rows, Vt, img);
 }
 
 // ---------------------------------------------------------------- FP64 partial sums

@@ -116,14 +116,21 @@ struct ResistEpiT {
   }
   __device__ __forceinline__ void store4p(int m, int n, float4 I, float4 T, int nvalid) {
     const size_t i = (size_t)m * N + n;
-    if (p.aerial) st4(p.aerial, i, I, vec, nvalid);
     if (p.mode == 0) {
+      if (p.aerial) st4(p.aerial, i, I, vec, nvalid);
       if (p.wafer) {
         const float4 W = make_float4(sigmoid(I.x), sigmoid(I.y), sigmoid(I.z), sigmoid(I.w));
         st4(p.wafer, i, W, vec, nvalid);
       }
       return;
     }
+    st4(p.dldi, i, dldi4(m, n, I, T, nvalid), vec, nvalid);
+  }
+  // Mode 1 without the dL/dI store: aerial / wafer stores and loss terms as in
+  // store4p, dL/dI returned (0 in lanes past nvalid).
+  __device__ __forceinline__ float4 dldi4(int m, int n, float4 I, float4 T, int nvalid) {
+    const size_t i = (size_t)m * N + n;
+    if (p.aerial) st4(p.aerial, i, I, vec, nvalid);
     const float4 one4 = make_float4(1.f, 1.f, 1.f, 1.f);
     const float4 pw = p.pe_window ? ld4(p.pe_window, i, vec, nvalid) : one4;
     const float4 qw = p.pen_window ? ld4(p.pen_window, i, vec, nvalid) : pw;
@@ -133,7 +140,7 @@ struct ResistEpiT {
     if (nvalid > 2) one(I.z, T.z, pw.z, qw.z, W.z, g.z);
     if (nvalid > 3) one(I.w, T.w, pw.w, qw.w, W.w, g.w);
     if (p.wafer) st4(p.wafer, i, W, vec, nvalid);
-    st4(p.dldi, i, g, vec, nvalid);
+    return g;
   }
   // All EPI_NT threads of the CTA must call finish.
   __device__ __forceinline__ void finish() {

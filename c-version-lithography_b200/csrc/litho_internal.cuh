@@ -162,14 +162,18 @@ cudaError_t launch_analysis(cudaStream_t s, int mode, const float* in, float* ma
 cudaError_t launch_reduce_tiles(cudaStream_t s, const float2* part, int tiles, int count,
                                 float scale, float2* out);
 // Small-grid stage of the forward: f.mband -> f.e, ik, iP and Ut (the row
-// synthesis operand). Shared memory of its per-kernel CTA: band_fields_smem.
+// synthesis operand), or, with img set, Ut's split-BF16 operand image for the
+// tensor-core synthesis (launch_pack_tc2_rows layout) instead of Ut.
+// Shared memory of its per-kernel CTA: band_fields_smem.
 size_t band_fields_smem(const BandGeom& g);
 size_t band_max_smem(const BandGeom& g);
 cudaError_t launch_band_forward(cudaStream_t s, const Cache& c, Field& f, float* ik, float* iP,
-                                float2* chat, float* Ut);
-// Small-grid stage of the adjoint: gh (the D-band DFT of dL/dI) -> gam, Zk and Vt.
+                                float2* chat, float* Ut, void* img);
+// Small-grid stage of the adjoint: gh (the D-band DFT of dL/dI) -> gam, Zk, X and Vt
+// (or Vt's operand image, as for the forward).
 cudaError_t launch_band_adjoint(cudaStream_t s, const Cache& c, const Field& f, const float2* gh,
-                                double scale, float* gam, float2* Zk, float* Vt);
+                                double scale, float* gam, float2* Zk, float2* X, float* Vt,
+                                void* img);
 
 // Row synthesis: out[y][x] = sum_f AY[y][f] * Bt[x][f] with a fused epilogue.
 struct ResistEpilogue {
@@ -225,6 +229,14 @@ cudaError_t launch_synth_resist_tc2(cudaStream_t s, const void* Aimg, const void
                                     int kp, const ResistEpilogue& ep, int* err, int* nblocks);
 cudaError_t launch_synth_grad_tc2(cudaStream_t s, const void* Aimg, const void* Bimg, int N,
                                   int kp, const GradEpilogue& ep, int* err, int* nblocks);
+// Resist synthesis fused with the adjoint tile analysis (CTM evaluation): loss
+// partials as launch_synth_resist_tc2 (ep.dldi unused), and the adjoint partials
+// part[tile][2 nr - 1][ncols] of dL/dI as launch_analysis_tc2 with the TXD / TYD
+// images; a non-finite dL/dI raises flag[0].
+cudaError_t launch_synth_resist_analysis_tc2(cudaStream_t s, const void* Aimg, const void* Bimg,
+                                             int N, int kp, const ResistEpilogue& ep, int ncols,
+                                             int nr, float2* part, int* flag, const void* tx_img,
+                                             const void* ty_img, int* err, int* nblocks);
 // The tensor-core path needs kp <= 128 and 2 Nc <= 128 (bands up to 64 x 64).
 inline bool tc2_supported(const BandGeom& g) {
   return g.kp_rows <= 128 && tc2_analysis_supported(g.Nc, g.Nr);

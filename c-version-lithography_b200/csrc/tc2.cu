@@ -164,6 +164,108 @@ struct Tc2Analysis {
 constexpr int A2_NT = 256;
 constexpr uint32_t A2_A_BYTES = s2_tile_bytes(128, 128);   // 64 KiB
 
+// Stages 1 and 2 of a tile analysis and the tile's partial, for a CTA whose 256
+// threads have written the [hi | lo] image tile into sA (64 KiB) and whose thread
+// 0 has issued the bulk copy of the TX image tile into sB on bars[0]. bars[1..3]
+// are initialised and unused; tmem holds at least BN columns. Every thread calls
+// it; on a bounded-wait expiry *fail is set and *err receives 3..6.
+template <int BN>
+__device__ __forceinline__ void analysis_stages(uint8_t* sA, uint8_t* sB, const uint64_t* bars,
+                                                uint32_t tmem, volatile int* fail,
+                                                const Tc2Analysis& a, const uint8_t* tyImg,
+                                                int xt, int yt, int* err) {
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const uint32_t uA = tc::smem_u32(sA), uB = tc::smem_u32(sB);
+  const uint32_t barX = tc::smem_u32(&bars[0]), barM1 = tc::smem_u32(&bars[1]);
+  const uint32_t barT = tc::smem_u32(&bars[2]), barM2 = tc::smem_u32(&bars[3]);
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  __syncthreads();
+  constexpr uint32_t idesc = tc::idesc_bf16(128, BN);
+  if (tid == 0 && !*fail) {
+    if (!tc::mbar_wait(barX, 0)) {
+      *fail = 1;
+      atomicExch(err, 3);
+      tc::mbar_wait(barX, 0);
+    } else {
+      tc::fence_after();
+      s2_mma(tmem, uA, 128, uB, BN, 128, idesc);
+      tc::mma_commit(barM1);
+      if (!tc::mbar_wait(barM1, 0)) {
+        *fail = 1;
+        atomicExch(err, 4);
+        tc::mbar_wait(barM1, 0);
+      } else {
+        // Stage 1 has read sA: bring this y tile's row-twiddle image into it.
+        bulk_tile(uA, tyImg + (size_t)yt * A2_A_BYTES, A2_A_BYTES, barT);
+      }
+    }
+  }
+  __syncthreads();
+  tc::fence_after();
+  const int lane_base = (warp & 3) * 32;
+  if (!*fail) {
+    // R (TMEM lanes y, columns f) -> sB as the K-major [hi | lo] operand of stage 2.
+    const int y = lane_base + lane;
+    for (int q = warp >> 2; q < BN / 16; q += 2) {
+      float rv[16];
+      tmem_ld16x(tmem + ((uint32_t)lane_base << 16) + (uint32_t)(16 * q), rv);
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        __nv_bfloat16 hi, lo;
+        split_bf16(rv[i], hi, lo);
+        *reinterpret_cast<__nv_bfloat16*>(sB + sw128_offset(BN, 16 * q + i, y)) = hi;
+        *reinterpret_cast<__nv_bfloat16*>(sB + sw128_offset(BN, 16 * q + i, 128 + y)) = lo;
+      }
+    }
+  }
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  tc::fence_before();
+  __syncthreads();
+  tc::fence_after();
+  if (tid == 0 && !*fail) {
+    if (!tc::mbar_wait(barT, 0)) {
+      *fail = 1;
+      atomicExch(err, 5);
+      tc::mbar_wait(barT, 0);
+    } else {
+      s2_mma(tmem, uA, 128, uB, BN, 128, idesc);
+      tc::mma_commit(barM2);
+      if (!tc::mbar_wait(barM2, 0)) {
+        *fail = 1;
+        atomicExch(err, 6);
+        tc::mbar_wait(barM2, 0);
+      }
+    }
+  }
+  __syncthreads();
+  tc::fence_after();
+  if (!*fail) {
+    const int n = lane_base + lane;
+    const int r = n >> 1, s = n & 1;
+    float2* out = a.part + (size_t)(yt * gridDim.x + xt) * a.nrows_out * a.ncols;
+    for (int q = warp >> 2; q < BN / 16; q += 2) {
+      float qv[16], pv[16];
+      tmem_ld16x(tmem + ((uint32_t)lane_base << 16) + (uint32_t)(16 * q), qv);
+#pragma unroll
+      for (int i = 0; i < 16; ++i) pv[i] = __shfl_xor_sync(0xffffffffu, qv[i], 1);
+      if (r >= a.nr) continue;
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const int c = 8 * q + i;
+        if (c >= a.ncols) break;
+        const float o0 = qv[2 * i], o1 = qv[2 * i + 1], p0 = pv[2 * i], p1 = pv[2 * i + 1];
+        if (!a.sym) {
+          if (s == 0) out[(size_t)r * a.ncols + c] = make_float2(o0 - p1, o1 + p0);
+        } else if (s == 0) {
+          out[(size_t)(a.nr - 1 + r) * a.ncols + c] = make_float2(o0 - p1, o1 + p0);
+        } else if (r >= 1) {
+          out[(size_t)(a.nr - 1 - r) * a.ncols + c] = make_float2(p0 + o1, p1 - o0);
+        }
+      }
+    }
+  }
+}
+
 template <int BN>
 __global__ void __launch_bounds__(A2_NT, 2)
 analysis_tc2_kernel(Tc2Analysis a, const uint8_t* __restrict__ txImg,
@@ -178,12 +280,11 @@ analysis_tc2_kernel(Tc2Analysis a, const uint8_t* __restrict__ txImg,
       (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
   uint8_t* sA = smem;
   uint8_t* sB = smem + A2_A_BYTES;
-  const uint32_t uA = tc::smem_u32(sA), uB = tc::smem_u32(sB);
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const uint32_t uB = tc::smem_u32(sB);
+  const int tid = threadIdx.x, warp = tid >> 5;
   const int xt = blockIdx.x, yt = blockIdx.y;
   const int x0 = xt * 128, y0 = yt * 128;
-  const uint32_t barX = tc::smem_u32(&bars[0]), barM1 = tc::smem_u32(&bars[1]);
-  const uint32_t barT = tc::smem_u32(&bars[2]), barM2 = tc::smem_u32(&bars[3]);
+  const uint32_t barX = tc::smem_u32(&bars[0]);
   pdl_trigger();
   if (tid == 0) {
     for (int i = 0; i < 4; ++i) tc::mbar_init(tc::smem_u32(&bars[i]), 1);
@@ -239,92 +340,7 @@ analysis_tc2_kernel(Tc2Analysis a, const uint8_t* __restrict__ txImg,
         *reinterpret_cast<const uint4*>(lo);
   }
   if (bad) atomicOr(a.flag, 1);
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-  __syncthreads();
-  constexpr uint32_t idesc = tc::idesc_bf16(128, BN);
-  if (tid == 0) {
-    if (!tc::mbar_wait(barX, 0)) {
-      fail = 1;
-      atomicExch(err, 3);
-      tc::mbar_wait(barX, 0);
-    } else {
-      tc::fence_after();
-      s2_mma(tmem, uA, 128, uB, BN, 128, idesc);
-      tc::mma_commit(barM1);
-      if (!tc::mbar_wait(barM1, 0)) {
-        fail = 1;
-        atomicExch(err, 4);
-        tc::mbar_wait(barM1, 0);
-      } else {
-        // Stage 1 has read sA: bring this y tile's row-twiddle image into it.
-        bulk_tile(uA, tyImg + (size_t)yt * A2_A_BYTES, A2_A_BYTES, barT);
-      }
-    }
-  }
-  __syncthreads();
-  tc::fence_after();
-  const int lane_base = (warp & 3) * 32;
-  if (!fail) {
-    // R (TMEM lanes y, columns f) -> sB as the K-major [hi | lo] operand of stage 2.
-    const int y = lane_base + lane;
-    for (int q = warp >> 2; q < BN / 16; q += 2) {
-      float rv[16];
-      tmem_ld16x(tmem + ((uint32_t)lane_base << 16) + (uint32_t)(16 * q), rv);
-#pragma unroll
-      for (int i = 0; i < 16; ++i) {
-        __nv_bfloat16 hi, lo;
-        split_bf16(rv[i], hi, lo);
-        *reinterpret_cast<__nv_bfloat16*>(sB + sw128_offset(BN, 16 * q + i, y)) = hi;
-        *reinterpret_cast<__nv_bfloat16*>(sB + sw128_offset(BN, 16 * q + i, 128 + y)) = lo;
-      }
-    }
-  }
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-  tc::fence_before();
-  __syncthreads();
-  tc::fence_after();
-  if (tid == 0 && !fail) {
-    if (!tc::mbar_wait(barT, 0)) {
-      fail = 1;
-      atomicExch(err, 5);
-      tc::mbar_wait(barT, 0);
-    } else {
-      s2_mma(tmem, uA, 128, uB, BN, 128, idesc);
-      tc::mma_commit(barM2);
-      if (!tc::mbar_wait(barM2, 0)) {
-        fail = 1;
-        atomicExch(err, 6);
-        tc::mbar_wait(barM2, 0);
-      }
-    }
-  }
-  __syncthreads();
-  tc::fence_after();
-  if (!fail) {
-    const int n = lane_base + lane;
-    const int r = n >> 1, s = n & 1;
-    float2* out = a.part + (size_t)(yt * gridDim.x + xt) * a.nrows_out * a.ncols;
-    for (int q = warp >> 2; q < BN / 16; q += 2) {
-      float qv[16], pv[16];
-      tmem_ld16x(tmem + ((uint32_t)lane_base << 16) + (uint32_t)(16 * q), qv);
-#pragma unroll
-      for (int i = 0; i < 16; ++i) pv[i] = __shfl_xor_sync(0xffffffffu, qv[i], 1);
-      if (r >= a.nr) continue;
-#pragma unroll
-      for (int i = 0; i < 8; ++i) {
-        const int c = 8 * q + i;
-        if (c >= a.ncols) break;
-        const float o0 = qv[2 * i], o1 = qv[2 * i + 1], p0 = pv[2 * i], p1 = pv[2 * i + 1];
-        if (!a.sym) {
-          if (s == 0) out[(size_t)r * a.ncols + c] = make_float2(o0 - p1, o1 + p0);
-        } else if (s == 0) {
-          out[(size_t)(a.nr - 1 + r) * a.ncols + c] = make_float2(o0 - p1, o1 + p0);
-        } else if (r >= 1) {
-          out[(size_t)(a.nr - 1 - r) * a.ncols + c] = make_float2(p0 + o1, p1 - o0);
-        }
-      }
-    }
-  }
+  analysis_stages<BN>(sA, sB, bars, tmem, &fail, a, tyImg, xt, yt, err);
   tc::fence_before();
   __syncthreads();
   if (warp == 0) tc::tmem_dealloc(tmem, TM_COLS);
@@ -546,6 +562,168 @@ cudaError_t launch_synth_grad_tc2(cudaStream_t s, const void* Aimg, const void* 
   const int vec = N % 4 == 0 && aligned16(ep.grad_mask) && aligned16(ep.theta) &&
                   aligned16(ep.grad_theta);
   return launch_tc2(s, Aimg, Bimg, N, kp, GradEpiT<true>{ep, N, vec, 0.0}, err, nblocks);
+}
+
+// ---------------------------------------------------------------- fused resist + adjoint analysis
+// For the CTM evaluation: per 128 x 128 tile, I = AYD . Ut^T in tensor memory; the
+// resist epilogue (FP64 loss partials, optional aerial / wafer stores) turns I
+// into dL/dI in registers, and dL/dI goes straight into shared memory as the
+// [hi | lo] image operand of the adjoint tile analysis (TXD, TYD, conjugate rows),
+// which leaves this tile's partial of the D-band spectrum of dL/dI. dL/dI is
+// never written to global memory. Shared memory holds the synthesis operands,
+// then the dL/dI tile (64 KiB) with the TXD image tile behind it, then the TYD
+// image tile in place of the dL/dI tile. The epilogue reads tensor memory
+// directly (thread = tile row), so its global accesses are per-row streams.
+template <int BN>
+__global__ void __launch_bounds__(S2_NT, 2)
+synth_resist_analysis_kernel(const uint8_t* __restrict__ Aimg, const uint8_t* __restrict__ Bimg,
+                             int N, int kp, ResistEpiT<true> epi, Tc2Analysis a,
+                             const uint8_t* __restrict__ txImg, const uint8_t* __restrict__ tyImg,
+                             int* __restrict__ err) {
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  __shared__ __align__(8) uint64_t bars[6];  // [0..3] analysis stages, [4] operands, [5] synthesis
+  __shared__ uint32_t tmem_slot;
+  __shared__ int fail;
+  constexpr uint32_t TX_BYTES = s2_tile_bytes(BN, 128);
+  uint8_t* smem = reinterpret_cast<uint8_t*>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
+  uint8_t* sA = smem;                  // dL/dI tile, then the TYD image tile
+  uint8_t* sB = smem + A2_A_BYTES;     // TXD image tile, then R
+  const uint32_t tile_bytes = s2_tile_bytes(128, kp);
+  const uint32_t uA = tc::smem_u32(smem), uB = uA + tile_bytes;  // synthesis operands
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int xt = blockIdx.x, yt = blockIdx.y;
+  const int x0 = xt * 128, y0 = yt * 128;
+  const int lane_base = (warp & 3) * 32;
+  const int row = lane_base + lane, col0 = (warp >> 2) * 64;
+  const int m = y0 + row;
+  const bool interior = epi.vec && y0 + 128 <= N && x0 + 128 <= N;
+  const uint32_t barL = tc::smem_u32(&bars[4]), barM = tc::smem_u32(&bars[5]);
+  pdl_trigger();
+  if (tid == 0) {
+    for (int i = 0; i < 6; ++i) tc::mbar_init(tc::smem_u32(&bars[i]), 1);
+    fail = 0;
+    tc::fence_mbar_init();
+  }
+  if (warp == 0) tc::tmem_alloc(tc::smem_u32(&tmem_slot), 128);
+  tc::fence_before();
+  __syncthreads();
+  tc::fence_after();
+  const uint32_t tmem = tmem_slot;
+  if (tid == 0) {
+    tc::mbar_expect_tx(barL, 2 * tile_bytes);
+    const uint8_t* ga = Aimg + (size_t)yt * tile_bytes;
+    for (uint32_t q = 0; q < tile_bytes; q += 16384)
+      tc::bulk_g2s(uA + q, ga + q, tile_bytes - q < 16384u ? tile_bytes - q : 16384u, barL);
+  }
+  pdl_wait();
+  if (tid == 0) {
+    const uint8_t* gb = Bimg + (size_t)xt * tile_bytes;
+    for (uint32_t q = 0; q < tile_bytes; q += 16384)
+      tc::bulk_g2s(uB + q, gb + q, tile_bytes - q < 16384u ? tile_bytes - q : 16384u, barL);
+  }
+  // This thread's 64 target values (its tile row, columns col0 .. col0 + 63).
+  float4 pre[16];
+  if (interior) {
+#pragma unroll
+    for (int i = 0; i < 16; ++i) pre[i] = epi.pre4(m, x0 + col0 + 4 * i, 4);
+  }
+  if (tid == 0) {
+    if (!tc::mbar_wait(barL, 0)) {
+      fail = 1;
+      atomicExch(err, 1);
+      tc::mbar_wait(barL, 0);
+    } else {
+      tc::fence_after();
+      s2_mma(tmem, uA, 128, uB, 128, kp, tc::idesc_bf16(128, 128));
+      tc::mma_commit(barM);
+      if (!tc::mbar_wait(barM, 0)) {
+        fail = 1;
+        atomicExch(err, 2);
+        tc::mbar_wait(barM, 0);
+      } else {
+        // The synthesis operands are dead: the TXD tile loads behind the dL/dI tile.
+        bulk_tile(tc::smem_u32(sB), txImg + (size_t)xt * TX_BYTES, TX_BYTES,
+                  tc::smem_u32(&bars[0]));
+      }
+    }
+  }
+  __syncthreads();
+  tc::fence_after();
+  bool bad = false;
+  if (!fail) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      float v[16];
+      tmem_ld16x(tmem + ((uint32_t)lane_base << 16) + (uint32_t)(col0 + 16 * q), v);
+#pragma unroll
+      for (int g4 = 0; g4 < 4; ++g4) {
+        const int c = col0 + 16 * q + 4 * g4, n = x0 + c;
+        const float4 I = make_float4(v[4 * g4], v[4 * g4 + 1], v[4 * g4 + 2], v[4 * g4 + 3]);
+        float4 g;
+        if (interior) {
+          g = epi.dldi4(m, n, I, pre[4 * q + g4], 4);
+        } else {
+          const int nv = m < N ? min(4, N - n) : 0;
+          g = nv > 0 ? epi.dldi4(m, n, I, epi.pre4(m, n, nv), nv) : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        bad |= !(isfinite(g.x) && isfinite(g.y) && isfinite(g.z) && isfinite(g.w));
+        __nv_bfloat16 hi[4], lo[4];
+        split_bf16(g.x, hi[0], lo[0]);
+        split_bf16(g.y, hi[1], lo[1]);
+        split_bf16(g.z, hi[2], lo[2]);
+        split_bf16(g.w, hi[3], lo[3]);
+        *reinterpret_cast<uint2*>(sA + sw128_offset(128, row, c)) = *reinterpret_cast<const uint2*>(hi);
+        *reinterpret_cast<uint2*>(sA + sw128_offset(128, row, 128 + c)) =
+            *reinterpret_cast<const uint2*>(lo);
+      }
+    }
+  }
+  if (bad) atomicOr(a.flag, 1);
+  epi.finish();
+  tc::fence_before();
+  analysis_stages<BN>(sA, sB, bars, tmem, &fail, a, tyImg, xt, yt, err);
+  tc::fence_before();
+  __syncthreads();
+  if (warp == 0) tc::tmem_dealloc(tmem, 128);
+}
+
+template <int BN>
+static cudaError_t fused_t(cudaStream_t s, const void* Aimg, const void* Bimg, int N, int kp,
+                          const ResistEpiT<true>& e, const Tc2Analysis& a, const void* tx,
+                          const void* ty, int* err, int* nblocks) {
+  const size_t ops = 2 * (size_t)s2_tile_bytes(128, kp);
+  const size_t ana = (size_t)A2_A_BYTES + s2_tile_bytes(BN, 128);
+  const size_t smem = (ops > ana ? ops : ana) + 1024;
+  cudaError_t r = cudaFuncSetAttribute(synth_resist_analysis_kernel<BN>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (r != cudaSuccess) return r;
+  dim3 grid((N + 127) / 128, (N + 127) / 128);
+  *nblocks = grid.x * grid.y;
+  return launch_pdl(synth_resist_analysis_kernel<BN>, grid, dim3(S2_NT), smem, s,
+                    static_cast<const uint8_t*>(Aimg), static_cast<const uint8_t*>(Bimg), N, kp, e,
+                    a, static_cast<const uint8_t*>(tx), static_cast<const uint8_t*>(ty), err);
+}
+
+cudaError_t launch_synth_resist_analysis_tc2(cudaStream_t s, const void* Aimg, const void* Bimg,
+                                             int N, int kp, const ResistEpilogue& ep, int ncols,
+                                             int nr, float2* part, int* flag, const void* tx_img,
+                                             const void* ty_img, int* err, int* nblocks) {
+  const int vec = N % 4 == 0 && aligned16(ep.aerial) && aligned16(ep.wafer) &&
+                  aligned16(ep.target) && aligned16(ep.pe_window) && aligned16(ep.pen_window);
+  const ResistEpiT<true> e{ep, N, vec, 0.0, 0.0};
+  const Tc2Analysis a{nullptr, nullptr, flag, N, 0, 0, ncols, 2 * nr - 1, nr, 1, part};
+  switch (tc2_analysis_rows(ncols)) {
+    case 16: return fused_t<16>(s, Aimg, Bimg, N, kp, e, a, tx_img, ty_img, err, nblocks);
+    case 32: return fused_t<32>(s, Aimg, Bimg, N, kp, e, a, tx_img, ty_img, err, nblocks);
+    case 48: return fused_t<48>(s, Aimg, Bimg, N, kp, e, a, tx_img, ty_img, err, nblocks);
+    case 64: return fused_t<64>(s, Aimg, Bimg, N, kp, e, a, tx_img, ty_img, err, nblocks);
+    case 80: return fused_t<80>(s, Aimg, Bimg, N, kp, e, a, tx_img, ty_img, err, nblocks);
+    case 96: return fused_t<96>(s, Aimg, Bimg, N, kp, e, a, tx_img, ty_img, err, nblocks);
+    case 112: return fused_t<112>(s, Aimg, Bimg, N, kp, e, a, tx_img, ty_img, err, nblocks);
+    case 128: return fused_t<128>(s, Aimg, Bimg, N, kp, e, a, tx_img, ty_img, err, nblocks);
+    default: return cudaErrorInvalidValue;
+  }
 }
 
 }  // namespace litho_b200
