@@ -571,9 +571,9 @@ cudaError_t launch_synth_grad_tc2(cudaStream_t s, const void* Aimg, const void* 
 // [hi | lo] image operand of the adjoint tile analysis (TXD, TYD, conjugate rows),
 // which leaves this tile's partial of the D-band spectrum of dL/dI. dL/dI is
 // never written to global memory. Shared memory holds the synthesis operands,
-// then the dL/dI tile (64 KiB) with the TXD image tile behind it, then the TYD
-// image tile in place of the dL/dI tile. The epilogue reads tensor memory
-// directly (thread = tile row), so its global accesses are per-row streams.
+// then the accumulator staging area with the TXD image tile behind it, then the
+// dL/dI tile over the staging area, then the TYD image tile in its place.
+constexpr uint32_t FUSED_TX_OFFSET = 68 * 1024;  // past the 128 x S2_SS float staging area
 template <int BN>
 __global__ void __launch_bounds__(S2_NT, 2)
 synth_resist_analysis_kernel(const uint8_t* __restrict__ Aimg, const uint8_t* __restrict__ Bimg,
@@ -587,16 +587,14 @@ synth_resist_analysis_kernel(const uint8_t* __restrict__ Aimg, const uint8_t* __
   constexpr uint32_t TX_BYTES = s2_tile_bytes(BN, 128);
   uint8_t* smem = reinterpret_cast<uint8_t*>(
       (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
-  uint8_t* sA = smem;                  // dL/dI tile, then the TYD image tile
-  uint8_t* sB = smem + A2_A_BYTES;     // TXD image tile, then R
+  uint8_t* sA = smem;                    // dL/dI tile, then the TYD image tile
+  uint8_t* sB = smem + FUSED_TX_OFFSET;  // TXD image tile, then R
+  float* Ss = reinterpret_cast<float*>(smem);  // accumulator staging [128][S2_SS]
   const uint32_t tile_bytes = s2_tile_bytes(128, kp);
   const uint32_t uA = tc::smem_u32(smem), uB = uA + tile_bytes;  // synthesis operands
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int xt = blockIdx.x, yt = blockIdx.y;
   const int x0 = xt * 128, y0 = yt * 128;
-  const int lane_base = (warp & 3) * 32;
-  const int row = lane_base + lane, col0 = (warp >> 2) * 64;
-  const int m = y0 + row;
   const bool interior = epi.vec && y0 + 128 <= N && x0 + 128 <= N;
   const uint32_t barL = tc::smem_u32(&bars[4]), barM = tc::smem_u32(&bars[5]);
   pdl_trigger();
@@ -622,11 +620,15 @@ synth_resist_analysis_kernel(const uint8_t* __restrict__ Aimg, const uint8_t* __
     for (uint32_t q = 0; q < tile_bytes; q += 16384)
       tc::bulk_g2s(uB + q, gb + q, tile_bytes - q < 16384u ? tile_bytes - q : 16384u, barL);
   }
-  // This thread's 64 target values (its tile row, columns col0 .. col0 + 63).
-  float4 pre[16];
+  // Targets of interior tiles, coalesced: chunk j covers row j / 32, columns
+  // 4 (j % 32) .. + 3; the same registers later carry this thread's dL/dI.
+  float4 pre[S2_CHUNKS];
   if (interior) {
 #pragma unroll
-    for (int i = 0; i < 16; ++i) pre[i] = epi.pre4(m, x0 + col0 + 4 * i, 4);
+    for (int i = 0; i < S2_CHUNKS; ++i) {
+      const int j = tid + i * S2_NT;
+      pre[i] = epi.pre4(y0 + (j >> 5), x0 + (j & 31) * 4, 4);
+    }
   }
   if (tid == 0) {
     if (!tc::mbar_wait(barL, 0)) {
@@ -642,7 +644,7 @@ synth_resist_analysis_kernel(const uint8_t* __restrict__ Aimg, const uint8_t* __
         atomicExch(err, 2);
         tc::mbar_wait(barM, 0);
       } else {
-        // The synthesis operands are dead: the TXD tile loads behind the dL/dI tile.
+        // The synthesis operands are dead: the TXD tile loads behind the staging area.
         bulk_tile(tc::smem_u32(sB), txImg + (size_t)xt * TX_BYTES, TX_BYTES,
                   tc::smem_u32(&bars[0]));
       }
@@ -650,33 +652,59 @@ synth_resist_analysis_kernel(const uint8_t* __restrict__ Aimg, const uint8_t* __
   }
   __syncthreads();
   tc::fence_after();
+  if (!fail) {
+    const int lane_base = (warp & 3) * 32;
+    const int row = lane_base + lane;
+    for (int q = (warp >> 2) * 4; q < (warp >> 2) * 4 + 4; ++q) {
+      float v[16];
+      tmem_ld16x(tmem + ((uint32_t)lane_base << 16) + (uint32_t)(16 * q), v);
+#pragma unroll
+      for (int i = 0; i < 16; i += 4)
+        *reinterpret_cast<float4*>(&Ss[row * S2_SS + 16 * q + i]) =
+            make_float4(v[i], v[i + 1], v[i + 2], v[i + 3]);
+    }
+  }
+  tc::fence_before();
+  __syncthreads();
   bool bad = false;
   if (!fail) {
+    if (interior) {
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      float v[16];
-      tmem_ld16x(tmem + ((uint32_t)lane_base << 16) + (uint32_t)(col0 + 16 * q), v);
-#pragma unroll
-      for (int g4 = 0; g4 < 4; ++g4) {
-        const int c = col0 + 16 * q + 4 * g4, n = x0 + c;
-        const float4 I = make_float4(v[4 * g4], v[4 * g4 + 1], v[4 * g4 + 2], v[4 * g4 + 3]);
-        float4 g;
-        if (interior) {
-          g = epi.dldi4(m, n, I, pre[4 * q + g4], 4);
-        } else {
-          const int nv = m < N ? min(4, N - n) : 0;
-          g = nv > 0 ? epi.dldi4(m, n, I, epi.pre4(m, n, nv), nv) : make_float4(0.f, 0.f, 0.f, 0.f);
-        }
-        bad |= !(isfinite(g.x) && isfinite(g.y) && isfinite(g.z) && isfinite(g.w));
-        __nv_bfloat16 hi[4], lo[4];
-        split_bf16(g.x, hi[0], lo[0]);
-        split_bf16(g.y, hi[1], lo[1]);
-        split_bf16(g.z, hi[2], lo[2]);
-        split_bf16(g.w, hi[3], lo[3]);
-        *reinterpret_cast<uint2*>(sA + sw128_offset(128, row, c)) = *reinterpret_cast<const uint2*>(hi);
-        *reinterpret_cast<uint2*>(sA + sw128_offset(128, row, 128 + c)) =
-            *reinterpret_cast<const uint2*>(lo);
+      for (int i = 0; i < S2_CHUNKS; ++i) {
+        const int j = tid + i * S2_NT;
+        const int r = j >> 5, c = (j & 31) * 4;
+        pre[i] = epi.dldi4(y0 + r, x0 + c, *reinterpret_cast<const float4*>(&Ss[r * S2_SS + c]),
+                           pre[i], 4);
       }
+    } else {
+#pragma unroll 1
+      for (int i = 0; i < S2_CHUNKS; ++i) {
+        const int j = tid + i * S2_NT;
+        const int r = j >> 5, c = (j & 31) * 4;
+        const int m = y0 + r, n = x0 + c;
+        const int nv = m < N ? min(4, N - n) : 0;
+        pre[i] = nv > 0 ? epi.dldi4(m, n, *reinterpret_cast<const float4*>(&Ss[r * S2_SS + c]),
+                                    epi.pre4(m, n, nv), nv)
+                        : make_float4(0.f, 0.f, 0.f, 0.f);
+      }
+    }
+  }
+  __syncthreads();  // every read of the staging area is done: the dL/dI tile replaces it
+  if (!fail) {
+#pragma unroll
+    for (int i = 0; i < S2_CHUNKS; ++i) {
+      const int j = tid + i * S2_NT;
+      const int r = j >> 5, c = (j & 31) * 4;
+      const float4 g = pre[i];
+      bad |= !(isfinite(g.x) && isfinite(g.y) && isfinite(g.z) && isfinite(g.w));
+      __nv_bfloat16 hi[4], lo[4];
+      split_bf16(g.x, hi[0], lo[0]);
+      split_bf16(g.y, hi[1], lo[1]);
+      split_bf16(g.z, hi[2], lo[2]);
+      split_bf16(g.w, hi[3], lo[3]);
+      *reinterpret_cast<uint2*>(sA + sw128_offset(128, r, c)) = *reinterpret_cast<const uint2*>(hi);
+      *reinterpret_cast<uint2*>(sA + sw128_offset(128, r, 128 + c)) =
+          *reinterpret_cast<const uint2*>(lo);
     }
   }
   if (bad) atomicOr(a.flag, 1);
@@ -693,7 +721,7 @@ static cudaError_t fused_t(cudaStream_t s, const void* Aimg, const void* Bimg, i
                           const ResistEpiT<true>& e, const Tc2Analysis& a, const void* tx,
                           const void* ty, int* err, int* nblocks) {
   const size_t ops = 2 * (size_t)s2_tile_bytes(128, kp);
-  const size_t ana = (size_t)A2_A_BYTES + s2_tile_bytes(BN, 128);
+  const size_t ana = (size_t)FUSED_TX_OFFSET + s2_tile_bytes(BN, 128);
   const size_t smem = (ops > ana ? ops : ana) + 1024;
   cudaError_t r = cudaFuncSetAttribute(synth_resist_analysis_kernel<BN>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
