@@ -413,9 +413,9 @@ __device__ __forceinline__ void fill_batched(T* dst, int n, Load load) {
 // columns jc in [q CW, q CW + CW): A = H_k m on the band, T = A ESc^T restricted
 // to those columns (Nr x CW) and e_k = ESr T (Pr x CW); ik = w_k |e_k|^2. Columns
 // are independent, so the split costs no recomputation.
-constexpr int BF_NT = 128;
-constexpr int BF_CW = 2;    // small-grid columns per CTA (forward fields)
-constexpr int BZ_UW = 1;    // band columns per CTA (adjoint Z)
+constexpr int BF_NT = 256;
+constexpr int BF_CW = 10;   // small-grid columns per CTA (forward fields)
+constexpr int BZ_UW = 7;    // band columns per CTA (adjoint Z)
 __global__ void __launch_bounds__(BF_NT)
 band_fields_kernel(const float2* __restrict__ H, const float2* __restrict__ mband,
                    const float* __restrict__ w, int Nr, int Nc, int Pr, int Pc,
@@ -548,7 +548,7 @@ static size_t chat_smem(const BandGeom& g) {
 // mode 0 (band S): phase = conj(TX[c][x]) (TX = e^{-2 pi i s_c x/N}), kappa = 1.
 // mode 1 (difference set D, c in [0, 2nc-1), d = c - (nc-1)):
 //   phase = d >= 0 ? conj(TX[d][x]) : TX[-d][x], kappa(a) = a > 0 ? 2 : 1 (Hermitian half).
-// Columns 2*nrows .. kp-1 of Ut are zero-filled by the first row block.
+// Columns 2*nrows .. kp-1 of Ut are zero.
 // With img set (tensor-core path) the result goes
 // straight into the split-BF16 operand image of the row synthesis instead of Ut:
 // x tile x / 128 at img + (x / 128) * img_tile_bytes, hi of column f at
@@ -582,39 +582,52 @@ expand_kernel(const float2* __restrict__ coef, int nrows, int ncoef, int ld,
     return (a0 + r < nrows) ? coef[(size_t)(a0 + r) * ld + c] : make_float2(0.f, 0.f);
   });
   __syncthreads();
-  const int xx = threadIdx.x % EX_X, rq = threadIdx.x / EX_X;  // rq in [0, 4): rows rq, rq + 4
+  // Thread (xx, rq): rows a0 + 2 rq and a0 + 2 rq + 1, i.e. the four consecutive
+  // output columns f0 .. f0 + 3 of image row x, written as one 8- or 16-byte store.
+  const int xx = threadIdx.x % EX_X, rq = threadIdx.x / EX_X;
   const int x = x0 + xx;
+  const int ra = a0 + 2 * rq, rb = ra + 1;
   float2 acc0 = make_float2(0.f, 0.f), acc1 = acc0;
   for (int c = 0; c < ncoef; ++c) {
     const float2 p = ph[c * EX_X + xx];
-    cfma(acc0, cf[rq * ncoef + c], p);
-    cfma(acc1, cf[(rq + 4) * ncoef + c], p);
+    cfma(acc0, cf[2 * rq * ncoef + c], p);
+    cfma(acc1, cf[(2 * rq + 1) * ncoef + c], p);
   }
   if (x >= N) return;
-  uint8_t* tile = img ? img + (size_t)(x / 128) * img_tile_bytes : nullptr;
-  auto put = [&](int f, float v) {
-    if (tile) {
-      const __nv_bfloat16 hi = __float2bfloat16_rn(v);
-      const __nv_bfloat16 lo = __float2bfloat16_rn(v - __bfloat162float(hi));
-      *reinterpret_cast<__nv_bfloat16*>(tile + sw128_offset(128, x % 128, f)) = hi;
-      *reinterpret_cast<__nv_bfloat16*>(tile + sw128_offset(128, x % 128, kp + f)) = lo;
+  const float ka = ra < nrows ? ((mode == 1 && ra > 0) ? 2.f : 1.f) : 0.f;
+  const float kb = rb < nrows ? ((mode == 1 && rb > 0) ? 2.f : 1.f) : 0.f;
+  const float4 v = make_float4(ka * acc0.x, ka * acc0.y, kb * acc1.x, kb * acc1.y);
+  const int f0 = 2 * ra;
+  if (f0 < kp) {
+    if (img) {
+      uint8_t* tile = img + (size_t)(x / 128) * img_tile_bytes;
+      __nv_bfloat16 hi[4], lo[4];
+      const float vv[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        hi[q] = __float2bfloat16_rn(vv[q]);
+        lo[q] = __float2bfloat16_rn(vv[q] - __bfloat162float(hi[q]));
+      }
+      *reinterpret_cast<uint2*>(tile + sw128_offset(128, x % 128, f0)) =
+          *reinterpret_cast<const uint2*>(hi);
+      *reinterpret_cast<uint2*>(tile + sw128_offset(128, x % 128, kp + f0)) =
+          *reinterpret_cast<const uint2*>(lo);
     } else {
-      Ut[(size_t)x * kp + f] = v;
+      *reinterpret_cast<float4*>(Ut + (size_t)x * kp + f0) = v;
     }
-  };
-  const int ra = a0 + rq, rb = a0 + rq + 4;
-  if (ra < nrows) {
-    const float k = (mode == 1 && ra > 0) ? 2.f : 1.f;
-    put(2 * ra, k * acc0.x);
-    put(2 * ra + 1, k * acc0.y);
   }
-  if (rb < nrows) {
-    const float k = (mode == 1 && rb > 0) ? 2.f : 1.f;
-    put(2 * rb, k * acc1.x);
-    put(2 * rb + 1, k * acc1.y);
+  // Columns past the last row group are zero.
+  if (blockIdx.y == gridDim.y - 1 && rq == 0) {
+    for (int f = 2 * EX_R * gridDim.y; f < kp; f += 4) {
+      if (img) {
+        uint8_t* tile = img + (size_t)(x / 128) * img_tile_bytes;
+        *reinterpret_cast<uint2*>(tile + sw128_offset(128, x % 128, f)) = make_uint2(0u, 0u);
+        *reinterpret_cast<uint2*>(tile + sw128_offset(128, x % 128, kp + f)) = make_uint2(0u, 0u);
+      } else {
+        *reinterpret_cast<float4*>(Ut + (size_t)x * kp + f) = make_float4(0.f, 0.f, 0.f, 0.f);
+      }
+    }
   }
-  if (blockIdx.y == 0 && rq == 0)
-    for (int f = 2 * nrows; f < kp; ++f) put(f, 0.f);
 }
 
 static cudaError_t launch_expand(cudaStream_t s, const float2* coef, int nrows, int ncoef, int ld,
