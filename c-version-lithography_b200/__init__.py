@@ -594,7 +594,8 @@ class CTMOptimizer:
                 best_mask = self.mask.clone()
             if norm <= self.tol:
                 break
-            theta = theta - self.learning_rate * gt
+            # in place: the evaluation's buffers stay fixed, so repeats replay its CUDA graph
+            theta.sub_(self.learning_rate * gt)
         self.theta = theta
         return best_mask
 

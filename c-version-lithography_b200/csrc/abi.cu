@@ -214,6 +214,7 @@ int litho_ctx_destroy(litho_ctx* ctx) {
   if (ctx->d_red) cudaFree(ctx->d_red);
   if (ctx->h_red) cudaFreeHost(ctx->h_red);
   if (ctx->host_stage.base) cudaFree(ctx->host_stage.base);
+  if (ctx->eval_graph) cudaGraphExecDestroy(ctx->eval_graph);
   for (cudaEvent_t e : ctx->ev_aux)
     if (e) cudaEventDestroy(e);
   if (ctx->aux) cudaStreamDestroy(ctx->aux);
@@ -853,7 +854,6 @@ static int ctm_evaluate_impl(litho_ctx* ctx, const litho_cache* cache, litho_fie
     tmp.cache = cache; tmp.e = tmp_e; tmp.mband = tmp_m;
     f = &tmp;
   }
-  const int N = cache->g.N;
   ResistEpilogue ep{};
   ep.mode = 1;
   ep.thr = (float)threshold;
@@ -866,27 +866,81 @@ static int ctm_evaluate_impl(litho_ctx* ctx, const litho_cache* cache, litho_fie
   ep.pen_thr = 0.01f;
   ep.dldi = at<float>(ctx, L.dldi);
   ep.loss_partial = ctx->d_red + RED_PART;
-  int nb = 0;
   // Tensor-core path: the resist synthesis also runs the adjoint tile analysis.
   const bool fuse = ctx->precision == LITHO_PRECISION_BF16X3 && cache->TXD_img != nullptr;
-  st = run_forward(ctx, *cache, *f, L, 1, d_theta, d_mask, ep, &nb, target_ready, fuse);
-  if (!st)
-    st = check_launch(ctx, launch_sum_partials(ctx->stream, ctx->d_red + RED_PART, nb, 2,
-                                               ctx->d_red + RED_SUM),
-                      "sum");
-  GradEpilogue gp{};
-  gp.grad_mask = d_grad_mask;
-  gp.theta = d_theta;
-  gp.grad_theta = d_grad_theta;
-  gp.norm_partial = ctx->d_red + RED_PART + 2 * (size_t)nb;
-  int nb2 = 0;
-  if (!st)
-    st = run_adjoint(ctx, *cache, *f, L, at<float>(ctx, L.dldi), 4.0 * alpha, gp, &nb2, fuse);
-  if (!st)
-    st = check_launch(ctx, launch_sum_partials(ctx->stream, gp.norm_partial, nb2, 1,
-                                               ctx->d_red + RED_SUM + 2),
-                      "sum");
-  ctx->launches += 2;
+  // The whole chain of launches, on ctx->stream.
+  auto launch_chain = [&]() -> int {
+    int nb = 0;
+    int r = run_forward(ctx, *cache, *f, L, 1, d_theta, d_mask, ep, &nb, target_ready, fuse);
+    if (!r)
+      r = check_launch(ctx, launch_sum_partials(ctx->stream, ctx->d_red + RED_PART, nb, 2,
+                                                ctx->d_red + RED_SUM),
+                       "sum");
+    GradEpilogue gp{};
+    gp.grad_mask = d_grad_mask;
+    gp.theta = d_theta;
+    gp.grad_theta = d_grad_theta;
+    gp.norm_partial = ctx->d_red + RED_PART + 2 * (size_t)nb;
+    int nb2 = 0;
+    if (!r)
+      r = run_adjoint(ctx, *cache, *f, L, at<float>(ctx, L.dldi), 4.0 * alpha, gp, &nb2, fuse);
+    if (!r)
+      r = check_launch(ctx, launch_sum_partials(ctx->stream, gp.norm_partial, nb2, 1,
+                                                ctx->d_red + RED_SUM + 2),
+                       "sum");
+    ctx->launches += 2;
+    return r;
+  };
+  // Repeated evaluations on the same buffers replay a CUDA graph of the chain.
+  const BandGeom& g = cache->g;
+  EvalKey key;
+  const void* ptrs[16] = {cache,       f->e,          f->mband,          d_theta,
+                          d_target,    d_mask,        d_aerial,          d_wafer,
+                          d_grad_mask, d_grad_theta,  ctx->scratch.base, ctx->d_red,
+                          cache->H,    cache->AYD_img, cache->TXS,
+                          reinterpret_cast<const void*>((uintptr_t)ctx->precision)};
+  for (int i = 0; i < 16; ++i) key.ptr[i] = ptrs[i];
+  const int geom[6] = {g.N, g.K, g.Nr, g.Nc, g.row0, g.col0};
+  for (int i = 0; i < 6; ++i) key.geom[i] = geom[i];
+  key.thr = threshold;
+  key.alpha = alpha;
+  const bool graphable = field != nullptr && target_ready == nullptr && !ctx->timing;
+  if (graphable && ctx->eval_graph && key == ctx->eval_graph_key) {
+    LITHO_CUDA_TRY(ctx, cudaGraphLaunch(ctx->eval_graph, ctx->stream));
+    ctx->launches += ctx->eval_graph_launches;
+    f->valid = true;
+  } else if (graphable && ctx->eval_last_valid && key == ctx->eval_last_key) {
+    if (ctx->eval_graph) {
+      cudaGraphExecDestroy(ctx->eval_graph);
+      ctx->eval_graph = nullptr;
+    }
+    const long long launches0 = ctx->launches;
+    cudaGraph_t graph = nullptr;
+    bool captured = false;
+    if (cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+      st = launch_chain();
+      const cudaError_t e = cudaStreamEndCapture(ctx->stream, &graph);
+      captured = st == LITHO_OK && e == cudaSuccess && graph &&
+                 cudaGraphInstantiate(&ctx->eval_graph, graph, 0) == cudaSuccess;
+      if (graph) cudaGraphDestroy(graph);
+    }
+    cudaGetLastError();
+    if (captured) {
+      ctx->eval_graph_key = key;
+      ctx->eval_graph_launches = ctx->launches - launches0;
+      LITHO_CUDA_TRY(ctx, cudaGraphLaunch(ctx->eval_graph, ctx->stream));
+    } else {
+      // Capture is not available here: launch the chain directly.
+      if (ctx->eval_graph) cudaGraphExecDestroy(ctx->eval_graph);
+      ctx->eval_graph = nullptr;
+      ctx->launches = launches0;
+      st = launch_chain();
+    }
+  } else {
+    st = launch_chain();
+  }
+  ctx->eval_last_key = key;
+  ctx->eval_last_valid = graphable;
   if (!st) st = fetch(ctx, 3);
   if (tmp_e) { cudaFree(tmp_e); cudaFree(tmp_m); }
   if (st) return st;
@@ -894,7 +948,6 @@ static int ctm_evaluate_impl(litho_ctx* ctx, const litho_cache* cache, litho_fie
     f->valid = false;
     return ctx->fail(LITHO_ERR_NONFINITE, "theta must be finite");
   }
-  (void)N;
   if (loss) *loss = ctx->h_red[RED_SUM];
   if (grad_norm) *grad_norm = std::sqrt(ctx->h_red[RED_SUM + 2]);
   return LITHO_OK;

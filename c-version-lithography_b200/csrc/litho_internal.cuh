@@ -92,6 +92,21 @@ struct Scratch {
   size_t bytes = 0;
 };
 
+// Identity of one CTM evaluation's launch chain: every device pointer it
+// touches, the band geometry and the scalars baked into its kernels.
+struct EvalKey {
+  const void* ptr[16] = {};
+  int geom[6] = {};
+  double thr = 0.0, alpha = 0.0;
+  bool operator==(const EvalKey& o) const {
+    for (int i = 0; i < 16; ++i)
+      if (ptr[i] != o.ptr[i]) return false;
+    for (int i = 0; i < 6; ++i)
+      if (geom[i] != o.geom[i]) return false;
+    return thr == o.thr && alpha == o.alpha;
+  }
+};
+
 struct Context {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -101,6 +116,12 @@ struct Context {
   Scratch host_stage;            // device staging of the host-buffer entry points
   cudaStream_t aux = nullptr;    // upload stream of the host-buffer entry points
   cudaEvent_t ev_aux[2] = {};    // [0] theta uploaded (main stream), [1] target uploaded (aux)
+  // CUDA graph of the last repeated CTM evaluation (litho_ctm_evaluate): captured
+  // on the second consecutive call with the same key, replayed while it stays.
+  cudaGraphExec_t eval_graph = nullptr;
+  EvalKey eval_graph_key, eval_last_key;
+  bool eval_last_valid = false;
+  long long eval_graph_launches = 0;
   double* d_red = nullptr;       // FP64 reduction partials
   size_t red_cap = 0;
   double* h_red = nullptr;       // pinned host mirror for results

@@ -330,3 +330,38 @@ def test_ctm_evaluate_host_buffers(L, wl, precision):
             0.02, 50.0, h_grad.data_ptr(), ctypes.byref(loss), ctypes.byref(norm)))
         assert loss.value == loss_d and norm.value == norm_d
         assert np.array_equal(h_grad.numpy(), g_d)
+
+
+@pytest.mark.parametrize("precision", ["fp32", "bf16x3"])
+def test_ctm_evaluate_graph_replay(L, wl, precision):
+    """Repeated litho_ctm_evaluate calls on the same buffers are captured once and
+    replayed as a CUDA graph: results equal the direct launches, and in-place
+    changes of theta are seen by the replay."""
+    N = 256
+    band, r0, c0, w, wss = wl.synthetic_socs_band()
+    ctx = L.Context()
+    ctx.set_precision(precision)
+    cache = L.ImagingCache.from_band(N, band, r0, c0, w, wss, ctx=ctx)
+    rng = np.random.default_rng(11)
+    theta0 = (rng.random((N, N)) * 3.0).astype(np.float32)
+    theta1 = (rng.random((N, N)) * 3.0).astype(np.float32)
+    target = (rng.random((N, N)) > 0.5).astype(np.float32)
+    fresh = L.CTMOptimizer(cache, target, 0.02, 50.0, iterations=1)
+    ref0 = fresh.evaluate(torch.from_numpy(theta0).cuda())
+    ref0 = (ref0[0], ref0[1].cpu().numpy(), ref0[2])
+    fresh2 = L.CTMOptimizer(cache, target, 0.02, 50.0, iterations=1)
+    ref1 = fresh2.evaluate(torch.from_numpy(theta1).cuda())
+    ref1 = (ref1[0], ref1[1].cpu().numpy(), ref1[2])
+    opt = L.CTMOptimizer(cache, target, 0.02, 50.0, iterations=1)
+    th = torch.from_numpy(theta0).cuda()
+    counts = []
+    for i in range(5):
+        if i == 3:
+            th.copy_(torch.from_numpy(theta1))   # same buffer, new content
+        c0 = ctx.launch_count
+        loss, g, norm = opt.evaluate(th)
+        counts.append(ctx.launch_count - c0)
+        ref = ref1 if i >= 3 else ref0
+        assert loss == ref[0] and norm == ref[2]
+        assert np.array_equal(g.cpu().numpy(), ref[1])
+    assert len(set(counts)) == 1   # replays count the kernels they launch
