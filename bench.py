@@ -124,14 +124,22 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def stage_bytes(N, Nr, Nc):
+def stage_bytes(N, Nr, Nc, fused):
     """Algorithmic DRAM bytes per launch of the full-resolution stages of one CTM
-    evaluation (float32 images; tile partials are complex64 per 128 x 128 tile)."""
+    evaluation (float32 images; tile partials are complex64 per 128 x 128 tile).
+    fused: the tensor-core chain, whose resist synthesis also runs the adjoint
+    tile analysis, so dL/dI is neither written nor read back."""
     px = 4 * N * N
     tiles = ((N + 127) // 128) ** 2
-    return {"tile_analysis": px + 8 * tiles * Nr * Nc,
+    fwd_part = 8 * tiles * Nr * Nc
+    adj_part = 8 * tiles * (2 * Nr - 1) * Nc
+    if fused:
+        return {"tile_analysis": px + fwd_part,
+                "row_synthesis_resist": px + adj_part,
+                "adjoint_row_synthesis_theta": 2 * px}
+    return {"tile_analysis": px + fwd_part,
             "row_synthesis_resist": 2 * px,
-            "adjoint_tile_analysis": px + 8 * tiles * (2 * Nr - 1) * Nc,
+            "adjoint_tile_analysis": px + adj_part,
             "adjoint_row_synthesis_theta": 2 * px}
 
 
@@ -331,7 +339,7 @@ def run_ours(args):
     # Roofline of the dominant full-resolution stage, live CUDA-event timing.
     hbm, src = peaks()
     stages = R["stages"]
-    sb = stage_bytes(N, cache.Nr, cache.Nc)
+    sb = stage_bytes(N, cache.Nr, cache.Nc, head == "bf16x3")
     dom = max(sb, key=lambda s: stages[s][0] / max(stages[s][1], 1))
     avg_ms = stages[dom][0] / max(stages[dom][1], 1)
     achieved = sb[dom] / (avg_ms / 1e3) / 1e9
