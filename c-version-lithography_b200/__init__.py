@@ -80,6 +80,7 @@ SIGNATURES = {
     "litho_ctx_synchronize": (_I, [_P]),
     "litho_ctx_set_precision": (_I, [_P, _I]),
     "litho_ctx_launch_count": (ctypes.c_longlong, [_P]),
+    "litho_ctx_enable_graphs": (_I, [_P, _I]),
     "litho_ctx_enable_stage_timing": (_I, [_P, _I]),
     "litho_ctx_stage_times": (_I, [_P, _PD, ctypes.POINTER(ctypes.c_longlong)]),
     "litho_cache_create_dense": (_I, [_P, _I, _I, _PD, _PD, _D, _PP]),
@@ -209,6 +210,10 @@ class Context:
     STAGES = ("tile_analysis", "tile_reduction", "band_forward", "row_synthesis_resist",
               "adjoint_tile_analysis", "adjoint_tile_reduction", "band_adjoint",
               "adjoint_row_synthesis_theta", "levelset")
+
+    def enable_graphs(self, on: bool = True):
+        """CUDA-graph replay of repeated CTM evaluations (on by default)."""
+        self._check(self.lib.litho_ctx_enable_graphs(self.handle, 1 if on else 0))
 
     def enable_stage_timing(self, on: bool = True):
         self._check(self.lib.litho_ctx_enable_stage_timing(self.handle, 1 if on else 0))

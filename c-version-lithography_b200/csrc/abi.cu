@@ -242,6 +242,18 @@ int litho_ctx_set_precision(litho_ctx* ctx, int precision) {
 
 long long litho_ctx_launch_count(const litho_ctx* ctx) { return ctx ? ctx->launches : 0; }
 
+int litho_ctx_enable_graphs(litho_ctx* ctx, int on) {
+  if (!ctx) return LITHO_ERR_INVALID_ARGUMENT;
+  ctx->graphs = on != 0;
+  ctx->eval_last_valid = false;
+  if (!ctx->graphs && ctx->eval_graph) {
+    cudaStreamSynchronize(ctx->stream);
+    cudaGraphExecDestroy(ctx->eval_graph);
+    ctx->eval_graph = nullptr;
+  }
+  return LITHO_OK;
+}
+
 int litho_ctx_enable_stage_timing(litho_ctx* ctx, int on) {
   if (!ctx) return LITHO_ERR_INVALID_ARGUMENT;
   if (cudaSetDevice(ctx->device) != cudaSuccess) return LITHO_ERR_CUDA;
@@ -904,7 +916,8 @@ static int ctm_evaluate_impl(litho_ctx* ctx, const litho_cache* cache, litho_fie
   for (int i = 0; i < 6; ++i) key.geom[i] = geom[i];
   key.thr = threshold;
   key.alpha = alpha;
-  const bool graphable = field != nullptr && target_ready == nullptr && !ctx->timing;
+  const bool graphable =
+      ctx->graphs && field != nullptr && target_ready == nullptr && !ctx->timing;
   if (graphable && ctx->eval_graph && key == ctx->eval_graph_key) {
     LITHO_CUDA_TRY(ctx, cudaGraphLaunch(ctx->eval_graph, ctx->stream));
     ctx->launches += ctx->eval_graph_launches;

@@ -118,6 +118,7 @@ struct Context {
   cudaEvent_t ev_aux[2] = {};    // [0] theta uploaded (main stream), [1] target uploaded (aux)
   // CUDA graph of the last repeated CTM evaluation (litho_ctm_evaluate): captured
   // on the second consecutive call with the same key, replayed while it stays.
+  bool graphs = true;
   cudaGraphExec_t eval_graph = nullptr;
   EvalKey eval_graph_key, eval_last_key;
   bool eval_last_valid = false;

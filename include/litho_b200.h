@@ -42,8 +42,9 @@ extern "C" {
 #define LITHO_ERR_UNSUPPORTED 7      /* size or option outside what is built */
 
 #define LITHO_PRECISION_FP32 0       /* plain FP32 DFT passes (SIMT) */
-#define LITHO_PRECISION_BF16X3 1     /* row syntheses on tcgen05 tensor cores in split-BF16
-                                        (hi*hi + hi*lo + lo*hi, FP32 accumulation) */
+#define LITHO_PRECISION_BF16X3 1     /* full-resolution analyses and syntheses on the tcgen05
+                                        tensor cores in split BF16 (hi*hi + hi*lo + lo*hi,
+                                        FP32 accumulation) */
 
 typedef struct litho_ctx litho_ctx;
 typedef struct litho_cache litho_cache;
@@ -62,6 +63,12 @@ int litho_ctx_synchronize(litho_ctx* ctx);
 int litho_ctx_set_precision(litho_ctx* ctx, int precision);
 /* Kernels this context has launched so far (a counter, for benchmarks). */
 long long litho_ctx_launch_count(const litho_ctx* ctx);
+/* CUDA-graph replay of litho_ctm_evaluate (on by default): the second consecutive
+ * call with the same buffers, cache, precision and scalars captures its launch
+ * chain into a graph; later identical calls replay it with one launch. Turn it off
+ * when the context's stream is itself being captured by the caller, or under
+ * tools that cannot follow a stream capture. */
+int litho_ctx_enable_graphs(litho_ctx* ctx, int on);
 
 /* Per-stage device timing with CUDA events on the context's stream. Stages:
  * 0 tile analysis of the mask (row DFT + column contraction per 128 x 128 tile),
