@@ -116,7 +116,7 @@ struct AnalysisArgs {
   int N, ncols;
   const float2* TY;    // [nr][N] row twiddles
   int nrows_out, nr, sym;
-  float2* part;        // [tiles][nrows_out][ncols]
+  float2* part;        // [nrows_out][ncols][tiles]
 };
 
 template <int BN>
@@ -202,13 +202,14 @@ __device__ void analysis_phase2(float* smem, const AnalysisArgs& a, int y0, int 
         cfma(p11, tb, rb);
       }
       const int row0 = r0 + 2 * rp;
-      float2* out0 = a.part + ((size_t)tile * a.nrows_out + row0) * a.ncols;
-      if (c0g < a.ncols) out0[c0g] = p00;
-      if (c0g + 1 < a.ncols) out0[c0g + 1] = p01;
+      const size_t tiles = (size_t)gridDim.x * gridDim.y;
+      float2* out0 = a.part + ((size_t)row0 * a.ncols) * tiles + tile;   // [row][c][tile]
+      if (c0g < a.ncols) out0[(size_t)c0g * tiles] = p00;
+      if (c0g + 1 < a.ncols) out0[(size_t)(c0g + 1) * tiles] = p01;
       if (row0 + 1 < a.nrows_out) {
-        float2* out1 = out0 + a.ncols;
-        if (c0g < a.ncols) out1[c0g] = p10;
-        if (c0g + 1 < a.ncols) out1[c0g + 1] = p11;
+        float2* out1 = out0 + (size_t)a.ncols * tiles;
+        if (c0g < a.ncols) out1[(size_t)c0g * tiles] = p10;
+        if (c0g + 1 < a.ncols) out1[(size_t)(c0g + 1) * tiles] = p11;
       }
     }
   }
@@ -235,7 +236,8 @@ int analysis_tiles(int N) {
 }
 
 // Tile partials of sum_{y, x} T(a, y) A[y][x] tw(c, x) for every 128 x 128 tile:
-// part[tile][a][c], tiles in row-major order of the tile grid.
+// part[a][c][tile], tiles in row-major order of the tile grid (each band entry's
+// partials contiguous, for the reduction).
 cudaError_t launch_analysis(cudaStream_t s, int mode, const float* in, float* mask_out,
                             int* flag, const float* tw, int N, int ncols, const float2* TY,
                             int nrows_out, int nr, int sym, float2* part) {
@@ -251,7 +253,8 @@ cudaError_t launch_analysis(cudaStream_t s, int mode, const float* in, float* ma
   return analysis_tile_t<8>(s, a);
 }
 
-// out[o] = scale * sum_t part[t][o] in a fixed tree order (one warp per output).
+// out[o] = scale * sum_t part[o][t] in a fixed tree order (one warp per output,
+// reading the entry's partials contiguously).
 __global__ void __launch_bounds__(256)
 reduce_tiles_kernel(const float2* __restrict__ part, int tiles, int count, float scale,
                     float2* __restrict__ out) {
@@ -263,13 +266,13 @@ reduce_tiles_kernel(const float2* __restrict__ part, int tiles, int count, float
   float2 v0 = make_float2(0.f, 0.f), v1 = v0;
   int t = lane;
   for (; t + 32 < tiles; t += 64) {
-    const float2 p = part[(size_t)t * count + o];
-    const float2 q = part[(size_t)(t + 32) * count + o];
+    const float2 p = part[(size_t)o * tiles + t];
+    const float2 q = part[(size_t)o * tiles + t + 32];
     v0.x += p.x; v0.y += p.y;
     v1.x += q.x; v1.y += q.y;
   }
   if (t < tiles) {
-    const float2 p = part[(size_t)t * count + o];
+    const float2 p = part[(size_t)o * tiles + t];
     v0.x += p.x; v0.y += p.y;
   }
   float vx = v0.x + v1.x, vy = v0.y + v1.y;

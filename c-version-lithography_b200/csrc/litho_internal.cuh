@@ -173,14 +173,14 @@ cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t s
 // All launchers return cudaGetLastError() of their launches.
 // Tile analysis: for every 128 x 128 tile t of the image A (A = in for mode 0,
 // (1 + cos in)/2 for mode 1, optionally stored to mask_out)
-//   part[t][a][c] = sum_{(y, x) in t} T(a, y) A[y][x] tw(c, x)
+//   part[a][c][t] = sum_{(y, x) in t} T(a, y) A[y][x] tw(c, x)
 // with tw = [2 ncols][N] real rows (Re, Im) and T(a, y) = TY[a][y] (sym 0,
 // a < nrows_out) or, for sym 1, d = a - (nr - 1), TY[d][y] / conj(TY[-d][y]).
 int analysis_tiles(int N);
 cudaError_t launch_analysis(cudaStream_t s, int mode, const float* in, float* mask_out,
                             int* flag, const float* tw, int N, int ncols, const float2* TY,
                             int nrows_out, int nr, int sym, float2* part);
-// out[o] = scale * sum_t part[t][o] (fixed order).
+// out[o] = scale * sum_t part[o][t] (fixed order).
 cudaError_t launch_reduce_tiles(cudaStream_t s, const float2* part, int tiles, int count,
                                 float scale, float2* out);
 // Small-grid stage of the forward: f.mband -> f.e, ik, iP and Ut (the row

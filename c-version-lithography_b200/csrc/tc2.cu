@@ -150,7 +150,7 @@ __device__ __forceinline__ void bulk_tile(uint32_t dst, const uint8_t* src, uint
 //   Re = Q[2r][2c] - Q[2r+1][2c+1],  Im = Q[2r][2c+1] + Q[2r+1][2c],
 // and with sym the conjugate rows -r come from the same Q:
 //   Re = Q[2r][2c] + Q[2r+1][2c+1],  Im = Q[2r][2c+1] - Q[2r+1][2c].
-// Output: part[tile][row][c] (row = r, or r + nr - 1 for +r / nr - 1 - r for -r with sym).
+// Output: part[row][c][tile] (row = r, or r + nr - 1 for +r / nr - 1 - r for -r with sym).
 struct Tc2Analysis {
   const float* in;
   float* mask_out;
@@ -242,7 +242,8 @@ __device__ __forceinline__ void analysis_stages(uint8_t* sA, uint8_t* sB, const 
   if (!*fail) {
     const int n = lane_base + lane;
     const int r = n >> 1, s = n & 1;
-    float2* out = a.part + (size_t)(yt * gridDim.x + xt) * a.nrows_out * a.ncols;
+    const size_t tiles = (size_t)gridDim.x * gridDim.y;
+    float2* out = a.part + (size_t)(yt * gridDim.x + xt);   // [row][c][tile]
     for (int q = warp >> 2; q < BN / 16; q += 2) {
       float qv[16], pv[16];
       tmem_ld16x(tmem + ((uint32_t)lane_base << 16) + (uint32_t)(16 * q), qv);
@@ -255,11 +256,11 @@ __device__ __forceinline__ void analysis_stages(uint8_t* sA, uint8_t* sB, const 
         if (c >= a.ncols) break;
         const float o0 = qv[2 * i], o1 = qv[2 * i + 1], p0 = pv[2 * i], p1 = pv[2 * i + 1];
         if (!a.sym) {
-          if (s == 0) out[(size_t)r * a.ncols + c] = make_float2(o0 - p1, o1 + p0);
+          if (s == 0) out[((size_t)r * a.ncols + c) * tiles] = make_float2(o0 - p1, o1 + p0);
         } else if (s == 0) {
-          out[(size_t)(a.nr - 1 + r) * a.ncols + c] = make_float2(o0 - p1, o1 + p0);
+          out[((size_t)(a.nr - 1 + r) * a.ncols + c) * tiles] = make_float2(o0 - p1, o1 + p0);
         } else if (r >= 1) {
-          out[(size_t)(a.nr - 1 - r) * a.ncols + c] = make_float2(p0 + o1, p1 - o0);
+          out[((size_t)(a.nr - 1 - r) * a.ncols + c) * tiles] = make_float2(p0 + o1, p1 - o0);
         }
       }
     }
