@@ -604,17 +604,18 @@ expand_kernel(const float2* __restrict__ coef, int nrows, int ncoef, int ld,
   if (f0 < kp) {
     if (img) {
       uint8_t* tile = img + (size_t)(x / 128) * img_tile_bytes;
-      __nv_bfloat16 hi[4], lo[4];
-      const float vv[4] = {v.x, v.y, v.z, v.w};
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        hi[q] = __float2bfloat16_rn(vv[q]);
-        lo[q] = __float2bfloat16_rn(vv[q] - __bfloat162float(hi[q]));
-      }
-      *reinterpret_cast<uint2*>(tile + sw128_offset(128, x % 128, f0)) =
-          *reinterpret_cast<const uint2*>(hi);
-      *reinterpret_cast<uint2*>(tile + sw128_offset(128, x % 128, kp + f0)) =
-          *reinterpret_cast<const uint2*>(lo);
+      const __nv_bfloat162 h01 = __floats2bfloat162_rn(v.x, v.y);
+      const __nv_bfloat162 h23 = __floats2bfloat162_rn(v.z, v.w);
+      const float2 f01 = __bfloat1622float2(h01), f23 = __bfloat1622float2(h23);
+      const __nv_bfloat162 l01 = __floats2bfloat162_rn(v.x - f01.x, v.y - f01.y);
+      const __nv_bfloat162 l23 = __floats2bfloat162_rn(v.z - f23.x, v.w - f23.y);
+      uint2 hw, lw;
+      hw.x = *reinterpret_cast<const uint32_t*>(&h01);
+      hw.y = *reinterpret_cast<const uint32_t*>(&h23);
+      lw.x = *reinterpret_cast<const uint32_t*>(&l01);
+      lw.y = *reinterpret_cast<const uint32_t*>(&l23);
+      *reinterpret_cast<uint2*>(tile + sw128_offset(128, x % 128, f0)) = hw;
+      *reinterpret_cast<uint2*>(tile + sw128_offset(128, x % 128, kp + f0)) = lw;
     } else {
       *reinterpret_cast<float4*>(Ut + (size_t)x * kp + f0) = v;
     }

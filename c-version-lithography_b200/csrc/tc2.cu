@@ -52,6 +52,15 @@ __device__ __forceinline__ void split_bf16(float v, __nv_bfloat16& hi, __nv_bflo
   hi = __float2bfloat16_rn(v);
   lo = __float2bfloat16_rn(v - __bfloat162float(hi));
 }
+// The same split for two values with packed conversions: hi2 / lo2 hold (a, b)
+// as consecutive bf16 (a at the lower address).
+__device__ __forceinline__ void split_pair(float a, float b, uint32_t& hi2, uint32_t& lo2) {
+  const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+  const float2 hf = __bfloat1622float2(h);
+  const __nv_bfloat162 l = __floats2bfloat162_rn(a - hf.x, b - hf.y);
+  hi2 = *reinterpret_cast<const uint32_t*>(&h);
+  lo2 = *reinterpret_cast<const uint32_t*>(&l);
+}
 
 // ---------------------------------------------------------------- image packing
 // Logical real matrix of a pack source: kind 0 reads src[row * ld + col];
@@ -205,16 +214,21 @@ __device__ __forceinline__ void analysis_stages(uint8_t* sA, uint8_t* sB, const 
   const int lane_base = (warp & 3) * 32;
   if (!*fail) {
     // R (TMEM lanes y, columns f) -> sB as the K-major [hi | lo] operand of stage 2.
+    // Lanes y and y ^ 1 share the 4-byte words (f, y & ~1): the even lane stores
+    // the hi pair, the odd lane the lo pair.
     const int y = lane_base + lane;
+    const int ye = y & ~1;
+    const bool odd = lane & 1;
     for (int q = warp >> 2; q < BN / 16; q += 2) {
       float rv[16];
       tmem_ld16x(tmem + ((uint32_t)lane_base << 16) + (uint32_t)(16 * q), rv);
 #pragma unroll
       for (int i = 0; i < 16; ++i) {
-        __nv_bfloat16 hi, lo;
-        split_bf16(rv[i], hi, lo);
-        *reinterpret_cast<__nv_bfloat16*>(sB + sw128_offset(BN, 16 * q + i, y)) = hi;
-        *reinterpret_cast<__nv_bfloat16*>(sB + sw128_offset(BN, 16 * q + i, 128 + y)) = lo;
+        const float pv = __shfl_xor_sync(0xffffffffu, rv[i], 1);
+        uint32_t h2, l2;
+        split_pair(odd ? pv : rv[i], odd ? rv[i] : pv, h2, l2);
+        *reinterpret_cast<uint32_t*>(sB + sw128_offset(BN, 16 * q + i, odd ? 128 + ye : ye)) =
+            odd ? l2 : h2;
       }
     }
   }
@@ -324,21 +338,24 @@ analysis_tc2_kernel(Tc2Analysis a, const uint8_t* __restrict__ txImg,
     const int j = tid + i * A2_NT;
     const int r = j >> 4, c8 = (j & 15) * 8;
     const int m = y0 + r, x = x0 + c8;
-    __nv_bfloat16 hi[8], lo[8];
+    float u[8];
 #pragma unroll
     for (int e = 0; e < 8; ++e) {
       const bool in_range = m < a.N && x + e < a.N;
-      float u = v[i][e];
-      if (in_range) bad |= !isfinite(u);
+      u[e] = v[i][e];
+      if (in_range) bad |= !isfinite(u[e]);
       if (a.mode == 1) {
-        u = in_range ? 0.5f * (1.f + fast_cos(u)) : 0.f;
-        if (a.mask_out && in_range) a.mask_out[(size_t)m * a.N + x + e] = u;
+        u[e] = in_range ? 0.5f * (1.f + fast_cos(u[e])) : 0.f;
+        if (a.mask_out && in_range) a.mask_out[(size_t)m * a.N + x + e] = u[e];
       }
-      split_bf16(u, hi[e], lo[e]);
     }
-    *reinterpret_cast<uint4*>(sA + sw128_offset(128, r, c8)) = *reinterpret_cast<const uint4*>(hi);
-    *reinterpret_cast<uint4*>(sA + sw128_offset(128, r, 128 + c8)) =
-        *reinterpret_cast<const uint4*>(lo);
+    uint4 h4, l4;
+    split_pair(u[0], u[1], h4.x, l4.x);
+    split_pair(u[2], u[3], h4.y, l4.y);
+    split_pair(u[4], u[5], h4.z, l4.z);
+    split_pair(u[6], u[7], h4.w, l4.w);
+    *reinterpret_cast<uint4*>(sA + sw128_offset(128, r, c8)) = h4;
+    *reinterpret_cast<uint4*>(sA + sw128_offset(128, r, 128 + c8)) = l4;
   }
   if (bad) atomicOr(a.flag, 1);
   analysis_stages<BN>(sA, sB, bars, tmem, &fail, a, tyImg, xt, yt, err);
@@ -698,14 +715,11 @@ synth_resist_analysis_kernel(const uint8_t* __restrict__ Aimg, const uint8_t* __
       const int r = j >> 5, c = (j & 31) * 4;
       const float4 g = pre[i];
       bad |= !(isfinite(g.x) && isfinite(g.y) && isfinite(g.z) && isfinite(g.w));
-      __nv_bfloat16 hi[4], lo[4];
-      split_bf16(g.x, hi[0], lo[0]);
-      split_bf16(g.y, hi[1], lo[1]);
-      split_bf16(g.z, hi[2], lo[2]);
-      split_bf16(g.w, hi[3], lo[3]);
-      *reinterpret_cast<uint2*>(sA + sw128_offset(128, r, c)) = *reinterpret_cast<const uint2*>(hi);
-      *reinterpret_cast<uint2*>(sA + sw128_offset(128, r, 128 + c)) =
-          *reinterpret_cast<const uint2*>(lo);
+      uint2 h2, l2;
+      split_pair(g.x, g.y, h2.x, l2.x);
+      split_pair(g.z, g.w, h2.y, l2.y);
+      *reinterpret_cast<uint2*>(sA + sw128_offset(128, r, c)) = h2;
+      *reinterpret_cast<uint2*>(sA + sw128_offset(128, r, 128 + c)) = l2;
     }
   }
   if (bad) atomicOr(a.flag, 1);
