@@ -111,6 +111,10 @@ SIGNATURES = {
                                     ctypes.POINTER(ExchangeOptionsC), _P, _P, _PD, _PD]),
     "litho_fullchip_theta_step": (_I, [_P, _P, _P, _P, _D, _P]),
     "litho_lsm_rk2_update_noalloc": (_I, [_P, _I, _I, _P, _P, _D, _D, _D, _D, _P, _P, _PD]),
+    "litho_render_levelset_mask": (_I, [_P, _I, _I, _P, _I, _I, _P]),
+    "litho_fullchip_lsm_init": (_I, [_P, _P, _P, _D, _D, _I, _I, _P, _P]),
+    "litho_fullchip_lsm_step": (_I, [_P, _P, _P, _P, _D, _D, _D, _D, _I, _I, _I, _P, _P, _PD,
+                                     _PD]),
 }
 
 
@@ -620,6 +624,23 @@ class CTMOptimizer:
                                                 max_iterations=self.iterations)
         self.theta = theta
         return 0.5 * (1.0 + torch.cos(theta))
+
+
+MASK_TYPES = {"Binary": 0, "Gray": 1}
+
+
+def render_levelset_mask(phi, mask_type: str = "Gray", scale: int = 4, ctx=None):
+    """render_levelset_mask (levelset_mask_renderer.cpp:7-33): Binary (phi >= 0) or
+    Gray (subpixel coverage of the scale-times bilinear upsampling of phi)."""
+    ctx = ctx or default_context()
+    if mask_type not in MASK_TYPES:
+        raise LithoError(1, f"mask_type must be one of {sorted(MASK_TYPES)}")
+    phi = _f32(phi, ctx.torch)
+    out = ctx.torch.empty_like(phi)
+    ctx._check(ctx.lib.litho_render_levelset_mask(ctx.handle, phi.shape[0], phi.shape[1],
+                                                  _ptr(phi), MASK_TYPES[mask_type], scale,
+                                                  _ptr(out)))
+    return out
 
 
 @dataclass

@@ -1499,3 +1499,145 @@ int litho_fullchip_theta_step(litho_ctx* ctx, const litho_partition* p, float* d
 }
 
 }  // extern "C"
+
+extern "C" {
+
+int litho_render_levelset_mask(litho_ctx* ctx, int rows, int cols, const float* d_phi,
+                               int mask_type, int scale, float* d_mask) {
+  if (!ctx || !d_phi || !d_mask || rows <= 0 || cols <= 0) return LITHO_ERR_INVALID_ARGUMENT;
+  if (mask_type != LITHO_MASK_BINARY && mask_type != LITHO_MASK_GRAY)
+    return ctx->fail(LITHO_ERR_INVALID_ARGUMENT, "render_levelset_mask: unknown mask type");
+  if (mask_type == LITHO_MASK_GRAY && (scale < 1 || scale > 64))
+    return ctx->fail(LITHO_ERR_INVALID_ARGUMENT, "render_levelset_mask: scale must be in 1..64");
+  if (cudaSetDevice(ctx->device) != cudaSuccess) return ctx->fail(LITHO_ERR_CUDA, "cudaSetDevice");
+  ctx->launches += 1;
+  int st = check_launch(ctx, launch_render_mask(ctx->stream, d_phi, rows, cols, 1,
+                                                mask_type == LITHO_MASK_GRAY, scale, d_mask),
+                        "render_levelset_mask");
+  if (!st) LITHO_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  return st;
+}
+
+int litho_fullchip_lsm_init(litho_ctx* ctx, const litho_partition* p, const float* d_global_mask,
+                            double dx, double dy, int mask_type, int scale, float* d_phi,
+                            float* d_masks) {
+  if (!ctx || !p || !d_global_mask || !d_phi || !d_masks) return LITHO_ERR_INVALID_ARGUMENT;
+  if (!(dx > 0.0) || !(dy > 0.0))
+    return ctx->fail(LITHO_ERR_INVALID_ARGUMENT, "full-chip LSM: dx and dy must be positive");
+  if ((mask_type != LITHO_MASK_BINARY && mask_type != LITHO_MASK_GRAY) ||
+      (mask_type == LITHO_MASK_GRAY && (scale < 1 || scale > 64)))
+    return ctx->fail(LITHO_ERR_INVALID_ARGUMENT, "full-chip LSM: bad mask type or scale");
+  if ((size_t)3 * p->ts * sizeof(float) > 200 * 1024)
+    return ctx->fail(LITHO_ERR_UNSUPPORTED, "reinit_sdf supports at most 17066 columns");
+  if (cudaSetDevice(ctx->device) != cudaSuccess) return ctx->fail(LITHO_ERR_CUDA, "cudaSetDevice");
+  const size_t tt = (size_t)p->ts * p->ts;
+  int st = ctx->ensure_scratch(4 * tt * sizeof(float));
+  if (st) return st;
+  float* shifted = static_cast<float*>(ctx->scratch.base);  // mask - 0.5 of one tile
+  float* work = shifted + tt;                               // 2 tt for the distance transform
+  cudaStream_t s = ctx->stream;
+  // The extracted masks go to d_masks first (they are replaced by the renders below).
+  st = check_launch(ctx, launch_tiles_extract(s, d_global_mask, p->height, p->width, p->ntiles,
+                                              p->d_meta + p->off_origin, p->ts, d_masks),
+                    "tile extraction");
+  for (int t = 0; t < p->ntiles && !st; ++t) {
+    st = check_launch(ctx, launch_levelset(s, 9, p->ts, p->ts, d_masks + t * tt, nullptr, nullptr,
+                                           (float)dx, (float)dy, 0.f, nullptr, shifted, nullptr),
+                      "mask shift");
+    if (!st)
+      st = check_launch(ctx, launch_reinit_sdf(s, p->ts, p->ts, shifted, (float)dx, work,
+                                               d_phi + t * tt),
+                        "reinit_sdf");
+  }
+  if (!st)
+    st = check_launch(ctx, launch_render_mask(s, d_phi, p->ts, p->ts, p->ntiles,
+                                              mask_type == LITHO_MASK_GRAY, scale, d_masks),
+                      "render_levelset_mask");
+  ctx->launches += 2 + 2 * p->ntiles;
+  if (!st) LITHO_CUDA_TRY(ctx, cudaStreamSynchronize(s));
+  return st;
+}
+
+int litho_fullchip_lsm_step(litho_ctx* ctx, const litho_partition* p, const float* d_phi,
+                            const float* d_grad, double dx, double dy, double cfl, double b,
+                            int reinit, int mask_type, int scale, float* d_phi_out,
+                            float* d_masks, double* dt_min, double* dt_max) {
+  if (!ctx || !p || !d_phi || !d_grad || !d_phi_out || !d_masks) return LITHO_ERR_INVALID_ARGUMENT;
+  if (d_phi_out == d_phi)
+    return ctx->fail(LITHO_ERR_INVALID_ARGUMENT, "full-chip LSM: phi_out must not alias phi");
+  if (!(dx > 0.0) || !(dy > 0.0) || !std::isfinite(cfl) || !std::isfinite(b))
+    return ctx->fail(LITHO_ERR_INVALID_ARGUMENT, "full-chip LSM: dx, dy must be positive");
+  if ((mask_type != LITHO_MASK_BINARY && mask_type != LITHO_MASK_GRAY) ||
+      (mask_type == LITHO_MASK_GRAY && (scale < 1 || scale > 64)))
+    return ctx->fail(LITHO_ERR_INVALID_ARGUMENT, "full-chip LSM: bad mask type or scale");
+  if (p->ts < 3) return ctx->fail(LITHO_ERR_SHAPE, "curvature needs at least 3 rows and 3 columns");
+  if ((size_t)3 * p->ts * sizeof(float) > 200 * 1024)
+    return ctx->fail(LITHO_ERR_UNSUPPORTED, "reinit_sdf supports at most 17066 columns");
+  if (cudaSetDevice(ctx->device) != cudaSuccess) return ctx->fail(LITHO_ERR_CUDA, "cudaSetDevice");
+  const size_t tt = (size_t)p->ts * p->ts;
+  const int n = p->ntiles;
+  int st = ctx->ensure_scratch(5 * tt * sizeof(float) + 256 * sizeof(float) + n * sizeof(float));
+  if (st) return st;
+  st = ctx->ensure_red(RED_PART + 2 * 600);
+  if (st) return st;
+  float* vw = static_cast<float*>(ctx->scratch.base);  // windowed speed of one tile
+  float* phi1 = vw + tt;                                // RK2 stage 1
+  float* signs = phi1 + tt;                             // +-0.5 image for reinit
+  float* work = signs + tt;                             // 2 tt: distance transform, then sdf
+  float* dts = work + 2 * tt + 256;                     // one dt per tile
+  cudaStream_t s = ctx->stream;
+  LITHO_CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_red, 0, RED_PART * sizeof(double), s));
+  float* part = reinterpret_cast<float*>(ctx->d_red + RED_PART);
+  float* vmax = reinterpret_cast<float*>(ctx->d_red + RED_SUM);
+  int* bad = reinterpret_cast<int*>(ctx->d_red + RED_FLAG);
+  for (int t = 0; t < n && !st; ++t) {
+    const int* win = p->rects.data() + 16 * (size_t)t + 12;  // update_local (host copy)
+    const float* ph = d_phi + t * tt;
+    float* out = d_phi_out + t * tt;
+    st = check_launch(ctx, launch_levelset(s, 6, p->ts, p->ts, ph, nullptr, d_grad + t * tt,
+                                           (float)dx, (float)dy, 0.f, nullptr, vw, nullptr, win),
+                      "windowed speed");
+    if (!st)
+      st = check_launch(ctx, launch_dt(s, vw, tt, (float)dx, (float)dy, (float)cfl, (float)b, part,
+                                       vmax, dts + t, bad),
+                        "dt");
+    if (!st)
+      st = check_launch(ctx, launch_levelset(s, 3, p->ts, p->ts, ph, nullptr, vw, (float)dx,
+                                             (float)dy, (float)b, dts + t, phi1, nullptr, win),
+                        "rk2 stage 1");
+    if (!st)
+      st = check_launch(ctx, launch_levelset(s, 4, p->ts, p->ts, phi1, ph, vw, (float)dx,
+                                             (float)dy, (float)b, dts + t, out, nullptr, win),
+                        "rk2 stage 2");
+    ctx->launches += 5;
+    if (!st && reinit) {
+      st = check_launch(ctx, launch_levelset(s, 7, p->ts, p->ts, out, nullptr, nullptr, (float)dx,
+                                             (float)dy, 0.f, nullptr, signs, nullptr),
+                        "sign image");
+      if (!st)
+        st = check_launch(ctx, launch_reinit_sdf(s, p->ts, p->ts, signs, (float)dx, work, phi1),
+                          "reinit_sdf");
+      if (!st)
+        st = check_launch(ctx, launch_levelset(s, 8, p->ts, p->ts, phi1, out, nullptr, (float)dx,
+                                               (float)dy, 0.f, nullptr, out, nullptr, win),
+                          "window commit");
+      ctx->launches += 3;
+    }
+  }
+  if (!st)
+    st = check_launch(ctx, launch_render_mask(s, d_phi_out, p->ts, p->ts, n,
+                                              mask_type == LITHO_MASK_GRAY, scale, d_masks),
+                      "render_levelset_mask");
+  ctx->launches += 1;
+  if (st) return st;
+  std::vector<float> h(n);
+  LITHO_CUDA_TRY(ctx, cudaMemcpyAsync(h.data(), dts, n * sizeof(float), cudaMemcpyDeviceToHost, s));
+  st = fetch(ctx, 0);
+  if (st) return st;
+  if (flag_set(ctx)) return ctx->fail(LITHO_ERR_NONFINITE, "normal speed must be finite");
+  if (dt_min) *dt_min = *std::min_element(h.begin(), h.end());
+  if (dt_max) *dt_max = *std::max_element(h.begin(), h.end());
+  return LITHO_OK;
+}
+
+}  // extern "C"

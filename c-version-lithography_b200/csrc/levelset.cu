@@ -153,16 +153,27 @@ struct LsArgs {
   const float* dt;    // device scalar (stages)
   float* out;
   float* out2;        // habs (what 0) or mask (what 4)
+  int wy0, wy1, wx0, wx1;  // update window [wy0, wy1) x [wx0, wx1) (stages 3, 4 and what 6, 8)
 };
 
 __global__ void __launch_bounds__(LS_NT) levelset_kernel(LsArgs a) {
-  if (a.what == 5) {  // printed mask: phi >= 0 (LSM_Optimizer.cpp:128)
+  if (a.what >= 5) {  // elementwise modes
     const int x = blockIdx.x * LS_TX + threadIdx.x % LS_TX;
     for (int r = 0; r < LS_RPT; ++r) {
       const int y = blockIdx.y * LS_TY * LS_RPT + threadIdx.x / LS_TX + r * LS_TY;
       if (y < a.rows && x < a.cols) {
         const size_t i = (size_t)y * a.cols + x;
-        a.out[i] = a.phi[i] >= 0.f ? 1.f : 0.f;
+        const bool in = y >= a.wy0 && y < a.wy1 && x >= a.wx0 && x < a.wx1;
+        if (a.what == 5)         // printed mask: phi >= 0 (LSM_Optimizer.cpp:128)
+          a.out[i] = a.phi[i] >= 0.f ? 1.f : 0.f;
+        else if (a.what == 6)    // speed restricted to the update window
+          a.out[i] = in ? a.vn[i] : 0.f;
+        else if (a.what == 7)    // +-0.5 sign image of phi >= 0 (full_chip_lsm.cpp:229-230)
+          a.out[i] = a.phi[i] >= 0.f ? 0.5f : -0.5f;
+        else if (a.what == 9)    // mask - 0.5 (full_chip_lsm.cpp:143)
+          a.out[i] = a.phi[i] - 0.5f;
+        else                     // commit phi inside the window over phi0 (out may be phi0)
+          a.out[i] = in ? a.phi[i] : a.phi0[i];
       }
     }
     return;
@@ -180,6 +191,13 @@ __global__ void __launch_bounds__(LS_NT) levelset_kernel(LsArgs a) {
     const int y = y0 + ly, x = x0 + lx;
     if (y >= a.rows || x >= a.cols) continue;
     const size_t i = (size_t)y * a.cols + x;
+    if (a.what >= 3 && !(y >= a.wy0 && y < a.wy1 && x >= a.wx0 && x < a.wx1)) {
+      // Outside the update window the step keeps phi (stage 1) / the starting phi (stage 2).
+      const float keep = a.what == 3 ? t[ly + LS_H][lx + LS_H] : __ldg(a.phi0 + i);
+      if (a.what == 4 && a.out2) a.out2[i] = keep >= 0.f ? 1.f : 0.f;
+      a.out[i] = keep;
+      continue;
+    }
     const float speed = a.what == 1 ? 0.f : __ldg(a.vn + i);
     float v;
     if (a.what == 0) {
@@ -209,8 +227,11 @@ static dim3 ls_grid(int rows, int cols) {
 
 cudaError_t launch_levelset(cudaStream_t s, int what, int rows, int cols, const float* phi,
                             const float* phi0, const float* vn, float dx, float dy, float b,
-                            const float* dt, float* out, float* out2) {
-  LsArgs a{rows, cols, what, phi, phi0, vn, dx, dy, b, dt, out, out2};
+                            const float* dt, float* out, float* out2, const int* window) {
+  LsArgs a{rows, cols, what, phi, phi0, vn, dx, dy, b, dt, out, out2, 0, rows, 0, cols};
+  if (window) {
+    a.wy0 = window[0]; a.wy1 = window[1]; a.wx0 = window[2]; a.wx1 = window[3];
+  }
   levelset_kernel<<<ls_grid(rows, cols), LS_NT, 0, s>>>(a);
   return cudaGetLastError();
 }
@@ -241,6 +262,75 @@ __global__ void dt_kernel(const float* __restrict__ part, int n, float dx, float
   const double den = normal + kap;
   *vmax = m;
   *dt = den < 1e-9 ? 1e-3f : (float)(cfl / den);
+}
+
+// ---------------------------------------------------------------- mask rendering
+// render_levelset_mask (levelset_mask_renderer.cpp:7-33), Gray mode: phi (float32)
+// upsampled by `scale` with pixel-centre bilinear interpolation and edge
+// replication (the cv::resize INTER_LINEAR convention), then the fraction of each
+// source pixel's scale x scale subpixels with phi >= 0. Upsampled coordinate X
+// samples the source at u = (X + 0.5) / scale - 0.5: columns floor(u) and
+// floor(u) + 1 with weights 1 - t and t, t = u - floor(u); before the first and
+// from the last source column on the edge value is used alone (t = 0). The two
+// passes are separable: rows first, then columns, each a product sum in FP32.
+// nimg images of rows x cols lie back to back; one thread per source pixel.
+__device__ __forceinline__ void bilinear_coord(int X, int n, double inv, int& i0, int& i1,
+                                               float& w0, float& w1) {
+  float u = (float)((X + 0.5) * inv - 0.5);
+  int i = (int)floorf(u);
+  float t = u - (float)i;
+  if (i < 0) { i = 0; t = 0.f; }
+  if (i >= n - 1) { i = n - 1; t = 0.f; }
+  i0 = i;
+  i1 = min(i + 1, n - 1);
+  w0 = 1.f - t;
+  w1 = t;
+}
+
+__global__ void render_gray_kernel(const float* __restrict__ phi, int rows, int cols, int nimg,
+                                   int scale, float* __restrict__ mask) {
+  const size_t per = (size_t)rows * cols;
+  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= per * nimg) return;
+  const int img = (int)(idx / per);
+  const int y = (int)((idx % per) / cols), x = (int)(idx % cols);
+  const float* p = phi + (size_t)img * per;
+  const double inv = 1.0 / scale;
+  int inside = 0;
+  for (int sy = 0; sy < scale; ++sy) {
+    int r0, r1;
+    float b0, b1;
+    bilinear_coord(y * scale + sy, rows, inv, r0, r1, b0, b1);
+    for (int sx = 0; sx < scale; ++sx) {
+      int c0, c1;
+      float a0, a1;
+      bilinear_coord(x * scale + sx, cols, inv, c0, c1, a0, a1);
+      const float h0 = __fadd_rn(__fmul_rn(p[(size_t)r0 * cols + c0], a0),
+                                 __fmul_rn(p[(size_t)r0 * cols + c1], a1));
+      const float h1 = __fadd_rn(__fmul_rn(p[(size_t)r1 * cols + c0], a0),
+                                 __fmul_rn(p[(size_t)r1 * cols + c1], a1));
+      const float v = __fadd_rn(__fmul_rn(h0, b0), __fmul_rn(h1, b1));
+      inside += v >= 0.f;
+    }
+  }
+  mask[idx] = (float)((double)inside / ((double)scale * scale));
+}
+
+__global__ void render_binary_kernel(const float* __restrict__ phi, size_t n,
+                                     float* __restrict__ mask) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) mask[i] = phi[i] >= 0.f ? 1.f : 0.f;
+}
+
+cudaError_t launch_render_mask(cudaStream_t s, const float* phi, int rows, int cols, int nimg,
+                               int gray, int scale, float* mask) {
+  const size_t n = (size_t)rows * cols * nimg;
+  const unsigned nb = (unsigned)((n + 255) / 256);
+  if (gray)
+    render_gray_kernel<<<nb, 256, 0, s>>>(phi, rows, cols, nimg, scale, mask);
+  else
+    render_binary_kernel<<<nb, 256, 0, s>>>(phi, n, mask);
+  return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------- reinit_sdf

@@ -265,10 +265,19 @@ inline bool tc2_supported(const BandGeom& g) {
 }
 
 // Level set (levelset.cu). what: 0 delta (+|Vn|), 1 kappa term, 2 normal,
-// 3 RK2 stage 1, 4 RK2 stage 2 (+ mask).
+// 3 RK2 stage 1, 4 RK2 stage 2 (+ mask), 5 mask phi >= 0, 6 speed restricted to the
+// window, 7 +-0.5 sign image of phi >= 0, 8 out = phi inside the window, phi0 outside,
+// 9 phi - 0.5.
+// window (host, nullable): {y0, y1, x0, x1}; stages 3 and 4 update only inside it
+// (outside they keep phi / phi0). NULL = the whole grid.
 cudaError_t launch_levelset(cudaStream_t s, int what, int rows, int cols, const float* phi,
                             const float* phi0, const float* vn, float dx, float dy, float b,
-                            const float* dt, float* out, float* out2);
+                            const float* dt, float* out, float* out2,
+                            const int* window = nullptr);
+// render_levelset_mask for nimg images of rows x cols: gray = 0 -> phi >= 0,
+// gray = 1 -> subpixel coverage of the scale-times bilinear upsampling.
+cudaError_t launch_render_mask(cudaStream_t s, const float* phi, int rows, int cols, int nimg,
+                               int gray, int scale, float* mask);
 cudaError_t launch_dt(cudaStream_t s, const float* vn, size_t n, float dx, float dy, float cfl,
                       float b, float* part, float* vmax, float* dt, int* bad);
 // Chamfer signed distance of reinit_sdf; work holds 2 * rows * cols floats.

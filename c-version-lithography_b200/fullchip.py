@@ -12,6 +12,9 @@ Mirrors the reference's full-chip classes:
 * :class:`FullChipCTMOptimizer` - ``FullChipCTMOptimizer::optimize``
   (source/optimizer/full_chip_ctm.cpp:25-152): fixed-step theta descent inside
   each tile's Core + Guard window, best state over all evaluations.
+* :class:`FullChipLSMOptimizer` - ``FullChipLSMOptimizer::optimize``
+  (source/optimizer/full_chip_lsm.cpp:38-254): per-tile SDF from the CTM binary
+  mask, windowed RK2 level-set steps, reinitialisation, Binary / Gray rendering.
 
 Local tiles are one float32 CUDA tensor of shape (num_tiles, tile_size,
 tile_size), tile id = row * grid_cols + col. Every computation runs in the
@@ -307,3 +310,112 @@ class FullChipCTMOptimizer:
         return FullChipCTMResult(best["iteration"], best["loss"],
                                  p.assemble_global(best["masks"]), best["masks"], best["theta"],
                                  masks.clone() if opt.retain_final_masks else None, history)
+
+
+@dataclass
+class FullChipLSMOptions:
+    """FullChipLSMOptions (include/optimizer/full_chip_lsm.h:8-20), PE loss types."""
+    iterations: int = 200
+    dx: float = 1.0
+    dy: float = 1.0
+    cfl: float = 0.7
+    curvature_weight: float = 0.01
+    reinit_interval: int = 20
+    mask_type: str = "Binary"
+    render_scale: int = 4
+    gradient_options: MicroGradientOptions = field(default_factory=MicroGradientOptions)
+    verbose: bool = False
+
+
+@dataclass
+class FullChipLSMIteration:
+    iteration: int
+    loss: float
+    data_loss: float
+    cept_loss: float
+    min_dt: float
+    max_dt: float
+    pe_contribution: float
+    penalty_contribution: float
+    cept_contribution: float
+
+
+@dataclass
+class FullChipLSMResult:
+    best_iteration: int
+    best_loss: float
+    global_mask: object
+    global_phi: object
+    initial_global_phi: object
+    initial_global_mask: object
+    local_masks: object
+    local_phi: object
+    history: List[FullChipLSMIteration]
+
+
+class FullChipLSMOptimizer:
+    """FullChipLSMOptimizer (include/optimizer/full_chip_lsm.h:52-69) over the device
+    partition: per-tile SDF initialisation, exchange, windowed RK2 level-set steps with
+    periodic reinitialisation, rendered masks, best state over all evaluations."""
+
+    def __init__(self, partition: Partition, cache: ImagingCache, threshold: float = 0.25,
+                 alpha: float = 85.0):
+        self.partition = partition
+        self.exchange = MicroGradientExchange(partition, cache, threshold, alpha)
+        self.ctx = partition.ctx
+
+    def optimize(self, initial_binary, global_target,
+                 options: Optional[FullChipLSMOptions] = None) -> FullChipLSMResult:
+        """optimize(initial_binary, global_target, options) (full_chip_lsm.cpp:38-254)."""
+        from . import MASK_TYPES
+        opt = options or FullChipLSMOptions()
+        if opt.mask_type not in MASK_TYPES:
+            raise LithoError(1, f"mask_type must be one of {sorted(MASK_TYPES)}")
+        if opt.iterations < 0:
+            raise LithoError(1, "FullChipLSM iterations must be non-negative")
+        # Core + Guard evaluation and guard-only CEPT (full_chip_lsm.cpp:43-46).
+        go = MicroGradientOptions(**{**opt.gradient_options.__dict__, "loss_region": "CoreGuard",
+                                     "cept_guard_only": True})
+        wpe, wpen = go.weights()
+        p = self.partition
+        torch = self.ctx.torch
+        lib, h = self.ctx.lib, self.ctx.handle
+        mt = MASK_TYPES[opt.mask_type]
+        init = _f32(initial_binary, torch, (p.height, p.width), "initial binary mask")
+        tgt = _f32(global_target, torch, (p.height, p.width), "global target")
+        phi, masks = p.empty_tiles(), p.empty_tiles()
+        self.ctx._check(lib.litho_fullchip_lsm_init(h, p.handle, _ptr(init), opt.dx, opt.dy, mt,
+                                                    opt.render_scale, _ptr(phi), _ptr(masks)))
+        initial_global_phi = p.assemble_global(phi)
+        initial_global_mask = p.assemble_global(masks)
+        history: List[FullChipLSMIteration] = []
+        best = dict(loss=math.inf, iteration=0, phi=None, masks=None)
+
+        def record(it, ev, dmin, dmax):
+            cept = go.cept_weight * ev.cept_loss if go.enable_cept else 0.0
+            history.append(FullChipLSMIteration(
+                it, ev.loss, ev.data_loss, ev.cept_loss, dmin, dmax,
+                sum(wpe * l.pe_loss for l in ev.locals), sum(l.penalty_loss for l in ev.locals),
+                cept))
+            if ev.loss < best["loss"]:
+                best.update(loss=ev.loss, iteration=it, phi=phi.clone(), masks=masks.clone())
+            if opt.verbose:
+                print(f"LSM {it:>3}/{opt.iterations} data={ev.data_loss:.3f} "
+                      f"cept={ev.cept_loss:.3f} total={ev.loss:.3f}")
+
+        ev = self.exchange.compute(masks, tgt, go)
+        record(0, ev, 0.0, 0.0)
+        nxt = p.empty_tiles()
+        dmin, dmax = ctypes.c_double(), ctypes.c_double()
+        for it in range(1, opt.iterations + 1):
+            reinit = 1 if opt.reinit_interval > 0 and it % opt.reinit_interval == 0 else 0
+            self.ctx._check(lib.litho_fullchip_lsm_step(
+                h, p.handle, _ptr(phi), _ptr(ev.mask_gradients), opt.dx, opt.dy, opt.cfl,
+                opt.curvature_weight, reinit, mt, opt.render_scale, _ptr(nxt), _ptr(masks),
+                ctypes.byref(dmin), ctypes.byref(dmax)))
+            phi, nxt = nxt, phi
+            ev = self.exchange.compute(masks, tgt, go)
+            record(it, ev, dmin.value, dmax.value)
+        return FullChipLSMResult(best["iteration"], best["loss"], p.assemble_global(best["masks"]),
+                                 p.assemble_global(best["phi"]), initial_global_phi,
+                                 initial_global_mask, best["masks"], best["phi"], history)

@@ -278,6 +278,31 @@ int litho_fullchip_theta_step(litho_ctx* ctx, const litho_partition* partition,
                               float* d_theta, const float* d_grad, double learning_rate,
                               float* d_masks);
 
+/* render_levelset_mask (source/utils/levelset_mask_renderer.cpp:7-33): Binary = phi >= 0;
+ * Gray = fraction of the scale x scale subpixels of each pixel with phi >= 0 after a
+ * pixel-centre bilinear upsampling (edge replicated) of the float32 phi by scale. */
+#define LITHO_MASK_BINARY 0
+#define LITHO_MASK_GRAY 1
+int litho_render_levelset_mask(litho_ctx* ctx, int rows, int cols, const float* d_phi,
+                               int mask_type, int scale, float* d_mask);
+
+/* Full-chip LSM (source/optimizer/full_chip_lsm.cpp:25-254) on a partition's tiles.
+ * init (:138-146): every tile's phi = reinit_sdf(extracted initial mask - 0.5, dx, dy)
+ * and its mask = render_levelset_mask(phi). step (:208-244): per tile, with the
+ * exchanged mask gradient restricted to the Core + Guard window as normal speed,
+ * the two-stage RK2 update (one CFL dt per tile, evolution term = curvature term -
+ * WENO/Godunov term) inside the window only; with reinit set, the window is then
+ * replaced by reinit_sdf of the +-0.5 sign image of phi >= 0; finally every tile's
+ * mask is rendered. dt_min / dt_max (host, nullable) receive the range of the
+ * tiles' steps. Tiles as for litho_exchange_compute. */
+int litho_fullchip_lsm_init(litho_ctx* ctx, const litho_partition* partition,
+                            const float* d_global_mask, double dx, double dy, int mask_type,
+                            int scale, float* d_phi, float* d_masks);
+int litho_fullchip_lsm_step(litho_ctx* ctx, const litho_partition* partition, const float* d_phi,
+                            const float* d_grad, double dx, double dy, double cfl, double b,
+                            int reinit, int mask_type, int scale, float* d_phi_out,
+                            float* d_masks, double* dt_min, double* dt_max);
+
 /* ------------------------------------------------------------ no-allocation variant
  * litho_lsm_rk2_update_noalloc: the RK2 level-set update of litho_lsm_rk2_update
  * (same kernels, same results) for callers that must not allocate device

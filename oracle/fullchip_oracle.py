@@ -264,3 +264,57 @@ def full_chip_ctm(initial_pattern, global_target, meta, cache, thr, alpha, opt, 
             best = dict(loss=ev["loss"], iteration=it, masks=[m.copy() for m in masks])
     return dict(history=history, best=best, global_mask=assemble_global(best["masks"], meta),
                 thetas=thetas)
+
+
+def full_chip_lsm(initial_binary, global_target, meta, cache, thr, alpha, opt: ExchangeOptions,
+                  iterations, dx=1.0, dy=1.0, cfl=0.7, b=0.01, reinit_interval=20,
+                  mask_type="Binary", render_scale=4):
+    """FullChipLSMOptimizer::optimize (source/optimizer/full_chip_lsm.cpp:25-254), PE types:
+    Core + Guard loss region, guard-only CEPT, per-tile windowed RK2 with its own CFL dt,
+    periodic reinitialisation inside the window, masks rendered from the full local phi."""
+    from . import levelset_oracle as lo
+    opt = dataclasses.replace(opt, loss_region="CoreGuard", cept_guard_only=True)
+    phis, masks = [], []
+    for t in meta.tiles:
+        m = extract_local_tile(initial_binary, t)
+        phi = lo.reinit_sdf(m - 0.5, dx, dy)
+        phis.append(phi)
+        masks.append(lo.render_levelset_mask(phi, mask_type, render_scale))
+    initial_global_phi = assemble_global(phis, meta)
+    ev = exchange(masks, global_target, meta, cache, thr, alpha, opt)
+    history = [dict(iteration=0, loss=ev["loss"], data_loss=ev["data_loss"],
+                    cept_loss=ev["cept_loss"], min_dt=0.0, max_dt=0.0)]
+    best = dict(loss=ev["loss"], iteration=0, phis=[p.copy() for p in phis],
+                masks=[m.copy() for m in masks])
+    for it in range(1, iterations + 1):
+        nphis, nmasks, steps = [], [], []
+        for t in meta.tiles:
+            w = t.update_local
+            win = np.zeros((meta.tile_size, meta.tile_size))
+            win[w.y0:w.y1, w.x0:w.x1] = 1.0
+            phi = phis[t.id]
+            grad = ev["locals"][t.id]["grad"] * win
+            n0, dt = lo.evolution_term(phi, grad, dx, dy, cfl, b)
+            steps.append(dt)
+            phi1 = phi.copy()
+            phi1[w.y0:w.y1, w.x0:w.x1] += dt * n0[w.y0:w.y1, w.x0:w.x1]
+            n1, _ = lo.evolution_term(phi1, grad, dx, dy, cfl, b)
+            nxt = phi.copy()
+            nxt[w.y0:w.y1, w.x0:w.x1] = 0.5 * phi[w.y0:w.y1, w.x0:w.x1] + 0.5 * (
+                phi1[w.y0:w.y1, w.x0:w.x1] + dt * n1[w.y0:w.y1, w.x0:w.x1])
+            if reinit_interval > 0 and it % reinit_interval == 0:
+                signs = (nxt >= 0.0).astype(np.float64) - 0.5
+                sdf = lo.reinit_sdf(signs, dx, dy)
+                nxt[w.y0:w.y1, w.x0:w.x1] = sdf[w.y0:w.y1, w.x0:w.x1]
+            nphis.append(nxt)
+            nmasks.append(lo.render_levelset_mask(nxt, mask_type, render_scale))
+        phis, masks = nphis, nmasks
+        ev = exchange(masks, global_target, meta, cache, thr, alpha, opt)
+        history.append(dict(iteration=it, loss=ev["loss"], data_loss=ev["data_loss"],
+                            cept_loss=ev["cept_loss"], min_dt=min(steps), max_dt=max(steps)))
+        if ev["loss"] < best["loss"]:
+            best = dict(loss=ev["loss"], iteration=it, phis=[p.copy() for p in phis],
+                        masks=[m.copy() for m in masks])
+    return dict(history=history, best=best, global_mask=assemble_global(best["masks"], meta),
+                global_phi=assemble_global(best["phis"], meta),
+                initial_global_phi=initial_global_phi, final_phis=phis)

@@ -151,3 +151,19 @@ def lsm_rk2_update(phi, Gm, dx, dy, cfl, b):
     phi1 = phi + dt * n0
     n1, _ = evolution_term(phi1, Gm, dx, dy, cfl, b)
     return 0.5 * phi + 0.5 * (phi1 + dt * n1), dt
+
+
+def render_levelset_mask(phi: np.ndarray, mask_type: str = "Gray", scale: int = 4) -> np.ndarray:
+    """render_levelset_mask (source/utils/levelset_mask_renderer.cpp:7-33).
+
+    Binary: phi >= 0. Gray: float32 phi bilinearly upsampled by `scale` with
+    cv2.resize(INTER_LINEAR) (the library the reference calls), each scale x scale
+    block of subpixels counted where phi >= 0, divided by scale^2."""
+    phi = np.asarray(phi)
+    if mask_type == "Binary":
+        return (phi >= 0.0).astype(np.float64)
+    import cv2
+    h, w = phi.shape
+    hi = cv2.resize(phi.astype(np.float32), (w * scale, h * scale), interpolation=cv2.INTER_LINEAR)
+    inside = (hi >= 0.0).reshape(h, scale, w, scale).sum(axis=(1, 3))
+    return inside / float(scale * scale)

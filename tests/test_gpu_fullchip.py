@@ -189,3 +189,52 @@ def test_fullchip_errors(L, FC, band128):
     with pytest.raises(L.LithoError) as e:
         ex.compute(masks, tgt)
     assert e.value.status == 3
+
+
+@pytest.mark.parametrize("mask_type", ["Binary", "Gray"])
+def test_fullchip_lsm_matches_oracle(L, FC, band128, mask_type):
+    """FullChipLSMOptimizer (full_chip_lsm.cpp:38-254) against the FP64 oracle: three steps
+    with a reinitialisation after the second, guard-only CEPT and fusion on. FP32 phi
+    differs from FP64 by ~1e-5, so a rendered pixel whose phi is within that of 0 may
+    flip: the loss history is compared to 1e-3 and the best masks to 0.5 % of pixels."""
+    oc, _ = band128
+    cfg = (192, 192, 2, 2, 16, 6)
+    meta = fc.build(*cfg)
+    part = FC.Partition(*cfg)
+    cache = L.ImagingCache.from_kernels(np.stack(oc.kernels), oc.source_ws, oc.eigenvalues)
+    target = make_target(192, 192, 5)
+    opts = dict(enable_cept=True, enable_grad_fusion=True)
+    kw = dict(dx=1.0, dy=1.0, cfl=0.7, b=0.01, reinit_interval=2, mask_type=mask_type,
+              render_scale=4)
+    ref = fc.full_chip_lsm(target, target, meta, oc, THR, ALPHA, fc.ExchangeOptions(**opts), 3, **kw)
+    optz = FC.FullChipLSMOptimizer(part, cache, THR, ALPHA)
+    res = optz.optimize(torch.from_numpy(target.astype(np.float32)).cuda(),
+                        torch.from_numpy(target.astype(np.float32)).cuda(),
+                        FC.FullChipLSMOptions(iterations=3, cfl=0.7, curvature_weight=0.01,
+                                              reinit_interval=2, mask_type=mask_type,
+                                              render_scale=4,
+                                              gradient_options=FC.MicroGradientOptions(**opts)))
+    assert np.allclose(cpu(res.initial_global_phi), ref["initial_global_phi"], atol=1e-5)
+    hist = [h.loss for h in res.history]
+    assert len(hist) == 4
+    assert abs(hist[0] - ref["history"][0]["loss"]) <= 1e-5 * ref["history"][0]["loss"]
+    for a, b in zip(res.history, ref["history"]):
+        assert abs(a.loss - b["loss"]) <= 1e-3 * b["loss"]
+        assert abs(a.min_dt - b["min_dt"]) <= 1e-4 * max(b["min_dt"], 1e-12)
+        assert abs(a.max_dt - b["max_dt"]) <= 1e-4 * max(b["max_dt"], 1e-12)
+    assert res.best_iteration == ref["best"]["iteration"]
+    gm = cpu(res.global_mask)
+    assert (np.abs(gm - ref["global_mask"]) > 1e-6).mean() <= 0.005
+    # phi outside each tile's Core + Guard window keeps its initial SDF values
+    init = [fc.extract_local_tile(target, t) for t in meta.tiles]
+    from oracle import levelset_oracle as lo
+    lp = cpu(res.local_phi)
+    for t in meta.tiles:
+        w = t.update_local
+        out = np.ones((meta.tile_size,) * 2, bool)
+        out[w.y0:w.y1, w.x0:w.x1] = False
+        phi0 = lo.reinit_sdf(init[t.id] - 0.5, 1.0, 1.0)
+        assert np.allclose(lp[t.id][out], phi0[out], atol=1e-5)
+        # the returned masks are the renders of the returned phi
+        assert np.array_equal(cpu(res.local_masks)[t.id],
+                              cpu(L.render_levelset_mask(res.local_phi[t.id], mask_type, 4)))
