@@ -210,7 +210,7 @@ def test_render_levelset_mask_matches_cv2(shape, scale):
     assert np.array_equal(b, lo.render_levelset_mask(phi, "Binary"))
     g = Lm.render_levelset_mask(t, "Gray", scale).cpu().numpy().astype(np.float64)
     ref = lo.render_levelset_mask(phi, "Gray", scale)
-    d = np.abs(g - ref)
-    assert d.max() <= 1.0 / scale ** 2 + 1e-12
-    assert (d > 0).mean() <= 0.005
+    d = np.abs(g - ref)          # coverage is k / scale^2, stored in float32
+    assert d.max() <= 1.0 / scale ** 2 + 1e-6
+    assert (d > 1e-6).mean() <= 0.005
     assert g.min() >= 0.0 and g.max() <= 1.0
