@@ -112,6 +112,8 @@ SIGNATURES = {
     "litho_fullchip_theta_step": (_I, [_P, _P, _P, _P, _D, _P]),
     "litho_lsm_rk2_update_noalloc": (_I, [_P, _I, _I, _P, _P, _D, _D, _D, _D, _P, _P, _PD]),
     "litho_render_levelset_mask": (_I, [_P, _I, _I, _P, _I, _I, _P]),
+    "litho_evaluate_sparse_epe": (_I, [_P, _I, _I, _P, _I, _PD, _PD, _D, _D, _PD, _PD]),
+    "litho_epe_gradient": (_I, [_P, _P, _P, _I, _PD, _PD, _D, _P]),
     "litho_fullchip_lsm_init": (_I, [_P, _P, _P, _D, _D, _I, _I, _P, _P]),
     "litho_fullchip_lsm_step": (_I, [_P, _P, _P, _P, _D, _D, _D, _D, _I, _I, _I, _P, _P, _PD,
                                      _PD]),
@@ -423,6 +425,30 @@ class Gradient:
                         penalty_window=penalty_window, pe_weight=pe_weight, penalty=penalty,
                         penalty_threshold=penalty_threshold)
 
+    def epe_gradient(self, aerial_image, electric_field: Field, eps, weights, threshold):
+        """Gradient::epe_gradient (gradient.cpp:198-227): eps n x 2 (y, x), weights n."""
+        torch = self.ctx.torch
+        N = self.cache.N
+        a = _f32(aerial_image, torch, (N, N), "aerial_image")
+        e = np.ascontiguousarray(np.asarray(eps, dtype=np.float64).reshape(-1, 2))
+        w = np.ascontiguousarray(np.asarray(weights, dtype=np.float64).reshape(-1))
+        if len(w) != len(e):
+            raise LithoError(1, "epe_gradient: eps and weights sizes must match")
+        out = torch.empty((N, N), dtype=torch.float32, device="cuda")
+        self.ctx._check(self.ctx.lib.litho_epe_gradient(
+            self.ctx.handle, electric_field.handle, _ptr(a), len(w), e.ctypes.data_as(_PD),
+            w.ctypes.data_as(_PD), float(threshold), _ptr(out)))
+        return out
+
+
+@dataclass
+class SparseEpeEvaluation:
+    """SparseEpeEvaluation (include/utils/loss.h): per-point signed EPE and totals."""
+    signed_epe_pixel: np.ndarray
+    weighted_squared_loss: float
+    absolute_sum_nm: float
+    active_count: int
+
 
 class Loss:
     """Loss statics (include/utils/loss.h:38-113) evaluated on the device."""
@@ -448,6 +474,24 @@ class Loss:
     def pe_loss_with_penalty(wafer, target, penalty, penalty_threshold, loss_window=None,
                              ctx=None) -> float:
         return Loss._run(wafer, target, loss_window, penalty, penalty_threshold, ctx=ctx)
+
+    @staticmethod
+    def evaluate_sparse_epe(aerial_image, eps, weights, threshold, pixel_size_nm,
+                            ctx=None) -> SparseEpeEvaluation:
+        """Loss::evaluate_sparse_epe (loss.cpp:125-163): eps n x 2 (y, x), weights n."""
+        ctx = ctx or default_context()
+        a = _f32(aerial_image, ctx.torch)
+        e = np.ascontiguousarray(np.asarray(eps, dtype=np.float64).reshape(-1, 2))
+        w = np.ascontiguousarray(np.asarray(weights, dtype=np.float64).reshape(-1))
+        if len(w) != len(e):
+            raise LithoError(1, "evaluate_sparse_epe: eps and weights sizes must match")
+        se = np.empty(len(w), dtype=np.float64)
+        tot = (ctypes.c_double * 3)()
+        ctx._check(ctx.lib.litho_evaluate_sparse_epe(
+            ctx.handle, a.shape[0], a.shape[1], _ptr(a), len(w), e.ctypes.data_as(_PD),
+            w.ctypes.data_as(_PD), float(threshold), float(pixel_size_nm),
+            se.ctypes.data_as(_PD), tot))
+        return SparseEpeEvaluation(se, tot[0], tot[1], int(round(tot[2])))
 
 
 @dataclass

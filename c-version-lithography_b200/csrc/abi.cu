@@ -1641,3 +1641,101 @@ int litho_fullchip_lsm_step(litho_ctx* ctx, const litho_partition* p, const floa
 }
 
 }  // extern "C"
+
+// ============================================================== sparse EPE
+extern "C" {
+
+int litho_evaluate_sparse_epe(litho_ctx* ctx, int rows, int cols, const float* d_aerial,
+                              int n_eps, const double* eps, const double* weights,
+                              double threshold, double pixel_size_nm, double* signed_epe,
+                              double* totals) {
+  if (!ctx || !d_aerial || n_eps < 0 || (n_eps > 0 && (!eps || !weights)))
+    return LITHO_ERR_INVALID_ARGUMENT;
+  if (rows < 3 || cols < 3)
+    return ctx->fail(LITHO_ERR_SHAPE, "evaluate_sparse_epe: the image needs at least 3 x 3 pixels");
+  if (!std::isfinite(threshold) || !std::isfinite(pixel_size_nm))
+    return ctx->fail(LITHO_ERR_NONFINITE, "evaluate_sparse_epe: threshold and pixel size must be finite");
+  if (cudaSetDevice(ctx->device) != cudaSuccess) return ctx->fail(LITHO_ERR_CUDA, "cudaSetDevice");
+  const int n = n_eps;
+  int st = ctx->ensure_scratch((size_t)(4 * n + 4) * sizeof(double));
+  if (st) return st;
+  const int nb = n == 0 ? 1 : (n + 255) / 256;
+  st = ctx->ensure_red(RED_PART + 3 * (size_t)nb + 8);
+  if (st) return st;
+  double* d_eps = static_cast<double*>(ctx->scratch.base);
+  double* d_w = d_eps + 2 * n;
+  double* d_se = d_w + n;
+  cudaStream_t s = ctx->stream;
+  LITHO_CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_red, 0, RED_PART * sizeof(double), s));
+  if (n > 0) {
+    LITHO_CUDA_TRY(ctx, cudaMemcpyAsync(d_eps, eps, 2 * n * sizeof(double), cudaMemcpyHostToDevice, s));
+    LITHO_CUDA_TRY(ctx, cudaMemcpyAsync(d_w, weights, n * sizeof(double), cudaMemcpyHostToDevice, s));
+  }
+  int used = 0;
+  st = check_launch(ctx, launch_epe(s, d_aerial, rows, cols, d_eps, d_w, n, threshold,
+                                    pixel_size_nm, d_se, ctx->d_red + RED_PART, nullptr, &used),
+                    "sparse EPE");
+  if (!st)
+    st = check_launch(ctx, launch_sum_partials(s, ctx->d_red + RED_PART, used, 3,
+                                               ctx->d_red + RED_SUM),
+                      "sum");
+  ctx->launches += 2;
+  if (st) return st;
+  if (signed_epe && n > 0)
+    LITHO_CUDA_TRY(ctx, cudaMemcpyAsync(signed_epe, d_se, n * sizeof(double),
+                                        cudaMemcpyDeviceToHost, s));
+  st = fetch(ctx, 3);
+  if (st) return st;
+  if (totals) std::memcpy(totals, ctx->h_red + RED_SUM, 3 * sizeof(double));
+  return LITHO_OK;
+}
+
+int litho_epe_gradient(litho_ctx* ctx, const litho_field* field, const float* d_aerial,
+                       int n_eps, const double* eps, const double* weights, double threshold,
+                       float* d_grad) {
+  if (!ctx || !field || !d_aerial || !d_grad || n_eps < 0 || (n_eps > 0 && (!eps || !weights)))
+    return LITHO_ERR_INVALID_ARGUMENT;
+  if (!field->valid) return ctx->fail(LITHO_ERR_NOT_READY, "Gradient: field not computed");
+  if (!std::isfinite(threshold))
+    return ctx->fail(LITHO_ERR_NONFINITE, "epe_gradient: threshold must be finite");
+  const Cache& c = *field->cache;
+  const int N = c.g.N;
+  if (N < 3) return ctx->fail(LITHO_ERR_SHAPE, "epe_gradient: the image needs at least 3 x 3 pixels");
+  Layout L;
+  int st = prepare(ctx, c, &L);
+  if (st) return st;
+  const int n = n_eps;
+  const size_t ep_off = align_up(L.total, 256);
+  st = ctx->ensure_scratch(ep_off + (size_t)(3 * n + 4) * sizeof(double));
+  if (st) return st;
+  const int nb = n == 0 ? 1 : (n + 255) / 256;
+  st = ctx->ensure_red(RED_PART + 3 * (size_t)nb + 8);
+  if (st) return st;
+  LITHO_CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_red, 0, RED_PART * sizeof(double), ctx->stream));
+  double* d_eps = at<double>(ctx, ep_off);
+  double* d_w = d_eps + 2 * n;
+  cudaStream_t s = ctx->stream;
+  float* dldi = at<float>(ctx, L.dldi);
+  LITHO_CUDA_TRY(ctx, cudaMemsetAsync(dldi, 0, (size_t)N * N * sizeof(float), s));
+  if (n > 0) {
+    LITHO_CUDA_TRY(ctx, cudaMemcpyAsync(d_eps, eps, 2 * n * sizeof(double), cudaMemcpyHostToDevice, s));
+    LITHO_CUDA_TRY(ctx, cudaMemcpyAsync(d_w, weights, n * sizeof(double), cudaMemcpyHostToDevice, s));
+  }
+  int used = 0;
+  st = check_launch(ctx, launch_epe(s, d_aerial, N, N, d_eps, d_w, n, threshold, 1.0, nullptr,
+                                    ctx->d_red + RED_PART, dldi, &used),
+                    "sparse EPE scatter");
+  ctx->launches += 1;
+  if (st) return st;
+  // dL/dI already holds the 2 of the squared EPE; |E|^2 gives another 2 (gradient.cpp:225-226).
+  GradEpilogue ep{};
+  ep.grad_mask = d_grad;
+  int nb2 = 0;
+  st = run_adjoint(ctx, c, *field, L, dldi, 2.0, ep, &nb2);
+  if (!st) st = fetch(ctx, 0);
+  if (st) return st;
+  if (flag_set(ctx)) return ctx->fail(LITHO_ERR_NONFINITE, "epe_gradient: dL/dI must be finite");
+  return LITHO_OK;
+}
+
+}  // extern "C"

@@ -284,6 +284,14 @@ cudaError_t launch_dt(cudaStream_t s, const float* vn, size_t n, float dx, float
 cudaError_t launch_reinit_sdf(cudaStream_t s, int rows, int cols, const float* phi, float dx,
                               float* work, float* sdf);
 
+// Sparse EPE at host-selected edge points (epe.cu): eps n x 2 (y, x) and weights n,
+// device FP64. signed_epe (nullable) per point; partial: 3 FP64 sums per block
+// (weighted squared loss, |EPE| nm, active count); dldi (nullable): scatter of
+// 2 w (I - thr) / G^2 onto each point's bilinear stencil (atomic adds).
+cudaError_t launch_epe(cudaStream_t s, const float* I, int rows, int cols, const double* eps,
+                       const double* w, int n, double thr, double pixel_nm, double* signed_epe,
+                       double* partial, float* dldi, int* nblocks);
+
 // Full-chip micro tiles (fullchip.cu). Rects are 4 ints (y0, y1, x0, x1) per tile;
 // origins 2 ints (y, x) per tile; rel holds max_rel entries of FC_REL_INTS ints
 // per tile: {neighbour, direction, my_guard[4], neighbour_overlap[4],

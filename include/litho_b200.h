@@ -176,6 +176,27 @@ int litho_ctm_evaluate_host(litho_ctx* ctx, const litho_cache* cache, litho_fiel
                             double alpha, float* h_grad_theta, double* loss,
                             double* grad_norm);
 
+/* ------------------------------------------------------------ sparse EPE
+ * Edge points (EPs) are chosen on the host (EpSelect, source/utils/ep_select.cpp);
+ * eps is n x 2 host doubles (y, x) in subpixel image coordinates, weights n host
+ * doubles (points with weight <= 0 are inactive).
+ * Loss::evaluate_sparse_epe (source/utils/loss.cpp:125-163): per active point the
+ * bilinear samples of I and of |grad I| (LevelSetUtils::_gradient_1d, floored at
+ * 1e-6) give the signed EPE (I - threshold) / |grad I| in pixels. signed_epe (host,
+ * nullable, n) receives it (NaN for inactive points); totals (host, nullable, 3)
+ * receives {sum w EPE^2, sum |EPE| * pixel_size_nm, active count}. */
+int litho_evaluate_sparse_epe(litho_ctx* ctx, int rows, int cols, const float* d_aerial,
+                              int n_eps, const double* eps, const double* weights,
+                              double threshold, double pixel_size_nm, double* signed_epe,
+                              double* totals);
+/* Gradient::epe_gradient (source/utils/gradient.cpp:198-227): with |grad I| frozen,
+ * dL/dI = 2 w (I - threshold) / |grad I|^2 scattered onto each point's bilinear
+ * stencil, back-propagated with output scale 2. The scatter uses atomic adds, so
+ * points whose stencils share a pixel may round differently from run to run. */
+int litho_epe_gradient(litho_ctx* ctx, const litho_field* field, const float* d_aerial,
+                       int n_eps, const double* eps, const double* weights, double threshold,
+                       float* d_grad);
+
 /* ------------------------------------------------------------ level set
  * LevelSetUtils::evolve_normal_WENO_godunov (source/utils/level_set_utils.cpp:150-225):
  * delta = Vn |grad phi|_Godunov with WENO5-JS one-sided derivatives and edge

@@ -269,3 +269,25 @@ def evaluate_sparse_epe(aerial, eps, weights, threshold, pixel_size_nm):
         active += 1
     return dict(signed_epe_pixel=signed, weighted_squared_loss=loss,
                 absolute_sum_nm=abs_nm, active_count=active)
+
+
+def epe_gradient(aerial, fields, cache, eps, weights, threshold):
+    """Gradient::epe_gradient (source/utils/gradient.cpp:198-227): frozen |grad I|,
+    dL/dI = 2 w (I - thr) / G^2 scattered onto the bilinear stencil (bilinear_scatter,
+    source/utils/epe_utils.cpp:76-80), back-propagated with output scale 2."""
+    from .levelset_oracle import gradient_1d
+    gx = gradient_1d(aerial, 1.0, 1)
+    gy = gradient_1d(aerial, 1.0, 0)
+    mag = np.maximum(np.sqrt(gx * gx + gy * gy), 1e-6)
+    N = cache.N
+    dldi = np.zeros((N, N))
+    for i in range(len(weights)):
+        if weights[i] <= 0.0:
+            continue
+        st = bilinear_stencil(N, N, eps[i][0], eps[i][1])
+        a = bilinear_sample(aerial, st)
+        m = max(bilinear_sample(mag, st), 1e-6)
+        g = 2.0 * weights[i] * (a - threshold) / (m * m)
+        for (y, x, w) in st:
+            dldi[y, x] += w * g
+    return backpropagate(dldi, fields, cache, 2.0)

@@ -365,3 +365,50 @@ def test_ctm_evaluate_graph_replay(L, wl, precision):
         assert loss == ref[0] and norm == ref[2]
         assert np.array_equal(g.cpu().numpy(), ref[1])
     assert len(set(counts)) == 1   # replays count the kernels they launch
+
+
+def _edge_points(target, rng, n_extra=20):
+    """Points on the target's 0.5 contour (midpoints between unequal neighbours) plus a
+    few random interior points; weights in [0, 1] with some inactive (0) points."""
+    pts = []
+    ys, xs = np.nonzero(target[:, 1:] != target[:, :-1])
+    pts += [(y + rng.uniform(-0.3, 0.3), x + 0.5) for y, x in zip(ys, xs)]
+    ys, xs = np.nonzero(target[1:, :] != target[:-1, :])
+    pts += [(y + 0.5, x + rng.uniform(-0.3, 0.3)) for y, x in zip(ys, xs)]
+    n = target.shape[0]
+    pts += [(rng.uniform(-1, n), rng.uniform(-1, n)) for _ in range(n_extra)]   # clamped too
+    eps = np.array(pts, dtype=np.float64)
+    w = rng.uniform(0.2, 1.0, len(eps))
+    w[rng.random(len(eps)) < 0.1] = 0.0
+    return eps, w
+
+
+def test_sparse_epe_and_gradient_match_oracle(L, wl):
+    """Loss::evaluate_sparse_epe and Gradient::epe_gradient (loss.cpp:125-163,
+    gradient.cpp:198-227) on real optics at 64 x 64 against the FP64 oracle, the same
+    FP32 aerial image fed to both. Tolerances: signed EPE and totals 1e-9 relative
+    (both FP64 on the same input); gradient relative L2 1e-4."""
+    oc = oo.prepare(64, 4.0, 193.0, 1.35, 0.6, 0.9, use_socs=True)
+    cache = device_cache(L, oc)
+    rng = np.random.default_rng(21)
+    target = np.zeros((64, 64))
+    target[14:40, 20:34] = 1.0
+    target[44:52, 10:50] = 1.0
+    mask = io.theta_to_mask(io.initialize_theta(target) + 0.2 * rng.standard_normal((64, 64)))
+    imaging = L.Imaging(cache)
+    r = imaging.compute(mask, 0.1, 50.0)
+    aerial = r.aerial_image
+    a64 = cpu(aerial)
+    eps, w = _edge_points(target, rng)
+    ev = L.Loss.evaluate_sparse_epe(aerial, eps, w, 0.1, 4.0)
+    ref = io.evaluate_sparse_epe(a64, eps, w, 0.1, 4.0)
+    assert np.array_equal(np.isnan(ev.signed_epe_pixel), np.isnan(ref["signed_epe_pixel"]))
+    ok = ~np.isnan(ref["signed_epe_pixel"])
+    assert np.allclose(ev.signed_epe_pixel[ok], ref["signed_epe_pixel"][ok], rtol=1e-9, atol=1e-12)
+    assert abs(ev.weighted_squared_loss - ref["weighted_squared_loss"]) <= 1e-9 * ref["weighted_squared_loss"]
+    assert abs(ev.absolute_sum_nm - ref["absolute_sum_nm"]) <= 1e-9 * ref["absolute_sum_nm"]
+    assert ev.active_count == ref["active_count"]
+    _, _, fields = io.imaging_compute(mask, oc, 0.1, 50.0, keep_fields=True)
+    g = L.Gradient(cache, 0.1, 50.0).epe_gradient(aerial, imaging.get_electric_field(), eps, w, 0.1)
+    gref = io.epe_gradient(a64, fields, oc, eps, w, 0.1)
+    assert rel_l2(cpu(g), gref) < 1e-4
