@@ -142,6 +142,28 @@ struct ResistEpiT {
     if (p.wafer) st4(p.wafer, i, W, vec, nvalid);
     return g;
   }
+  // dldi4 for four in-range pixels when there is no window and no penalty (the CTM
+  // evaluation): the same arithmetic with pw = qw = 1, which x * 1.f leaves exact.
+  __device__ __forceinline__ float4 plain4(int m, int n, float4 I, float4 T) {
+    const size_t i = (size_t)m * N + n;
+    if (p.aerial) st4(p.aerial, i, I, vec, 4);
+    float4 W, g;
+    auto one_plain = [&](float x, float t, float& w, float& d) {
+      w = sigmoid(x);
+      const float r = w - t;
+      pe += FAST ? (double)(r * r) : (double)r * (double)r;
+      d = p.pe_weight * r * w * (1.f - w);
+    };
+    one_plain(I.x, T.x, W.x, g.x);
+    one_plain(I.y, T.y, W.y, g.y);
+    one_plain(I.z, T.z, W.z, g.z);
+    one_plain(I.w, T.w, W.w, g.w);
+    if (p.wafer) st4(p.wafer, i, W, vec, 4);
+    return g;
+  }
+  __host__ __device__ bool plain() const {
+    return p.pe_window == nullptr && p.pen_window == nullptr && p.penalty == 0.f;
+  }
   // All EPI_NT threads of the CTA must call finish.
   __device__ __forceinline__ void finish() {
     if (p.mode != 1) return;

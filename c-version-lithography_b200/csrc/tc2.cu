@@ -592,7 +592,22 @@ cudaError_t launch_synth_grad_tc2(cudaStream_t s, const void* Aimg, const void* 
 // then the accumulator staging area with the TXD image tile behind it, then the
 // dL/dI tile over the staging area, then the TYD image tile in its place.
 constexpr uint32_t FUSED_TX_OFFSET = 68 * 1024;  // past the 128 x S2_SS float staging area
-template <int BN>
+// dL/dI of an edge tile, written over this thread's own staging chunks. Kept out of
+// line: inlined, its register demand spills the interior path.
+__device__ __noinline__ void edge_dldi(ResistEpiT<true>& epi, float* Ss, int y0, int x0,
+                                       int N) {
+#pragma unroll 1
+  for (int i = 0; i < S2_CHUNKS; ++i) {
+    const int j = threadIdx.x + i * S2_NT;
+    const int r = j >> 5, c = (j & 31) * 4;
+    const int m = y0 + r, n = x0 + c;
+    const int nv = m < N ? min(4, N - n) : 0;
+    float4* sp = reinterpret_cast<float4*>(&Ss[r * S2_SS + c]);
+    *sp = nv > 0 ? epi.dldi4(m, n, *sp, epi.pre4(m, n, nv), nv) : make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+}
+
+template <int BN, bool PLAIN>
 __global__ void __launch_bounds__(S2_NT, 2)
 synth_resist_analysis_kernel(const uint8_t* __restrict__ Aimg, const uint8_t* __restrict__ Bimg,
                              int N, int kp, ResistEpiT<true> epi, Tc2Analysis a,
@@ -673,6 +688,7 @@ synth_resist_analysis_kernel(const uint8_t* __restrict__ Aimg, const uint8_t* __
   if (!fail) {
     const int lane_base = (warp & 3) * 32;
     const int row = lane_base + lane;
+#pragma unroll 1
     for (int q = (warp >> 2) * 4; q < (warp >> 2) * 4 + 4; ++q) {
       float v[16];
       tmem_ld16x(tmem + ((uint32_t)lane_base << 16) + (uint32_t)(16 * q), v);
@@ -691,19 +707,18 @@ synth_resist_analysis_kernel(const uint8_t* __restrict__ Aimg, const uint8_t* __
       for (int i = 0; i < S2_CHUNKS; ++i) {
         const int j = tid + i * S2_NT;
         const int r = j >> 5, c = (j & 31) * 4;
-        pre[i] = epi.dldi4(y0 + r, x0 + c, *reinterpret_cast<const float4*>(&Ss[r * S2_SS + c]),
-                           pre[i], 4);
+        const float4 I4 = *reinterpret_cast<const float4*>(&Ss[r * S2_SS + c]);
+        pre[i] = PLAIN ? epi.plain4(y0 + r, x0 + c, I4, pre[i])
+                       : epi.dldi4(y0 + r, x0 + c, I4, pre[i], 4);
       }
     } else {
-#pragma unroll 1
+      // Edge tiles: dL/dI in place in the staging area, then into pre[] (a rolled
+      // loop may not index pre[], which would move it to local memory).
+      edge_dldi(epi, Ss, y0, x0, N);
+#pragma unroll
       for (int i = 0; i < S2_CHUNKS; ++i) {
         const int j = tid + i * S2_NT;
-        const int r = j >> 5, c = (j & 31) * 4;
-        const int m = y0 + r, n = x0 + c;
-        const int nv = m < N ? min(4, N - n) : 0;
-        pre[i] = nv > 0 ? epi.dldi4(m, n, *reinterpret_cast<const float4*>(&Ss[r * S2_SS + c]),
-                                    epi.pre4(m, n, nv), nv)
-                        : make_float4(0.f, 0.f, 0.f, 0.f);
+        pre[i] = *reinterpret_cast<const float4*>(&Ss[(j >> 5) * S2_SS + (j & 31) * 4]);
       }
     }
   }
@@ -731,21 +746,31 @@ synth_resist_analysis_kernel(const uint8_t* __restrict__ Aimg, const uint8_t* __
   if (warp == 0) tc::tmem_dealloc(tmem, 128);
 }
 
-template <int BN>
-static cudaError_t fused_t(cudaStream_t s, const void* Aimg, const void* Bimg, int N, int kp,
+template <int BN, bool PLAIN>
+static cudaError_t fused_v(cudaStream_t s, const void* Aimg, const void* Bimg, int N, int kp,
                           const ResistEpiT<true>& e, const Tc2Analysis& a, const void* tx,
                           const void* ty, int* err, int* nblocks) {
   const size_t ops = 2 * (size_t)s2_tile_bytes(128, kp);
   const size_t ana = (size_t)FUSED_TX_OFFSET + s2_tile_bytes(BN, 128);
   const size_t smem = (ops > ana ? ops : ana) + 1024;
-  cudaError_t r = cudaFuncSetAttribute(synth_resist_analysis_kernel<BN>,
+  cudaError_t r = cudaFuncSetAttribute(synth_resist_analysis_kernel<BN, PLAIN>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (r != cudaSuccess) return r;
   dim3 grid((N + 127) / 128, (N + 127) / 128);
   *nblocks = grid.x * grid.y;
-  return launch_pdl(synth_resist_analysis_kernel<BN>, grid, dim3(S2_NT), smem, s,
+  return launch_pdl(synth_resist_analysis_kernel<BN, PLAIN>, grid, dim3(S2_NT), smem, s,
                     static_cast<const uint8_t*>(Aimg), static_cast<const uint8_t*>(Bimg), N, kp, e,
                     a, static_cast<const uint8_t*>(tx), static_cast<const uint8_t*>(ty), err);
+}
+
+// No window and no penalty (the CTM evaluation) takes a leaner epilogue: the general one
+// needs more than the 128 registers of two CTAs per SM.
+template <int BN>
+static cudaError_t fused_t(cudaStream_t s, const void* Aimg, const void* Bimg, int N, int kp,
+                          const ResistEpiT<true>& e, const Tc2Analysis& a, const void* tx,
+                          const void* ty, int* err, int* nblocks) {
+  return e.plain() ? fused_v<BN, true>(s, Aimg, Bimg, N, kp, e, a, tx, ty, err, nblocks)
+                   : fused_v<BN, false>(s, Aimg, Bimg, N, kp, e, a, tx, ty, err, nblocks);
 }
 
 cudaError_t launch_synth_resist_analysis_tc2(cudaStream_t s, const void* Aimg, const void* Bimg,
