@@ -116,7 +116,7 @@ struct AnalysisArgs {
   int N, ncols;
   const float2* TY;    // [nr][N] row twiddles
   int nrows_out, nr, sym;
-  float2* part;        // [nrows_out][ncols][tiles]
+  float2* part;        // [tiles][nrows_out][ncols]
 };
 
 template <int BN>
@@ -202,14 +202,13 @@ __device__ void analysis_phase2(float* smem, const AnalysisArgs& a, int y0, int 
         cfma(p11, tb, rb);
       }
       const int row0 = r0 + 2 * rp;
-      const size_t tiles = (size_t)gridDim.x * gridDim.y;
-      float2* out0 = a.part + ((size_t)row0 * a.ncols) * tiles + tile;   // [row][c][tile]
-      if (c0g < a.ncols) out0[(size_t)c0g * tiles] = p00;
-      if (c0g + 1 < a.ncols) out0[(size_t)(c0g + 1) * tiles] = p01;
+      float2* out0 = a.part + ((size_t)tile * a.nrows_out + row0) * a.ncols;  // [tile][row][c]
+      if (c0g < a.ncols) out0[c0g] = p00;
+      if (c0g + 1 < a.ncols) out0[c0g + 1] = p01;
       if (row0 + 1 < a.nrows_out) {
-        float2* out1 = out0 + (size_t)a.ncols * tiles;
-        if (c0g < a.ncols) out1[(size_t)c0g * tiles] = p10;
-        if (c0g + 1 < a.ncols) out1[(size_t)(c0g + 1) * tiles] = p11;
+        float2* out1 = out0 + a.ncols;
+        if (c0g < a.ncols) out1[c0g] = p10;
+        if (c0g + 1 < a.ncols) out1[c0g + 1] = p11;
       }
     }
   }
@@ -236,8 +235,8 @@ int analysis_tiles(int N) {
 }
 
 // Tile partials of sum_{y, x} T(a, y) A[y][x] tw(c, x) for every 128 x 128 tile:
-// part[a][c][tile], tiles in row-major order of the tile grid (each band entry's
-// partials contiguous, for the reduction).
+// part[tile][a][c], tiles in row-major order of the tile grid (each tile's partials
+// contiguous, so that the tensor-core epilogue writes them as one coalesced block).
 cudaError_t launch_analysis(cudaStream_t s, int mode, const float* in, float* mask_out,
                             int* flag, const float* tw, int N, int ncols, const float2* TY,
                             int nrows_out, int nr, int sym, float2* part) {
@@ -253,41 +252,44 @@ cudaError_t launch_analysis(cudaStream_t s, int mode, const float* in, float* ma
   return analysis_tile_t<8>(s, a);
 }
 
-// out[o] = scale * sum_t part[o][t] in a fixed tree order (one warp per output,
-// reading the entry's partials contiguously).
-__global__ void __launch_bounds__(256)
+// out[o] = scale * sum_t part[t][o] in a fixed order: RT_G tile groups (group g sums
+// tiles g, g + RT_G, ... in turn), then a fixed tree over the groups. A CTA covers
+// RT_E consecutive entries, so each group's loads are coalesced.
+constexpr int RT_E = 16, RT_G = 32;
+__global__ void __launch_bounds__(RT_E * RT_G)
 reduce_tiles_kernel(const float2* __restrict__ part, int tiles, int count, float scale,
                     float2* __restrict__ out) {
   pdl_trigger();
   pdl_wait();
-  const int o = blockIdx.x * 8 + (threadIdx.x >> 5);
-  const int lane = threadIdx.x & 31;
-  if (o >= count) return;
-  float2 v0 = make_float2(0.f, 0.f), v1 = v0;
-  int t = lane;
-  for (; t + 32 < tiles; t += 64) {
-    const float2 p = part[(size_t)o * tiles + t];
-    const float2 q = part[(size_t)o * tiles + t + 32];
-    v0.x += p.x; v0.y += p.y;
-    v1.x += q.x; v1.y += q.y;
+  __shared__ float2 sh[RT_G][RT_E];
+  const int e = threadIdx.x % RT_E, g = threadIdx.x / RT_E;
+  const int o = blockIdx.x * RT_E + e;
+  float2 v = make_float2(0.f, 0.f);
+  if (o < count) {
+#pragma unroll 8
+    for (int t = g; t < tiles; t += RT_G) {
+      const float2 p = __ldg(part + (size_t)t * count + o);
+      v.x += p.x;
+      v.y += p.y;
+    }
   }
-  if (t < tiles) {
-    const float2 p = part[(size_t)o * tiles + t];
-    v0.x += p.x; v0.y += p.y;
-  }
-  float vx = v0.x + v1.x, vy = v0.y + v1.y;
+  sh[g][e] = v;
+  __syncthreads();
 #pragma unroll
-  for (int off = 16; off > 0; off >>= 1) {
-    vx += __shfl_xor_sync(0xffffffffu, vx, off);
-    vy += __shfl_xor_sync(0xffffffffu, vy, off);
+  for (int h = RT_G / 2; h > 0; h >>= 1) {
+    if (g < h) {
+      sh[g][e].x += sh[g + h][e].x;
+      sh[g][e].y += sh[g + h][e].y;
+    }
+    __syncthreads();
   }
-  if (lane == 0) out[o] = make_float2(vx * scale, vy * scale);
+  if (g == 0 && o < count) out[o] = make_float2(sh[0][e].x * scale, sh[0][e].y * scale);
 }
 
 cudaError_t launch_reduce_tiles(cudaStream_t s, const float2* part, int tiles, int count,
                                 float scale, float2* out) {
-  return launch_pdl(reduce_tiles_kernel, dim3((count + 7) / 8), dim3(256), 0, s, part, tiles, count,
-                    scale, out);
+  return launch_pdl(reduce_tiles_kernel, dim3((count + RT_E - 1) / RT_E), dim3(RT_E * RT_G), 0, s,
+                    part, tiles, count, scale, out);
 }
 
 // ---------------------------------------------------------------- row synthesis

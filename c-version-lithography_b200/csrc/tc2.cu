@@ -253,11 +253,13 @@ __device__ __forceinline__ void analysis_stages(uint8_t* sA, uint8_t* sB, const 
   }
   __syncthreads();
   tc::fence_after();
+  // P (TMEM) -> the tile's partials, staged in sA (the row-twiddle tile is dead once
+  // stage 2 has completed) as [row][c], then copied out as one contiguous block.
+  const int count = a.nrows_out * a.ncols;
+  float2* stage = reinterpret_cast<float2*>(sA);
   if (!*fail) {
     const int n = lane_base + lane;
     const int r = n >> 1, s = n & 1;
-    const size_t tiles = (size_t)gridDim.x * gridDim.y;
-    float2* out = a.part + (size_t)(yt * gridDim.x + xt);   // [row][c][tile]
     for (int q = warp >> 2; q < BN / 16; q += 2) {
       float qv[16], pv[16];
       tmem_ld16x(tmem + ((uint32_t)lane_base << 16) + (uint32_t)(16 * q), qv);
@@ -270,14 +272,19 @@ __device__ __forceinline__ void analysis_stages(uint8_t* sA, uint8_t* sB, const 
         if (c >= a.ncols) break;
         const float o0 = qv[2 * i], o1 = qv[2 * i + 1], p0 = pv[2 * i], p1 = pv[2 * i + 1];
         if (!a.sym) {
-          if (s == 0) out[((size_t)r * a.ncols + c) * tiles] = make_float2(o0 - p1, o1 + p0);
+          if (s == 0) stage[r * a.ncols + c] = make_float2(o0 - p1, o1 + p0);
         } else if (s == 0) {
-          out[((size_t)(a.nr - 1 + r) * a.ncols + c) * tiles] = make_float2(o0 - p1, o1 + p0);
+          stage[(a.nr - 1 + r) * a.ncols + c] = make_float2(o0 - p1, o1 + p0);
         } else if (r >= 1) {
-          out[((size_t)(a.nr - 1 - r) * a.ncols + c) * tiles] = make_float2(p0 + o1, p1 - o0);
+          stage[(a.nr - 1 - r) * a.ncols + c] = make_float2(p0 + o1, p1 - o0);
         }
       }
     }
+  }
+  __syncthreads();
+  if (!*fail) {
+    float2* out = a.part + (size_t)(yt * gridDim.x + xt) * count;   // [tile][row][c]
+    for (int e = tid; e < count; e += blockDim.x) out[e] = stage[e];
   }
 }
 
@@ -401,6 +408,8 @@ bool tc2_analysis_supported(int ncols, int nr) {
 cudaError_t launch_analysis_tc2(cudaStream_t s, int mode, const float* in, float* mask_out,
                                 int* flag, int N, int ncols, int nrows_out, int nr, int sym,
                                 float2* part, const void* tx_img, const void* ty_img, int* err) {
+  // The epilogue stages the tile's partials in the 64 KiB operand area.
+  if ((size_t)nrows_out * ncols * sizeof(float2) > A2_A_BYTES) return cudaErrorInvalidValue;
   const int vec4 = (N % 4 == 0) && (reinterpret_cast<uintptr_t>(in) % 16 == 0);
   Tc2Analysis a{in, mask_out, flag, N, mode, vec4, ncols, nrows_out, nr, sym, part};
   switch (tc2_analysis_rows(ncols)) {
@@ -779,6 +788,7 @@ cudaError_t launch_synth_resist_analysis_tc2(cudaStream_t s, const void* Aimg, c
                                              const void* ty_img, int* err, int* nblocks) {
   const int vec = N % 4 == 0 && aligned16(ep.aerial) && aligned16(ep.wafer) &&
                   aligned16(ep.target) && aligned16(ep.pe_window) && aligned16(ep.pen_window);
+  if ((size_t)(2 * nr - 1) * ncols * sizeof(float2) > A2_A_BYTES) return cudaErrorInvalidValue;
   const ResistEpiT<true> e{ep, N, vec, 0.0, 0.0};
   const Tc2Analysis a{nullptr, nullptr, flag, N, 0, 0, ncols, 2 * nr - 1, nr, 1, part};
   switch (tc2_analysis_rows(ncols)) {
