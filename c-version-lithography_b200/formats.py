@@ -7,13 +7,18 @@
 * :func:`binarize`, :func:`binarize_otsu` - ``Imbinarize::binarize`` /
   ``binarize_OTSU`` (source/utils/imbinarize.cpp:12-37): the gray CTM mask scaled to
   8 bits and thresholded with OpenCV's adaptive Gaussian or Otsu threshold, the
-  same library calls the reference makes, giving the 0/1 mask that seeds LSM.
+  same library calls the reference makes.
+* :func:`binarize_advanced` - ``Imbinarize::binarize_advanced``
+  (source/utils/imbinarize.cpp:84-189), the CTM -> LSM hand-off of the demos: peak
+  quantile threshold, small-component removal, SRAFs kept outside a keep-out disk
+  around the target, final small-component pass.
 
 These run once per optimisation on the host; they accept NumPy arrays or tensors.
 """
 from __future__ import annotations
 
 import os
+from dataclasses import dataclass
 
 import numpy as np
 
@@ -82,3 +87,72 @@ def binarize_otsu(gray_mask) -> np.ndarray:
     import cv2
     _, bw = cv2.threshold(_gray_u8(gray_mask), 0, 255, cv2.THRESH_BINARY | cv2.THRESH_OTSU)
     return bw.astype(np.float64) / 255.0
+
+
+@dataclass
+class BinarizeResult:
+    """BinarizeResult (include/utils/imbinarize.h:13-20): 0/1 float64 masks."""
+    initial_binary_mask: np.ndarray
+    filtered_binary_mask: np.ndarray
+    sraf_mask_initial: np.ndarray
+    sraf_mask_final: np.ndarray
+    final_mask: np.ndarray
+    keep_out_zone: np.ndarray
+
+
+def _quantile_linear(vals: np.ndarray, q: float) -> float:
+    """_quantile (imbinarize.cpp:50-63): order statistics at floor/ceil of q (n - 1),
+    then v_lo + (v_hi - v_lo) (pos - lo)."""
+    if vals.size == 0:
+        return 0.0
+    q = min(max(q, 0.0), 1.0)
+    pos = q * (vals.size - 1)
+    lo, hi = int(np.floor(pos)), int(np.ceil(pos))
+    v = np.sort(vals)
+    if lo == hi:
+        return float(v[lo])
+    return float(v[lo] + (v[hi] - v[lo]) * (pos - lo))
+
+
+def _drop_small_components(bin01: np.ndarray, area_threshold: int) -> np.ndarray:
+    """8-connected components (OpenCV, CV_32S labels) with area < area_threshold cleared."""
+    import cv2
+    n, labels, stats, _ = cv2.connectedComponentsWithStats(bin01, connectivity=8, ltype=cv2.CV_32S)
+    small = np.zeros(n, dtype=bool)
+    small[1:] = stats[1:, cv2.CC_STAT_AREA] < area_threshold
+    out = bin01.copy()
+    out[small[labels]] = 0
+    return out
+
+
+def binarize_advanced(gray_mask, target_pattern, peak_min_intensity: float = 0.1,
+                      quantile_val: float = 0.2, area_threshold: int = 50,
+                      min_spacing_pixels: int = 15) -> BinarizeResult:
+    """Imbinarize::binarize_advanced (imbinarize.cpp:84-189)."""
+    import cv2
+    gray = _numpy(gray_mask)
+    tgt = _numpy(target_pattern)
+    if gray.shape != tgt.shape:
+        raise ValueError("binarize_advanced: gray mask and target sizes must match")
+    H, W = gray.shape
+    # peak_local_max(min_distance=1): >= its 3x3 dilation and > peak_min_intensity.
+    dil = cv2.dilate(gray, cv2.getStructuringElement(cv2.MORPH_RECT, (3, 3)))
+    peaks = gray[(gray >= dil) & (gray > peak_min_intensity)]
+    if peaks.size == 0:
+        z = np.zeros((H, W))
+        return BinarizeResult(z, z.copy(), z.copy(), z.copy(), z.copy(), z.copy())
+    thr = _quantile_linear(peaks, quantile_val)
+    initial = (gray >= thr).astype(np.uint8)
+    filtered = _drop_small_components(initial, area_threshold)
+    tgt_bin = (tgt > 0.5).astype(np.uint8)
+    sraf_initial = filtered * (1 - tgt_bin)
+    sraf_final = sraf_initial.copy()
+    keep_out = np.zeros((H, W), dtype=np.uint8)
+    if min_spacing_pixels > 0:
+        k = 2 * min_spacing_pixels + 1
+        keep_out = cv2.dilate(tgt_bin, cv2.getStructuringElement(cv2.MORPH_ELLIPSE, (k, k)))
+        sraf_final = sraf_initial * (1 - keep_out)
+    final = _drop_small_components(np.bitwise_or(tgt_bin, sraf_final), area_threshold)
+    f = lambda m: m.astype(np.float64)
+    return BinarizeResult(f(initial), f(filtered), f(sraf_initial), f(sraf_final), f(final),
+                          f(keep_out))
