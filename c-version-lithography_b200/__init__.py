@@ -71,6 +71,14 @@ class ExchangeOptionsC(ctypes.Structure):
                 ("fusion_weight_neighbor", _D)]
 
 
+class ExchangeEpeC(ctypes.Structure):
+    """litho_exchange_epe (include/litho_b200.h)."""
+    _fields_ = [("epe_weight", _D), ("main_region_dilation_pixels", _I), ("epe_pixel_size", _D),
+                ("collect_core_metrics", _I), ("eps", _PD), ("weights", _PD), ("n_eps", _I)]
+
+
+EXCHANGE_TILE_METRICS = 17
+
 SIGNATURES = {
     "litho_version": (_I, []),
     "litho_status_string": (ctypes.c_char_p, [_I]),
@@ -109,6 +117,9 @@ SIGNATURES = {
     "litho_partition_assemble": (_I, [_P, _P, _P, _P]),
     "litho_exchange_compute": (_I, [_P, _P, _P, _P, _P, _D, _D,
                                     ctypes.POINTER(ExchangeOptionsC), _P, _P, _PD, _PD]),
+    "litho_exchange_compute_epe": (_I, [_P, _P, _P, _P, _P, _D, _D,
+                                        ctypes.POINTER(ExchangeOptionsC),
+                                        ctypes.POINTER(ExchangeEpeC), _P, _P, _PD, _PD]),
     "litho_fullchip_theta_step": (_I, [_P, _P, _P, _P, _D, _P]),
     "litho_lsm_rk2_update_noalloc": (_I, [_P, _I, _I, _P, _P, _D, _D, _D, _D, _P, _P, _PD]),
     "litho_render_levelset_mask": (_I, [_P, _I, _I, _P, _I, _I, _P]),

@@ -1197,8 +1197,18 @@ struct litho_partition {
   float2* fe = nullptr;
   float2* fm = nullptr;
   size_t fe_n = 0, fm_n = 0;
-  double* d_loss = nullptr;  // 2 per tile (PE, background penalty) then 1 per tile (CEPT)
+  // Loss sums: kSlots per tile (see litho_exchange_compute_epe), then 1 per tile (CEPT).
+  static constexpr int kSlots = 14;
+  double* d_loss = nullptr;
   std::vector<double> h_loss;
+  // EPE work, allocated when an EPE term or the Core metrics are asked for: EPE
+  // windows, the PE_EPE main region and its row-pass temporary (ntiles * ts * ts
+  // each), then one tile each of aerial and wafer image.
+  float* d_epe_work = nullptr;
+  size_t epe_work_n = 0;
+  // EPs as uploaded (y, x | w) and one tile's candidates (y, x | w), in doubles.
+  double* d_ep = nullptr;
+  size_t ep_n = 0;
 };
 
 namespace {
@@ -1222,6 +1232,8 @@ void free_partition(litho_partition* p) {
   if (p->fe) cudaFree(p->fe);
   if (p->fm) cudaFree(p->fm);
   if (p->d_loss) cudaFree(p->d_loss);
+  if (p->d_epe_work) cudaFree(p->d_epe_work);
+  if (p->d_ep) cudaFree(p->d_ep);
 }
 
 }  // namespace
@@ -1357,28 +1369,37 @@ int litho_partition_assemble(litho_ctx* ctx, const litho_partition* p, const flo
                       "tile assembly");
 }
 
-int litho_exchange_compute(litho_ctx* ctx, const litho_partition* cp, const litho_cache* cache,
-                           const float* d_masks, const float* d_global_target, double threshold,
-                           double alpha, const litho_exchange_options* opt, float* d_raw,
-                           float* d_grad, double* tile_losses, double* totals) {
+int litho_exchange_compute_epe(litho_ctx* ctx, const litho_partition* cp, const litho_cache* cache,
+                               const float* d_masks, const float* d_global_target, double threshold,
+                               double alpha, const litho_exchange_options* opt,
+                               const litho_exchange_epe* epe_in, float* d_raw, float* d_grad,
+                               double* tile_metrics, double* totals) {
   if (!ctx || !cp || !cache || !d_masks || !d_global_target || !d_grad)
     return LITHO_ERR_INVALID_ARGUMENT;
   auto* p = const_cast<litho_partition*>(cp);  // owns mutable work buffers only
   litho_exchange_options o{LITHO_MICRO_LOSS_PE, LITHO_MICRO_REGION_CORE, 1.0, 2.0, 0.01, 0, 0,
                            1.1, 0, LITHO_FUSION_AVERAGE, 0.5, 0.5};
   if (opt) o = *opt;
-  if ((o.loss_type != LITHO_MICRO_LOSS_PE && o.loss_type != LITHO_MICRO_LOSS_PE_PENALTY) ||
+  litho_exchange_epe e{1.0, 2, 1.0, 0, nullptr, nullptr, 0};
+  if (epe_in) e = *epe_in;
+  if (o.loss_type < LITHO_MICRO_LOSS_PE || o.loss_type > LITHO_MICRO_LOSS_PE_EPE ||
       (o.loss_region != LITHO_MICRO_REGION_CORE && o.loss_region != LITHO_MICRO_REGION_CORE_GUARD) ||
       (o.fusion_mode != LITHO_FUSION_AVERAGE && o.fusion_mode != LITHO_FUSION_LINEAR))
     return ctx->fail(LITHO_ERR_UNSUPPORTED, "MicroGradientOptions: unsupported loss type, region or fusion mode");
-  const double w8[] = {o.pe_weight, o.penalty_weight, o.penalty_threshold, o.cept_weight,
-                       o.fusion_weight_owner, o.fusion_weight_neighbor, threshold, alpha};
-  if (!finite_all(w8, 8))
+  const double w10[] = {o.pe_weight, o.penalty_weight, o.penalty_threshold, o.cept_weight,
+                        o.fusion_weight_owner, o.fusion_weight_neighbor, threshold, alpha,
+                        e.epe_weight, e.epe_pixel_size};
+  if (!finite_all(w10, 10))
     return ctx->fail(LITHO_ERR_NONFINITE, "MicroGradientOptions: weights must be finite");
   if (o.enable_grad_fusion && (o.fusion_weight_owner < 0.0 || o.fusion_weight_neighbor < 0.0 ||
                                o.fusion_weight_owner + o.fusion_weight_neighbor <= 0.0))
     return ctx->fail(LITHO_ERR_INVALID_ARGUMENT,
                      "MicroGradientOptions: fusion weights must be non-negative with a positive sum");
+  if (e.n_eps < 0 || (e.n_eps > 0 && (!e.eps || !e.weights)) || e.main_region_dilation_pixels < 0)
+    return ctx->fail(LITHO_ERR_INVALID_ARGUMENT,
+                     "MicroGradientOptions: EPs need coordinates and weights; dilation must be >= 0");
+  if (!finite_all(e.eps, 2 * (size_t)e.n_eps) || !finite_all(e.weights, (size_t)e.n_eps))
+    return ctx->fail(LITHO_ERR_NONFINITE, "MicroGradientExchange: EP coordinates and weights must be finite");
   if (cache->g.N != p->ts)
     return ctx->fail(LITHO_ERR_SHAPE, "MicroGradientExchange: cache N must equal the tile size");
   if (d_raw && d_raw == d_grad)
@@ -1386,15 +1407,47 @@ int litho_exchange_compute(litho_ctx* ctx, const litho_partition* cp, const lith
   Layout L;
   int st = prepare(ctx, *cache, &L);
   if (st) return st;
-  const int n = p->ntiles;
-  const size_t tt = (size_t)p->ts * p->ts;
+  const int n = p->ntiles, ts = p->ts;
+  const size_t tt = (size_t)ts * ts;
+  const int S = litho_partition::kSlots;
+  const bool epe_terms = o.loss_type == LITHO_MICRO_LOSS_EPE || o.loss_type == LITHO_MICRO_LOSS_PE_EPE;
+  const bool core = e.collect_core_metrics != 0;
+  const bool eval_epe = epe_terms || core;   // micro_gradient_exchange.cpp:144-148
+  const bool guard_region = o.loss_region == LITHO_MICRO_REGION_CORE_GUARD;
+  const int periods = guard_region ? 1 : 0;
+  const size_t ncand = (size_t)e.n_eps * (2 * periods + 1) * (2 * periods + 1);
+  if (ncand > (size_t)1 << 30)
+    return ctx->fail(LITHO_ERR_INVALID_ARGUMENT, "MicroGradientExchange: too many EPs");
   if (!p->d_work) {
     if (cudaMalloc(&p->d_work, 4 * n * tt * sizeof(float)) != cudaSuccess ||
-        cudaMalloc(&p->d_loss, 3 * (size_t)n * sizeof(double)) != cudaSuccess) {
+        cudaMalloc(&p->d_loss, (size_t)(S + 1) * n * sizeof(double)) != cudaSuccess) {
       cudaGetLastError();
       return ctx->fail(LITHO_ERR_OOM, "full-chip work allocation failed");
     }
-    p->h_loss.assign(3 * (size_t)n, 0.0);
+    p->h_loss.assign((size_t)(S + 1) * n, 0.0);
+  }
+  const size_t epe_work_n = eval_epe ? (3 * n + 2) * tt : 0;
+  const size_t ep_n = eval_epe ? 3 * ((size_t)e.n_eps + ncand) : 0;
+  if (p->epe_work_n < epe_work_n || p->ep_n < ep_n) {
+    LITHO_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    if (p->epe_work_n < epe_work_n) {
+      if (p->d_epe_work) cudaFree(p->d_epe_work);
+      p->d_epe_work = nullptr; p->epe_work_n = 0;
+      if (cudaMalloc(&p->d_epe_work, epe_work_n * sizeof(float)) != cudaSuccess) {
+        cudaGetLastError();
+        return ctx->fail(LITHO_ERR_OOM, "full-chip EPE work allocation failed");
+      }
+      p->epe_work_n = epe_work_n;
+    }
+    if (p->ep_n < ep_n) {
+      if (p->d_ep) cudaFree(p->d_ep);
+      p->d_ep = nullptr; p->ep_n = 0;
+      if (cudaMalloc(&p->d_ep, ep_n * sizeof(double)) != cudaSuccess) {
+        cudaGetLastError();
+        return ctx->fail(LITHO_ERR_OOM, "full-chip EP allocation failed");
+      }
+      p->ep_n = ep_n;
+    }
   }
   const BandGeom& g = cache->g;
   const size_t fe_n = (size_t)g.K * g.Pr * g.Pc, fm_n = (size_t)g.Nr * g.Nc;
@@ -1410,78 +1463,214 @@ int litho_exchange_compute(litho_ctx* ctx, const litho_partition* cp, const lith
     }
     p->fe_n = fe_n; p->fm_n = fm_n;
   }
+  // Per-block partials of the EPE and rectangle sums share the reduction area.
+  const int epe_blocks = ncand == 0 ? 1 : (int)((ncand + 255) / 256);
+  st = ctx->ensure_red(RED_PART + 3 * (size_t)std::max(epe_blocks, 64) + 8);
+  if (st) return st;
+  LITHO_CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_red, 0, RED_PART * sizeof(double), ctx->stream));
   float* targets = p->d_work;
   float* pe_w = targets + n * tt;
   float* pen_w = pe_w + n * tt;
   float* raw = d_raw ? d_raw : pen_w + n * tt;
+  float* epe_w = eval_epe ? p->d_epe_work : nullptr;
+  float* main_dil = eval_epe ? epe_w + n * tt : nullptr;
+  float* dil_tmp = eval_epe ? main_dil + n * tt : nullptr;
+  float* aerial = eval_epe ? dil_tmp + n * tt : nullptr;
+  float* wafer = eval_epe ? aerial + tt : nullptr;
+  double* ep_in = p->d_ep;                                   // 2 n_eps coordinates | n_eps weights
+  double* cand = eval_epe ? ep_in + 3 * (size_t)e.n_eps : nullptr;   // 2 ncand | ncand
   Field f;
   f.cache = cache; f.e = p->fe; f.mband = p->fm;
   cudaStream_t s = ctx->stream;
+  float* dldi = at<float>(ctx, L.dldi);
+  double* part = ctx->d_red + RED_PART;
+  LITHO_CUDA_TRY(ctx, cudaMemsetAsync(p->d_loss, 0, (size_t)(S + 1) * n * sizeof(double), s));
+  if (eval_epe && e.n_eps > 0) {
+    LITHO_CUDA_TRY(ctx, cudaMemcpyAsync(ep_in, e.eps, 2 * (size_t)e.n_eps * sizeof(double),
+                                        cudaMemcpyHostToDevice, s));
+    LITHO_CUDA_TRY(ctx, cudaMemcpyAsync(ep_in + 2 * (size_t)e.n_eps, e.weights,
+                                        (size_t)e.n_eps * sizeof(double), cudaMemcpyHostToDevice, s));
+  }
   st = check_launch(ctx, launch_tiles_extract(s, d_global_target, p->height, p->width, n,
-                                              p->d_meta + p->off_origin, p->ts, targets),
+                                              p->d_meta + p->off_origin, ts, targets),
                     "target extraction");
+  const bool pe_epe = o.loss_type == LITHO_MICRO_LOSS_PE_EPE;
+  if (!st && pe_epe)
+    st = check_launch(ctx, launch_dilate_main(s, targets, n, ts, e.main_region_dilation_pixels,
+                                              dil_tmp, main_dil),
+                      "main-region dilation");
   if (!st)
-    st = check_launch(ctx, launch_loss_windows(
-                               s, targets, n, p->ts,
-                               p->d_meta + (o.loss_region == LITHO_MICRO_REGION_CORE_GUARD
-                                                ? p->off_update : p->off_core_l),
-                               o.loss_type == LITHO_MICRO_LOSS_PE_PENALTY, pe_w, pen_w),
+    st = check_launch(ctx, launch_loss_windows(s, targets, n, ts,
+                                               p->d_meta + (guard_region ? p->off_update : p->off_core_l),
+                                               o.loss_type, pe_epe ? main_dil : nullptr, pe_w, pen_w,
+                                               epe_w),
                       "loss windows");
-  ctx->launches += 2;
-  // micro_loss_weights (micro_gradient_exchange.cpp:95-99): the penalty term only for PEPenalty.
-  const double wpe = o.pe_weight;
+  ctx->launches += 2 + (pe_epe ? 2 : 0);
+  // micro_loss_weights (micro_gradient_exchange.cpp:95-99).
+  const double wpe = o.loss_type == LITHO_MICRO_LOSS_EPE ? 0.0 : o.pe_weight;
+  const double wepe = epe_terms ? e.epe_weight : 0.0;
   const double wpen = o.loss_type == LITHO_MICRO_LOSS_PE_PENALTY ? o.penalty_weight : 0.0;
+  // One adjoint per tile: dL/dI = PE part (written by the resist epilogue, adjoint scale
+  // 4 alpha) + wepe * EPE part (adjoint scale 2), the latter pre-scaled onto 4 alpha.
+  const bool epe_grad = epe_terms && wepe != 0.0;
+  double adj_scale = 4.0 * alpha, epe_fac = 0.0;
+  bool zero_pe_dldi = false;
+  if (epe_grad) {
+    if (adj_scale != 0.0) {
+      epe_fac = 2.0 * wepe / adj_scale;
+    } else {
+      adj_scale = 2.0 * wepe;   // alpha = 0: the PE part is multiplied by 0 anyway
+      epe_fac = 1.0;
+      zero_pe_dldi = true;
+    }
+  }
   for (int t = 0; t < n && !st; ++t) {
+    const int* R = &p->rects[16 * (size_t)t];   // core_global | tile_global | core_local | update_local
+    const int* region = guard_region ? R + 12 : R + 8;
+    const int oy = R[4], ox = R[6];
     ResistEpilogue ep{};
     ep.mode = 1;
     ep.thr = (float)threshold;
     ep.alpha = (float)alpha;
+    ep.aerial = eval_epe ? aerial : nullptr;
+    ep.wafer = core ? wafer : nullptr;
     ep.target = targets + t * tt;
     ep.pe_window = pe_w + t * tt;
     ep.pen_window = pen_w + t * tt;
     ep.pe_weight = (float)wpe;
     ep.penalty = (float)wpen;
     ep.pen_thr = (float)o.penalty_threshold;
-    ep.dldi = at<float>(ctx, L.dldi);
-    ep.loss_partial = ctx->d_red + RED_PART;
+    ep.dldi = dldi;
+    ep.loss_partial = part;
+    double* slot = p->d_loss + (size_t)S * t;
     int nb = 0;
     st = run_forward(ctx, *cache, f, L, 0, d_masks + t * tt, nullptr, ep, &nb);
-    if (!st)
-      st = check_launch(ctx, launch_sum_partials(s, ctx->d_red + RED_PART, nb, 2, p->d_loss + 2 * t),
-                        "sum");
+    if (!st) st = check_launch(ctx, launch_sum_partials(s, part, nb, 2, slot), "sum");
     ctx->launches += 1;
+    if (!st && zero_pe_dldi) LITHO_CUDA_TRY(ctx, cudaMemsetAsync(dldi, 0, tt * sizeof(float), s));
+    if (!st && eval_epe) {
+      // Loss-region EPs (periodic copies with a Core + Guard region): EPE sums and,
+      // for the EPE types, the scatter of their dL/dI.
+      const int grect[4] = {region[0] + oy, region[1] + oy, region[2] + ox, region[3] + ox};
+      int used = 0;
+      st = check_launch(ctx, launch_ep_candidates(s, ep_in, ep_in + 2 * (size_t)e.n_eps, e.n_eps,
+                                                  periods, p->height, p->width, oy, ox, grect, ts,
+                                                  epe_w + t * tt, cand, cand + 2 * ncand),
+                        "EP candidates");
+      if (!st)
+        st = check_launch(ctx, launch_epe(s, aerial, ts, ts, cand, cand + 2 * ncand, (int)ncand,
+                                          threshold, e.epe_pixel_size, nullptr, part,
+                                          epe_grad ? dldi : nullptr, epe_fac, &used),
+                          "sparse EPE");
+      if (!st) st = check_launch(ctx, launch_sum_partials(s, part, used, 3, slot + 2), "sum");
+      ctx->launches += 3;
+    }
+    if (!st && core) {
+      // Loss-region and Core sums from the wafer image; Core EPs without copies.
+      int used = 0;
+      st = check_launch(ctx, launch_rect_losses(s, wafer, targets + t * tt, pe_w + t * tt,
+                                                pen_w + t * tt, ts, region,
+                                                (float)o.penalty_threshold, part, &used),
+                        "region losses");
+      if (!st) st = check_launch(ctx, launch_sum_partials(s, part, used, 3, slot + 5), "sum");
+      if (!st)
+        st = check_launch(ctx, launch_rect_losses(s, wafer, targets + t * tt, pe_w + t * tt,
+                                                  pen_w + t * tt, ts, R + 8,
+                                                  (float)o.penalty_threshold, part, &used),
+                          "core losses");
+      if (!st) st = check_launch(ctx, launch_sum_partials(s, part, used, 3, slot + 8), "sum");
+      const int crect[4] = {R[0], R[1], R[2], R[3]};   // core_global
+      if (!st)
+        st = check_launch(ctx, launch_ep_candidates(s, ep_in, ep_in + 2 * (size_t)e.n_eps, e.n_eps,
+                                                    0, p->height, p->width, oy, ox, crect, ts,
+                                                    epe_w + t * tt, cand, cand + 2 * ncand),
+                          "core EP candidates");
+      if (!st)
+        st = check_launch(ctx, launch_epe(s, aerial, ts, ts, cand, cand + 2 * ncand, e.n_eps,
+                                          threshold, e.epe_pixel_size, nullptr, part, nullptr, 0.0,
+                                          &used),
+                          "core sparse EPE");
+      if (!st) st = check_launch(ctx, launch_sum_partials(s, part, used, 3, slot + 11), "sum");
+      ctx->launches += 8;
+    }
     GradEpilogue gp{};
     gp.grad_mask = raw + t * tt;
     int nb2 = 0;
-    if (!st) st = run_adjoint(ctx, *cache, f, L, at<float>(ctx, L.dldi), 4.0 * alpha, gp, &nb2);
+    if (!st) st = run_adjoint(ctx, *cache, f, L, dldi, adj_scale, gp, &nb2);
   }
   if (!st)
     LITHO_CUDA_TRY(ctx, cudaMemcpyAsync(d_grad, raw, n * tt * sizeof(float),
                                         cudaMemcpyDeviceToDevice, s));
   if (!st)
-    st = check_launch(ctx, launch_exchange(s, d_masks, raw, n, p->ts, p->d_meta + p->off_nrel,
+    st = check_launch(ctx, launch_exchange(s, d_masks, raw, n, ts, p->d_meta + p->off_nrel,
                                            p->d_meta + p->off_rel, litho_partition::kMaxRel, o,
-                                           d_grad, p->d_loss + 2 * n),
+                                           d_grad, p->d_loss + (size_t)S * n),
                       "micro-gradient exchange");
   ctx->launches += 1;
   if (!st)
-    LITHO_CUDA_TRY(ctx, cudaMemcpyAsync(p->h_loss.data(), p->d_loss, 3 * n * sizeof(double),
+    LITHO_CUDA_TRY(ctx, cudaMemcpyAsync(p->h_loss.data(), p->d_loss,
+                                        (size_t)(S + 1) * n * sizeof(double),
                                         cudaMemcpyDeviceToHost, s));
   if (!st) st = fetch(ctx, 0);
   if (st) return st;
   if (flag_set(ctx)) return ctx->fail(LITHO_ERR_NONFINITE, "Imaging: mask, threshold, and alpha must be finite");
   double tot[3] = {0.0, 0.0, 0.0};
+  const bool report_bg = o.loss_type == LITHO_MICRO_LOSS_PE_PENALTY || core;
   for (int t = 0; t < n; ++t) {
-    const double pe = p->h_loss[2 * t], bg = p->h_loss[2 * t + 1], cept = p->h_loss[2 * n + t];
-    const double data = wpe * pe + wpen * bg;
+    const double* h = &p->h_loss[(size_t)S * t];
+    // With the wafer image at hand the loss-region sums come from it; otherwise from
+    // the resist epilogue (whose background sum runs only under a penalty).
+    const double pe = core ? h[5] : h[0];
+    const double bg = core ? h[6] : h[1];
+    const double cept = p->h_loss[(size_t)S * n + t];
+    const double epe_loss = eval_epe ? h[2] : 0.0;
+    const double data = wpe * pe + wpen * bg + wepe * epe_loss;
     const double loss = data + (o.enable_cept ? o.cept_weight * cept : 0.0);
-    if (tile_losses) {
-      double* r = tile_losses + 5 * (size_t)t;
-      r[0] = pe; r[1] = wpen != 0.0 ? bg : 0.0; r[2] = data; r[3] = cept; r[4] = loss;
+    if (tile_metrics) {
+      double* r = tile_metrics + (size_t)LITHO_EXCHANGE_TILE_METRICS * t;
+      std::fill(r, r + LITHO_EXCHANGE_TILE_METRICS, 0.0);
+      r[LITHO_TM_PE_LOSS] = pe;
+      r[LITHO_TM_BG_PENALTY_RAW] = report_bg ? bg : 0.0;
+      r[LITHO_TM_PENALTY_LOSS] = wpen * bg;
+      r[LITHO_TM_EPE_LOSS] = epe_loss;
+      r[LITHO_TM_EPE_ABS_SUM_NM] = eval_epe ? h[3] : 0.0;
+      r[LITHO_TM_EPE_COUNT] = eval_epe ? h[4] : 0.0;
+      r[LITHO_TM_DATA_LOSS] = data;
+      r[LITHO_TM_CEPT_LOSS] = cept;
+      r[LITHO_TM_LOSS] = loss;
+      if (core) {
+        const double cnt = h[13];
+        r[LITHO_TM_CORE_PE_LOSS] = h[8];
+        r[LITHO_TM_CORE_BG_PENALTY_RAW] = h[9];
+        r[LITHO_TM_CORE_PE_PENALTY_LOSS] = o.pe_weight * h[10] + o.penalty_weight * h[9];
+        r[LITHO_TM_CORE_EPE_LOSS] = h[11];
+        r[LITHO_TM_CORE_EPE_ABS_SUM_NM] = h[12];
+        r[LITHO_TM_CORE_EP_COUNT] = cnt;
+        r[LITHO_TM_CORE_EPE_MEAN] = cnt == 0.0 ? 0.0 : h[12] / cnt;
+        r[LITHO_TM_CORE_DATA_LOSS] = wpe * h[8] + wpen * h[9] + wepe * h[11];
+      }
     }
     tot[0] += loss; tot[1] += data; tot[2] += cept;
   }
   if (totals) std::memcpy(totals, tot, sizeof(tot));
+  return LITHO_OK;
+}
+
+int litho_exchange_compute(litho_ctx* ctx, const litho_partition* cp, const litho_cache* cache,
+                           const float* d_masks, const float* d_global_target, double threshold,
+                           double alpha, const litho_exchange_options* opt, float* d_raw,
+                           float* d_grad, double* tile_losses, double* totals) {
+  if (!ctx || !cp) return LITHO_ERR_INVALID_ARGUMENT;
+  std::vector<double> m((size_t)LITHO_EXCHANGE_TILE_METRICS * cp->ntiles);
+  const int st = litho_exchange_compute_epe(ctx, cp, cache, d_masks, d_global_target, threshold,
+                                            alpha, opt, nullptr, d_raw, d_grad, m.data(), totals);
+  if (st || !tile_losses) return st;
+  for (int t = 0; t < cp->ntiles; ++t) {
+    const double* r = &m[(size_t)LITHO_EXCHANGE_TILE_METRICS * t];
+    double* o = tile_losses + 5 * (size_t)t;
+    o[0] = r[LITHO_TM_PE_LOSS]; o[1] = r[LITHO_TM_BG_PENALTY_RAW]; o[2] = r[LITHO_TM_DATA_LOSS];
+    o[3] = r[LITHO_TM_CEPT_LOSS]; o[4] = r[LITHO_TM_LOSS];
+  }
   return LITHO_OK;
 }
 
@@ -1673,7 +1862,8 @@ int litho_evaluate_sparse_epe(litho_ctx* ctx, int rows, int cols, const float* d
   }
   int used = 0;
   st = check_launch(ctx, launch_epe(s, d_aerial, rows, cols, d_eps, d_w, n, threshold,
-                                    pixel_size_nm, d_se, ctx->d_red + RED_PART, nullptr, &used),
+                                    pixel_size_nm, d_se, ctx->d_red + RED_PART, nullptr, 1.0,
+                                    &used),
                     "sparse EPE");
   if (!st)
     st = check_launch(ctx, launch_sum_partials(s, ctx->d_red + RED_PART, used, 3,
@@ -1723,7 +1913,7 @@ int litho_epe_gradient(litho_ctx* ctx, const litho_field* field, const float* d_
   }
   int used = 0;
   st = check_launch(ctx, launch_epe(s, d_aerial, N, N, d_eps, d_w, n, threshold, 1.0, nullptr,
-                                    ctx->d_red + RED_PART, dldi, &used),
+                                    ctx->d_red + RED_PART, dldi, 1.0, &used),
                     "sparse EPE scatter");
   ctx->launches += 1;
   if (st) return st;

@@ -58,12 +58,13 @@ __device__ __forceinline__ double sample(const Stencil& s, F f) {
 
 // eps: n x 2 (y, x); w: n weights. Per EP: signed EPE (pixels; NaN when inactive) and,
 // per CTA, FP64 partial sums (weighted squared loss, |EPE| nm, active count). With
-// dldi set, 2 w (I - thr) / G^2 is scattered onto its stencil (float atomics).
+// dldi set, scatter_scale x 2 w (I - thr) / G^2 is added onto its stencil (float atomics).
 constexpr int EPE_NT = 256;
 __global__ void __launch_bounds__(EPE_NT)
 epe_kernel(const float* __restrict__ I, int rows, int cols, const double* __restrict__ eps,
            const double* __restrict__ w, int n, double thr, double pixel_nm,
-           double* __restrict__ signed_epe, double* __restrict__ partial, float* __restrict__ dldi) {
+           double* __restrict__ signed_epe, double* __restrict__ partial, float* __restrict__ dldi,
+           double scatter_scale) {
   pdl_trigger();
   pdl_wait();
   __shared__ double sh[EPE_NT / 32];
@@ -81,7 +82,7 @@ epe_kernel(const float* __restrict__ I, int rows, int cols, const double* __rest
       absn = fabs(se) * pixel_nm;
       active = 1.0;
       if (dldi) {
-        const double g = 2.0 * wi * (a - thr) / (m * m);
+        const double g = scatter_scale * (2.0 * wi * (a - thr) / (m * m));
         const double wa = (1.0 - s.wy1) * (1.0 - s.wx1), wb = (1.0 - s.wy1) * s.wx1;
         const double wc = s.wy1 * (1.0 - s.wx1), wd = s.wy1 * s.wx1;
         if (wa > 0.0) atomicAdd(dldi + (size_t)s.y0 * cols + s.x0, (float)(wa * g));
@@ -104,11 +105,11 @@ epe_kernel(const float* __restrict__ I, int rows, int cols, const double* __rest
 
 cudaError_t launch_epe(cudaStream_t s, const float* I, int rows, int cols, const double* eps,
                        const double* w, int n, double thr, double pixel_nm, double* signed_epe,
-                       double* partial, float* dldi, int* nblocks) {
+                       double* partial, float* dldi, double scatter_scale, int* nblocks) {
   *nblocks = (n + EPE_NT - 1) / EPE_NT;
   if (*nblocks == 0) *nblocks = 1;
   return launch_pdl(epe_kernel, dim3(*nblocks), dim3(EPE_NT), 0, s, I, rows, cols, eps, w, n, thr,
-                    pixel_nm, signed_epe, partial, dldi);
+                    pixel_nm, signed_epe, partial, dldi, scatter_scale);
 }
 
 }  // namespace litho_b200

@@ -55,12 +55,14 @@ cudaError_t launch_tiles_assemble(cudaStream_t s, const float* loc, int ntiles, 
   return cudaGetLastError();
 }
 
-// build_micro_loss_windows (micro_gradient_exchange.cpp:65-93) for the PE types, every
-// tile at once: inside the tile's loss region pe = 1 (PE) or [T > 0.5] (PEPenalty) and
-// pen = [T < 0.5]; both are 0 outside it.
+// build_micro_loss_windows (micro_gradient_exchange.cpp:65-93), every tile at once.
+// Inside the tile's loss region: pen = [T < 0.5]; epe = 1, or for PE_EPE the dilated
+// main region; pe = [T > 0.5] for PEPenalty, 1 - epe for PE_EPE, else 1. All three are
+// 0 outside the region. main_dil (PE_EPE only) and epe_w are nullable.
 __global__ void loss_windows_kernel(const float* __restrict__ target, int ts,
-                                    const int* __restrict__ region, int pe_from_target,
-                                    float* __restrict__ pe_w, float* __restrict__ pen_w) {
+                                    const int* __restrict__ region, int loss_type,
+                                    const float* __restrict__ main_dil, float* __restrict__ pe_w,
+                                    float* __restrict__ pen_w, float* __restrict__ epe_w) {
   const int t = blockIdx.y;
   const int y0 = region[4 * t], y1 = region[4 * t + 1], x0 = region[4 * t + 2],
             x1 = region[4 * t + 3];
@@ -69,16 +71,137 @@ __global__ void loss_windows_kernel(const float* __restrict__ target, int ts,
     const size_t k = (size_t)t * ts * ts + i;
     const bool in = y >= y0 && y < y1 && x >= x0 && x < x1;
     const float T = target[k];
-    pe_w[k] = in ? (pe_from_target ? (T > 0.5f ? 1.f : 0.f) : 1.f) : 0.f;
+    const float e = loss_type == LITHO_MICRO_LOSS_PE_EPE ? main_dil[k] : 1.f;
+    float pe = loss_type == LITHO_MICRO_LOSS_PE_PENALTY ? (T > 0.5f ? 1.f : 0.f) : 1.f;
+    if (loss_type == LITHO_MICRO_LOSS_PE_EPE) pe = 1.f - e;
+    pe_w[k] = in ? pe : 0.f;
     pen_w[k] = in && T < 0.5f ? 1.f : 0.f;
+    if (epe_w) epe_w[k] = in ? e : 0.f;
   }
 }
 
 cudaError_t launch_loss_windows(cudaStream_t s, const float* target, int ntiles, int ts,
-                                const int* region, int pe_from_target, float* pe_w,
-                                float* pen_w) {
+                                const int* region, int loss_type, const float* main_dil,
+                                float* pe_w, float* pen_w, float* epe_w) {
   dim3 grid((ts * ts + 255) / 256 < 128 ? (ts * ts + 255) / 256 : 128, ntiles);
-  loss_windows_kernel<<<grid, 256, 0, s>>>(target, ts, region, pe_from_target, pe_w, pen_w);
+  loss_windows_kernel<<<grid, 256, 0, s>>>(target, ts, region, loss_type, main_dil, pe_w, pen_w,
+                                           epe_w);
+  return cudaGetLastError();
+}
+
+// The PE_EPE main region: [T > 0.5] dilated `iterations` times by a 3 x 3 square
+// with zeros outside the tile (cv::dilate with BORDER_CONSTANT 0,
+// micro_gradient_exchange.cpp:71-80), i.e. a Chebyshev-distance dilation by
+// `iterations`, done as a row pass then a column pass.
+__global__ void dilate_main_kernel(const float* __restrict__ src, int ts, int r, int rows_pass,
+                                   float* __restrict__ dst) {
+  const int t = blockIdx.y;
+  const float* a = src + (size_t)t * ts * ts;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ts * ts; i += gridDim.x * blockDim.x) {
+    const int y = i / ts, x = i % ts;
+    float m = 0.f;
+    if (rows_pass) {
+      for (int d = max(0, x - r); d <= min(ts - 1, x + r) && m == 0.f; ++d)
+        m = a[(size_t)y * ts + d] > 0.5f ? 1.f : 0.f;
+    } else {
+      for (int d = max(0, y - r); d <= min(ts - 1, y + r) && m == 0.f; ++d) m = a[(size_t)d * ts + x];
+    }
+    dst[(size_t)t * ts * ts + i] = m;
+  }
+}
+
+cudaError_t launch_dilate_main(cudaStream_t s, const float* target, int ntiles, int ts,
+                               int iterations, float* tmp, float* out) {
+  dim3 grid((ts * ts + 255) / 256 < 128 ? (ts * ts + 255) / 256 : 128, ntiles);
+  dilate_main_kernel<<<grid, 256, 0, s>>>(target, ts, iterations, 1, tmp);
+  dilate_main_kernel<<<grid, 256, 0, s>>>(tmp, ts, iterations, 0, out);
+  return cudaGetLastError();
+}
+
+// region_eps_local (micro_gradient_exchange.cpp:18-50) for one tile: candidate
+// c = (i * P + py') * P + px' (P = 2 periods + 1) is EP i shifted by (py, px) whole
+// layouts; it is kept, at local (y, x) with EP i's weight, when it lies in the
+// region (global half-open rect) and any pixel of its bilinear stencil on the tile
+// has a nonzero EPE window. Dropped candidates get weight 0 (inactive).
+__global__ void ep_candidates_kernel(const double* __restrict__ eps, const double* __restrict__ w,
+                                     int n, int periods, int H, int W, int oy, int ox, int gy0,
+                                     int gy1, int gx0, int gx1, int ts,
+                                     const float* __restrict__ win, double* __restrict__ out_eps,
+                                     double* __restrict__ out_w) {
+  const int P = 2 * periods + 1;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n * P * P) return;
+  const int i = c / (P * P), py = (c / P) % P - periods, px = c % P - periods;
+  const double y = eps[2 * i] + (double)py * H, x = eps[2 * i + 1] + (double)px * W;
+  double ly = 0.0, lx = 0.0, wc = 0.0;
+  if (y >= gy0 && y < gy1 && x >= gx0 && x < gx1) {
+    ly = y - oy;
+    lx = x - ox;
+    const double yy = fmin(fmax(ly, 0.0), ts - 1.0), xx = fmin(fmax(lx, 0.0), ts - 1.0);
+    const int y0 = (int)floor(yy), x0 = (int)floor(xx);
+    const int y1 = min(y0 + 1, ts - 1), x1 = min(x0 + 1, ts - 1);
+    const double wy1 = y1 == y0 ? 0.0 : yy - y0, wx1 = x1 == x0 ? 0.0 : xx - x0;
+    const bool touch = ((1.0 - wy1) * (1.0 - wx1) > 0.0 && win[(size_t)y0 * ts + x0] != 0.f) ||
+                       ((1.0 - wy1) * wx1 > 0.0 && win[(size_t)y0 * ts + x1] != 0.f) ||
+                       (wy1 * (1.0 - wx1) > 0.0 && win[(size_t)y1 * ts + x0] != 0.f) ||
+                       (wy1 * wx1 > 0.0 && win[(size_t)y1 * ts + x1] != 0.f);
+    if (touch) wc = w[i];
+  }
+  out_eps[2 * (size_t)c] = ly;
+  out_eps[2 * (size_t)c + 1] = lx;
+  out_w[c] = wc;
+}
+
+cudaError_t launch_ep_candidates(cudaStream_t s, const double* eps, const double* w, int n,
+                                 int periods, int H, int W, int oy, int ox, const int* grect,
+                                 int ts, const float* win, double* out_eps, double* out_w) {
+  const int P = 2 * periods + 1;
+  const long long nc = (long long)n * P * P;
+  if (nc == 0) return cudaSuccess;
+  ep_candidates_kernel<<<(unsigned)((nc + 255) / 256), 256, 0, s>>>(
+      eps, w, n, periods, H, W, oy, ox, grect[0], grect[1], grect[2], grect[3], ts, win, out_eps,
+      out_w);
+  return cudaGetLastError();
+}
+
+// Loss sums over one rectangle of a tile (the Core metrics of
+// micro_gradient_exchange.cpp:224-233), per CTA in FP64: sum pe_w (W - T)^2,
+// sum_{T < 0.5} pen_w max(W - pen_thr, 0)^2 and sum_{T > 0.5} (W - T)^2.
+constexpr int RL_NT = 256;
+__global__ void __launch_bounds__(RL_NT)
+rect_losses_kernel(const float* __restrict__ Wf, const float* __restrict__ T,
+                   const float* __restrict__ pe_w, const float* __restrict__ pen_w, int ts, int y0,
+                   int y1, int x0, int x1, float pen_thr, double* __restrict__ partial) {
+  __shared__ double sh[RL_NT / 32];
+  const int cols = x1 - x0, n = (y1 - y0) * cols;
+  double pe = 0.0, bg = 0.0, mainpe = 0.0;
+  for (int i = blockIdx.x * RL_NT + threadIdx.x; i < n; i += gridDim.x * RL_NT) {
+    const size_t k = (size_t)(y0 + i / cols) * ts + x0 + i % cols;
+    const double w = Wf[k], t = T[k], r = w - t;
+    pe += r * r * (double)pe_w[k];
+    if (t < 0.5) {
+      const double ex = fmax(0.0, w - (double)pen_thr);
+      bg += (double)pen_w[k] * ex * ex;
+    }
+    if (t > 0.5) mainpe += r * r;
+  }
+  const double a = block_sum<RL_NT>(pe, sh);
+  const double b = block_sum<RL_NT>(bg, sh);
+  const double c = block_sum<RL_NT>(mainpe, sh);
+  if (threadIdx.x == 0) {
+    partial[3 * blockIdx.x] = a;
+    partial[3 * blockIdx.x + 1] = b;
+    partial[3 * blockIdx.x + 2] = c;
+  }
+}
+
+cudaError_t launch_rect_losses(cudaStream_t s, const float* Wf, const float* T, const float* pe_w,
+                               const float* pen_w, int ts, const int* rect, float pen_thr,
+                               double* partial, int* nblocks) {
+  const int n = (rect[1] - rect[0]) * (rect[3] - rect[2]);
+  *nblocks = n <= 0 ? 1 : ((n + RL_NT - 1) / RL_NT < 64 ? (n + RL_NT - 1) / RL_NT : 64);
+  rect_losses_kernel<<<*nblocks, RL_NT, 0, s>>>(Wf, T, pe_w, pen_w, ts, rect[0], rect[1], rect[2],
+                                                rect[3], pen_thr, partial);
   return cudaGetLastError();
 }
 

@@ -290,7 +290,7 @@ cudaError_t launch_reinit_sdf(cudaStream_t s, int rows, int cols, const float* p
 // 2 w (I - thr) / G^2 onto each point's bilinear stencil (atomic adds).
 cudaError_t launch_epe(cudaStream_t s, const float* I, int rows, int cols, const double* eps,
                        const double* w, int n, double thr, double pixel_nm, double* signed_epe,
-                       double* partial, float* dldi, int* nblocks);
+                       double* partial, float* dldi, double scatter_scale, int* nblocks);
 
 // Full-chip micro tiles (fullchip.cu). Rects are 4 ints (y0, y1, x0, x1) per tile;
 // origins 2 ints (y, x) per tile; rel holds max_rel entries of FC_REL_INTS ints
@@ -302,8 +302,17 @@ cudaError_t launch_tiles_extract(cudaStream_t s, const float* g, int H, int W, i
 cudaError_t launch_tiles_assemble(cudaStream_t s, const float* loc, int ntiles, int ts,
                                   const int* core_g, const int* core_l, int W, float* g);
 cudaError_t launch_loss_windows(cudaStream_t s, const float* target, int ntiles, int ts,
-                                const int* region, int pe_from_target, float* pe_w,
-                                float* pen_w);
+                                const int* region, int loss_type, const float* main_dil,
+                                float* pe_w, float* pen_w, float* epe_w);
+cudaError_t launch_dilate_main(cudaStream_t s, const float* target, int ntiles, int ts,
+                               int iterations, float* tmp, float* out);
+// grect: the region as a global half-open rect (y0, y1, x0, x1); oy, ox the tile origin.
+cudaError_t launch_ep_candidates(cudaStream_t s, const double* eps, const double* w, int n,
+                                 int periods, int H, int W, int oy, int ox, const int* grect,
+                                 int ts, const float* win, double* out_eps, double* out_w);
+cudaError_t launch_rect_losses(cudaStream_t s, const float* Wf, const float* T, const float* pe_w,
+                               const float* pen_w, int ts, const int* rect, float pen_thr,
+                               double* partial, int* nblocks);
 cudaError_t launch_exchange(cudaStream_t s, const float* masks, const float* raw, int ntiles,
                             int ts, const int* nrel, const int* rel, int max_rel,
                             const litho_exchange_options& o, float* grad, double* cept_loss);

@@ -12,6 +12,10 @@
   (source/utils/imbinarize.cpp:84-189), the CTM -> LSM hand-off of the demos: peak
   quantile threshold, small-component removal, SRAFs kept outside a keep-out disk
   around the target, final small-component pass.
+* :func:`write_lsm_history_csv`, :func:`write_core_metrics_csv`,
+  :func:`write_summary_csv` - the ``history.csv``, ``core_metrics_best.csv`` and
+  ``summary.csv`` of a full-chip LSM run (demo/demo_full_chip_lsm.cpp:170-201): the
+  same columns, values printed with 17 significant digits.
 
 These run once per optimisation on the host; they accept NumPy arrays or tensors.
 """
@@ -156,3 +160,61 @@ def binarize_advanced(gray_mask, target_pattern, peak_min_intensity: float = 0.1
     f = lambda m: m.astype(np.float64)
     return BinarizeResult(f(initial), f(filtered), f(sraf_initial), f(sraf_final), f(final),
                           f(keep_out))
+
+
+def _g17(v) -> str:
+    """An ostream value under std::setprecision(17): integers as integers, else %.17g."""
+    if isinstance(v, (int, np.integer)) and not isinstance(v, bool):
+        return str(int(v))
+    return "%.17g" % float(v)
+
+
+LSM_HISTORY_COLUMNS = (
+    "iteration,loss,data_loss,cept_loss,min_dt,max_dt,pe_contribution,penalty_contribution,"
+    "epe_contribution,cept_contribution,core_pe,core_bg_penalty_raw,core_pe_penalty,"
+    "core_epe_squared_pixel,core_epe_abs_sum_nm,core_ep_count,core_epe_mean_nm,core_data_loss,"
+    "total_pe,total_bg_penalty_raw,total_epe_squared_pixel,total_epe_abs_sum_nm,total_ep_count,"
+    "epe_mean_nm")
+
+
+def write_lsm_history_csv(history, path: str) -> None:
+    """history.csv (demo_full_chip_lsm.cpp:170-186): one row per FullChipLSMIteration."""
+    with open(path, "w") as f:
+        f.write(LSM_HISTORY_COLUMNS + "\n")
+        for r in history:
+            c = r.core
+            row = (r.iteration, r.loss, r.data_loss, r.cept_loss, r.min_dt, r.max_dt,
+                   r.pe_contribution, r.penalty_contribution, r.epe_contribution,
+                   r.cept_contribution, c.pe_loss, c.bg_penalty_raw, c.pe_penalty_loss, c.epe_loss,
+                   c.epe_abs_sum_nm, int(c.ep_count), c.epe_mean, c.data_loss, r.total_pe_loss,
+                   r.total_bg_penalty_raw, r.total_epe_loss, r.total_epe_abs_sum_nm,
+                   int(r.total_ep_count), r.epe_mean)
+            f.write(",".join(_g17(v) for v in row) + "\n")
+
+
+CORE_METRICS_COLUMNS = (
+    "best_iteration,micro_id,y0,y1,x0,x1,core_pe,core_bg_penalty_raw,core_pe_penalty,"
+    "core_epe_squared_pixel,core_epe_abs_sum_nm,core_ep_count,core_epe_mean_nm,core_data_loss")
+
+
+def write_core_metrics_csv(result, partition, path: str) -> None:
+    """core_metrics_best.csv (demo_full_chip_lsm.cpp:187-196): the best round's Core
+    metrics per Micro, with its global Core rectangle."""
+    with open(path, "w") as f:
+        f.write(CORE_METRICS_COLUMNS + "\n")
+        for tile, m in zip(partition.tiles, result.best_core_metrics):
+            c = tile.core_global
+            row = (int(result.best_iteration), int(tile.id), c.y0, c.y1, c.x0, c.x1, m.pe_loss,
+                   m.bg_penalty_raw, m.pe_penalty_loss, m.epe_loss, m.epe_abs_sum_nm,
+                   int(m.ep_count), m.epe_mean, m.data_loss)
+            f.write(",".join(_g17(v) for v in row) + "\n")
+
+
+def write_summary_csv(result, seconds: float, path: str) -> None:
+    """summary.csv (demo_full_chip_lsm.cpp:197-201)."""
+    last = result.history[-1]
+    with open(path, "w") as f:
+        f.write("best_iteration,best_loss,final_iteration,final_loss,seconds\n")
+        row = (int(result.best_iteration), result.best_loss, int(last.iteration), last.loss,
+               float(seconds))
+        f.write(",".join(_g17(v) for v in row) + "\n")

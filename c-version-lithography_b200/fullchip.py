@@ -6,9 +6,10 @@ Mirrors the reference's full-chip classes:
   source/utils/partition.cpp:21-120): Cores, Halo tiles with periodic wrap,
   Core + Guard update windows, four-neighbour relations.
 * :class:`MicroGradientExchange` - ``MicroGradientExchange::compute``
-  (source/utils/micro_gradient_exchange.cpp:134-334) for the PE and PEPenalty
-  loss types: per-tile imaging and windowed data loss, raw mask gradients,
-  CEPT against the neighbours' Cores and Average / Linear guard fusion.
+  (source/utils/micro_gradient_exchange.cpp:134-334) for all four loss types (PE,
+  PEPenalty, EPE, PE_EPE) with optional Core metrics: per-tile imaging, windowed
+  data loss, sparse EPE at caller-selected edge points, raw mask gradients, CEPT
+  against the neighbours' Cores and Average / Linear guard fusion.
 * :class:`FullChipCTMOptimizer` - ``FullChipCTMOptimizer::optimize``
   (source/optimizer/full_chip_ctm.cpp:25-152): fixed-step theta descent inside
   each tile's Core + Guard window, best state over all evaluations.
@@ -29,21 +30,29 @@ from typing import List, Optional
 
 import numpy as np
 
-from . import (ExchangeOptionsC, ImagingCache, LithoError, _f32, _ptr, default_context)
+from . import (EXCHANGE_TILE_METRICS, ExchangeEpeC, ExchangeOptionsC, ImagingCache, LithoError,
+               _f32, _ptr, default_context)
 
-LOSS_TYPES = {"PE": 0, "PEPenalty": 1}
+LOSS_TYPES = {"PE": 0, "PEPenalty": 1, "EPE": 2, "PE_EPE": 3}
 LOSS_REGIONS = {"Core": 0, "CoreGuard": 1}
 FUSION_MODES = {"Average": 0, "Linear": 1}
 
 
 @dataclass
 class MicroGradientOptions:
-    """MicroGradientOptions (include/utils/micro_gradient_exchange.h:19-40), PE types."""
+    """MicroGradientOptions (include/utils/micro_gradient_exchange.h:19-40). EP
+    selection stays with the caller: the EPE types evaluate the edge points given to
+    :meth:`MicroGradientExchange.compute`; ``epe_all_eps`` sets all their weights to 1."""
     loss_type: str = "PE"
     loss_region: str = "Core"
+    main_region_dilation_pixels: int = 2
     pe_weight: float = 1.0
+    epe_weight: float = 1.0
     penalty_weight: float = 2.0
     penalty_threshold: float = 0.01
+    epe_all_eps: bool = False
+    epe_pixel_size: float = 1.0
+    collect_core_metrics: bool = False
     enable_cept: bool = False
     cept_guard_only: bool = False
     cept_weight: float = 1.1
@@ -65,8 +74,10 @@ class MicroGradientOptions:
             FUSION_MODES[self.fusion_mode], self.fusion_weight_owner, self.fusion_weight_neighbor)
 
     def weights(self):
-        """micro_loss_weights (micro_gradient_exchange.cpp:95-99): (pe, penalty)."""
-        return self.pe_weight, (self.penalty_weight if self.loss_type == "PEPenalty" else 0.0)
+        """micro_loss_weights (micro_gradient_exchange.cpp:95-99): (pe, epe, penalty)."""
+        return ((0.0 if self.loss_type == "EPE" else self.pe_weight),
+                (self.epe_weight if self.loss_type in ("EPE", "PE_EPE") else 0.0),
+                (self.penalty_weight if self.loss_type == "PEPenalty" else 0.0))
 
 
 @dataclass(frozen=True)
@@ -155,13 +166,31 @@ class Partition:
 
 
 @dataclass
+class CoreLossMetrics:
+    """CoreLossMetrics (include/utils/micro_gradient_exchange.h:66-75)."""
+    pe_loss: float = 0.0
+    bg_penalty_raw: float = 0.0
+    pe_penalty_loss: float = 0.0
+    epe_loss: float = 0.0
+    epe_abs_sum_nm: float = 0.0
+    ep_count: int = 0
+    epe_mean: float = 0.0
+    data_loss: float = 0.0
+
+
+@dataclass
 class MicroLocalLoss:
+    """The scalars of MicroGradientData (micro_gradient_exchange.h:86-97)."""
     pe_loss: float
     bg_penalty_raw: float
     penalty_loss: float
     data_loss: float
     cept_loss: float
     loss: float
+    epe_loss: float = 0.0
+    epe_abs_sum_nm: float = 0.0
+    epe_count: int = 0
+    core: CoreLossMetrics = field(default_factory=CoreLossMetrics)
 
 
 @dataclass
@@ -173,6 +202,20 @@ class MicroGradientExchangeResult:
     locals: List[MicroLocalLoss]
     mask_gradients: object     # (num_tiles, ts, ts) exchanged gradients
     raw_gradients: object      # (num_tiles, ts, ts) before CEPT and fusion
+
+
+def _edge_points(eps, eps_weights, all_ones: bool):
+    """Global EP coordinates (n x 2, y then x) and weight_epe as contiguous float64."""
+    if eps is None:
+        return np.zeros((0, 2)), np.zeros(0)
+    pts = np.ascontiguousarray(np.asarray(eps, dtype=np.float64).reshape(-1, 2))
+    if all_ones or eps_weights is None:
+        w = np.ones(len(pts))
+    else:
+        w = np.ascontiguousarray(np.asarray(eps_weights, dtype=np.float64).reshape(-1))
+        if len(w) != len(pts):
+            raise LithoError(2, "eps and eps_weights must have the same length")
+    return pts, w
 
 
 class MicroGradientExchange:
@@ -189,26 +232,38 @@ class MicroGradientExchange:
         self.grad = partition.empty_tiles()
         self.raw = partition.empty_tiles()
 
-    def compute(self, local_masks, global_target, options: Optional[MicroGradientOptions] = None):
+    def compute(self, local_masks, global_target, options: Optional[MicroGradientOptions] = None,
+                eps=None, eps_weights=None):
         """compute(local_masks, global_target, options) (micro_gradient_exchange.cpp:134-334).
 
+        eps: the selected edge points as global subpixel (y, x) rows (select_micro_epe_points'
+        output), eps_weights their weight_epe; used by the EPE types and the Core metrics.
         The returned gradient tensors are reused by the next call."""
         p = self.partition
         torch = self.ctx.torch
         opt = options or MicroGradientOptions()
         copt = opt.to_c()
+        pts, w = _edge_points(eps, eps_weights, opt.epe_all_eps)
+        cepe = ExchangeEpeC(opt.epe_weight, opt.main_region_dilation_pixels, opt.epe_pixel_size,
+                            int(opt.collect_core_metrics),
+                            pts.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                            w.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), len(pts))
         ts = p.tile_size
         masks = _f32(local_masks, torch, (p.num_tiles, ts, ts), "local masks")
         tgt = _f32(global_target, torch, (p.height, p.width), "global target")
-        per = (ctypes.c_double * (5 * p.num_tiles))()
+        M = EXCHANGE_TILE_METRICS
+        per = (ctypes.c_double * (M * p.num_tiles))()
         tot = (ctypes.c_double * 3)()
-        self.ctx._check(self.ctx.lib.litho_exchange_compute(
+        self.ctx._check(self.ctx.lib.litho_exchange_compute_epe(
             self.ctx.handle, p.handle, self.cache.handle, _ptr(masks), _ptr(tgt),
-            self.threshold, self.alpha, ctypes.byref(copt), _ptr(self.raw), _ptr(self.grad),
-            per, tot))
-        _, wpen = opt.weights()
-        locs = [MicroLocalLoss(per[5 * t], per[5 * t + 1], wpen * per[5 * t + 1], per[5 * t + 2],
-                               per[5 * t + 3], per[5 * t + 4]) for t in range(p.num_tiles)]
+            self.threshold, self.alpha, ctypes.byref(copt), ctypes.byref(cepe), _ptr(self.raw),
+            _ptr(self.grad), per, tot))
+        locs = []
+        for t in range(p.num_tiles):
+            r = per[M * t:M * (t + 1)]
+            locs.append(MicroLocalLoss(r[0], r[1], r[2], r[6], r[7], r[8], r[3], r[4], int(r[5]),
+                                       CoreLossMetrics(r[9], r[10], r[11], r[12], r[13],
+                                                       int(r[14]), r[15], r[16])))
         return MicroGradientExchangeResult(tot[0], tot[1], tot[2], locs, self.grad, self.raw)
 
 
@@ -225,15 +280,20 @@ class FullChipCTMOptions:
 
 @dataclass
 class FullChipCTMIteration:
+    """FullChipCTMIteration (include/optimizer/full_chip_ctm.h:19-28)."""
     iteration: int
     loss: float
     data_loss: float
     cept_loss: float
     pe_contribution: float
     penalty_contribution: float
+    epe_contribution: float
     cept_contribution: float
     pe_loss_raw: float
     bg_penalty_raw: float
+    epe_loss_raw: float
+    epe_abs_sum_nm: float
+    epe_point_count: int
 
 
 @dataclass
@@ -264,15 +324,18 @@ class FullChipCTMOptimizer:
                            torch.full_like(pattern, 0.7 * pi))
 
     def optimize(self, global_target, options: Optional[FullChipCTMOptions] = None,
-                 initial_pattern=None) -> FullChipCTMResult:
-        """optimize([initial_pattern,] global_target, options) (full_chip_ctm.cpp:25-152)."""
+                 initial_pattern=None, eps=None, eps_weights=None) -> FullChipCTMResult:
+        """optimize([initial_pattern,] global_target, options) (full_chip_ctm.cpp:25-152).
+
+        eps / eps_weights: the edge points of the EPE loss types (see
+        MicroGradientExchange.compute)."""
         opt = options or FullChipCTMOptions()
         if opt.iterations < 0:
             raise LithoError(1, "FullChipCTM iterations must be non-negative")
         if not math.isfinite(opt.learning_rate):
             raise LithoError(3, "FullChipCTM learning_rate must be finite")
         go = MicroGradientOptions(**{**opt.gradient_options.__dict__, "cept_guard_only": True})
-        wpe, wpen = go.weights()
+        wpe, wepe, _ = go.weights()
         p = self.partition
         torch = self.ctx.torch
         tgt = _f32(global_target, torch, (p.height, p.width), "global target")
@@ -287,25 +350,27 @@ class FullChipCTMOptimizer:
         best = dict(loss=math.inf, iteration=0, masks=None, theta=None)
 
         def record(it, ev):
-            pe = sum(wpe * l.pe_loss for l in ev.locals)
-            pen = sum(l.penalty_loss for l in ev.locals)
+            L = ev.locals
             cept = go.cept_weight * ev.cept_loss if go.enable_cept else 0.0
             history.append(FullChipCTMIteration(
-                it, ev.loss, ev.data_loss, ev.cept_loss, pe, pen, cept,
-                sum(l.pe_loss for l in ev.locals), sum(l.bg_penalty_raw for l in ev.locals)))
+                it, ev.loss, ev.data_loss, ev.cept_loss, sum(wpe * l.pe_loss for l in L),
+                sum(l.penalty_loss for l in L), sum(wepe * l.epe_loss for l in L), cept,
+                sum(l.pe_loss for l in L), sum(l.bg_penalty_raw for l in L),
+                sum(l.epe_loss for l in L), sum(l.epe_abs_sum_nm for l in L),
+                sum(l.epe_count for l in L)))
             if ev.loss < best["loss"]:
                 best.update(loss=ev.loss, iteration=it, masks=masks.clone(), theta=theta.clone())
             if opt.verbose:
                 print(f"CTM {it:>3}/{opt.iterations} data={ev.data_loss:.3f} "
                       f"cept={ev.cept_loss:.3f} total={ev.loss:.3f}")
 
-        ev = self.exchange.compute(masks, tgt, go)
+        ev = self.exchange.compute(masks, tgt, go, eps, eps_weights)
         record(0, ev)
         for it in range(1, opt.iterations + 1):
             self.ctx._check(lib.litho_fullchip_theta_step(h, p.handle, _ptr(theta),
                                                           _ptr(ev.mask_gradients),
                                                           opt.learning_rate, _ptr(masks)))
-            ev = self.exchange.compute(masks, tgt, go)
+            ev = self.exchange.compute(masks, tgt, go, eps, eps_weights)
             record(it, ev)
         return FullChipCTMResult(best["iteration"], best["loss"],
                                  p.assemble_global(best["masks"]), best["masks"], best["theta"],
@@ -314,7 +379,7 @@ class FullChipCTMOptimizer:
 
 @dataclass
 class FullChipLSMOptions:
-    """FullChipLSMOptions (include/optimizer/full_chip_lsm.h:8-20), PE loss types."""
+    """FullChipLSMOptions (include/optimizer/full_chip_lsm.h:8-21)."""
     iterations: int = 200
     dx: float = 1.0
     dy: float = 1.0
@@ -323,12 +388,14 @@ class FullChipLSMOptions:
     reinit_interval: int = 20
     mask_type: str = "Binary"
     render_scale: int = 4
-    gradient_options: MicroGradientOptions = field(default_factory=MicroGradientOptions)
+    gradient_options: MicroGradientOptions = field(
+        default_factory=lambda: MicroGradientOptions(epe_all_eps=True))
     verbose: bool = False
 
 
 @dataclass
 class FullChipLSMIteration:
+    """FullChipLSMIteration (include/optimizer/full_chip_lsm.h:23-36)."""
     iteration: int
     loss: float
     data_loss: float
@@ -337,7 +404,15 @@ class FullChipLSMIteration:
     max_dt: float
     pe_contribution: float
     penalty_contribution: float
+    epe_contribution: float
     cept_contribution: float
+    core: CoreLossMetrics
+    total_pe_loss: float
+    total_bg_penalty_raw: float
+    total_epe_loss: float
+    total_epe_abs_sum_nm: float
+    total_ep_count: int
+    epe_mean: float
 
 
 @dataclass
@@ -351,6 +426,7 @@ class FullChipLSMResult:
     local_masks: object
     local_phi: object
     history: List[FullChipLSMIteration]
+    best_core_metrics: List[CoreLossMetrics] = field(default_factory=list)
 
 
 class FullChipLSMOptimizer:
@@ -365,18 +441,22 @@ class FullChipLSMOptimizer:
         self.ctx = partition.ctx
 
     def optimize(self, initial_binary, global_target,
-                 options: Optional[FullChipLSMOptions] = None) -> FullChipLSMResult:
-        """optimize(initial_binary, global_target, options) (full_chip_lsm.cpp:38-254)."""
+                 options: Optional[FullChipLSMOptions] = None, eps=None,
+                 eps_weights=None) -> FullChipLSMResult:
+        """optimize(initial_binary, global_target, options) (full_chip_lsm.cpp:38-254).
+
+        eps / eps_weights: the edge points of the EPE loss types and of the Core EPE
+        statistics (see MicroGradientExchange.compute)."""
         from . import MASK_TYPES
         opt = options or FullChipLSMOptions()
         if opt.mask_type not in MASK_TYPES:
             raise LithoError(1, f"mask_type must be one of {sorted(MASK_TYPES)}")
         if opt.iterations < 0:
             raise LithoError(1, "FullChipLSM iterations must be non-negative")
-        # Core + Guard evaluation and guard-only CEPT (full_chip_lsm.cpp:43-46).
+        # Core + Guard evaluation, guard-only CEPT, Core metrics (full_chip_lsm.cpp:43-46).
         go = MicroGradientOptions(**{**opt.gradient_options.__dict__, "loss_region": "CoreGuard",
-                                     "cept_guard_only": True})
-        wpe, wpen = go.weights()
+                                     "cept_guard_only": True, "collect_core_metrics": True})
+        wpe, wepe, _ = go.weights()
         p = self.partition
         torch = self.ctx.torch
         lib, h = self.ctx.lib, self.ctx.handle
@@ -389,21 +469,32 @@ class FullChipLSMOptimizer:
         initial_global_phi = p.assemble_global(phi)
         initial_global_mask = p.assemble_global(masks)
         history: List[FullChipLSMIteration] = []
-        best = dict(loss=math.inf, iteration=0, phi=None, masks=None)
+        best = dict(loss=math.inf, iteration=0, phi=None, masks=None, core=[])
 
         def record(it, ev, dmin, dmax):
+            # full_chip_lsm.cpp:152-186: weighted contributions, raw totals over the
+            # Core + Guard regions, Core sums with the mean over all Core EPs.
+            L = ev.locals
+            core = CoreLossMetrics(*(sum(getattr(l.core, k) for l in L) for k in (
+                "pe_loss", "bg_penalty_raw", "pe_penalty_loss", "epe_loss", "epe_abs_sum_nm",
+                "ep_count")), 0.0, sum(l.core.data_loss for l in L))
+            core.epe_mean = core.epe_abs_sum_nm / core.ep_count if core.ep_count else 0.0
             cept = go.cept_weight * ev.cept_loss if go.enable_cept else 0.0
+            total_abs, total_n = sum(l.epe_abs_sum_nm for l in L), sum(l.epe_count for l in L)
             history.append(FullChipLSMIteration(
                 it, ev.loss, ev.data_loss, ev.cept_loss, dmin, dmax,
-                sum(wpe * l.pe_loss for l in ev.locals), sum(l.penalty_loss for l in ev.locals),
-                cept))
+                sum(wpe * l.pe_loss for l in L), sum(l.penalty_loss for l in L),
+                sum(wepe * l.epe_loss for l in L), cept, core, sum(l.pe_loss for l in L),
+                sum(l.bg_penalty_raw for l in L), sum(l.epe_loss for l in L), total_abs, total_n,
+                total_abs / total_n if total_n else 0.0))
             if ev.loss < best["loss"]:
-                best.update(loss=ev.loss, iteration=it, phi=phi.clone(), masks=masks.clone())
+                best.update(loss=ev.loss, iteration=it, phi=phi.clone(), masks=masks.clone(),
+                            core=[l.core for l in L])
             if opt.verbose:
                 print(f"LSM {it:>3}/{opt.iterations} data={ev.data_loss:.3f} "
                       f"cept={ev.cept_loss:.3f} total={ev.loss:.3f}")
 
-        ev = self.exchange.compute(masks, tgt, go)
+        ev = self.exchange.compute(masks, tgt, go, eps, eps_weights)
         record(0, ev, 0.0, 0.0)
         nxt = p.empty_tiles()
         dmin, dmax = ctypes.c_double(), ctypes.c_double()
@@ -414,8 +505,9 @@ class FullChipLSMOptimizer:
                 opt.curvature_weight, reinit, mt, opt.render_scale, _ptr(nxt), _ptr(masks),
                 ctypes.byref(dmin), ctypes.byref(dmax)))
             phi, nxt = nxt, phi
-            ev = self.exchange.compute(masks, tgt, go)
+            ev = self.exchange.compute(masks, tgt, go, eps, eps_weights)
             record(it, ev, dmin.value, dmax.value)
         return FullChipLSMResult(best["iteration"], best["loss"], p.assemble_global(best["masks"]),
                                  p.assemble_global(best["phi"]), initial_global_phi,
-                                 initial_global_mask, best["masks"], best["phi"], history)
+                                 initial_global_mask, best["masks"], best["phi"], history,
+                                 best["core"])

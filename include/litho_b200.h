@@ -253,10 +253,13 @@ int litho_partition_extract(litho_ctx* ctx, const litho_partition* partition,
 int litho_partition_assemble(litho_ctx* ctx, const litho_partition* partition,
                              const float* d_tiles, float* d_global);
 
-/* MicroGradientOptions (include/utils/micro_gradient_exchange.h:19-40) for the
- * PE loss types; the reference's defaults are given beside each field. */
+/* MicroGradientOptions (include/utils/micro_gradient_exchange.h:19-40); the
+ * reference's defaults are given beside each field. The EPE terms are in
+ * litho_exchange_epe below. */
 #define LITHO_MICRO_LOSS_PE 0
 #define LITHO_MICRO_LOSS_PE_PENALTY 1
+#define LITHO_MICRO_LOSS_EPE 2
+#define LITHO_MICRO_LOSS_PE_EPE 3
 #define LITHO_MICRO_REGION_CORE 0
 #define LITHO_MICRO_REGION_CORE_GUARD 1
 #define LITHO_FUSION_AVERAGE 0
@@ -291,6 +294,58 @@ int litho_exchange_compute(litho_ctx* ctx, const litho_partition* partition,
                            const float* d_global_target, double threshold, double alpha,
                            const litho_exchange_options* opt, float* d_raw, float* d_grad,
                            double* tile_losses, double* totals);
+
+/* The EPE side of MicroGradientOptions (micro_gradient_exchange.h:22-32) and the edge
+ * points (EPs) it evaluates. EP selection (select_micro_epe_points, ep_select.cpp)
+ * stays with the caller: eps (host, n_eps x 2) holds each selected EP's global
+ * subpixel (y, x) on the layout and weights (host, n_eps) its weight_epe. */
+typedef struct litho_exchange_epe {
+  double epe_weight;                /* 1.0: EPE and PE_EPE */
+  int main_region_dilation_pixels;  /* 2: PE_EPE, 3 x 3 dilations of target > 0.5 */
+  double epe_pixel_size;            /* 1.0 nm per pixel: absolute EPE statistics only */
+  int collect_core_metrics;         /* 0 */
+  const double* eps;
+  const double* weights;
+  int n_eps;
+} litho_exchange_epe;
+
+/* Per-tile results of litho_exchange_compute_epe (MicroGradientData and its
+ * CoreLossMetrics, micro_gradient_exchange.h:66-99), LITHO_EXCHANGE_TILE_METRICS
+ * doubles per tile in this order. */
+#define LITHO_EXCHANGE_TILE_METRICS 17
+enum {
+  LITHO_TM_PE_LOSS = 0,        /* unweighted PE over the PE window of the loss region */
+  LITHO_TM_BG_PENALTY_RAW,     /* PEPenalty or core metrics, else 0 */
+  LITHO_TM_PENALTY_LOSS,       /* penalty weight x raw background penalty (PEPenalty) */
+  LITHO_TM_EPE_LOSS,           /* sum weight_epe x EPE^2 (pixel^2) over the region's EPs */
+  LITHO_TM_EPE_ABS_SUM_NM,
+  LITHO_TM_EPE_COUNT,
+  LITHO_TM_DATA_LOSS,
+  LITHO_TM_CEPT_LOSS,
+  LITHO_TM_LOSS,
+  LITHO_TM_CORE_PE_LOSS,       /* core metrics (collect_core_metrics), else 0 */
+  LITHO_TM_CORE_BG_PENALTY_RAW,
+  LITHO_TM_CORE_PE_PENALTY_LOSS,
+  LITHO_TM_CORE_EPE_LOSS,
+  LITHO_TM_CORE_EPE_ABS_SUM_NM,
+  LITHO_TM_CORE_EP_COUNT,
+  LITHO_TM_CORE_EPE_MEAN,
+  LITHO_TM_CORE_DATA_LOSS
+};
+
+/* MicroGradientExchange::compute with every loss type (PE, PEPenalty, EPE,
+ * PE_EPE) and the optional Core metrics. EPs of the loss region come with their
+ * periodic copies when the region is Core + Guard; Core metrics use the EPs of
+ * the Core alone. The EPE data gradient (Gradient::epe_gradient, gradient.cpp:198-227)
+ * joins the PE gradient in one adjoint pass per tile. epe == NULL means
+ * no EPs and the defaults above. tile_metrics (host, nullable):
+ * LITHO_EXCHANGE_TILE_METRICS doubles per tile; totals as for litho_exchange_compute. */
+int litho_exchange_compute_epe(litho_ctx* ctx, const litho_partition* partition,
+                               const litho_cache* cache, const float* d_masks,
+                               const float* d_global_target, double threshold, double alpha,
+                               const litho_exchange_options* opt, const litho_exchange_epe* epe,
+                               float* d_raw, float* d_grad, double* tile_metrics,
+                               double* totals);
 /* One fixed-step theta update of FullChipCTMOptimizer (source/optimizer/full_chip_ctm.cpp:127-147):
  * inside each tile's update window theta -= lr * (-1/2 grad sin theta); the
  * whole tile's mask = (1 + cos theta) / 2. d_grad == NULL only refreshes the

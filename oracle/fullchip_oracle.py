@@ -1,11 +1,11 @@
 """FP64 restatement of the reference full-chip partition, micro-gradient exchange and
 full-chip CTM (test infrastructure only, see ``oracle/__init__.py``).
 
-Follows source/utils/partition.cpp:21-120, source/utils/micro_gradient_exchange.cpp:65-334
-(PE and PEPenalty loss types, Core or Core+Guard loss region, guard-only or
-two-sided CEPT, Average or Linear guard-gradient fusion) and
-source/optimizer/full_chip_ctm.cpp:25-152. EPE loss types need EP selection
-(ep_select.cpp), which is outside the restated path.
+Follows source/utils/partition.cpp:21-120, source/utils/micro_gradient_exchange.cpp:18-334
+(PE, PEPenalty, EPE and PE_EPE loss types, Core or Core+Guard loss region, Core
+metrics, guard-only or two-sided CEPT, Average or Linear guard-gradient fusion) and
+source/optimizer/full_chip_ctm.cpp:25-152. EP selection (ep_select.cpp) is outside
+the restated path: the edge points are inputs, as they are for the device exchange.
 """
 from __future__ import annotations
 
@@ -152,12 +152,16 @@ def linear_strength(direction, y, x, rows, cols):
 
 @dataclasses.dataclass
 class ExchangeOptions:
-    """MicroGradientOptions (include/utils/micro_gradient_exchange.h:19-40), PE types."""
-    loss_type: str = "PE"            # "PE" or "PEPenalty"
+    """MicroGradientOptions (include/utils/micro_gradient_exchange.h:19-40)."""
+    loss_type: str = "PE"            # "PE", "PEPenalty", "EPE" or "PE_EPE"
     loss_region: str = "Core"        # "Core" or "CoreGuard"
+    main_region_dilation_pixels: int = 2
     pe_weight: float = 1.0
+    epe_weight: float = 1.0
     penalty_weight: float = 2.0
     penalty_threshold: float = 0.01
+    epe_pixel_size: float = 1.0
+    collect_core_metrics: bool = False
     enable_cept: bool = False
     cept_guard_only: bool = False
     cept_weight: float = 1.1
@@ -168,30 +172,72 @@ class ExchangeOptions:
 
 
 def loss_windows(local_target, region, opt):
-    """build_micro_loss_windows (micro_gradient_exchange.cpp:65-93), PE / PEPenalty."""
+    """build_micro_loss_windows (micro_gradient_exchange.cpp:65-93): (pe, penalty, epe)."""
+    import cv2
     pe = np.zeros_like(local_target)
     pen = np.zeros_like(local_target)
+    epe = np.zeros_like(local_target)
     sl = (slice(region.y0, region.y1), slice(region.x0, region.x1))
     pen[sl] = (local_target[sl] < 0.5)
+    epe[sl] = 1.0
     pe[sl] = (local_target[sl] > 0.5) if opt.loss_type == "PEPenalty" else 1.0
-    return pe, pen
+    if opt.loss_type == "PE_EPE":
+        main = (local_target > 0.5).astype(np.uint8)
+        if opt.main_region_dilation_pixels > 0:
+            main = cv2.dilate(main, np.ones((3, 3), np.uint8),
+                              iterations=opt.main_region_dilation_pixels,
+                              borderType=cv2.BORDER_CONSTANT, borderValue=0)
+        epe[sl] = (main[sl] != 0)
+        pe[sl] = 1.0 - epe[sl]
+    return pe, pen, epe
 
 
-def exchange(local_masks, global_target, meta, cache, thr, alpha, opt: ExchangeOptions):
-    """MicroGradientExchange::compute (micro_gradient_exchange.cpp:134-334) for PE types."""
-    wpe = opt.pe_weight
-    wpen = opt.penalty_weight if opt.loss_type == "PEPenalty" else 0.0
+def loss_weights(opt):
+    """micro_loss_weights (micro_gradient_exchange.cpp:95-99): (pe, epe, penalty)."""
+    return (0.0 if opt.loss_type == "EPE" else opt.pe_weight,
+            opt.epe_weight if opt.loss_type in ("EPE", "PE_EPE") else 0.0,
+            opt.penalty_weight if opt.loss_type == "PEPenalty" else 0.0)
+
+
+def region_eps_local(eps, weights, tile, region, height, width, periodic_guard, epe_window):
+    """region_eps_local (micro_gradient_exchange.cpp:18-50): the EPs (and, across the
+    layout edge, their periodic copies) inside the region whose bilinear stencil touches
+    the EPE window, in local coordinates, in EP order then copy order."""
+    g = region.shifted(tile.tile_global.y0, tile.tile_global.x0)
+    periods = 1 if periodic_guard else 0
+    out, w = [], []
+    for i in range(len(weights)):
+        for py in range(-periods, periods + 1):
+            for px in range(-periods, periods + 1):
+                y = eps[i][0] + py * height
+                x = eps[i][1] + px * width
+                if g.y0 <= y < g.y1 and g.x0 <= x < g.x1:
+                    ly, lx = y - tile.tile_global.y0, x - tile.tile_global.x0
+                    st = io.bilinear_stencil(epe_window.shape[0], epe_window.shape[1], ly, lx)
+                    if any(epe_window[sy, sx] != 0.0 for (sy, sx, _) in st):
+                        out.append((ly, lx))
+                        w.append(weights[i])
+    return np.array(out, dtype=np.float64).reshape(-1, 2), np.array(w, dtype=np.float64)
+
+
+def exchange(local_masks, global_target, meta, cache, thr, alpha, opt: ExchangeOptions,
+             eps=None, eps_weights=None):
+    """MicroGradientExchange::compute (micro_gradient_exchange.cpp:134-334)."""
+    wpe, wepe, wpen = loss_weights(opt)
+    evaluate_epe = opt.loss_type in ("EPE", "PE_EPE") or opt.collect_core_metrics
+    eps = np.zeros((0, 2)) if eps is None else np.asarray(eps, dtype=np.float64)
+    eps_weights = np.zeros(0) if eps_weights is None else np.asarray(eps_weights, dtype=np.float64)
     locals_ = []
     for t in meta.tiles:
         m = local_masks[t.id]
         tgt = extract_local_tile(global_target, t)
-        _, wafer, E = io.imaging_compute(m, cache, thr, alpha)
+        aerial, wafer, E = io.imaging_compute(m, cache, thr, alpha)
         region = t.update_local if opt.loss_region == "CoreGuard" else t.core_local
-        pe_w, pen_w = loss_windows(tgt, region, opt)
+        pe_w, pen_w, epe_w = loss_windows(tgt, region, opt)
         pe_loss = io.pe_loss(_blk(wafer, region), _blk(tgt, region), _blk(pe_w, region))
         bg = io.background_penalty_loss(_blk(wafer, region), _blk(tgt, region),
                                         opt.penalty_threshold, _blk(pen_w, region)) \
-            if opt.loss_type == "PEPenalty" else 0.0
+            if (opt.loss_type == "PEPenalty" or opt.collect_core_metrics) else 0.0
         if wpen != 0.0:
             raw = io.pe_gradient(wafer, tgt, E, cache, alpha, pe_window=pe_w, pe_weight=wpe,
                                  penalty=wpen, penalty_threshold=opt.penalty_threshold,
@@ -200,10 +246,38 @@ def exchange(local_masks, global_target, meta, cache, thr, alpha, opt: ExchangeO
             raw = wpe * io.pe_gradient(wafer, tgt, E, cache, alpha, pe_window=pe_w)
         else:
             raw = np.zeros_like(m)
-        data = wpe * pe_loss + wpen * bg
-        locals_.append(dict(pe_loss=pe_loss, bg_penalty_raw=bg, data_loss=data, loss=data,
-                            raw=raw, grad=raw.copy(), cept_loss=0.0,
-                            cept_grad=np.zeros_like(m)))
+        epe = dict(weighted_squared_loss=0.0, absolute_sum_nm=0.0, active_count=0)
+        if evaluate_epe:
+            le, lw = region_eps_local(eps, eps_weights, t, region, meta.height, meta.width,
+                                      opt.loss_region == "CoreGuard", epe_w)
+            epe = io.evaluate_sparse_epe(aerial, le, lw, thr, opt.epe_pixel_size)
+            if wepe != 0.0:
+                raw = raw + wepe * io.epe_gradient(aerial, E, cache, le, lw, thr)
+        data = wpe * pe_loss + wpen * bg + wepe * epe["weighted_squared_loss"]
+        core = dict(pe_loss=0.0, bg_penalty_raw=0.0, pe_penalty_loss=0.0, epe_loss=0.0,
+                    epe_abs_sum_nm=0.0, ep_count=0, epe_mean=0.0, data_loss=0.0)
+        if opt.collect_core_metrics:
+            c = t.core_local
+            cw, ct = _blk(wafer, c), _blk(tgt, c)
+            core["pe_loss"] = io.pe_loss(cw, ct, _blk(pe_w, c))
+            core["bg_penalty_raw"] = io.background_penalty_loss(cw, ct, opt.penalty_threshold,
+                                                                _blk(pen_w, c))
+            core["pe_penalty_loss"] = opt.pe_weight * io.pe_loss(cw, ct, (ct > 0.5) * 1.0) + \
+                opt.penalty_weight * core["bg_penalty_raw"]
+            ce, cwt = region_eps_local(eps, eps_weights, t, c, meta.height, meta.width, False,
+                                       epe_w)
+            cev = io.evaluate_sparse_epe(aerial, ce, cwt, thr, opt.epe_pixel_size)
+            core["epe_loss"] = cev["weighted_squared_loss"]
+            core["epe_abs_sum_nm"] = cev["absolute_sum_nm"]
+            core["ep_count"] = cev["active_count"]
+            core["epe_mean"] = core["epe_abs_sum_nm"] / core["ep_count"] if core["ep_count"] else 0.0
+            core["data_loss"] = wpe * core["pe_loss"] + wpen * core["bg_penalty_raw"] + \
+                wepe * core["epe_loss"]
+        locals_.append(dict(pe_loss=pe_loss, bg_penalty_raw=bg, penalty_loss=wpen * bg,
+                            epe_loss=epe["weighted_squared_loss"],
+                            epe_abs_sum_nm=epe["absolute_sum_nm"], epe_count=epe["active_count"],
+                            data_loss=data, loss=data, core=core, raw=raw, grad=raw.copy(),
+                            cept_loss=0.0, cept_grad=np.zeros_like(m)))
     for t in meta.tiles:
         L = locals_[t.id]
         for nb in t.neighbors:
@@ -241,13 +315,13 @@ def exchange(local_masks, global_target, meta, cache, thr, alpha, opt: ExchangeO
 
 
 def full_chip_ctm(initial_pattern, global_target, meta, cache, thr, alpha, opt, iterations,
-                  learning_rate):
+                  learning_rate, eps=None, eps_weights=None):
     """FullChipCTMOptimizer::optimize (source/optimizer/full_chip_ctm.cpp:25-152), CEPT guard-only."""
     opt = dataclasses.replace(opt, cept_guard_only=True)
     theta_g = io.initialize_theta(initial_pattern)
     thetas = [extract_local_tile(theta_g, t) for t in meta.tiles]
     masks = [io.theta_to_mask(th) for th in thetas]
-    ev = exchange(masks, global_target, meta, cache, thr, alpha, opt)
+    ev = exchange(masks, global_target, meta, cache, thr, alpha, opt, eps, eps_weights)
     history = [ev["loss"]]
     best = dict(loss=ev["loss"], iteration=0, masks=[m.copy() for m in masks])
     for it in range(1, iterations + 1):
@@ -258,7 +332,7 @@ def full_chip_ctm(initial_pattern, global_target, meta, cache, thr, alpha, opt, 
             gt = -0.5 * g * np.sin(th[w.y0:w.y1, w.x0:w.x1])
             th[w.y0:w.y1, w.x0:w.x1] -= learning_rate * gt
             masks[t.id] = io.theta_to_mask(th)
-        ev = exchange(masks, global_target, meta, cache, thr, alpha, opt)
+        ev = exchange(masks, global_target, meta, cache, thr, alpha, opt, eps, eps_weights)
         history.append(ev["loss"])
         if ev["loss"] < best["loss"]:
             best = dict(loss=ev["loss"], iteration=it, masks=[m.copy() for m in masks])
@@ -268,12 +342,34 @@ def full_chip_ctm(initial_pattern, global_target, meta, cache, thr, alpha, opt, 
 
 def full_chip_lsm(initial_binary, global_target, meta, cache, thr, alpha, opt: ExchangeOptions,
                   iterations, dx=1.0, dy=1.0, cfl=0.7, b=0.01, reinit_interval=20,
-                  mask_type="Binary", render_scale=4):
-    """FullChipLSMOptimizer::optimize (source/optimizer/full_chip_lsm.cpp:25-254), PE types:
-    Core + Guard loss region, guard-only CEPT, per-tile windowed RK2 with its own CFL dt,
-    periodic reinitialisation inside the window, masks rendered from the full local phi."""
+                  mask_type="Binary", render_scale=4, eps=None, eps_weights=None):
+    """FullChipLSMOptimizer::optimize (source/optimizer/full_chip_lsm.cpp:25-254):
+    Core + Guard loss region, guard-only CEPT, Core metrics, per-tile windowed RK2 with
+    its own CFL dt, periodic reinitialisation inside the window, masks rendered from the
+    full local phi. History rows carry the fields of full_chip_lsm.cpp:152-186."""
     from . import levelset_oracle as lo
-    opt = dataclasses.replace(opt, loss_region="CoreGuard", cept_guard_only=True)
+    opt = dataclasses.replace(opt, loss_region="CoreGuard", cept_guard_only=True,
+                              collect_core_metrics=True)
+    wpe, wepe, _ = loss_weights(opt)
+
+    def row(it, ev, dmin, dmax):
+        L = ev["locals"]
+        core = {k: sum(l["core"][k] for l in L) for k in (
+            "pe_loss", "bg_penalty_raw", "pe_penalty_loss", "epe_loss", "epe_abs_sum_nm",
+            "ep_count", "data_loss")}
+        core["epe_mean"] = core["epe_abs_sum_nm"] / core["ep_count"] if core["ep_count"] else 0.0
+        n = sum(l["epe_count"] for l in L)
+        a = sum(l["epe_abs_sum_nm"] for l in L)
+        return dict(iteration=it, loss=ev["loss"], data_loss=ev["data_loss"],
+                    cept_loss=ev["cept_loss"], min_dt=dmin, max_dt=dmax,
+                    pe_contribution=sum(wpe * l["pe_loss"] for l in L),
+                    penalty_contribution=sum(l["penalty_loss"] for l in L),
+                    epe_contribution=sum(wepe * l["epe_loss"] for l in L), core=core,
+                    total_pe_loss=sum(l["pe_loss"] for l in L),
+                    total_bg_penalty_raw=sum(l["bg_penalty_raw"] for l in L),
+                    total_epe_loss=sum(l["epe_loss"] for l in L), total_epe_abs_sum_nm=a,
+                    total_ep_count=n, epe_mean=a / n if n else 0.0)
+
     phis, masks = [], []
     for t in meta.tiles:
         m = extract_local_tile(initial_binary, t)
@@ -281,9 +377,8 @@ def full_chip_lsm(initial_binary, global_target, meta, cache, thr, alpha, opt: E
         phis.append(phi)
         masks.append(lo.render_levelset_mask(phi, mask_type, render_scale))
     initial_global_phi = assemble_global(phis, meta)
-    ev = exchange(masks, global_target, meta, cache, thr, alpha, opt)
-    history = [dict(iteration=0, loss=ev["loss"], data_loss=ev["data_loss"],
-                    cept_loss=ev["cept_loss"], min_dt=0.0, max_dt=0.0)]
+    ev = exchange(masks, global_target, meta, cache, thr, alpha, opt, eps, eps_weights)
+    history = [row(0, ev, 0.0, 0.0)]
     best = dict(loss=ev["loss"], iteration=0, phis=[p.copy() for p in phis],
                 masks=[m.copy() for m in masks])
     for it in range(1, iterations + 1):
@@ -309,9 +404,8 @@ def full_chip_lsm(initial_binary, global_target, meta, cache, thr, alpha, opt: E
             nphis.append(nxt)
             nmasks.append(lo.render_levelset_mask(nxt, mask_type, render_scale))
         phis, masks = nphis, nmasks
-        ev = exchange(masks, global_target, meta, cache, thr, alpha, opt)
-        history.append(dict(iteration=it, loss=ev["loss"], data_loss=ev["data_loss"],
-                            cept_loss=ev["cept_loss"], min_dt=min(steps), max_dt=max(steps)))
+        ev = exchange(masks, global_target, meta, cache, thr, alpha, opt, eps, eps_weights)
+        history.append(row(it, ev, min(steps), max(steps)))
         if ev["loss"] < best["loss"]:
             best = dict(loss=ev["loss"], iteration=it, phis=[p.copy() for p in phis],
                         masks=[m.copy() for m in masks])

@@ -85,3 +85,34 @@ def test_binarize_advanced_no_peaks_and_quantile():
     assert F._quantile_linear(v, -1.0) == 1.0 and F._quantile_linear(np.array([]), 0.3) == 0.0
     with pytest.raises(ValueError, match="sizes must match"):
         F.binarize_advanced(np.zeros((4, 4)), np.zeros((4, 5)))
+
+
+def test_full_chip_lsm_csv_schemas(tmp_path):
+    """history.csv / core_metrics_best.csv / summary.csv (demo_full_chip_lsm.cpp:170-201)."""
+    from types import SimpleNamespace as NS
+    core = NS(pe_loss=1.25, bg_penalty_raw=0.5, pe_penalty_loss=2.25, epe_loss=3.0 / 7.0,
+              epe_abs_sum_nm=12.0, ep_count=5, epe_mean=2.4, data_loss=1.0 / 3.0)
+    rows = [NS(iteration=i, loss=10.0 - i, data_loss=9.0 - i, cept_loss=0.1 * i, min_dt=0.01 * i,
+               max_dt=0.02 * i, pe_contribution=1.0, penalty_contribution=0.0,
+               epe_contribution=0.2, cept_contribution=0.11 * i, core=core, total_pe_loss=2.0,
+               total_bg_penalty_raw=0.0, total_epe_loss=0.5, total_epe_abs_sum_nm=20.0,
+               total_ep_count=9, epe_mean=20.0 / 9.0) for i in range(3)]
+    p = tmp_path / "history.csv"
+    F.write_lsm_history_csv(rows, str(p))
+    lines = p.read_text().splitlines()
+    assert lines[0].split(",")[:4] == ["iteration", "loss", "data_loss", "cept_loss"]
+    assert len(lines[0].split(",")) == 24 and len(lines) == 4
+    v = lines[2].split(",")
+    assert v[0] == "1" and float(v[1]) == 9.0 and v[15] == "5" and v[22] == "9"
+    assert float(v[13]) == 3.0 / 7.0 and float(v[23]) == 20.0 / 9.0     # 17 digits round-trip
+    tiles = [NS(id=t, core_global=NS(y0=10 * t, y1=10 * t + 10, x0=0, x1=16)) for t in range(2)]
+    res = NS(best_iteration=2, best_loss=8.0, history=rows, best_core_metrics=[core, core])
+    p = tmp_path / "core.csv"
+    F.write_core_metrics_csv(res, NS(tiles=tiles), str(p))
+    lines = p.read_text().splitlines()
+    assert lines[0].startswith("best_iteration,micro_id,y0,y1,x0,x1,core_pe")
+    assert lines[2].split(",")[:6] == ["2", "1", "10", "20", "0", "16"]
+    p = tmp_path / "summary.csv"
+    F.write_summary_csv(res, 1.5, str(p))
+    assert p.read_text().splitlines() == ["best_iteration,best_loss,final_iteration,final_loss,seconds",
+                                          "2,8,2,8,1.5"]

@@ -183,8 +183,16 @@ def test_fullchip_errors(L, FC, band128):
                                                        fusion_weight_owner=-1.0))
     assert e.value.status == 1
     with pytest.raises(L.LithoError) as e:
-        ex.compute(masks, tgt, FC.MicroGradientOptions(loss_type="EPE"))
+        ex.compute(masks, tgt, FC.MicroGradientOptions(loss_type="Contour"))
     assert e.value.status == 7
+    with pytest.raises(L.LithoError) as e:
+        ex.compute(masks, tgt, FC.MicroGradientOptions(loss_type="EPE"),
+                   eps=np.array([[1.0, float("nan")]]))
+    assert e.value.status == 3
+    with pytest.raises(L.LithoError) as e:
+        ex.compute(masks, tgt, FC.MicroGradientOptions(loss_type="PE_EPE",
+                                                       main_region_dilation_pixels=-1))
+    assert e.value.status == 1
     masks[1, 5, 7] = float("nan")
     with pytest.raises(L.LithoError) as e:
         ex.compute(masks, tgt)
@@ -238,3 +246,140 @@ def test_fullchip_lsm_matches_oracle(L, FC, band128, mask_type):
         # the returned masks are the renders of the returned phi
         assert np.array_equal(cpu(res.local_masks)[t.id],
                               cpu(L.render_levelset_mask(res.local_phi[t.id], mask_type, 4)))
+
+
+THR_E = 0.17   # about the aerial intensity at the edges of big_target's features
+
+
+def big_target(H, W, seed):
+    """Rectangles of 80-160 nm (20-40 px): resolved edges, |grad I| ~ 0.015 / px. Two
+    of them have an edge 3 px from the layout border, so that the periodic copies of
+    their edge points fall into the Guards across the border."""
+    rng = np.random.default_rng(seed)
+    t = np.zeros((H, W))
+    for _ in range(6):
+        h, w = rng.integers(20, 40), rng.integers(20, 40)
+        y, x = rng.integers(8, H - h - 8), rng.integers(8, W - w - 8)
+        t[y:y + h, x:x + w] = 1.0
+    t[3:30, W // 3:W // 3 + 30] = 1.0
+    t[H // 2:H // 2 + 26, 3:28] = 1.0
+    return t
+
+
+def contour_eps(target, seed, stride=3):
+    """Synthetic edge points on the 0.5 contour of a binary layout (pixel-edge midlines,
+    jittered along the edge), every stride-th kept; every seventh has weight 0
+    (inactive)."""
+    rng = np.random.default_rng(seed)
+    H, W = target.shape
+    pts = []
+    ys, xs = np.nonzero(np.diff(target, axis=0))
+    pts += [(y + 0.5, x + rng.uniform(-0.3, 0.3)) for y, x in zip(ys, xs)]
+    ys, xs = np.nonzero(np.diff(target, axis=1))
+    pts += [(y + rng.uniform(-0.3, 0.3), x + 0.5) for y, x in zip(ys, xs)]
+    eps = np.clip(np.array(pts[::stride]), 0.0, [H - 1e-6, W - 1e-6])
+    w = np.ones(len(eps))
+    w[::7] = 0.0
+    return eps, w
+
+
+EPE_OPTION_SETS = [
+    dict(loss_type="EPE", epe_weight=0.3, epe_pixel_size=2.0),
+    dict(loss_type="PE_EPE", loss_region="CoreGuard", main_region_dilation_pixels=2,
+         pe_weight=0.8, epe_weight=0.05, collect_core_metrics=True, enable_cept=True,
+         cept_guard_only=True, enable_grad_fusion=True, fusion_mode="Linear"),
+    dict(loss_type="PEPenalty", loss_region="Core", collect_core_metrics=True, epe_pixel_size=4.0),
+]
+
+
+@pytest.mark.parametrize("oi", range(len(EPE_OPTION_SETS)))
+def test_exchange_epe_matches_oracle(L, FC, band128, oi):
+    """EPE / PE_EPE loss types and Core metrics (micro_gradient_exchange.cpp:144-245)
+    against the oracle, with caller-supplied EPs. EP counts are exact. The EPE divides
+    by |grad I| (~0.015 / px here), so the FP32 image error (~1e-6 absolute) reaches
+    ~1e-4 relative per point: EPE sums and EPE-driven gradients are held to 1e-3
+    relative, PE terms to 1e-5."""
+    oc, _ = band128
+    cfg = (280, 190, 3, 2, 16, 6)
+    meta = fc.build(*cfg)
+    part = FC.Partition(*cfg)
+    cache = L.ImagingCache.from_kernels(np.stack(oc.kernels), oc.source_ws, oc.eigenvalues)
+    target = big_target(cfg[0], cfg[1], 20 + oi)
+    eps, w = contour_eps(target, oi)
+    rng = np.random.default_rng(30 + oi)
+    theta_g = io.initialize_theta(target)     # edges where the EPs are
+    masks32 = [io.theta_to_mask(fc.extract_local_tile(theta_g, t)
+                                + 0.02 * rng.standard_normal((meta.tile_size,) * 2)).astype(np.float32)
+               for t in meta.tiles]
+    masks = [m.astype(np.float64) for m in masks32]
+    opts = EPE_OPTION_SETS[oi]
+    ev = fc.exchange(masks, target, meta, oc, THR_E, ALPHA, fc.ExchangeOptions(**opts), eps, w)
+    ex = FC.MicroGradientExchange(part, cache, THR_E, ALPHA)
+    res = ex.compute(torch.from_numpy(np.stack(masks32)).cuda(),
+                     torch.from_numpy(target.astype(np.float32)).cuda(),
+                     FC.MicroGradientOptions(**opts), eps=eps, eps_weights=w)
+    raw, grad = cpu(res.raw_gradients), cpu(res.mask_gradients)
+
+    def close(a, b, tol=1e-4, floor=1e-9):
+        return abs(a - b) <= tol * max(abs(b), floor)
+
+    n_active = 0
+    for t in meta.tiles:
+        o, g = ev["locals"][t.id], res.locals[t.id]
+        assert rel_l2(raw[t.id], o["raw"]) < 1e-3, t.id
+        assert rel_l2(grad[t.id], o["grad"]) < 1e-3, t.id
+        assert g.epe_count == o["epe_count"], t.id
+        n_active += g.epe_count
+        assert close(g.epe_loss, o["epe_loss"], 1e-3) and close(g.epe_abs_sum_nm, o["epe_abs_sum_nm"], 1e-3)
+        assert close(g.pe_loss, o["pe_loss"], 1e-5) and close(g.bg_penalty_raw, o["bg_penalty_raw"], 1e-5)
+        assert close(g.data_loss, o["data_loss"], 1e-3) and close(g.loss, o["loss"], 1e-3)
+        c, oc_ = g.core, o["core"]
+        assert c.ep_count == oc_["ep_count"]
+        for k in ("pe_loss", "bg_penalty_raw", "pe_penalty_loss"):
+            assert close(getattr(c, k), oc_[k], 1e-5), (t.id, k)
+        for k in ("epe_loss", "epe_abs_sum_nm", "epe_mean", "data_loss"):
+            assert close(getattr(c, k), oc_[k], 1e-3), (t.id, k)
+    if opts["loss_type"] in ("EPE", "PE_EPE") or opts.get("collect_core_metrics"):
+        assert n_active > 0
+    assert close(res.loss, ev["loss"], 1e-3) and close(res.data_loss, ev["data_loss"], 1e-3)
+    if opts.get("collect_core_metrics"):
+        assert sum(l.core.ep_count for l in res.locals) > 0
+
+
+def test_fullchip_lsm_pe_epe_history(L, FC, band128):
+    """FullChipLSMOptimizer with the PE_EPE loss type: history rows (contributions, Core
+    sums, EP totals; full_chip_lsm.cpp:152-186) and best Core metrics against the oracle
+    over two steps."""
+    oc, _ = band128
+    cfg = (192, 192, 2, 2, 16, 6)
+    meta = fc.build(*cfg)
+    part = FC.Partition(*cfg)
+    cache = L.ImagingCache.from_kernels(np.stack(oc.kernels), oc.source_ws, oc.eigenvalues)
+    target = big_target(192, 192, 9)
+    eps, _ = contour_eps(target, 9)
+    opts = dict(loss_type="PE_EPE", epe_weight=0.02, enable_cept=True)
+    kw = dict(dx=1.0, dy=1.0, cfl=0.7, b=0.01, reinit_interval=0, mask_type="Binary",
+              render_scale=4)
+    ones = np.ones(len(eps))     # the LSM default epe_all_eps = true
+    ref = fc.full_chip_lsm(target, target, meta, oc, THR_E, ALPHA, fc.ExchangeOptions(**opts), 2,
+                           eps=eps, eps_weights=ones, **kw)
+    optz = FC.FullChipLSMOptimizer(part, cache, THR_E, ALPHA)
+    res = optz.optimize(torch.from_numpy(target.astype(np.float32)).cuda(),
+                        torch.from_numpy(target.astype(np.float32)).cuda(),
+                        FC.FullChipLSMOptions(iterations=2, cfl=0.7, curvature_weight=0.01,
+                                              reinit_interval=0,
+                                              gradient_options=FC.MicroGradientOptions(
+                                                  **opts, epe_all_eps=True)),
+                        eps=eps)
+    assert len(res.history) == 3
+    for a, b in zip(res.history, ref["history"]):
+        tol = 1e-3
+        for k in ("loss", "data_loss", "pe_contribution", "epe_contribution", "total_pe_loss",
+                  "total_epe_loss", "total_epe_abs_sum_nm", "epe_mean"):
+            assert abs(getattr(a, k) - b[k]) <= tol * max(abs(b[k]), 1e-9), (a.iteration, k)
+        assert a.total_ep_count == b["total_ep_count"] and a.core.ep_count == b["core"]["ep_count"]
+        for k in ("pe_loss", "epe_loss", "epe_mean", "data_loss"):
+            assert abs(getattr(a.core, k) - b["core"][k]) <= tol * max(abs(b["core"][k]), 1e-9), k
+    assert res.history[0].total_ep_count > 0 and res.history[0].epe_contribution > 0.0
+    assert res.best_iteration == ref["best"]["iteration"]
+    assert len(res.best_core_metrics) == part.num_tiles

@@ -81,3 +81,61 @@ def test_guard_only_cept_and_fusion():
         c = t.core_local
         assert np.linalg.norm(ev["locals"][t.id]["cept_grad"][c.y0:c.y1, c.x0:c.x1]) == 0.0
     assert res["best"]["iteration"] > 0
+
+
+def _literal_windows(target, region, radius, loss_type):
+    """The independent window restatement of test_micro_gradient_exchange.cpp:497-518:
+    the PE_EPE main region as "a target pixel > 0.5 within L-infinity distance radius"."""
+    pe = np.zeros_like(target); epe = np.zeros_like(target); pen = np.zeros_like(target)
+    H, W = target.shape
+    for y in range(region.y0, region.y1):
+        for x in range(region.x0, region.x1):
+            main = bool(np.any(target[max(0, y - radius):min(H - 1, y + radius) + 1,
+                                      max(0, x - radius):min(W - 1, x + radius) + 1] > 0.5))
+            epe[y, x] = main if loss_type == "PE_EPE" else 1.0
+            pe[y, x] = (not main) if loss_type == "PE_EPE" else \
+                (target[y, x] > 0.5 if loss_type == "PEPenalty" else 1.0)
+            pen[y, x] = target[y, x] < 0.5
+    return pe, pen, epe
+
+
+def test_loss_windows_match_reference_known_answer():
+    """check_loss_windows (test_micro_gradient_exchange.cpp:520-546): dilation before the
+    region cut, zero border, strict > 0.5, mutually exclusive PE / EPE windows."""
+    target = np.zeros((12, 15))
+    target[0, 0] = 1.0
+    target[2, 2] = 0.5
+    target[4:8, 5:9] = 1.0
+    target[5, 6] = 0.0
+    target[1, 8] = 1.0
+    region = fc.Rect(2, 11, 3, 14)
+    for radius in (0, 1, 2, 4):
+        opt = fc.ExchangeOptions(loss_type="PE_EPE", main_region_dilation_pixels=radius)
+        pe, pen, epe = fc.loss_windows(target, region, opt)
+        rpe, rpen, repe = _literal_windows(target, region, radius, "PE_EPE")
+        assert np.array_equal(pe, rpe) and np.array_equal(epe, repe) and np.array_equal(pen, rpen)
+        assert np.sum(pe * epe) == 0.0 and pe.sum() + epe.sum() == region.rows * region.cols
+    for lt in ("PE", "PEPenalty", "EPE"):
+        pe, pen, epe = fc.loss_windows(target, region, fc.ExchangeOptions(loss_type=lt))
+        rpe, rpen, repe = _literal_windows(target, region, 0, lt)
+        assert np.array_equal(pe, rpe) and np.array_equal(epe, repe) and np.array_equal(pen, rpen)
+
+
+def test_region_eps_local_periodic_copies():
+    """region_eps_local (micro_gradient_exchange.cpp:18-50): half-open global region,
+    periodic copies only for Core + Guard, window test on the clamped bilinear stencil."""
+    meta = fc.build(32, 32, 2, 2, 8, 3)
+    t0 = meta.tiles[0]                      # Core [0,16) x [0,16), tile origin (-8, -8)
+    win = np.zeros((meta.tile_size,) * 2)
+    r = t0.update_local
+    win[r.y0:r.y1, r.x0:r.x1] = 1.0
+    eps = np.array([[5.25, 6.5], [31.5, 4.0], [16.0, 3.0], [15.99, 15.5], [2.0, 30.6]])
+    w = np.array([1.0, 0.5, 1.0, 0.0, 2.0])
+    le, lw = fc.region_eps_local(eps, w, t0, t0.core_local, 32, 32, False, win)
+    # (16.0, 3.0) is on the Core's open edge; the periodic points stay out without copies
+    assert np.allclose(le, [[13.25, 14.5], [23.99, 23.5]]) and np.allclose(lw, [1.0, 0.0])
+    le, lw = fc.region_eps_local(eps, w, t0, t0.update_local, 32, 32, True, win)
+    got = {(round(a, 3), round(b, 3)) for a, b in le}
+    # copies one layout up / left land in the Guard: y 31.5 - 32 = -0.5, x 30.6 - 32 = -1.4
+    assert (7.5, 12.0) in got and (10.0, 6.6) in got and (24.0, 11.0) in got
+    assert len(le) == len(lw) == 5
