@@ -62,6 +62,28 @@ def workload(N, K, seed):
     return band, r0, c0, w, wss, target, theta
 
 
+def rank_env():
+    """(rank, world size, local rank) of this process under torchrun, else (0, 1, 0)."""
+    return (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
+            int(os.environ.get("LOCAL_RANK", "0")))
+
+
+def max_over_ranks(value, dist, device):
+    """The largest value over all ranks (every rank calls this in the same order)."""
+    if not dist:
+        return float(value)
+    import torch
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_throughput(world, steps, total_ms):
+    """Whole-job tile-iterations per second: every rank ran `steps` evaluations of its
+    own tile and the slowest rank took total_ms."""
+    return world * steps / (total_ms / 1e3)
+
+
 def peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -185,8 +207,7 @@ def cpu_baseline(N, K, band, r0, c0, w, wss, target, theta, seconds):
 
 
 def run_reference(args):
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank, world, _ = rank_env()
     if rank != 0:
         return
     from oracle import imaging_oracle as io
@@ -271,11 +292,8 @@ def _measure(L, torch, ctx, stream, cache, target, th, flush, steps, warmup, dis
     torch.cuda.synchronize()
     stages = ctx.stage_times()
     ctx.enable_stage_timing(False)
-    total_ms = sum(times)
+    total_ms = max_over_ranks(sum(times), dist, "cuda")
     if dist:
-        t = torch.tensor([total_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
         dist.barrier()
     return dict(opt=opt, times=times, total_ms=total_ms, stages=stages, launches=launches)
 
@@ -283,9 +301,7 @@ def _measure(L, torch, ctx, stream, cache, target, th, flush, steps, warmup, dis
 def run_ours(args):
     import ctypes
     import torch
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    rank, world, local = rank_env()
     torch.cuda.set_device(local)
     dist = None
     if world > 1:
@@ -317,7 +333,7 @@ def run_ours(args):
     head = modes[-1]          # the tensor-core path when both ran
     R = runs[head]
     ctx, cache, opt = R["ctx"], R["cache"], R["opt"]
-    value = world * args.steps / (R["total_ms"] / 1e3)
+    value = job_throughput(world, args.steps, R["total_ms"])
 
     # End to end through the host-buffer entry point (H2D + compute + D2H per step).
     h_theta = torch.tensor(theta, dtype=torch.float32).pin_memory()
@@ -346,12 +362,8 @@ def run_ours(args):
         e1.record(stream)
         e1.synchronize()
         e2e_times.append(e0.elapsed_time(e1))
-    e2e_total = sum(e2e_times)
-    if dist:
-        t = torch.tensor([e2e_total], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_total = float(t.item())
-    e2e_value = world * args.steps / (e2e_total / 1e3)
+    e2e_total = max_over_ranks(sum(e2e_times), dist, "cuda")
+    e2e_value = job_throughput(world, args.steps, e2e_total)
 
     if rank != 0:
         if dist:
@@ -377,7 +389,7 @@ def run_ours(args):
         "stages_ms_per_step": {k: v[0] / max(v[1], 1) for k, v in stages.items() if v[1]},
         "latency_ms": {"p50": float(np.percentile(R["times"], 50)),
                        "p99": float(np.percentile(R["times"], 99))},
-        "precision_modes": {m: {"value": world * args.steps / (runs[m]["total_ms"] / 1e3),
+        "precision_modes": {m: {"value": job_throughput(world, args.steps, runs[m]["total_ms"]),
                                 "ms_per_step": runs[m]["total_ms"] / args.steps}
                             for m in runs},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * 4 * N * N,

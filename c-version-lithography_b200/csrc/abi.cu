@@ -617,7 +617,7 @@ int run_forward(Context* ctx, const Cache& c, Field& f, const Layout& L, int inp
                       "row synthesis");
   }
   ctx->stage_end(3);
-  ctx->launches += 7;
+  ctx->launches += 3 + band_forward_launches(g);   // analysis, reduction, band, synthesis
   f.valid = (st == LITHO_OK);
   return st;
 }
@@ -884,10 +884,6 @@ static int ctm_evaluate_impl(litho_ctx* ctx, const litho_cache* cache, litho_fie
   auto launch_chain = [&]() -> int {
     int nb = 0;
     int r = run_forward(ctx, *cache, *f, L, 1, d_theta, d_mask, ep, &nb, target_ready, fuse);
-    if (!r)
-      r = check_launch(ctx, launch_sum_partials(ctx->stream, ctx->d_red + RED_PART, nb, 2,
-                                                ctx->d_red + RED_SUM),
-                       "sum");
     GradEpilogue gp{};
     gp.grad_mask = d_grad_mask;
     gp.theta = d_theta;
@@ -896,11 +892,14 @@ static int ctm_evaluate_impl(litho_ctx* ctx, const litho_cache* cache, litho_fie
     int nb2 = 0;
     if (!r)
       r = run_adjoint(ctx, *cache, *f, L, at<float>(ctx, L.dldi), 4.0 * alpha, gp, &nb2, fuse);
+    // Both FP64 sums (loss terms and the gradient norm) in one launch at the end, off
+    // the path between the forward and the adjoint.
     if (!r)
-      r = check_launch(ctx, launch_sum_partials(ctx->stream, gp.norm_partial, nb2, 1,
-                                                ctx->d_red + RED_SUM + 2),
+      r = check_launch(ctx, launch_sum_partials2(ctx->stream, ctx->d_red + RED_PART, nb, 2,
+                                                 ctx->d_red + RED_SUM, gp.norm_partial, nb2, 1,
+                                                 ctx->d_red + RED_SUM + 2),
                        "sum");
-    ctx->launches += 2;
+    ctx->launches += 1;
     return r;
   };
   // Repeated evaluations on the same buffers replay a CUDA graph of the chain.

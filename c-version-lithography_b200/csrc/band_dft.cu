@@ -559,34 +559,12 @@ static size_t chat_smem(const BandGeom& g) {
 // x tile x / 128 at img + (x / 128) * img_tile_bytes, hi of column f at
 // sw128_offset(128, x % 128, f) and lo at sw128_offset(128, x % 128, kp + f).
 constexpr int EX_X = 64, EX_R = 8, EX_NT = 256;
-__global__ void __launch_bounds__(EX_NT)
-expand_kernel(const float2* __restrict__ coef, int nrows, int ncoef, int ld,
-              const float2* __restrict__ TX, int N, int mode, int nc, int kp,
-              float* __restrict__ Ut, uint8_t* __restrict__ img, uint32_t img_tile_bytes) {
-  extern __shared__ float2 se[];
-  float2* cf = se;                    // [EX_R][ncoef]
-  float2* ph = se + EX_R * ncoef;     // [ncoef][EX_X]
-  const int x0 = blockIdx.x * EX_X, a0 = blockIdx.y * EX_R;
-  pdl_trigger();
-  fill_batched<EX_NT>(ph, ncoef * EX_X, [&](int i) {
-    const int c = i / EX_X, xx = i % EX_X, x = x0 + xx;
-    float2 t = make_float2(0.f, 0.f);
-    if (x < N) {
-      if (mode == 0) {
-        t = conjf2(TX[(size_t)c * N + x]);
-      } else {
-        const int d = c - (nc - 1);
-        t = d >= 0 ? conjf2(TX[(size_t)d * N + x]) : TX[(size_t)(-d) * N + x];
-      }
-    }
-    return t;
-  });
-  pdl_wait();
-  fill_batched<EX_NT>(cf, EX_R * ncoef, [&](int i) {
-    const int r = i / ncoef, c = i % ncoef;
-    return (a0 + r < nrows) ? coef[(size_t)(a0 + r) * ld + c] : make_float2(0.f, 0.f);
-  });
-  __syncthreads();
+// The accumulation and store of the expansion for one CTA, from its staged
+// coefficients cf [EX_R][ncoef] and phases ph [ncoef][EX_X].
+__device__ __forceinline__ void expand_store(const float2* cf, const float2* ph, int nrows,
+                                             int ncoef, int N, int mode, int kp, int a0, int x0,
+                                             float* __restrict__ Ut, uint8_t* __restrict__ img,
+                                             uint32_t img_tile_bytes) {
   // Thread (xx, rq): rows a0 + 2 rq and a0 + 2 rq + 1, i.e. the four consecutive
   // output columns f0 .. f0 + 3 of image row x, written as one 8- or 16-byte store.
   const int xx = threadIdx.x % EX_X, rq = threadIdx.x / EX_X;
@@ -636,6 +614,117 @@ expand_kernel(const float2* __restrict__ coef, int nrows, int ncoef, int ld,
   }
 }
 
+__global__ void __launch_bounds__(EX_NT)
+expand_kernel(const float2* __restrict__ coef, int nrows, int ncoef, int ld,
+              const float2* __restrict__ TX, int N, int mode, int nc, int kp,
+              float* __restrict__ Ut, uint8_t* __restrict__ img, uint32_t img_tile_bytes) {
+  extern __shared__ float2 se[];
+  float2* cf = se;                    // [EX_R][ncoef]
+  float2* ph = se + EX_R * ncoef;     // [ncoef][EX_X]
+  const int x0 = blockIdx.x * EX_X, a0 = blockIdx.y * EX_R;
+  pdl_trigger();
+  fill_batched<EX_NT>(ph, ncoef * EX_X, [&](int i) {
+    const int c = i / EX_X, xx = i % EX_X, x = x0 + xx;
+    float2 t = make_float2(0.f, 0.f);
+    if (x < N) {
+      if (mode == 0) {
+        t = conjf2(TX[(size_t)c * N + x]);
+      } else {
+        const int d = c - (nc - 1);
+        t = d >= 0 ? conjf2(TX[(size_t)d * N + x]) : TX[(size_t)(-d) * N + x];
+      }
+    }
+    return t;
+  });
+  pdl_wait();
+  fill_batched<EX_NT>(cf, EX_R * ncoef, [&](int i) {
+    const int r = i / ncoef, c = i % ncoef;
+    return (a0 + r < nrows) ? coef[(size_t)(a0 + r) * ld + c] : make_float2(0.f, 0.f);
+  });
+  __syncthreads();
+  expand_store(cf, ph, nrows, ncoef, N, mode, kp, a0, x0, Ut, img, img_tile_bytes);
+}
+
+// Forward 3 + 4 in one launch: the CTA's rows of chat (band_chat_kernel's arithmetic
+// for rows a0 .. a0 + EX_R - 1) straight from the small-grid intensity, then the
+// mode-1 expansion of expand_kernel. Every x strip of a row group recomputes the
+// same rows (about 0.2 MFLOP), which is cheaper than a launch between them.
+__global__ void __launch_bounds__(EX_NT)
+expand_intensity_kernel(const float* __restrict__ iP, int Nr, int Nc, int Pr, int Pc,
+                        const float2* __restrict__ EDr_t, const float2* __restrict__ EDc,
+                        float inv, const float2* __restrict__ TX, int N, int kp,
+                        float* __restrict__ Ut, uint8_t* __restrict__ img,
+                        uint32_t img_tile_bytes) {
+  extern __shared__ float2 se[];
+  const int nd = 2 * Nc - 1;
+  float2* cf = se;                      // [EX_R][nd]
+  float2* ph = cf + EX_R * nd;          // [nd][EX_X]
+  float2* edr = ph + nd * EX_X;         // [EX_R][Pr]
+  float2* edc = edr + EX_R * Pr;        // [Pc][nd]
+  float2* v = edc + Pc * nd;            // [EX_R][Pc]
+  float* ip = reinterpret_cast<float*>(v + EX_R * Pc);   // [Pr][Pc]
+  const int x0 = blockIdx.x * EX_X, a0 = blockIdx.y * EX_R;
+  pdl_trigger();
+  fill_batched<EX_NT>(ph, nd * EX_X, [&](int i) {
+    const int c = i / EX_X, x = x0 + i % EX_X;
+    const int d = c - (Nc - 1);
+    float2 t = make_float2(0.f, 0.f);
+    if (x < N) t = d >= 0 ? conjf2(TX[(size_t)d * N + x]) : TX[(size_t)(-d) * N + x];
+    return t;
+  });
+  fill_batched<EX_NT>(edr, EX_R * Pr, [&](int i) {
+    const int r = i / Pr, jr = i % Pr;
+    return a0 + r < Nr ? EDr_t[(size_t)(a0 + r + Nr - 1) * Pr + jr] : make_float2(0.f, 0.f);
+  });
+  fill_batched<EX_NT>(edc, Pc * nd, [&](int i) { return EDc[i]; });
+  pdl_wait();
+  fill_batched<EX_NT>(ip, Pr * Pc, [&](int i) { return iP[i]; });
+  __syncthreads();
+  for (int i = threadIdx.x; i < EX_R * Pc; i += EX_NT) {
+    const int r = i / Pc, jc = i % Pc;
+    const float2* ed = edr + r * Pr;
+    float2 a = make_float2(0.f, 0.f), b = a;
+    int jr = 0;
+    for (; jr + 1 < Pr; jr += 2) {
+      const float i0 = ip[jr * Pc + jc], i1 = ip[(jr + 1) * Pc + jc];
+      a.x = fmaf(ed[jr].x, i0, a.x); a.y = fmaf(-ed[jr].y, i0, a.y);
+      b.x = fmaf(ed[jr + 1].x, i1, b.x); b.y = fmaf(-ed[jr + 1].y, i1, b.y);
+    }
+    if (jr < Pr) {
+      const float i0 = ip[jr * Pc + jc];
+      a.x = fmaf(ed[jr].x, i0, a.x); a.y = fmaf(-ed[jr].y, i0, a.y);
+    }
+    v[i] = make_float2(a.x + b.x, a.y + b.y);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < EX_R * nd; i += EX_NT) {
+    const int r = i / nd, dc = i % nd;
+    const float2* vr = v + r * Pc;
+    float2 a = make_float2(0.f, 0.f), b = a;
+    int jc = 0;
+    for (; jc + 1 < Pc; jc += 2) {
+      cfma(a, vr[jc], conjf2(edc[jc * nd + dc]));
+      cfma(b, vr[jc + 1], conjf2(edc[(jc + 1) * nd + dc]));
+    }
+    if (jc < Pc) cfma(a, vr[jc], conjf2(edc[jc * nd + dc]));
+    cf[i] = make_float2((a.x + b.x) * inv, (a.y + b.y) * inv);
+  }
+  __syncthreads();
+  expand_store(cf, ph, Nr, nd, N, 1, kp, a0, x0, Ut, img, img_tile_bytes);
+}
+
+static size_t expand_intensity_smem(const BandGeom& g) {
+  const int nd = 2 * g.Nc - 1;
+  return (size_t)(EX_R * nd + nd * EX_X + EX_R * g.Pr + g.Pc * nd + EX_R * g.Pc) * sizeof(float2) +
+         (size_t)g.Pr * g.Pc * sizeof(float);
+}
+// Up to this much shared memory two CTAs of the merged kernel share an SM.
+constexpr size_t EXPAND_INTENSITY_MAX_SMEM = 112 * 1024;
+
+int band_forward_launches(const BandGeom& g) {
+  return expand_intensity_smem(g) <= EXPAND_INTENSITY_MAX_SMEM ? 3 : 4;
+}
+
 static cudaError_t launch_expand(cudaStream_t s, const float2* coef, int nrows, int ncoef, int ld,
                                  const float2* TX, int N, int mode, int nc, int kp, float* Ut,
                                  void* img) {
@@ -668,6 +757,18 @@ cudaError_t launch_band_forward(cudaStream_t s, const Cache& c, Field& f, float*
                    static_cast<const float*>(ik), g.K, n, iP);
   if (err != cudaSuccess) return err;
   const int nd = 2 * g.Nc - 1;
+  const size_t smx = expand_intensity_smem(g);
+  if (smx <= EXPAND_INTENSITY_MAX_SMEM) {
+    err = cudaFuncSetAttribute(expand_intensity_kernel,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx);
+    if (err != cudaSuccess) return err;
+    const uint32_t img_tile_bytes = (uint32_t)((2 * g.kp_rows + 63) / 64) * 128u * 128u;
+    dim3 grid((g.N + EX_X - 1) / EX_X, (g.Nr + EX_R - 1) / EX_R);
+    return launch_pdl(expand_intensity_kernel, grid, dim3(EX_NT), smx, s,
+                      static_cast<const float*>(iP), g.Nr, g.Nc, g.Pr, g.Pc, c.EDr_t, c.EDc,
+                      1.f / ((float)g.Pr * (float)g.Pc), c.TXDc, g.N, g.kp_rows, Ut,
+                      static_cast<uint8_t*>(img), img_tile_bytes);
+  }
   const size_t smc = chat_smem(g);
   err = cudaFuncSetAttribute(band_chat_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)smc);
@@ -874,6 +975,29 @@ __global__ void sum_partials_kernel(const double* __restrict__ part, int n, int 
 cudaError_t launch_sum_partials(cudaStream_t s, const double* part, int n, int stride,
                                 double* out) {
   return launch_pdl(sum_partials_kernel, dim3(stride), dim3(32), 0, s, part, n, stride, out);
+}
+
+// Two partial sets in one launch: blocks [0, sa) sum a's components, the rest b's.
+__global__ void sum_partials2_kernel(const double* __restrict__ a, int na, int sa,
+                                     double* __restrict__ out_a, const double* __restrict__ b,
+                                     int nb, int sb, double* __restrict__ out_b) {
+  pdl_trigger();
+  pdl_wait();
+  const bool first = (int)blockIdx.x < sa;
+  const int comp = first ? blockIdx.x : blockIdx.x - sa;
+  const double* part = first ? a : b;
+  const int n = first ? na : nb, stride = first ? sa : sb;
+  double s = 0.0;
+  for (int i = threadIdx.x; i < n; i += 32) s += part[(size_t)i * stride + comp];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (threadIdx.x == 0) (first ? out_a : out_b)[comp] = s;
+}
+
+cudaError_t launch_sum_partials2(cudaStream_t s, const double* a, int na, int sa, double* out_a,
+                                 const double* b, int nb, int sb, double* out_b) {
+  return launch_pdl(sum_partials2_kernel, dim3(sa + sb), dim3(32), 0, s, a, na, sa, out_a, b, nb,
+                    sb, out_b);
 }
 
 // ---------------------------------------------------------------- field export

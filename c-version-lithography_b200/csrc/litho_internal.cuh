@@ -189,6 +189,9 @@ cudaError_t launch_reduce_tiles(cudaStream_t s, const float2* part, int tiles, i
 // Shared memory of its per-kernel CTA: band_fields_smem.
 size_t band_fields_smem(const BandGeom& g);
 size_t band_max_smem(const BandGeom& g);
+// Kernels launch_band_forward issues: fields, sum over k, then either the merged
+// chat + expansion (when its staging fits two CTAs per SM) or the two separately.
+int band_forward_launches(const BandGeom& g);
 cudaError_t launch_band_forward(cudaStream_t s, const Cache& c, Field& f, float* ik, float* iP,
                                 float2* chat, float* Ut, void* img);
 // Small-grid stage of the adjoint: gh (the D-band DFT of dL/dI) -> gam, Zk, X and Vt
@@ -222,6 +225,8 @@ cudaError_t launch_synth_grad(cudaStream_t s, const float* AY, const float* Bt, 
                               const GradEpilogue& ep, int* nblocks);
 cudaError_t launch_sum_partials(cudaStream_t s, const double* part, int n, int stride,
                                 double* out);
+cudaError_t launch_sum_partials2(cudaStream_t s, const double* a, int na, int sa, double* out_a,
+                                 const double* b, int nb, int sb, double* out_b);
 cudaError_t launch_export_field(cudaStream_t s, const Cache& c, const Field& f, int k,
                                 float2* tmp_rows, float2* out);
 cudaError_t launch_pe_loss(cudaStream_t s, const float* w, const float* t, const float* pe_win,
