@@ -418,7 +418,7 @@ __device__ __forceinline__ void fill_batched(T* dst, int n, Load load) {
 // columns jc in [q CW, q CW + CW): A = H_k m on the band, T = A ESc^T restricted
 // to those columns (Nr x CW) and e_k = ESr T (Pr x CW); ik = w_k |e_k|^2. Columns
 // are independent, so the split costs no recomputation.
-constexpr int BF_NT = 256;
+constexpr int BF_NT = 512;   // threads of the fields and Z kernels (more loads in flight while staging)
 constexpr int BF_CW = 10;   // small-grid columns per CTA (forward fields)
 constexpr int BZ_UW = 7;    // band columns per CTA (adjoint Z)
 __global__ void __launch_bounds__(BF_NT)
