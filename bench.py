@@ -50,6 +50,9 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=12.0)
     p.add_argument("--precision", default="auto", choices=["auto", "fp32", "bf16x3"],
                    help="auto: time both, report the split-BF16 tensor-core path")
+    p.add_argument("--batch", type=int, default=16,
+                   help="tiles per step of the batched split-BF16 evaluation (the headline); "
+                        "1 reports the single-tile chain")
     return p.parse_args()
 
 
@@ -247,23 +250,28 @@ def run_reference(args):
     print(json.dumps(out), flush=True)
 
 
-def config_dict(N, K, precision):
-    return {"workload": f"CTM objective evaluation (forward + adjoint) on one {N}^2 tile, "
-                        f"{K} SOCS kernels of 35x35, 2 nm pixels, sigmoid resist alpha 50 "
-                        f"thr 0.225, L2 pattern error, dPE/dtheta",
-            "tile": N, "kernels": K, "kernel_support": [35, 35], "tiles_per_gpu": 1,
+def config_dict(N, K, precision, tiles=1):
+    what = "one" if tiles == 1 else f"a batch of {tiles}"
+    return {"workload": f"CTM objective evaluation (forward + adjoint) on {what} {N}^2 tile"
+                        f"{'' if tiles == 1 else 's'} per step, {K} SOCS kernels of 35x35, 2 nm "
+                        f"pixels, sigmoid resist alpha 50 thr 0.225, L2 pattern error, dPE/dtheta",
+            "tile": N, "kernels": K, "kernel_support": [35, 35], "tiles_per_gpu": tiles,
             "precision": precision, "theta_init": "0.3pi on target / 0.7pi off target",
             "l2": "flushed between timed steps (256 MiB write)", "parallelism": "tile-sharded"}
 
 
-def _measure(L, torch, ctx, stream, cache, target, th, flush, steps, warmup, dist):
-    """Times `steps` device-resident CTM evaluations (L2 flushed before each)."""
+def _measure(L, torch, ctx, stream, cache, target, th, flush, steps, warmup, dist, batch=None):
+    """Times `steps` device-resident CTM evaluations (L2 flushed before each). With
+    batch = (thetas, targets, grads) every step is one batched evaluation of all of
+    them (litho_ctm_evaluate_batch)."""
     with torch.cuda.stream(stream):
         opt = L.CTMOptimizer(cache, target, THRESHOLD, ALPHA, iterations=1)
+    step = (lambda: opt.evaluate(th)) if batch is None else (
+        lambda: L.ctm_evaluate_batch(cache, batch[0], batch[1], THRESHOLD, ALPHA, batch[2]))
     t_warm = time.perf_counter()
     nwarm = 0
     while nwarm < max(3, warmup) or time.perf_counter() - t_warm < 0.5:
-        opt.evaluate(th)
+        step()
         nwarm += 1
     launches0 = ctx.launch_count
     times = []
@@ -276,7 +284,7 @@ def _measure(L, torch, ctx, stream, cache, target, th, flush, steps, warmup, dis
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        opt.evaluate(th)
+        step()
         e1.record(stream)
         e1.synchronize()
         times.append(e0.elapsed_time(e1))
@@ -288,7 +296,7 @@ def _measure(L, torch, ctx, stream, cache, target, th, flush, steps, warmup, dis
     for _ in range(min(steps, 5)):
         with torch.cuda.stream(stream):
             flush.zero_()
-        opt.evaluate(th)
+        step()
     torch.cuda.synchronize()
     stages = ctx.stage_times()
     ctx.enable_stage_timing(False)
@@ -327,13 +335,32 @@ def run_ours(args):
         ctx.enable_graphs(not args.no_graphs)
         cache = L.ImagingCache.from_band(N, band, r0, c0, w, wss, ctx=ctx)
         r = _measure(L, torch, ctx, stream, cache, target, th, flush, args.steps, args.warmup, dist)
-        r.update(ctx=ctx, cache=cache)
+        r.update(ctx=ctx, cache=cache, tiles=1)
         runs[mode] = r
+    B = max(1, args.batch)
+    if modes[-1] == "bf16x3" and B > 1:
+        # The batched evaluation: B tiles per step (the first one is the tile above),
+        # each kernel of the chain covering all of them.
+        extra = [workload(N, K, seed=1 + world + rank * (B - 1) + b)[5:] for b in range(B - 1)]
+        with torch.cuda.stream(stream):
+            ths = torch.tensor(np.stack([theta] + [e[1] for e in extra]), dtype=torch.float32,
+                               device="cuda")
+            tgs = torch.tensor(np.stack([target] + [e[0] for e in extra]), dtype=torch.float32,
+                               device="cuda")
+            grs = torch.empty_like(ths)
+        torch.cuda.synchronize()
+        ctx = runs["bf16x3"]["ctx"]
+        cache = runs["bf16x3"]["cache"]
+        r = _measure(L, torch, ctx, stream, cache, target, th, flush, args.steps, args.warmup, dist,
+                     batch=(ths, tgs, grs))
+        r.update(ctx=ctx, cache=cache, tiles=B)
+        runs[f"bf16x3_batch{B}"] = r
     clk.__exit__(None, None, None)
-    head = modes[-1]          # the tensor-core path when both ran
+    head = list(runs)[-1]     # the batched tensor-core path when it ran
     R = runs[head]
     ctx, cache, opt = R["ctx"], R["cache"], R["opt"]
-    value = job_throughput(world, args.steps, R["total_ms"])
+    tiles = R["tiles"]
+    value = job_throughput(world, args.steps * tiles, R["total_ms"])
 
     # End to end through the host-buffer entry point (H2D + compute + D2H per step).
     h_theta = torch.tensor(theta, dtype=torch.float32).pin_memory()
@@ -372,25 +399,29 @@ def run_ours(args):
     # Roofline of the dominant full-resolution stage, live CUDA-event timing.
     hbm, src = peaks()
     stages = R["stages"]
-    sb = stage_bytes(N, cache.Nr, cache.Nc, head == "bf16x3")
+    sb = {k: v * tiles for k, v in stage_bytes(N, cache.Nr, cache.Nc, head != "fp32").items()}
     dom = max(sb, key=lambda s: stages[s][0] / max(stages[s][1], 1))
     avg_ms = stages[dom][0] / max(stages[dom][1], 1)
     achieved = sb[dom] / (avg_ms / 1e3) / 1e9
-    traffic = _ncu_traffic(dom, N, head)
+    traffic = _ncu_traffic(dom, N, "fp32" if head == "fp32" else "bf16x3")
+    if traffic is not None:
+        traffic *= tiles      # one launch covers every tile of the batch
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": max(3, args.warmup), "ms_per_step": R["total_ms"] / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "bf16x3" if head == "bf16x3" else "f32",
-        "data": "synthetic", "config": config_dict(N, K, head),
+        "dtype": "f32" if head == "fp32" else "bf16x3",
+        "data": "synthetic", "config": config_dict(N, K, head, tiles),
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm,
                      "peak_source": src, "unit": "GB/s", "frac": achieved / hbm,
                      "traffic": traffic, "algorithmic_bytes": sb[dom], "avg_launch_ms": avg_ms},
         "stages_ms_per_step": {k: v[0] / max(v[1], 1) for k, v in stages.items() if v[1]},
         "latency_ms": {"p50": float(np.percentile(R["times"], 50)),
                        "p99": float(np.percentile(R["times"], 99))},
-        "precision_modes": {m: {"value": job_throughput(world, args.steps, runs[m]["total_ms"]),
-                                "ms_per_step": runs[m]["total_ms"] / args.steps}
+        "precision_modes": {m: {"value": job_throughput(world, args.steps * runs[m]["tiles"],
+                                                        runs[m]["total_ms"]),
+                                "ms_per_step": runs[m]["total_ms"] / args.steps,
+                                "tiles_per_step": runs[m]["tiles"]}
                             for m in runs},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * 4 * N * N,
                 "d2h_bytes_per_step": 4 * N * N + 8 * 3},
@@ -405,13 +436,19 @@ def run_ours(args):
     out["roofline_evaluation"] = {
         "bound": "tensor", "kernel": "CTM evaluation (forward + adjoint, all kernels)",
         "achieved": achieved_tf, "peak": tb, "peak_sustained": ts_, "peak_source": tsrc,
-        "unit": "TFLOP/s", "frac": achieved_tf / tb, "algorithmic_flops_per_step": flops,
+        "unit": "TFLOP/s", "frac": achieved_tf / tb, "algorithmic_flops_per_tile": flops,
+        "algorithmic_flops_per_step": flops * tiles,
         "basis": "(16K+12) N^2 Nk + (16K+16) N Nk^2 per tile-iteration (per-kernel pruned "
                  "band DFTs); the band formulation here executes fewer FLOPs"}
-    out["config"]["launch"] = ("direct kernel launches (PDL)" if args.no_graphs else
-                               "CUDA graph replay of the evaluation chain (PDL edges)")
+    out["config"]["launch"] = (
+        "direct kernel launches (PDL), each kernel covering the whole batch" if tiles > 1 else
+        "direct kernel launches (PDL)" if args.no_graphs else
+        "CUDA graph replay of the evaluation chain (PDL edges)")
     if "fp32" in runs and "bf16x3" in runs:
-        out["precision_modes"]["bf16x3_over_fp32"] = runs["fp32"]["total_ms"] / runs["bf16x3"]["total_ms"]
+        pm = out["precision_modes"]
+        pm["bf16x3_over_fp32"] = pm["bf16x3"]["value"] / pm["fp32"]["value"]
+        if head not in ("fp32", "bf16x3"):
+            pm["batched_over_fp32"] = pm[head]["value"] / pm["fp32"]["value"]
     if world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(N, K, band, r0, c0, w, wss, target, theta,
                                            args.cpu_seconds)

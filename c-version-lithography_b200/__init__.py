@@ -104,6 +104,7 @@ SIGNATURES = {
     "litho_pe_loss": (_I, [_P, _P, _P, _I, _I, ctypes.POINTER(PeOptions), _PD]),
     "litho_ctm_evaluate": (_I, [_P, _P, _P, _P, _P, _D, _D, _P, _P, _P, _P, _P, _PD, _PD]),
     "litho_ctm_evaluate_host": (_I, [_P, _P, _P, _P, _P, _D, _D, _P, _PD, _PD]),
+    "litho_ctm_evaluate_batch": (_I, [_P, _P, _I, _P, _P, _D, _D, _P, _PD, _PD]),
     "litho_weno_godunov": (_I, [_P, _I, _I, _P, _P, _D, _D, _P, _P]),
     "litho_kappa": (_I, [_P, _I, _I, _P, _D, _D, _D, _P]),
     "litho_evolution_term": (_I, [_P, _I, _I, _P, _P, _D, _D, _D, _D, _P, _PD]),
@@ -590,6 +591,34 @@ class LevelSetUtils:
                                                 float(dx), float(dy), float(cfl), float(b),
                                                 _ptr(out), _ptr(mask), ctypes.byref(dt)))
         return out, mask, dt.value
+
+
+def ctm_evaluate_batch(cache: "ImagingCache", thetas, targets, threshold: float, alpha: float,
+                       grads=None):
+    """The CTM objective of CTM_Optimizer::_evaluate_theta_objective
+    (CTM_Optimizer.cpp:175-187) for a batch of images in one pass of the kernel chain.
+
+    thetas, targets: (batch, N, N) float32 CUDA tensors. Returns (losses, grads, norms):
+    per-image PE and ||dPE/dtheta||_2 (lists of floats) and dPE/dtheta (batch, N, N),
+    written into `grads` when given. Each image's results equal its own single-image
+    evaluation."""
+    ctx = cache.ctx
+    torch = ctx.torch
+    N = cache.N
+    th = _f32(thetas, torch)
+    if th.dim() != 3 or th.shape[1:] != (N, N):
+        raise LithoError(2, f"thetas must be (batch, {N}, {N})")
+    B = th.shape[0]
+    tg = _f32(targets, torch, (B, N, N), "targets")
+    out = grads if grads is not None else torch.empty_like(th)
+    if out.shape != th.shape or out.dtype != torch.float32 or not out.is_contiguous():
+        raise LithoError(2, "grads must be a contiguous float32 tensor shaped like thetas")
+    losses = (ctypes.c_double * B)()
+    norms = (ctypes.c_double * B)()
+    ctx._check(ctx.lib.litho_ctm_evaluate_batch(ctx.handle, cache.handle, B, _ptr(th), _ptr(tg),
+                                                float(threshold), float(alpha), _ptr(out),
+                                                losses, norms))
+    return list(losses), out, list(norms)
 
 
 class CTMOptimizer:

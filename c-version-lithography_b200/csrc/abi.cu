@@ -58,12 +58,16 @@ void free_cache(Cache* c) {
 
 // Scratch layout of one imaging + adjoint evaluation.
 struct Layout {
-  size_t part, gh, ik, iP, chat, X, Ut, Vt, dldi, gam, Zk, rows_tmp, img, total;
+  size_t part, gh, ik, iP, chat, X, Ut, Vt, dldi, gam, Zk, rows_tmp, img, fm, fe, total;
   int tiles;
 };
 
-Layout make_layout(const BandGeom& g) {
+// batch > 1 (the batched CTM evaluation): every per-image buffer repeated batch times
+// back to back, plus the band state of the batch (fm: m on the band, fe: the K
+// small-grid fields per image).
+Layout make_layout(const BandGeom& g, int batch = 1) {
   Layout L{};
+  const size_t B = (size_t)batch;
   const int N = g.N;
   L.tiles = analysis_tiles(N);
   size_t off = 0;
@@ -72,19 +76,21 @@ Layout make_layout(const BandGeom& g) {
     off = align_up(off + bytes, 256);
     return o;
   };
-  L.part = take((size_t)L.tiles * (2 * g.Nr - 1) * g.Nc * sizeof(float2));
-  L.gh = take((size_t)(2 * g.Nr - 1) * g.Nc * sizeof(float2));
-  L.ik = take((size_t)g.K * g.Pr * g.Pc * sizeof(float));
-  L.iP = take((size_t)g.Pr * g.Pc * sizeof(float));
-  L.Ut = take((size_t)N * g.kp_rows * sizeof(float));
-  L.Vt = take((size_t)N * g.kp_rows * sizeof(float));
+  L.part = take(B * L.tiles * (2 * g.Nr - 1) * g.Nc * sizeof(float2));
+  L.gh = take(B * (2 * g.Nr - 1) * g.Nc * sizeof(float2));
+  L.ik = take(B * g.K * g.Pr * g.Pc * sizeof(float));
+  L.iP = take(B * g.Pr * g.Pc * sizeof(float));
+  L.Ut = take(B * N * g.kp_rows * sizeof(float));
+  L.Vt = take(B * N * g.kp_rows * sizeof(float));
   L.dldi = take((size_t)N * N * sizeof(float));
-  L.gam = take((size_t)g.Pr * g.Pc * sizeof(float));
-  L.Zk = take((size_t)g.K * g.Nr * g.Nc * sizeof(float2));
-  L.chat = take((size_t)g.Nr * (2 * g.Nc - 1) * sizeof(float2));
-  L.X = take((size_t)g.Nr * g.Nc * sizeof(float2));
+  L.gam = take(B * g.Pr * g.Pc * sizeof(float));
+  L.Zk = take(B * g.K * g.Nr * g.Nc * sizeof(float2));
+  L.chat = take(B * g.Nr * (2 * g.Nc - 1) * sizeof(float2));
+  L.X = take(B * g.Nr * g.Nc * sizeof(float2));
   L.rows_tmp = take((size_t)g.Nr * N * sizeof(float2));
-  L.img = take(tc2_supported(g) ? tc2_rows_image_bytes(N, g.kp_rows) : 16);  // band operand image
+  L.img = take(B * (tc2_supported(g) ? tc2_rows_image_bytes(N, g.kp_rows) : 16));  // band operand images
+  L.fm = batch > 1 ? take(B * g.Nr * g.Nc * sizeof(float2)) : 0;
+  L.fe = batch > 1 ? take(B * g.K * g.Pr * g.Pc * sizeof(float2)) : 0;
   L.total = off;
   return L;
 }
@@ -565,7 +571,8 @@ int check_launch(Context* ctx, cudaError_t e, const char* what) {
 // with analysed set; dL/dI is then not stored.
 int run_forward(Context* ctx, const Cache& c, Field& f, const Layout& L, int input_mode,
                 const float* input, float* mask_out, ResistEpilogue ep, int* nblocks,
-                cudaEvent_t before_synthesis = nullptr, bool fuse_adjoint = false) {
+                cudaEvent_t before_synthesis = nullptr, bool fuse_adjoint = false,
+                int batch = 1) {
   const BandGeom& g = c.g;
   cudaStream_t s = ctx->stream;
   int* flag = reinterpret_cast<int*>(ctx->d_red + RED_FLAG);
@@ -575,7 +582,7 @@ int run_forward(Context* ctx, const Cache& c, Field& f, const Layout& L, int inp
   if (tc)
     st = check_launch(ctx, launch_analysis_tc2(s, input_mode, input, mask_out, flag, g.N, g.Nc,
                                                g.Nr, g.Nr, 0, at<float2>(ctx, L.part), c.TXS_img,
-                                               c.TYS_img, flag + 1),
+                                               c.TYS_img, flag + 1, batch),
                       "tensor-core tile analysis");
   else
     st = check_launch(ctx, launch_analysis(s, input_mode, input, mask_out, flag, c.TXS, g.N, g.Nc,
@@ -585,14 +592,14 @@ int run_forward(Context* ctx, const Cache& c, Field& f, const Layout& L, int inp
   if (st) return st;
   ctx->stage_begin(1);
   st = check_launch(ctx, launch_reduce_tiles(s, at<float2>(ctx, L.part), L.tiles, g.Nr * g.Nc,
-                                             1.f / ((float)g.N * g.N), f.mband),
+                                             1.f / ((float)g.N * g.N), f.mband, batch),
                     "tile reduction");
   ctx->stage_end(1);
   if (st) return st;
   ctx->stage_begin(2);
   st = check_launch(ctx, launch_band_forward(s, c, f, at<float>(ctx, L.ik), at<float>(ctx, L.iP),
                                              at<float2>(ctx, L.chat), at<float>(ctx, L.Ut),
-                                             tc ? at<void>(ctx, L.img) : nullptr),
+                                             tc ? at<void>(ctx, L.img) : nullptr, batch),
                     "band forward");
   ctx->stage_end(2);
   if (st) return st;
@@ -605,11 +612,11 @@ int run_forward(Context* ctx, const Cache& c, Field& f, const Layout& L, int inp
       st = check_launch(ctx, launch_synth_resist_analysis_tc2(
                                  s, c.AYD_img, at<void>(ctx, L.img), g.N, g.kp_rows, ep, g.Nc,
                                  g.Nr, at<float2>(ctx, L.part), flag, c.TXD_img, c.TYD_img, err,
-                                 nblocks),
+                                 nblocks, batch),
                         "tensor-core row synthesis with adjoint tile analysis");
     else
       st = check_launch(ctx, launch_synth_resist_tc2(s, c.AYD_img, at<void>(ctx, L.img), g.N,
-                                                     g.kp_rows, ep, err, nblocks),
+                                                     g.kp_rows, ep, err, nblocks, batch),
                         "tensor-core row synthesis");
   } else {
     st = check_launch(ctx, launch_synth_resist(s, c.AYD, at<float>(ctx, L.Ut), g.N, g.kp_rows, ep,
@@ -617,13 +624,14 @@ int run_forward(Context* ctx, const Cache& c, Field& f, const Layout& L, int inp
                       "row synthesis");
   }
   ctx->stage_end(3);
-  ctx->launches += 3 + band_forward_launches(g);   // analysis, reduction, band, synthesis
+  ctx->launches += 7;  // analysis, reduction, fields, sum over k, chat, expansion, synthesis
   f.valid = (st == LITHO_OK);
   return st;
 }
 
 int run_adjoint(Context* ctx, const Cache& c, const Field& f, const Layout& L, const float* dldi,
-                double scale, GradEpilogue ep, int* nblocks, bool analysed = false) {
+                double scale, GradEpilogue ep, int* nblocks, bool analysed = false,
+                int batch = 1) {
   const BandGeom& g = c.g;
   cudaStream_t s = ctx->stream;
   int* flag = reinterpret_cast<int*>(ctx->d_red + RED_FLAG);
@@ -646,7 +654,7 @@ int run_adjoint(Context* ctx, const Cache& c, const Field& f, const Layout& L, c
   if (st) return st;
   ctx->stage_begin(5);
   st = check_launch(ctx, launch_reduce_tiles(s, at<float2>(ctx, L.part), L.tiles, na * g.Nc,
-                                             1.f / ((float)g.N * g.N), at<float2>(ctx, L.gh)),
+                                             1.f / ((float)g.N * g.N), at<float2>(ctx, L.gh), batch),
                     "adjoint tile reduction");
   ctx->stage_end(5);
   if (st) return st;
@@ -654,7 +662,7 @@ int run_adjoint(Context* ctx, const Cache& c, const Field& f, const Layout& L, c
   st = check_launch(ctx, launch_band_adjoint(s, c, f, at<float2>(ctx, L.gh), scale,
                                              at<float>(ctx, L.gam), at<float2>(ctx, L.Zk),
                                              at<float2>(ctx, L.X), at<float>(ctx, L.Vt),
-                                             tc ? at<void>(ctx, L.img) : nullptr),
+                                             tc ? at<void>(ctx, L.img) : nullptr, batch),
                     "band adjoint");
   ctx->stage_end(6);
   if (st) return st;
@@ -662,7 +670,7 @@ int run_adjoint(Context* ctx, const Cache& c, const Field& f, const Layout& L, c
   if (tc) {
     int* err = reinterpret_cast<int*>(ctx->d_red + RED_FLAG) + 1;
     st = check_launch(ctx, launch_synth_grad_tc2(s, c.AYS_img, at<void>(ctx, L.img), g.N,
-                                                 g.kp_rows, ep, err, nblocks),
+                                                 g.kp_rows, ep, err, nblocks, batch),
                       "tensor-core adjoint row synthesis");
   } else {
     st = check_launch(ctx, launch_synth_grad(s, c.AYS, at<float>(ctx, L.Vt), g.N, g.kp_rows, ep,
@@ -674,13 +682,13 @@ int run_adjoint(Context* ctx, const Cache& c, const Field& f, const Layout& L, c
   return st;
 }
 
-int prepare(Context* ctx, const Cache& c, Layout* L) {
+int prepare(Context* ctx, const Cache& c, Layout* L, int batch = 1) {
   if (cudaSetDevice(ctx->device) != cudaSuccess) return ctx->fail(LITHO_ERR_CUDA, "cudaSetDevice");
-  *L = make_layout(c.g);
+  *L = make_layout(c.g, batch);
   int st = ctx->ensure_scratch(L->total);
   if (st) return st;
   const int blocks = ((c.g.N + 127) / 128) * ((c.g.N + 127) / 128);
-  st = ctx->ensure_red(RED_PART + 3 * (size_t)blocks + 1200);
+  st = ctx->ensure_red(RED_PART + (3 * (size_t)blocks + 3) * batch + 1200);
   if (st) return st;
   LITHO_CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_red, 0, RED_PART * sizeof(double), ctx->stream));
   return LITHO_OK;
@@ -973,6 +981,72 @@ int litho_ctm_evaluate(litho_ctx* ctx, const litho_cache* cache, litho_field* fi
   return ctm_evaluate_impl(ctx, cache, field, d_theta, d_target, threshold, alpha, d_mask,
                            d_aerial, d_wafer, d_grad_mask, d_grad_theta, loss, grad_norm,
                            nullptr);
+}
+
+int litho_ctm_evaluate_batch(litho_ctx* ctx, const litho_cache* cache, int batch,
+                             const float* d_theta, const float* d_target, double threshold,
+                             double alpha, float* d_grad_theta, double* losses, double* norms) {
+  if (!ctx || !cache || batch < 1 || !d_theta || !d_target || !d_grad_theta)
+    return LITHO_ERR_INVALID_ARGUMENT;
+  if (!std::isfinite(threshold) || !std::isfinite(alpha))
+    return ctx->fail(LITHO_ERR_NONFINITE, "Imaging: mask, threshold, and alpha must be finite");
+  const BandGeom& g = cache->g;
+  const size_t px = (size_t)g.N * g.N;
+  const bool tc = ctx->precision == LITHO_PRECISION_BF16X3 && cache->TXD_img != nullptr;
+  if (!tc || batch == 1) {
+    // One image after another (FP32 parity mode, or a single image).
+    for (int b = 0; b < batch; ++b) {
+      double lo = 0.0, no = 0.0;
+      const int st = ctm_evaluate_impl(ctx, cache, nullptr, d_theta + b * px, d_target + b * px,
+                                       threshold, alpha, nullptr, nullptr, nullptr, nullptr,
+                                       d_grad_theta + b * px, &lo, &no, nullptr);
+      if (st) return st;
+      if (losses) losses[b] = lo;
+      if (norms) norms[b] = no;
+    }
+    return LITHO_OK;
+  }
+  Layout L;
+  int st = prepare(ctx, *cache, &L, batch);
+  if (st) return st;
+  Field f;
+  f.cache = cache;
+  f.e = at<float2>(ctx, L.fe);
+  f.mband = at<float2>(ctx, L.fm);
+  ResistEpilogue ep{};
+  ep.mode = 1;
+  ep.thr = (float)threshold;
+  ep.alpha = (float)alpha;
+  ep.target = d_target;
+  ep.pe_weight = 1.f;
+  ep.penalty = 0.f;
+  ep.pen_thr = 0.01f;
+  ep.loss_partial = ctx->d_red + RED_PART;
+  int nb = 0, nb2 = 0;
+  st = run_forward(ctx, *cache, f, L, 1, d_theta, nullptr, ep, &nb, nullptr, true, batch);
+  GradEpilogue gp{};
+  gp.theta = d_theta;
+  gp.grad_theta = d_grad_theta;
+  gp.norm_partial = ctx->d_red + RED_PART + 2 * (size_t)nb * batch;
+  if (!st) st = run_adjoint(ctx, *cache, f, L, nullptr, 4.0 * alpha, gp, &nb2, true, batch);
+  double* d_sums = gp.norm_partial + (size_t)nb2 * batch;
+  if (!st)
+    st = check_launch(ctx, launch_sum_partials_batch(ctx->stream, ctx->d_red + RED_PART, nb, 2,
+                                                     gp.norm_partial, nb2, 1, d_sums, batch),
+                      "sum");
+  ctx->launches += 1;
+  std::vector<double> sums(3 * (size_t)batch);
+  if (!st)
+    LITHO_CUDA_TRY(ctx, cudaMemcpyAsync(sums.data(), d_sums, sums.size() * sizeof(double),
+                                        cudaMemcpyDeviceToHost, ctx->stream));
+  if (!st) st = fetch(ctx, 0);
+  if (st) return st;
+  if (flag_set(ctx)) return ctx->fail(LITHO_ERR_NONFINITE, "theta must be finite");
+  for (int b = 0; b < batch; ++b) {
+    if (losses) losses[b] = sums[3 * (size_t)b];
+    if (norms) norms[b] = std::sqrt(sums[3 * (size_t)b + 2]);
+  }
+  return LITHO_OK;
 }
 
 // Host buffers: theta goes up first on the context's stream; the target follows on

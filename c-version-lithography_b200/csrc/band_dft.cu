@@ -261,6 +261,8 @@ reduce_tiles_kernel(const float2* __restrict__ part, int tiles, int count, float
                     float2* __restrict__ out) {
   pdl_trigger();
   pdl_wait();
+  part += (size_t)blockIdx.y * tiles * count;   // image b of a batch: [b][tile][entry]
+  out += (size_t)blockIdx.y * count;
   __shared__ float2 sh[RT_G][RT_E];
   const int e = threadIdx.x % RT_E, g = threadIdx.x / RT_E;
   const int o = blockIdx.x * RT_E + e;
@@ -287,9 +289,9 @@ reduce_tiles_kernel(const float2* __restrict__ part, int tiles, int count, float
 }
 
 cudaError_t launch_reduce_tiles(cudaStream_t s, const float2* part, int tiles, int count,
-                                float scale, float2* out) {
-  return launch_pdl(reduce_tiles_kernel, dim3((count + RT_E - 1) / RT_E), dim3(RT_E * RT_G), 0, s,
-                    part, tiles, count, scale, out);
+                                float scale, float2* out, int batch) {
+  return launch_pdl(reduce_tiles_kernel, dim3((count + RT_E - 1) / RT_E, batch),
+                    dim3(RT_E * RT_G), 0, s, part, tiles, count, scale, out);
 }
 
 // ---------------------------------------------------------------- row synthesis
@@ -429,6 +431,12 @@ band_fields_kernel(const float2* __restrict__ H, const float2* __restrict__ mban
   extern __shared__ float2 sm2[];
   const int k = blockIdx.x;
   const int j0 = blockIdx.y * BF_CW;
+  {  // image b of a batch
+    const size_t b = blockIdx.z;
+    mband += b * Nr * Nc;
+    e += b * gridDim.x * Pr * Pc;
+    ik += b * gridDim.x * Pr * Pc;
+  }
   const int cw = min(BF_CW, Pc - j0);
   float2* A = sm2;                  // [Nr][Nc]
   float2* T = A + Nr * Nc;          // [Nr][BF_CW]
@@ -487,6 +495,8 @@ size_t band_fields_smem(const BandGeom& g) {
 __global__ void sum_k_kernel(const float* __restrict__ ik, int K, int n, float* __restrict__ iP) {
   pdl_trigger();
   pdl_wait();
+  ik += (size_t)blockIdx.y * K * n;   // image b of a batch
+  iP += (size_t)blockIdx.y * n;
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= n) return;
   float s = 0.f;
@@ -510,6 +520,8 @@ band_chat_kernel(const float* __restrict__ iP, int Nr, int Nc, int Pr, int Pc,
   float2* edc = ed + Pr;                             // [Pc][nd]
   float* ip = reinterpret_cast<float*>(edc + Pc * nd);  // [Pr][Pc]
   const int dr = blockIdx.x;
+  iP += (size_t)blockIdx.y * Pr * Pc;   // image b of a batch
+  chat += (size_t)blockIdx.y * Nr * nd;
   pdl_trigger();
   fill_batched<BI_NT>(ed, Pr, [&](int jr) { return EDr_t[(size_t)(dr + Nr - 1) * Pr + jr]; });
   fill_batched<BI_NT>(edc, Pc * nd, [&](int i) { return EDc[i]; });
@@ -622,6 +634,12 @@ expand_kernel(const float2* __restrict__ coef, int nrows, int ncoef, int ld,
   float2* cf = se;                    // [EX_R][ncoef]
   float2* ph = se + EX_R * ncoef;     // [ncoef][EX_X]
   const int x0 = blockIdx.x * EX_X, a0 = blockIdx.y * EX_R;
+  {  // image b of a batch
+    const size_t b = blockIdx.z;
+    coef += b * nrows * ld;
+    if (img) img += b * ((N + 127) / 128) * (size_t)img_tile_bytes;
+    else Ut += b * N * kp;
+  }
   pdl_trigger();
   fill_batched<EX_NT>(ph, ncoef * EX_X, [&](int i) {
     const int c = i / EX_X, xx = i % EX_X, x = x0 + xx;
@@ -645,102 +663,22 @@ expand_kernel(const float2* __restrict__ coef, int nrows, int ncoef, int ld,
   expand_store(cf, ph, nrows, ncoef, N, mode, kp, a0, x0, Ut, img, img_tile_bytes);
 }
 
-// Forward 3 + 4 in one launch: the CTA's rows of chat (band_chat_kernel's arithmetic
-// for rows a0 .. a0 + EX_R - 1) straight from the small-grid intensity, then the
-// mode-1 expansion of expand_kernel. Every x strip of a row group recomputes the
-// same rows (about 0.2 MFLOP), which is cheaper than a launch between them.
-__global__ void __launch_bounds__(EX_NT)
-expand_intensity_kernel(const float* __restrict__ iP, int Nr, int Nc, int Pr, int Pc,
-                        const float2* __restrict__ EDr_t, const float2* __restrict__ EDc,
-                        float inv, const float2* __restrict__ TX, int N, int kp,
-                        float* __restrict__ Ut, uint8_t* __restrict__ img,
-                        uint32_t img_tile_bytes) {
-  extern __shared__ float2 se[];
-  const int nd = 2 * Nc - 1;
-  float2* cf = se;                      // [EX_R][nd]
-  float2* ph = cf + EX_R * nd;          // [nd][EX_X]
-  float2* edr = ph + nd * EX_X;         // [EX_R][Pr]
-  float2* edc = edr + EX_R * Pr;        // [Pc][nd]
-  float2* v = edc + Pc * nd;            // [EX_R][Pc]
-  float* ip = reinterpret_cast<float*>(v + EX_R * Pc);   // [Pr][Pc]
-  const int x0 = blockIdx.x * EX_X, a0 = blockIdx.y * EX_R;
-  pdl_trigger();
-  fill_batched<EX_NT>(ph, nd * EX_X, [&](int i) {
-    const int c = i / EX_X, x = x0 + i % EX_X;
-    const int d = c - (Nc - 1);
-    float2 t = make_float2(0.f, 0.f);
-    if (x < N) t = d >= 0 ? conjf2(TX[(size_t)d * N + x]) : TX[(size_t)(-d) * N + x];
-    return t;
-  });
-  fill_batched<EX_NT>(edr, EX_R * Pr, [&](int i) {
-    const int r = i / Pr, jr = i % Pr;
-    return a0 + r < Nr ? EDr_t[(size_t)(a0 + r + Nr - 1) * Pr + jr] : make_float2(0.f, 0.f);
-  });
-  fill_batched<EX_NT>(edc, Pc * nd, [&](int i) { return EDc[i]; });
-  pdl_wait();
-  fill_batched<EX_NT>(ip, Pr * Pc, [&](int i) { return iP[i]; });
-  __syncthreads();
-  for (int i = threadIdx.x; i < EX_R * Pc; i += EX_NT) {
-    const int r = i / Pc, jc = i % Pc;
-    const float2* ed = edr + r * Pr;
-    float2 a = make_float2(0.f, 0.f), b = a;
-    int jr = 0;
-    for (; jr + 1 < Pr; jr += 2) {
-      const float i0 = ip[jr * Pc + jc], i1 = ip[(jr + 1) * Pc + jc];
-      a.x = fmaf(ed[jr].x, i0, a.x); a.y = fmaf(-ed[jr].y, i0, a.y);
-      b.x = fmaf(ed[jr + 1].x, i1, b.x); b.y = fmaf(-ed[jr + 1].y, i1, b.y);
-    }
-    if (jr < Pr) {
-      const float i0 = ip[jr * Pc + jc];
-      a.x = fmaf(ed[jr].x, i0, a.x); a.y = fmaf(-ed[jr].y, i0, a.y);
-    }
-    v[i] = make_float2(a.x + b.x, a.y + b.y);
-  }
-  __syncthreads();
-  for (int i = threadIdx.x; i < EX_R * nd; i += EX_NT) {
-    const int r = i / nd, dc = i % nd;
-    const float2* vr = v + r * Pc;
-    float2 a = make_float2(0.f, 0.f), b = a;
-    int jc = 0;
-    for (; jc + 1 < Pc; jc += 2) {
-      cfma(a, vr[jc], conjf2(edc[jc * nd + dc]));
-      cfma(b, vr[jc + 1], conjf2(edc[(jc + 1) * nd + dc]));
-    }
-    if (jc < Pc) cfma(a, vr[jc], conjf2(edc[jc * nd + dc]));
-    cf[i] = make_float2((a.x + b.x) * inv, (a.y + b.y) * inv);
-  }
-  __syncthreads();
-  expand_store(cf, ph, Nr, nd, N, 1, kp, a0, x0, Ut, img, img_tile_bytes);
-}
-
-static size_t expand_intensity_smem(const BandGeom& g) {
-  const int nd = 2 * g.Nc - 1;
-  return (size_t)(EX_R * nd + nd * EX_X + EX_R * g.Pr + g.Pc * nd + EX_R * g.Pc) * sizeof(float2) +
-         (size_t)g.Pr * g.Pc * sizeof(float);
-}
-// Up to this much shared memory two CTAs of the merged kernel share an SM.
-constexpr size_t EXPAND_INTENSITY_MAX_SMEM = 112 * 1024;
-
-int band_forward_launches(const BandGeom& g) {
-  return expand_intensity_smem(g) <= EXPAND_INTENSITY_MAX_SMEM ? 3 : 4;
-}
-
 static cudaError_t launch_expand(cudaStream_t s, const float2* coef, int nrows, int ncoef, int ld,
                                  const float2* TX, int N, int mode, int nc, int kp, float* Ut,
-                                 void* img) {
+                                 void* img, int batch) {
   // Split-BF16 image tile: 128 rows x [hi | lo] of kp columns, in 64-column atoms.
   const uint32_t img_tile_bytes = (uint32_t)((2 * kp + 63) / 64) * 128u * 128u;
   const size_t smem = (size_t)(EX_R * ncoef + ncoef * EX_X) * sizeof(float2);
   cudaError_t e = cudaFuncSetAttribute(expand_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
   if (e != cudaSuccess) return e;
-  dim3 grid((N + EX_X - 1) / EX_X, (nrows + EX_R - 1) / EX_R);
+  dim3 grid((N + EX_X - 1) / EX_X, (nrows + EX_R - 1) / EX_R, batch);
   return launch_pdl(expand_kernel, grid, dim3(EX_NT), smem, s, coef, nrows, ncoef, ld, TX, N, mode,
                     nc, kp, Ut, static_cast<uint8_t*>(img), img_tile_bytes);
 }
 
 cudaError_t launch_band_forward(cudaStream_t s, const Cache& c, Field& f, float* ik, float* iP,
-                                float2* chat, float* Ut, void* img) {
+                                float2* chat, float* Ut, void* img, int batch) {
   const BandGeom& g = c.g;
   const size_t full = fields_smem_full(g);
   const int stage = full <= SMEM_STAGE;
@@ -748,36 +686,24 @@ cudaError_t launch_band_forward(cudaStream_t s, const Cache& c, Field& f, float*
   cudaError_t err = cudaFuncSetAttribute(band_fields_kernel,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1);
   if (err != cudaSuccess) return err;
-  err = launch_pdl(band_fields_kernel, dim3(g.K, (g.Pc + BF_CW - 1) / BF_CW), dim3(BF_NT), sm1, s,
+  err = launch_pdl(band_fields_kernel, dim3(g.K, (g.Pc + BF_CW - 1) / BF_CW, batch), dim3(BF_NT), sm1, s,
                    c.H, static_cast<const float2*>(f.mband), c.w, g.Nr, g.Nc, g.Pr, g.Pc, c.ESc_t,
                    c.ESr_t, stage, f.e, ik);
   if (err != cudaSuccess) return err;
   const int n = g.Pr * g.Pc;
-  err = launch_pdl(sum_k_kernel, dim3((n + 255) / 256), dim3(256), 0, s,
+  err = launch_pdl(sum_k_kernel, dim3((n + 255) / 256, batch), dim3(256), 0, s,
                    static_cast<const float*>(ik), g.K, n, iP);
   if (err != cudaSuccess) return err;
   const int nd = 2 * g.Nc - 1;
-  const size_t smx = expand_intensity_smem(g);
-  if (smx <= EXPAND_INTENSITY_MAX_SMEM) {
-    err = cudaFuncSetAttribute(expand_intensity_kernel,
-                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx);
-    if (err != cudaSuccess) return err;
-    const uint32_t img_tile_bytes = (uint32_t)((2 * g.kp_rows + 63) / 64) * 128u * 128u;
-    dim3 grid((g.N + EX_X - 1) / EX_X, (g.Nr + EX_R - 1) / EX_R);
-    return launch_pdl(expand_intensity_kernel, grid, dim3(EX_NT), smx, s,
-                      static_cast<const float*>(iP), g.Nr, g.Nc, g.Pr, g.Pc, c.EDr_t, c.EDc,
-                      1.f / ((float)g.Pr * (float)g.Pc), c.TXDc, g.N, g.kp_rows, Ut,
-                      static_cast<uint8_t*>(img), img_tile_bytes);
-  }
   const size_t smc = chat_smem(g);
   err = cudaFuncSetAttribute(band_chat_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)smc);
   if (err != cudaSuccess) return err;
-  err = launch_pdl(band_chat_kernel, dim3(g.Nr), dim3(BI_NT), smc, s,
+  err = launch_pdl(band_chat_kernel, dim3(g.Nr, batch), dim3(BI_NT), smc, s,
                    static_cast<const float*>(iP), g.Nr, g.Nc, g.Pr, g.Pc, c.EDr_t, c.EDc,
                    1.f / ((float)g.Pr * (float)g.Pc), chat);
   if (err != cudaSuccess) return err;
-  return launch_expand(s, chat, g.Nr, nd, nd, c.TXDc, g.N, 1, g.Nc, g.kp_rows, Ut, img);
+  return launch_expand(s, chat, g.Nr, nd, nd, c.TXDc, g.N, 1, g.Nc, g.kp_rows, Ut, img, batch);
 }
 
 // Adjoint 1 (one CTA per small-grid row jr):
@@ -790,6 +716,8 @@ band_gamma_kernel(const float2* __restrict__ gh, int Nr, int Nc, int Pr, int Pc,
   extern __shared__ float2 sg[];
   const int jr = blockIdx.x;
   const int na = 2 * Nr - 1;
+  gh += (size_t)blockIdx.y * na * Nc;   // image b of a batch
+  gam += (size_t)blockIdx.y * Pr * Pc;
   float2* wv = sg;               // [Nc]
   float2* edr = wv + Nc;         // [na]   column jr of EDr_t
   float2* ghs = edr + na;        // [na][Nc]
@@ -844,6 +772,12 @@ band_z_kernel(const float2* __restrict__ e, const float* __restrict__ gam, int N
   const int k = blockIdx.x;
   const int u0 = blockIdx.y * BZ_UW;
   const int uw = min(BZ_UW, Nc - u0);
+  {  // image b of a batch
+    const size_t b = blockIdx.z;
+    e += b * gridDim.x * Pr * Pc;
+    gam += b * Pr * Pc;
+    Zk += b * gridDim.x * Nr * Nc;
+  }
   float2* Z1 = sz;                  // [Pr][BZ_UW]
   float2* esc = Z1 + Pr * BZ_UW;    // [Pc][BZ_UW]
   float2* q = esc + Pc * BZ_UW;     // [Pr][Pc]   (staged)
@@ -907,6 +841,8 @@ __global__ void band_x_kernel(const float2* __restrict__ Zk, const float2* __res
                               float2* __restrict__ X) {
   pdl_trigger();
   pdl_wait();
+  Zk += (size_t)blockIdx.y * K * nb;   // image b of a batch
+  X += (size_t)blockIdx.y * nb;
   const int u = blockIdx.x * blockDim.x + threadIdx.x;
   if (u >= nb) return;
   float2 acc = make_float2(0.f, 0.f);
@@ -931,13 +867,13 @@ __global__ void band_x_kernel(const float2* __restrict__ Zk, const float2* __res
 
 cudaError_t launch_band_adjoint(cudaStream_t s, const Cache& c, const Field& f, const float2* gh,
                                 double scale, float* gam, float2* Zk, float2* X, float* Vt,
-                                void* img) {
+                                void* img, int batch) {
   const BandGeom& g = c.g;
   const size_t smg = gamma_smem(g);
   cudaError_t e0 = cudaFuncSetAttribute(band_gamma_kernel,
                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smg);
   if (e0 != cudaSuccess) return e0;
-  e0 = launch_pdl(band_gamma_kernel, dim3(g.Pr), dim3(256), smg, s, gh, g.Nr, g.Nc, g.Pr, g.Pc,
+  e0 = launch_pdl(band_gamma_kernel, dim3(g.Pr, batch), dim3(256), smg, s, gh, g.Nr, g.Nc, g.Pr, g.Pc,
                   c.EDr_t, c.EDc_t, gam);
   if (e0 != cudaSuccess) return e0;
   const size_t base = (size_t)(g.Pr * BZ_UW + g.Pc * BZ_UW) * sizeof(float2);
@@ -947,15 +883,15 @@ cudaError_t launch_band_adjoint(cudaStream_t s, const Cache& c, const Field& f, 
   cudaError_t err = cudaFuncSetAttribute(band_z_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smz);
   if (err != cudaSuccess) return err;
-  err = launch_pdl(band_z_kernel, dim3(g.K, (g.Nc + BZ_UW - 1) / BZ_UW), dim3(BF_NT), smz, s,
+  err = launch_pdl(band_z_kernel, dim3(g.K, (g.Nc + BZ_UW - 1) / BZ_UW, batch), dim3(BF_NT), smz, s,
                    static_cast<const float2*>(f.e), static_cast<const float*>(gam), g.Nr, g.Nc,
                    g.Pr, g.Pc, c.ESc, c.ESr_t, stage, 1.f / ((float)g.Pr * (float)g.Pc), Zk);
   if (err != cudaSuccess) return err;
   const int nb = g.Nr * g.Nc;
-  err = launch_pdl(band_x_kernel, dim3((nb + 127) / 128), dim3(128), 0, s,
+  err = launch_pdl(band_x_kernel, dim3((nb + 127) / 128, batch), dim3(128), 0, s,
                    static_cast<const float2*>(Zk), c.H, c.w, g.K, nb, (float)scale, X);
   if (err != cudaSuccess) return err;
-  return launch_expand(s, X, g.Nr, g.Nc, g.Nc, c.TXSc, g.N, 0, g.Nc, g.kp_rows, Vt, img);
+  return launch_expand(s, X, g.Nr, g.Nc, g.Nc, c.TXSc, g.N, 0, g.Nc, g.kp_rows, Vt, img, batch);
 }
 
 // ---------------------------------------------------------------- FP64 partial sums
@@ -998,6 +934,31 @@ cudaError_t launch_sum_partials2(cudaStream_t s, const double* a, int na, int sa
                                  const double* b, int nb, int sb, double* out_b) {
   return launch_pdl(sum_partials2_kernel, dim3(sa + sb), dim3(32), 0, s, a, na, sa, out_a, b, nb,
                     sb, out_b);
+}
+
+// Per image b of a batch: out[b][0..sa) from a + b na sa (sa components over na
+// blocks) and out[b][sa..sa+sb) from b + b nb sb, each in the fixed shuffle order.
+__global__ void sum_partials_batch_kernel(const double* __restrict__ a, int na, int sa,
+                                          const double* __restrict__ b, int nb, int sb,
+                                          double* __restrict__ out) {
+  pdl_trigger();
+  pdl_wait();
+  const size_t img = blockIdx.y;
+  const bool first = (int)blockIdx.x < sa;
+  const int comp = first ? blockIdx.x : blockIdx.x - sa;
+  const int n = first ? na : nb, stride = first ? sa : sb;
+  const double* part = first ? a + img * na * sa : b + img * nb * sb;
+  double v = 0.0;
+  for (int i = threadIdx.x; i < n; i += 32) v += part[(size_t)i * stride + comp];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if (threadIdx.x == 0) out[img * (sa + sb) + blockIdx.x] = v;
+}
+
+cudaError_t launch_sum_partials_batch(cudaStream_t s, const double* a, int na, int sa,
+                                      const double* b, int nb, int sb, double* out, int batch) {
+  return launch_pdl(sum_partials_batch_kernel, dim3(sa + sb, batch), dim3(32), 0, s, a, na, sa, b,
+                    nb, sb, out);
 }
 
 // ---------------------------------------------------------------- field export

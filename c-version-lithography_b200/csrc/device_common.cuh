@@ -89,6 +89,10 @@ struct ResistEpiT {
   ResistEpilogue p;
   int N, vec;
   double pe, pen;
+  // Pixel (m, n) of image blockIdx.z: the images of a batched launch lie N * N apart.
+  __device__ __forceinline__ size_t pix(int m, int n) const {
+    return ((size_t)blockIdx.z * N + m) * N + n;
+  }
   __device__ __forceinline__ float sigmoid(float I) const {
     const float z = -p.alpha * (I - p.thr);
     return FAST ? __fdividef(1.f, 1.f + __expf(z)) : 1.f / (1.f + expf(z));
@@ -112,10 +116,10 @@ struct ResistEpiT {
   // store that consumes it.
   __device__ __forceinline__ float4 pre4(int m, int n, int nvalid) const {
     if (p.mode == 0 || nvalid <= 0) return make_float4(0.f, 0.f, 0.f, 0.f);
-    return ld4(p.target, (size_t)m * N + n, vec, nvalid);
+    return ld4(p.target, pix(m, n), vec, nvalid);
   }
   __device__ __forceinline__ void store4p(int m, int n, float4 I, float4 T, int nvalid) {
-    const size_t i = (size_t)m * N + n;
+    const size_t i = pix(m, n);
     if (p.mode == 0) {
       if (p.aerial) st4(p.aerial, i, I, vec, nvalid);
       if (p.wafer) {
@@ -129,7 +133,7 @@ struct ResistEpiT {
   // Mode 1 without the dL/dI store: aerial / wafer stores and loss terms as in
   // store4p, dL/dI returned (0 in lanes past nvalid).
   __device__ __forceinline__ float4 dldi4(int m, int n, float4 I, float4 T, int nvalid) {
-    const size_t i = (size_t)m * N + n;
+    const size_t i = pix(m, n);
     if (p.aerial) st4(p.aerial, i, I, vec, nvalid);
     const float4 one4 = make_float4(1.f, 1.f, 1.f, 1.f);
     const float4 pw = p.pe_window ? ld4(p.pe_window, i, vec, nvalid) : one4;
@@ -145,7 +149,7 @@ struct ResistEpiT {
   // dldi4 for four in-range pixels when there is no window and no penalty (the CTM
   // evaluation): the same arithmetic with pw = qw = 1, which x * 1.f leaves exact.
   __device__ __forceinline__ float4 plain4(int m, int n, float4 I, float4 T) {
-    const size_t i = (size_t)m * N + n;
+    const size_t i = pix(m, n);
     if (p.aerial) st4(p.aerial, i, I, vec, 4);
     float4 W, g;
     auto one_plain = [&](float x, float t, float& w, float& d) {
@@ -171,7 +175,7 @@ struct ResistEpiT {
     const double a = block_sum<EPI_NT>(pe, sh);
     const double b = block_sum<EPI_NT>(pen, sh);
     if (threadIdx.x == 0) {
-      const int bid = blockIdx.y * gridDim.x + blockIdx.x;
+      const size_t bid = ((size_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
       p.loss_partial[2 * bid] = a;
       p.loss_partial[2 * bid + 1] = b;
     }
@@ -186,16 +190,19 @@ struct GradEpiT {
   GradEpilogue p;
   int N, vec;
   double nrm;
+  __device__ __forceinline__ size_t pix(int m, int n) const {
+    return ((size_t)blockIdx.z * N + m) * N + n;
+  }
   __device__ __forceinline__ float sn(float t) const { return FAST ? fast_sin(t) : sinf(t); }
   __device__ __forceinline__ void store4(int m, int n, float4 G, int nvalid) {
     store4p(m, n, G, pre4(m, n, nvalid), nvalid);
   }
   __device__ __forceinline__ float4 pre4(int m, int n, int nvalid) const {
     if (!p.theta || nvalid <= 0) return make_float4(0.f, 0.f, 0.f, 0.f);
-    return ld4(p.theta, (size_t)m * N + n, vec, nvalid);
+    return ld4(p.theta, pix(m, n), vec, nvalid);
   }
   __device__ __forceinline__ void store4p(int m, int n, float4 G, float4 th, int nvalid) {
-    const size_t i = (size_t)m * N + n;
+    const size_t i = pix(m, n);
     if (p.grad_mask) st4(p.grad_mask, i, G, vec, nvalid);
     if (!p.theta) return;
     float4 gt;
@@ -218,7 +225,8 @@ struct GradEpiT {
     if (!p.theta) return;
     __shared__ double sh[EPI_NT / 32];
     const double a = block_sum<EPI_NT>(nrm, sh);
-    if (threadIdx.x == 0) p.norm_partial[blockIdx.y * gridDim.x + blockIdx.x] = a;
+    if (threadIdx.x == 0)   // [image][tile] over a batched launch
+      p.norm_partial[((size_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x] = a;
   }
 };
 

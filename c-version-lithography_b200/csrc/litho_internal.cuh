@@ -182,23 +182,20 @@ cudaError_t launch_analysis(cudaStream_t s, int mode, const float* in, float* ma
                             int nrows_out, int nr, int sym, float2* part);
 // out[o] = scale * sum_t part[o][t] (fixed order).
 cudaError_t launch_reduce_tiles(cudaStream_t s, const float2* part, int tiles, int count,
-                                float scale, float2* out);
+                                float scale, float2* out, int batch = 1);
 // Small-grid stage of the forward: f.mband -> f.e, ik, iP and Ut (the row
 // synthesis operand), or, with img set, Ut's split-BF16 operand image for the
 // tensor-core synthesis (launch_pack_tc2_rows layout) instead of Ut.
 // Shared memory of its per-kernel CTA: band_fields_smem.
 size_t band_fields_smem(const BandGeom& g);
 size_t band_max_smem(const BandGeom& g);
-// Kernels launch_band_forward issues: fields, sum over k, then either the merged
-// chat + expansion (when its staging fits two CTAs per SM) or the two separately.
-int band_forward_launches(const BandGeom& g);
 cudaError_t launch_band_forward(cudaStream_t s, const Cache& c, Field& f, float* ik, float* iP,
-                                float2* chat, float* Ut, void* img);
+                                float2* chat, float* Ut, void* img, int batch = 1);
 // Small-grid stage of the adjoint: gh (the D-band DFT of dL/dI) -> gam, Zk, X and Vt
 // (or Vt's operand image, as for the forward).
 cudaError_t launch_band_adjoint(cudaStream_t s, const Cache& c, const Field& f, const float2* gh,
                                 double scale, float* gam, float2* Zk, float2* X, float* Vt,
-                                void* img);
+                                void* img, int batch = 1);
 
 // Row synthesis: out[y][x] = sum_f AY[y][f] * Bt[x][f] with a fused epilogue.
 struct ResistEpilogue {
@@ -227,6 +224,10 @@ cudaError_t launch_sum_partials(cudaStream_t s, const double* part, int n, int s
                                 double* out);
 cudaError_t launch_sum_partials2(cudaStream_t s, const double* a, int na, int sa, double* out_a,
                                  const double* b, int nb, int sb, double* out_b);
+// Batched sums: per image b, sa components over na blocks of a (stride na sa per
+// image) then sb over nb blocks of b, into out[b][sa + sb].
+cudaError_t launch_sum_partials_batch(cudaStream_t s, const double* a, int na, int sa,
+                                      const double* b, int nb, int sb, double* out, int batch);
 cudaError_t launch_export_field(cudaStream_t s, const Cache& c, const Field& f, int k,
                                 float2* tmp_rows, float2* out);
 cudaError_t launch_pe_loss(cudaStream_t s, const float* w, const float* t, const float* pe_win,
@@ -247,15 +248,18 @@ cudaError_t launch_pack_tc2_tx(cudaStream_t s, const float* tw, int ncols, int N
 cudaError_t launch_pack_tc2_ty(cudaStream_t s, const float2* T, int nr, int N, void* dst);
 cudaError_t launch_analysis_tc2(cudaStream_t s, int mode, const float* in, float* mask_out,
                                 int* flag, int N, int ncols, int nrows_out, int nr, int sym,
-                                float2* part, const void* tx_img, const void* ty_img, int* err);
+                                float2* part, const void* tx_img, const void* ty_img, int* err,
+                                int batch = 1);
 // Row synthesis: Aimg = image of AY ([N][kp], launch_pack_tc2_rows), Bimg = image
 // of the band operand Bt ([N][kp]); kp % 16 == 0 and kp <= 128.
 size_t tc2_rows_image_bytes(int N, int kp);
 cudaError_t launch_pack_tc2_rows(cudaStream_t s, const float* src, int N, int kp, void* dst);
 cudaError_t launch_synth_resist_tc2(cudaStream_t s, const void* Aimg, const void* Bimg, int N,
-                                    int kp, const ResistEpilogue& ep, int* err, int* nblocks);
+                                    int kp, const ResistEpilogue& ep, int* err, int* nblocks,
+                                    int batch = 1);
 cudaError_t launch_synth_grad_tc2(cudaStream_t s, const void* Aimg, const void* Bimg, int N,
-                                  int kp, const GradEpilogue& ep, int* err, int* nblocks);
+                                  int kp, const GradEpilogue& ep, int* err, int* nblocks,
+                                  int batch = 1);
 // Resist synthesis fused with the adjoint tile analysis (CTM evaluation): loss
 // partials as launch_synth_resist_tc2 (ep.dldi unused), and the adjoint partials
 // part[tile][2 nr - 1][ncols] of dL/dI as launch_analysis_tc2 with the TXD / TYD
@@ -263,7 +267,8 @@ cudaError_t launch_synth_grad_tc2(cudaStream_t s, const void* Aimg, const void* 
 cudaError_t launch_synth_resist_analysis_tc2(cudaStream_t s, const void* Aimg, const void* Bimg,
                                              int N, int kp, const ResistEpilogue& ep, int ncols,
                                              int nr, float2* part, int* flag, const void* tx_img,
-                                             const void* ty_img, int* err, int* nblocks);
+                                             const void* ty_img, int* err, int* nblocks,
+                                             int batch = 1);
 // The tensor-core path needs kp <= 128 and 2 Nc <= 128 (bands up to 64 x 64).
 inline bool tc2_supported(const BandGeom& g) {
   return g.kp_rows <= 128 && tc2_analysis_supported(g.Nc, g.Nr);

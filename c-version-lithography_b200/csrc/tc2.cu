@@ -23,6 +23,12 @@
 
 namespace litho_b200 {
 
+// First element of row m of image blockIdx.z (the images of a batched launch lie
+// N * N apart).
+__device__ __forceinline__ size_t img_row(int N, int m) {
+  return ((size_t)blockIdx.z * N + m) * N;
+}
+
 __host__ __device__ constexpr uint32_t s2_atoms(int K) { return (uint32_t)(2 * K + 63) / 64; }
 __host__ __device__ constexpr uint32_t s2_tile_bytes(int RB, int K) {
   return s2_atoms(K) * (uint32_t)RB * 128u;
@@ -283,7 +289,8 @@ __device__ __forceinline__ void analysis_stages(uint8_t* sA, uint8_t* sB, const 
   }
   __syncthreads();
   if (!*fail) {
-    float2* out = a.part + (size_t)(yt * gridDim.x + xt) * count;   // [tile][row][c]
+    // [image][tile][row][c]; the image of a batched launch is blockIdx.z
+    float2* out = a.part + (((size_t)blockIdx.z * gridDim.y + yt) * gridDim.x + xt) * count;
     for (int e = tid; e < count; e += blockDim.x) out[e] = stage[e];
   }
 }
@@ -329,14 +336,14 @@ analysis_tc2_kernel(Tc2Analysis a, const uint8_t* __restrict__ txImg,
     const int r = j >> 4, c8 = (j & 15) * 8;
     const int m = y0 + r, x = x0 + c8;
     if (a.vec4 && m < a.N && x + 7 < a.N) {
-      const float4 p = __ldg(reinterpret_cast<const float4*>(a.in + (size_t)m * a.N + x));
-      const float4 q = __ldg(reinterpret_cast<const float4*>(a.in + (size_t)m * a.N + x + 4));
+      const float4 p = __ldg(reinterpret_cast<const float4*>(a.in + img_row(a.N, m) + x));
+      const float4 q = __ldg(reinterpret_cast<const float4*>(a.in + img_row(a.N, m) + x + 4));
       v[i][0] = p.x; v[i][1] = p.y; v[i][2] = p.z; v[i][3] = p.w;
       v[i][4] = q.x; v[i][5] = q.y; v[i][6] = q.z; v[i][7] = q.w;
     } else {
 #pragma unroll
       for (int e = 0; e < 8; ++e)
-        v[i][e] = (m < a.N && x + e < a.N) ? __ldg(a.in + (size_t)m * a.N + x + e) : 0.f;
+        v[i][e] = (m < a.N && x + e < a.N) ? __ldg(a.in + img_row(a.N, m) + x + e) : 0.f;
     }
   }
   bool bad = false;
@@ -353,7 +360,7 @@ analysis_tc2_kernel(Tc2Analysis a, const uint8_t* __restrict__ txImg,
       if (in_range) bad |= !isfinite(u[e]);
       if (a.mode == 1) {
         u[e] = in_range ? 0.5f * (1.f + fast_cos(u[e])) : 0.f;
-        if (a.mask_out && in_range) a.mask_out[(size_t)m * a.N + x + e] = u[e];
+        if (a.mask_out && in_range) a.mask_out[img_row(a.N, m) + x + e] = u[e];
       }
     }
     uint4 h4, l4;
@@ -373,13 +380,13 @@ analysis_tc2_kernel(Tc2Analysis a, const uint8_t* __restrict__ txImg,
 
 template <int BN>
 static cudaError_t analysis_tc2_t(cudaStream_t s, const Tc2Analysis& a, const void* tx,
-                                  const void* ty, int* err) {
+                                  const void* ty, int* err, int batch) {
   const size_t smem = A2_A_BYTES + s2_tile_bytes(BN, 128) + 1024;
   cudaError_t e = cudaFuncSetAttribute(analysis_tc2_kernel<BN>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   const int t = (a.N + 127) / 128;
-  return launch_pdl(analysis_tc2_kernel<BN>, dim3(t, t), dim3(A2_NT), smem, s, a,
+  return launch_pdl(analysis_tc2_kernel<BN>, dim3(t, t, batch), dim3(A2_NT), smem, s, a,
                     static_cast<const uint8_t*>(tx), static_cast<const uint8_t*>(ty), err);
 }
 
@@ -407,20 +414,21 @@ bool tc2_analysis_supported(int ncols, int nr) {
 
 cudaError_t launch_analysis_tc2(cudaStream_t s, int mode, const float* in, float* mask_out,
                                 int* flag, int N, int ncols, int nrows_out, int nr, int sym,
-                                float2* part, const void* tx_img, const void* ty_img, int* err) {
+                                float2* part, const void* tx_img, const void* ty_img, int* err,
+                                int batch) {
   // The epilogue stages the tile's partials in the 64 KiB operand area.
   if ((size_t)nrows_out * ncols * sizeof(float2) > A2_A_BYTES) return cudaErrorInvalidValue;
   const int vec4 = (N % 4 == 0) && (reinterpret_cast<uintptr_t>(in) % 16 == 0);
   Tc2Analysis a{in, mask_out, flag, N, mode, vec4, ncols, nrows_out, nr, sym, part};
   switch (tc2_analysis_rows(ncols)) {
-    case 16: return analysis_tc2_t<16>(s, a, tx_img, ty_img, err);
-    case 32: return analysis_tc2_t<32>(s, a, tx_img, ty_img, err);
-    case 48: return analysis_tc2_t<48>(s, a, tx_img, ty_img, err);
-    case 64: return analysis_tc2_t<64>(s, a, tx_img, ty_img, err);
-    case 80: return analysis_tc2_t<80>(s, a, tx_img, ty_img, err);
-    case 96: return analysis_tc2_t<96>(s, a, tx_img, ty_img, err);
-    case 112: return analysis_tc2_t<112>(s, a, tx_img, ty_img, err);
-    case 128: return analysis_tc2_t<128>(s, a, tx_img, ty_img, err);
+    case 16: return analysis_tc2_t<16>(s, a, tx_img, ty_img, err, batch);
+    case 32: return analysis_tc2_t<32>(s, a, tx_img, ty_img, err, batch);
+    case 48: return analysis_tc2_t<48>(s, a, tx_img, ty_img, err, batch);
+    case 64: return analysis_tc2_t<64>(s, a, tx_img, ty_img, err, batch);
+    case 80: return analysis_tc2_t<80>(s, a, tx_img, ty_img, err, batch);
+    case 96: return analysis_tc2_t<96>(s, a, tx_img, ty_img, err, batch);
+    case 112: return analysis_tc2_t<112>(s, a, tx_img, ty_img, err, batch);
+    case 128: return analysis_tc2_t<128>(s, a, tx_img, ty_img, err, batch);
     default: return cudaErrorInvalidValue;
   }
 }
@@ -482,7 +490,8 @@ synth_tc2_kernel(const uint8_t* __restrict__ Aimg, const uint8_t* __restrict__ B
   }
   pdl_wait();
   if (tid == 0) {
-    const uint8_t* gb = Bimg + (size_t)xt * tile_bytes;
+    // The band operand image of this launch's image blockIdx.z.
+    const uint8_t* gb = Bimg + ((size_t)blockIdx.z * gridDim.x + xt) * tile_bytes;
     for (uint32_t q = 0; q < tile_bytes; q += 16384)
       tc::bulk_g2s(uB + q, gb + q, tile_bytes - q < 16384u ? tile_bytes - q : 16384u, barL);
   }
@@ -556,12 +565,12 @@ synth_tc2_kernel(const uint8_t* __restrict__ Aimg, const uint8_t* __restrict__ B
 
 template <class Epi>
 static cudaError_t launch_tc2(cudaStream_t s, const void* Aimg, const void* Bimg, int N, int kp,
-                              const Epi& e, int* err, int* nblocks) {
+                              const Epi& e, int* err, int* nblocks, int batch) {
   const int smem = (int)tc2_synth_smem(kp);
   cudaError_t r = cudaFuncSetAttribute(synth_tc2_kernel<Epi>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (r != cudaSuccess) return r;
-  dim3 grid((N + 127) / 128, (N + 127) / 128);
+  dim3 grid((N + 127) / 128, (N + 127) / 128, batch);
   *nblocks = grid.x * grid.y;
   return launch_pdl(synth_tc2_kernel<Epi>, grid, dim3(S2_NT), (size_t)smem, s,
                     static_cast<const uint8_t*>(Aimg), static_cast<const uint8_t*>(Bimg), N, kp,
@@ -576,19 +585,21 @@ cudaError_t launch_pack_tc2_rows(cudaStream_t s, const float* src, int N, int kp
 }
 
 cudaError_t launch_synth_resist_tc2(cudaStream_t s, const void* Aimg, const void* Bimg, int N,
-                                    int kp, const ResistEpilogue& ep, int* err, int* nblocks) {
+                                    int kp, const ResistEpilogue& ep, int* err, int* nblocks,
+                                    int batch) {
   const int vec = N % 4 == 0 && aligned16(ep.aerial) && aligned16(ep.wafer) &&
                   aligned16(ep.target) && aligned16(ep.pe_window) && aligned16(ep.pen_window) &&
                   aligned16(ep.dldi);
   return launch_tc2(s, Aimg, Bimg, N, kp, ResistEpiT<true>{ep, N, vec, 0.0, 0.0}, err,
-                    nblocks);
+                    nblocks, batch);
 }
 
 cudaError_t launch_synth_grad_tc2(cudaStream_t s, const void* Aimg, const void* Bimg, int N,
-                                  int kp, const GradEpilogue& ep, int* err, int* nblocks) {
+                                  int kp, const GradEpilogue& ep, int* err, int* nblocks,
+                                  int batch) {
   const int vec = N % 4 == 0 && aligned16(ep.grad_mask) && aligned16(ep.theta) &&
                   aligned16(ep.grad_theta);
-  return launch_tc2(s, Aimg, Bimg, N, kp, GradEpiT<true>{ep, N, vec, 0.0}, err, nblocks);
+  return launch_tc2(s, Aimg, Bimg, N, kp, GradEpiT<true>{ep, N, vec, 0.0}, err, nblocks, batch);
 }
 
 // ---------------------------------------------------------------- fused resist + adjoint analysis
@@ -658,7 +669,8 @@ synth_resist_analysis_kernel(const uint8_t* __restrict__ Aimg, const uint8_t* __
   }
   pdl_wait();
   if (tid == 0) {
-    const uint8_t* gb = Bimg + (size_t)xt * tile_bytes;
+    // The band operand image of this launch's image blockIdx.z.
+    const uint8_t* gb = Bimg + ((size_t)blockIdx.z * gridDim.x + xt) * tile_bytes;
     for (uint32_t q = 0; q < tile_bytes; q += 16384)
       tc::bulk_g2s(uB + q, gb + q, tile_bytes - q < 16384u ? tile_bytes - q : 16384u, barL);
   }
@@ -758,14 +770,14 @@ synth_resist_analysis_kernel(const uint8_t* __restrict__ Aimg, const uint8_t* __
 template <int BN, bool PLAIN>
 static cudaError_t fused_v(cudaStream_t s, const void* Aimg, const void* Bimg, int N, int kp,
                           const ResistEpiT<true>& e, const Tc2Analysis& a, const void* tx,
-                          const void* ty, int* err, int* nblocks) {
+                          const void* ty, int* err, int* nblocks, int batch) {
   const size_t ops = 2 * (size_t)s2_tile_bytes(128, kp);
   const size_t ana = (size_t)FUSED_TX_OFFSET + s2_tile_bytes(BN, 128);
   const size_t smem = (ops > ana ? ops : ana) + 1024;
   cudaError_t r = cudaFuncSetAttribute(synth_resist_analysis_kernel<BN, PLAIN>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (r != cudaSuccess) return r;
-  dim3 grid((N + 127) / 128, (N + 127) / 128);
+  dim3 grid((N + 127) / 128, (N + 127) / 128, batch);
   *nblocks = grid.x * grid.y;
   return launch_pdl(synth_resist_analysis_kernel<BN, PLAIN>, grid, dim3(S2_NT), smem, s,
                     static_cast<const uint8_t*>(Aimg), static_cast<const uint8_t*>(Bimg), N, kp, e,
@@ -777,29 +789,30 @@ static cudaError_t fused_v(cudaStream_t s, const void* Aimg, const void* Bimg, i
 template <int BN>
 static cudaError_t fused_t(cudaStream_t s, const void* Aimg, const void* Bimg, int N, int kp,
                           const ResistEpiT<true>& e, const Tc2Analysis& a, const void* tx,
-                          const void* ty, int* err, int* nblocks) {
-  return e.plain() ? fused_v<BN, true>(s, Aimg, Bimg, N, kp, e, a, tx, ty, err, nblocks)
-                   : fused_v<BN, false>(s, Aimg, Bimg, N, kp, e, a, tx, ty, err, nblocks);
+                          const void* ty, int* err, int* nblocks, int batch) {
+  return e.plain() ? fused_v<BN, true>(s, Aimg, Bimg, N, kp, e, a, tx, ty, err, nblocks, batch)
+                   : fused_v<BN, false>(s, Aimg, Bimg, N, kp, e, a, tx, ty, err, nblocks, batch);
 }
 
 cudaError_t launch_synth_resist_analysis_tc2(cudaStream_t s, const void* Aimg, const void* Bimg,
                                              int N, int kp, const ResistEpilogue& ep, int ncols,
                                              int nr, float2* part, int* flag, const void* tx_img,
-                                             const void* ty_img, int* err, int* nblocks) {
+                                             const void* ty_img, int* err, int* nblocks,
+                                             int batch) {
   const int vec = N % 4 == 0 && aligned16(ep.aerial) && aligned16(ep.wafer) &&
                   aligned16(ep.target) && aligned16(ep.pe_window) && aligned16(ep.pen_window);
   if ((size_t)(2 * nr - 1) * ncols * sizeof(float2) > A2_A_BYTES) return cudaErrorInvalidValue;
   const ResistEpiT<true> e{ep, N, vec, 0.0, 0.0};
   const Tc2Analysis a{nullptr, nullptr, flag, N, 0, 0, ncols, 2 * nr - 1, nr, 1, part};
   switch (tc2_analysis_rows(ncols)) {
-    case 16: return fused_t<16>(s, Aimg, Bimg, N, kp, e, a, tx_img, ty_img, err, nblocks);
-    case 32: return fused_t<32>(s, Aimg, Bimg, N, kp, e, a, tx_img, ty_img, err, nblocks);
-    case 48: return fused_t<48>(s, Aimg, Bimg, N, kp, e, a, tx_img, ty_img, err, nblocks);
-    case 64: return fused_t<64>(s, Aimg, Bimg, N, kp, e, a, tx_img, ty_img, err, nblocks);
-    case 80: return fused_t<80>(s, Aimg, Bimg, N, kp, e, a, tx_img, ty_img, err, nblocks);
-    case 96: return fused_t<96>(s, Aimg, Bimg, N, kp, e, a, tx_img, ty_img, err, nblocks);
-    case 112: return fused_t<112>(s, Aimg, Bimg, N, kp, e, a, tx_img, ty_img, err, nblocks);
-    case 128: return fused_t<128>(s, Aimg, Bimg, N, kp, e, a, tx_img, ty_img, err, nblocks);
+    case 16: return fused_t<16>(s, Aimg, Bimg, N, kp, e, a, tx_img, ty_img, err, nblocks, batch);
+    case 32: return fused_t<32>(s, Aimg, Bimg, N, kp, e, a, tx_img, ty_img, err, nblocks, batch);
+    case 48: return fused_t<48>(s, Aimg, Bimg, N, kp, e, a, tx_img, ty_img, err, nblocks, batch);
+    case 64: return fused_t<64>(s, Aimg, Bimg, N, kp, e, a, tx_img, ty_img, err, nblocks, batch);
+    case 80: return fused_t<80>(s, Aimg, Bimg, N, kp, e, a, tx_img, ty_img, err, nblocks, batch);
+    case 96: return fused_t<96>(s, Aimg, Bimg, N, kp, e, a, tx_img, ty_img, err, nblocks, batch);
+    case 112: return fused_t<112>(s, Aimg, Bimg, N, kp, e, a, tx_img, ty_img, err, nblocks, batch);
+    case 128: return fused_t<128>(s, Aimg, Bimg, N, kp, e, a, tx_img, ty_img, err, nblocks, batch);
     default: return cudaErrorInvalidValue;
   }
 }

@@ -176,6 +176,16 @@ int litho_ctm_evaluate_host(litho_ctx* ctx, const litho_cache* cache, litho_fiel
                             double alpha, float* h_grad_theta, double* loss,
                             double* grad_norm);
 
+/* Batched CTM objective: `batch` images of the cache's size N (theta, target and
+ * d_grad_theta hold them back to back, [batch][N][N]) in one pass of the chain,
+ * every kernel covering all images at once, so the per-image latency of the
+ * small-grid stages and of each tile's pipeline overlaps across images. losses and
+ * norms (host, nullable) receive one value per image, as litho_ctm_evaluate's loss
+ * and grad_norm. In LITHO_PRECISION_FP32 the images are evaluated one after another. */
+int litho_ctm_evaluate_batch(litho_ctx* ctx, const litho_cache* cache, int batch,
+                             const float* d_theta, const float* d_target, double threshold,
+                             double alpha, float* d_grad_theta, double* losses, double* norms);
+
 /* ------------------------------------------------------------ sparse EPE
  * Edge points (EPs) are chosen on the host (EpSelect, source/utils/ep_select.cpp);
  * eps is n x 2 host doubles (y, x) in subpixel image coordinates, weights n host

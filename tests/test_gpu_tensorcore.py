@@ -100,3 +100,53 @@ def test_bf16x3_agrees_with_fp32_path(L, wl, tc_ctx):
         outs[mode] = (loss, cpu(gt))
     assert abs(outs["fp32"][0] - outs["bf16x3"][0]) <= 1e-4 * outs["fp32"][0]
     assert rel_l2(outs["bf16x3"][1], outs["fp32"][1]) <= 1e-3
+
+
+@pytest.mark.parametrize("N,B", [(300, 3), (2048, 4)])
+def test_batched_evaluation_equals_single_images(L, wl, tc_ctx, N, B):
+    """litho_ctm_evaluate_batch: every image's loss, gradient and norm are the same alone
+    and in the batch (same kernels, same summation order: bit for bit), and image 0
+    matches the FP64 oracle within the split-BF16 tolerance."""
+    band, r0, c0, w, wss = wl.synthetic_socs_band()
+    cache = L.ImagingCache.from_band(N, band, r0, c0, w, wss, ctx=tc_ctx)
+    rng = np.random.default_rng(N)
+    targets = np.stack([wl.manhattan_target(N, max(4, N // 20), seed=N + b) for b in range(B)])
+    thetas = np.stack([wl.theta_init_reference(t) for t in targets])
+    thetas = thetas + 0.2 * rng.standard_normal(thetas.shape)
+    th = torch.tensor(thetas, dtype=torch.float32, device="cuda")
+    tg = torch.tensor(targets, dtype=torch.float32, device="cuda")
+    losses, grads, norms = L.ctm_evaluate_batch(cache, th, tg, 0.225, 50.0)
+    for b in range(B):
+        opt = L.CTMOptimizer(cache, tg[b], 0.225, 50.0, iterations=1)
+        loss, gt, norm = opt.evaluate(th[b])
+        assert losses[b] == loss and norms[b] == norm, b
+        assert torch.equal(grads[b], gt), b
+    if N <= 300:
+        oc = io.OracleCache(N=N, kernels=list(wl.band_to_dense(band, r0, c0, N)),
+                            source_ws=np.array([wss]), eigenvalues=tuple(w))
+        ref = io.ctm_evaluate(thetas[0].astype(np.float32).astype(np.float64), targets[0], oc,
+                              0.225, 50.0)
+        assert abs(losses[0] - ref["loss"]) <= 1e-4 * ref["loss"]
+        assert rel_l2(cpu(grads[0]), ref["grad_theta"]) <= 1e-3
+
+
+def test_batched_evaluation_fp32_and_errors(L, wl):
+    ctx = L.Context()
+    band, r0, c0, w, wss = wl.synthetic_socs_band()
+    cache = L.ImagingCache.from_band(128, band, r0, c0, w, wss, ctx=ctx)
+    targets = np.stack([wl.manhattan_target(128, 6, seed=s) for s in range(2)])
+    th = torch.tensor(np.stack([wl.theta_init_reference(t) for t in targets]), dtype=torch.float32,
+                      device="cuda")
+    tg = torch.tensor(targets, dtype=torch.float32, device="cuda")
+    losses, grads, _ = L.ctm_evaluate_batch(cache, th, tg, 0.225, 50.0)
+    for b in range(2):
+        loss, gt, _ = L.CTMOptimizer(cache, tg[b], 0.225, 50.0, iterations=1).evaluate(th[b])
+        assert losses[b] == loss and torch.equal(grads[b], gt)
+    with pytest.raises(L.LithoError):
+        L.ctm_evaluate_batch(cache, th[:, :64], tg, 0.225, 50.0)
+    bad = th.clone()
+    bad[1, 3, 4] = float("nan")
+    with pytest.raises(L.LithoError) as e:
+        L.ctm_evaluate_batch(cache, bad, tg, 0.225, 50.0)
+    assert e.value.status == 3
+    ctx.close()
