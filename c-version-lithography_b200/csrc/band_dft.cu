@@ -16,6 +16,8 @@
 // a fused elementwise epilogue. The K-dependent work lives on the small grid.
 #include <cuda_runtime.h>
 
+#include <type_traits>
+
 #include <algorithm>
 
 #include <cuda_bf16.h>
@@ -416,35 +418,48 @@ __device__ __forceinline__ void fill_batched(T* dst, int n, Load load) {
   }
 }
 
-// Forward 1: grid (K, column chunks of the small grid). CTA (k, q) owns small-grid
-// columns jc in [q CW, q CW + CW): A = H_k m on the band, T = A ESc^T restricted
-// to those columns (Nr x CW) and e_k = ESr T (Pr x CW); ik = w_k |e_k|^2. Columns
-// are independent, so the split costs no recomputation.
+// Forward 1: grid (K, column chunks of W, batch). CTA (k, q) owns small-grid
+// columns jc in [q W, q W + W): A = H_k m on the band, T = A ESc^T restricted to
+// those columns (Nr x W) and e_k = ESr T (Pr x W); ik = w_k |e_k|^2. Columns are
+// independent, so the split costs no recomputation. Every thread accumulates four
+// adjacent columns, so one row operand from shared memory feeds four complex FMAs.
 constexpr int BF_NT = 512;   // threads of the fields and Z kernels (more loads in flight while staging)
-constexpr int BF_CW = 10;   // small-grid columns per CTA (forward fields)
-constexpr int BZ_UW = 7;    // band columns per CTA (adjoint Z)
+constexpr int BW_ONE = 8, BW_BATCH = 16;   // chunk widths (multiples of 4): one image, a batch
+__host__ __device__ constexpr int even_up(int n) { return (n + 1) & ~1; }
+__device__ __forceinline__ void cfma4(float2 (&acc)[4], float2 a, const float2* b4) {
+  const float4 b01 = *reinterpret_cast<const float4*>(b4);
+  const float4 b23 = *reinterpret_cast<const float4*>(b4 + 2);
+  cfma(acc[0], a, make_float2(b01.x, b01.y));
+  cfma(acc[1], a, make_float2(b01.z, b01.w));
+  cfma(acc[2], a, make_float2(b23.x, b23.y));
+  cfma(acc[3], a, make_float2(b23.z, b23.w));
+}
+
+template <int W>
 __global__ void __launch_bounds__(BF_NT)
 band_fields_kernel(const float2* __restrict__ H, const float2* __restrict__ mband,
                    const float* __restrict__ w, int Nr, int Nc, int Pr, int Pc,
                    const float2* __restrict__ ESc_t, const float2* __restrict__ ESr_t,
                    int stage_tables, float2* __restrict__ e, float* __restrict__ ik) {
-  extern __shared__ float2 sm2[];
+  static_assert(W % 4 == 0, "four columns per thread");
+  constexpr int JB = W / 4;
+  extern __shared__ __align__(16) float2 sm2[];
   const int k = blockIdx.x;
-  const int j0 = blockIdx.y * BF_CW;
+  const int j0 = blockIdx.y * W;
+  const int cw = min(W, Pc - j0);
   {  // image b of a batch
     const size_t b = blockIdx.z;
     mband += b * Nr * Nc;
     e += b * gridDim.x * Pr * Pc;
     ik += b * gridDim.x * Pr * Pc;
   }
-  const int cw = min(BF_CW, Pc - j0);
-  float2* A = sm2;                  // [Nr][Nc]
-  float2* T = A + Nr * Nc;          // [Nr][BF_CW]
-  float2* esc = T + Nr * BF_CW;     // [Nc][BF_CW]
-  float2* esr = esc + Nc * BF_CW;   // [Nr][Pr] (staged when stage_tables)
+  float2* A = sm2;                      // [Nr][Nc]
+  float2* T = A + even_up(Nr * Nc);     // [Nr][W]
+  float2* esc = T + Nr * W;             // [Nc][W] (columns past cw are zero)
+  float2* esr = esc + Nc * W;           // [Nr][Pr] (staged when stage_tables)
   pdl_trigger();
-  fill_batched<BF_NT>(esc, Nc * BF_CW, [&](int i) {
-    const int c = i / BF_CW, jj = i % BF_CW;
+  fill_batched<BF_NT>(esc, Nc * W, [&](int i) {
+    const int c = i / W, jj = i % W;
     return jj < cw ? ESc_t[(size_t)c * Pc + j0 + jj] : make_float2(0.f, 0.f);
   });
   const float2* ESR = ESr_t;
@@ -455,40 +470,37 @@ band_fields_kernel(const float2* __restrict__ H, const float2* __restrict__ mban
   pdl_wait();
   fill_batched<BF_NT>(A, Nr * Nc, [&](int i) { return cmul(H[(size_t)k * Nr * Nc + i], mband[i]); });
   __syncthreads();
-  for (int i = threadIdx.x; i < Nr * BF_CW; i += BF_NT) {
-    const int r = i / BF_CW, jj = i % BF_CW;
-    float2 a0 = make_float2(0.f, 0.f), a1 = a0;
-    int c = 0;
-    for (; c + 1 < Nc; c += 2) {
-      cfma(a0, A[r * Nc + c], esc[c * BF_CW + jj]);
-      cfma(a1, A[r * Nc + c + 1], esc[(c + 1) * BF_CW + jj]);
-    }
-    if (c < Nc) cfma(a0, A[r * Nc + c], esc[c * BF_CW + jj]);
-    T[i] = make_float2(a0.x + a1.x, a0.y + a1.y);
+  for (int it = threadIdx.x; it < Nr * JB; it += BF_NT) {
+    const int r = it / JB, jb = 4 * (it % JB);
+    float2 acc[4] = {};
+    for (int c = 0; c < Nc; ++c) cfma4(acc, A[r * Nc + c], esc + c * W + jb);
+    *reinterpret_cast<float4*>(T + r * W + jb) = make_float4(acc[0].x, acc[0].y, acc[1].x, acc[1].y);
+    *reinterpret_cast<float4*>(T + r * W + jb + 2) =
+        make_float4(acc[2].x, acc[2].y, acc[3].x, acc[3].y);
   }
   __syncthreads();
   const float wk = w[k];
-  for (int i = threadIdx.x; i < Pr * cw; i += BF_NT) {
-    const int jr = i / cw, jj = i % cw;
-    float2 a0 = make_float2(0.f, 0.f), a1 = a0;
-    int r = 0;
-    for (; r + 1 < Nr; r += 2) {
-      cfma(a0, ESR[r * Pr + jr], T[r * BF_CW + jj]);
-      cfma(a1, ESR[(r + 1) * Pr + jr], T[(r + 1) * BF_CW + jj]);
+  for (int it = threadIdx.x; it < Pr * JB; it += BF_NT) {
+    const int jr = it / JB, jb = 4 * (it % JB);
+    float2 acc[4] = {};
+    for (int r = 0; r < Nr; ++r) cfma4(acc, ESR[r * Pr + jr], T + r * W + jb);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      if (jb + q >= cw) break;
+      const size_t o = ((size_t)k * Pr + jr) * Pc + j0 + jb + q;
+      e[o] = acc[q];
+      ik[o] = wk * (acc[q].x * acc[q].x + acc[q].y * acc[q].y);
     }
-    if (r < Nr) cfma(a0, ESR[r * Pr + jr], T[r * BF_CW + jj]);
-    const float2 v = make_float2(a0.x + a1.x, a0.y + a1.y);
-    const size_t o = ((size_t)k * Pr + jr) * Pc + j0 + jj;
-    e[o] = v;
-    ik[o] = wk * (v.x * v.x + v.y * v.y);
   }
 }
 
-static size_t fields_smem_full(const BandGeom& g) {
-  return (size_t)(g.Nr * g.Nc + g.Nr * BF_CW + g.Nc * BF_CW + g.Nr * g.Pr) * sizeof(float2);
+template <int W>
+static size_t fields_smem(const BandGeom& g, bool staged) {
+  return (size_t)(even_up(g.Nr * g.Nc) + g.Nr * W + g.Nc * W + (staged ? g.Nr * g.Pr : 0)) *
+         sizeof(float2);
 }
 size_t band_fields_smem(const BandGeom& g) {
-  return (size_t)(g.Nr * g.Nc + g.Nr * BF_CW + g.Nc * BF_CW) * sizeof(float2);
+  return fields_smem<(BW_ONE > BW_BATCH ? BW_ONE : BW_BATCH)>(g, false);
 }
 
 // Forward 2: i[j] = sum_k ik[k][j] in k order.
@@ -680,15 +692,19 @@ static cudaError_t launch_expand(cudaStream_t s, const float2* coef, int nrows, 
 cudaError_t launch_band_forward(cudaStream_t s, const Cache& c, Field& f, float* ik, float* iP,
                                 float2* chat, float* Ut, void* img, int batch) {
   const BandGeom& g = c.g;
-  const size_t full = fields_smem_full(g);
-  const int stage = full <= SMEM_STAGE;
-  const size_t sm1 = stage ? full : band_fields_smem(g);
-  cudaError_t err = cudaFuncSetAttribute(band_fields_kernel,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1);
-  if (err != cudaSuccess) return err;
-  err = launch_pdl(band_fields_kernel, dim3(g.K, (g.Pc + BF_CW - 1) / BF_CW, batch), dim3(BF_NT), sm1, s,
-                   c.H, static_cast<const float2*>(f.mband), c.w, g.Nr, g.Nc, g.Pr, g.Pc, c.ESc_t,
-                   c.ESr_t, stage, f.e, ik);
+  auto fields = [&](auto wtag) -> cudaError_t {
+    constexpr int W = decltype(wtag)::value;
+    const bool staged = fields_smem<W>(g, true) <= SMEM_STAGE;
+    const size_t sm1 = fields_smem<W>(g, staged);
+    cudaError_t e1 = cudaFuncSetAttribute(band_fields_kernel<W>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1);
+    if (e1 != cudaSuccess) return e1;
+    return launch_pdl(band_fields_kernel<W>, dim3(g.K, (g.Pc + W - 1) / W, batch), dim3(BF_NT),
+                      sm1, s, c.H, static_cast<const float2*>(f.mband), c.w, g.Nr, g.Nc, g.Pr,
+                      g.Pc, c.ESc_t, c.ESr_t, (int)staged, f.e, ik);
+  };
+  cudaError_t err = batch >= 4 ? fields(std::integral_constant<int, BW_BATCH>{})
+                               : fields(std::integral_constant<int, BW_ONE>{});
   if (err != cudaSuccess) return err;
   const int n = g.Pr * g.Pc;
   err = launch_pdl(sum_k_kernel, dim3((n + 255) / 256, batch), dim3(256), 0, s,
@@ -753,39 +769,44 @@ static size_t gamma_smem(const BandGeom& g) {
 // Largest dynamic shared memory any small-grid kernel needs for this band
 // (the per-kernel CTAs fall back to unstaged tables above their staging limit).
 size_t band_max_smem(const BandGeom& g) {
+  constexpr int WMAX = BW_ONE > BW_BATCH ? BW_ONE : BW_BATCH;
   size_t m = band_fields_smem(g);
-  m = std::max(m, (size_t)(g.Pr * BZ_UW + g.Pc * BZ_UW) * sizeof(float2));
+  m = std::max(m, (size_t)(g.Pr * WMAX + g.Pc * WMAX) * sizeof(float2));
   m = std::max(m, chat_smem(g));
   m = std::max(m, gamma_smem(g));
   m = std::max(m, (size_t)72 * (2 * g.Nc - 1) * sizeof(float2));
   return m;
 }
 
-// Adjoint 2: grid (K, band column chunks). CTA (k, q) owns band columns uc in
-// [q UW, q UW + UW): q_k = e_k gamma (Pr x Pc, staged), Z1 = q_k conj(ESc)
-// restricted to those columns (Pr x UW), Zk = conj(ESr_t) Z1 / (Pr Pc) (Nr x UW).
+// Adjoint 2: grid (K, band column chunks of W, batch). CTA (k, q) owns band columns
+// uc in [q W, q W + W): q_k = e_k gamma (Pr x Pc, staged), Z1 = q_k conj(ESc)
+// restricted to those columns (Pr x W), Zk = conj(ESr_t) Z1 / (Pr Pc) (Nr x W); four
+// adjacent columns per thread as in the fields kernel.
+template <int W>
 __global__ void __launch_bounds__(BF_NT)
 band_z_kernel(const float2* __restrict__ e, const float* __restrict__ gam, int Nr, int Nc, int Pr,
               int Pc, const float2* __restrict__ ESc, const float2* __restrict__ ESr_t,
               int stage_tables, float inv, float2* __restrict__ Zk) {
-  extern __shared__ float2 sz[];
+  static_assert(W % 4 == 0, "four columns per thread");
+  constexpr int JB = W / 4;
+  extern __shared__ __align__(16) float2 sz[];
   const int k = blockIdx.x;
-  const int u0 = blockIdx.y * BZ_UW;
-  const int uw = min(BZ_UW, Nc - u0);
+  const int u0 = blockIdx.y * W;
+  const int uw = min(W, Nc - u0);
   {  // image b of a batch
     const size_t b = blockIdx.z;
     e += b * gridDim.x * Pr * Pc;
     gam += b * Pr * Pc;
     Zk += b * gridDim.x * Nr * Nc;
   }
-  float2* Z1 = sz;                  // [Pr][BZ_UW]
-  float2* esc = Z1 + Pr * BZ_UW;    // [Pc][BZ_UW]
-  float2* q = esc + Pc * BZ_UW;     // [Pr][Pc]   (staged)
+  float2* Z1 = sz;                  // [Pr][W]
+  float2* esc = Z1 + Pr * W;        // [Pc][W] (columns past uw are zero)
+  float2* q = esc + Pc * W;         // [Pr][Pc]   (staged)
   float2* esr = q + Pr * Pc;        // [Nr][Pr]   (staged)
   const float2* ek = e + (size_t)k * Pr * Pc;
   pdl_trigger();
-  fill_batched<BF_NT>(esc, Pc * BZ_UW, [&](int i) {
-    const int jc = i / BZ_UW, uu = i % BZ_UW;
+  fill_batched<BF_NT>(esc, Pc * W, [&](int i) {
+    const int jc = i / W, uu = i % W;
     return uu < uw ? conjf2(ESc[(size_t)jc * Nc + u0 + uu]) : make_float2(0.f, 0.f);
   });
   const float2* ESR = ESr_t;
@@ -802,9 +823,9 @@ band_z_kernel(const float2* __restrict__ e, const float* __restrict__ gam, int N
     });
   }
   __syncthreads();
-  for (int i = threadIdx.x; i < Pr * BZ_UW; i += BF_NT) {
-    const int jr = i / BZ_UW, uu = i % BZ_UW;
-    float2 a0 = make_float2(0.f, 0.f), a1 = a0;
+  for (int it = threadIdx.x; it < Pr * JB; it += BF_NT) {
+    const int jr = it / JB, jb = 4 * (it % JB);
+    float2 acc[4] = {};
     for (int jc = 0; jc < Pc; ++jc) {
       float2 v;
       if (stage_tables) {
@@ -814,23 +835,23 @@ band_z_kernel(const float2* __restrict__ e, const float* __restrict__ gam, int N
         const float gv = gam[(size_t)jr * Pc + jc];
         v = make_float2(t.x * gv, t.y * gv);
       }
-      if (jc & 1) cfma(a1, v, esc[jc * BZ_UW + uu]);
-      else cfma(a0, v, esc[jc * BZ_UW + uu]);
+      cfma4(acc, v, esc + jc * W + jb);
     }
-    Z1[i] = make_float2(a0.x + a1.x, a0.y + a1.y);
+    *reinterpret_cast<float4*>(Z1 + jr * W + jb) = make_float4(acc[0].x, acc[0].y, acc[1].x, acc[1].y);
+    *reinterpret_cast<float4*>(Z1 + jr * W + jb + 2) =
+        make_float4(acc[2].x, acc[2].y, acc[3].x, acc[3].y);
   }
   __syncthreads();
-  for (int i = threadIdx.x; i < Nr * uw; i += BF_NT) {
-    const int ur = i / uw, uu = i % uw;
-    float2 a0 = make_float2(0.f, 0.f), a1 = a0;
-    int jr = 0;
-    for (; jr + 1 < Pr; jr += 2) {
-      cfma(a0, conjf2(ESR[ur * Pr + jr]), Z1[jr * BZ_UW + uu]);
-      cfma(a1, conjf2(ESR[ur * Pr + jr + 1]), Z1[(jr + 1) * BZ_UW + uu]);
+  for (int it = threadIdx.x; it < Nr * JB; it += BF_NT) {
+    const int ur = it / JB, jb = 4 * (it % JB);
+    float2 acc[4] = {};
+    for (int jr = 0; jr < Pr; ++jr) cfma4(acc, conjf2(ESR[ur * Pr + jr]), Z1 + jr * W + jb);
+#pragma unroll
+    for (int qq = 0; qq < 4; ++qq) {
+      if (jb + qq >= uw) break;
+      Zk[((size_t)k * Nr + ur) * Nc + u0 + jb + qq] =
+          make_float2(acc[qq].x * inv, acc[qq].y * inv);
     }
-    if (jr < Pr) cfma(a0, conjf2(ESR[ur * Pr + jr]), Z1[jr * BZ_UW + uu]);
-    Zk[((size_t)k * Nr + ur) * Nc + u0 + uu] =
-        make_float2((a0.x + a1.x) * inv, (a0.y + a1.y) * inv);
   }
 }
 
@@ -876,16 +897,21 @@ cudaError_t launch_band_adjoint(cudaStream_t s, const Cache& c, const Field& f, 
   e0 = launch_pdl(band_gamma_kernel, dim3(g.Pr, batch), dim3(256), smg, s, gh, g.Nr, g.Nc, g.Pr, g.Pc,
                   c.EDr_t, c.EDc_t, gam);
   if (e0 != cudaSuccess) return e0;
-  const size_t base = (size_t)(g.Pr * BZ_UW + g.Pc * BZ_UW) * sizeof(float2);
-  const size_t full = base + (size_t)(g.Pr * g.Pc + g.Nr * g.Pr) * sizeof(float2);
-  const int stage = full <= SMEM_STAGE;
-  const size_t smz = stage ? full : base;
-  cudaError_t err = cudaFuncSetAttribute(band_z_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smz);
-  if (err != cudaSuccess) return err;
-  err = launch_pdl(band_z_kernel, dim3(g.K, (g.Nc + BZ_UW - 1) / BZ_UW, batch), dim3(BF_NT), smz, s,
-                   static_cast<const float2*>(f.e), static_cast<const float*>(gam), g.Nr, g.Nc,
-                   g.Pr, g.Pc, c.ESc, c.ESr_t, stage, 1.f / ((float)g.Pr * (float)g.Pc), Zk);
+  auto zk = [&](auto wtag) -> cudaError_t {
+    constexpr int W = decltype(wtag)::value;
+    const size_t base = (size_t)(g.Pr * W + g.Pc * W) * sizeof(float2);
+    const size_t full = base + (size_t)(g.Pr * g.Pc + g.Nr * g.Pr) * sizeof(float2);
+    const int stage = full <= SMEM_STAGE;
+    const size_t smz = stage ? full : base;
+    cudaError_t e1 = cudaFuncSetAttribute(band_z_kernel<W>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smz);
+    if (e1 != cudaSuccess) return e1;
+    return launch_pdl(band_z_kernel<W>, dim3(g.K, (g.Nc + W - 1) / W, batch), dim3(BF_NT), smz, s,
+                      static_cast<const float2*>(f.e), static_cast<const float*>(gam), g.Nr, g.Nc,
+                      g.Pr, g.Pc, c.ESc, c.ESr_t, stage, 1.f / ((float)g.Pr * (float)g.Pc), Zk);
+  };
+  cudaError_t err = batch >= 4 ? zk(std::integral_constant<int, BW_BATCH>{})
+                               : zk(std::integral_constant<int, BW_ONE>{});
   if (err != cudaSuccess) return err;
   const int nb = g.Nr * g.Nc;
   err = launch_pdl(band_x_kernel, dim3((nb + 127) / 128, batch), dim3(128), 0, s,
