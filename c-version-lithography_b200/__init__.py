@@ -105,6 +105,7 @@ SIGNATURES = {
     "litho_ctm_evaluate": (_I, [_P, _P, _P, _P, _P, _D, _D, _P, _P, _P, _P, _P, _PD, _PD]),
     "litho_ctm_evaluate_host": (_I, [_P, _P, _P, _P, _P, _D, _D, _P, _PD, _PD]),
     "litho_ctm_evaluate_batch": (_I, [_P, _P, _I, _P, _P, _D, _D, _P, _PD, _PD]),
+    "litho_pe_gradient_batch": (_I, [_P, _P, _I, _P, _P, _D, _D, _P, _PD]),
     "litho_weno_godunov": (_I, [_P, _I, _I, _P, _P, _D, _D, _P, _P]),
     "litho_kappa": (_I, [_P, _I, _I, _P, _D, _D, _D, _P]),
     "litho_evolution_term": (_I, [_P, _I, _I, _P, _P, _D, _D, _D, _D, _P, _PD]),
@@ -619,6 +620,30 @@ def ctm_evaluate_batch(cache: "ImagingCache", thetas, targets, threshold: float,
                                                 float(threshold), float(alpha), _ptr(out),
                                                 losses, norms))
     return list(losses), out, list(norms)
+
+
+def pe_gradient_batch(cache: "ImagingCache", masks, targets, threshold: float, alpha: float,
+                      grads=None):
+    """Imaging, PE loss and dPE/dM (Gradient::pe_gradient, gradient.cpp:121-133) for a
+    batch of masks in one pass of the kernel chain.
+
+    masks, targets: (batch, N, N) float32 CUDA tensors. Returns (losses, grads): the
+    PE of every image and dPE/dM (batch, N, N), written into `grads` when given."""
+    ctx = cache.ctx
+    torch = ctx.torch
+    N = cache.N
+    m = _f32(masks, torch)
+    if m.dim() != 3 or m.shape[1:] != (N, N):
+        raise LithoError(2, f"masks must be (batch, {N}, {N})")
+    B = m.shape[0]
+    tg = _f32(targets, torch, (B, N, N), "targets")
+    out = grads if grads is not None else torch.empty_like(m)
+    if out.shape != m.shape or out.dtype != torch.float32 or not out.is_contiguous():
+        raise LithoError(2, "grads must be a contiguous float32 tensor shaped like masks")
+    losses = (ctypes.c_double * B)()
+    ctx._check(ctx.lib.litho_pe_gradient_batch(ctx.handle, cache.handle, B, _ptr(m), _ptr(tg),
+                                               float(threshold), float(alpha), _ptr(out), losses))
+    return list(losses), out
 
 
 class CTMOptimizer:

@@ -65,7 +65,7 @@ struct Layout {
 // batch > 1 (the batched CTM evaluation): every per-image buffer repeated batch times
 // back to back, plus the band state of the batch (fm: m on the band, fe: the K
 // small-grid fields per image).
-Layout make_layout(const BandGeom& g, int batch = 1) {
+Layout make_layout(const BandGeom& g, int batch = 1, bool own_field = false) {
   Layout L{};
   const size_t B = (size_t)batch;
   const int N = g.N;
@@ -89,8 +89,9 @@ Layout make_layout(const BandGeom& g, int batch = 1) {
   L.X = take(B * g.Nr * g.Nc * sizeof(float2));
   L.rows_tmp = take((size_t)g.Nr * N * sizeof(float2));
   L.img = take(B * (tc2_supported(g) ? tc2_rows_image_bytes(N, g.kp_rows) : 16));  // band operand images
-  L.fm = batch > 1 ? take(B * g.Nr * g.Nc * sizeof(float2)) : 0;
-  L.fe = batch > 1 ? take(B * g.K * g.Pr * g.Pc * sizeof(float2)) : 0;
+  const bool field = batch > 1 || own_field;
+  L.fm = field ? take(B * g.Nr * g.Nc * sizeof(float2)) : 0;
+  L.fe = field ? take(B * g.K * g.Pr * g.Pc * sizeof(float2)) : 0;
   L.total = off;
   return L;
 }
@@ -682,9 +683,9 @@ int run_adjoint(Context* ctx, const Cache& c, const Field& f, const Layout& L, c
   return st;
 }
 
-int prepare(Context* ctx, const Cache& c, Layout* L, int batch = 1) {
+int prepare(Context* ctx, const Cache& c, Layout* L, int batch = 1, bool own_field = false) {
   if (cudaSetDevice(ctx->device) != cudaSuccess) return ctx->fail(LITHO_ERR_CUDA, "cudaSetDevice");
-  *L = make_layout(c.g, batch);
+  *L = make_layout(c.g, batch, own_field);
   int st = ctx->ensure_scratch(L->total);
   if (st) return st;
   const int blocks = ((c.g.N + 127) / 128) * ((c.g.N + 127) / 128);
@@ -1045,6 +1046,78 @@ int litho_ctm_evaluate_batch(litho_ctx* ctx, const litho_cache* cache, int batch
   for (int b = 0; b < batch; ++b) {
     if (losses) losses[b] = sums[3 * (size_t)b];
     if (norms) norms[b] = std::sqrt(sums[3 * (size_t)b + 2]);
+  }
+  return LITHO_OK;
+}
+
+int litho_pe_gradient_batch(litho_ctx* ctx, const litho_cache* cache, int batch,
+                            const float* d_masks, const float* d_targets, double threshold,
+                            double alpha, float* d_grad_masks, double* losses) {
+  if (!ctx || !cache || batch < 1 || !d_masks || !d_targets || !d_grad_masks)
+    return LITHO_ERR_INVALID_ARGUMENT;
+  if (!std::isfinite(threshold) || !std::isfinite(alpha))
+    return ctx->fail(LITHO_ERR_NONFINITE, "Imaging: mask, threshold, and alpha must be finite");
+  const BandGeom& g = cache->g;
+  const size_t px = (size_t)g.N * g.N;
+  const bool tc = ctx->precision == LITHO_PRECISION_BF16X3 && cache->TXD_img != nullptr;
+  Layout L;
+  int st = prepare(ctx, *cache, &L, tc ? batch : 1, true);
+  if (st) return st;
+  Field f;
+  f.cache = cache;
+  f.e = at<float2>(ctx, L.fe);
+  f.mband = at<float2>(ctx, L.fm);
+  ResistEpilogue ep{};
+  ep.mode = 1;
+  ep.thr = (float)threshold;
+  ep.alpha = (float)alpha;
+  ep.pe_weight = 1.f;
+  ep.penalty = 0.f;
+  ep.pen_thr = 0.01f;
+  ep.loss_partial = ctx->d_red + RED_PART;
+  GradEpilogue gp{};
+  cudaStream_t s = ctx->stream;
+  if (tc) {
+    // Every image in one pass: the resist synthesis runs the adjoint tile analysis.
+    ep.target = d_targets;
+    gp.grad_mask = d_grad_masks;
+    int nb = 0, nb2 = 0;
+    st = run_forward(ctx, *cache, f, L, 0, d_masks, nullptr, ep, &nb, nullptr, true, batch);
+    if (!st) st = run_adjoint(ctx, *cache, f, L, nullptr, 4.0 * alpha, gp, &nb2, true, batch);
+    double* d_sums = ctx->d_red + RED_PART + 2 * (size_t)nb * batch;
+    if (!st)
+      st = check_launch(ctx, launch_sum_partials_batch(s, ctx->d_red + RED_PART, nb, 2,
+                                                       ctx->d_red + RED_PART, 0, 0, d_sums, batch),
+                        "sum");
+    ctx->launches += 1;
+    std::vector<double> sums(2 * (size_t)batch);
+    if (!st)
+      LITHO_CUDA_TRY(ctx, cudaMemcpyAsync(sums.data(), d_sums, sums.size() * sizeof(double),
+                                          cudaMemcpyDeviceToHost, s));
+    if (!st) st = fetch(ctx, 0);
+    if (st) return st;
+    if (flag_set(ctx)) return ctx->fail(LITHO_ERR_NONFINITE, "mask must be finite");
+    for (int b = 0; b < batch && losses; ++b) losses[b] = sums[2 * (size_t)b];
+    return LITHO_OK;
+  }
+  // FP32: one image after another through the same chain with dL/dI stored between
+  // the resist synthesis and the adjoint.
+  for (int b = 0; b < batch; ++b) {
+    ep.target = d_targets + b * px;
+    ep.dldi = at<float>(ctx, L.dldi);
+    gp.grad_mask = d_grad_masks + b * px;
+    int nb = 0, nb2 = 0;
+    st = run_forward(ctx, *cache, f, L, 0, d_masks + b * px, nullptr, ep, &nb);
+    if (!st)
+      st = check_launch(ctx, launch_sum_partials(s, ctx->d_red + RED_PART, nb, 2,
+                                                 ctx->d_red + RED_SUM),
+                        "sum");
+    ctx->launches += 1;
+    if (!st) st = run_adjoint(ctx, *cache, f, L, at<float>(ctx, L.dldi), 4.0 * alpha, gp, &nb2);
+    if (!st) st = fetch(ctx, 2);
+    if (st) return st;
+    if (flag_set(ctx)) return ctx->fail(LITHO_ERR_NONFINITE, "mask must be finite");
+    if (losses) losses[b] = ctx->h_red[RED_SUM];
   }
   return LITHO_OK;
 }

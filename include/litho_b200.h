@@ -186,6 +186,17 @@ int litho_ctm_evaluate_batch(litho_ctx* ctx, const litho_cache* cache, int batch
                              const float* d_theta, const float* d_target, double threshold,
                              double alpha, float* d_grad_theta, double* losses, double* norms);
 
+/* Batched imaging + Gradient::pe_gradient (gradient.cpp:121-133) for the level-set
+ * path: `batch` binary or gray masks ([batch][N][N]) through imaging, the sigmoid
+ * resist and the PE loss against their targets, and dPE/dM of each into
+ * d_grad_masks (the normal speed of LSM_Optimizer). losses (host, nullable): the PE
+ * of each image. In LITHO_PRECISION_BF16X3 all images share one pass of the chain;
+ * in LITHO_PRECISION_FP32 they are evaluated one after another. Each image's results
+ * equal its own evaluation in a batch of one. */
+int litho_pe_gradient_batch(litho_ctx* ctx, const litho_cache* cache, int batch,
+                            const float* d_masks, const float* d_targets, double threshold,
+                            double alpha, float* d_grad_masks, double* losses);
+
 /* ------------------------------------------------------------ sparse EPE
  * Edge points (EPs) are chosen on the host (EpSelect, source/utils/ep_select.cpp);
  * eps is n x 2 host doubles (y, x) in subpixel image coordinates, weights n host
