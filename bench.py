@@ -53,6 +53,9 @@ def parse():
     p.add_argument("--batch", type=int, default=16,
                    help="tiles per step of the batched split-BF16 evaluation (the headline); "
                         "1 reports the single-tile chain")
+    p.add_argument("--serving-requests", type=int, default=24,
+                   help="LSM tile solves of the serving stream reported beside the headline "
+                        "(0 skips it)")
     return p.parse_args()
 
 
@@ -248,6 +251,42 @@ def run_reference(args):
            "latency_ms": {"p50": 1e3 * float(np.percentile(times, 50)),
                           "p99": 1e3 * float(np.percentile(times, 99))}}
     print(json.dumps(out), flush=True)
+
+
+def serving_run(L, K, requests, seed=7):
+    """The serving configuration at a bounded size: a seeded Poisson stream (mean 400
+    requests/s) of LSM tile solves of 20 iterations, tile sizes 256^2 / 512^2 / 1024^2 /
+    2048^2 in proportions 4:3:2:1, through the continuous-batching TileServer in
+    split-BF16 (16 solves per size batched, 120 GB HBM budget), and the same stream
+    through the plain FP32 one-tile-at-a-time loop (max_batch 1)."""
+    S = importlib.import_module("c-version-lithography_b200.serving")
+    wl = importlib.import_module("c-version-lithography_b200.workloads")
+    band, r0, c0, w, wss = wl.synthetic_socs_band(K=K)
+    sizes, props = [256, 512, 1024, 2048], [4, 3, 2, 1]
+
+    def make(N, rng):
+        t = wl.manhattan_target(N, max(4, N // 25), seed=int(rng.integers(1 << 30)))
+        return t, t
+
+    arrivals = S.poisson_arrivals(400.0, requests, sizes, props, make, 20, seed=seed)
+    out = {"workload": f"{requests} LSM tile solves x 20 iterations, Poisson 400 req/s, sizes "
+                       f"{sizes} in proportions 4:3:2:1, {K} SOCS kernels",
+           "initial_mask": "the target (binary)"}
+    for mode, max_batch in (("bf16x3", 16), ("fp32", 1)):
+        ctx = L.Context()
+        ctx.set_precision(mode)
+        caches = {N: L.ImagingCache.from_band(N, band, r0, c0, w, wss, ctx=ctx) for N in sizes}
+        warm = S.TileServer(caches, THRESHOLD, ALPHA, max_batch=max_batch)
+        for N in sizes:
+            t = wl.manhattan_target(N, 4, seed=N)
+            warm.submit(t, t, 2)
+        warm.drain()
+        srv = S.TileServer(caches, THRESHOLD, ALPHA, max_batch=max_batch, hbm_budget=120e9)
+        key = ("bf16x3_continuous_batching" if mode == "bf16x3" else "fp32_one_tile_at_a_time")
+        out[key] = srv.serve(arrivals)
+    a, b = out["bf16x3_continuous_batching"], out["fp32_one_tile_at_a_time"]
+    out["throughput_ratio"] = a["tile_iterations_per_s"] / b["tile_iterations_per_s"]
+    return out
 
 
 def config_dict(N, K, precision, tiles=1):
@@ -449,6 +488,8 @@ def run_ours(args):
         pm["bf16x3_over_fp32"] = pm["bf16x3"]["value"] / pm["fp32"]["value"]
         if head not in ("fp32", "bf16x3"):
             pm["batched_over_fp32"] = pm[head]["value"] / pm["fp32"]["value"]
+    if world == 1 and args.serving_requests > 0:
+        out["serving"] = serving_run(L, K, args.serving_requests)
     if world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(N, K, band, r0, c0, w, wss, target, theta,
                                            args.cpu_seconds)

@@ -106,6 +106,7 @@ SIGNATURES = {
     "litho_ctm_evaluate_host": (_I, [_P, _P, _P, _P, _P, _D, _D, _P, _PD, _PD]),
     "litho_ctm_evaluate_batch": (_I, [_P, _P, _I, _P, _P, _D, _D, _P, _PD, _PD]),
     "litho_pe_gradient_batch": (_I, [_P, _P, _I, _P, _P, _D, _D, _P, _PD]),
+    "litho_lsm_rk2_update_batch": (_I, [_P, _I, _I, _I, _P, _P, _D, _D, _D, _D, _P, _P, _PD]),
     "litho_weno_godunov": (_I, [_P, _I, _I, _P, _P, _D, _D, _P, _P]),
     "litho_kappa": (_I, [_P, _I, _I, _P, _D, _D, _D, _P]),
     "litho_evolution_term": (_I, [_P, _I, _I, _P, _P, _D, _D, _D, _D, _P, _PD]),
@@ -577,6 +578,27 @@ class LevelSetUtils:
         ctx._check(ctx.lib.litho_reinit_sdf(ctx.handle, p.shape[0], p.shape[1], _ptr(p), float(dx),
                                             float(dy), _ptr(out), _ptr(mask)))
         return (out, mask) if with_mask else out
+
+    @staticmethod
+    def rk2_update_batch(phi, Vn, dx, dy, cfl, b, phi_out, mask_out=None, ctx=None):
+        """rk2_update for a batch (batch, rows, cols) of images with one host round trip;
+        writes phi_out (and mask_out) and returns the per-image dt."""
+        ctx = ctx or default_context()
+        torch = ctx.torch
+        p = _f32(phi, torch)
+        if p.dim() != 3:
+            raise LithoError(2, "phi must be (batch, rows, cols)")
+        v = _f32(Vn, torch, tuple(p.shape), "Vn")
+        for t in (phi_out, mask_out):
+            if t is not None and (t.shape != p.shape or t.dtype != torch.float32
+                                  or not t.is_contiguous()):
+                raise LithoError(2, "outputs must be contiguous float32 shaped like phi")
+        B = p.shape[0]
+        dts = (ctypes.c_double * B)()
+        ctx._check(ctx.lib.litho_lsm_rk2_update_batch(
+            ctx.handle, B, p.shape[1], p.shape[2], _ptr(p), _ptr(v), float(dx), float(dy),
+            float(cfl), float(b), _ptr(phi_out), _ptr(mask_out), dts))
+        return list(dts)
 
     @staticmethod
     def rk2_update(phi, Vn, dx, dy, cfl, b, ctx=None):

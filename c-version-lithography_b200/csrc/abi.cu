@@ -1324,6 +1324,55 @@ int litho_lsm_rk2_update(litho_ctx* ctx, int rows, int cols, const float* d_phi,
   return LITHO_OK;
 }
 
+int litho_lsm_rk2_update_batch(litho_ctx* ctx, int batch, int rows, int cols, const float* d_phi,
+                               const float* d_vn, double dx, double dy, double cfl, double b,
+                               float* d_phi_out, float* d_mask, double* dts) {
+  if (!ctx || batch < 1 || !d_phi || !d_vn || !d_phi_out) return LITHO_ERR_INVALID_ARGUMENT;
+  if (d_phi_out == d_phi) return ctx->fail(LITHO_ERR_INVALID_ARGUMENT, "phi_out must not alias phi");
+  int st = ls_check(ctx, rows, cols, dx, dy, 3);
+  if (st) return st;
+  const size_t n = (size_t)rows * cols;
+  st = ctx->ensure_scratch(n * sizeof(float));
+  if (st) return st;
+  // Per-image (max |Vn|, dt) pairs after the reduction area of launch_dt.
+  constexpr size_t kDtPart = 2 * 600;
+  st = ctx->ensure_red(RED_PART + kDtPart + (size_t)batch + 8);
+  if (st) return st;
+  LITHO_CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_red, 0, RED_PART * sizeof(double), ctx->stream));
+  float* phi1 = static_cast<float*>(ctx->scratch.base);
+  float* part = reinterpret_cast<float*>(ctx->d_red + RED_PART);
+  float* vd = reinterpret_cast<float*>(ctx->d_red + RED_PART + kDtPart);   // [batch][2]
+  int* bad = reinterpret_cast<int*>(ctx->d_red + RED_FLAG);
+  cudaStream_t s = ctx->stream;
+  for (int i = 0; i < batch && !st; ++i) {
+    const float* phi = d_phi + i * n;
+    const float* vn = d_vn + i * n;
+    float* dtd = vd + 2 * i + 1;
+    st = check_launch(ctx, launch_dt(s, vn, n, (float)dx, (float)dy, (float)cfl, (float)b, part,
+                                     vd + 2 * i, dtd, bad),
+                      "dt");
+    if (!st)
+      st = check_launch(ctx, launch_levelset(s, 3, rows, cols, phi, nullptr, vn, (float)dx,
+                                             (float)dy, (float)b, dtd, phi1, nullptr),
+                        "rk2 stage 1");
+    if (!st)
+      st = check_launch(ctx, launch_levelset(s, 4, rows, cols, phi1, phi, vn, (float)dx, (float)dy,
+                                             (float)b, dtd, d_phi_out + i * n,
+                                             d_mask ? d_mask + i * n : nullptr),
+                        "rk2 stage 2");
+    ctx->launches += 4;
+  }
+  std::vector<float> h(2 * (size_t)batch);
+  if (!st)
+    LITHO_CUDA_TRY(ctx, cudaMemcpyAsync(h.data(), vd, h.size() * sizeof(float),
+                                        cudaMemcpyDeviceToHost, s));
+  if (!st) st = fetch(ctx, 0);
+  if (st) return st;
+  if (flag_set(ctx)) return ctx->fail(LITHO_ERR_NONFINITE, "normal speed must be finite");
+  for (int i = 0; i < batch && dts; ++i) dts[i] = h[2 * (size_t)i + 1];
+  return LITHO_OK;
+}
+
 }  // extern "C"
 
 // ============================================================== full chip

@@ -9,7 +9,8 @@ re-initialisation; the best (lowest PE) mask is kept.
 :class:`TileServer` keeps every admitted solve's phi, mask and target resident on
 the device and advances all of them together: each :meth:`TileServer.step` runs,
 per tile size, ONE batched imaging + gradient pass over every admitted solve of that
-size (``litho_pe_gradient_batch``), then each solve's level-set update. Requests
+size (``litho_pe_gradient_batch``), then one batched RK2 level-set update
+(``litho_lsm_rk2_update_batch``, each solve with its own CFL step). Requests
 that arrive while others run are admitted at the next step, as slots and the HBM
 budget allow; finished solves leave at once and free their slot. Because the
 batched pass computes every image exactly as it would alone, a solve's results do
@@ -60,6 +61,7 @@ class _SizeClass:
         N = cache.N
         self.cache = cache
         self.phi = torch.empty((slots, N, N), dtype=torch.float32, device="cuda")
+        self.phi_next = torch.empty_like(self.phi)
         self.mask = torch.empty_like(self.phi)
         self.target = torch.empty_like(self.phi)
         self.grad = torch.empty_like(self.phi)
@@ -167,14 +169,17 @@ class TileServer:
                 if pe < s.best_loss:
                     s.best_loss = pe
                     s.best_mask = cls.mask[i].clone()
+            # every solve's RK2 update, each with its own CFL step, in one call
+            LevelSetUtils.rk2_update_batch(cls.phi[:n], cls.grad[:n], self.dx, self.dy, self.cfl,
+                                           self.b, cls.phi_next[:n], cls.mask[:n], ctx=self.ctx)
+            cls.phi, cls.phi_next = cls.phi_next, cls.phi
+            for i, s in enumerate(cls.solves):
                 it = s.done_iterations
-                phi, mask, _ = LevelSetUtils.rk2_update(cls.phi[i], cls.grad[i], self.dx, self.dy,
-                                                        self.cfl, self.b, ctx=self.ctx)
                 if self.reinit_interval > 0 and it % self.reinit_interval == 0 and it > 0:
-                    phi, mask = LevelSetUtils.reinit_sdf(phi, self.dx, self.dy, ctx=self.ctx,
+                    phi, mask = LevelSetUtils.reinit_sdf(cls.phi[i], self.dx, self.dy, ctx=self.ctx,
                                                          with_mask=True)
-                cls.phi[i].copy_(phi)
-                cls.mask[i].copy_(mask)
+                    cls.phi[i].copy_(phi)
+                    cls.mask[i].copy_(mask)
                 s.done_iterations += 1
             self.tile_iterations += n
             for i in range(n - 1, -1, -1):

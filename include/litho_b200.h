@@ -246,6 +246,13 @@ int litho_reinit_sdf(litho_ctx* ctx, int rows, int cols, const float* d_phi, dou
 int litho_lsm_rk2_update(litho_ctx* ctx, int rows, int cols, const float* d_phi,
                          const float* d_vn, double dx, double dy, double cfl, double b,
                          float* d_phi_out, float* d_mask, double* dt);
+/* litho_lsm_rk2_update for `batch` images ([batch][rows][cols] phi, Vn, phi_out, mask),
+ * each with its own CFL dt (dts, host, nullable: one per image); the dt of each image
+ * stays on the device between its stages, so the whole batch costs one host
+ * round trip. phi_out must not alias phi. */
+int litho_lsm_rk2_update_batch(litho_ctx* ctx, int batch, int rows, int cols, const float* d_phi,
+                               const float* d_vn, double dx, double dy, double cfl, double b,
+                               float* d_phi_out, float* d_mask, double* dts);
 
 /* ------------------------------------------------------------ full chip
  * Partition (include/utils/partition.h, source/utils/partition.cpp:21-120): the

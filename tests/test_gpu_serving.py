@@ -4,6 +4,7 @@
   bit, and matches the single-image Imaging + Gradient.pe_gradient path within the
   split-BF16 tolerance (gradient relative L2 <= 1e-3, PE relative 1e-4); the FP32
   mode (one image after another) matches it within the FP32 tolerance (1e-4, 1e-5).
+* litho_lsm_rk2_update_batch: every image equals its own litho_lsm_rk2_update.
 * TileServer: a solve's results are the same alone and in a mix of other solves of
   other sizes that arrive while it runs (bit for bit); slot and HBM-budget admission;
   a seeded Poisson stream reports latency percentiles.
@@ -137,7 +138,7 @@ def test_server_first_iteration_matches_lsm_step(L, S, wl, setup):
     r = L.Imaging(cache).compute(m, THR, ALPHA)
     pe = L.Loss.pe_loss(r.wafer_image, tgt, ctx=ctx)
     assert abs(s.losses[0] - pe) <= 1e-4 * pe
-    phi0 =L.LevelSetUtils.reinit_sdf(m - 0.5, 1.0, 1.0, ctx=ctx)
+    phi0 = L.LevelSetUtils.reinit_sdf(m - 0.5, 1.0, 1.0, ctx=ctx)
     imaging = L.Imaging(cache)
     r = imaging.compute(m, THR, ALPHA)
     gm = L.Gradient(cache, THR, ALPHA).pe_gradient(r.wafer_image, tgt, imaging.get_electric_field())
@@ -179,3 +180,23 @@ def test_server_poisson_stream(L, S, wl, setup):
     assert st["requests"] == 12 and st["completed"] == 12
     assert st["latency_p99_s"] >= st["latency_p50_s"] > 0.0
     assert st["tile_iterations_per_s"] > 0.0
+
+
+def test_rk2_update_batch_equals_single(L, wl, setup):
+    """litho_lsm_rk2_update_batch: each image's phi, mask and dt equal those of
+    litho_lsm_rk2_update on that image alone (same kernels, one host round trip)."""
+    ctx, _, _ = setup
+    rng = np.random.default_rng(4)
+    B, n = 3, 96
+    m = torch.tensor(rng.random((B, n, n)) > 0.5, dtype=torch.float32, device="cuda")
+    phi = torch.stack([L.LevelSetUtils.reinit_sdf(m[b] - 0.5, 1.0, 1.0, ctx=ctx) for b in range(B)])
+    vn = torch.tensor(rng.standard_normal((B, n, n)) * (1.0 + np.arange(B))[:, None, None],
+                      dtype=torch.float32, device="cuda")
+    out, mask = torch.empty_like(phi), torch.empty_like(phi)
+    dts = L.LevelSetUtils.rk2_update_batch(phi, vn, 1.0, 1.0, 0.5, 0.01, out, mask, ctx=ctx)
+    for b in range(B):
+        p1, m1, dt = L.LevelSetUtils.rk2_update(phi[b], vn[b], 1.0, 1.0, 0.5, 0.01, ctx=ctx)
+        assert dts[b] == dt and torch.equal(out[b], p1) and torch.equal(mask[b], m1), b
+    assert len(set(dts)) == B      # each image its own CFL step
+    with pytest.raises(L.LithoError):
+        L.LevelSetUtils.rk2_update_batch(phi, vn, 1.0, 1.0, 0.5, 0.01, phi, mask, ctx=ctx)
