@@ -106,6 +106,7 @@ SIGNATURES = {
     "litho_ctm_evaluate_host": (_I, [_P, _P, _P, _P, _P, _D, _D, _P, _PD, _PD]),
     "litho_ctm_evaluate_batch": (_I, [_P, _P, _I, _P, _P, _D, _D, _P, _PD, _PD]),
     "litho_pe_gradient_batch": (_I, [_P, _P, _I, _P, _P, _D, _D, _P, _PD]),
+    "litho_ctm_evaluate_host_batch": (_I, [_P, _P, _I, _P, _P, _D, _D, _P, _PD, _PD]),
     "litho_lsm_rk2_update_batch": (_I, [_P, _I, _I, _I, _P, _P, _D, _D, _D, _D, _P, _P, _PD]),
     "litho_weno_godunov": (_I, [_P, _I, _I, _P, _P, _D, _D, _P, _P]),
     "litho_kappa": (_I, [_P, _I, _I, _P, _D, _D, _D, _P]),

@@ -225,6 +225,11 @@ int litho_ctx_destroy(litho_ctx* ctx) {
   for (cudaEvent_t e : ctx->ev_aux)
     if (e) cudaEventDestroy(e);
   if (ctx->aux) cudaStreamDestroy(ctx->aux);
+  if (ctx->pipe_stage.base) cudaFree(ctx->pipe_stage.base);
+  for (auto& slot : ctx->ev_pipe)
+    for (cudaEvent_t e : slot)
+      if (e) cudaEventDestroy(e);
+  if (ctx->dn) cudaStreamDestroy(ctx->dn);
   for (int i = 0; i < LITHO_NUM_STAGES; ++i)
     for (int j = 0; j < 2; ++j)
       if (ctx->ev[i][j]) cudaEventDestroy(ctx->ev[i][j]);
@@ -984,6 +989,41 @@ int litho_ctm_evaluate(litho_ctx* ctx, const litho_cache* cache, litho_field* fi
                            nullptr);
 }
 
+// The batched tensor-core chain on ctx->stream, without a host round trip: per
+// image {PE, penalty term, ||dPE/dtheta||^2} into d_sums ([batch][3], device). L
+// comes from prepare(ctx, c, &L, batch, true) (band state of every image included;
+// batch > 1 includes it anyway); the partials use the reduction area.
+static int ctm_batch_chain(Context* ctx, const Cache& c, const Layout& L, int batch,
+                           const float* d_theta, const float* d_target, double threshold,
+                           double alpha, float* d_grad_theta, double* d_sums) {
+  Field f;
+  f.cache = &c;
+  f.e = at<float2>(ctx, L.fe);
+  f.mband = at<float2>(ctx, L.fm);
+  ResistEpilogue ep{};
+  ep.mode = 1;
+  ep.thr = (float)threshold;
+  ep.alpha = (float)alpha;
+  ep.target = d_target;
+  ep.pe_weight = 1.f;
+  ep.penalty = 0.f;
+  ep.pen_thr = 0.01f;
+  ep.loss_partial = ctx->d_red + RED_PART;
+  int nb = 0, nb2 = 0;
+  int st = run_forward(ctx, c, f, L, 1, d_theta, nullptr, ep, &nb, nullptr, true, batch);
+  GradEpilogue gp{};
+  gp.theta = d_theta;
+  gp.grad_theta = d_grad_theta;
+  gp.norm_partial = ctx->d_red + RED_PART + 2 * (size_t)nb * batch;
+  if (!st) st = run_adjoint(ctx, c, f, L, nullptr, 4.0 * alpha, gp, &nb2, true, batch);
+  if (!st)
+    st = check_launch(ctx, launch_sum_partials_batch(ctx->stream, ctx->d_red + RED_PART, nb, 2,
+                                                     gp.norm_partial, nb2, 1, d_sums, batch),
+                      "sum");
+  ctx->launches += 1;
+  return st;
+}
+
 int litho_ctm_evaluate_batch(litho_ctx* ctx, const litho_cache* cache, int batch,
                              const float* d_theta, const float* d_target, double threshold,
                              double alpha, float* d_grad_theta, double* losses, double* norms) {
@@ -1010,32 +1050,9 @@ int litho_ctm_evaluate_batch(litho_ctx* ctx, const litho_cache* cache, int batch
   Layout L;
   int st = prepare(ctx, *cache, &L, batch);
   if (st) return st;
-  Field f;
-  f.cache = cache;
-  f.e = at<float2>(ctx, L.fe);
-  f.mband = at<float2>(ctx, L.fm);
-  ResistEpilogue ep{};
-  ep.mode = 1;
-  ep.thr = (float)threshold;
-  ep.alpha = (float)alpha;
-  ep.target = d_target;
-  ep.pe_weight = 1.f;
-  ep.penalty = 0.f;
-  ep.pen_thr = 0.01f;
-  ep.loss_partial = ctx->d_red + RED_PART;
-  int nb = 0, nb2 = 0;
-  st = run_forward(ctx, *cache, f, L, 1, d_theta, nullptr, ep, &nb, nullptr, true, batch);
-  GradEpilogue gp{};
-  gp.theta = d_theta;
-  gp.grad_theta = d_grad_theta;
-  gp.norm_partial = ctx->d_red + RED_PART + 2 * (size_t)nb * batch;
-  if (!st) st = run_adjoint(ctx, *cache, f, L, nullptr, 4.0 * alpha, gp, &nb2, true, batch);
-  double* d_sums = gp.norm_partial + (size_t)nb2 * batch;
-  if (!st)
-    st = check_launch(ctx, launch_sum_partials_batch(ctx->stream, ctx->d_red + RED_PART, nb, 2,
-                                                     gp.norm_partial, nb2, 1, d_sums, batch),
-                      "sum");
-  ctx->launches += 1;
+  double* d_sums = ctx->d_red + RED_PART + 3 * (size_t)L.tiles * batch;
+  st = ctm_batch_chain(ctx, *cache, L, batch, d_theta, d_target, threshold, alpha, d_grad_theta,
+                       d_sums);
   std::vector<double> sums(3 * (size_t)batch);
   if (!st)
     LITHO_CUDA_TRY(ctx, cudaMemcpyAsync(sums.data(), d_sums, sums.size() * sizeof(double),
@@ -1173,6 +1190,127 @@ int litho_ctm_evaluate_host(litho_ctx* ctx, const litho_cache* cache, litho_fiel
   if (cudaStreamSynchronize(ctx->aux) != cudaSuccess && !st)
     st = ctx->fail(LITHO_ERR_CUDA, "upload stream synchronize failed");
   return st;
+}
+
+int litho_ctm_evaluate_host_batch(litho_ctx* ctx, const litho_cache* cache, int batch,
+                                  const float* h_theta, const float* h_target, double threshold,
+                                  double alpha, float* h_grad_theta, double* losses,
+                                  double* norms) {
+  if (!ctx || !cache || batch < 1 || !h_theta || !h_target || !h_grad_theta)
+    return LITHO_ERR_INVALID_ARGUMENT;
+  if (!std::isfinite(threshold) || !std::isfinite(alpha))
+    return ctx->fail(LITHO_ERR_NONFINITE, "Imaging: mask, threshold, and alpha must be finite");
+  const size_t n = (size_t)cache->g.N * cache->g.N;
+  const bool tc = ctx->precision == LITHO_PRECISION_BF16X3 && cache->TXD_img != nullptr;
+  if (!tc) {
+    // FP32 parity mode: the single-image host call, image after image.
+    for (int b = 0; b < batch; ++b) {
+      double lo = 0.0, no = 0.0;
+      const int st = litho_ctm_evaluate_host(ctx, cache, nullptr, h_theta + b * n,
+                                             h_target + b * n, threshold, alpha,
+                                             h_grad_theta + b * n, &lo, &no);
+      if (st) return st;
+      if (losses) losses[b] = lo;
+      if (norms) norms[b] = no;
+    }
+    return LITHO_OK;
+  }
+  if (cudaSetDevice(ctx->device) != cudaSuccess) return LITHO_ERR_CUDA;
+  // Groups of G images through two device slots: the upload of group g + 1, the
+  // batched chain of group g and the download of group g - 1 run on three streams.
+  // Large images are link-bound (a 2048^2 image takes about 0.6 ms to upload and
+  // 0.13 ms to evaluate alone): one per group keeps the pipeline's fill and drain
+  // short. Small ones are grouped so that the chain keeps up with the copies.
+  const int G = std::min(batch, cache->g.N >= 1024 ? 1 : 4);
+  const int ngroups = (batch + G - 1) / G;
+  const size_t slot_floats = 3 * (size_t)G * n;                 // theta | target | gradient
+  const size_t need = 2 * slot_floats * sizeof(float) + 3 * (size_t)batch * sizeof(double);
+  if (ctx->pipe_stage.bytes < need) {
+    cudaStreamSynchronize(ctx->stream);
+    if (ctx->dn) cudaStreamSynchronize(ctx->dn);
+    if (ctx->pipe_stage.base) cudaFree(ctx->pipe_stage.base);
+    ctx->pipe_stage.base = nullptr;
+    ctx->pipe_stage.bytes = 0;
+    if (cudaMalloc(&ctx->pipe_stage.base, need) != cudaSuccess) {
+      cudaGetLastError();
+      return ctx->fail(LITHO_ERR_OOM, "host-batch staging allocation failed");
+    }
+    ctx->pipe_stage.bytes = need;
+  }
+  if (!ctx->aux) {
+    if (cudaStreamCreateWithFlags(&ctx->aux, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ctx->ev_aux[0], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ctx->ev_aux[1], cudaEventDisableTiming) != cudaSuccess) {
+      cudaGetLastError();
+      return ctx->fail(LITHO_ERR_CUDA, "upload stream creation failed");
+    }
+  }
+  if (!ctx->dn) {
+    bool ok = cudaStreamCreateWithFlags(&ctx->dn, cudaStreamNonBlocking) == cudaSuccess;
+    for (auto& slot : ctx->ev_pipe)
+      for (cudaEvent_t& e : slot)
+        ok = ok && cudaEventCreateWithFlags(&e, cudaEventDisableTiming) == cudaSuccess;
+    if (!ok) {
+      cudaGetLastError();
+      return ctx->fail(LITHO_ERR_CUDA, "download stream creation failed");
+    }
+  }
+  Layout L;
+  int st = prepare(ctx, *cache, &L, G, true);   // with the band state of G images
+  if (st) return st;
+  float* base = static_cast<float*>(ctx->pipe_stage.base);
+  double* d_sums = reinterpret_cast<double*>(base + 2 * slot_floats);
+  cudaStream_t up = ctx->aux, cp = ctx->stream, dn = ctx->dn;
+  enum { UP = 0, CP = 1, DN = 2 };
+  // The uploads must not start before work already queued on the compute stream.
+  if (cudaEventRecord(ctx->ev_aux[0], cp) != cudaSuccess ||
+      cudaStreamWaitEvent(up, ctx->ev_aux[0], 0) != cudaSuccess)
+    st = ctx->fail(LITHO_ERR_CUDA, "stream ordering failed");
+  for (int g = 0; g < ngroups && !st; ++g) {
+    const int s = g & 1;
+    const int t0 = g * G, m = batch - t0 < G ? batch - t0 : G;
+    float* th = base + s * slot_floats;
+    float* tg = th + (size_t)G * n;
+    float* gr = tg + (size_t)G * n;
+    cudaEvent_t* ev = ctx->ev_pipe[s];
+    bool ok = true;
+    if (g >= 2) ok = cudaStreamWaitEvent(up, ev[CP], 0) == cudaSuccess;   // slot's inputs read
+    ok = ok && cudaMemcpyAsync(th, h_theta + t0 * n, m * n * sizeof(float),
+                               cudaMemcpyHostToDevice, up) == cudaSuccess;
+    ok = ok && cudaMemcpyAsync(tg, h_target + t0 * n, m * n * sizeof(float),
+                               cudaMemcpyHostToDevice, up) == cudaSuccess;
+    ok = ok && cudaEventRecord(ev[UP], up) == cudaSuccess;
+    ok = ok && cudaStreamWaitEvent(cp, ev[UP], 0) == cudaSuccess;
+    if (g >= 2) ok = ok && cudaStreamWaitEvent(cp, ev[DN], 0) == cudaSuccess;   // slot's gradients out
+    if (!ok) {
+      st = ctx->fail(LITHO_ERR_CUDA, "host batch: copy scheduling failed");
+      break;
+    }
+    st = ctm_batch_chain(ctx, *cache, L, m, th, tg, threshold, alpha, gr, d_sums + 3 * (size_t)t0);
+    if (st) break;
+    ok = cudaEventRecord(ev[CP], cp) == cudaSuccess &&
+         cudaStreamWaitEvent(dn, ev[CP], 0) == cudaSuccess &&
+         cudaMemcpyAsync(h_grad_theta + t0 * n, gr, m * n * sizeof(float), cudaMemcpyDeviceToHost,
+                         dn) == cudaSuccess &&
+         cudaEventRecord(ev[DN], dn) == cudaSuccess;
+    if (!ok) st = ctx->fail(LITHO_ERR_CUDA, "host batch: download failed");
+  }
+  std::vector<double> sums(3 * (size_t)batch);
+  if (!st)
+    LITHO_CUDA_TRY(ctx, cudaMemcpyAsync(sums.data(), d_sums, sums.size() * sizeof(double),
+                                        cudaMemcpyDeviceToHost, cp));
+  if (cudaStreamSynchronize(dn) != cudaSuccess && !st)
+    st = ctx->fail(LITHO_ERR_CUDA, "download stream synchronize failed");
+  if (cudaStreamSynchronize(up) != cudaSuccess && !st)
+    st = ctx->fail(LITHO_ERR_CUDA, "upload stream synchronize failed");
+  if (!st) st = fetch(ctx, 0);
+  if (st) return st;
+  if (flag_set(ctx)) return ctx->fail(LITHO_ERR_NONFINITE, "theta must be finite");
+  for (int b = 0; b < batch; ++b) {
+    if (losses) losses[b] = sums[3 * (size_t)b];
+    if (norms) norms[b] = std::sqrt(sums[3 * (size_t)b + 2]);
+  }
+  return LITHO_OK;
 }
 
 int litho_field_export(litho_ctx* ctx, const litho_field* field, int k, float* d_E) {

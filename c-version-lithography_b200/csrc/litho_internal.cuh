@@ -116,6 +116,11 @@ struct Context {
   Scratch host_stage;            // device staging of the host-buffer entry points
   cudaStream_t aux = nullptr;    // upload stream of the host-buffer entry points
   cudaEvent_t ev_aux[2] = {};    // [0] theta uploaded (main stream), [1] target uploaded (aux)
+  // Pipelined host-buffer batches: download stream and per-slot events (uploaded,
+  // computed, downloaded) of the two device staging slots.
+  Scratch pipe_stage;
+  cudaStream_t dn = nullptr;
+  cudaEvent_t ev_pipe[2][3] = {};
   // CUDA graph of the last repeated CTM evaluation (litho_ctm_evaluate): captured
   // on the second consecutive call with the same key, replayed while it stays.
   bool graphs = true;

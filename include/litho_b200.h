@@ -197,6 +197,17 @@ int litho_pe_gradient_batch(litho_ctx* ctx, const litho_cache* cache, int batch,
                             const float* d_masks, const float* d_targets, double threshold,
                             double alpha, float* d_grad_masks, double* losses);
 
+/* litho_ctm_evaluate_batch through host buffers ([batch][N][N] theta, target and
+ * h_grad_theta): in LITHO_PRECISION_BF16X3 the images go through in groups whose
+ * uploads, batched evaluation and downloads overlap on three streams, so the call
+ * is bound by the host link rather than by the sum of copies and compute; pass
+ * page-locked (pinned) host buffers, or the copies cannot overlap. In
+ * LITHO_PRECISION_FP32 it calls litho_ctm_evaluate_host image after image. */
+int litho_ctm_evaluate_host_batch(litho_ctx* ctx, const litho_cache* cache, int batch,
+                                  const float* h_theta, const float* h_target, double threshold,
+                                  double alpha, float* h_grad_theta, double* losses,
+                                  double* norms);
+
 /* ------------------------------------------------------------ sparse EPE
  * Edge points (EPs) are chosen on the host (EpSelect, source/utils/ep_select.cpp);
  * eps is n x 2 host doubles (y, x) in subpixel image coordinates, weights n host

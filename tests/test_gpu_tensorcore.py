@@ -150,3 +150,32 @@ def test_batched_evaluation_fp32_and_errors(L, wl):
         L.ctm_evaluate_batch(cache, bad, tg, 0.225, 50.0)
     assert e.value.status == 3
     ctx.close()
+
+
+@pytest.mark.parametrize("N,B,pinned", [(256, 6, True), (256, 6, False), (1024, 3, True)])
+def test_host_batch_equals_device_batch(L, wl, tc_ctx, N, B, pinned):
+    """litho_ctm_evaluate_host_batch (groups through two staging slots, copies and
+    compute overlapped on three streams: four small images per group, ending here in a
+    partial group, or one large image per group) returns exactly what the
+    device-buffer batch returns."""
+    import ctypes
+    band, r0, c0, w, wss = wl.synthetic_socs_band()
+    cache = L.ImagingCache.from_band(N, band, r0, c0, w, wss, ctx=tc_ctx)
+    rng = np.random.default_rng(11)
+    tg = np.stack([wl.manhattan_target(N, 10, seed=40 + b) for b in range(B)]).astype(np.float32)
+    th = (np.stack([wl.theta_init_reference(t) for t in tg])
+          + 0.2 * rng.standard_normal((B, N, N))).astype(np.float32)
+    losses, grads, norms = L.ctm_evaluate_batch(cache, torch.tensor(th, device="cuda"),
+                                                torch.tensor(tg, device="cuda"), 0.225, 50.0)
+    h_th, h_tg = torch.tensor(th), torch.tensor(tg)
+    h_gr = torch.empty((B, N, N), dtype=torch.float32)
+    if pinned:
+        h_th, h_tg, h_gr = h_th.pin_memory(), h_tg.pin_memory(), h_gr.pin_memory()
+    lo = (ctypes.c_double * B)()
+    no = (ctypes.c_double * B)()
+    for _ in range(2):          # the second call reuses the staging slots and streams
+        tc_ctx._check(tc_ctx.lib.litho_ctm_evaluate_host_batch(
+            tc_ctx.handle, cache.handle, B, h_th.data_ptr(), h_tg.data_ptr(), 0.225, 50.0,
+            h_gr.data_ptr(), lo, no))
+        assert list(lo) == losses and list(no) == norms
+        assert torch.equal(h_gr, grads.cpu())
