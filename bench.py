@@ -53,6 +53,10 @@ def parse():
     p.add_argument("--batch", type=int, default=16,
                    help="tiles per step of the batched split-BF16 evaluation (the headline); "
                         "1 reports the single-tile chain")
+    p.add_argument("--fullchip-size", type=int, default=16384,
+                   help="layout size of the full-chip CTM leg (0: skip it)")
+    p.add_argument("--fullchip-grid", type=int, default=16,
+                   help="micro tiles per side of the full-chip layout")
     p.add_argument("--serving-requests", type=int, default=24,
                    help="LSM tile solves of the serving stream reported beside the headline "
                         "(0 skips it)")
@@ -289,6 +293,52 @@ def serving_run(L, K, requests, seed=7):
     return out
 
 
+def fullchip_run(L, K, size, grid, halo, guard, iterations=3, seed=11):
+    """Full-chip CTM at the batched full-chip configuration's scale: a size x size
+    layout (2 nm pixels, seeded rectangles at about 34 % density) cut into grid x grid
+    micro tiles (Core size / grid plus a `halo` pixel halo on every side), one
+    FullChipCTMOptimizer run of `iterations` steps (each the exchange: imaging, windowed
+    PE loss, adjoint of every tile, CEPT and neighbour gradient fusion, then the
+    windowed theta step). Split-BF16 images the tiles in batched groups; the plain
+    FP32 mode one tile after another. Timed on the wall clock around the run (the
+    exchange returns its losses to the host every iteration)."""
+    import torch
+    FC = importlib.import_module("c-version-lithography_b200.fullchip")
+    wl = importlib.import_module("c-version-lithography_b200.workloads")
+    band, r0, c0, w, wss = wl.synthetic_socs_band(K=K)
+    layout = torch.from_numpy(wl.cell_layout(size, size, seed)).cuda()
+    gopt = FC.MicroGradientOptions(enable_cept=True, enable_grad_fusion=True)
+    out = {"workload": f"full-chip CTM, {size}^2 layout (2 nm pixels, ~34% density), "
+                       f"{grid}x{grid} micro tiles, halo {halo}, guard {guard}, CEPT + "
+                       f"average gradient fusion, {iterations} steps + the initial exchange, "
+                       f"{K} SOCS kernels"}
+    for mode in ("bf16x3", "fp32"):
+        ctx = L.Context()
+        ctx.set_precision(mode)
+        part = FC.Partition(size, size, grid, grid, halo, guard, ctx=ctx)
+        cache = L.ImagingCache.from_band(part.tile_size, band, r0, c0, w, wss, ctx=ctx)
+        opt = FC.FullChipCTMOptimizer(part, cache, THRESHOLD, ALPHA)
+        opt.optimize(layout, FC.FullChipCTMOptions(iterations=1, gradient_options=gopt))  # warm-up
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        res = opt.optimize(layout, FC.FullChipCTMOptions(iterations=iterations,
+                                                         gradient_options=gopt))
+        torch.cuda.synchronize()
+        sec = time.perf_counter() - t0
+        evals = part.num_tiles * (iterations + 1)
+        out[mode] = {"tile_size": part.tile_size, "tiles": part.num_tiles, "seconds": sec,
+                     "tile_iterations_per_s": evals / sec,
+                     "layout_mpx_per_s": (iterations + 1) * size * size / sec / 1e6,
+                     "final_loss": res.history[-1].loss, "initial_loss": res.history[0].loss}
+        del opt, res
+        part.close()
+        ctx.close()
+        torch.cuda.empty_cache()
+    out["batched_bf16x3_over_fp32"] = (out["bf16x3"]["tile_iterations_per_s"] /
+                                       out["fp32"]["tile_iterations_per_s"])
+    return out
+
+
 def config_dict(N, K, precision, tiles=1):
     what = "one" if tiles == 1 else f"a batch of {tiles}"
     return {"workload": f"CTM objective evaluation (forward + adjoint) on {what} {N}^2 tile"
@@ -506,6 +556,8 @@ def run_ours(args):
             pm["batched_over_fp32"] = pm[head]["value"] / pm["fp32"]["value"]
     if world == 1 and args.serving_requests > 0:
         out["serving"] = serving_run(L, K, args.serving_requests)
+    if world == 1 and args.fullchip_size > 0:
+        out["fullchip"] = fullchip_run(L, K, args.fullchip_size, args.fullchip_grid, 128, 32)
     if world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(N, K, band, r0, c0, w, wss, target, theta,
                                            args.cpu_seconds)

@@ -650,7 +650,7 @@ int run_adjoint(Context* ctx, const Cache& c, const Field& f, const Layout& L, c
   else if (tc)
     st = check_launch(ctx, launch_analysis_tc2(s, 0, dldi, nullptr, flag, g.N, g.Nc, na, g.Nr, 1,
                                                at<float2>(ctx, L.part), c.TXD_img, c.TYD_img,
-                                               flag + 1),
+                                               flag + 1, batch),
                       "tensor-core adjoint tile analysis");
   else
     st = check_launch(ctx, launch_analysis(s, 0, dldi, nullptr, flag, c.TXD, g.N, g.Nc, c.TYD, na,
@@ -1702,6 +1702,10 @@ int litho_partition_assemble(litho_ctx* ctx, const litho_partition* p, const flo
                       "tile assembly");
 }
 
+// Tiles per batched pass of the exchange (tensor-core path): enough to fill the GPU
+// at 1024-2048 pixel tiles, with the group's scratch a few hundred MB at most.
+constexpr int kExchangeGroup = 16;
+
 int litho_exchange_compute_epe(litho_ctx* ctx, const litho_partition* cp, const litho_cache* cache,
                                const float* d_masks, const float* d_global_target, double threshold,
                                double alpha, const litho_exchange_options* opt,
@@ -1737,15 +1741,21 @@ int litho_exchange_compute_epe(litho_ctx* ctx, const litho_partition* cp, const 
     return ctx->fail(LITHO_ERR_SHAPE, "MicroGradientExchange: cache N must equal the tile size");
   if (d_raw && d_raw == d_grad)
     return ctx->fail(LITHO_ERR_INVALID_ARGUMENT, "raw and exchanged gradients must not alias");
-  Layout L;
-  int st = prepare(ctx, *cache, &L);
-  if (st) return st;
   const int n = p->ntiles, ts = p->ts;
   const size_t tt = (size_t)ts * ts;
   const int S = litho_partition::kSlots;
   const bool epe_terms = o.loss_type == LITHO_MICRO_LOSS_EPE || o.loss_type == LITHO_MICRO_LOSS_PE_EPE;
   const bool core = e.collect_core_metrics != 0;
   const bool eval_epe = epe_terms || core;   // micro_gradient_exchange.cpp:144-148
+  // Tensor-core path: the tiles go through the imaging + adjoint chain in groups of
+  // kExchangeGroup, one batched pass per group (the EP work stays per tile between
+  // the forward and the adjoint pass).
+  const bool batched = ctx->precision == LITHO_PRECISION_BF16X3 && cache->TXD_img != nullptr &&
+                       n > 1;
+  const int group = batched ? std::min(n, kExchangeGroup) : 1;
+  Layout L;
+  int st = prepare(ctx, *cache, &L, group, batched);
+  if (st) return st;
   const bool guard_region = o.loss_region == LITHO_MICRO_REGION_CORE_GUARD;
   const int periods = guard_region ? 1 : 0;
   const size_t ncand = (size_t)e.n_eps * (2 * periods + 1) * (2 * periods + 1);
@@ -1759,7 +1769,9 @@ int litho_exchange_compute_epe(litho_ctx* ctx, const litho_partition* cp, const 
     }
     p->h_loss.assign((size_t)(S + 1) * n, 0.0);
   }
-  const size_t epe_work_n = eval_epe ? (3 * n + 2) * tt : 0;
+  // EP work: EPE window, main region, dilation scratch (n tiles each), then the
+  // aerial and wafer images and the dL/dI of a group of tiles.
+  const size_t epe_work_n = eval_epe ? (3 * (size_t)n + 3 * (size_t)group) * tt : 0;
   const size_t ep_n = eval_epe ? 3 * ((size_t)e.n_eps + ncand) : 0;
   if (p->epe_work_n < epe_work_n || p->ep_n < ep_n) {
     LITHO_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
@@ -1809,7 +1821,8 @@ int litho_exchange_compute_epe(litho_ctx* ctx, const litho_partition* cp, const 
   float* main_dil = eval_epe ? epe_w + n * tt : nullptr;
   float* dil_tmp = eval_epe ? main_dil + n * tt : nullptr;
   float* aerial = eval_epe ? dil_tmp + n * tt : nullptr;
-  float* wafer = eval_epe ? aerial + tt : nullptr;
+  float* wafer = eval_epe ? aerial + group * tt : nullptr;
+  float* dldi_group = eval_epe ? wafer + group * tt : nullptr;
   double* ep_in = p->d_ep;                                   // 2 n_eps coordinates | n_eps weights
   double* cand = eval_epe ? ep_in + 3 * (size_t)e.n_eps : nullptr;   // 2 ncand | ncand
   Field f;
@@ -1857,10 +1870,102 @@ int litho_exchange_compute_epe(litho_ctx* ctx, const litho_partition* cp, const 
       zero_pe_dldi = true;
     }
   }
-  for (int t = 0; t < n && !st; ++t) {
+  // Per-tile EP work after the forward pass of tile t (aerial / wafer images and dL/dI
+  // of that tile at the given pointers): loss-region EPs (periodic copies with a
+  // Core + Guard region) give the EPE sums and, for the EPE types, the scatter of
+  // their dL/dI; with the Core metrics, the loss-region and Core sums from the wafer
+  // image and the Core EPs without copies.
+  auto ep_work = [&](int t, const float* aer, const float* waf, float* dl) -> int {
     const int* R = &p->rects[16 * (size_t)t];   // core_global | tile_global | core_local | update_local
     const int* region = guard_region ? R + 12 : R + 8;
     const int oy = R[4], ox = R[6];
+    double* slot = p->d_loss + (size_t)S * t;
+    const int grect[4] = {region[0] + oy, region[1] + oy, region[2] + ox, region[3] + ox};
+    int used = 0;
+    int r = check_launch(ctx, launch_ep_candidates(s, ep_in, ep_in + 2 * (size_t)e.n_eps, e.n_eps,
+                                                   periods, p->height, p->width, oy, ox, grect, ts,
+                                                   epe_w + t * tt, cand, cand + 2 * ncand),
+                         "EP candidates");
+    if (!r)
+      r = check_launch(ctx, launch_epe(s, aer, ts, ts, cand, cand + 2 * ncand, (int)ncand,
+                                       threshold, e.epe_pixel_size, nullptr, part,
+                                       epe_grad ? dl : nullptr, epe_fac, &used),
+                       "sparse EPE");
+    if (!r) r = check_launch(ctx, launch_sum_partials(s, part, used, 3, slot + 2), "sum");
+    ctx->launches += 3;
+    if (r || !core) return r;
+    r = check_launch(ctx, launch_rect_losses(s, waf, targets + t * tt, pe_w + t * tt,
+                                             pen_w + t * tt, ts, region,
+                                             (float)o.penalty_threshold, part, &used),
+                     "region losses");
+    if (!r) r = check_launch(ctx, launch_sum_partials(s, part, used, 3, slot + 5), "sum");
+    if (!r)
+      r = check_launch(ctx, launch_rect_losses(s, waf, targets + t * tt, pe_w + t * tt,
+                                               pen_w + t * tt, ts, R + 8,
+                                               (float)o.penalty_threshold, part, &used),
+                       "core losses");
+    if (!r) r = check_launch(ctx, launch_sum_partials(s, part, used, 3, slot + 8), "sum");
+    const int crect[4] = {R[0], R[1], R[2], R[3]};   // core_global
+    if (!r)
+      r = check_launch(ctx, launch_ep_candidates(s, ep_in, ep_in + 2 * (size_t)e.n_eps, e.n_eps,
+                                                 0, p->height, p->width, oy, ox, crect, ts,
+                                                 epe_w + t * tt, cand, cand + 2 * ncand),
+                       "core EP candidates");
+    if (!r)
+      r = check_launch(ctx, launch_epe(s, aer, ts, ts, cand, cand + 2 * ncand, e.n_eps, threshold,
+                                       e.epe_pixel_size, nullptr, part, nullptr, 0.0, &used),
+                       "core sparse EPE");
+    if (!r) r = check_launch(ctx, launch_sum_partials(s, part, used, 3, slot + 11), "sum");
+    ctx->launches += 8;
+    return r;
+  };
+  // With an EPE gradient the adjoint needs dL/dI after the EP scatter, so the resist
+  // synthesis stores it; otherwise it stays on chip (fused adjoint tile analysis).
+  const bool fuse = !epe_grad;
+  for (int t0 = 0; batched && t0 < n && !st; t0 += group) {
+    // Tiles t0 .. t0 + B - 1 in one pass: windows and penalty in the resist epilogue,
+    // raw gradients straight to their slots, per-tile {PE, penalty} sums to the
+    // first two loss slots.
+    const int B = std::min(group, n - t0);
+    Field fb;
+    fb.cache = cache;
+    fb.e = at<float2>(ctx, L.fe);
+    fb.mband = at<float2>(ctx, L.fm);
+    ResistEpilogue ep{};
+    ep.mode = 1;
+    ep.thr = (float)threshold;
+    ep.alpha = (float)alpha;
+    ep.aerial = eval_epe ? aerial : nullptr;
+    ep.wafer = core ? wafer : nullptr;
+    ep.target = targets + t0 * tt;
+    ep.pe_window = pe_w + t0 * tt;
+    ep.pen_window = pen_w + t0 * tt;
+    ep.pe_weight = (float)wpe;
+    ep.penalty = (float)wpen;
+    ep.pen_thr = (float)o.penalty_threshold;
+    ep.dldi = fuse ? nullptr : dldi_group;
+    ep.loss_partial = part;
+    int nb = 0, nb2 = 0;
+    st = run_forward(ctx, *cache, fb, L, 0, d_masks + t0 * tt, nullptr, ep, &nb, nullptr, fuse, B);
+    double* sums = part + 2 * (size_t)nb * B;
+    if (!st)
+      st = check_launch(ctx, launch_sum_partials_batch(s, part, nb, 2, part, 0, 0, sums, B), "sum");
+    ctx->launches += 1;
+    if (!st)
+      LITHO_CUDA_TRY(ctx, cudaMemcpy2DAsync(p->d_loss + (size_t)S * t0, S * sizeof(double), sums,
+                                            2 * sizeof(double), 2 * sizeof(double), B,
+                                            cudaMemcpyDeviceToDevice, s));
+    if (!st && zero_pe_dldi)
+      LITHO_CUDA_TRY(ctx, cudaMemsetAsync(dldi_group, 0, B * tt * sizeof(float), s));
+    for (int b = 0; eval_epe && b < B && !st; ++b)
+      st = ep_work(t0 + b, aerial + b * tt, core ? wafer + b * tt : nullptr,
+                   fuse ? nullptr : dldi_group + b * tt);
+    GradEpilogue gp{};
+    gp.grad_mask = raw + t0 * tt;
+    if (!st)
+      st = run_adjoint(ctx, *cache, fb, L, fuse ? nullptr : dldi_group, adj_scale, gp, &nb2, fuse, B);
+  }
+  for (int t = 0; !batched && t < n && !st; ++t) {
     ResistEpilogue ep{};
     ep.mode = 1;
     ep.thr = (float)threshold;
@@ -1881,51 +1986,7 @@ int litho_exchange_compute_epe(litho_ctx* ctx, const litho_partition* cp, const 
     if (!st) st = check_launch(ctx, launch_sum_partials(s, part, nb, 2, slot), "sum");
     ctx->launches += 1;
     if (!st && zero_pe_dldi) LITHO_CUDA_TRY(ctx, cudaMemsetAsync(dldi, 0, tt * sizeof(float), s));
-    if (!st && eval_epe) {
-      // Loss-region EPs (periodic copies with a Core + Guard region): EPE sums and,
-      // for the EPE types, the scatter of their dL/dI.
-      const int grect[4] = {region[0] + oy, region[1] + oy, region[2] + ox, region[3] + ox};
-      int used = 0;
-      st = check_launch(ctx, launch_ep_candidates(s, ep_in, ep_in + 2 * (size_t)e.n_eps, e.n_eps,
-                                                  periods, p->height, p->width, oy, ox, grect, ts,
-                                                  epe_w + t * tt, cand, cand + 2 * ncand),
-                        "EP candidates");
-      if (!st)
-        st = check_launch(ctx, launch_epe(s, aerial, ts, ts, cand, cand + 2 * ncand, (int)ncand,
-                                          threshold, e.epe_pixel_size, nullptr, part,
-                                          epe_grad ? dldi : nullptr, epe_fac, &used),
-                          "sparse EPE");
-      if (!st) st = check_launch(ctx, launch_sum_partials(s, part, used, 3, slot + 2), "sum");
-      ctx->launches += 3;
-    }
-    if (!st && core) {
-      // Loss-region and Core sums from the wafer image; Core EPs without copies.
-      int used = 0;
-      st = check_launch(ctx, launch_rect_losses(s, wafer, targets + t * tt, pe_w + t * tt,
-                                                pen_w + t * tt, ts, region,
-                                                (float)o.penalty_threshold, part, &used),
-                        "region losses");
-      if (!st) st = check_launch(ctx, launch_sum_partials(s, part, used, 3, slot + 5), "sum");
-      if (!st)
-        st = check_launch(ctx, launch_rect_losses(s, wafer, targets + t * tt, pe_w + t * tt,
-                                                  pen_w + t * tt, ts, R + 8,
-                                                  (float)o.penalty_threshold, part, &used),
-                          "core losses");
-      if (!st) st = check_launch(ctx, launch_sum_partials(s, part, used, 3, slot + 8), "sum");
-      const int crect[4] = {R[0], R[1], R[2], R[3]};   // core_global
-      if (!st)
-        st = check_launch(ctx, launch_ep_candidates(s, ep_in, ep_in + 2 * (size_t)e.n_eps, e.n_eps,
-                                                    0, p->height, p->width, oy, ox, crect, ts,
-                                                    epe_w + t * tt, cand, cand + 2 * ncand),
-                          "core EP candidates");
-      if (!st)
-        st = check_launch(ctx, launch_epe(s, aerial, ts, ts, cand, cand + 2 * ncand, e.n_eps,
-                                          threshold, e.epe_pixel_size, nullptr, part, nullptr, 0.0,
-                                          &used),
-                          "core sparse EPE");
-      if (!st) st = check_launch(ctx, launch_sum_partials(s, part, used, 3, slot + 11), "sum");
-      ctx->launches += 8;
-    }
+    if (!st && eval_epe) st = ep_work(t, aerial, wafer, dldi);
     GradEpilogue gp{};
     gp.grad_mask = raw + t * tt;
     int nb2 = 0;
