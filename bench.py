@@ -293,49 +293,106 @@ def serving_run(L, K, requests, seed=7):
     return out
 
 
-def fullchip_run(L, K, size, grid, halo, guard, iterations=3, seed=11):
-    """Full-chip CTM at the batched full-chip configuration's scale: a size x size
-    layout (2 nm pixels, seeded rectangles at about 34 % density) cut into grid x grid
-    micro tiles (Core size / grid plus a `halo` pixel halo on every side), one
-    FullChipCTMOptimizer run of `iterations` steps (each the exchange: imaging, windowed
-    PE loss, adjoint of every tile, CEPT and neighbour gradient fusion, then the
-    windowed theta step). Split-BF16 images the tiles in batched groups; the plain
-    FP32 mode one tile after another. Timed on the wall clock around the run (the
-    exchange returns its losses to the host every iteration)."""
+def levelset_run(L, torch, stream, N=2048, B=16, steps=10, warmup=3):
+    """The WENO5-Godunov RK2 level-set update (litho_lsm_rk2_update_batch) on B
+    N x N images per call: per image the CFL dt (max |Vn|), RK2 stage 1 and stage 2 with
+    the printed mask. Algorithmic bytes per pixel: Vn once for dt (4), stage 1 phi and
+    Vn in, phi1 out (12), stage 2 phi1, phi and Vn in, phi and mask out (20): 36 B/px.
+    The working set (about 5 x 4 B x B N^2) exceeds L2, so nothing is flushed. The
+    time is CUDA events around each call on its stream (the call returns the per-image
+    dt to the host, so one host round trip per call is inside it)."""
+    ctx = L.Context(torch.cuda.current_device(), stream=stream)
+    rng = np.random.default_rng(5)
+    yy, xx = np.mgrid[0:N, 0:N].astype(np.float32)
+    with torch.cuda.stream(stream):
+        base = torch.from_numpy(np.sin(0.013 * xx) * np.cos(0.011 * yy) * 40.0).cuda()
+        phi = torch.stack([base.roll(17 * b, 1) for b in range(B)]).contiguous()
+        vn = torch.from_numpy(rng.standard_normal((B, N, N)).astype(np.float32)).cuda()
+        out, mask = torch.empty_like(phi), torch.empty_like(phi)
+    torch.cuda.synchronize()
+    call = lambda: L.LevelSetUtils.rk2_update_batch(phi, vn, 1.0, 1.0, 0.5, 0.01, out, mask, ctx=ctx)
+    for _ in range(max(3, warmup)):
+        call()
+    times = []
+    for _ in range(steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        call()
+        e1.record(stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+    ctx.close()
+    ms = float(np.median(times))
+    byts = 36.0 * B * N * N
+    hbm, src = peaks()
+    gbs = byts / (ms * 1e-3) / 1e9
+    return {"bound": "hbm", "kernel": "levelset_kernel RK2 stages + absmax/dt (one batched call)",
+            "workload": f"{B} images of {N}^2 per call, CFL 0.5, curvature weight 0.01",
+            "ms_per_call": ms, "ms_per_image_update": ms / B, "algorithmic_bytes": byts,
+            "achieved": gbs, "peak": hbm, "peak_source": src, "unit": "GB/s", "frac": gbs / hbm,
+            "pixel_updates_per_s": B * N * N / (ms * 1e-3)}
+
+
+def fullchip_run(L, K, size, grid, halo, guard, ctm_steps=3, lsm_steps=20, seed=11):
+    """The batched full-chip configuration: a size x size layout (2 nm pixels, seeded
+    rectangles at about 34 % density) cut into grid x grid micro tiles (Core size / grid
+    plus a `halo` pixel halo on every side). Two runs per precision mode:
+    FullChipCTMOptimizer for `ctm_steps` steps (each the exchange: imaging, windowed PE
+    loss and adjoint of every tile, CEPT and neighbour gradient fusion, then the
+    windowed theta step) and FullChipLSMOptimizer for `lsm_steps` WENO5-Godunov steps
+    (exchange over Core + Guard with the Core metrics, windowed RK2 per tile, reinit
+    every 20, rendered masks, best-round state). Split-BF16 images the tiles in
+    batched groups, the plain FP32 mode one tile after another. Timed on the wall
+    clock around each run (the exchange returns its losses to the host every step);
+    tile-iterations count every tile of every exchange (the initial one included)."""
     import torch
     FC = importlib.import_module("c-version-lithography_b200.fullchip")
     wl = importlib.import_module("c-version-lithography_b200.workloads")
     band, r0, c0, w, wss = wl.synthetic_socs_band(K=K)
     layout = torch.from_numpy(wl.cell_layout(size, size, seed)).cuda()
     gopt = FC.MicroGradientOptions(enable_cept=True, enable_grad_fusion=True)
-    out = {"workload": f"full-chip CTM, {size}^2 layout (2 nm pixels, ~34% density), "
-                       f"{grid}x{grid} micro tiles, halo {halo}, guard {guard}, CEPT + "
-                       f"average gradient fusion, {iterations} steps + the initial exchange, "
-                       f"{K} SOCS kernels"}
+    out = {"workload": f"{size}^2 layout (2 nm pixels, ~34% density), {grid}x{grid} micro tiles, "
+                       f"halo {halo}, guard {guard}, {K} SOCS kernels; CTM: {ctm_steps} steps "
+                       f"with CEPT + average gradient fusion; LSM: {lsm_steps} WENO5-Godunov "
+                       f"steps, Binary masks, reinit every 20, Core metrics",
+           "ctm": {}, "lsm": {}}
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        res = fn()
+        torch.cuda.synchronize()
+        return res, time.perf_counter() - t0
+
     for mode in ("bf16x3", "fp32"):
         ctx = L.Context()
         ctx.set_precision(mode)
         part = FC.Partition(size, size, grid, grid, halo, guard, ctx=ctx)
         cache = L.ImagingCache.from_band(part.tile_size, band, r0, c0, w, wss, ctx=ctx)
-        opt = FC.FullChipCTMOptimizer(part, cache, THRESHOLD, ALPHA)
-        opt.optimize(layout, FC.FullChipCTMOptions(iterations=1, gradient_options=gopt))  # warm-up
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        res = opt.optimize(layout, FC.FullChipCTMOptions(iterations=iterations,
-                                                         gradient_options=gopt))
-        torch.cuda.synchronize()
-        sec = time.perf_counter() - t0
-        evals = part.num_tiles * (iterations + 1)
-        out[mode] = {"tile_size": part.tile_size, "tiles": part.num_tiles, "seconds": sec,
-                     "tile_iterations_per_s": evals / sec,
-                     "layout_mpx_per_s": (iterations + 1) * size * size / sec / 1e6,
-                     "final_loss": res.history[-1].loss, "initial_loss": res.history[0].loss}
-        del opt, res
+        ctm = FC.FullChipCTMOptimizer(part, cache, THRESHOLD, ALPHA)
+        ctm.optimize(layout, FC.FullChipCTMOptions(iterations=1, gradient_options=gopt))  # warm-up
+        res, sec = timed(lambda: ctm.optimize(
+            layout, FC.FullChipCTMOptions(iterations=ctm_steps, gradient_options=gopt)))
+        evals = part.num_tiles * (ctm_steps + 1)
+        out["ctm"][mode] = {"tile_size": part.tile_size, "tiles": part.num_tiles, "seconds": sec,
+                            "tile_iterations_per_s": evals / sec,
+                            "initial_loss": res.history[0].loss, "final_loss": res.history[-1].loss}
+        del ctm, res
+        lsm = FC.FullChipLSMOptimizer(part, cache, THRESHOLD, ALPHA)
+        lsm.optimize(layout, layout, FC.FullChipLSMOptions(iterations=1))               # warm-up
+        res, sec = timed(lambda: lsm.optimize(layout, layout,
+                                              FC.FullChipLSMOptions(iterations=lsm_steps)))
+        evals = part.num_tiles * (lsm_steps + 1)
+        out["lsm"][mode] = {"tile_size": part.tile_size, "tiles": part.num_tiles, "seconds": sec,
+                            "tile_iterations_per_s": evals / sec,
+                            "initial_loss": res.history[0].loss, "best_loss": res.best_loss}
+        del lsm, res
         part.close()
         ctx.close()
         torch.cuda.empty_cache()
-    out["batched_bf16x3_over_fp32"] = (out["bf16x3"]["tile_iterations_per_s"] /
-                                       out["fp32"]["tile_iterations_per_s"])
+    for k in ("ctm", "lsm"):
+        out[k]["batched_bf16x3_over_fp32"] = (out[k]["bf16x3"]["tile_iterations_per_s"] /
+                                              out[k]["fp32"]["tile_iterations_per_s"])
     return out
 
 
@@ -554,6 +611,8 @@ def run_ours(args):
         pm["bf16x3_over_fp32"] = pm["bf16x3"]["value"] / pm["fp32"]["value"]
         if head not in ("fp32", "bf16x3"):
             pm["batched_over_fp32"] = pm[head]["value"] / pm["fp32"]["value"]
+    if world == 1:
+        out["roofline_levelset"] = levelset_run(L, torch, stream)
     if world == 1 and args.serving_requests > 0:
         out["serving"] = serving_run(L, K, args.serving_requests)
     if world == 1 and args.fullchip_size > 0:

@@ -1412,12 +1412,9 @@ int litho_reinit_sdf(litho_ctx* ctx, int rows, int cols, const float* d_phi, dou
   if (st) return st;
   if ((size_t)3 * cols * sizeof(float) > 200 * 1024)
     return ctx->fail(LITHO_ERR_UNSUPPORTED, "reinit_sdf supports at most 17066 columns");
-  const size_t n = (size_t)rows * cols;
-  st = ctx->ensure_scratch(2 * n * sizeof(float));
-  if (st) return st;
+  if (d_sdf == d_phi) return ctx->fail(LITHO_ERR_INVALID_ARGUMENT, "reinit_sdf: sdf must not alias phi");
   ctx->stage_begin(8);
-  st = check_launch(ctx, launch_reinit_sdf(ctx->stream, rows, cols, d_phi, (float)dx,
-                                           static_cast<float*>(ctx->scratch.base), d_sdf),
+  st = check_launch(ctx, launch_reinit_sdf(ctx->stream, rows, cols, d_phi, 0.f, 0, (float)dx, d_sdf),
                     "reinit_sdf");
   if (!st && d_mask)
     st = check_launch(ctx, launch_levelset(ctx->stream, 5, rows, cols, d_sdf, nullptr, nullptr,
@@ -1469,37 +1466,36 @@ int litho_lsm_rk2_update_batch(litho_ctx* ctx, int batch, int rows, int cols, co
   if (d_phi_out == d_phi) return ctx->fail(LITHO_ERR_INVALID_ARGUMENT, "phi_out must not alias phi");
   int st = ls_check(ctx, rows, cols, dx, dy, 3);
   if (st) return st;
+  if (batch > 65535) return ctx->fail(LITHO_ERR_INVALID_ARGUMENT, "at most 65535 images per call");
   const size_t n = (size_t)rows * cols;
-  st = ctx->ensure_scratch(n * sizeof(float));
+  st = ctx->ensure_scratch(n * batch * sizeof(float));
   if (st) return st;
-  // Per-image (max |Vn|, dt) pairs after the reduction area of launch_dt.
-  constexpr size_t kDtPart = 2 * 600;
-  st = ctx->ensure_red(RED_PART + kDtPart + (size_t)batch + 8);
+  // Per-image absmax partials, then the per-image (max |Vn|, dt) pairs.
+  const size_t nparts = (size_t)batch * dt_batch_blocks(n, batch);
+  const size_t part_dbl = (nparts + 1) / 2 + 8;
+  st = ctx->ensure_red(RED_PART + part_dbl + (size_t)batch + 8);
   if (st) return st;
   LITHO_CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_red, 0, RED_PART * sizeof(double), ctx->stream));
   float* phi1 = static_cast<float*>(ctx->scratch.base);
   float* part = reinterpret_cast<float*>(ctx->d_red + RED_PART);
-  float* vd = reinterpret_cast<float*>(ctx->d_red + RED_PART + kDtPart);   // [batch][2]
+  float* vd = reinterpret_cast<float*>(ctx->d_red + RED_PART + part_dbl);   // [batch][2]
   int* bad = reinterpret_cast<int*>(ctx->d_red + RED_FLAG);
   cudaStream_t s = ctx->stream;
-  for (int i = 0; i < batch && !st; ++i) {
-    const float* phi = d_phi + i * n;
-    const float* vn = d_vn + i * n;
-    float* dtd = vd + 2 * i + 1;
-    st = check_launch(ctx, launch_dt(s, vn, n, (float)dx, (float)dy, (float)cfl, (float)b, part,
-                                     vd + 2 * i, dtd, bad),
-                      "dt");
-    if (!st)
-      st = check_launch(ctx, launch_levelset(s, 3, rows, cols, phi, nullptr, vn, (float)dx,
-                                             (float)dy, (float)b, dtd, phi1, nullptr),
-                        "rk2 stage 1");
-    if (!st)
-      st = check_launch(ctx, launch_levelset(s, 4, rows, cols, phi1, phi, vn, (float)dx, (float)dy,
-                                             (float)b, dtd, d_phi_out + i * n,
-                                             d_mask ? d_mask + i * n : nullptr),
-                        "rk2 stage 2");
-    ctx->launches += 4;
-  }
+  // Every image in each launch: dt per image, then the two RK2 stages with dt[2 i + 1].
+  st = check_launch(ctx, launch_dt_batch(s, d_vn, n, batch, (float)dx, (float)dy, (float)cfl,
+                                         (float)b, part, vd, bad),
+                    "dt");
+  if (!st)
+    st = check_launch(ctx, launch_levelset(s, 3, rows, cols, d_phi, nullptr, d_vn, (float)dx,
+                                           (float)dy, (float)b, vd + 1, phi1, nullptr, nullptr,
+                                           batch, nullptr, 2),
+                      "rk2 stage 1");
+  if (!st)
+    st = check_launch(ctx, launch_levelset(s, 4, rows, cols, phi1, d_phi, d_vn, (float)dx,
+                                           (float)dy, (float)b, vd + 1, d_phi_out, d_mask, nullptr,
+                                           batch, nullptr, 2),
+                      "rk2 stage 2");
+  ctx->launches += 4;
   std::vector<float> h(2 * (size_t)batch);
   if (!st)
     LITHO_CUDA_TRY(ctx, cudaMemcpyAsync(h.data(), vd, h.size() * sizeof(float),
@@ -1810,7 +1806,9 @@ int litho_exchange_compute_epe(litho_ctx* ctx, const litho_partition* cp, const 
   }
   // Per-block partials of the EPE and rectangle sums share the reduction area.
   const int epe_blocks = ncand == 0 ? 1 : (int)((ncand + 255) / 256);
-  st = ctx->ensure_red(RED_PART + 3 * (size_t)std::max(epe_blocks, 64) + 8);
+  st = ctx->ensure_red(RED_PART + std::max<size_t>(3 * (size_t)std::max(epe_blocks, 64) + 8,
+                                                   6 * ((size_t)rect_losses_batch_blocks(ts) + 1) *
+                                                           group + 8));
   if (st) return st;
   LITHO_CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_red, 0, RED_PART * sizeof(double), ctx->stream));
   float* targets = p->d_work;
@@ -1875,7 +1873,7 @@ int litho_exchange_compute_epe(litho_ctx* ctx, const litho_partition* cp, const 
   // Core + Guard region) give the EPE sums and, for the EPE types, the scatter of
   // their dL/dI; with the Core metrics, the loss-region and Core sums from the wafer
   // image and the Core EPs without copies.
-  auto ep_work = [&](int t, const float* aer, const float* waf, float* dl) -> int {
+  auto ep_work = [&](int t, const float* aer, const float* waf, float* dl, bool rects) -> int {
     const int* R = &p->rects[16 * (size_t)t];   // core_global | tile_global | core_local | update_local
     const int* region = guard_region ? R + 12 : R + 8;
     const int oy = R[4], ox = R[6];
@@ -1894,17 +1892,20 @@ int litho_exchange_compute_epe(litho_ctx* ctx, const litho_partition* cp, const 
     if (!r) r = check_launch(ctx, launch_sum_partials(s, part, used, 3, slot + 2), "sum");
     ctx->launches += 3;
     if (r || !core) return r;
-    r = check_launch(ctx, launch_rect_losses(s, waf, targets + t * tt, pe_w + t * tt,
-                                             pen_w + t * tt, ts, region,
-                                             (float)o.penalty_threshold, part, &used),
-                     "region losses");
-    if (!r) r = check_launch(ctx, launch_sum_partials(s, part, used, 3, slot + 5), "sum");
-    if (!r)
+    if (rects) {
       r = check_launch(ctx, launch_rect_losses(s, waf, targets + t * tt, pe_w + t * tt,
-                                               pen_w + t * tt, ts, R + 8,
+                                               pen_w + t * tt, ts, region,
                                                (float)o.penalty_threshold, part, &used),
-                       "core losses");
-    if (!r) r = check_launch(ctx, launch_sum_partials(s, part, used, 3, slot + 8), "sum");
+                       "region losses");
+      if (!r) r = check_launch(ctx, launch_sum_partials(s, part, used, 3, slot + 5), "sum");
+      if (!r)
+        r = check_launch(ctx, launch_rect_losses(s, waf, targets + t * tt, pe_w + t * tt,
+                                                 pen_w + t * tt, ts, R + 8,
+                                                 (float)o.penalty_threshold, part, &used),
+                         "core losses");
+      if (!r) r = check_launch(ctx, launch_sum_partials(s, part, used, 3, slot + 8), "sum");
+      ctx->launches += 4;
+    }
     const int crect[4] = {R[0], R[1], R[2], R[3]};   // core_global
     if (!r)
       r = check_launch(ctx, launch_ep_candidates(s, ep_in, ep_in + 2 * (size_t)e.n_eps, e.n_eps,
@@ -1916,7 +1917,7 @@ int litho_exchange_compute_epe(litho_ctx* ctx, const litho_partition* cp, const 
                                        e.epe_pixel_size, nullptr, part, nullptr, 0.0, &used),
                        "core sparse EPE");
     if (!r) r = check_launch(ctx, launch_sum_partials(s, part, used, 3, slot + 11), "sum");
-    ctx->launches += 8;
+    ctx->launches += 3;
     return r;
   };
   // With an EPE gradient the adjoint needs dL/dI after the EP scatter, so the resist
@@ -1957,9 +1958,28 @@ int litho_exchange_compute_epe(litho_ctx* ctx, const litho_partition* cp, const 
                                             cudaMemcpyDeviceToDevice, s));
     if (!st && zero_pe_dldi)
       LITHO_CUDA_TRY(ctx, cudaMemsetAsync(dldi_group, 0, B * tt * sizeof(float), s));
+    if (!st && core) {
+      // Loss-region and Core sums of the group's tiles in one launch, to slots 5..10.
+      const int nbr = rect_losses_batch_blocks(ts);
+      double* sums6 = part + 6 * (size_t)nbr * B;
+      st = check_launch(ctx, launch_rect_losses_batch(
+                                 s, wafer, targets + t0 * tt, pe_w + t0 * tt, pen_w + t0 * tt, ts,
+                                 p->d_meta + (guard_region ? p->off_update : p->off_core_l) + 4 * t0,
+                                 p->d_meta + p->off_core_l + 4 * t0, (float)o.penalty_threshold,
+                                 part, B),
+                        "region and core losses");
+      if (!st)
+        st = check_launch(ctx, launch_sum_partials_batch(s, part, nbr, 6, part, 0, 0, sums6, B),
+                          "sum");
+      if (!st)
+        LITHO_CUDA_TRY(ctx, cudaMemcpy2DAsync(p->d_loss + (size_t)S * t0 + 5, S * sizeof(double),
+                                              sums6, 6 * sizeof(double), 6 * sizeof(double), B,
+                                              cudaMemcpyDeviceToDevice, s));
+      ctx->launches += 2;
+    }
     for (int b = 0; eval_epe && b < B && !st; ++b)
       st = ep_work(t0 + b, aerial + b * tt, core ? wafer + b * tt : nullptr,
-                   fuse ? nullptr : dldi_group + b * tt);
+                   fuse ? nullptr : dldi_group + b * tt, false);
     GradEpilogue gp{};
     gp.grad_mask = raw + t0 * tt;
     if (!st)
@@ -1986,7 +2006,7 @@ int litho_exchange_compute_epe(litho_ctx* ctx, const litho_partition* cp, const 
     if (!st) st = check_launch(ctx, launch_sum_partials(s, part, nb, 2, slot), "sum");
     ctx->launches += 1;
     if (!st && zero_pe_dldi) LITHO_CUDA_TRY(ctx, cudaMemsetAsync(dldi, 0, tt * sizeof(float), s));
-    if (!st && eval_epe) st = ep_work(t, aerial, wafer, dldi);
+    if (!st && eval_epe) st = ep_work(t, aerial, wafer, dldi, true);
     GradEpilogue gp{};
     gp.grad_mask = raw + t * tt;
     int nb2 = 0;
@@ -2113,30 +2133,23 @@ int litho_fullchip_lsm_init(litho_ctx* ctx, const litho_partition* p, const floa
   if ((size_t)3 * p->ts * sizeof(float) > 200 * 1024)
     return ctx->fail(LITHO_ERR_UNSUPPORTED, "reinit_sdf supports at most 17066 columns");
   if (cudaSetDevice(ctx->device) != cudaSuccess) return ctx->fail(LITHO_ERR_CUDA, "cudaSetDevice");
-  const size_t tt = (size_t)p->ts * p->ts;
-  int st = ctx->ensure_scratch(4 * tt * sizeof(float));
-  if (st) return st;
-  float* shifted = static_cast<float*>(ctx->scratch.base);  // mask - 0.5 of one tile
-  float* work = shifted + tt;                               // 2 tt for the distance transform
+  if (d_phi == d_masks) return ctx->fail(LITHO_ERR_INVALID_ARGUMENT, "full-chip LSM: phi must not alias the masks");
   cudaStream_t s = ctx->stream;
   // The extracted masks go to d_masks first (they are replaced by the renders below).
-  st = check_launch(ctx, launch_tiles_extract(s, d_global_mask, p->height, p->width, p->ntiles,
-                                              p->d_meta + p->off_origin, p->ts, d_masks),
-                    "tile extraction");
-  for (int t = 0; t < p->ntiles && !st; ++t) {
-    st = check_launch(ctx, launch_levelset(s, 9, p->ts, p->ts, d_masks + t * tt, nullptr, nullptr,
-                                           (float)dx, (float)dy, 0.f, nullptr, shifted, nullptr),
-                      "mask shift");
-    if (!st)
-      st = check_launch(ctx, launch_reinit_sdf(s, p->ts, p->ts, shifted, (float)dx, work,
-                                               d_phi + t * tt),
-                        "reinit_sdf");
-  }
+  int st = check_launch(ctx, launch_tiles_extract(s, d_global_mask, p->height, p->width, p->ntiles,
+                                                  p->d_meta + p->off_origin, p->ts, d_masks),
+                        "tile extraction");
+  // reinit_sdf(mask - 0.5) of every tile at once: mask - 0.5 > 0 exactly when mask > 0.5.
+  for (int t0 = 0; t0 < p->ntiles && !st; t0 += 65535)
+    st = check_launch(ctx, launch_reinit_sdf(s, p->ts, p->ts, d_masks + (size_t)t0 * p->ts * p->ts,
+                                             0.5f, 0, (float)dx, d_phi + (size_t)t0 * p->ts * p->ts,
+                                             std::min(p->ntiles - t0, 65535)),
+                      "reinit_sdf");
   if (!st)
     st = check_launch(ctx, launch_render_mask(s, d_phi, p->ts, p->ts, p->ntiles,
                                               mask_type == LITHO_MASK_GRAY, scale, d_masks),
                       "render_levelset_mask");
-  ctx->launches += 2 + 2 * p->ntiles;
+  ctx->launches += 3;
   if (!st) LITHO_CUDA_TRY(ctx, cudaStreamSynchronize(s));
   return st;
 }
@@ -2146,8 +2159,9 @@ int litho_fullchip_lsm_step(litho_ctx* ctx, const litho_partition* p, const floa
                             int reinit, int mask_type, int scale, float* d_phi_out,
                             float* d_masks, double* dt_min, double* dt_max) {
   if (!ctx || !p || !d_phi || !d_grad || !d_phi_out || !d_masks) return LITHO_ERR_INVALID_ARGUMENT;
-  if (d_phi_out == d_phi)
-    return ctx->fail(LITHO_ERR_INVALID_ARGUMENT, "full-chip LSM: phi_out must not alias phi");
+  if (d_phi_out == d_phi || d_masks == d_phi || d_masks == d_phi_out)
+    return ctx->fail(LITHO_ERR_INVALID_ARGUMENT,
+                     "full-chip LSM: phi, phi_out and the masks must not alias");
   if (!(dx > 0.0) || !(dy > 0.0) || !std::isfinite(cfl) || !std::isfinite(b))
     return ctx->fail(LITHO_ERR_INVALID_ARGUMENT, "full-chip LSM: dx, dy must be positive");
   if ((mask_type != LITHO_MASK_BINARY && mask_type != LITHO_MASK_GRAY) ||
@@ -2158,54 +2172,62 @@ int litho_fullchip_lsm_step(litho_ctx* ctx, const litho_partition* p, const floa
     return ctx->fail(LITHO_ERR_UNSUPPORTED, "reinit_sdf supports at most 17066 columns");
   if (cudaSetDevice(ctx->device) != cudaSuccess) return ctx->fail(LITHO_ERR_CUDA, "cudaSetDevice");
   const size_t tt = (size_t)p->ts * p->ts;
-  const int n = p->ntiles;
-  int st = ctx->ensure_scratch(5 * tt * sizeof(float) + 256 * sizeof(float) + n * sizeof(float));
+  const int n = p->ntiles, ts = p->ts;
+  // Tiles per chunk: the chunk's windowed speed and RK2 stage-1 images live in scratch
+  // (512 MB at most); every launch below covers the whole chunk.
+  const int G = (int)std::max<size_t>(
+      1, std::min<size_t>({(size_t)n, (size_t)65535, ((size_t)512 << 20) / (2 * tt * sizeof(float))}));
+  int st = ctx->ensure_scratch(2 * (size_t)G * tt * sizeof(float));
   if (st) return st;
-  st = ctx->ensure_red(RED_PART + 2 * 600);
+  const size_t part_dbl = (std::max<size_t>(1184, (size_t)G) + 1) / 2 + 8;  // absmax partials
+  st = ctx->ensure_red(RED_PART + part_dbl + (size_t)n + 8);
   if (st) return st;
-  float* vw = static_cast<float*>(ctx->scratch.base);  // windowed speed of one tile
-  float* phi1 = vw + tt;                                // RK2 stage 1
-  float* signs = phi1 + tt;                             // +-0.5 image for reinit
-  float* work = signs + tt;                             // 2 tt: distance transform, then sdf
-  float* dts = work + 2 * tt + 256;                     // one dt per tile
+  float* vw = static_cast<float*>(ctx->scratch.base);  // windowed speed of the chunk
+  float* phi1 = vw + (size_t)G * tt;                   // RK2 stage 1, then the reinit distance
   cudaStream_t s = ctx->stream;
   LITHO_CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_red, 0, RED_PART * sizeof(double), s));
   float* part = reinterpret_cast<float*>(ctx->d_red + RED_PART);
-  float* vmax = reinterpret_cast<float*>(ctx->d_red + RED_SUM);
+  float* vd = reinterpret_cast<float*>(ctx->d_red + RED_PART + part_dbl);  // [tile][max |V|, dt]
   int* bad = reinterpret_cast<int*>(ctx->d_red + RED_FLAG);
-  for (int t = 0; t < n && !st; ++t) {
-    const int* win = p->rects.data() + 16 * (size_t)t + 12;  // update_local (host copy)
-    const float* ph = d_phi + t * tt;
-    float* out = d_phi_out + t * tt;
-    st = check_launch(ctx, launch_levelset(s, 6, p->ts, p->ts, ph, nullptr, d_grad + t * tt,
-                                           (float)dx, (float)dy, 0.f, nullptr, vw, nullptr, win),
+  const int* wins = p->d_meta + p->off_update;                            // update_local per tile
+  for (int t0 = 0; t0 < n && !st; t0 += G) {
+    const int B = std::min(G, n - t0);
+    const float* ph = d_phi + t0 * tt;
+    float* out = d_phi_out + t0 * tt;
+    const int* w = wins + 4 * (size_t)t0;
+    float* dtd = vd + 2 * (size_t)t0 + 1;
+    st = check_launch(ctx, launch_levelset(s, 6, ts, ts, ph, nullptr, d_grad + t0 * tt, (float)dx,
+                                           (float)dy, 0.f, nullptr, vw, nullptr, nullptr, B, w, 0),
                       "windowed speed");
     if (!st)
-      st = check_launch(ctx, launch_dt(s, vw, tt, (float)dx, (float)dy, (float)cfl, (float)b, part,
-                                       vmax, dts + t, bad),
+      st = check_launch(ctx, launch_dt_batch(s, vw, tt, B, (float)dx, (float)dy, (float)cfl,
+                                             (float)b, part, vd + 2 * (size_t)t0, bad),
                         "dt");
     if (!st)
-      st = check_launch(ctx, launch_levelset(s, 3, p->ts, p->ts, ph, nullptr, vw, (float)dx,
-                                             (float)dy, (float)b, dts + t, phi1, nullptr, win),
+      st = check_launch(ctx, launch_levelset(s, 3, ts, ts, ph, nullptr, vw, (float)dx, (float)dy,
+                                             (float)b, dtd, phi1, nullptr, nullptr, B, w, 2),
                         "rk2 stage 1");
     if (!st)
-      st = check_launch(ctx, launch_levelset(s, 4, p->ts, p->ts, phi1, ph, vw, (float)dx,
-                                             (float)dy, (float)b, dts + t, out, nullptr, win),
+      st = check_launch(ctx, launch_levelset(s, 4, ts, ts, phi1, ph, vw, (float)dx, (float)dy,
+                                             (float)b, dtd, out, nullptr, nullptr, B, w, 2),
                         "rk2 stage 2");
     ctx->launches += 5;
-    if (!st && reinit) {
-      st = check_launch(ctx, launch_levelset(s, 7, p->ts, p->ts, out, nullptr, nullptr, (float)dx,
-                                             (float)dy, 0.f, nullptr, signs, nullptr),
-                        "sign image");
-      if (!st)
-        st = check_launch(ctx, launch_reinit_sdf(s, p->ts, p->ts, signs, (float)dx, work, phi1),
-                          "reinit_sdf");
-      if (!st)
-        st = check_launch(ctx, launch_levelset(s, 8, p->ts, p->ts, phi1, out, nullptr, (float)dx,
-                                               (float)dy, 0.f, nullptr, out, nullptr, win),
-                          "window commit");
-      ctx->launches += 3;
-    }
+  }
+  // reinit_sdf of the +-0.5 sign image of phi >= 0 (full_chip_lsm.cpp:229-230) of every
+  // tile at once: the chamfer transform with inside = phi >= 0, into the mask buffer
+  // (rendered afresh below), then phi inside each tile's window only.
+  for (int t0 = 0; reinit && t0 < n && !st; t0 += 65535) {
+    const int B = std::min(n - t0, 65535);
+    st = check_launch(ctx, launch_reinit_sdf(s, ts, ts, d_phi_out + t0 * tt, 0.f, 1, (float)dx,
+                                             d_masks + t0 * tt, B),
+                      "reinit_sdf");
+    if (!st)
+      st = check_launch(ctx, launch_levelset(s, 8, ts, ts, d_masks + t0 * tt, d_phi_out + t0 * tt,
+                                             nullptr, (float)dx, (float)dy, 0.f, nullptr,
+                                             d_phi_out + t0 * tt, nullptr, nullptr, B,
+                                             wins + 4 * (size_t)t0, 0),
+                        "window commit");
+    ctx->launches += 2;
   }
   if (!st)
     st = check_launch(ctx, launch_render_mask(s, d_phi_out, p->ts, p->ts, n,
@@ -2213,13 +2235,19 @@ int litho_fullchip_lsm_step(litho_ctx* ctx, const litho_partition* p, const floa
                       "render_levelset_mask");
   ctx->launches += 1;
   if (st) return st;
-  std::vector<float> h(n);
-  LITHO_CUDA_TRY(ctx, cudaMemcpyAsync(h.data(), dts, n * sizeof(float), cudaMemcpyDeviceToHost, s));
+  std::vector<float> h(2 * (size_t)n);
+  LITHO_CUDA_TRY(ctx, cudaMemcpyAsync(h.data(), vd, h.size() * sizeof(float),
+                                      cudaMemcpyDeviceToHost, s));
   st = fetch(ctx, 0);
   if (st) return st;
   if (flag_set(ctx)) return ctx->fail(LITHO_ERR_NONFINITE, "normal speed must be finite");
-  if (dt_min) *dt_min = *std::min_element(h.begin(), h.end());
-  if (dt_max) *dt_max = *std::max_element(h.begin(), h.end());
+  float lo = h[1], hi = h[1];
+  for (int t = 1; t < n; ++t) {
+    lo = std::min(lo, h[2 * (size_t)t + 1]);
+    hi = std::max(hi, h[2 * (size_t)t + 1]);
+  }
+  if (dt_min) *dt_min = lo;
+  if (dt_max) *dt_max = hi;
   return LITHO_OK;
 }
 

@@ -205,6 +205,62 @@ cudaError_t launch_rect_losses(cudaStream_t s, const float* Wf, const float* T, 
   return cudaGetLastError();
 }
 
+// The loss-region and Core sums of a group of tiles in one launch: tile blockIdx.y
+// (images ts x ts back to back, rectangles {y0, y1, x0, x1} 4 ints per tile), the
+// Core being inside the region. partial[(tile * gridDim.x + block) * 6 + k]: k = 0..2
+// the three sums over the region, 3..5 over the Core.
+__global__ void __launch_bounds__(RL_NT)
+rect_losses_batch_kernel(const float* __restrict__ Wf, const float* __restrict__ T,
+                         const float* __restrict__ pe_w, const float* __restrict__ pen_w, int ts,
+                         const int* __restrict__ regions, const int* __restrict__ cores,
+                         float pen_thr, double* __restrict__ partial) {
+  __shared__ double sh[RL_NT / 32];
+  const size_t img = (size_t)blockIdx.y * ts * ts;
+  const int* rg = regions + 4 * (size_t)blockIdx.y;
+  const int* cr = cores + 4 * (size_t)blockIdx.y;
+  const int y0 = rg[0], x0 = rg[2], cols = rg[3] - rg[2], n = (rg[1] - rg[0]) * cols;
+  const int cy0 = cr[0], cy1 = cr[1], cx0 = cr[2], cx1 = cr[3];
+  double v[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  for (int i = blockIdx.x * RL_NT + threadIdx.x; i < n; i += gridDim.x * RL_NT) {
+    const int y = y0 + i / cols, x = x0 + i % cols;
+    const size_t k = img + (size_t)y * ts + x;
+    const double w = Wf[k], t = T[k], r = w - t;
+    const double pe = r * r * (double)pe_w[k];
+    double bg = 0.0;
+    if (t < 0.5) {
+      const double ex = fmax(0.0, w - (double)pen_thr);
+      bg = (double)pen_w[k] * ex * ex;
+    }
+    const double mainpe = t > 0.5 ? r * r : 0.0;
+    v[0] += pe; v[1] += bg; v[2] += mainpe;
+    if (y >= cy0 && y < cy1 && x >= cx0 && x < cx1) {
+      v[3] += pe; v[4] += bg; v[5] += mainpe;
+    }
+  }
+  double* out = partial + ((size_t)blockIdx.y * gridDim.x + blockIdx.x) * 6;
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    const double a = block_sum<RL_NT>(v[k], sh);
+    if (threadIdx.x == 0) out[k] = a;
+  }
+}
+
+int rect_losses_batch_blocks(int ts) {
+  const int n = ts * ts;
+  const int b = (n + RL_NT - 1) / RL_NT;
+  return b < 1 ? 1 : (b > 48 ? 48 : b);
+}
+
+cudaError_t launch_rect_losses_batch(cudaStream_t s, const float* Wf, const float* T,
+                                     const float* pe_w, const float* pen_w, int ts,
+                                     const int* d_regions, const int* d_cores, float pen_thr,
+                                     double* partial, int nimg) {
+  if (nimg < 1 || nimg > 65535) return cudaErrorInvalidValue;
+  rect_losses_batch_kernel<<<dim3(rect_losses_batch_blocks(ts), nimg), RL_NT, 0, s>>>(
+      Wf, T, pe_w, pen_w, ts, d_regions, d_cores, pen_thr, partial);
+  return cudaGetLastError();
+}
+
 // Neighbour relations of one tile come in the reference's order (left, right,
 // top, bottom; absent neighbours omitted).
 constexpr int REL_INTS = FC_REL_INTS;

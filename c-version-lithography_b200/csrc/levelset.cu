@@ -7,6 +7,7 @@
 // phi[i][clamp(j-3 .. j+3)] and phi[clamp(i-3 .. i+3)][j]. The tile loader
 // therefore clamps every halo index into the image.
 #include <cuda_runtime.h>
+#include <algorithm>
 #include <cfloat>
 
 #include "litho_internal.cuh"
@@ -42,10 +43,12 @@ __device__ __forceinline__ float weno5(float v1, float v2, float v3, float v4, f
   const float S1 = ((13.f / 12.f) * t1 * t1 + 0.25f * q1 * q1) * inv + 1e-6f;
   const float S2 = ((13.f / 12.f) * t2 * t2 + 0.25f * q2 * q2) * inv + 1e-6f;
   const float S3 = ((13.f / 12.f) * t3 * t3 + 0.25f * q3 * q3) * inv + 1e-6f;
-  const float a1 = 0.1f / (S1 * S1);
-  const float a2 = 0.6f / (S2 * S2);
-  const float a3 = 0.3f / (S3 * S3);
-  return (a1 * d1 + a2 * d2 + a3 * d3) / (a1 + a2 + a3);
+  // alpha_i = gamma_i / S_i^2 and the result sum(alpha_i d_i) / sum(alpha_i), both
+  // multiplied by S1^2 S2^2 S3^2: one division instead of four. The scaled S_i lie in
+  // [1e-6, 34], so the products stay well inside FP32 range.
+  const float s1 = S1 * S1, s2 = S2 * S2, s3 = S3 * S3;
+  const float b1 = 0.1f * (s2 * s3), b2 = 0.6f * (s1 * s3), b3 = 0.3f * (s1 * s2);
+  return (b1 * d1 + b2 * d2 + b3 * d3) / (b1 + b2 + b3);
 }
 
 // Godunov |grad phi| for the sign of the normal speed (level_set_utils.cpp:180-213).
@@ -154,26 +157,38 @@ struct LsArgs {
   float* out;
   float* out2;        // habs (what 0) or mask (what 4)
   int wy0, wy1, wx0, wx1;  // update window [wy0, wy1) x [wx0, wx1) (stages 3, 4 and what 6, 8)
+  // Batched launches: image blockIdx.z of rows x cols images back to back; its dt at
+  // dt[blockIdx.z * dt_stride]; its window from wins[4 blockIdx.z ..] when wins is set.
+  const int* wins;
+  int dt_stride;
 };
 
 __global__ void __launch_bounds__(LS_NT) levelset_kernel(LsArgs a) {
+  const size_t img = (size_t)blockIdx.z * a.rows * a.cols;
+  const float* phi = a.phi + img;
+  float* out = a.out + img;
+  int wy0 = a.wy0, wy1 = a.wy1, wx0 = a.wx0, wx1 = a.wx1;
+  if (a.wins) {
+    const int* w = a.wins + 4 * (size_t)blockIdx.z;
+    wy0 = w[0]; wy1 = w[1]; wx0 = w[2]; wx1 = w[3];
+  }
   if (a.what >= 5) {  // elementwise modes
     const int x = blockIdx.x * LS_TX + threadIdx.x % LS_TX;
     for (int r = 0; r < LS_RPT; ++r) {
       const int y = blockIdx.y * LS_TY * LS_RPT + threadIdx.x / LS_TX + r * LS_TY;
       if (y < a.rows && x < a.cols) {
         const size_t i = (size_t)y * a.cols + x;
-        const bool in = y >= a.wy0 && y < a.wy1 && x >= a.wx0 && x < a.wx1;
+        const bool in = y >= wy0 && y < wy1 && x >= wx0 && x < wx1;
         if (a.what == 5)         // printed mask: phi >= 0 (LSM_Optimizer.cpp:128)
-          a.out[i] = a.phi[i] >= 0.f ? 1.f : 0.f;
+          out[i] = phi[i] >= 0.f ? 1.f : 0.f;
         else if (a.what == 6)    // speed restricted to the update window
-          a.out[i] = in ? a.vn[i] : 0.f;
+          out[i] = in ? a.vn[img + i] : 0.f;
         else if (a.what == 7)    // +-0.5 sign image of phi >= 0 (full_chip_lsm.cpp:229-230)
-          a.out[i] = a.phi[i] >= 0.f ? 0.5f : -0.5f;
+          out[i] = phi[i] >= 0.f ? 0.5f : -0.5f;
         else if (a.what == 9)    // mask - 0.5 (full_chip_lsm.cpp:143)
-          a.out[i] = a.phi[i] - 0.5f;
+          out[i] = phi[i] - 0.5f;
         else                     // commit phi inside the window over phi0 (out may be phi0)
-          a.out[i] = in ? a.phi[i] : a.phi0[i];
+          out[i] = in ? phi[i] : a.phi0[img + i];
       }
     }
     return;
@@ -181,28 +196,31 @@ __global__ void __launch_bounds__(LS_NT) levelset_kernel(LsArgs a) {
   __shared__ float t[LS_SH][LS_SW];
   const int x0 = blockIdx.x * LS_TX;
   const int y0 = blockIdx.y * LS_TY * LS_RPT;
-  load_tile(t, a.phi, a.rows, a.cols, y0, x0);
+  load_tile(t, phi, a.rows, a.cols, y0, x0);
   __syncthreads();
   const float idx = 1.f / a.dx, idy = 1.f / a.dy;
-  const float dt = (a.what >= 3) ? *a.dt : 0.f;
+  const float dt = (a.what >= 3) ? a.dt[(size_t)blockIdx.z * a.dt_stride] : 0.f;
+  const float* phi0 = a.phi0 ? a.phi0 + img : nullptr;
+  const float* vn = a.vn ? a.vn + img : nullptr;
+  float* out2 = a.out2 ? a.out2 + img : nullptr;
   const int lx = threadIdx.x % LS_TX;
   for (int r = 0; r < LS_RPT; ++r) {
     const int ly = threadIdx.x / LS_TX + r * LS_TY;
     const int y = y0 + ly, x = x0 + lx;
     if (y >= a.rows || x >= a.cols) continue;
     const size_t i = (size_t)y * a.cols + x;
-    if (a.what >= 3 && !(y >= a.wy0 && y < a.wy1 && x >= a.wx0 && x < a.wx1)) {
+    if (a.what >= 3 && !(y >= wy0 && y < wy1 && x >= wx0 && x < wx1)) {
       // Outside the update window the step keeps phi (stage 1) / the starting phi (stage 2).
-      const float keep = a.what == 3 ? t[ly + LS_H][lx + LS_H] : __ldg(a.phi0 + i);
-      if (a.what == 4 && a.out2) a.out2[i] = keep >= 0.f ? 1.f : 0.f;
-      a.out[i] = keep;
+      const float keep = a.what == 3 ? t[ly + LS_H][lx + LS_H] : __ldg(phi0 + i);
+      if (a.what == 4 && out2) out2[i] = keep >= 0.f ? 1.f : 0.f;
+      out[i] = keep;
       continue;
     }
-    const float speed = a.what == 1 ? 0.f : __ldg(a.vn + i);
+    const float speed = a.what == 1 ? 0.f : __ldg(vn + i);
     float v;
     if (a.what == 0) {
       v = weno_delta(t, ly + LS_H, lx + LS_H, speed, idx, idy);
-      if (a.out2) a.out2[i] = fabsf(speed);
+      if (out2) out2[i] = fabsf(speed);
     } else if (a.what == 1) {
       v = kappa_term(t, ly + LS_H, lx + LS_H, y, x, a.rows, a.cols, a.dx, a.dy, a.b);
     } else {
@@ -213,11 +231,11 @@ __global__ void __launch_bounds__(LS_NT) levelset_kernel(LsArgs a) {
       } else if (a.what == 3) {
         v = t[ly + LS_H][lx + LS_H] + dt * n;
       } else {
-        v = 0.5f * __ldg(a.phi0 + i) + 0.5f * (t[ly + LS_H][lx + LS_H] + dt * n);
-        if (a.out2) a.out2[i] = v >= 0.f ? 1.f : 0.f;
+        v = 0.5f * __ldg(phi0 + i) + 0.5f * (t[ly + LS_H][lx + LS_H] + dt * n);
+        if (out2) out2[i] = v >= 0.f ? 1.f : 0.f;
       }
     }
-    a.out[i] = v;
+    out[i] = v;
   }
 }
 
@@ -227,12 +245,17 @@ static dim3 ls_grid(int rows, int cols) {
 
 cudaError_t launch_levelset(cudaStream_t s, int what, int rows, int cols, const float* phi,
                             const float* phi0, const float* vn, float dx, float dy, float b,
-                            const float* dt, float* out, float* out2, const int* window) {
-  LsArgs a{rows, cols, what, phi, phi0, vn, dx, dy, b, dt, out, out2, 0, rows, 0, cols};
+                            const float* dt, float* out, float* out2, const int* window,
+                            int nimg, const int* d_windows, int dt_stride) {
+  if (nimg < 1 || nimg > 65535) return cudaErrorInvalidValue;
+  LsArgs a{rows, cols, what, phi, phi0, vn, dx, dy, b, dt, out, out2, 0, rows, 0, cols,
+           d_windows, dt_stride};
   if (window) {
     a.wy0 = window[0]; a.wy1 = window[1]; a.wx0 = window[2]; a.wx1 = window[3];
   }
-  levelset_kernel<<<ls_grid(rows, cols), LS_NT, 0, s>>>(a);
+  dim3 g = ls_grid(rows, cols);
+  g.z = nimg;
+  levelset_kernel<<<g, LS_NT, 0, s>>>(a);
   return cudaGetLastError();
 }
 
@@ -240,6 +263,8 @@ cudaError_t launch_levelset(cudaStream_t s, int what, int rows, int cols, const 
 __global__ void __launch_bounds__(LS_NT) absmax_kernel(const float* __restrict__ v, size_t n,
                                                        float* __restrict__ part, int* bad) {
   __shared__ float sh[LS_NT / 32];
+  v += (size_t)blockIdx.y * n;                 // image blockIdx.y of a batched launch
+  part += (size_t)blockIdx.y * gridDim.x;
   float m = 0.f;
   bool nonfinite = false;
   for (size_t i = (size_t)blockIdx.x * LS_NT + threadIdx.x; i < n; i += (size_t)gridDim.x * LS_NT) {
@@ -262,6 +287,37 @@ __global__ void dt_kernel(const float* __restrict__ part, int n, float dx, float
   const double den = normal + kap;
   *vmax = m;
   *dt = den < 1e-9 ? 1e-3f : (float)(cfl / den);
+}
+
+// dt of every image of a batched launch: vd[2 i] = max |Vn|, vd[2 i + 1] = dt.
+__global__ void dt_batch_kernel(const float* __restrict__ part, int nb, float dx, float dy,
+                                float cfl, float b, float* __restrict__ vd) {
+  const float* p = part + (size_t)blockIdx.x * nb;
+  float m = 0.f;
+  for (int i = threadIdx.x; i < nb; i += 32) m = fmaxf(m, p[i]);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if (threadIdx.x != 0) return;
+  const double normal = (double)m / dx + (double)m / dy;
+  const double kap = (double)b * (1.0 / ((double)dx * dx) + 1.0 / ((double)dy * dy)) * 2.0;
+  const double den = normal + kap;
+  vd[2 * (size_t)blockIdx.x] = m;
+  vd[2 * (size_t)blockIdx.x + 1] = den < 1e-9 ? 1e-3f : (float)(cfl / den);
+}
+
+int dt_batch_blocks(size_t n, int nimg) {
+  const size_t want = (n + LS_NT - 1) / LS_NT;
+  const size_t cap = std::max<size_t>(1, 1184 / (size_t)std::max(nimg, 1));
+  return (int)std::max<size_t>(1, std::min(want, cap));
+}
+
+cudaError_t launch_dt_batch(cudaStream_t s, const float* vn, size_t n, int nimg, float dx,
+                            float dy, float cfl, float b, float* part, float* vd, int* bad) {
+  if (nimg < 1 || nimg > 65535) return cudaErrorInvalidValue;
+  const int nb = dt_batch_blocks(n, nimg);
+  absmax_kernel<<<dim3(nb, nimg), LS_NT, 0, s>>>(vn, n, part, bad);
+  dt_batch_kernel<<<nimg, 32, 0, s>>>(part, nb, dx, dy, cfl, b, vd);
+  return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------- mask rendering
@@ -342,16 +398,20 @@ cudaError_t launch_render_mask(cudaStream_t s, const float* phi, int rows, int c
 // which is evaluated exactly as a min-plus prefix scan
 //   d(j) = j + min_{k <= j} (g(k) - k)     (double precision, then float),
 // g being the minimum over the already final rows above (below) plus the
-// pixel's own value. One CTA runs one transform; blockIdx.x = 0 measures
-// inside pixels (phi > 0) to the outside and writes +d dx to sdf there,
-// blockIdx.x = 1 measures outside pixels to the inside and writes -d dx. Each
-// pixel of sdf is written by exactly one of the two CTAs. With no feature
-// pixel at all the distance stays FLT_MAX, as OpenCV returns.
-constexpr int DT_NT = 1024;
+// pixel's own value. One CTA runs one transform of one image (blockIdx.y):
+// blockIdx.x = 0 measures inside pixels to the outside and writes +d dx at the
+// inside pixels, blockIdx.x = 1 measures outside pixels to the inside and writes
+// -d dx at the outside pixels. A transform's distance is 0 at its feature pixels
+// (the other class), so each CTA keeps its forward-pass values in the output at
+// its own pixels only: the two CTAs of an image touch disjoint pixels and need no
+// other buffer. Inside means phi > level (phi >= level when `inclusive`). With no
+// feature pixel at all the distance stays FLT_MAX, as OpenCV returns.
 constexpr float DT_A = 1.0f, DT_B = 1.4f, DT_C = 2.1969f;
 
+template <int NT>
 __device__ __forceinline__ double dt_block_min_scan(double v, double* wsum, bool reverse) {
   // inclusive prefix (reverse: suffix) minimum over the block in thread order
+  constexpr int NW = NT / 32;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
@@ -361,7 +421,7 @@ __device__ __forceinline__ double dt_block_min_scan(double v, double* wsum, bool
   if (lane == (reverse ? 0 : 31)) wsum[warp] = v;
   __syncthreads();
   if (warp == 0) {
-    double t = wsum[lane];
+    double t = lane < NW ? wsum[lane] : 1e300;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
       const double u = reverse ? __shfl_down_sync(0xffffffffu, t, o) : __shfl_up_sync(0xffffffffu, t, o);
@@ -372,24 +432,28 @@ __device__ __forceinline__ double dt_block_min_scan(double v, double* wsum, bool
   __syncthreads();
   double carry = 1e300;
   if (!reverse && warp > 0) carry = wsum[32 + warp - 1];
-  if (reverse && warp < 31) carry = wsum[32 + warp + 1];
+  if (reverse && warp < NW - 1) carry = wsum[32 + warp + 1];
   __syncthreads();
   return fmin(v, carry);
 }
 
-__global__ void __launch_bounds__(DT_NT)
-chamfer_sdf_kernel(const float* __restrict__ phi, int rows, int cols, float dx,
-                   float* __restrict__ work, float* __restrict__ sdf) {
+template <int NT>
+__global__ void __launch_bounds__(NT)
+chamfer_sdf_kernel(const float* __restrict__ phi_all, int rows, int cols, float level,
+                   int inclusive, float dx, float* __restrict__ sdf_all) {
   extern __shared__ float rowbuf[];  // 3 rows of cols floats: ring of the last rows
   __shared__ double wsum[64];
+  constexpr int NW = NT / 32;
   const bool inside_pass = blockIdx.x == 0;
-  float* d = work + (size_t)blockIdx.x * rows * cols;
-  const int per = (cols + DT_NT - 1) / DT_NT;  // contiguous columns per thread
+  const size_t img = (size_t)blockIdx.y * rows * cols;
+  const float* phi = phi_all + img;
+  float* sdf = sdf_all + img;
+  const int per = (cols + NT - 1) / NT;  // contiguous columns per thread
   const int j0 = threadIdx.x * per;
   const float FMAX = 3.402823466e38f;
-  auto feature = [&](int i, int j) {
+  auto inside = [&](int i, int j) {
     const float p = phi[(size_t)i * cols + j];
-    return inside_pass ? !(p > 0.f) : (p > 0.f);
+    return inclusive ? p >= level : p > level;
   };
   // ---- forward pass
   for (int i = 0; i < rows; ++i) {
@@ -401,7 +465,7 @@ chamfer_sdf_kernel(const float* __restrict__ phi, int rows, int cols, float dx,
       const int j = j0 + q;
       if (j >= cols) break;
       float g = FMAX;
-      if (feature(i, j)) {
+      if (inside(i, j) != inside_pass) {  // a feature pixel of this transform
         g = 0.f;
       } else {
         if (i >= 1) {
@@ -421,10 +485,9 @@ chamfer_sdf_kernel(const float* __restrict__ phi, int rows, int cols, float dx,
       r0[j] = g;  // provisional
     }
     // exclusive carry from the threads on the left
-    const double incl = dt_block_min_scan(local, wsum, false);
+    const double incl = dt_block_min_scan<NT>(local, wsum, false);
     double run = 1e300;
     {
-      // recover the exclusive prefix of this thread: scan again within the thread
       const double left = __shfl_up_sync(0xffffffffu, incl, 1);
       const int lane = threadIdx.x & 31;
       if (lane > 0) run = left;
@@ -438,7 +501,7 @@ chamfer_sdf_kernel(const float* __restrict__ phi, int rows, int cols, float dx,
       run = fmin(run, u);
       const double v = run + (double)j;
       r0[j] = v >= 1e299 ? FMAX : fminf(g, (float)v);
-      d[(size_t)i * cols + j] = r0[j];
+      if (inside(i, j) == inside_pass) sdf[(size_t)i * cols + j] = r0[j];
     }
     __syncthreads();
   }
@@ -452,7 +515,8 @@ chamfer_sdf_kernel(const float* __restrict__ phi, int rows, int cols, float dx,
     for (int q = 0; q < per; ++q) {
       const int j = j0 + q;
       if (j >= cols) break;
-      float g = d[(size_t)i * cols + j];
+      const bool own = inside(i, j) == inside_pass;
+      float g = own ? sdf[(size_t)i * cols + j] : 0.f;   // the forward-pass value
       if (g > DT_A) {
         if (i + 1 < rows) {
           g = fminf(g, r1[j] + DT_A);
@@ -470,13 +534,13 @@ chamfer_sdf_kernel(const float* __restrict__ phi, int rows, int cols, float dx,
       local = fmin(local, u);
       r0[j] = g;
     }
-    const double incl = dt_block_min_scan(local, wsum, true);
+    const double incl = dt_block_min_scan<NT>(local, wsum, true);
     double run = 1e300;
     {
       const double right = __shfl_down_sync(0xffffffffu, incl, 1);
       const int lane = threadIdx.x & 31;
       if (lane < 31) run = right;
-      else if ((threadIdx.x >> 5) < 31) run = wsum[32 + (threadIdx.x >> 5) + 1];
+      else if ((threadIdx.x >> 5) < NW - 1) run = wsum[32 + (threadIdx.x >> 5) + 1];
     }
     for (int q = per - 1; q >= 0; --q) {
       const int j = j0 + q;
@@ -487,25 +551,38 @@ chamfer_sdf_kernel(const float* __restrict__ phi, int rows, int cols, float dx,
       const double v = run - (double)j;
       const float out = v >= 1e299 ? FMAX : fminf(g, (float)v);
       r0[j] = out;
-      const float p = phi[(size_t)i * cols + j];
-      const bool in = p > 0.f;
-      if (inside_pass && in) sdf[(size_t)i * cols + j] = out >= FMAX ? FMAX : out * dx;
-      if (!inside_pass && !in) sdf[(size_t)i * cols + j] = out >= FMAX ? -FMAX : -out * dx;
+      if (inside(i, j) == inside_pass) {
+        if (inside_pass) sdf[(size_t)i * cols + j] = out >= FMAX ? FMAX : out * dx;
+        else sdf[(size_t)i * cols + j] = out >= FMAX ? -FMAX : -out * dx;
+      }
     }
     __syncthreads();
   }
 }
 
-cudaError_t launch_reinit_sdf(cudaStream_t s, int rows, int cols, const float* phi, float dx,
-                              float* work, float* sdf) {
+template <int NT>
+static cudaError_t chamfer_launch(cudaStream_t s, int rows, int cols, const float* phi,
+                                  float level, int inclusive, float dx, float* sdf, int nimg) {
   const size_t smem = (size_t)3 * cols * sizeof(float);
   if (smem > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(chamfer_sdf_kernel,
+    cudaError_t e = cudaFuncSetAttribute(chamfer_sdf_kernel<NT>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
   }
-  chamfer_sdf_kernel<<<2, DT_NT, smem, s>>>(phi, rows, cols, dx, work, sdf);
+  chamfer_sdf_kernel<NT><<<dim3(2, nimg), NT, smem, s>>>(phi, rows, cols, level, inclusive, dx, sdf);
   return cudaGetLastError();
+}
+
+cudaError_t launch_reinit_sdf(cudaStream_t s, int rows, int cols, const float* phi, float level,
+                              int inclusive, float dx, float* sdf, int nimg, int threads) {
+  if (nimg < 1 || nimg > 65535) return cudaErrorInvalidValue;
+  if (threads <= 0) threads = cols >= 3072 ? 1024 : cols >= 768 ? 512 : 256;
+  switch (threads) {
+    case 256: return chamfer_launch<256>(s, rows, cols, phi, level, inclusive, dx, sdf, nimg);
+    case 512: return chamfer_launch<512>(s, rows, cols, phi, level, inclusive, dx, sdf, nimg);
+    case 1024: return chamfer_launch<1024>(s, rows, cols, phi, level, inclusive, dx, sdf, nimg);
+    default: return cudaErrorInvalidValue;
+  }
 }
 
 cudaError_t launch_dt(cudaStream_t s, const float* vn, size_t n, float dx, float dy, float cfl,

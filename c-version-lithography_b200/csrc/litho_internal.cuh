@@ -288,16 +288,24 @@ inline bool tc2_supported(const BandGeom& g) {
 cudaError_t launch_levelset(cudaStream_t s, int what, int rows, int cols, const float* phi,
                             const float* phi0, const float* vn, float dx, float dy, float b,
                             const float* dt, float* out, float* out2,
-                            const int* window = nullptr);
+                            const int* window = nullptr, int nimg = 1,
+                            const int* d_windows = nullptr, int dt_stride = 0);
 // render_levelset_mask for nimg images of rows x cols: gray = 0 -> phi >= 0,
 // gray = 1 -> subpixel coverage of the scale-times bilinear upsampling.
 cudaError_t launch_render_mask(cudaStream_t s, const float* phi, int rows, int cols, int nimg,
                                int gray, int scale, float* mask);
 cudaError_t launch_dt(cudaStream_t s, const float* vn, size_t n, float dx, float dy, float cfl,
                       float b, float* part, float* vmax, float* dt, int* bad);
-// Chamfer signed distance of reinit_sdf; work holds 2 * rows * cols floats.
-cudaError_t launch_reinit_sdf(cudaStream_t s, int rows, int cols, const float* phi, float dx,
-                              float* work, float* sdf);
+// Chamfer signed distance of reinit_sdf over nimg rows x cols images back to back:
+// inside = phi > level (phi >= level when inclusive); sdf must not alias phi.
+// threads: CTA size (256, 512 or 1024; 0 picks by the row length).
+cudaError_t launch_reinit_sdf(cudaStream_t s, int rows, int cols, const float* phi, float level,
+                              int inclusive, float dx, float* sdf, int nimg = 1, int threads = 0);
+// max |Vn| and dt of nimg images of n pixels: vd[2 i] = max |Vn_i|, vd[2 i + 1] = dt_i;
+// part holds nimg * dt_batch_blocks(n, nimg) floats.
+int dt_batch_blocks(size_t n, int nimg);
+cudaError_t launch_dt_batch(cudaStream_t s, const float* vn, size_t n, int nimg, float dx,
+                            float dy, float cfl, float b, float* part, float* vd, int* bad);
 
 // Sparse EPE at host-selected edge points (epe.cu): eps n x 2 (y, x) and weights n,
 // device FP64. signed_epe (nullable) per point; partial: 3 FP64 sums per block
@@ -328,6 +336,13 @@ cudaError_t launch_ep_candidates(cudaStream_t s, const double* eps, const double
 cudaError_t launch_rect_losses(cudaStream_t s, const float* Wf, const float* T, const float* pe_w,
                                const float* pen_w, int ts, const int* rect, float pen_thr,
                                double* partial, int* nblocks);
+// Loss-region and Core sums of nimg tiles in one launch (rectangles: device, 4 ints
+// per tile); partial holds nimg * rect_losses_batch_blocks(ts) * 6 doubles.
+int rect_losses_batch_blocks(int ts);
+cudaError_t launch_rect_losses_batch(cudaStream_t s, const float* Wf, const float* T,
+                                     const float* pe_w, const float* pen_w, int ts,
+                                     const int* d_regions, const int* d_cores, float pen_thr,
+                                     double* partial, int nimg);
 cudaError_t launch_exchange(cudaStream_t s, const float* masks, const float* raw, int ntiles,
                             int ts, const int* nrel, const int* rel, int max_rel,
                             const litho_exchange_options& o, float* grad, double* cept_loss);
