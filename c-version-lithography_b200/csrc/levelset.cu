@@ -15,12 +15,13 @@
 namespace litho_b200 {
 
 constexpr int LS_TX = 32;      // tile width (x, columns)
-constexpr int LS_TY = 8;       // tile height (y, rows); each thread computes 2 rows
-constexpr int LS_RPT = 2;
+constexpr int LS_TY = 8;       // rows per pass of the CTA; each thread computes LS_RPT rows
+constexpr int LS_RPT = 4;
 constexpr int LS_H = 3;        // halo
 constexpr int LS_SW = LS_TX + 2 * LS_H;
 constexpr int LS_SH = LS_TY * LS_RPT + 2 * LS_H;
 constexpr int LS_NT = LS_TX * LS_TY;
+static_assert(LS_TX == 32 && LS_SW <= 64, "the tile loader maps one warp to one tile row");
 
 // WENO5-JS one-sided derivative from the five differences v1..v5 (already
 // divided by the spacing), level_set_utils.cpp:45-113. The smoothness
@@ -39,7 +40,10 @@ __device__ __forceinline__ float weno5(float v1, float v2, float v3, float v4, f
   const float q1 = v1 - 4.f * v2 + 3.f * v3;
   const float q2 = v2 - v4;
   const float q3 = 3.f * v3 - 4.f * v4 + v5;
-  const float inv = 1.f / vmax2;
+  // Approximate reciprocal and division (__fdividef, within 2 ulp): vmax2 and the
+  // weight sum below stay far inside the range where they are accurate, and the
+  // weights are a smooth function of both.
+  const float inv = __fdividef(1.f, vmax2);
   const float S1 = ((13.f / 12.f) * t1 * t1 + 0.25f * q1 * q1) * inv + 1e-6f;
   const float S2 = ((13.f / 12.f) * t2 * t2 + 0.25f * q2 * q2) * inv + 1e-6f;
   const float S3 = ((13.f / 12.f) * t3 * t3 + 0.25f * q3 * q3) * inv + 1e-6f;
@@ -48,7 +52,7 @@ __device__ __forceinline__ float weno5(float v1, float v2, float v3, float v4, f
   // [1e-6, 34], so the products stay well inside FP32 range.
   const float s1 = S1 * S1, s2 = S2 * S2, s3 = S3 * S3;
   const float b1 = 0.1f * (s2 * s3), b2 = 0.6f * (s1 * s3), b3 = 0.3f * (s1 * s2);
-  return (b1 * d1 + b2 * d2 + b3 * d3) / (b1 + b2 + b3);
+  return __fdividef(b1 * d1 + b2 * d2 + b3 * d3, b1 + b2 + b3);
 }
 
 // Godunov |grad phi| for the sign of the normal speed (level_set_utils.cpp:180-213).
@@ -70,11 +74,14 @@ __device__ __forceinline__ float godunov(float speed, float xm, float xp, float 
 
 __device__ __forceinline__ void load_tile(float (*t)[LS_SW], const float* __restrict__ phi,
                                           int rows, int cols, int y0, int x0) {
-  for (int e = threadIdx.x; e < LS_SH * LS_SW; e += LS_NT) {
-    const int ty = e / LS_SW, tx = e % LS_SW;
-    const int y = min(max(y0 - LS_H + ty, 0), rows - 1);
-    const int x = min(max(x0 - LS_H + tx, 0), cols - 1);
-    t[ty][tx] = __ldg(phi + (size_t)y * cols + x);
+  // warp w loads tile rows w, w + 8, ...; each lane columns lane and lane + 32
+  const int lane = threadIdx.x & 31;
+  const int xa = min(max(x0 - LS_H + lane, 0), cols - 1);
+  const int xb = min(max(x0 - LS_H + lane + 32, 0), cols - 1);
+  for (int ty = threadIdx.x >> 5; ty < LS_SH; ty += LS_NT / 32) {
+    const float* row = phi + (size_t)min(max(y0 - LS_H + ty, 0), rows - 1) * cols;
+    t[ty][lane] = __ldg(row + xa);
+    if (lane + 32 < LS_SW) t[ty][lane + 32] = __ldg(row + xb);
   }
 }
 
@@ -129,7 +136,7 @@ __device__ float kappa_term(const float (*t)[LS_SW], int ly, int lx, int y, int 
   else pyy = (py_at(1) - py_at(-1)) * iy;
   const float g2 = px * px + py * py;
   const float num = pxx * py * py - 2.f * px * py * pxy + pyy * px * px;
-  return g2 > (float)DBL_EPSILON ? b * (num / g2) : 0.f;
+  return g2 > (float)DBL_EPSILON ? b * __fdividef(num, g2) : 0.f;
 }
 
 __device__ float block_max(float v, float* sh) {
