@@ -1529,6 +1529,8 @@ struct litho_partition {
   // Loss sums: kSlots per tile (see litho_exchange_compute_epe), then 1 per tile (CEPT).
   static constexpr int kSlots = 14;
   double* d_loss = nullptr;
+  double* d_xpart = nullptr;   // exchange partial sums: ntiles * kMaxRel * 32
+
   std::vector<double> h_loss;
   // EPE work, allocated when an EPE term or the Core metrics are asked for: EPE
   // windows, the PE_EPE main region and its row-pass temporary (ntiles * ts * ts
@@ -1561,6 +1563,7 @@ void free_partition(litho_partition* p) {
   if (p->fe) cudaFree(p->fe);
   if (p->fm) cudaFree(p->fm);
   if (p->d_loss) cudaFree(p->d_loss);
+  if (p->d_xpart) cudaFree(p->d_xpart);
   if (p->d_epe_work) cudaFree(p->d_epe_work);
   if (p->d_ep) cudaFree(p->d_ep);
 }
@@ -1759,7 +1762,9 @@ int litho_exchange_compute_epe(litho_ctx* ctx, const litho_partition* cp, const 
     return ctx->fail(LITHO_ERR_INVALID_ARGUMENT, "MicroGradientExchange: too many EPs");
   if (!p->d_work) {
     if (cudaMalloc(&p->d_work, 4 * n * tt * sizeof(float)) != cudaSuccess ||
-        cudaMalloc(&p->d_loss, (size_t)(S + 1) * n * sizeof(double)) != cudaSuccess) {
+        cudaMalloc(&p->d_loss, (size_t)(S + 1) * n * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&p->d_xpart, (size_t)litho_partition::kMaxRel * n * 32 * sizeof(double)) !=
+            cudaSuccess) {
       cudaGetLastError();
       return ctx->fail(LITHO_ERR_OOM, "full-chip work allocation failed");
     }
@@ -1880,17 +1885,22 @@ int litho_exchange_compute_epe(litho_ctx* ctx, const litho_partition* cp, const 
     double* slot = p->d_loss + (size_t)S * t;
     const int grect[4] = {region[0] + oy, region[1] + oy, region[2] + ox, region[3] + ox};
     int used = 0;
-    int r = check_launch(ctx, launch_ep_candidates(s, ep_in, ep_in + 2 * (size_t)e.n_eps, e.n_eps,
-                                                   periods, p->height, p->width, oy, ox, grect, ts,
-                                                   epe_w + t * tt, cand, cand + 2 * ncand),
-                         "EP candidates");
-    if (!r)
-      r = check_launch(ctx, launch_epe(s, aer, ts, ts, cand, cand + 2 * ncand, (int)ncand,
-                                       threshold, e.epe_pixel_size, nullptr, part,
-                                       epe_grad ? dl : nullptr, epe_fac, &used),
-                       "sparse EPE");
-    if (!r) r = check_launch(ctx, launch_sum_partials(s, part, used, 3, slot + 2), "sum");
-    ctx->launches += 3;
+    int r = LITHO_OK;
+    // Without EPs the EPE sums and counts stay at their zeroed slots.
+    const bool eps_any = e.n_eps > 0;
+    if (eps_any) {
+      r = check_launch(ctx, launch_ep_candidates(s, ep_in, ep_in + 2 * (size_t)e.n_eps, e.n_eps,
+                                                 periods, p->height, p->width, oy, ox, grect, ts,
+                                                 epe_w + t * tt, cand, cand + 2 * ncand),
+                       "EP candidates");
+      if (!r)
+        r = check_launch(ctx, launch_epe(s, aer, ts, ts, cand, cand + 2 * ncand, (int)ncand,
+                                         threshold, e.epe_pixel_size, nullptr, part,
+                                         epe_grad ? dl : nullptr, epe_fac, &used),
+                         "sparse EPE");
+      if (!r) r = check_launch(ctx, launch_sum_partials(s, part, used, 3, slot + 2), "sum");
+      ctx->launches += 3;
+    }
     if (r || !core) return r;
     if (rects) {
       r = check_launch(ctx, launch_rect_losses(s, waf, targets + t * tt, pe_w + t * tt,
@@ -1907,17 +1917,19 @@ int litho_exchange_compute_epe(litho_ctx* ctx, const litho_partition* cp, const 
       ctx->launches += 4;
     }
     const int crect[4] = {R[0], R[1], R[2], R[3]};   // core_global
-    if (!r)
+    if (!r && eps_any) {
       r = check_launch(ctx, launch_ep_candidates(s, ep_in, ep_in + 2 * (size_t)e.n_eps, e.n_eps,
                                                  0, p->height, p->width, oy, ox, crect, ts,
                                                  epe_w + t * tt, cand, cand + 2 * ncand),
                        "core EP candidates");
-    if (!r)
-      r = check_launch(ctx, launch_epe(s, aer, ts, ts, cand, cand + 2 * ncand, e.n_eps, threshold,
-                                       e.epe_pixel_size, nullptr, part, nullptr, 0.0, &used),
-                       "core sparse EPE");
-    if (!r) r = check_launch(ctx, launch_sum_partials(s, part, used, 3, slot + 11), "sum");
-    ctx->launches += 3;
+      if (!r)
+        r = check_launch(ctx, launch_epe(s, aer, ts, ts, cand, cand + 2 * ncand, e.n_eps,
+                                         threshold, e.epe_pixel_size, nullptr, part, nullptr, 0.0,
+                                         &used),
+                         "core sparse EPE");
+      if (!r) r = check_launch(ctx, launch_sum_partials(s, part, used, 3, slot + 11), "sum");
+      ctx->launches += 3;
+    }
     return r;
   };
   // With an EPE gradient the adjoint needs dL/dI after the EP scatter, so the resist
@@ -2018,7 +2030,7 @@ int litho_exchange_compute_epe(litho_ctx* ctx, const litho_partition* cp, const 
   if (!st)
     st = check_launch(ctx, launch_exchange(s, d_masks, raw, n, ts, p->d_meta + p->off_nrel,
                                            p->d_meta + p->off_rel, litho_partition::kMaxRel, o,
-                                           d_grad, p->d_loss + (size_t)S * n),
+                                           d_grad, p->d_loss + (size_t)S * n, p->d_xpart),
                       "micro-gradient exchange");
   ctx->launches += 1;
   if (!st)

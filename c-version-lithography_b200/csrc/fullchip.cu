@@ -8,6 +8,7 @@
 // All tiles of a partition share one tile size ts and live contiguously as
 // [tile][ts][ts] float32 arrays.
 #include <cuda_runtime.h>
+#include <algorithm>
 
 #include "device_common.cuh"
 
@@ -218,11 +219,11 @@ rect_losses_batch_kernel(const float* __restrict__ Wf, const float* __restrict__
   const size_t img = (size_t)blockIdx.y * ts * ts;
   const int* rg = regions + 4 * (size_t)blockIdx.y;
   const int* cr = cores + 4 * (size_t)blockIdx.y;
-  const int y0 = rg[0], x0 = rg[2], cols = rg[3] - rg[2], n = (rg[1] - rg[0]) * cols;
   const int cy0 = cr[0], cy1 = cr[1], cx0 = cr[2], cx1 = cr[3];
   double v[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-  for (int i = blockIdx.x * RL_NT + threadIdx.x; i < n; i += gridDim.x * RL_NT) {
-    const int y = y0 + i / cols, x = x0 + i % cols;
+  // block b takes rows rg[0] + b, + gridDim.x, ...; the threads sweep the columns
+  for (int y = rg[0] + blockIdx.x; y < rg[1]; y += gridDim.x)
+  for (int x = rg[2] + threadIdx.x; x < rg[3]; x += RL_NT) {
     const size_t k = img + (size_t)y * ts + x;
     const double w = Wf[k], t = T[k], r = w - t;
     const double pe = r * r * (double)pe_w[k];
@@ -245,11 +246,7 @@ rect_losses_batch_kernel(const float* __restrict__ Wf, const float* __restrict__
   }
 }
 
-int rect_losses_batch_blocks(int ts) {
-  const int n = ts * ts;
-  const int b = (n + RL_NT - 1) / RL_NT;
-  return b < 1 ? 1 : (b > 48 ? 48 : b);
-}
+int rect_losses_batch_blocks(int ts) { return ts < 1 ? 1 : (ts > 96 ? 96 : ts); }
 
 cudaError_t launch_rect_losses_batch(cudaStream_t s, const float* Wf, const float* T,
                                      const float* pe_w, const float* pen_w, int ts,
@@ -275,75 +272,101 @@ __device__ __forceinline__ float linear_strength(int dir, int y, int x, int rows
   }
 }
 
-// One CTA per tile, over the guard strips only: grad holds a copy of raw on entry
-// and leaves as raw (fused on guards) + cept_weight * cept_grad; cept_loss[t] = sum
-// over neighbours of sum (A guard mask - B core mask)^2. Guard strips of different
-// neighbours are disjoint; the two-sided overlaps can share corner pixels, so the
-// neighbours are taken one after another.
+// Relation slot j of every tile (tile blockIdx.y; its j-th neighbour in the
+// reference's order), spread over gridDim.x CTAs per tile. grad holds a copy of raw
+// before slot 0 and leaves the last slot as raw (fused on guards) + cept_weight *
+// cept_grad. A relation's guard strip (outside the Core) and, two-sided, its
+// overlap strip (inside the Core) are disjoint, so one launch covers both; the
+// overlap strips of different relations share Core corners, so the slots run as
+// separate launches in the reference's order. part[(tile * max_rel + j) * gridDim.x +
+// block] = this block's sum of (A guard mask - B core mask)^2.
 __global__ void __launch_bounds__(EX_NT)
-exchange_kernel(const float* __restrict__ masks, const float* __restrict__ raw, int ts,
-                const int* __restrict__ nrel, const int* __restrict__ rel, int max_rel,
-                litho_exchange_options o, float* __restrict__ grad, double* __restrict__ cept_loss) {
+exchange_rel_kernel(const float* __restrict__ masks, const float* __restrict__ raw, int ts,
+                    const int* __restrict__ nrel, const int* __restrict__ rel, int max_rel, int j,
+                    litho_exchange_options o, float* __restrict__ grad,
+                    double* __restrict__ part) {
   __shared__ double sh[EX_NT / 32];
-  const int t = blockIdx.x;
+  const int t = blockIdx.y, nch = gridDim.x;
+  double* out = part + ((size_t)t * max_rel + j) * nch + blockIdx.x;
+  if (j >= nrel[t]) {
+    if (threadIdx.x == 0) *out = 0.0;
+    return;
+  }
   const size_t tt = (size_t)ts * ts;
   const float* mA = masks + t * tt;
   const float* rA = raw + t * tt;
   float* gA = grad + t * tt;
-  double loss = 0.0;
-  for (int j = 0; j < nrel[t]; ++j) {
-    const int* R = rel + ((size_t)t * max_rel + j) * REL_INTS;
-    const int nb = R[0], dir = R[1];
-    const int gy0 = R[2], gy1 = R[3], gx0 = R[4], gx1 = R[5];       // my guard (local A)
-    const int sy0 = R[6], sx0 = R[8];                                // neighbour overlap (local B)
-    const float* mB = masks + (size_t)nb * tt;
-    const float* rB = raw + (size_t)nb * tt;
-    const int rows = gy1 - gy0, cols = gx1 - gx0;
-    double part = 0.0;
-    for (int i = threadIdx.x; i < rows * cols; i += EX_NT) {
-      const int y = i / cols, x = i % cols;
-      const size_t ia = (size_t)(gy0 + y) * ts + gx0 + x;
-      const size_t ib = (size_t)(sy0 + y) * ts + sx0 + x;
-      float g = gA[ia];
-      if (o.enable_grad_fusion) {
-        const float s = o.fusion_mode == 0 ? 1.f : linear_strength(dir, y, x, rows, cols);
-        const float wn = (float)o.fusion_weight_neighbor * s;
-        if (wn != 0.f)
-          g = ((float)o.fusion_weight_owner * rA[ia] + wn * rB[ib]) /
-              ((float)o.fusion_weight_owner + wn);
-      }
-      if (o.enable_cept) {
-        const float d = mA[ia] - mB[ib];
-        part += (double)d * (double)d;
-        g += (float)o.cept_weight * 2.f * d;
-      }
-      gA[ia] = g;
+  const int* R = rel + ((size_t)t * max_rel + j) * REL_INTS;
+  const int nb = R[0], dir = R[1];
+  const int gy0 = R[2], gy1 = R[3], gx0 = R[4], gx1 = R[5];       // my guard (local A)
+  const int sy0 = R[6], sx0 = R[8];                                // neighbour overlap (local B)
+  const float* mB = masks + (size_t)nb * tt;
+  const float* rB = raw + (size_t)nb * tt;
+  const int rows = gy1 - gy0, cols = gx1 - gx0;
+  double acc = 0.0;
+  for (int i = blockIdx.x * EX_NT + threadIdx.x; i < rows * cols; i += nch * EX_NT) {
+    const int y = i / cols, x = i % cols;
+    const size_t ia = (size_t)(gy0 + y) * ts + gx0 + x;
+    const size_t ib = (size_t)(sy0 + y) * ts + sx0 + x;
+    float g = gA[ia];
+    if (o.enable_grad_fusion) {
+      const float st = o.fusion_mode == 0 ? 1.f : linear_strength(dir, y, x, rows, cols);
+      const float wn = (float)o.fusion_weight_neighbor * st;
+      if (wn != 0.f)
+        g = ((float)o.fusion_weight_owner * rA[ia] + wn * rB[ib]) /
+            ((float)o.fusion_weight_owner + wn);
     }
-    loss += part;
-    __syncthreads();
-    if (o.enable_cept && !o.cept_guard_only) {
-      // The neighbour's guard over this tile's Core edge drives the Core side too.
-      const int oy0 = R[10], oy1 = R[11], ox0 = R[12], ox1 = R[13];   // my overlap (local A)
-      const int ny0 = R[14], nx0 = R[16];                              // neighbour guard (local B)
-      const int orows = oy1 - oy0, ocols = ox1 - ox0;
-      for (int i = threadIdx.x; i < orows * ocols; i += EX_NT) {
-        const int y = i / ocols, x = i % ocols;
-        const size_t ia = (size_t)(oy0 + y) * ts + ox0 + x;
-        const size_t ib = (size_t)(ny0 + y) * ts + nx0 + x;
-        gA[ia] += (float)o.cept_weight * 2.f * (mA[ia] - mB[ib]);
-      }
-      __syncthreads();
+    if (o.enable_cept) {
+      const float d = mA[ia] - mB[ib];
+      acc += (double)d * (double)d;
+      g += (float)o.cept_weight * 2.f * d;
+    }
+    gA[ia] = g;
+  }
+  if (o.enable_cept && !o.cept_guard_only) {
+    // The neighbour's guard over this tile's Core edge drives the Core side too.
+    const int oy0 = R[10], oy1 = R[11], ox0 = R[12], ox1 = R[13];   // my overlap (local A)
+    const int ny0 = R[14], nx0 = R[16];                              // neighbour guard (local B)
+    const int orows = oy1 - oy0, ocols = ox1 - ox0;
+    for (int i = blockIdx.x * EX_NT + threadIdx.x; i < orows * ocols; i += nch * EX_NT) {
+      const int y = i / ocols, x = i % ocols;
+      const size_t ia = (size_t)(oy0 + y) * ts + ox0 + x;
+      const size_t ib = (size_t)(ny0 + y) * ts + nx0 + x;
+      gA[ia] += (float)o.cept_weight * 2.f * (mA[ia] - mB[ib]);
     }
   }
-  const double total = block_sum<EX_NT>(loss, sh);
-  if (threadIdx.x == 0) cept_loss[t] = total;
+  const double total = block_sum<EX_NT>(acc, sh);
+  if (threadIdx.x == 0) *out = total;
+}
+
+// cept_loss[t] = the tile's partial sums in a fixed order.
+__global__ void exchange_sum_kernel(const double* __restrict__ part, int per_tile, int ntiles,
+                                    double* __restrict__ cept_loss) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ntiles) return;
+  double s = 0.0;
+  for (int k = 0; k < per_tile; ++k) s += part[(size_t)t * per_tile + k];
+  cept_loss[t] = s;
+}
+
+int exchange_chunks(int ntiles) {
+  const int c = (4 * 148 + ntiles - 1) / std::max(ntiles, 1);
+  return c < 4 ? 4 : (c > 32 ? 32 : c);
 }
 
 cudaError_t launch_exchange(cudaStream_t s, const float* masks, const float* raw, int ntiles,
                             int ts, const int* nrel, const int* rel, int max_rel,
-                            const litho_exchange_options& o, float* grad, double* cept_loss) {
-  exchange_kernel<<<ntiles, EX_NT, 0, s>>>(masks, raw, ts, nrel, rel, max_rel, o, grad,
-                                           cept_loss);
+                            const litho_exchange_options& o, float* grad, double* cept_loss,
+                            double* part) {
+  if (ntiles < 1 || ntiles > 65535) return cudaErrorInvalidValue;
+  const int nch = exchange_chunks(ntiles);
+  for (int j = 0; j < max_rel; ++j) {
+    exchange_rel_kernel<<<dim3(nch, ntiles), EX_NT, 0, s>>>(masks, raw, ts, nrel, rel, max_rel, j,
+                                                           o, grad, part);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  exchange_sum_kernel<<<(ntiles + 127) / 128, 128, 0, s>>>(part, max_rel * nch, ntiles, cept_loss);
   return cudaGetLastError();
 }
 

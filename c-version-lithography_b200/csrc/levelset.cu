@@ -401,193 +401,279 @@ cudaError_t launch_render_mask(cudaStream_t s, const float* phi, int rows, int c
 // distanceTransform(DIST_L2, 5) calls, i.e. the 5x5 chamfer distance with
 // weights a = 1, b = 1.4, c = 2.1969 (float32) to the nearest feature pixel,
 // computed by a forward raster pass (rows top to bottom, left to right) and a
-// backward pass. Within a row the only dependency is d(j) = min(g(j), d(j-1) + a),
-// which is evaluated exactly as a min-plus prefix scan
-//   d(j) = j + min_{k <= j} (g(k) - k)     (double precision, then float),
-// g being the minimum over the already final rows above (below) plus the
-// pixel's own value. One CTA runs one transform of one image (blockIdx.y):
-// blockIdx.x = 0 measures inside pixels to the outside and writes +d dx at the
-// inside pixels, blockIdx.x = 1 measures outside pixels to the inside and writes
-// -d dx at the outside pixels. A transform's distance is 0 at its feature pixels
-// (the other class), so each CTA keeps its forward-pass values in the output at
-// its own pixels only: the two CTAs of an image touch disjoint pixels and need no
-// other buffer. Inside means phi > level (phi >= level when `inclusive`). With no
-// feature pixel at all the distance stays FLT_MAX, as OpenCV returns.
+// backward pass, each pixel taking the minimum of its own value and its already
+// final neighbours plus the weights. Within a row the only dependency is
+// d(j) = min(g(j), d(j-1) + a), g being the minimum over the rows above (below)
+// plus the pixel's own value. A CTA splits a row into one contiguous segment per
+// thread: each thread runs the recurrence over its segment from +inf, the segment
+// results are combined by a block scan with the composition
+//   (A1, L1) then (A2, L2)  ->  (min(A2, A1 + L2), L1 + L2)
+// (A: the value at the segment's last column, L: its length), and each thread reruns
+// its segment from the carry it receives. Float throughout, in a fixed order.
+//
+// One CTA runs one transform of one image (blockIdx.y): blockIdx.x = 0 measures
+// inside pixels to the outside and writes +d dx at the inside pixels, blockIdx.x = 1
+// measures outside pixels to the inside and writes -d dx at the outside pixels. A
+// transform's distance is 0 at its feature pixels (the other class), so each CTA keeps
+// its forward-pass values in the output at its own pixels only: the two CTAs of an
+// image touch disjoint pixels and need no other buffer. Inside means phi > level
+// (phi >= level when `inclusive`). With no feature pixel at all the distance stays
+// FLT_MAX, as OpenCV returns.
+//
+// PMAX > 0: a thread owns at most PMAX columns and holds their classification (and,
+// backward, their forward-pass values) in registers, loading the following rows'
+// while the current row is processed, so that the row loop waits on no global load.
+// PMAX == 0: the same transform with direct loads (very long rows).
 constexpr float DT_A = 1.0f, DT_B = 1.4f, DT_C = 2.1969f;
 
-template <int NT>
-__device__ __forceinline__ double dt_block_min_scan(double v, double* wsum, bool reverse) {
-  // inclusive prefix (reverse: suffix) minimum over the block in thread order
-  constexpr int NW = NT / 32;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const double u = reverse ? __shfl_down_sync(0xffffffffu, v, o) : __shfl_up_sync(0xffffffffu, v, o);
-    if (reverse ? (lane + o < 32) : (lane >= o)) v = fmin(v, u);
-  }
-  if (lane == (reverse ? 0 : 31)) wsum[warp] = v;
-  __syncthreads();
-  if (warp == 0) {
-    double t = lane < NW ? wsum[lane] : 1e300;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const double u = reverse ? __shfl_down_sync(0xffffffffu, t, o) : __shfl_up_sync(0xffffffffu, t, o);
-      if (reverse ? (lane + o < 32) : (lane >= o)) t = fmin(t, u);
-    }
-    wsum[32 + lane] = t;  // inclusive scan of warp totals
-  }
-  __syncthreads();
-  double carry = 1e300;
-  if (!reverse && warp > 0) carry = wsum[32 + warp - 1];
-  if (reverse && warp < NW - 1) carry = wsum[32 + warp + 1];
-  __syncthreads();
-  return fmin(v, carry);
-}
-
-template <int NT>
+template <int NT, int PMAX>
 __global__ void __launch_bounds__(NT)
 chamfer_sdf_kernel(const float* __restrict__ phi_all, int rows, int cols, float level,
                    int inclusive, float dx, float* __restrict__ sdf_all) {
-  extern __shared__ float rowbuf[];  // 3 rows of cols floats: ring of the last rows
-  __shared__ double wsum[64];
+  extern __shared__ float rowbuf[];  // ring of 3 rows of W = cols + 4 floats, column j at j + 2
+  __shared__ float wtot[32];
   constexpr int NW = NT / 32;
+  constexpr int QN = PMAX > 0 ? PMAX : 1;
+  const float FMAX = 3.402823466e38f;
+  const int W = cols + 4;
   const bool inside_pass = blockIdx.x == 0;
   const size_t img = (size_t)blockIdx.y * rows * cols;
   const float* phi = phi_all + img;
   float* sdf = sdf_all + img;
-  const int per = (cols + NT - 1) / NT;  // contiguous columns per thread
-  const int j0 = threadIdx.x * per;
-  const float FMAX = 3.402823466e38f;
-  auto inside = [&](int i, int j) {
-    const float p = phi[(size_t)i * cols + j];
-    return inclusive ? p >= level : p > level;
+  const int per = (cols + NT - 1) / NT;  // columns per thread
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int j0 = min((int)threadIdx.x * per, cols);
+  const int nq = min(per, cols - j0);    // columns this thread owns (0 past the row end)
+  auto seg_end = [&](int t) { return min((t + 1) * per, cols); };   // one past the last column
+  auto seg_start = [&](int t) { return min(t * per, cols); };
+  if (threadIdx.x < 3) {  // +inf pads: two columns on each side of every ring row
+    float* r = rowbuf + threadIdx.x * W;
+    r[0] = r[1] = r[W - 2] = r[W - 1] = FMAX;
+  }
+  auto cls = [&](float p) { return (inclusive ? p >= level : p > level) == inside_pass; };
+  auto load_bits = [&](int i) {
+    unsigned b = 0;
+#pragma unroll
+    for (int q = 0; q < QN; ++q)
+      if (q < nq && cls(phi[(size_t)i * cols + j0 + q])) b |= 1u << q;
+    return b;
   };
+  unsigned bits0 = 0, bits1 = 0;   // own-pixel bits of the current row and the next one
+  float pf[QN];                    // phi of a following row, in flight
+  float fv[QN];                    // backward: forward-pass values of the current row
+  auto own = [&](int i, int q) -> bool {
+    if constexpr (PMAX > 0) return ((bits0 >> q) & 1u) != 0u;
+    else return cls(phi[(size_t)i * cols + j0 + q]);
+  };
+  const int qn = PMAX > 0 ? QN : per;
+
   // ---- forward pass
+  if constexpr (PMAX > 0) bits0 = load_bits(0);
   for (int i = 0; i < rows; ++i) {
-    float* r0 = rowbuf + (i % 3) * cols;
-    const float* r1 = rowbuf + ((i + 2) % 3) * cols;  // row i-1
-    const float* r2 = rowbuf + ((i + 1) % 3) * cols;  // row i-2
-    double local = 1e300;
-    for (int q = 0; q < per; ++q) {
+    float* r0 = rowbuf + (i % 3) * W + 2;
+    const float* r1 = rowbuf + ((i + 2) % 3) * W + 2;  // row i-1
+    const float* r2 = rowbuf + ((i + 1) % 3) * W + 2;  // row i-2
+    float a = FMAX;
+#pragma unroll
+    for (int q = 0; q < qn; ++q) {
+      if (q >= nq) break;
       const int j = j0 + q;
-      if (j >= cols) break;
-      float g = FMAX;
-      if (inside(i, j) != inside_pass) {  // a feature pixel of this transform
-        g = 0.f;
-      } else {
-        if (i >= 1) {
-          g = fminf(g, r1[j] + DT_A);
-          if (j >= 1) g = fminf(g, r1[j - 1] + DT_B);
-          if (j + 1 < cols) g = fminf(g, r1[j + 1] + DT_B);
-          if (j >= 2) g = fminf(g, r1[j - 2] + DT_C);
-          if (j + 2 < cols) g = fminf(g, r1[j + 2] + DT_C);
-        }
-        if (i >= 2) {
-          if (j >= 1) g = fminf(g, r2[j - 1] + DT_C);
-          if (j + 1 < cols) g = fminf(g, r2[j + 1] + DT_C);
-        }
+      float g = 0.f;   // a feature pixel of this transform
+      if (own(i, q)) {
+        g = FMAX;
+        if (i >= 1)
+          g = fminf(fminf(fminf(r1[j] + DT_A, r1[j - 1] + DT_B), fminf(r1[j + 1] + DT_B, r1[j - 2] + DT_C)),
+                    r1[j + 2] + DT_C);
+        if (i >= 2) g = fminf(g, fminf(r2[j - 1] + DT_C, r2[j + 1] + DT_C));
       }
-      const double u = (g >= FMAX ? 1e300 : (double)g - (double)j);
-      local = fmin(local, u);
-      r0[j] = g;  // provisional
+      a = fminf(g, a + DT_A);
+      r0[j] = g;
     }
-    // exclusive carry from the threads on the left
-    const double incl = dt_block_min_scan<NT>(local, wsum, false);
-    double run = 1e300;
-    {
-      const double left = __shfl_up_sync(0xffffffffu, incl, 1);
-      const int lane = threadIdx.x & 31;
-      if (lane > 0) run = left;
-      else if (threadIdx.x > 0) run = wsum[32 + (threadIdx.x >> 5) - 1];
+    if constexpr (PMAX > 0) {
+      if (i + 1 < rows) {
+#pragma unroll
+        for (int q = 0; q < QN; ++q) pf[q] = q < nq ? phi[(size_t)(i + 1) * cols + j0 + q] : 0.f;
+      }
     }
-    for (int q = 0; q < per; ++q) {
+    // inclusive scan over the threads of the segment results
+    float v = a;
+    const int e = seg_end(threadIdx.x);
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const float u = __shfl_up_sync(0xffffffffu, v, o);
+      if (lane >= o) v = fminf(v, u + (float)(e - seg_end(threadIdx.x - o)));
+    }
+    if (lane == 31) wtot[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+      float x = lane < NW ? wtot[lane] : FMAX;
+      const int ew = seg_end(32 * lane + 31);
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const float u = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o && lane < NW) x = fminf(x, u + (float)(ew - seg_end(32 * (lane - o) + 31)));
+      }
+      if (lane < NW) wtot[lane] = x;
+    }
+    __syncthreads();
+    // carry: the value at column j0 - 1
+    float c = __shfl_up_sync(0xffffffffu, v, 1);
+    if (lane == 0) c = FMAX;
+    if (warp > 0) {
+      const int wend = seg_end(32 * warp - 1);   // end of the previous warp's segments
+      const float wc = wtot[warp - 1] + (float)(j0 - wend);
+      c = lane == 0 ? wtot[warp - 1] : fminf(c, wc);
+    }
+    float d = c;
+#pragma unroll
+    for (int q = 0; q < qn; ++q) {
+      if (q >= nq) break;
       const int j = j0 + q;
-      if (j >= cols) break;
-      const float g = r0[j];
-      const double u = (g >= FMAX ? 1e300 : (double)g - (double)j);
-      run = fmin(run, u);
-      const double v = run + (double)j;
-      r0[j] = v >= 1e299 ? FMAX : fminf(g, (float)v);
-      if (inside(i, j) == inside_pass) sdf[(size_t)i * cols + j] = r0[j];
+      d = fminf(r0[j], d + DT_A);
+      r0[j] = d;
+      if (own(i, q)) sdf[(size_t)i * cols + j] = d;
+    }
+    if constexpr (PMAX > 0) {
+      if (i + 1 < rows) {
+        unsigned b = 0;
+#pragma unroll
+        for (int q = 0; q < QN; ++q)
+          if (q < nq && cls(pf[q])) b |= 1u << q;
+        bits0 = b;
+      }
     }
     __syncthreads();
   }
   // ---- backward pass
+  if constexpr (PMAX > 0) {
+    bits0 = load_bits(rows - 1);
+    bits1 = rows >= 2 ? load_bits(rows - 2) : 0u;
+#pragma unroll
+    for (int q = 0; q < QN; ++q)
+      fv[q] = (q < nq && ((bits0 >> q) & 1u)) ? sdf[(size_t)(rows - 1) * cols + j0 + q] : 0.f;
+  }
   for (int i = rows - 1; i >= 0; --i) {
     const int slot = (rows - 1 - i);
-    float* r0 = rowbuf + (slot % 3) * cols;
-    const float* r1 = rowbuf + ((slot + 2) % 3) * cols;  // row i+1 (final)
-    const float* r2 = rowbuf + ((slot + 1) % 3) * cols;  // row i+2 (final)
-    double local = 1e300;
-    for (int q = 0; q < per; ++q) {
+    float* r0 = rowbuf + (slot % 3) * W + 2;
+    const float* r1 = rowbuf + ((slot + 2) % 3) * W + 2;  // row i+1 (final)
+    const float* r2 = rowbuf + ((slot + 1) % 3) * W + 2;  // row i+2 (final)
+    float a = FMAX;
+#pragma unroll
+    for (int qq = 0; qq < qn; ++qq) {
+      const int q = qn - 1 - qq;   // right to left
+      if (q >= nq) continue;
       const int j = j0 + q;
-      if (j >= cols) break;
-      const bool own = inside(i, j) == inside_pass;
-      float g = own ? sdf[(size_t)i * cols + j] : 0.f;   // the forward-pass value
+      float g;   // the forward-pass value (0 at a feature pixel)
+      if constexpr (PMAX > 0) g = fv[q];
+      else g = own(i, q) ? sdf[(size_t)i * cols + j] : 0.f;
       if (g > DT_A) {
-        if (i + 1 < rows) {
-          g = fminf(g, r1[j] + DT_A);
-          if (j + 1 < cols) g = fminf(g, r1[j + 1] + DT_B);
-          if (j >= 1) g = fminf(g, r1[j - 1] + DT_B);
-          if (j + 2 < cols) g = fminf(g, r1[j + 2] + DT_C);
-          if (j >= 2) g = fminf(g, r1[j - 2] + DT_C);
-        }
-        if (i + 2 < rows) {
-          if (j + 1 < cols) g = fminf(g, r2[j + 1] + DT_C);
-          if (j >= 1) g = fminf(g, r2[j - 1] + DT_C);
-        }
+        if (i + 1 < rows)
+          g = fminf(g, fminf(fminf(fminf(r1[j] + DT_A, r1[j + 1] + DT_B), fminf(r1[j - 1] + DT_B, r1[j + 2] + DT_C)),
+                             r1[j - 2] + DT_C));
+        if (i + 2 < rows) g = fminf(g, fminf(r2[j + 1] + DT_C, r2[j - 1] + DT_C));
       }
-      const double u = (g >= FMAX ? 1e300 : (double)g + (double)j);
-      local = fmin(local, u);
+      a = fminf(g, a + DT_A);
       r0[j] = g;
     }
-    const double incl = dt_block_min_scan<NT>(local, wsum, true);
-    double run = 1e300;
-    {
-      const double right = __shfl_down_sync(0xffffffffu, incl, 1);
-      const int lane = threadIdx.x & 31;
-      if (lane < 31) run = right;
-      else if ((threadIdx.x >> 5) < NW - 1) run = wsum[32 + (threadIdx.x >> 5) + 1];
-    }
-    for (int q = per - 1; q >= 0; --q) {
-      const int j = j0 + q;
-      if (j >= cols) continue;
-      const float g = r0[j];
-      const double u = (g >= FMAX ? 1e300 : (double)g + (double)j);
-      run = fmin(run, u);
-      const double v = run - (double)j;
-      const float out = v >= 1e299 ? FMAX : fminf(g, (float)v);
-      r0[j] = out;
-      if (inside(i, j) == inside_pass) {
-        if (inside_pass) sdf[(size_t)i * cols + j] = out >= FMAX ? FMAX : out * dx;
-        else sdf[(size_t)i * cols + j] = out >= FMAX ? -FMAX : -out * dx;
+    if constexpr (PMAX > 0) {
+      // forward values of row i - 1 (its bits are known), phi of row i - 2
+      if (i >= 1) {
+#pragma unroll
+        for (int q = 0; q < QN; ++q)
+          fv[q] = (q < nq && ((bits1 >> q) & 1u)) ? sdf[(size_t)(i - 1) * cols + j0 + q] : 0.f;
       }
+      if (i >= 2) {
+#pragma unroll
+        for (int q = 0; q < QN; ++q) pf[q] = q < nq ? phi[(size_t)(i - 2) * cols + j0 + q] : 0.f;
+      }
+    }
+    // inclusive scan from the right of the segment results (value at a segment's first column)
+    float v = a;
+    const int st = seg_start(threadIdx.x);
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const float u = __shfl_down_sync(0xffffffffu, v, o);
+      if (lane + o < 32) v = fminf(v, u + (float)(seg_start(threadIdx.x + o) - st));
+    }
+    if (lane == 0) wtot[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+      float x = lane < NW ? wtot[lane] : FMAX;
+      const int sw = seg_start(32 * lane);
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const float u = __shfl_down_sync(0xffffffffu, x, o);
+        if (lane + o < NW) x = fminf(x, u + (float)(seg_start(32 * (lane + o)) - sw));
+      }
+      if (lane < NW) wtot[lane] = x;
+    }
+    __syncthreads();
+    // carry: the value at column j0 + nq (the next segment's first column)
+    float c = __shfl_down_sync(0xffffffffu, v, 1);
+    if (lane == 31) c = FMAX;
+    if (warp < NW - 1) {
+      const int wst = seg_start(32 * (warp + 1));   // first column of the next warp's segments
+      const float wc = wtot[warp + 1] + (float)(wst - seg_start(threadIdx.x + 1));
+      c = lane == 31 ? wtot[warp + 1] : fminf(c, wc);
+    }
+    float d = c;
+#pragma unroll
+    for (int qq = 0; qq < qn; ++qq) {
+      const int q = qn - 1 - qq;
+      if (q >= nq) continue;
+      const int j = j0 + q;
+      d = fminf(r0[j], d + DT_A);
+      r0[j] = d;
+      if (own(i, q)) {
+        if (inside_pass) sdf[(size_t)i * cols + j] = d >= FMAX ? FMAX : d * dx;
+        else sdf[(size_t)i * cols + j] = d >= FMAX ? -FMAX : -d * dx;
+      }
+    }
+    if constexpr (PMAX > 0) {
+      unsigned b = 0;
+      if (i >= 2) {
+#pragma unroll
+        for (int q = 0; q < QN; ++q)
+          if (q < nq && cls(pf[q])) b |= 1u << q;
+      }
+      bits0 = bits1;
+      bits1 = b;
     }
     __syncthreads();
   }
 }
 
-template <int NT>
+template <int NT, int PMAX>
 static cudaError_t chamfer_launch(cudaStream_t s, int rows, int cols, const float* phi,
                                   float level, int inclusive, float dx, float* sdf, int nimg) {
-  const size_t smem = (size_t)3 * cols * sizeof(float);
+  const size_t smem = (size_t)3 * (cols + 4) * sizeof(float);
   if (smem > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(chamfer_sdf_kernel<NT>,
+    cudaError_t e = cudaFuncSetAttribute(chamfer_sdf_kernel<NT, PMAX>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
   }
-  chamfer_sdf_kernel<NT><<<dim3(2, nimg), NT, smem, s>>>(phi, rows, cols, level, inclusive, dx, sdf);
+  chamfer_sdf_kernel<NT, PMAX><<<dim3(2, nimg), NT, smem, s>>>(phi, rows, cols, level, inclusive,
+                                                               dx, sdf);
   return cudaGetLastError();
 }
 
 cudaError_t launch_reinit_sdf(cudaStream_t s, int rows, int cols, const float* phi, float level,
                               int inclusive, float dx, float* sdf, int nimg, int threads) {
-  if (nimg < 1 || nimg > 65535) return cudaErrorInvalidValue;
-  if (threads <= 0) threads = cols >= 3072 ? 1024 : cols >= 768 ? 512 : 256;
+  if (nimg < 1 || nimg > 65535 || rows < 1 || cols < 1) return cudaErrorInvalidValue;
+  if (threads <= 0) threads = cols <= 4096 ? 128 : cols <= 8192 ? 256 : 1024;
+  const int per = (cols + threads - 1) / threads;
+  // the register arrays hold the smallest of 8, 16, 32 columns that covers a segment
   switch (threads) {
-    case 256: return chamfer_launch<256>(s, rows, cols, phi, level, inclusive, dx, sdf, nimg);
-    case 512: return chamfer_launch<512>(s, rows, cols, phi, level, inclusive, dx, sdf, nimg);
-    case 1024: return chamfer_launch<1024>(s, rows, cols, phi, level, inclusive, dx, sdf, nimg);
+    case 128:
+      if (per <= 8) return chamfer_launch<128, 8>(s, rows, cols, phi, level, inclusive, dx, sdf, nimg);
+      if (per <= 16) return chamfer_launch<128, 16>(s, rows, cols, phi, level, inclusive, dx, sdf, nimg);
+      if (per <= 32) return chamfer_launch<128, 32>(s, rows, cols, phi, level, inclusive, dx, sdf, nimg);
+      return cudaErrorInvalidValue;
+    case 256:
+      if (per <= 32) return chamfer_launch<256, 32>(s, rows, cols, phi, level, inclusive, dx, sdf, nimg);
+      return cudaErrorInvalidValue;
+    case 1024:
+      return chamfer_launch<1024, 0>(s, rows, cols, phi, level, inclusive, dx, sdf, nimg);
     default: return cudaErrorInvalidValue;
   }
 }

@@ -298,7 +298,8 @@ cudaError_t launch_dt(cudaStream_t s, const float* vn, size_t n, float dx, float
                       float b, float* part, float* vmax, float* dt, int* bad);
 // Chamfer signed distance of reinit_sdf over nimg rows x cols images back to back:
 // inside = phi > level (phi >= level when inclusive); sdf must not alias phi.
-// threads: CTA size (256, 512 or 1024; 0 picks by the row length).
+// threads: CTA size (128 or 256 for rows of up to 32 columns per thread, 1024; 0 picks
+// by the row length).
 cudaError_t launch_reinit_sdf(cudaStream_t s, int rows, int cols, const float* phi, float level,
                               int inclusive, float dx, float* sdf, int nimg = 1, int threads = 0);
 // max |Vn| and dt of nimg images of n pixels: vd[2 i] = max |Vn_i|, vd[2 i + 1] = dt_i;
@@ -345,7 +346,10 @@ cudaError_t launch_rect_losses_batch(cudaStream_t s, const float* Wf, const floa
                                      double* partial, int nimg);
 cudaError_t launch_exchange(cudaStream_t s, const float* masks, const float* raw, int ntiles,
                             int ts, const int* nrel, const int* rel, int max_rel,
-                            const litho_exchange_options& o, float* grad, double* cept_loss);
+                            const litho_exchange_options& o, float* grad, double* cept_loss,
+                            double* part);
+// CTAs per tile and relation of launch_exchange; part holds ntiles * max_rel * that.
+int exchange_chunks(int ntiles);
 cudaError_t launch_theta_update(cudaStream_t s, float* theta, const float* grad, int ntiles,
                                 int ts, const int* win, float lr, float* mask);
 
