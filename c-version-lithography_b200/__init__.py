@@ -113,6 +113,7 @@ SIGNATURES = {
     "litho_evolution_term": (_I, [_P, _I, _I, _P, _P, _D, _D, _D, _D, _P, _PD]),
     "litho_lsm_rk2_update": (_I, [_P, _I, _I, _P, _P, _D, _D, _D, _D, _P, _P, _PD]),
     "litho_reinit_sdf": (_I, [_P, _I, _I, _P, _D, _D, _P, _P]),
+    "litho_reinit_sdf_batch": (_I, [_P, _I, _I, _I, _P, _D, _D, _D, _P, _P]),
     "litho_partition_create": (_I, [_P, _I, _I, _I, _I, _I, _I, _PP]),
     "litho_partition_destroy": (_I, [_P]),
     "litho_partition_info": (_I, [_P, _PI, _PI]),
@@ -579,6 +580,27 @@ class LevelSetUtils:
         ctx._check(ctx.lib.litho_reinit_sdf(ctx.handle, p.shape[0], p.shape[1], _ptr(p), float(dx),
                                             float(dy), _ptr(out), _ptr(mask)))
         return (out, mask) if with_mask else out
+
+    @staticmethod
+    def reinit_sdf_batch(phi, dx, dy, level=0.0, out=None, mask_out=None, ctx=None):
+        """reinit_sdf of a batch (batch, rows, cols) in one launch, inside = phi > level
+        (level 0.5 on binary masks: the LSM initialisation reinit_sdf(mask - 0.5)).
+        Writes `out` (allocated when None) and `mask_out` (optional); returns out."""
+        ctx = ctx or default_context()
+        torch = ctx.torch
+        p = _f32(phi, torch)
+        if p.dim() != 3:
+            raise LithoError(2, "phi must be (batch, rows, cols)")
+        if out is None:
+            out = torch.empty_like(p)
+        for t in (out, mask_out):
+            if t is not None and (t.shape != p.shape or t.dtype != torch.float32
+                                  or not t.is_contiguous() or not t.is_cuda):
+                raise LithoError(2, "outputs must be contiguous float32 CUDA tensors shaped like phi")
+        ctx._check(ctx.lib.litho_reinit_sdf_batch(ctx.handle, p.shape[0], p.shape[1], p.shape[2],
+                                                  _ptr(p), float(level), float(dx), float(dy),
+                                                  _ptr(out), _ptr(mask_out)))
+        return out
 
     @staticmethod
     def rk2_update_batch(phi, Vn, dx, dy, cfl, b, phi_out, mask_out=None, ctx=None):

@@ -1427,6 +1427,33 @@ int litho_reinit_sdf(litho_ctx* ctx, int rows, int cols, const float* d_phi, dou
   return st;
 }
 
+int litho_reinit_sdf_batch(litho_ctx* ctx, int batch, int rows, int cols, const float* d_phi,
+                           double level, double dx, double dy, float* d_sdf, float* d_mask) {
+  if (!ctx || batch < 1 || !d_phi || !d_sdf) return LITHO_ERR_INVALID_ARGUMENT;
+  int st = ls_check(ctx, rows, cols, dx, dy, 1);
+  if (st) return st;
+  if (!std::isfinite(level)) return ctx->fail(LITHO_ERR_NONFINITE, "reinit_sdf: level must be finite");
+  if ((size_t)3 * cols * sizeof(float) > 200 * 1024)
+    return ctx->fail(LITHO_ERR_UNSUPPORTED, "reinit_sdf supports at most 17066 columns");
+  if (d_sdf == d_phi || (d_mask && (d_mask == d_phi || d_mask == d_sdf)))
+    return ctx->fail(LITHO_ERR_INVALID_ARGUMENT, "reinit_sdf: sdf, mask and phi must not alias");
+  const size_t n = (size_t)rows * cols;
+  for (int b0 = 0; b0 < batch && !st; b0 += 65535) {
+    const int B = std::min(batch - b0, 65535);
+    st = check_launch(ctx, launch_reinit_sdf(ctx->stream, rows, cols, d_phi + b0 * n, (float)level,
+                                             0, (float)dx, d_sdf + b0 * n, B),
+                      "reinit_sdf");
+    if (!st && d_mask)
+      st = check_launch(ctx, launch_levelset(ctx->stream, 5, rows, cols, d_sdf + b0 * n, nullptr,
+                                             nullptr, (float)dx, (float)dy, 0.f, nullptr,
+                                             d_mask + b0 * n, nullptr, nullptr, B),
+                        "mask");
+    ctx->launches += d_mask ? 2 : 1;
+  }
+  if (!st) LITHO_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  return st;
+}
+
 int litho_lsm_rk2_update(litho_ctx* ctx, int rows, int cols, const float* d_phi,
                          const float* d_vn, double dx, double dy, double cfl, double b,
                          float* d_phi_out, float* d_mask, double* dt) {

@@ -660,7 +660,12 @@ static cudaError_t chamfer_launch(cudaStream_t s, int rows, int cols, const floa
 cudaError_t launch_reinit_sdf(cudaStream_t s, int rows, int cols, const float* phi, float level,
                               int inclusive, float dx, float* sdf, int nimg, int threads) {
   if (nimg < 1 || nimg > 65535 || rows < 1 || cols < 1) return cudaErrorInvalidValue;
-  if (threads <= 0) threads = cols <= 4096 ? 128 : cols <= 8192 ? 256 : 1024;
+  // Many images: small CTAs (long segments, little scan overhead, many CTAs per SM).
+  // Few images: the row latency decides, so short segments over more threads.
+  if (threads <= 0) {
+    if (nimg >= 64) threads = cols <= 4096 ? 128 : cols <= 8192 ? 256 : 1024;
+    else threads = cols <= 1536 ? 512 : 1024;
+  }
   const int per = (cols + threads - 1) / threads;
   // the register arrays hold the smallest of 8, 16, 32 columns that covers a segment
   switch (threads) {
@@ -671,6 +676,10 @@ cudaError_t launch_reinit_sdf(cudaStream_t s, int rows, int cols, const float* p
       return cudaErrorInvalidValue;
     case 256:
       if (per <= 32) return chamfer_launch<256, 32>(s, rows, cols, phi, level, inclusive, dx, sdf, nimg);
+      return cudaErrorInvalidValue;
+    case 512:
+      if (per <= 8) return chamfer_launch<512, 8>(s, rows, cols, phi, level, inclusive, dx, sdf, nimg);
+      if (per <= 16) return chamfer_launch<512, 16>(s, rows, cols, phi, level, inclusive, dx, sdf, nimg);
       return cudaErrorInvalidValue;
     case 1024:
       return chamfer_launch<1024, 0>(s, rows, cols, phi, level, inclusive, dx, sdf, nimg);

@@ -132,7 +132,7 @@ class TileServer:
         return sum(len(c.solves) for c in self.classes.values())
 
     def _admit(self):
-        torch = self.ctx.torch
+        first: Dict[int, int] = {}      # size -> first slot admitted by this call
         while self.queue:
             s = self.queue[0]
             cls = self.classes.get(s.N)
@@ -143,14 +143,20 @@ class TileServer:
                 break   # first come, first served: a blocked head blocks the queue
             self.queue.popleft()
             i = len(cls.solves)
+            first.setdefault(s.N, i)
             cls.solves.append(s)
             self.held += need
             s.t_admit = time.perf_counter()
-            phi = LevelSetUtils.reinit_sdf(s.mask0 - 0.5, self.dx, self.dy, ctx=self.ctx)
-            cls.phi[i].copy_(phi)
             cls.mask[i].copy_(s.mask0)
             cls.target[i].copy_(s.target)
             s.best_mask = s.mask0.clone()
+        # phi = reinit_sdf(mask - 0.5) (LSM_Optimizer.cpp:62) of every solve admitted
+        # here, one launch per size: inside = mask > 0.5 is the same classification.
+        for N, i0 in first.items():
+            cls = self.classes[N]
+            n = len(cls.solves)
+            LevelSetUtils.reinit_sdf_batch(cls.mask[i0:n], self.dx, self.dy, level=0.5,
+                                           out=cls.phi[i0:n], ctx=self.ctx)
 
     def step(self) -> List[TileSolve]:
         """Admit what fits, advance every admitted solve by one iteration, retire the

@@ -251,6 +251,12 @@ int litho_evolution_term(litho_ctx* ctx, int rows, int cols, const float* d_phi,
  * value). d_mask (nullable) receives the printed mask sdf >= 0 as 1/0 floats. */
 int litho_reinit_sdf(litho_ctx* ctx, int rows, int cols, const float* d_phi, double dx,
                      double dy, float* d_sdf, float* d_mask);
+/* litho_reinit_sdf for `batch` images ([batch][rows][cols]) in one launch, inside =
+ * phi > level: level 0.5 on a binary mask gives reinit_sdf(mask - 0.5), the LSM
+ * initialisation (LSM_Optimizer.cpp:62), without the shifted copy. d_sdf and d_mask
+ * must not alias d_phi. */
+int litho_reinit_sdf_batch(litho_ctx* ctx, int batch, int rows, int cols, const float* d_phi,
+                           double level, double dx, double dy, float* d_sdf, float* d_mask);
 /* One RK2 level-set update (LSM_Optimizer.cpp:109-115, the second stage reuses
  * the first stage's dt) and the printed mask (phi >= 0) (LSM_Optimizer.cpp:128).
  * d_phi_out may alias nothing else; d_mask (nullable) receives 1/0 floats. */

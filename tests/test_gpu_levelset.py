@@ -158,6 +158,25 @@ def test_reinit_sdf_of_binary_mask(L):
     assert np.all(np.abs(got - ref) <= 1e-5 * np.abs(ref) + 1e-6)
 
 
+def test_reinit_sdf_batch(L):
+    """reinit_sdf_batch with level 0.5 on binary masks equals reinit_sdf(mask - 0.5) of
+    each image (one launch for the batch; the printed mask is sdf >= 0)."""
+    torch = pytest.importorskip("torch")
+    wl = importlib.import_module("c-version-lithography_b200.workloads")
+    masks = np.stack([wl.manhattan_target(300, 6, seed=s) for s in range(3)])
+    m = torch.tensor(masks, dtype=torch.float32, device="cuda")
+    mask_out = torch.empty_like(m)
+    out = L.LevelSetUtils.reinit_sdf_batch(m, 2.0, 2.0, level=0.5, mask_out=mask_out)
+    for b in range(3):
+        ref = L.LevelSetUtils.reinit_sdf(m[b] - 0.5, 2.0, 2.0)
+        assert torch.equal(out[b], ref), b
+        assert torch.equal(mask_out[b], (ref >= 0).float()), b
+        oc = lo.reinit_sdf(masks[b] - 0.5, 2.0, 2.0)
+        assert np.all(np.abs(cpu(out[b]) - oc) <= 1e-5 * np.abs(oc) + 1e-6)
+    with pytest.raises(L.LithoError):
+        L.LevelSetUtils.reinit_sdf_batch(m, 2.0, 2.0, out=m)
+
+
 def test_reinit_without_boundary(L):
     """No feature pixel: OpenCV returns FLT_MAX; the sign follows inside/outside."""
     got = cpu(L.LevelSetUtils.reinit_sdf(np.full((8, 8), 2.0), 1.0, 1.0))
