@@ -119,12 +119,26 @@ __device__ __forceinline__ float grad_y(const float (*t)[LS_SW], int ly, int lx,
 __device__ float kappa_term(const float (*t)[LS_SW], int ly, int lx, int y, int x, int rows,
                             int cols, float dx, float dy, float b) {
   const float ix = 1.f / (2.f * dx), iy = 1.f / (2.f * dy);
+  float px, py, pxy, pxx, pyy;
+  if (x >= 2 && x < cols - 2 && y >= 2 && y < rows - 2) {
+    // Away from the image border every difference below is the central one: the
+    // same arithmetic as the general path, without its border tests.
+    auto cx = [&](int oy, int ox) { return (t[ly + oy][lx + ox + 1] - t[ly + oy][lx + ox - 1]) * ix; };
+    auto cy = [&](int oy) { return (t[ly + oy + 1][lx] - t[ly + oy - 1][lx]) * iy; };
+    px = cx(0, 0);
+    py = cy(0);
+    pxy = (cx(1, 0) - cx(-1, 0)) * iy;
+    pxx = (cx(0, 1) - cx(0, -1)) * ix;
+    pyy = (cy(1) - cy(-1)) * iy;
+    const float g2 = px * px + py * py;
+    const float num = pxx * py * py - 2.f * px * py * pxy + pyy * px * px;
+    return g2 > (float)DBL_EPSILON ? b * __fdividef(num, g2) : 0.f;
+  }
   // phi_x at (y, x) and its row/column neighbours used by the second derivatives.
   auto px_at = [&](int oy, int ox) { return grad_x(t, ly + oy, lx + ox, x + ox, cols, ix); };
   auto py_at = [&](int oy) { return grad_y(t, ly + oy, lx, y + oy, rows, iy); };
-  const float px = px_at(0, 0);
-  const float py = py_at(0);
-  float pxy, pxx, pyy;
+  px = px_at(0, 0);
+  py = py_at(0);
   if (y == 0) pxy = (-3.f * px + 4.f * px_at(1, 0) - px_at(2, 0)) * iy;
   else if (y == rows - 1) pxy = (3.f * px - 4.f * px_at(-1, 0) + px_at(-2, 0)) * iy;
   else pxy = (px_at(1, 0) - px_at(-1, 0)) * iy;
