@@ -1,7 +1,7 @@
 """Split-BF16 tensor-core (tcgen05) row syntheses against the FP64 oracle.
 
 Tolerances for the split-BF16 path: aerial image max|dI| <= 1e-4 of peak (the
-north star allows 1e-3 for split-BF16), gradients relative L2 <= 1e-3, PE
+bound stated for split-BF16 is 1e-3), gradients relative L2 <= 1e-3, PE
 relative 1e-4. Results must also agree with the FP32 path of the same library.
 """
 import importlib
