@@ -1930,18 +1930,18 @@ int litho_exchange_compute_epe(litho_ctx* ctx, const litho_partition* cp, const 
     }
     if (r || !core) return r;
     if (rects) {
-      r = check_launch(ctx, launch_rect_losses(s, waf, targets + t * tt, pe_w + t * tt,
-                                               pen_w + t * tt, ts, region,
-                                               (float)o.penalty_threshold, part, &used),
-                       "region losses");
-      if (!r) r = check_launch(ctx, launch_sum_partials(s, part, used, 3, slot + 5), "sum");
+      // Loss-region and Core sums of this tile in one pass, straight to slots 5..10.
+      r = check_launch(ctx, launch_rect_losses_batch(
+                                s, waf, targets + t * tt, pe_w + t * tt, pen_w + t * tt, ts,
+                                p->d_meta + (guard_region ? p->off_update : p->off_core_l) + 4 * t,
+                                p->d_meta + p->off_core_l + 4 * t, (float)o.penalty_threshold,
+                                part, 1),
+                       "region and core losses");
       if (!r)
-        r = check_launch(ctx, launch_rect_losses(s, waf, targets + t * tt, pe_w + t * tt,
-                                                 pen_w + t * tt, ts, R + 8,
-                                                 (float)o.penalty_threshold, part, &used),
-                         "core losses");
-      if (!r) r = check_launch(ctx, launch_sum_partials(s, part, used, 3, slot + 8), "sum");
-      ctx->launches += 4;
+        r = check_launch(ctx, launch_sum_partials_batch(s, part, rect_losses_batch_blocks(ts), 6,
+                                                        part, 0, 0, slot + 5, 1),
+                         "sum");
+      ctx->launches += 2;
     }
     const int crect[4] = {R[0], R[1], R[2], R[3]};   // core_global
     if (!r && eps_any) {

@@ -15,21 +15,28 @@
 namespace litho_b200 {
 
 // out[t][y][x] = global[(oy_t + y) mod H][(ox_t + x) mod W]
+// Tile t's rows are spread over the CTAs of grid row t, the threads over the columns;
+// the periodic wrap of a row start is taken once per row and column once per thread.
 __global__ void tiles_extract_kernel(const float* __restrict__ g, int H, int W,
                                      const int* __restrict__ origins, int ts,
                                      float* __restrict__ out) {
   const int t = blockIdx.y;
   const int oy = origins[2 * t], ox = origins[2 * t + 1];
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ts * ts; i += gridDim.x * blockDim.x) {
-    const int y = i / ts, x = i % ts;
-    const int gy = ((oy + y) % H + H) % H, gx = ((ox + x) % W + W) % W;
-    out[(size_t)t * ts * ts + i] = g[(size_t)gy * W + gx];
+  const int gx0 = ((ox % W) + W) % W;
+  for (int y = blockIdx.x; y < ts; y += gridDim.x) {
+    const float* grow = g + (size_t)(((oy + y) % H + H) % H) * W;
+    float* orow = out + ((size_t)t * ts + y) * ts;
+    for (int x = threadIdx.x; x < ts; x += blockDim.x) {
+      int gx = gx0 + x;
+      if (gx >= W) gx = gx - W < W ? gx - W : gx % W;
+      orow[x] = __ldg(grow + gx);
+    }
   }
 }
 
 cudaError_t launch_tiles_extract(cudaStream_t s, const float* g, int H, int W, int ntiles,
                                  const int* origins, int ts, float* out) {
-  dim3 grid((ts * ts + 255) / 256 < 64 ? (ts * ts + 255) / 256 : 64, ntiles);
+  dim3 grid(ts < 256 ? ts : 256, ntiles);
   tiles_extract_kernel<<<grid, 256, 0, s>>>(g, H, W, origins, ts, out);
   return cudaGetLastError();
 }
@@ -67,24 +74,26 @@ __global__ void loss_windows_kernel(const float* __restrict__ target, int ts,
   const int t = blockIdx.y;
   const int y0 = region[4 * t], y1 = region[4 * t + 1], x0 = region[4 * t + 2],
             x1 = region[4 * t + 3];
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ts * ts; i += gridDim.x * blockDim.x) {
-    const int y = i / ts, x = i % ts;
-    const size_t k = (size_t)t * ts * ts + i;
-    const bool in = y >= y0 && y < y1 && x >= x0 && x < x1;
-    const float T = target[k];
-    const float e = loss_type == LITHO_MICRO_LOSS_PE_EPE ? main_dil[k] : 1.f;
-    float pe = loss_type == LITHO_MICRO_LOSS_PE_PENALTY ? (T > 0.5f ? 1.f : 0.f) : 1.f;
-    if (loss_type == LITHO_MICRO_LOSS_PE_EPE) pe = 1.f - e;
-    pe_w[k] = in ? pe : 0.f;
-    pen_w[k] = in && T < 0.5f ? 1.f : 0.f;
-    if (epe_w) epe_w[k] = in ? e : 0.f;
+  for (int y = blockIdx.x; y < ts; y += gridDim.x) {
+    const bool row_in = y >= y0 && y < y1;
+    for (int x = threadIdx.x; x < ts; x += blockDim.x) {
+      const size_t k = ((size_t)t * ts + y) * ts + x;
+      const bool in = row_in && x >= x0 && x < x1;
+      const float T = target[k];
+      const float e = loss_type == LITHO_MICRO_LOSS_PE_EPE ? main_dil[k] : 1.f;
+      float pe = loss_type == LITHO_MICRO_LOSS_PE_PENALTY ? (T > 0.5f ? 1.f : 0.f) : 1.f;
+      if (loss_type == LITHO_MICRO_LOSS_PE_EPE) pe = 1.f - e;
+      pe_w[k] = in ? pe : 0.f;
+      pen_w[k] = in && T < 0.5f ? 1.f : 0.f;
+      if (epe_w) epe_w[k] = in ? e : 0.f;
+    }
   }
 }
 
 cudaError_t launch_loss_windows(cudaStream_t s, const float* target, int ntiles, int ts,
                                 const int* region, int loss_type, const float* main_dil,
                                 float* pe_w, float* pen_w, float* epe_w) {
-  dim3 grid((ts * ts + 255) / 256 < 128 ? (ts * ts + 255) / 256 : 128, ntiles);
+  dim3 grid(ts < 256 ? ts : 256, ntiles);
   loss_windows_kernel<<<grid, 256, 0, s>>>(target, ts, region, loss_type, main_dil, pe_w, pen_w,
                                            epe_w);
   return cudaGetLastError();
@@ -165,51 +174,14 @@ cudaError_t launch_ep_candidates(cudaStream_t s, const double* eps, const double
   return cudaGetLastError();
 }
 
-// Loss sums over one rectangle of a tile (the Core metrics of
-// micro_gradient_exchange.cpp:224-233), per CTA in FP64: sum pe_w (W - T)^2,
-// sum_{T < 0.5} pen_w max(W - pen_thr, 0)^2 and sum_{T > 0.5} (W - T)^2.
+// Loss sums over the loss region and the Core of a group of tiles in one launch
+// (the Core metrics of micro_gradient_exchange.cpp:224-233), per CTA in FP64:
+// sum pe_w (W - T)^2, sum_{T < 0.5} pen_w max(W - pen_thr, 0)^2 and
+// sum_{T > 0.5} (W - T)^2. Tile blockIdx.y (images ts x ts back to back, rectangles
+// {y0, y1, x0, x1} 4 ints per tile), the Core being inside the region.
+// partial[(tile * gridDim.x + block) * 6 + k]: k = 0..2 the three sums over the
+// region, 3..5 over the Core.
 constexpr int RL_NT = 256;
-__global__ void __launch_bounds__(RL_NT)
-rect_losses_kernel(const float* __restrict__ Wf, const float* __restrict__ T,
-                   const float* __restrict__ pe_w, const float* __restrict__ pen_w, int ts, int y0,
-                   int y1, int x0, int x1, float pen_thr, double* __restrict__ partial) {
-  __shared__ double sh[RL_NT / 32];
-  const int cols = x1 - x0, n = (y1 - y0) * cols;
-  double pe = 0.0, bg = 0.0, mainpe = 0.0;
-  for (int i = blockIdx.x * RL_NT + threadIdx.x; i < n; i += gridDim.x * RL_NT) {
-    const size_t k = (size_t)(y0 + i / cols) * ts + x0 + i % cols;
-    const double w = Wf[k], t = T[k], r = w - t;
-    pe += r * r * (double)pe_w[k];
-    if (t < 0.5) {
-      const double ex = fmax(0.0, w - (double)pen_thr);
-      bg += (double)pen_w[k] * ex * ex;
-    }
-    if (t > 0.5) mainpe += r * r;
-  }
-  const double a = block_sum<RL_NT>(pe, sh);
-  const double b = block_sum<RL_NT>(bg, sh);
-  const double c = block_sum<RL_NT>(mainpe, sh);
-  if (threadIdx.x == 0) {
-    partial[3 * blockIdx.x] = a;
-    partial[3 * blockIdx.x + 1] = b;
-    partial[3 * blockIdx.x + 2] = c;
-  }
-}
-
-cudaError_t launch_rect_losses(cudaStream_t s, const float* Wf, const float* T, const float* pe_w,
-                               const float* pen_w, int ts, const int* rect, float pen_thr,
-                               double* partial, int* nblocks) {
-  const int n = (rect[1] - rect[0]) * (rect[3] - rect[2]);
-  *nblocks = n <= 0 ? 1 : ((n + RL_NT - 1) / RL_NT < 64 ? (n + RL_NT - 1) / RL_NT : 64);
-  rect_losses_kernel<<<*nblocks, RL_NT, 0, s>>>(Wf, T, pe_w, pen_w, ts, rect[0], rect[1], rect[2],
-                                                rect[3], pen_thr, partial);
-  return cudaGetLastError();
-}
-
-// The loss-region and Core sums of a group of tiles in one launch: tile blockIdx.y
-// (images ts x ts back to back, rectangles {y0, y1, x0, x1} 4 ints per tile), the
-// Core being inside the region. partial[(tile * gridDim.x + block) * 6 + k]: k = 0..2
-// the three sums over the region, 3..5 over the Core.
 __global__ void __launch_bounds__(RL_NT)
 rect_losses_batch_kernel(const float* __restrict__ Wf, const float* __restrict__ T,
                          const float* __restrict__ pe_w, const float* __restrict__ pen_w, int ts,
@@ -378,21 +350,23 @@ __global__ void theta_update_kernel(float* __restrict__ theta, const float* __re
                                     float* __restrict__ mask) {
   const int t = blockIdx.y;
   const int y0 = win[4 * t], y1 = win[4 * t + 1], x0 = win[4 * t + 2], x1 = win[4 * t + 3];
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ts * ts; i += gridDim.x * blockDim.x) {
-    const int y = i / ts, x = i % ts;
-    const size_t k = (size_t)t * ts * ts + i;
-    float th = theta[k];
-    if (grad && y >= y0 && y < y1 && x >= x0 && x < x1) {
-      th -= lr * (-0.5f * grad[k] * sinf(th));
-      theta[k] = th;
+  for (int y = blockIdx.x; y < ts; y += gridDim.x) {
+    const bool row_in = grad && y >= y0 && y < y1;
+    for (int x = threadIdx.x; x < ts; x += blockDim.x) {
+      const size_t k = ((size_t)t * ts + y) * ts + x;
+      float th = theta[k];
+      if (row_in && x >= x0 && x < x1) {
+        th -= lr * (-0.5f * grad[k] * sinf(th));
+        theta[k] = th;
+      }
+      mask[k] = 0.5f * (1.f + cosf(th));
     }
-    mask[k] = 0.5f * (1.f + cosf(th));
   }
 }
 
 cudaError_t launch_theta_update(cudaStream_t s, float* theta, const float* grad, int ntiles,
                                 int ts, const int* win, float lr, float* mask) {
-  dim3 grid((ts * ts + 255) / 256 < 64 ? (ts * ts + 255) / 256 : 64, ntiles);
+  dim3 grid(ts < 256 ? ts : 256, ntiles);
   theta_update_kernel<<<grid, 256, 0, s>>>(theta, grad, ts, win, lr, mask);
   return cudaGetLastError();
 }

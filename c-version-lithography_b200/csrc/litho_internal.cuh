@@ -334,9 +334,6 @@ cudaError_t launch_dilate_main(cudaStream_t s, const float* target, int ntiles, 
 cudaError_t launch_ep_candidates(cudaStream_t s, const double* eps, const double* w, int n,
                                  int periods, int H, int W, int oy, int ox, const int* grect,
                                  int ts, const float* win, double* out_eps, double* out_w);
-cudaError_t launch_rect_losses(cudaStream_t s, const float* Wf, const float* T, const float* pe_w,
-                               const float* pen_w, int ts, const int* rect, float pen_thr,
-                               double* partial, int* nblocks);
 // Loss-region and Core sums of nimg tiles in one launch (rectangles: device, 4 ints
 // per tile); partial holds nimg * rect_losses_batch_blocks(ts) * 6 doubles.
 int rect_losses_batch_blocks(int ts);
