@@ -114,6 +114,9 @@ SIGNATURES = {
     "litho_lsm_rk2_update": (_I, [_P, _I, _I, _P, _P, _D, _D, _D, _D, _P, _P, _PD]),
     "litho_reinit_sdf": (_I, [_P, _I, _I, _P, _D, _D, _P, _P]),
     "litho_reinit_sdf_batch": (_I, [_P, _I, _I, _I, _P, _D, _D, _D, _P, _P]),
+    "litho_lbfgs_dots": (_I, [_P, _I, ctypes.c_longlong, _P, ctypes.c_longlong, _P, _PD]),
+    "litho_lbfgs_combine": (_I, [_P, _I, ctypes.c_longlong, _P, ctypes.c_longlong, _PD, _P, _D,
+                                 _P]),
     "litho_partition_create": (_I, [_P, _I, _I, _I, _I, _I, _I, _PP]),
     "litho_partition_destroy": (_I, [_P]),
     "litho_partition_info": (_I, [_P, _PI, _PI]),
@@ -775,7 +778,7 @@ class CTMOptimizer:
             return pe, gt.clone(), norm
 
         theta, self.lbfgs_info = minimize_lbfgs(fg, theta, m=self.m, epsilon=self.tol,
-                                                max_iterations=self.iterations)
+                                                max_iterations=self.iterations, ctx=self.ctx)
         self.theta = theta
         return 0.5 * (1.0 + torch.cos(theta))
 

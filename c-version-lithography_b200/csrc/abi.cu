@@ -1427,6 +1427,48 @@ int litho_reinit_sdf(litho_ctx* ctx, int rows, int cols, const float* d_phi, dou
   return st;
 }
 
+int litho_lbfgs_dots(litho_ctx* ctx, int k, long long n, const float* d_rows, long long ld,
+                     const float* d_v, double* out) {
+  if (!ctx || k < 1 || k > 64 || n < 1 || ld < n || !d_rows || !d_v || !out)
+    return LITHO_ERR_INVALID_ARGUMENT;
+  if (cudaSetDevice(ctx->device) != cudaSuccess) return ctx->fail(LITHO_ERR_CUDA, "cudaSetDevice");
+  const int nb = multi_dot_blocks((size_t)n);
+  int st = ctx->ensure_red(RED_PART + (size_t)nb * k + (size_t)k + 8);
+  if (st) return st;
+  double* part = ctx->d_red + RED_PART;
+  double* res = part + (size_t)nb * k;
+  st = check_launch(ctx, launch_multi_dot(ctx->stream, d_rows, (size_t)ld, k, (size_t)n, d_v, part,
+                                          res),
+                    "L-BFGS inner products");
+  ctx->launches += 2;
+  if (st) return st;
+  LITHO_CUDA_TRY(ctx, cudaMemcpyAsync(out, res, (size_t)k * sizeof(double), cudaMemcpyDeviceToHost,
+                                      ctx->stream));
+  LITHO_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  return LITHO_OK;
+}
+
+int litho_lbfgs_combine(litho_ctx* ctx, int k, long long n, const float* d_rows, long long ld,
+                        const double* coef, const float* d_v, double cv, float* d_out) {
+  if (!ctx || k < 0 || k > 64 || n < 1 || !d_v || !d_out ||
+      (k > 0 && (!d_rows || ld < n || !coef)))
+    return LITHO_ERR_INVALID_ARGUMENT;
+  if (d_out == d_v) return ctx->fail(LITHO_ERR_INVALID_ARGUMENT, "L-BFGS combine: out must not alias v");
+  if (!std::isfinite(cv) || (k > 0 && !finite_all(coef, (size_t)k)))
+    return ctx->fail(LITHO_ERR_NONFINITE, "L-BFGS combine: coefficients must be finite");
+  if (cudaSetDevice(ctx->device) != cudaSuccess) return ctx->fail(LITHO_ERR_CUDA, "cudaSetDevice");
+  int st = ctx->ensure_red(RED_PART + 64 + 8);
+  if (st) return st;
+  double* dc = ctx->d_red + RED_PART;
+  if (k > 0)
+    LITHO_CUDA_TRY(ctx, cudaMemcpyAsync(dc, coef, (size_t)k * sizeof(double), cudaMemcpyHostToDevice,
+                                        ctx->stream));
+  ctx->launches += 1;
+  return check_launch(ctx, launch_combine(ctx->stream, d_rows, (size_t)ld, k, (size_t)n, dc, d_v,
+                                          cv, d_out),
+                      "L-BFGS direction");
+}
+
 int litho_reinit_sdf_batch(litho_ctx* ctx, int batch, int rows, int cols, const float* d_phi,
                            double level, double dx, double dy, float* d_sdf, float* d_mask) {
   if (!ctx || batch < 1 || !d_phi || !d_sdf) return LITHO_ERR_INVALID_ARGUMENT;

@@ -334,6 +334,14 @@ cudaError_t launch_dilate_main(cudaStream_t s, const float* target, int ntiles, 
 cudaError_t launch_ep_candidates(cudaStream_t s, const double* eps, const double* w, int n,
                                  int periods, int H, int W, int oy, int ox, const int* grect,
                                  int ts, const float* win, double* out_eps, double* out_w);
+// L-BFGS vector kernels (lbfgs.cu): out[j] = rows[j] . v in FP64 (k <= 64 rows of
+// length n, row stride ld; partial holds multi_dot_blocks(n) * k doubles), and
+// out = cv v + sum_j coef[j] rows[j] (coef: k device doubles).
+int multi_dot_blocks(size_t n);
+cudaError_t launch_multi_dot(cudaStream_t s, const float* rows, size_t ld, int k, size_t n,
+                             const float* v, double* partial, double* out);
+cudaError_t launch_combine(cudaStream_t s, const float* rows, size_t ld, int k, size_t n,
+                           const double* coef, const float* v, double cv, float* out);
 // Loss-region and Core sums of nimg tiles in one launch (rectangles: device, 4 ints
 // per tile); partial holds nimg * rect_losses_batch_blocks(ts) * 6 doubles.
 int rect_losses_batch_blocks(int ts);

@@ -9,33 +9,110 @@ Alg. 3.5/3.6 strong-Wolfe line search, ftol 1e-4, wolfe 0.9, first step
 1/||g||, later steps 1): the vectors stay float32 on the device, every inner
 product and the recursion scalars are float64.
 
+The two-loop recursion is evaluated in its Gram form: every inner product it takes
+is a combination of s_i . y_j, y_i . y_j, s_i . g and y_i . g, so the library keeps
+the history pairs as rows of one device array, returns those inner products in one
+pass over the rows (litho_lbfgs_dots, FP64 accumulation), the recursion's scalars
+are formed on the host in FP64 exactly as the two loops form them, and one more pass
+builds the direction -H g (litho_lbfgs_combine). Per iteration that is three passes
+over the history (the new gradient, the new pair's two vectors) instead of one pass
+per inner product.
+
 Stopping rule, as LBFGS++: ||g|| <= epsilon before the first step (zero
 iterations, one evaluation) or after any iteration, or ``max_iterations``
 iterations done.
 """
 from __future__ import annotations
 
+import ctypes
 import math
 
+import numpy as np
 
-def _dot(a, b) -> float:
-    return float((a.double() * b.double()).sum())
+
+class _Device:
+    """The library's L-BFGS vector kernels on float32 CUDA tensors of n elements."""
+
+    def __init__(self, ctx, n: int):
+        self.ctx, self.n = ctx, n
+
+    def dots(self, rows, k: int, v) -> np.ndarray:
+        """rows[0..k) . v in FP64; rows: a (>= k, n) contiguous float32 tensor."""
+        out = np.empty(k, dtype=np.float64)
+        self.ctx._check(self.ctx.lib.litho_lbfgs_dots(
+            self.ctx.handle, k, self.n, ctypes.c_void_p(rows.data_ptr()), self.n,
+            ctypes.c_void_p(v.data_ptr()), out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+        return out
+
+    def dot(self, a, b) -> float:
+        return float(self.dots(a, 1, b)[0])
+
+    def combine(self, rows, coef: np.ndarray, v, cv: float, out):
+        """out = cv v + sum_j coef[j] rows[j]."""
+        c = np.ascontiguousarray(coef, dtype=np.float64)
+        self.ctx._check(self.ctx.lib.litho_lbfgs_combine(
+            self.ctx.handle, len(c), self.n, ctypes.c_void_p(rows.data_ptr()), self.n,
+            c.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), ctypes.c_void_p(v.data_ptr()),
+            float(cv), ctypes.c_void_p(out.data_ptr())))
+        return out
+
+
+def two_loop_coefficients(order, SY, YY, rho, gp, m):
+    """The two-loop recursion (Nocedal & Wright Alg. 7.4) in Gram form, FP64.
+
+    order: history slots, oldest first; SY[a, b] = s_a . y_b, YY[a, b] = y_a . y_b,
+    rho[a] = 1 / (s_a . y_a); gp = (s_0 . g .. s_{m-1} . g, y_0 . g .. y_{m-1} . g).
+    Returns (coef, gamma) with -H g = -gamma g + sum_j coef[j] s_j + coef[m + j] y_j:
+    the same alpha_i = rho_i s_i . q (newest first) and beta_i = rho_i y_i . r (oldest
+    first) as the loops over vectors, with q and r expanded on the basis {g, s, y}."""
+    alpha, beta = {}, {}
+    done = []
+    for i in reversed(order):                       # q = g - sum_{newer j} alpha_j y_j
+        alpha[i] = rho[i] * (gp[i] - sum(alpha[j] * SY[i, j] for j in done))
+        done.append(i)
+    gamma = SY[order[-1], order[-1]] / YY[order[-1], order[-1]] if order else 1.0
+    done = []
+    for i in order:                                 # r = gamma q + sum_{older p} (a_p - b_p) s_p
+        yr = gamma * (gp[m + i] - sum(alpha[j] * YY[i, j] for j in order))
+        yr += sum((alpha[p] - beta[p]) * SY[p, i] for p in done)
+        beta[i] = rho[i] * yr
+        done.append(i)
+    coef = np.zeros(2 * m)
+    for j in order:
+        coef[j] = -(alpha[j] - beta[j])
+        coef[m + j] = gamma * alpha[j]
+    return coef, gamma
 
 
 def minimize_lbfgs(fg, x, m=10, epsilon=1e-5, max_iterations=100, ftol=1e-4, wolfe=0.9,
-                   max_linesearch=20, min_step=1e-20, max_step=1e20):
-    """Minimise f from x. ``fg(x) -> (f, g, ||g||)``; returns (x, info)."""
+                   max_linesearch=20, min_step=1e-20, max_step=1e20, ctx=None):
+    """Minimise f from x (a contiguous float32 CUDA tensor). ``fg(x) -> (f, g, ||g||)``;
+    returns (x, info). ctx: the library context whose stream the vectors live on."""
+    if ctx is None:
+        from . import default_context
+        ctx = default_context()
+    torch = ctx.torch
+    dev = _Device(ctx, x.numel())
     f, g, gnorm = fg(x)
     info = dict(iterations=0, evaluations=1, f=f, grad_norm=gnorm, reason="gradient tolerance")
     if gnorm <= epsilon:
         return x, info
-    S, Y, RHO = [], [], []
+    n = x.numel()
+    rows = torch.zeros((2 * m, n), dtype=torch.float32, device=x.device)   # s slots | y slots
+    pair = torch.empty((2, n), dtype=torch.float32, device=x.device)        # new s, y
+    # Every trial point is formed in the same buffer, so that the evaluations of a
+    # line search see the same input (the library replays its captured chain).
+    trial = torch.empty_like(x)
+    SY = np.zeros((m, m))   # SY[a, b] = s_a . y_b  (slots)
+    YY = np.zeros((m, m))   # YY[a, b] = y_a . y_b
+    rho = np.zeros(m)
+    order: list = []        # slots, oldest first
     d = -g
-    step = 1.0 / math.sqrt(_dot(d, d))
+    step = 1.0 / math.sqrt(dev.dot(d, d))
     k = 0
     while True:
         x_old, g_old, f_old = x, g, f
-        dg0 = _dot(g, d)
+        dg0 = dev.dot(g, d)
         if dg0 >= 0:
             info["reason"] = "not a descent direction"
             break
@@ -44,16 +121,16 @@ def minimize_lbfgs(fg, x, m=10, epsilon=1e-5, max_iterations=100, ftol=1e-4, wol
         f_lo, dg_lo = f_old, dg0
         accepted = False
         for _ in range(max_linesearch):
-            xt = x_old + step * d
-            ft, gt, gn = fg(xt)
+            torch.add(x_old, d, alpha=step, out=trial)
+            ft, gt, gn = fg(trial)
             info["evaluations"] += 1
-            dgt = _dot(gt, d)
+            dgt = dev.dot(gt, d)
             if ft > f_old + ftol * step * dg0 or (lo > 0 and ft >= f_lo):
                 hi = step
             else:
                 if abs(dgt) <= -wolfe * dg0:
                     accepted = True
-                    x, f, g, gnorm = xt, ft, gt, gn
+                    x, f, g, gnorm = trial.clone(), ft, gt, gn
                     break
                 if dgt * (hi - lo if math.isfinite(hi) else 1.0) >= 0:
                     hi = lo
@@ -67,8 +144,9 @@ def minimize_lbfgs(fg, x, m=10, epsilon=1e-5, max_iterations=100, ftol=1e-4, wol
         if not accepted:
             # Keep the best Armijo point found, as a failed search still moves.
             if lo > 0:
-                x = x_old + lo * d
-                f, g, gnorm = fg(x)
+                torch.add(x_old, d, alpha=lo, out=trial)
+                f, g, gnorm = fg(trial)
+                x = trial.clone()
                 info["evaluations"] += 1
             else:
                 info["reason"] = "line search failed"
@@ -80,26 +158,26 @@ def minimize_lbfgs(fg, x, m=10, epsilon=1e-5, max_iterations=100, ftol=1e-4, wol
         if k >= max_iterations:
             info["reason"] = "maximum iterations"
             break
-        s = x - x_old
-        y = g - g_old
-        sy = _dot(s, y)
-        if sy > 1e-10 * _dot(y, y):
-            if len(S) == m:
-                S.pop(0); Y.pop(0); RHO.pop(0)
-            S.append(s); Y.append(y); RHO.append(1.0 / sy)
-        # Two-loop recursion (FP64 scalars).
-        q = g.clone()
-        alphas = []
-        for s_i, y_i, r_i in zip(reversed(S), reversed(Y), reversed(RHO)):
-            a = r_i * _dot(s_i, q)
-            alphas.append(a)
-            q = q - a * y_i
-        if S:
-            q = q * (_dot(S[-1], Y[-1]) / _dot(Y[-1], Y[-1]))
-        for (s_i, y_i, r_i), a in zip(zip(S, Y, RHO), reversed(alphas)):
-            b = r_i * _dot(y_i, q)
-            q = q + (a - b) * s_i
-        d = -q
+        torch.sub(x.view(-1), x_old.view(-1), out=pair[0])
+        torch.sub(g.view(-1), g_old.view(-1), out=pair[1])
+        sy, yy = dev.dots(pair, 2, pair[1])
+        if sy > 1e-10 * yy:
+            if len(order) == m:
+                order.pop(0)
+            slot = next(i for i in range(m) if i not in order)
+            rows[slot].copy_(pair[0])
+            rows[m + slot].copy_(pair[1])
+            order.append(slot)
+            ds = dev.dots(rows, 2 * m, pair[0])   # s . s_b | s . y_b
+            dy = dev.dots(rows, 2 * m, pair[1])   # y . s_b | y . y_b
+            for b in order:
+                SY[slot, b] = ds[m + b]
+                SY[b, slot] = dy[b]
+                YY[slot, b] = YY[b, slot] = dy[m + b]
+            rho[slot] = 1.0 / sy
+        gp = dev.dots(rows, 2 * m, g.view(-1)) if order else np.zeros(2 * m)
+        coef, gamma = two_loop_coefficients(order, SY, YY, rho, gp, m)
+        d = dev.combine(rows, coef, g.view(-1), -gamma, torch.empty_like(g)).view_as(g)
         step = 1.0
     info.update(iterations=k, f=f, grad_norm=gnorm)
     return x, info

@@ -251,6 +251,17 @@ int litho_evolution_term(litho_ctx* ctx, int rows, int cols, const float* d_phi,
  * value). d_mask (nullable) receives the printed mask sdf >= 0 as 1/0 floats. */
 int litho_reinit_sdf(litho_ctx* ctx, int rows, int cols, const float* d_phi, double dx,
                      double dy, float* d_sdf, float* d_mask);
+/* Vector kernels of the CTM L-BFGS driver (CTM_Optimizer.cpp:189-227, LBFGS++'s
+ * two-loop recursion evaluated on FP64 Gram matrices of the stored pairs).
+ * litho_lbfgs_dots: out[j] = sum_i rows[j][i] v[i] accumulated in FP64 for the k
+ * (1..64) float32 device rows of length n, row j at d_rows + j * ld; out is k host
+ * doubles (the call waits for them). litho_lbfgs_combine: d_out[i] = cv v[i] +
+ * sum_j coef[j] rows[j][i], in FP64 per element, stored float32 (coef: k host doubles,
+ * k may be 0; d_out must not alias d_v). */
+int litho_lbfgs_dots(litho_ctx* ctx, int k, long long n, const float* d_rows, long long ld,
+                     const float* d_v, double* out);
+int litho_lbfgs_combine(litho_ctx* ctx, int k, long long n, const float* d_rows, long long ld,
+                        const double* coef, const float* d_v, double cv, float* d_out);
 /* litho_reinit_sdf for `batch` images ([batch][rows][cols]) in one launch, inside =
  * phi > level: level 0.5 on a binary mask gives reinit_sdf(mask - 0.5), the LSM
  * initialisation (LSM_Optimizer.cpp:62), without the shifted copy. d_sdf and d_mask
