@@ -294,7 +294,7 @@ def serving_run(L, K, requests, seed=7):
 
 
 def ctm_full_run(L, torch, stream, N, band, r0, c0, w, wss, target, iterations=50,
-                 lsm_steps=20):
+                 lsm_steps=20, graphs=True):
     """The CTM full run on one N x N tile: CTM_Optimizer with L-BFGS (history 10,
     `iterations` iterations) from the reference's theta initialisation, then
     LSM_Optimizer for `lsm_steps` WENO5-Godunov updates (CFL 0.5) from the CTM mask
@@ -309,6 +309,7 @@ def ctm_full_run(L, torch, stream, N, band, r0, c0, w, wss, target, iterations=5
     for mode in ("bf16x3", "fp32"):
         ctx = L.Context(torch.cuda.current_device(), stream=stream)
         ctx.set_precision(mode)
+        ctx.enable_graphs(graphs)
         cache = L.ImagingCache.from_band(N, band, r0, c0, w, wss, ctx=ctx)
         with torch.cuda.stream(stream):
             warm = L.CTMOptimizer(cache, tgt, THRESHOLD, ALPHA, iterations=2,
@@ -660,7 +661,8 @@ def run_ours(args):
             pm["batched_over_fp32"] = pm[head]["value"] / pm["fp32"]["value"]
     if world == 1:
         out["roofline_levelset"] = levelset_run(L, torch, stream)
-        out["ctm_full_run"] = ctm_full_run(L, torch, stream, N, band, r0, c0, w, wss, target)
+        out["ctm_full_run"] = ctm_full_run(L, torch, stream, N, band, r0, c0, w, wss, target,
+                                           graphs=not args.no_graphs)
     if world == 1 and args.serving_requests > 0:
         out["serving"] = serving_run(L, K, args.serving_requests)
     if world == 1 and args.fullchip_size > 0:
