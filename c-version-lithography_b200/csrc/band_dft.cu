@@ -855,8 +855,10 @@ band_z_kernel(const float2* __restrict__ e, const float* __restrict__ gam, int N
   }
 }
 
-// Adjoint 3: X[u] = scale sum_k w_k conj(H_k(u)) Z_k(u), k in order, one thread per
-// u; the loads of 8 consecutive k are issued together.
+// Adjoint 3: X[u] = scale sum_k w_k conj(H_k(u)) Z_k(u). Four lanes per u: lane j
+// sums k = j, j + 4, ... in order (the loads of up to 8 of its k issued together),
+// then the four partial sums are added in a fixed order.
+constexpr int BX_SPLIT = 4;
 __global__ void band_x_kernel(const float2* __restrict__ Zk, const float2* __restrict__ H,
                               const float* __restrict__ w, int K, int nb, float scale,
                               float2* __restrict__ X) {
@@ -864,26 +866,38 @@ __global__ void band_x_kernel(const float2* __restrict__ Zk, const float2* __res
   pdl_wait();
   Zk += (size_t)blockIdx.y * K * nb;   // image b of a batch
   X += (size_t)blockIdx.y * nb;
-  const int u = blockIdx.x * blockDim.x + threadIdx.x;
-  if (u >= nb) return;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int u = t / BX_SPLIT, j = t % BX_SPLIT;
   float2 acc = make_float2(0.f, 0.f);
-  for (int k0 = 0; k0 < K; k0 += 8) {
-    float2 hv[8], zv[8];
+  if (u < nb) {
+    for (int k0 = j; k0 < K; k0 += 8 * BX_SPLIT) {
+      float2 hv[8], zv[8];
 #pragma unroll
-    for (int q = 0; q < 8; ++q)
-      if (k0 + q < K) {
-        hv[q] = H[(size_t)(k0 + q) * nb + u];
-        zv[q] = Zk[(size_t)(k0 + q) * nb + u];
+      for (int q = 0; q < 8; ++q) {
+        const int k = k0 + q * BX_SPLIT;
+        if (k < K) {
+          hv[q] = H[(size_t)k * nb + u];
+          zv[q] = Zk[(size_t)k * nb + u];
+        }
       }
 #pragma unroll
-    for (int q = 0; q < 8; ++q)
-      if (k0 + q < K) {
-        const float2 t = cmul(conjf2(hv[q]), zv[q]);
-        acc.x = fmaf(w[k0 + q], t.x, acc.x);
-        acc.y = fmaf(w[k0 + q], t.y, acc.y);
+      for (int q = 0; q < 8; ++q) {
+        const int k = k0 + q * BX_SPLIT;
+        if (k < K) {
+          const float2 c = cmul(conjf2(hv[q]), zv[q]);
+          acc.x = fmaf(w[k], c.x, acc.x);
+          acc.y = fmaf(w[k], c.y, acc.y);
+        }
       }
+    }
   }
-  X[u] = make_float2(acc.x * scale, acc.y * scale);
+  // lanes 4u .. 4u + 3 are adjacent in one warp: (0 + 1) + (2 + 3)
+#pragma unroll
+  for (int o = 1; o < BX_SPLIT; o <<= 1) {
+    acc.x += __shfl_xor_sync(0xffffffffu, acc.x, o);
+    acc.y += __shfl_xor_sync(0xffffffffu, acc.y, o);
+  }
+  if (u < nb && j == 0) X[u] = make_float2(acc.x * scale, acc.y * scale);
 }
 
 cudaError_t launch_band_adjoint(cudaStream_t s, const Cache& c, const Field& f, const float2* gh,
@@ -914,7 +928,7 @@ cudaError_t launch_band_adjoint(cudaStream_t s, const Cache& c, const Field& f, 
                                : zk(std::integral_constant<int, BW_ONE>{});
   if (err != cudaSuccess) return err;
   const int nb = g.Nr * g.Nc;
-  err = launch_pdl(band_x_kernel, dim3((nb + 127) / 128, batch), dim3(128), 0, s,
+  err = launch_pdl(band_x_kernel, dim3((nb * BX_SPLIT + 127) / 128, batch), dim3(128), 0, s,
                    static_cast<const float2*>(Zk), c.H, c.w, g.K, nb, (float)scale, X);
   if (err != cudaSuccess) return err;
   return launch_expand(s, X, g.Nr, g.Nc, g.Nc, c.TXSc, g.N, 0, g.Nc, g.kp_rows, Vt, img, batch);
