@@ -516,6 +516,18 @@ __global__ void sum_k_kernel(const float* __restrict__ ik, int K, int n, float* 
   iP[j] = s;
 }
 
+// Sum of a value over SPLIT adjacent lanes (a power of two dividing 32), added in a
+// fixed order ((0 + 1) + (2 + 3) for 4); every lane of the warp must call it.
+template <int SPLIT>
+__device__ __forceinline__ float2 split_sum(float2 a) {
+#pragma unroll
+  for (int o = 1; o < SPLIT; o <<= 1) {
+    a.x += __shfl_xor_sync(0xffffffffu, a.x, o);
+    a.y += __shfl_xor_sync(0xffffffffu, a.y, o);
+  }
+  return a;
+}
+
 // Forward 3 (one CTA per band row dr >= 0): chat[dr][dc] = DFT_P(i)(dr, dc) / (Pr Pc)
 // for dc in [-(Nc-1), Nc-1].
 constexpr int BI_NT = 256;
@@ -540,30 +552,29 @@ band_chat_kernel(const float* __restrict__ iP, int Nr, int Nc, int Pr, int Pc,
   pdl_wait();
   fill_batched<BI_NT>(ip, Pr * Pc, [&](int i) { return iP[i]; });
   __syncthreads();
-  for (int jc = threadIdx.x; jc < Pc; jc += BI_NT) {
-    float2 a = make_float2(0.f, 0.f), b = a;
-    int jr = 0;
-    for (; jr + 1 < Pr; jr += 2) {
-      const float i0 = ip[jr * Pc + jc], i1 = ip[(jr + 1) * Pc + jc];
-      a.x = fmaf(ed[jr].x, i0, a.x); a.y = fmaf(-ed[jr].y, i0, a.y);
-      b.x = fmaf(ed[jr + 1].x, i1, b.x); b.y = fmaf(-ed[jr + 1].y, i1, b.y);
-    }
-    if (jr < Pr) {
-      const float i0 = ip[jr * Pc + jc];
-      a.x = fmaf(ed[jr].x, i0, a.x); a.y = fmaf(-ed[jr].y, i0, a.y);
-    }
-    v[jc] = make_float2(a.x + b.x, a.y + b.y);
+  // Each output is summed by SPLIT adjacent lanes (terms sub, sub + SPLIT, ...), their
+  // partial sums then added in a fixed order; whole warps iterate together.
+  constexpr int SPLIT = 4, GROUPS = BI_NT / SPLIT;
+  const int sub = threadIdx.x % SPLIT, grp = threadIdx.x / SPLIT;
+  for (int base = 0; base < Pc; base += GROUPS) {
+    const int jc = base + grp;
+    float2 a = make_float2(0.f, 0.f);
+    if (jc < Pc)
+      for (int jr = sub; jr < Pr; jr += SPLIT) {
+        const float i0 = ip[jr * Pc + jc];
+        a.x = fmaf(ed[jr].x, i0, a.x); a.y = fmaf(-ed[jr].y, i0, a.y);
+      }
+    a = split_sum<SPLIT>(a);
+    if (jc < Pc && sub == 0) v[jc] = a;
   }
   __syncthreads();
-  for (int dc = threadIdx.x; dc < nd; dc += BI_NT) {
-    float2 a = make_float2(0.f, 0.f), b = a;
-    int jc = 0;
-    for (; jc + 1 < Pc; jc += 2) {
-      cfma(a, v[jc], conjf2(edc[jc * nd + dc]));
-      cfma(b, v[jc + 1], conjf2(edc[(jc + 1) * nd + dc]));
-    }
-    if (jc < Pc) cfma(a, v[jc], conjf2(edc[jc * nd + dc]));
-    chat[(size_t)dr * nd + dc] = make_float2((a.x + b.x) * inv, (a.y + b.y) * inv);
+  for (int base = 0; base < nd; base += GROUPS) {
+    const int dc = base + grp;
+    float2 a = make_float2(0.f, 0.f);
+    if (dc < nd)
+      for (int jc = sub; jc < Pc; jc += SPLIT) cfma(a, v[jc], conjf2(edc[jc * nd + dc]));
+    a = split_sum<SPLIT>(a);
+    if (dc < nd && sub == 0) chat[(size_t)dr * nd + dc] = make_float2(a.x * inv, a.y * inv);
   }
 }
 
@@ -744,20 +755,29 @@ band_gamma_kernel(const float2* __restrict__ gh, int Nr, int Nc, int Pr, int Pc,
   pdl_wait();
   fill_batched<256>(ghs, na * Nc, [&](int i) { return gh[i]; });
   __syncthreads();
-  for (int c = threadIdx.x; c < Nc; c += blockDim.x) {
+  // SPLIT adjacent lanes per output, as in band_chat_kernel.
+  constexpr int SPLIT = 4, GROUPS = 256 / SPLIT;
+  const int sub = threadIdx.x % SPLIT, grp = threadIdx.x / SPLIT;
+  for (int base = 0; base < Nc; base += GROUPS) {
+    const int c = base + grp;
     float2 a = make_float2(0.f, 0.f);
-    for (int r = 0; r < na; ++r) cfma(a, edr[r], ghs[r * Nc + c]);
+    if (c < Nc)
+      for (int r = sub; r < na; r += SPLIT) cfma(a, edr[r], ghs[r * Nc + c]);
+    a = split_sum<SPLIT>(a);
     const float kc = c > 0 ? 2.f : 1.f;
-    wv[c] = make_float2(kc * a.x, kc * a.y);
+    if (c < Nc && sub == 0) wv[c] = make_float2(kc * a.x, kc * a.y);
   }
   __syncthreads();
-  for (int jc = threadIdx.x; jc < Pc; jc += blockDim.x) {
+  for (int base = 0; base < Pc; base += GROUPS) {
+    const int jc = base + grp;
     float acc = 0.f;
-    for (int c = 0; c < Nc; ++c) {
-      const float2 t = edc[c * Pc + jc];
-      acc = fmaf(wv[c].x, t.x, fmaf(-wv[c].y, t.y, acc));
-    }
-    gam[(size_t)jr * Pc + jc] = acc;
+    if (jc < Pc)
+      for (int c = sub; c < Nc; c += SPLIT) {
+        const float2 t = edc[c * Pc + jc];
+        acc = fmaf(wv[c].x, t.x, fmaf(-wv[c].y, t.y, acc));
+      }
+    acc = split_sum<SPLIT>(make_float2(acc, 0.f)).x;
+    if (jc < Pc && sub == 0) gam[(size_t)jr * Pc + jc] = acc;
   }
 }
 
