@@ -262,7 +262,9 @@ def serving_run(L, K, requests, seed=7):
     requests/s) of LSM tile solves of 20 iterations, tile sizes 256^2 / 512^2 / 1024^2 /
     2048^2 in proportions 4:3:2:1, through the continuous-batching TileServer in
     split-BF16 (16 solves per size batched, 120 GB HBM budget), and the same stream
-    through the plain FP32 one-tile-at-a-time loop (max_batch 1)."""
+    through the plain FP32 one-tile-at-a-time loop (max_batch 1). Each server first
+    serves the stream once unmeasured (start-up: kernels loaded, memory sized), then
+    the measured pass runs on a fresh server of the same context."""
     S = importlib.import_module("c-version-lithography_b200.serving")
     wl = importlib.import_module("c-version-lithography_b200.workloads")
     band, r0, c0, w, wss = wl.synthetic_socs_band(K=K)
@@ -280,11 +282,9 @@ def serving_run(L, K, requests, seed=7):
         ctx = L.Context()
         ctx.set_precision(mode)
         caches = {N: L.ImagingCache.from_band(N, band, r0, c0, w, wss, ctx=ctx) for N in sizes}
-        warm = S.TileServer(caches, THRESHOLD, ALPHA, max_batch=max_batch)
-        for N in sizes:
-            t = wl.manhattan_target(N, 4, seed=N)
-            warm.submit(t, t, 2)
-        warm.drain()
+        # Server start-up: one unmeasured pass of the same stream loads every kernel
+        # the mix uses and sizes the working memory; the measured pass follows.
+        S.TileServer(caches, THRESHOLD, ALPHA, max_batch=max_batch, hbm_budget=120e9).serve(arrivals)
         srv = S.TileServer(caches, THRESHOLD, ALPHA, max_batch=max_batch, hbm_budget=120e9)
         key = ("bf16x3_continuous_batching" if mode == "bf16x3" else "fp32_one_tile_at_a_time")
         out[key] = srv.serve(arrivals)
@@ -417,6 +417,11 @@ def fullchip_run(L, K, size, grid, halo, guard, ctm_steps=3, lsm_steps=20, seed=
         ctx.set_precision(mode)
         part = FC.Partition(size, size, grid, grid, halo, guard, ctx=ctx)
         cache = L.ImagingCache.from_band(part.tile_size, band, r0, c0, w, wss, ctx=ctx)
+        # schedules of this layout: small-grid stage of the exchange's tile groups,
+        # chamfer re-initialisation of all tiles at once
+        out.setdefault("autotune", {})[mode] = ctx.autotune(
+            cache, batch=min(16, part.num_tiles), shape=(part.tile_size, part.tile_size),
+            nimg=part.num_tiles)
         ctm = FC.FullChipCTMOptimizer(part, cache, THRESHOLD, ALPHA)
         ctm.optimize(layout, FC.FullChipCTMOptions(iterations=1, gradient_options=gopt))  # warm-up
         res, sec = timed(lambda: ctm.optimize(
@@ -545,9 +550,10 @@ def run_ours(args):
         torch.cuda.synchronize()
         ctx = runs["bf16x3"]["ctx"]
         cache = runs["bf16x3"]["cache"]
+        tuned = ctx.autotune(cache, batch=B)    # schedule of the batched small-grid stage
         r = _measure(L, torch, ctx, stream, cache, target, th, flush, args.steps, args.warmup, dist,
                      batch=(ths, tgs, grs))
-        r.update(ctx=ctx, cache=cache, tiles=B)
+        r.update(ctx=ctx, cache=cache, tiles=B, autotune=tuned)
         runs[f"bf16x3_batch{B}"] = r
     clk.__exit__(None, None, None)
     head = list(runs)[-1]     # the batched tensor-core path when it ran
@@ -659,6 +665,8 @@ def run_ours(args):
         pm["bf16x3_over_fp32"] = pm["bf16x3"]["value"] / pm["fp32"]["value"]
         if head not in ("fp32", "bf16x3"):
             pm["batched_over_fp32"] = pm[head]["value"] / pm["fp32"]["value"]
+    if "autotune" in R:
+        out["config"]["autotune"] = R["autotune"]
     if world == 1:
         out["roofline_levelset"] = levelset_run(L, torch, stream)
         out["ctm_full_run"] = ctm_full_run(L, torch, stream, N, band, r0, c0, w, wss, target,

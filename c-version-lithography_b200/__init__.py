@@ -114,6 +114,8 @@ SIGNATURES = {
     "litho_lsm_rk2_update": (_I, [_P, _I, _I, _P, _P, _D, _D, _D, _D, _P, _P, _PD]),
     "litho_reinit_sdf": (_I, [_P, _I, _I, _P, _D, _D, _P, _P]),
     "litho_reinit_sdf_batch": (_I, [_P, _I, _I, _I, _P, _D, _D, _D, _P, _P]),
+    "litho_ctx_autotune": (_I, [_P, _P, _I, _I, _I, _I, _PI, _PI]),
+    "litho_ctx_reserve": (_I, [_P, _P, _I]),
     "litho_lbfgs_dots": (_I, [_P, _I, ctypes.c_longlong, _P, ctypes.c_longlong, _P, _PD]),
     "litho_lbfgs_combine": (_I, [_P, _I, ctypes.c_longlong, _P, ctypes.c_longlong, _PD, _P, _D,
                                  _P]),
@@ -249,6 +251,23 @@ class Context:
         cnt = (ctypes.c_longlong * 9)()
         self._check(self.lib.litho_ctx_stage_times(self.handle, ms, cnt))
         return {name: (ms[i], cnt[i]) for i, name in enumerate(self.STAGES)}
+
+    def reserve(self, cache, batch: int):
+        """Grow the device scratch to what batched calls on `batch` images of `cache`
+        need (litho_ctx_reserve), so that later calls do not allocate."""
+        self._check(self.lib.litho_ctx_reserve(self.handle, cache.handle, int(batch)))
+
+    def autotune(self, cache=None, batch: int = 1, shape=None, nimg: int = 0):
+        """Time the candidate schedules on this GPU and keep the fastest for the calls
+        that follow (litho_ctx_autotune): with `cache`, the small-grid chunk width for
+        `batch` images of it; with `shape` (rows, cols) and nimg > 0, the chamfer CTA
+        size of reinit_sdf for nimg such images. Returns the choices."""
+        bw, ct = ctypes.c_int(), ctypes.c_int()
+        rows, cols = shape if shape is not None else (0, 0)
+        self._check(self.lib.litho_ctx_autotune(self.handle, cache.handle if cache else None,
+                                                int(batch), int(rows), int(cols), int(nimg),
+                                                ctypes.byref(bw), ctypes.byref(ct)))
+        return {"band_chunk_width": bw.value, "chamfer_threads": ct.value}
 
     def close(self):
         if getattr(self, "handle", None):

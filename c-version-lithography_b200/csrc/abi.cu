@@ -605,7 +605,8 @@ int run_forward(Context* ctx, const Cache& c, Field& f, const Layout& L, int inp
   ctx->stage_begin(2);
   st = check_launch(ctx, launch_band_forward(s, c, f, at<float>(ctx, L.ik), at<float>(ctx, L.iP),
                                              at<float2>(ctx, L.chat), at<float>(ctx, L.Ut),
-                                             tc ? at<void>(ctx, L.img) : nullptr, batch),
+                                             tc ? at<void>(ctx, L.img) : nullptr, batch,
+                                             ctx->band_width(g.N, batch)),
                     "band forward");
   ctx->stage_end(2);
   if (st) return st;
@@ -668,7 +669,8 @@ int run_adjoint(Context* ctx, const Cache& c, const Field& f, const Layout& L, c
   st = check_launch(ctx, launch_band_adjoint(s, c, f, at<float2>(ctx, L.gh), scale,
                                              at<float>(ctx, L.gam), at<float2>(ctx, L.Zk),
                                              at<float2>(ctx, L.X), at<float>(ctx, L.Vt),
-                                             tc ? at<void>(ctx, L.img) : nullptr, batch),
+                                             tc ? at<void>(ctx, L.img) : nullptr, batch,
+                                             ctx->band_width(g.N, batch)),
                     "band adjoint");
   ctx->stage_end(6);
   if (st) return st;
@@ -1414,7 +1416,8 @@ int litho_reinit_sdf(litho_ctx* ctx, int rows, int cols, const float* d_phi, dou
     return ctx->fail(LITHO_ERR_UNSUPPORTED, "reinit_sdf supports at most 17066 columns");
   if (d_sdf == d_phi) return ctx->fail(LITHO_ERR_INVALID_ARGUMENT, "reinit_sdf: sdf must not alias phi");
   ctx->stage_begin(8);
-  st = check_launch(ctx, launch_reinit_sdf(ctx->stream, rows, cols, d_phi, 0.f, 0, (float)dx, d_sdf),
+  st = check_launch(ctx, launch_reinit_sdf(ctx->stream, rows, cols, d_phi, 0.f, 0, (float)dx, d_sdf,
+                                           1, ctx->chamfer_threads(cols, 1)),
                     "reinit_sdf");
   if (!st && d_mask)
     st = check_launch(ctx, launch_levelset(ctx->stream, 5, rows, cols, d_sdf, nullptr, nullptr,
@@ -1424,6 +1427,114 @@ int litho_reinit_sdf(litho_ctx* ctx, int rows, int cols, const float* d_phi, dou
   ctx->launches += d_mask ? 2 : 1;
   if (!st) LITHO_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
   if (!st) ctx->collect_stages();
+  return st;
+}
+
+int litho_ctx_reserve(litho_ctx* ctx, const litho_cache* cache, int batch) {
+  if (!ctx || !cache || batch < 1) return LITHO_ERR_INVALID_ARGUMENT;
+  Layout L;
+  int st = prepare(ctx, *cache, &L, batch, true);
+  if (st) return st;
+  // The batched RK2 update of `batch` images of this size (its stage-1 images).
+  const size_t n = (size_t)cache->g.N * cache->g.N;
+  st = ctx->ensure_scratch(std::max(L.total, n * batch * sizeof(float)));
+  if (st) return st;
+  st = ctx->ensure_red(RED_PART + ((size_t)batch * dt_batch_blocks(n, batch) + 1) / 2 + 8 +
+                       (size_t)batch + 8);
+  if (st) return st;
+  LITHO_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  return LITHO_OK;
+}
+
+int litho_ctx_autotune(litho_ctx* ctx, const litho_cache* cache, int batch, int rows, int cols,
+                       int nimg, int* band_width, int* chamfer_threads) {
+  if (!ctx || (cache && batch < 1) || (nimg > 0 && (rows < 3 || cols < 3)))
+    return LITHO_ERR_INVALID_ARGUMENT;
+  if (band_width) *band_width = 0;
+  if (chamfer_threads) *chamfer_threads = 0;
+  if (cudaSetDevice(ctx->device) != cudaSuccess) return ctx->fail(LITHO_ERR_CUDA, "cudaSetDevice");
+  cudaStream_t s = ctx->stream;
+  cudaEvent_t e0, e1;
+  if (cudaEventCreate(&e0) != cudaSuccess) return ctx->fail(LITHO_ERR_CUDA, "cudaEventCreate");
+  if (cudaEventCreate(&e1) != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return ctx->fail(LITHO_ERR_CUDA, "cudaEventCreate");
+  }
+  // Mean time of three runs after one warm-up run, on the context's stream.
+  auto timed = [&](auto&& run, float* ms) -> int {
+    cudaError_t e = run();
+    if (e == cudaSuccess) e = cudaEventRecord(e0, s);
+    for (int r = 0; r < 3 && e == cudaSuccess; ++r) e = run();
+    if (e == cudaSuccess) e = cudaEventRecord(e1, s);
+    if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+    if (e == cudaSuccess) e = cudaEventElapsedTime(ms, e0, e1);
+    return check_launch(ctx, e, "autotune timing");
+  };
+  int st = LITHO_OK;
+  if (cache) {
+    // Chunk width of the small-grid field and Z kernels (the results do not depend on
+    // it): the forward and adjoint band stages of `batch` images, on zeroed inputs.
+    Layout L;
+    st = prepare(ctx, *cache, &L, batch, true);
+    if (!st) LITHO_CUDA_TRY(ctx, cudaMemsetAsync(ctx->scratch.base, 0, L.total, s));
+    const bool tc = ctx->precision == LITHO_PRECISION_BF16X3 && cache->TXS_img;
+    Field f;
+    f.cache = cache;
+    f.e = at<float2>(ctx, L.fe);
+    f.mband = at<float2>(ctx, L.fm);
+    float best = 0.f;
+    int bw = 0;
+    for (const int w : {8, 16}) {
+      if (st) break;
+      float ms = 0.f;
+      st = timed([&]() -> cudaError_t {
+        cudaError_t e = launch_band_forward(s, *cache, f, at<float>(ctx, L.ik), at<float>(ctx, L.iP),
+                                            at<float2>(ctx, L.chat), at<float>(ctx, L.Ut),
+                                            tc ? at<void>(ctx, L.img) : nullptr, batch, w);
+        if (e != cudaSuccess) return e;
+        return launch_band_adjoint(s, *cache, f, at<float2>(ctx, L.gh), 1.0, at<float>(ctx, L.gam),
+                                   at<float2>(ctx, L.Zk), at<float2>(ctx, L.X),
+                                   at<float>(ctx, L.Vt), tc ? at<void>(ctx, L.img) : nullptr,
+                                   batch, w);
+      }, &ms);
+      if (!st && (bw == 0 || ms < best)) { best = ms; bw = w; }
+    }
+    if (!st) {
+      ctx->tuned_band[{cache->g.N, batch}] = bw;
+      if (band_width) *band_width = bw;
+    }
+  }
+  if (!st && nimg > 0) {
+    // Chamfer CTA size for nimg images of rows x cols (timed on at most 512 MB of them).
+    if ((size_t)3 * (cols + 4) * sizeof(float) > 200 * 1024) {
+      st = ctx->fail(LITHO_ERR_UNSUPPORTED, "reinit_sdf supports at most 17066 columns");
+    } else {
+      const size_t px = (size_t)rows * cols;
+      const int nt = (int)std::max<size_t>(1, std::min<size_t>(nimg, ((size_t)512 << 20) / (8 * px)));
+      st = ctx->ensure_scratch(2 * px * nt * sizeof(float));
+      float* phi = static_cast<float*>(ctx->scratch.base);
+      float* out = phi + px * nt;
+      if (!st) st = check_launch(ctx, launch_chamfer_probe(s, phi, rows, cols, nt), "autotune pattern");
+      float best = 0.f;
+      int bt = 0;
+      for (const int t : {128, 256, 512, 1024}) {
+        if (st) break;
+        const int per = (cols + t - 1) / t;
+        if ((t <= 256 && per > 32) || (t == 512 && per > 16)) continue;
+        float ms = 0.f;
+        st = timed([&]() {
+          return launch_reinit_sdf(s, rows, cols, phi, 0.f, 0, 1.f, out, nt, t);
+        }, &ms);
+        if (!st && (bt == 0 || ms < best)) { best = ms; bt = t; }
+      }
+      if (!st) {
+        ctx->tuned_chamfer[{cols, nimg}] = bt;
+        if (chamfer_threads) *chamfer_threads = bt;
+      }
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
   return st;
 }
 
@@ -1483,7 +1594,8 @@ int litho_reinit_sdf_batch(litho_ctx* ctx, int batch, int rows, int cols, const 
   for (int b0 = 0; b0 < batch && !st; b0 += 65535) {
     const int B = std::min(batch - b0, 65535);
     st = check_launch(ctx, launch_reinit_sdf(ctx->stream, rows, cols, d_phi + b0 * n, (float)level,
-                                             0, (float)dx, d_sdf + b0 * n, B),
+                                             0, (float)dx, d_sdf + b0 * n, B,
+                                             ctx->chamfer_threads(cols, B)),
                       "reinit_sdf");
     if (!st && d_mask)
       st = check_launch(ctx, launch_levelset(ctx->stream, 5, rows, cols, d_sdf + b0 * n, nullptr,
@@ -2224,7 +2336,9 @@ int litho_fullchip_lsm_init(litho_ctx* ctx, const litho_partition* p, const floa
   for (int t0 = 0; t0 < p->ntiles && !st; t0 += 65535)
     st = check_launch(ctx, launch_reinit_sdf(s, p->ts, p->ts, d_masks + (size_t)t0 * p->ts * p->ts,
                                              0.5f, 0, (float)dx, d_phi + (size_t)t0 * p->ts * p->ts,
-                                             std::min(p->ntiles - t0, 65535)),
+                                             std::min(p->ntiles - t0, 65535),
+                                             ctx->chamfer_threads(p->ts,
+                                                                  std::min(p->ntiles - t0, 65535))),
                       "reinit_sdf");
   if (!st)
     st = check_launch(ctx, launch_render_mask(s, d_phi, p->ts, p->ts, p->ntiles,
@@ -2300,7 +2414,7 @@ int litho_fullchip_lsm_step(litho_ctx* ctx, const litho_partition* p, const floa
   for (int t0 = 0; reinit && t0 < n && !st; t0 += 65535) {
     const int B = std::min(n - t0, 65535);
     st = check_launch(ctx, launch_reinit_sdf(s, ts, ts, d_phi_out + t0 * tt, 0.f, 1, (float)dx,
-                                             d_masks + t0 * tt, B),
+                                             d_masks + t0 * tt, B, ctx->chamfer_threads(ts, B)),
                       "reinit_sdf");
     if (!st)
       st = check_launch(ctx, launch_levelset(s, 8, ts, ts, d_masks + t0 * tt, d_phi_out + t0 * tt,

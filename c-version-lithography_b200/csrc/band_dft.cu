@@ -701,7 +701,7 @@ static cudaError_t launch_expand(cudaStream_t s, const float2* coef, int nrows, 
 }
 
 cudaError_t launch_band_forward(cudaStream_t s, const Cache& c, Field& f, float* ik, float* iP,
-                                float2* chat, float* Ut, void* img, int batch) {
+                                float2* chat, float* Ut, void* img, int batch, int width) {
   const BandGeom& g = c.g;
   auto fields = [&](auto wtag) -> cudaError_t {
     constexpr int W = decltype(wtag)::value;
@@ -714,8 +714,10 @@ cudaError_t launch_band_forward(cudaStream_t s, const Cache& c, Field& f, float*
                       sm1, s, c.H, static_cast<const float2*>(f.mband), c.w, g.Nr, g.Nc, g.Pr,
                       g.Pc, c.ESc_t, c.ESr_t, (int)staged, f.e, ik);
   };
-  cudaError_t err = batch >= 4 ? fields(std::integral_constant<int, BW_BATCH>{})
-                               : fields(std::integral_constant<int, BW_ONE>{});
+  // Chunk width: the autotuned one when set, else wide chunks for batches.
+  const bool wide = width > 0 ? width >= BW_BATCH : batch >= 4;
+  cudaError_t err = wide ? fields(std::integral_constant<int, BW_BATCH>{})
+                         : fields(std::integral_constant<int, BW_ONE>{});
   if (err != cudaSuccess) return err;
   const int n = g.Pr * g.Pc;
   err = launch_pdl(sum_k_kernel, dim3((n + 255) / 256, batch), dim3(256), 0, s,
@@ -922,7 +924,7 @@ __global__ void band_x_kernel(const float2* __restrict__ Zk, const float2* __res
 
 cudaError_t launch_band_adjoint(cudaStream_t s, const Cache& c, const Field& f, const float2* gh,
                                 double scale, float* gam, float2* Zk, float2* X, float* Vt,
-                                void* img, int batch) {
+                                void* img, int batch, int width) {
   const BandGeom& g = c.g;
   const size_t smg = gamma_smem(g);
   cudaError_t e0 = cudaFuncSetAttribute(band_gamma_kernel,
@@ -944,8 +946,9 @@ cudaError_t launch_band_adjoint(cudaStream_t s, const Cache& c, const Field& f, 
                       static_cast<const float2*>(f.e), static_cast<const float*>(gam), g.Nr, g.Nc,
                       g.Pr, g.Pc, c.ESc, c.ESr_t, stage, 1.f / ((float)g.Pr * (float)g.Pc), Zk);
   };
-  cudaError_t err = batch >= 4 ? zk(std::integral_constant<int, BW_BATCH>{})
-                               : zk(std::integral_constant<int, BW_ONE>{});
+  const bool wide = width > 0 ? width >= BW_BATCH : batch >= 4;
+  cudaError_t err = wide ? zk(std::integral_constant<int, BW_BATCH>{})
+                         : zk(std::integral_constant<int, BW_ONE>{});
   if (err != cudaSuccess) return err;
   const int nb = g.Nr * g.Nc;
   err = launch_pdl(band_x_kernel, dim3((nb * BX_SPLIT + 127) / 128, batch), dim3(128), 0, s,

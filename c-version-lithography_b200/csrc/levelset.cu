@@ -657,6 +657,22 @@ chamfer_sdf_kernel(const float* __restrict__ phi_all, int rows, int cols, float 
   }
 }
 
+// A smooth test pattern (sin x cos y with a per-image phase) whose zero set crosses
+// every row: the input of the chamfer timing of litho_ctx_autotune.
+__global__ void chamfer_probe_kernel(float* __restrict__ p, int rows, int cols, int nimg) {
+  const size_t n = (size_t)rows * cols * nimg;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const int x = (int)(i % cols), y = (int)((i / cols) % rows), k = (int)(i / ((size_t)rows * cols));
+    p[i] = sinf(0.031f * x + k) * cosf(0.027f * y) - 0.1f;
+  }
+}
+
+cudaError_t launch_chamfer_probe(cudaStream_t s, float* p, int rows, int cols, int nimg) {
+  chamfer_probe_kernel<<<1184, 256, 0, s>>>(p, rows, cols, nimg);
+  return cudaGetLastError();
+}
+
 template <int NT, int PMAX>
 static cudaError_t chamfer_launch(cudaStream_t s, int rows, int cols, const float* phi,
                                   float level, int inclusive, float dx, float* sdf, int nimg) {

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 #include <cstddef>
 #include <cstdint>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -153,6 +154,17 @@ struct Context {
   }
   int ensure_scratch(size_t bytes);
   int ensure_red(size_t n);
+  // Schedules chosen by litho_ctx_autotune: the small-grid chunk width per (N, batch)
+  // and the chamfer CTA size per (columns, images); 0 where nothing was tuned.
+  std::map<std::pair<int, int>, int> tuned_band, tuned_chamfer;
+  int band_width(int N, int batch) const {
+    const auto it = tuned_band.find({N, batch});
+    return it == tuned_band.end() ? 0 : it->second;
+  }
+  int chamfer_threads(int cols, int nimg) const {
+    const auto it = tuned_chamfer.find({cols, nimg});
+    return it == tuned_chamfer.end() ? 0 : it->second;
+  }
 };
 
 // ---------------------------------------------------------------- launch helper
@@ -194,13 +206,16 @@ cudaError_t launch_reduce_tiles(cudaStream_t s, const float2* part, int tiles, i
 // Shared memory of its per-kernel CTA: band_fields_smem.
 size_t band_fields_smem(const BandGeom& g);
 size_t band_max_smem(const BandGeom& g);
+// width: the chunk width of the small-grid field and Z kernels (8 or 16 columns;
+// 0: 16 for batches of 4 or more images, else 8). The results do not depend on it.
 cudaError_t launch_band_forward(cudaStream_t s, const Cache& c, Field& f, float* ik, float* iP,
-                                float2* chat, float* Ut, void* img, int batch = 1);
+                                float2* chat, float* Ut, void* img, int batch = 1,
+                                int width = 0);
 // Small-grid stage of the adjoint: gh (the D-band DFT of dL/dI) -> gam, Zk, X and Vt
 // (or Vt's operand image, as for the forward).
 cudaError_t launch_band_adjoint(cudaStream_t s, const Cache& c, const Field& f, const float2* gh,
                                 double scale, float* gam, float2* Zk, float2* X, float* Vt,
-                                void* img, int batch = 1);
+                                void* img, int batch = 1, int width = 0);
 
 // Row synthesis: out[y][x] = sum_f AY[y][f] * Bt[x][f] with a fused epilogue.
 struct ResistEpilogue {
@@ -302,6 +317,8 @@ cudaError_t launch_dt(cudaStream_t s, const float* vn, size_t n, float dx, float
 // by the row length).
 cudaError_t launch_reinit_sdf(cudaStream_t s, int rows, int cols, const float* phi, float level,
                               int inclusive, float dx, float* sdf, int nimg = 1, int threads = 0);
+// Fills nimg rows x cols images with a pattern whose zero set crosses every row.
+cudaError_t launch_chamfer_probe(cudaStream_t s, float* p, int rows, int cols, int nimg);
 // max |Vn| and dt of nimg images of n pixels: vd[2 i] = max |Vn_i|, vd[2 i + 1] = dt_i;
 // part holds nimg * dt_batch_blocks(n, nimg) floats.
 int dt_batch_blocks(size_t n, int nimg);

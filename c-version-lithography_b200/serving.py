@@ -104,6 +104,10 @@ class TileServer:
         self._next_id = 0
         self.steps = 0
         self.tile_iterations = 0
+        # The working memory of a full batch of every size, allocated now: the steps
+        # that follow never allocate device memory.
+        for cache in self.caches.values():
+            self.ctx.reserve(cache, self.max_batch)
 
     @staticmethod
     def solve_bytes(N: int) -> float:

@@ -251,6 +251,20 @@ int litho_evolution_term(litho_ctx* ctx, int rows, int cols, const float* d_phi,
  * value). d_mask (nullable) receives the printed mask sdf >= 0 as 1/0 floats. */
 int litho_reinit_sdf(litho_ctx* ctx, int rows, int cols, const float* d_phi, double dx,
                      double dy, float* d_sdf, float* d_mask);
+/* Grows the context's device scratch to what the batched calls on `batch` images of
+ * this cache need (the CTM / PE-gradient chain and the batched RK2 update), so that a
+ * serving loop never allocates between its steps. */
+int litho_ctx_reserve(litho_ctx* ctx, const litho_cache* cache, int batch);
+/* Autotuner: times the candidate schedules on this device and keeps the fastest in
+ * the context for the calls that follow. With a cache: the chunk width (8 or 16
+ * columns) of the small-grid field and Z kernels for `batch` images of that cache,
+ * timed on the forward and adjoint band stages (results do not depend on it). With
+ * nimg > 0: the CTA size (128, 256, 512 or 1024 threads) of the chamfer transform of
+ * reinit_sdf for nimg images of rows x cols (the batched re-initialisations of that
+ * many images use it; the result may differ from another CTA size's in the last
+ * bit). Writes the choices (0: not tuned) to band_width / chamfer_threads (nullable). */
+int litho_ctx_autotune(litho_ctx* ctx, const litho_cache* cache, int batch, int rows, int cols,
+                       int nimg, int* band_width, int* chamfer_threads);
 /* Vector kernels of the CTM L-BFGS driver (CTM_Optimizer.cpp:189-227, LBFGS++'s
  * two-loop recursion evaluated on FP64 Gram matrices of the stored pairs).
  * litho_lbfgs_dots: out[j] = sum_i rows[j][i] v[i] accumulated in FP64 for the k

@@ -179,3 +179,31 @@ def test_host_batch_equals_device_batch(L, wl, tc_ctx, N, B, pinned):
             h_gr.data_ptr(), lo, no))
         assert list(lo) == losses and list(no) == norms
         assert torch.equal(h_gr, grads.cpu())
+
+
+def test_autotune_keeps_results(L, wl, tc_ctx):
+    """litho_ctx_autotune picks a chunk width for the batched small-grid stage (8 or 16)
+    and a chamfer CTA size; the batched evaluation is bit-identical before and after
+    (the width only distributes the outputs), and the tuned re-initialisation of a
+    batch stays within the OpenCV tolerance."""
+    from oracle import levelset_oracle as lo
+    band, r0, c0, w, wss = wl.synthetic_socs_band()
+    N, B = 256, 5
+    cache = L.ImagingCache.from_band(N, band, r0, c0, w, wss, ctx=tc_ctx)
+    targets = np.stack([wl.manhattan_target(N, 8, seed=60 + b) for b in range(B)])
+    th = torch.tensor(np.stack([wl.theta_init_reference(t) for t in targets]), dtype=torch.float32,
+                      device="cuda")
+    tg = torch.tensor(targets, dtype=torch.float32, device="cuda")
+    before = L.ctm_evaluate_batch(cache, th, tg, 0.225, 50.0)
+    g0 = before[1].clone()
+    tuned = tc_ctx.autotune(cache, batch=B, shape=(N, N), nimg=B)
+    assert tuned["band_chunk_width"] in (8, 16)
+    assert tuned["chamfer_threads"] in (128, 256, 512, 1024)
+    after = L.ctm_evaluate_batch(cache, th, tg, 0.225, 50.0)
+    assert list(before[0]) == list(after[0]) and torch.equal(g0, after[1])
+    sdf = L.LevelSetUtils.reinit_sdf_batch(tg, 2.0, 2.0, level=0.5, ctx=tc_ctx)
+    for b in range(B):
+        ref = lo.reinit_sdf(targets[b] - 0.5, 2.0, 2.0)
+        assert np.all(np.abs(cpu(sdf[b]) - ref) <= 1e-5 * np.abs(ref) + 1e-6), b
+    with pytest.raises(L.LithoError):
+        tc_ctx.autotune(shape=(2, 2), nimg=1)
