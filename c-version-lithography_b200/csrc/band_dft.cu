@@ -593,30 +593,39 @@ static size_t chat_smem(const BandGeom& g) {
 // straight into the split-BF16 operand image of the row synthesis instead of Ut:
 // x tile x / 128 at img + (x / 128) * img_tile_bytes, hi of column f at
 // sw128_offset(128, x % 128, f) and lo at sw128_offset(128, x % 128, kp + f).
-constexpr int EX_X = 64, EX_R = 8, EX_NT = 256;
-// The accumulation and store of the expansion for one CTA, from its staged
-// coefficients cf [EX_R][ncoef] and phases ph [ncoef][EX_X].
+constexpr int EX_X = 64, EX_NT = 256;
+// The accumulation and store of the expansion for one CTA of 8 PAIRS band rows, from
+// its staged coefficients cf [8 PAIRS][ncoef] and phases ph [ncoef][EX_X]. Each output
+// is summed over c in order whatever PAIRS is.
+template <int PAIRS>
 __device__ __forceinline__ void expand_store(const float2* cf, const float2* ph, int nrows,
                                              int ncoef, int N, int mode, int kp, int a0, int x0,
                                              float* __restrict__ Ut, uint8_t* __restrict__ img,
                                              uint32_t img_tile_bytes) {
-  // Thread (xx, rq): rows a0 + 2 rq and a0 + 2 rq + 1, i.e. the four consecutive
-  // output columns f0 .. f0 + 3 of image row x, written as one 8- or 16-byte store.
+  // Thread (xx, rq): row pairs p of rows a0 + 2 (PAIRS rq + p) + {0, 1}, each pair the
+  // four consecutive output columns f0 .. f0 + 3 of image row x, written as one 8- or
+  // 16-byte store.
+  constexpr int R = 8 * PAIRS;
   const int xx = threadIdx.x % EX_X, rq = threadIdx.x / EX_X;
   const int x = x0 + xx;
-  const int ra = a0 + 2 * rq, rb = ra + 1;
-  float2 acc0 = make_float2(0.f, 0.f), acc1 = acc0;
+  float2 acc[2 * PAIRS];
+#pragma unroll
+  for (int i = 0; i < 2 * PAIRS; ++i) acc[i] = make_float2(0.f, 0.f);
   for (int c = 0; c < ncoef; ++c) {
     const float2 p = ph[c * EX_X + xx];
-    cfma(acc0, cf[2 * rq * ncoef + c], p);
-    cfma(acc1, cf[(2 * rq + 1) * ncoef + c], p);
+#pragma unroll
+    for (int i = 0; i < 2 * PAIRS; ++i) cfma(acc[i], cf[(2 * PAIRS * rq + i) * ncoef + c], p);
   }
   if (x >= N) return;
-  const float ka = ra < nrows ? ((mode == 1 && ra > 0) ? 2.f : 1.f) : 0.f;
-  const float kb = rb < nrows ? ((mode == 1 && rb > 0) ? 2.f : 1.f) : 0.f;
-  const float4 v = make_float4(ka * acc0.x, ka * acc0.y, kb * acc1.x, kb * acc1.y);
-  const int f0 = 2 * ra;
-  if (f0 < kp) {
+#pragma unroll
+  for (int q = 0; q < PAIRS; ++q) {
+    const int ra = a0 + 2 * (PAIRS * rq + q), rb = ra + 1;
+    const float ka = ra < nrows ? ((mode == 1 && ra > 0) ? 2.f : 1.f) : 0.f;
+    const float kb = rb < nrows ? ((mode == 1 && rb > 0) ? 2.f : 1.f) : 0.f;
+    const float4 v = make_float4(ka * acc[2 * q].x, ka * acc[2 * q].y, kb * acc[2 * q + 1].x,
+                                 kb * acc[2 * q + 1].y);
+    const int f0 = 2 * ra;
+    if (f0 >= kp) continue;
     if (img) {
       uint8_t* tile = img + (size_t)(x / 128) * img_tile_bytes;
       const __nv_bfloat162 h01 = __floats2bfloat162_rn(v.x, v.y);
@@ -637,7 +646,7 @@ __device__ __forceinline__ void expand_store(const float2* cf, const float2* ph,
   }
   // Columns past the last row group are zero.
   if (blockIdx.y == gridDim.y - 1 && rq == 0) {
-    for (int f = 2 * EX_R * gridDim.y; f < kp; f += 4) {
+    for (int f = 2 * R * gridDim.y; f < kp; f += 4) {
       if (img) {
         uint8_t* tile = img + (size_t)(x / 128) * img_tile_bytes;
         *reinterpret_cast<uint2*>(tile + sw128_offset(128, x % 128, f)) = make_uint2(0u, 0u);
@@ -649,14 +658,16 @@ __device__ __forceinline__ void expand_store(const float2* cf, const float2* ph,
   }
 }
 
+template <int PAIRS>
 __global__ void __launch_bounds__(EX_NT)
 expand_kernel(const float2* __restrict__ coef, int nrows, int ncoef, int ld,
               const float2* __restrict__ TX, int N, int mode, int nc, int kp,
               float* __restrict__ Ut, uint8_t* __restrict__ img, uint32_t img_tile_bytes) {
+  constexpr int R = 8 * PAIRS;
   extern __shared__ float2 se[];
-  float2* cf = se;                    // [EX_R][ncoef]
-  float2* ph = se + EX_R * ncoef;     // [ncoef][EX_X]
-  const int x0 = blockIdx.x * EX_X, a0 = blockIdx.y * EX_R;
+  float2* cf = se;                    // [R][ncoef]
+  float2* ph = se + R * ncoef;        // [ncoef][EX_X]
+  const int x0 = blockIdx.x * EX_X, a0 = blockIdx.y * R;
   {  // image b of a batch
     const size_t b = blockIdx.z;
     coef += b * nrows * ld;
@@ -678,26 +689,37 @@ expand_kernel(const float2* __restrict__ coef, int nrows, int ncoef, int ld,
     return t;
   });
   pdl_wait();
-  fill_batched<EX_NT>(cf, EX_R * ncoef, [&](int i) {
+  fill_batched<EX_NT>(cf, R * ncoef, [&](int i) {
     const int r = i / ncoef, c = i % ncoef;
     return (a0 + r < nrows) ? coef[(size_t)(a0 + r) * ld + c] : make_float2(0.f, 0.f);
   });
   __syncthreads();
-  expand_store(cf, ph, nrows, ncoef, N, mode, kp, a0, x0, Ut, img, img_tile_bytes);
+  expand_store<PAIRS>(cf, ph, nrows, ncoef, N, mode, kp, a0, x0, Ut, img, img_tile_bytes);
 }
 
+template <int PAIRS>
+static cudaError_t launch_expand_t(cudaStream_t s, const float2* coef, int nrows, int ncoef,
+                                   int ld, const float2* TX, int N, int mode, int nc, int kp,
+                                   float* Ut, void* img, int batch) {
+  constexpr int R = 8 * PAIRS;
+  // Split-BF16 image tile: 128 rows x [hi | lo] of kp columns, in 64-column atoms.
+  const uint32_t img_tile_bytes = (uint32_t)((2 * kp + 63) / 64) * 128u * 128u;
+  const size_t smem = (size_t)(R * ncoef + ncoef * EX_X) * sizeof(float2);
+  cudaError_t e = cudaFuncSetAttribute(expand_kernel<PAIRS>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  dim3 grid((N + EX_X - 1) / EX_X, (nrows + R - 1) / R, batch);
+  return launch_pdl(expand_kernel<PAIRS>, grid, dim3(EX_NT), smem, s, coef, nrows, ncoef, ld, TX,
+                    N, mode, nc, kp, Ut, static_cast<uint8_t*>(img), img_tile_bytes);
+}
+
+// Batches take 16 rows per CTA (fewer phase-table stagings, more reuse of each phase),
+// single images 8 (more CTAs); the results are the same.
 static cudaError_t launch_expand(cudaStream_t s, const float2* coef, int nrows, int ncoef, int ld,
                                  const float2* TX, int N, int mode, int nc, int kp, float* Ut,
                                  void* img, int batch) {
-  // Split-BF16 image tile: 128 rows x [hi | lo] of kp columns, in 64-column atoms.
-  const uint32_t img_tile_bytes = (uint32_t)((2 * kp + 63) / 64) * 128u * 128u;
-  const size_t smem = (size_t)(EX_R * ncoef + ncoef * EX_X) * sizeof(float2);
-  cudaError_t e = cudaFuncSetAttribute(expand_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)smem);
-  if (e != cudaSuccess) return e;
-  dim3 grid((N + EX_X - 1) / EX_X, (nrows + EX_R - 1) / EX_R, batch);
-  return launch_pdl(expand_kernel, grid, dim3(EX_NT), smem, s, coef, nrows, ncoef, ld, TX, N, mode,
-                    nc, kp, Ut, static_cast<uint8_t*>(img), img_tile_bytes);
+  return batch >= 4 ? launch_expand_t<2>(s, coef, nrows, ncoef, ld, TX, N, mode, nc, kp, Ut, img, batch)
+                    : launch_expand_t<1>(s, coef, nrows, ncoef, ld, TX, N, mode, nc, kp, Ut, img, batch);
 }
 
 cudaError_t launch_band_forward(cudaStream_t s, const Cache& c, Field& f, float* ik, float* iP,
@@ -796,7 +818,7 @@ size_t band_max_smem(const BandGeom& g) {
   m = std::max(m, (size_t)(g.Pr * WMAX + g.Pc * WMAX) * sizeof(float2));
   m = std::max(m, chat_smem(g));
   m = std::max(m, gamma_smem(g));
-  m = std::max(m, (size_t)72 * (2 * g.Nc - 1) * sizeof(float2));
+  m = std::max(m, (size_t)(16 + EX_X) * (2 * g.Nc - 1) * sizeof(float2));   // expand, 16 rows
   return m;
 }
 
