@@ -119,6 +119,7 @@ SIGNATURES = {
     "litho_lbfgs_dots": (_I, [_P, _I, ctypes.c_longlong, _P, ctypes.c_longlong, _P, _PD]),
     "litho_lbfgs_combine": (_I, [_P, _I, ctypes.c_longlong, _P, ctypes.c_longlong, _PD, _P, _D,
                                  _P]),
+    "litho_lbfgs_dots3": (_I, [_P, _I, ctypes.c_longlong, _P, ctypes.c_longlong, _P, _P, _P, _PD]),
     "litho_partition_create": (_I, [_P, _I, _I, _I, _I, _I, _I, _PP]),
     "litho_partition_destroy": (_I, [_P]),
     "litho_partition_info": (_I, [_P, _PI, _PI]),

@@ -1559,6 +1559,28 @@ int litho_lbfgs_dots(litho_ctx* ctx, int k, long long n, const float* d_rows, lo
   return LITHO_OK;
 }
 
+int litho_lbfgs_dots3(litho_ctx* ctx, int k, long long n, const float* d_rows, long long ld,
+                      const float* d_v0, const float* d_v1, const float* d_v2, double* out) {
+  if (!ctx || k < 1 || k > 64 || n < 1 || ld < n || !d_rows || !d_v0 || !out || (d_v2 && !d_v1))
+    return LITHO_ERR_INVALID_ARGUMENT;
+  if (cudaSetDevice(ctx->device) != cudaSuccess) return ctx->fail(LITHO_ERR_CUDA, "cudaSetDevice");
+  const int nv = d_v2 ? 3 : (d_v1 ? 2 : 1);
+  const size_t npart = (size_t)multi_dot3_blocks((size_t)n, k) * ((k + 7) / 8) * 24;
+  int st = ctx->ensure_red(RED_PART + npart + (size_t)nv * k + 8);
+  if (st) return st;
+  double* part = ctx->d_red + RED_PART;
+  double* res = part + npart;
+  st = check_launch(ctx, launch_multi_dot3(ctx->stream, d_rows, (size_t)ld, k, (size_t)n, d_v0, d_v1,
+                                           d_v2, part, res),
+                    "L-BFGS inner products");
+  ctx->launches += 2;
+  if (st) return st;
+  LITHO_CUDA_TRY(ctx, cudaMemcpyAsync(out, res, (size_t)nv * k * sizeof(double),
+                                      cudaMemcpyDeviceToHost, ctx->stream));
+  LITHO_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  return LITHO_OK;
+}
+
 int litho_lbfgs_combine(litho_ctx* ctx, int k, long long n, const float* d_rows, long long ld,
                         const double* coef, const float* d_v, double cv, float* d_out) {
   if (!ctx || k < 0 || k > 64 || n < 1 || !d_v || !d_out ||

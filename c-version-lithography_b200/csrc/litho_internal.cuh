@@ -359,6 +359,12 @@ cudaError_t launch_multi_dot(cudaStream_t s, const float* rows, size_t ld, int k
                              const float* v, double* partial, double* out);
 cudaError_t launch_combine(cudaStream_t s, const float* rows, size_t ld, int k, size_t n,
                            const double* coef, const float* v, double cv, float* out);
+// The inner products of k rows with up to three vectors (v1, v2 nullable) in one pass:
+// out[v k + j]; partial holds multi_dot3_blocks(n, k) * ((k + 7) / 8) * 24 doubles.
+int multi_dot3_blocks(size_t n, int k);
+cudaError_t launch_multi_dot3(cudaStream_t s, const float* rows, size_t ld, int k, size_t n,
+                              const float* v0, const float* v1, const float* v2, double* partial,
+                              double* out);
 // Loss-region and Core sums of nimg tiles in one launch (rectangles: device, 4 ints
 // per tile); partial holds nimg * rect_losses_batch_blocks(ts) * 6 doubles.
 int rect_losses_batch_blocks(int ts);

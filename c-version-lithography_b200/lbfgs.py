@@ -14,9 +14,9 @@ is a combination of s_i . y_j, y_i . y_j, s_i . g and y_i . g, so the library ke
 the history pairs as rows of one device array, returns those inner products in one
 pass over the rows (litho_lbfgs_dots, FP64 accumulation), the recursion's scalars
 are formed on the host in FP64 exactly as the two loops form them, and one more pass
-builds the direction -H g (litho_lbfgs_combine). Per iteration that is three passes
-over the history (the new gradient, the new pair's two vectors) instead of one pass
-per inner product.
+builds the direction -H g (litho_lbfgs_combine). Per iteration that is one pass over
+the history for the new pair's two vectors and the new gradient together
+(litho_lbfgs_dots3) and one for the direction, instead of one pass per inner product.
 
 Stopping rule, as LBFGS++: ||g|| <= epsilon before the first step (zero
 iterations, one evaluation) or after any iteration, or ``max_iterations``
@@ -43,6 +43,15 @@ class _Device:
             self.ctx.handle, k, self.n, ctypes.c_void_p(rows.data_ptr()), self.n,
             ctypes.c_void_p(v.data_ptr()), out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
         return out
+
+    def dots3(self, rows, k: int, vs) -> np.ndarray:
+        """rows[0..k) . v for up to three vectors in one pass: an (len(vs), k) array."""
+        ptr = [ctypes.c_void_p(v.data_ptr()) for v in vs] + [None] * (3 - len(vs))
+        out = np.empty(len(vs) * k, dtype=np.float64)
+        self.ctx._check(self.ctx.lib.litho_lbfgs_dots3(
+            self.ctx.handle, k, self.n, ctypes.c_void_p(rows.data_ptr()), self.n, *ptr,
+            out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+        return out.reshape(len(vs), k)
 
     def dot(self, a, b) -> float:
         return float(self.dots(a, 1, b)[0])
@@ -161,6 +170,7 @@ def minimize_lbfgs(fg, x, m=10, epsilon=1e-5, max_iterations=100, ftol=1e-4, wol
         torch.sub(x.view(-1), x_old.view(-1), out=pair[0])
         torch.sub(g.view(-1), g_old.view(-1), out=pair[1])
         sy, yy = dev.dots(pair, 2, pair[1])
+        gp = np.zeros(2 * m)
         if sy > 1e-10 * yy:
             if len(order) == m:
                 order.pop(0)
@@ -168,14 +178,15 @@ def minimize_lbfgs(fg, x, m=10, epsilon=1e-5, max_iterations=100, ftol=1e-4, wol
             rows[slot].copy_(pair[0])
             rows[m + slot].copy_(pair[1])
             order.append(slot)
-            ds = dev.dots(rows, 2 * m, pair[0])   # s . s_b | s . y_b
-            dy = dev.dots(rows, 2 * m, pair[1])   # y . s_b | y . y_b
+            # s . s_b | s . y_b, y . s_b | y . y_b and the new gradient's, in one pass
+            ds, dy, gp = dev.dots3(rows, 2 * m, (pair[0], pair[1], g.view(-1)))
             for b in order:
                 SY[slot, b] = ds[m + b]
                 SY[b, slot] = dy[b]
                 YY[slot, b] = YY[b, slot] = dy[m + b]
             rho[slot] = 1.0 / sy
-        gp = dev.dots(rows, 2 * m, g.view(-1)) if order else np.zeros(2 * m)
+        elif order:
+            gp = dev.dots(rows, 2 * m, g.view(-1))
         coef, gamma = two_loop_coefficients(order, SY, YY, rho, gp, m)
         d = dev.combine(rows, coef, g.view(-1), -gamma, torch.empty_like(g)).view_as(g)
         step = 1.0

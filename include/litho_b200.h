@@ -276,6 +276,10 @@ int litho_lbfgs_dots(litho_ctx* ctx, int k, long long n, const float* d_rows, lo
                      const float* d_v, double* out);
 int litho_lbfgs_combine(litho_ctx* ctx, int k, long long n, const float* d_rows, long long ld,
                         const double* coef, const float* d_v, double cv, float* d_out);
+/* litho_lbfgs_dots against up to three vectors in one pass over the rows (d_v1, d_v2
+ * nullable, d_v2 only with d_v1): out[v * k + j] = rows[j] . v_v, nv * k host doubles. */
+int litho_lbfgs_dots3(litho_ctx* ctx, int k, long long n, const float* d_rows, long long ld,
+                      const float* d_v0, const float* d_v1, const float* d_v2, double* out);
 /* litho_reinit_sdf for `batch` images ([batch][rows][cols]) in one launch, inside =
  * phi > level: level 0.5 on a binary mask gives reinit_sdf(mask - 0.5), the LSM
  * initialisation (LSM_Optimizer.cpp:62), without the shifted copy. d_sdf and d_mask

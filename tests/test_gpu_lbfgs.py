@@ -61,3 +61,21 @@ def test_lbfgs_errors(L):
     assert lib.litho_lbfgs_combine(ctx.handle, 1, 16, ctypes.c_void_p(V.data_ptr()), 16, p,
                                    ctypes.c_void_p(V.data_ptr()), 1.0,
                                    ctypes.c_void_p(W.data_ptr())) != 0          # NaN coefficient
+
+
+@pytest.mark.parametrize("nv", [1, 2, 3])
+def test_lbfgs_dots3(L, LB, nv):
+    """litho_lbfgs_dots3: the inner products of 20 rows with nv vectors in one pass
+    equal those of litho_lbfgs_dots per vector (FP64 accumulation, same tolerance)."""
+    ctx = L.default_context()
+    rng = np.random.default_rng(nv)
+    k, n = 20, 123_457
+    rows = rng.standard_normal((k, n)).astype(np.float32)
+    vs = [rng.standard_normal(n).astype(np.float32) for _ in range(nv)]
+    R = torch.from_numpy(rows).cuda()
+    Vs = [torch.from_numpy(v).cuda() for v in vs]
+    got = LB._Device(ctx, n).dots3(R, k, Vs)
+    r64 = rows.astype(np.float64)
+    for i, v in enumerate(vs):
+        ref = r64 @ v.astype(np.float64)
+        assert np.all(np.abs(got[i] - ref) <= 1e-11 * np.abs(r64 * v).sum(axis=1)), i
