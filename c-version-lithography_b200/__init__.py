@@ -718,7 +718,8 @@ class CTMOptimizer:
     """CTM_Optimizer (source/optimizer/CTM_Optimizer.cpp) over the fused evaluation."""
 
     def __init__(self, cache: ImagingCache, target, threshold, alpha, iterations, learning_rate=0.9,
-                 optimizer_method="lbfgs", lbfgs_history_size=10, gradient_tolerance=0.0):
+                 optimizer_method="lbfgs", lbfgs_history_size=10, gradient_tolerance=0.0,
+                 lbfgs_strict=True):
         if optimizer_method not in ("gradient_descent", "lbfgs"):
             raise LithoError(1, "CTM optimizer must be gradient_descent or lbfgs")
         if iterations <= 0:
@@ -740,6 +741,9 @@ class CTMOptimizer:
         self.method = optimizer_method
         self.m = lbfgs_history_size
         self.tol = gradient_tolerance
+        # strict: a failed L-BFGS line search raises lbfgs.LineSearchError, as LBFGS++
+        # throws; False moves to the best Armijo point instead
+        self.lbfgs_strict = bool(lbfgs_strict)
         self.field = Field(cache)
         self.error_history: List[float] = []
         self.grad_theta = torch.empty((N, N), dtype=torch.float32, device="cuda")
@@ -798,7 +802,8 @@ class CTMOptimizer:
             return pe, gt.clone(), norm
 
         theta, self.lbfgs_info = minimize_lbfgs(fg, theta, m=self.m, epsilon=self.tol,
-                                                max_iterations=self.iterations, ctx=self.ctx)
+                                                max_iterations=self.iterations, ctx=self.ctx,
+                                                strict=self.lbfgs_strict)
         self.theta = theta
         return 0.5 * (1.0 + torch.cos(theta))
 

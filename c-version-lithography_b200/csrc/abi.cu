@@ -735,22 +735,17 @@ int litho_imaging_compute(litho_ctx* ctx, const litho_cache* cache, const float*
     return ctx->fail(LITHO_ERR_NONFINITE, "Imaging: mask, threshold, and alpha must be finite");
   if (field && field->cache != cache)
     return ctx->fail(LITHO_ERR_INVALID_ARGUMENT, "field belongs to another cache");
+  // Without a caller's field the band state of this call lives in the context's
+  // scratch (no allocation per call once the scratch has grown to this cache).
   Layout L;
-  int st = prepare(ctx, *cache, &L);
+  int st = prepare(ctx, *cache, &L, 1, field == nullptr);
   if (st) return st;
   Field tmp;
   Field* f = field;
-  float2* tmp_e = nullptr;
-  float2* tmp_m = nullptr;
-  if (!f) {  // a throw-away field lives in the adjoint part of the scratch
-    const BandGeom& g = cache->g;
-    if (cudaMalloc(&tmp_e, (size_t)g.K * g.Pr * g.Pc * sizeof(float2)) != cudaSuccess ||
-        cudaMalloc(&tmp_m, (size_t)g.Nr * g.Nc * sizeof(float2)) != cudaSuccess) {
-      cudaGetLastError();
-      if (tmp_e) cudaFree(tmp_e);
-      return ctx->fail(LITHO_ERR_OOM, "temporary field allocation failed");
-    }
-    tmp.cache = cache; tmp.e = tmp_e; tmp.mband = tmp_m;
+  if (!f) {
+    tmp.cache = cache;
+    tmp.e = at<float2>(ctx, L.fe);
+    tmp.mband = at<float2>(ctx, L.fm);
     f = &tmp;
   }
   f->valid = false;
@@ -763,7 +758,6 @@ int litho_imaging_compute(litho_ctx* ctx, const litho_cache* cache, const float*
   int nb = 0;
   st = run_forward(ctx, *cache, *f, L, 0, d_mask, nullptr, ep, &nb);
   if (!st) st = fetch(ctx, 0);
-  if (tmp_e) { cudaFree(tmp_e); cudaFree(tmp_m); }
   if (st) return st;
   if (flag_set(ctx)) {
     f->valid = false;
@@ -864,22 +858,16 @@ static int ctm_evaluate_impl(litho_ctx* ctx, const litho_cache* cache, litho_fie
     return ctx->fail(LITHO_ERR_NONFINITE, "Imaging: mask, threshold, and alpha must be finite");
   if (field && field->cache != cache)
     return ctx->fail(LITHO_ERR_INVALID_ARGUMENT, "field belongs to another cache");
+  // Without a caller's field the band state lives in the context's scratch.
   Layout L;
-  int st = prepare(ctx, *cache, &L);
+  int st = prepare(ctx, *cache, &L, 1, field == nullptr);
   if (st) return st;
   Field tmp;
   Field* f = field;
-  float2* tmp_e = nullptr;
-  float2* tmp_m = nullptr;
   if (!f) {
-    const BandGeom& g = cache->g;
-    if (cudaMalloc(&tmp_e, (size_t)g.K * g.Pr * g.Pc * sizeof(float2)) != cudaSuccess ||
-        cudaMalloc(&tmp_m, (size_t)g.Nr * g.Nc * sizeof(float2)) != cudaSuccess) {
-      cudaGetLastError();
-      if (tmp_e) cudaFree(tmp_e);
-      return ctx->fail(LITHO_ERR_OOM, "temporary field allocation failed");
-    }
-    tmp.cache = cache; tmp.e = tmp_e; tmp.mband = tmp_m;
+    tmp.cache = cache;
+    tmp.e = at<float2>(ctx, L.fe);
+    tmp.mband = at<float2>(ctx, L.fm);
     f = &tmp;
   }
   ResistEpilogue ep{};
@@ -970,7 +958,6 @@ static int ctm_evaluate_impl(litho_ctx* ctx, const litho_cache* cache, litho_fie
   ctx->eval_last_key = key;
   ctx->eval_last_valid = graphable;
   if (!st) st = fetch(ctx, 3);
-  if (tmp_e) { cudaFree(tmp_e); cudaFree(tmp_m); }
   if (st) return st;
   if (flag_set(ctx)) {
     f->valid = false;

@@ -69,8 +69,9 @@ cudaError_t launch_multi_dot(cudaStream_t s, const float* rows, size_t ld, int k
   return cudaGetLastError();
 }
 
-// Inner products of the k rows with up to three vectors in one pass over the rows:
-// CTA (bx, by) takes rows 8 by .. 8 by + 7 and a stride of the elements;
+// Inner products of the k rows with up to three vectors in one launch: CTA (bx, by)
+// takes rows 8 by .. 8 by + 7 and a stride of the elements, so every row is read
+// once and the three vectors once per group of 8 rows (three times for 20 rows);
 // partial[((by * gridDim.x + bx) * 8 + r) * 3 + v].
 __global__ void __launch_bounds__(LB_NT)
 multi_dot3_kernel(const float* __restrict__ rows, size_t ld, int k, size_t n,

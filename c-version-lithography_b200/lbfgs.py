@@ -14,13 +14,23 @@ is a combination of s_i . y_j, y_i . y_j, s_i . g and y_i . g, so the library ke
 the history pairs as rows of one device array, returns those inner products in one
 pass over the rows (litho_lbfgs_dots, FP64 accumulation), the recursion's scalars
 are formed on the host in FP64 exactly as the two loops form them, and one more pass
-builds the direction -H g (litho_lbfgs_combine). Per iteration that is one pass over
-the history for the new pair's two vectors and the new gradient together
-(litho_lbfgs_dots3) and one for the direction, instead of one pass per inner product.
+builds the direction -H g (litho_lbfgs_combine). Per iteration that is one launch
+that reads the history once for the new pair's two vectors and the new gradient
+together (litho_lbfgs_dots3; those three vectors are read once per group of 8 history
+rows) and one for the direction, instead of one pass per inner product.
 
 Stopping rule, as LBFGS++: ||g|| <= epsilon before the first step (zero
 iterations, one evaluation) or after any iteration, or ``max_iterations``
 iterations done.
+
+Failures, as LBFGS++ (whose std::runtime_error the reference does not catch, so the
+run aborts): a search direction that does not descend raises LineSearchError("the
+moving direction increases the objective function value"), and a line search that
+ends without a strong-Wolfe point raises LineSearchError("the line search routine
+reached the maximum number of iterations"). With strict=False the driver instead
+moves to the best Armijo point the failed search found (or stops, with the reason in
+``info["reason"]``, when it found none), which a long fixed-length benchmark run
+uses so that a stall near the optimum does not end it.
 """
 from __future__ import annotations
 
@@ -28,6 +38,10 @@ import ctypes
 import math
 
 import numpy as np
+
+
+class LineSearchError(RuntimeError):
+    """A failed L-BFGS step (LBFGS++ throws std::runtime_error in these cases)."""
 
 
 class _Device:
@@ -94,14 +108,18 @@ def two_loop_coefficients(order, SY, YY, rho, gp, m):
 
 
 def minimize_lbfgs(fg, x, m=10, epsilon=1e-5, max_iterations=100, ftol=1e-4, wolfe=0.9,
-                   max_linesearch=20, min_step=1e-20, max_step=1e20, ctx=None):
+                   max_linesearch=20, min_step=1e-20, max_step=1e20, ctx=None, strict=True,
+                   dev=None):
     """Minimise f from x (a contiguous float32 CUDA tensor). ``fg(x) -> (f, g, ||g||)``;
-    returns (x, info). ctx: the library context whose stream the vectors live on."""
-    if ctx is None:
-        from . import default_context
-        ctx = default_context()
-    torch = ctx.torch
-    dev = _Device(ctx, x.numel())
+    returns (x, info). ctx: the library context whose stream the vectors live on.
+    strict: raise LineSearchError where LBFGS++ throws (see the module docstring).
+    dev: the vector operations (default: the library's kernels on ctx)."""
+    if dev is None:
+        if ctx is None:
+            from . import default_context
+            ctx = default_context()
+        dev = _Device(ctx, x.numel())
+    import torch
     f, g, gnorm = fg(x)
     info = dict(iterations=0, evaluations=1, f=f, grad_norm=gnorm, reason="gradient tolerance")
     if gnorm <= epsilon:
@@ -123,6 +141,8 @@ def minimize_lbfgs(fg, x, m=10, epsilon=1e-5, max_iterations=100, ftol=1e-4, wol
         x_old, g_old, f_old = x, g, f
         dg0 = dev.dot(g, d)
         if dg0 >= 0:
+            if strict:
+                raise LineSearchError("the moving direction increases the objective function value")
             info["reason"] = "not a descent direction"
             break
         # Strong-Wolfe line search (bracketing + zoom by bisection/interpolation).
@@ -151,6 +171,9 @@ def minimize_lbfgs(fg, x, m=10, epsilon=1e-5, max_iterations=100, ftol=1e-4, wol
             if step < min_step:
                 break
         if not accepted:
+            if strict:
+                raise LineSearchError("the line search routine reached the maximum number of "
+                                      "iterations")
             # Keep the best Armijo point found, as a failed search still moves.
             if lo > 0:
                 torch.add(x_old, d, alpha=lo, out=trial)

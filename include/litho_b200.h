@@ -466,14 +466,15 @@ int litho_fullchip_lsm_step(litho_ctx* ctx, const litho_partition* partition, co
  * grids return LITHO_ERR_UNSUPPORTED without launching anything (use
  * litho_lsm_rk2_update for them). Nothing has to be zero beforehand: each call
  * clears the non-finite flag it uses. The first call on each device looks up
- * the scratch address (cudaGetSymbolAddress) and loads the module; make that
- * call before any stream capture begins. The calling thread's current device
- * must be the stream's device. Calls share the one scratch array per device,
- * so two calls that overlap in time (different host threads or streams) race:
- * serialise them. The call waits for its stream to return dt (host, nullable).
+ * the scratch address (cudaGetSymbolAddress) and loads the module. Every call
+ * copies dt and the flag back and waits on its stream, so it must never be
+ * called while that stream is being captured into a CUDA graph (the wait
+ * would invalidate the capture). The calling thread's current device must be
+ * the stream's device. Calls share the one scratch array per device, so two
+ * calls that overlap in time (different host threads or streams) race:
+ * serialise them. dt (host, nullable) receives the step used.
  * Status as litho_lsm_rk2_update; LITHO_ERR_NONFINITE for non-finite Vn.
- * This entry point has no counterpart in the reference (its LSM_Optimizer
- * allocates Eigen matrices on every step, source/optimizer/LSM_Optimizer.cpp:109-115).
+ * This entry point has no counterpart in the reference.
  */
 #define LITHO_RK2_NOALLOC_MAX_PIXELS (2048 * 2048)
 int litho_lsm_rk2_update_noalloc(void* stream, int rows, int cols, const float* d_phi,

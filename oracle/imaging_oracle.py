@@ -196,6 +196,43 @@ def ctm_evaluate(theta, target, cache, threshold, alpha):
                 grad_mask=gm, grad_theta=gt, grad_norm=float(np.linalg.norm(gt)))
 
 
+def pe_evaluate_streamed(mask, target, kernel_at, weights, ws_sum, threshold, alpha):
+    """Imaging::compute then Gradient::pe_gradient (imaging.cpp:60-171,
+    gradient.cpp:34-133) with the kernels produced one at a time by kernel_at(k)
+    (an N x N DC-at-corner array) and no field kept: the forward accumulates
+    sum_k w_k |E_k|^2 in k order; the adjoint recomputes E_k from the cached mask
+    spectrum before its two FFTs. The FFTs, shifts and sums are the reference's;
+    only the storage differs, so that 4096^2 x 48 kernels fits in host memory.
+
+    Returns dict(aerial, wafer, loss, grad_mask)."""
+    mask = np.asarray(mask, dtype=np.float64)
+    N = mask.shape[0]
+    inv = 1.0 / float(N * N)
+    K = len(weights)
+    mask_frequency = _fft2(ifftshift(mask.astype(np.complex128)))
+    aerial = np.zeros((N, N), dtype=np.float64)
+    for k in range(K):
+        e = fftshift(_ifft2_unnormalised(mask_frequency * kernel_at(k)) * inv)
+        aerial += weights[k] * (e.real ** 2 + e.imag ** 2)
+        del e
+    aerial /= ws_sum
+    wafer = 1.0 / (1.0 + np.exp(-alpha * (aerial - threshold)))
+    dldi = pe_dLdI(wafer, target)
+    grad = np.zeros((N, N), dtype=np.float64)
+    scale = 4.0 * alpha
+    for k in range(K):
+        h = kernel_at(k)
+        e = fftshift(_ifft2_unnormalised(mask_frequency * h) * inv)
+        buf = _fft2(ifftshift(e * dldi))
+        del e
+        buf *= np.conj(h)
+        buf = fftshift(_ifft2_unnormalised(buf))
+        grad += scale * weights[k] * inv * buf.real
+        del buf
+    grad /= ws_sum
+    return dict(aerial=aerial, wafer=wafer, loss=pe_loss(wafer, target), grad_mask=grad)
+
+
 def ctm_gradient_descent(target, cache, threshold, alpha, iterations, learning_rate,
                          tolerance):
     """CTM_Optimizer::_optimize_gradient_descent (CTM_Optimizer.cpp:109-173)."""

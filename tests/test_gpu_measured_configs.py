@@ -1,0 +1,206 @@
+"""Parity at the sizes the benchmark measures, against the FP64 oracle.
+
+* 4096^2 with 48 SOCS kernels of 35 x 35 (the large case of the precision sweep): the
+  FP32 and the split-BF16 paths each against the FP64 restatement of the reference's
+  FFT algorithm (Imaging::compute, Gradient::pe_gradient; imaging.cpp:60-171,
+  gradient.cpp:34-133), streamed over the kernels so that the oracle's memory stays
+  bounded (one mask spectrum, one field at a time, E_k recomputed in the adjoint).
+  Checked: max|dI| / max I, dPE/dM relative L2, PE, the printed binary image
+  (I >= threshold) identical except pixels within 1e-4 of the threshold, and the EPE at
+  64 seeded edge points of the target (|dEPE| / max(|EPE|, 1 px)).
+* The plain single CTM gradient step of one 512^2 tile: seeded Manhattan target of
+  6-12 rectangles, theta = pi (1 - target), 24 SOCS kernels, resist steepness 50,
+  threshold 0.225. The mask (1 + cos theta) / 2 is the target itself, so sin theta is 0
+  up to rounding and dPE/dtheta vanishes; the aerial image, the wafer image, PE and
+  dPE/dM are checked against the oracle, and dPE/dtheta against the oracle's
+  -1/2 dPE/dM sin(theta) of the same FP32 theta (absolute, relative to max |dPE/dM|).
+* 2048^2 with 24 kernels in split-BF16: the printed-image criterion of the headline tile.
+
+Bounds (written per test): FP32 1e-5 of peak intensity, gradient relative L2 1e-4, PE
+1e-5 relative; split-BF16 1e-3 of peak (its stated bound), gradient 1e-3, PE 1e-4.
+"""
+import importlib
+
+import numpy as np
+import pytest
+
+from oracle import imaging_oracle as io
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+THR, ALPHA = 0.225, 50.0
+BOUNDS = {"fp32": dict(image=1e-5, grad=1e-4, loss=1e-5, epe=1e-3),
+          "bf16x3": dict(image=1e-3, grad=1e-3, loss=1e-4, epe=1e-2)}
+PRINT_BAND = 1e-4   # printed pixels may differ only within this distance of the threshold
+
+
+@pytest.fixture(scope="module")
+def L():
+    p = importlib.import_module("c-version-lithography_b200")
+    assert torch.cuda.is_available(), "GPU tests need a CUDA device"
+    p.load_library()
+    return p
+
+
+@pytest.fixture(scope="module")
+def wl():
+    return importlib.import_module("c-version-lithography_b200.workloads")
+
+
+def cpu(t):
+    return t.detach().cpu().numpy().astype(np.float64)
+
+
+def peak_err(a, ref):
+    return float(np.max(np.abs(a - ref)) / np.max(np.abs(ref)))
+
+
+def rel_l2(a, ref):
+    return float(np.linalg.norm(a - ref) / np.linalg.norm(ref))
+
+
+def printed_mismatch(aerial, ref_aerial):
+    """Pixels whose printed state (I >= threshold) differs from the oracle's while the
+    oracle's intensity is more than PRINT_BAND away from the threshold."""
+    differ = (aerial >= THR) != (ref_aerial >= THR)
+    return int(np.count_nonzero(differ & (np.abs(ref_aerial - THR) > PRINT_BAND))), int(differ.sum())
+
+
+def edge_points(target, n, seed, aerial, min_grad=0.01):
+    """n seeded points on the 0.5 contour of a binary target whose nearest pixel has
+    |grad I| >= min_grad in the oracle's image (the EPE divides by |grad I|)."""
+    from oracle.levelset_oracle import gradient_1d
+    rng = np.random.default_rng(seed)
+    ys, xs = np.nonzero(np.diff(target, axis=0))
+    pts = [(y + 0.5, x + rng.uniform(-0.3, 0.3)) for y, x in zip(ys, xs)]
+    ys, xs = np.nonzero(np.diff(target, axis=1))
+    pts += [(y + rng.uniform(-0.3, 0.3), x + 0.5) for y, x in zip(ys, xs)]
+    pts = np.array(pts)
+    mag = np.hypot(gradient_1d(aerial, 1.0, 1), gradient_1d(aerial, 1.0, 0))
+    iy = np.clip(np.rint(pts[:, 0]).astype(int), 0, aerial.shape[0] - 1)
+    ix = np.clip(np.rint(pts[:, 1]).astype(int), 0, aerial.shape[1] - 1)
+    pts = pts[mag[iy, ix] >= min_grad]
+    return pts[rng.choice(len(pts), size=n, replace=False)]
+
+
+def band_kernel_at(band, r0, c0, N):
+    rows = (r0 + np.arange(band.shape[1])) % N
+    cols = (c0 + np.arange(band.shape[2])) % N
+
+    def at(k):
+        h = np.zeros((N, N), dtype=np.complex128)
+        h[rows[:, None], cols[None, :]] = band[k]
+        return h
+    return at
+
+
+def device_mask_eval(L, cache, mask, target, eps=None):
+    imaging = L.Imaging(cache)
+    r = imaging.compute(mask, THR, ALPHA)
+    grad = L.Gradient(cache, THR, ALPHA)
+    g = grad.pe_gradient(r.wafer_image, target, imaging.get_electric_field())
+    out = dict(aerial=cpu(r.aerial_image), wafer=cpu(r.wafer_image), grad_mask=cpu(g),
+               loss=grad.last_loss)
+    if eps is not None:
+        e = L.Loss.evaluate_sparse_epe(r.aerial_image, eps, np.ones(len(eps)), THR, 1.0,
+                                       ctx=cache.ctx)
+        out["epe"] = np.asarray(e.signed_epe_pixel, dtype=np.float64)
+    return out
+
+
+@pytest.fixture(scope="module")
+def case4096(wl):
+    N, K = 4096, 48
+    band, r0, c0, w, wss = wl.synthetic_socs_band(K=K)
+    target = wl.manhattan_target(N, 120, seed=41)
+    ref = io.pe_evaluate_streamed(target, target, band_kernel_at(band, r0, c0, N), w, wss,
+                                  THR, ALPHA)
+    eps = edge_points(target, 64, 42, ref["aerial"])
+    ref["epe"] = io.evaluate_sparse_epe(ref["aerial"], eps, np.ones(64), THR,
+                                        1.0)["signed_epe_pixel"]
+    return N, (band, r0, c0, w, wss), target, eps, ref
+
+
+@pytest.mark.parametrize("prec", ["fp32", "bf16x3"])
+def test_4096_k48_against_fp64(L, case4096, prec):
+    N, (band, r0, c0, w, wss), target, eps, ref = case4096
+    ctx = L.Context()
+    ctx.set_precision(prec)
+    cache = L.ImagingCache.from_band(N, band, r0, c0, w, wss, ctx=ctx)
+    got = device_mask_eval(L, cache, target, target, eps)
+    ctx.close()
+    b = BOUNDS[prec]
+    di = peak_err(got["aerial"], ref["aerial"])
+    dg = rel_l2(got["grad_mask"], ref["grad_mask"])
+    dl = abs(got["loss"] - ref["loss"]) / ref["loss"]
+    de = float(np.max(np.abs(got["epe"] - ref["epe"]) / np.maximum(np.abs(ref["epe"]), 1.0)))
+    bad, differ = printed_mismatch(got["aerial"], ref["aerial"])
+    print(f"\n4096^2 K=48 {prec} vs FP64: max|dI|/max I {di:.2e}, grad rel L2 {dg:.2e}, "
+          f"PE rel {dl:.2e}, EPE rel {de:.2e}, printed pixels differing {differ} "
+          f"(beyond {PRINT_BAND:g} of threshold: {bad})")
+    assert di <= b["image"] and dg <= b["grad"] and dl <= b["loss"] and de <= b["epe"]
+    assert bad == 0
+
+
+@pytest.mark.parametrize("prec", ["fp32", "bf16x3"])
+def test_single_ctm_step_512_theta_from_target(L, wl, prec):
+    N = 512
+    band, r0, c0, w, wss = wl.synthetic_socs_band(K=24)
+    n_rect = int(np.random.default_rng(12).integers(6, 13))
+    target = wl.manhattan_target(N, n_rect, seed=12)
+    theta32 = wl.theta_init_from_target(target).astype(np.float32)
+    theta = theta32.astype(np.float64)
+    oc = io.OracleCache(N=N, kernels=list(wl.band_to_dense(band, r0, c0, N)),
+                        source_ws=np.array([wss]), eigenvalues=tuple(w))
+    ref = io.ctm_evaluate(theta, target, oc, THR, ALPHA)
+    assert np.array_equal(ref["mask"].round(6), target)     # mask = target for this theta
+
+    ctx = L.Context()
+    ctx.set_precision(prec)
+    cache = L.ImagingCache.from_band(N, band, r0, c0, w, wss, ctx=ctx)
+    opt = L.CTMOptimizer(cache, target, THR, ALPHA, iterations=1)
+    loss, gt, norm = opt.evaluate(torch.tensor(theta32, device="cuda"), want_mask=True)
+    got = device_mask_eval(L, cache, cpu(opt.mask), target)
+    ctx.close()
+    b = BOUNDS[prec]
+    di = peak_err(got["aerial"], ref["aerial"])
+    dw = float(np.max(np.abs(got["wafer"] - ref["wafer"])))
+    dg = rel_l2(got["grad_mask"], ref["grad_mask"])
+    dl = abs(loss - ref["loss"]) / ref["loss"]
+    gscale = float(np.max(np.abs(ref["grad_mask"])))
+    dth = float(np.max(np.abs(cpu(gt) - ref["grad_theta"]))) / gscale
+    bad, differ = printed_mismatch(got["aerial"], ref["aerial"])
+    print(f"\n512^2 K=24 theta=pi(1-target) {prec}: max|dI|/max I {di:.2e}, max|dW| {dw:.2e}, "
+          f"dPE/dM rel L2 {dg:.2e}, PE rel {dl:.2e}, max|dPE/dtheta - ref| / max|dPE/dM| "
+          f"{dth:.2e}, printed pixels differing {differ}")
+    assert di <= b["image"] and dg <= b["grad"] and dl <= b["loss"]
+    # the wafer image is the sigmoid of I: its error is at most alpha/4 times I's
+    assert dw <= ALPHA / 4 * b["image"] * float(np.max(ref["aerial"]))
+    assert dth <= 1e-6 and bad == 0
+    assert norm <= 1e-6 * float(np.linalg.norm(ref["grad_mask"]))
+
+
+def test_2048_bf16x3_printed_image(L, wl):
+    N = 2048
+    band, r0, c0, w, wss = wl.synthetic_socs_band()
+    target = wl.manhattan_target(N, 100, seed=1, n_lt=10)
+    theta = wl.theta_init_reference(target)
+    oc = io.OracleCache(N=N, kernels=list(wl.band_to_dense(band, r0, c0, N)),
+                        source_ws=np.array([wss]), eigenvalues=tuple(w))
+    ref = io.ctm_evaluate(theta, target, oc, THR, ALPHA)
+    ctx = L.Context()
+    ctx.set_precision("bf16x3")
+    cache = L.ImagingCache.from_band(N, band, r0, c0, w, wss, ctx=ctx)
+    opt = L.CTMOptimizer(cache, target, THR, ALPHA, iterations=1)
+    loss, gt, _ = opt.evaluate(torch.tensor(theta, dtype=torch.float32, device="cuda"))
+    r = L.Imaging(cache).compute(io.theta_to_mask(theta), THR, ALPHA)
+    a = cpu(r.aerial_image)
+    ctx.close()
+    di = peak_err(a, ref["aerial"])
+    dg = rel_l2(cpu(gt), ref["grad_theta"])
+    bad, differ = printed_mismatch(a, ref["aerial"])
+    print(f"\n2048^2 K=24 bf16x3: max|dI|/max I {di:.2e}, dPE/dtheta rel L2 {dg:.2e}, "
+          f"printed pixels differing {differ} (beyond {PRINT_BAND:g}: {bad})")
+    assert di <= 1e-3 and dg <= 1e-3 and abs(loss - ref["loss"]) <= 1e-4 * ref["loss"]
+    assert bad == 0

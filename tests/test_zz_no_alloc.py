@@ -4,6 +4,11 @@ purpose: it must pass alone and after every other test in the process.
 
 Tolerance: both entry points run the same kernels, so phi, mask and dt must agree
 to max|d| <= 1e-6 (in practice bit-identical).
+
+The no-allocation check reads the device's free memory (torch.cuda.mem_get_info),
+which counts every process and context on the GPU, so it assumes the GPU to itself:
+it measures warm calls (the first call loads the module, whose static scratch array
+is resident from then on) and retries, failing only if free memory drops on every try.
 """
 import ctypes
 import importlib
@@ -84,12 +89,19 @@ def test_noalloc_limits_and_flag(L):
     assert st == 3
     st, dt = noalloc(L, phi, vn, 1.0, 1.0, 0.5, 0.01, out, None)
     assert st == 0 and dt > 0.0
-    # no device memory is taken by repeated calls
-    torch.cuda.synchronize()
-    free0 = torch.cuda.mem_get_info()[0]
+    # no device memory is taken by repeated calls (another tenant's allocation between
+    # the two readings would read as a drop, hence the retries)
+    drops = []
     for _ in range(3):
-        assert noalloc(L, phi, vn, 1.0, 1.0, 0.5, 0.01, out, None)[0] == 0
-    assert torch.cuda.mem_get_info()[0] == free0
+        torch.cuda.synchronize()
+        free0 = torch.cuda.mem_get_info()[0]
+        for _ in range(3):
+            assert noalloc(L, phi, vn, 1.0, 1.0, 0.5, 0.01, out, None)[0] == 0
+        torch.cuda.synchronize()
+        drops.append(free0 - torch.cuda.mem_get_info()[0])
+        if drops[-1] <= 0:
+            break
+    assert min(drops) <= 0, drops
 
 
 def noalloc_shape(L, rows, cols, phi, vn, out):
