@@ -71,6 +71,23 @@ class ExchangeOptionsC(ctypes.Structure):
                 ("fusion_weight_neighbor", _D)]
 
 
+class SocsParamsC(ctypes.Structure):
+    """litho_socs_params (include/litho_b200.h)."""
+    _fields_ = [("N", ctypes.c_int), ("pixel_nm", ctypes.c_double),
+                ("wavelength_nm", ctypes.c_double), ("na", ctypes.c_double),
+                ("sigma_in", ctypes.c_double), ("sigma_out", ctypes.c_double),
+                ("smoothing", ctypes.c_double), ("upsample", ctypes.c_int),
+                ("num_socs", ctypes.c_int), ("compact", ctypes.c_int),
+                ("zernike", ctypes.POINTER(ctypes.c_double))]
+
+
+class SocsInfoC(ctypes.Structure):
+    """litho_socs_info (include/litho_b200.h)."""
+    _fields_ = [("K", ctypes.c_int), ("Ns", ctypes.c_int), ("Nr", ctypes.c_int),
+                ("Nc", ctypes.c_int), ("row0", ctypes.c_int), ("col0", ctypes.c_int),
+                ("ws_sum", ctypes.c_double), ("energy_captured", ctypes.c_double)]
+
+
 class ExchangeEpeC(ctypes.Structure):
     """litho_exchange_epe (include/litho_b200.h)."""
     _fields_ = [("epe_weight", _D), ("main_region_dilation_pixels", _I), ("epe_pixel_size", _D),
@@ -89,10 +106,12 @@ SIGNATURES = {
     "litho_ctx_set_precision": (_I, [_P, _I]),
     "litho_ctx_launch_count": (ctypes.c_longlong, [_P]),
     "litho_ctx_enable_graphs": (_I, [_P, _I]),
+    "litho_ctx_set_tc_schedule": (_I, [_P, _I]),
     "litho_ctx_enable_stage_timing": (_I, [_P, _I]),
     "litho_ctx_stage_times": (_I, [_P, _PD, ctypes.POINTER(ctypes.c_longlong)]),
     "litho_cache_create_dense": (_I, [_P, _I, _I, _PD, _PD, _D, _PP]),
     "litho_cache_create_band": (_I, [_P, _I, _I, _I, _I, _I, _I, _PD, _PD, _D, _PP]),
+    "litho_socs_prepare": (_I, [_P, _P, _PP, _P, _PD, _PD]),
     "litho_cache_info": (_I, [_P, _PI, _PI, _PI, _PI, _PI, _PI]),
     "litho_cache_destroy": (_I, [_P]),
     "litho_field_create": (_I, [_P, _P, _PP]),
@@ -243,6 +262,14 @@ class Context:
         """CUDA-graph replay of repeated CTM evaluations (on by default)."""
         self._check(self.lib.litho_ctx_enable_graphs(self.handle, 1 if on else 0))
 
+    TC_SCHEDULES = {"auto": 0, "per_tile": 1, "persistent": 2}
+
+    def set_tc_schedule(self, mode: str):
+        """Schedule of the split-BF16 tensor-core passes: 'auto' (the persistent
+        pipelines where supported), 'per_tile' (one CTA per 128 x 128 tile) or
+        'persistent' (one CTA per SM, warp-specialised, pipelined over the tiles)."""
+        self._check(self.lib.litho_ctx_set_tc_schedule(self.handle, self.TC_SCHEDULES[mode]))
+
     def enable_stage_timing(self, on: bool = True):
         self._check(self.lib.litho_ctx_enable_stage_timing(self.handle, 1 if on else 0))
 
@@ -350,6 +377,51 @@ class ImagingCache:
             self.close()
         except Exception:
             pass
+
+
+class LithoPrepare:
+    """LithoPrepare's SOCS set-up (source/litho_model/litho_prepare.cpp:16-385): the
+    optics (grid N x N of pixel_nm, wavelength, NA, annular sigma_in..sigma_out, Fringe
+    Zernike aberrations {index: waves}) give the source points, the shifted-pupil matrix
+    and its num_socs strongest coherent modes, computed in FP64 on the device
+    (litho_socs_prepare). ``cache`` is the resulting ImagingCache; ``eigenvalues`` the
+    kept sigma_k^2 (largest first), ``source_ws_sum`` the image normaliser, ``info`` the
+    sizes and ``band_kernels`` (K x Nr x Nc) the kernels on their band (integer
+    frequencies row0.., col0..)."""
+
+    def __init__(self, N: int, pixel_nm: float, wavelength_nm: float, na: float, sigma_in: float,
+                 sigma_out: float, num_socs: int = 36, compact: bool = True, aberrations=None,
+                 smoothing: float = 0.0, upsample: int = 10, ctx: Optional[Context] = None):
+        ctx = ctx or default_context()
+        z = None
+        if aberrations:
+            zc = np.zeros(11)
+            for idx, c in dict(aberrations).items():
+                if 1 <= int(idx) <= 11:
+                    zc[int(idx) - 1] = float(c)
+            z = np.ascontiguousarray(zc)
+        prm = SocsParamsC(int(N), float(pixel_nm), float(wavelength_nm), float(na),
+                          float(sigma_in), float(sigma_out), float(smoothing), int(upsample),
+                          int(num_socs), 1 if compact else 0,
+                          z.ctypes.data_as(_PD) if z is not None else None)
+        info = SocsInfoC()
+        h = ctypes.c_void_p()
+        ctx._check(ctx.lib.litho_socs_prepare(ctx.handle, ctypes.byref(prm), ctypes.byref(h),
+                                              ctypes.byref(info), None, None))
+        ctx.lib.litho_cache_destroy(h)
+        # second pass with buffers sized from the first (the set-up is deterministic)
+        K, M = info.K, info.Nr * info.Nc
+        ev = np.zeros(K)
+        band = np.zeros(2 * K * M)
+        h = ctypes.c_void_p()
+        ctx._check(ctx.lib.litho_socs_prepare(ctx.handle, ctypes.byref(prm), ctypes.byref(h),
+                                              ctypes.byref(info), ev.ctypes.data_as(_PD),
+                                              band.ctypes.data_as(_PD)))
+        self.cache = ImagingCache(h, ctx)
+        self.eigenvalues = ev
+        self.band_kernels = band.view(np.complex128).reshape(K, info.Nr, info.Nc)
+        self.source_ws_sum = info.ws_sum
+        self.info = {f: getattr(info, f) for f, _ in SocsInfoC._fields_}
 
 
 class Field:

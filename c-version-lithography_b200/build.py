@@ -39,7 +39,7 @@ def build(verbose=False, force=False):
         subprocess.run(cmd, check=True)
         objs.append(o)
     cmd = [NVCC, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", *objs, "-o", OUT,
-           "-lcudart"]
+           "-lcudart", "-lcusolver"]
     subprocess.run(cmd, check=True)
     return OUT
 

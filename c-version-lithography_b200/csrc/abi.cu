@@ -15,10 +15,6 @@
 
 using namespace litho_b200;
 
-struct litho_ctx : public Context {};
-struct litho_cache : public Cache {};
-struct litho_field : public Field {};
-
 namespace {
 
 constexpr double kTwoPi = 6.283185307179586476925286766559;
@@ -263,6 +259,15 @@ int litho_ctx_enable_graphs(litho_ctx* ctx, int on) {
     cudaGraphExecDestroy(ctx->eval_graph);
     ctx->eval_graph = nullptr;
   }
+  return LITHO_OK;
+}
+
+int litho_ctx_set_tc_schedule(litho_ctx* ctx, int schedule) {
+  if (!ctx) return LITHO_ERR_INVALID_ARGUMENT;
+  if (schedule != LITHO_TC_SCHEDULE_AUTO && schedule != LITHO_TC_SCHEDULE_PER_TILE &&
+      schedule != LITHO_TC_SCHEDULE_PERSISTENT)
+    return ctx->fail(LITHO_ERR_INVALID_ARGUMENT, "unknown tensor-core schedule");
+  ctx->tc_schedule = schedule;
   return LITHO_OK;
 }
 
@@ -585,7 +590,13 @@ int run_forward(Context* ctx, const Cache& c, Field& f, const Layout& L, int inp
   int st;
   ctx->stage_begin(0);
   const bool tc = ctx->precision == LITHO_PRECISION_BF16X3 && c.TXS_img;
-  if (tc)
+  const bool pers = tc && ctx->tc_persistent();
+  if (tc && pers && tc3_analysis_supported(g.Nc, g.Nr))
+    st = check_launch(ctx, launch_analysis_tc3(s, input_mode, input, mask_out, flag, g.N, g.Nc,
+                                               g.Nr, g.Nr, 0, at<float2>(ctx, L.part), c.TXS_img,
+                                               c.TYS_img, flag + 1, batch),
+                      "tensor-core tile analysis (persistent)");
+  else if (tc)
     st = check_launch(ctx, launch_analysis_tc2(s, input_mode, input, mask_out, flag, g.N, g.Nc,
                                                g.Nr, g.Nr, 0, at<float2>(ctx, L.part), c.TXS_img,
                                                c.TYS_img, flag + 1, batch),
@@ -615,12 +626,22 @@ int run_forward(Context* ctx, const Cache& c, Field& f, const Layout& L, int inp
   ctx->stage_begin(3);
   if (tc) {
     int* err = reinterpret_cast<int*>(ctx->d_red + RED_FLAG) + 1;
-    if (fuse_adjoint)
+    if (fuse_adjoint && pers && tc3_fused_supported(g.kp_rows, g.Nc, g.Nr))
+      st = check_launch(ctx, launch_synth_resist_analysis_tc3(
+                                 s, c.AYD_img, at<void>(ctx, L.img), g.N, g.kp_rows, ep, g.Nc,
+                                 g.Nr, at<float2>(ctx, L.part), flag, c.TXD_img, c.TYD_img, err,
+                                 nblocks, batch),
+                        "tensor-core row synthesis with adjoint tile analysis (persistent)");
+    else if (fuse_adjoint)
       st = check_launch(ctx, launch_synth_resist_analysis_tc2(
                                  s, c.AYD_img, at<void>(ctx, L.img), g.N, g.kp_rows, ep, g.Nc,
                                  g.Nr, at<float2>(ctx, L.part), flag, c.TXD_img, c.TYD_img, err,
                                  nblocks, batch),
                         "tensor-core row synthesis with adjoint tile analysis");
+    else if (pers && tc3_synth_supported(g.kp_rows))
+      st = check_launch(ctx, launch_synth_resist_tc3(s, c.AYD_img, at<void>(ctx, L.img), g.N,
+                                                     g.kp_rows, ep, err, nblocks, batch),
+                        "tensor-core row synthesis (persistent)");
     else
       st = check_launch(ctx, launch_synth_resist_tc2(s, c.AYD_img, at<void>(ctx, L.img), g.N,
                                                      g.kp_rows, ep, err, nblocks, batch),
@@ -646,8 +667,14 @@ int run_adjoint(Context* ctx, const Cache& c, const Field& f, const Layout& L, c
   int st;
   ctx->stage_begin(4);
   const bool tc = ctx->precision == LITHO_PRECISION_BF16X3 && c.TXD_img;
+  const bool pers = tc && ctx->tc_persistent();
   if (analysed)
     st = LITHO_OK;  // the partials are already in L.part
+  else if (tc && pers && tc3_analysis_supported(g.Nc, g.Nr))
+    st = check_launch(ctx, launch_analysis_tc3(s, 0, dldi, nullptr, flag, g.N, g.Nc, na, g.Nr, 1,
+                                               at<float2>(ctx, L.part), c.TXD_img, c.TYD_img,
+                                               flag + 1, batch),
+                      "tensor-core adjoint tile analysis (persistent)");
   else if (tc)
     st = check_launch(ctx, launch_analysis_tc2(s, 0, dldi, nullptr, flag, g.N, g.Nc, na, g.Nr, 1,
                                                at<float2>(ctx, L.part), c.TXD_img, c.TYD_img,
@@ -677,9 +704,14 @@ int run_adjoint(Context* ctx, const Cache& c, const Field& f, const Layout& L, c
   ctx->stage_begin(7);
   if (tc) {
     int* err = reinterpret_cast<int*>(ctx->d_red + RED_FLAG) + 1;
-    st = check_launch(ctx, launch_synth_grad_tc2(s, c.AYS_img, at<void>(ctx, L.img), g.N,
-                                                 g.kp_rows, ep, err, nblocks, batch),
-                      "tensor-core adjoint row synthesis");
+    if (pers && tc3_synth_supported(g.kp_rows))
+      st = check_launch(ctx, launch_synth_grad_tc3(s, c.AYS_img, at<void>(ctx, L.img), g.N,
+                                                   g.kp_rows, ep, err, nblocks, batch),
+                        "tensor-core adjoint row synthesis (persistent)");
+    else
+      st = check_launch(ctx, launch_synth_grad_tc2(s, c.AYS_img, at<void>(ctx, L.img), g.N,
+                                                   g.kp_rows, ep, err, nblocks, batch),
+                        "tensor-core adjoint row synthesis");
   } else {
     st = check_launch(ctx, launch_synth_grad(s, c.AYS, at<float>(ctx, L.Vt), g.N, g.kp_rows, ep,
                                              nblocks),
@@ -913,7 +945,9 @@ static int ctm_evaluate_impl(litho_ctx* ctx, const litho_cache* cache, litho_fie
                           d_target,    d_mask,        d_aerial,          d_wafer,
                           d_grad_mask, d_grad_theta,  ctx->scratch.base, ctx->d_red,
                           cache->H,    cache->AYD_img, cache->TXS,
-                          reinterpret_cast<const void*>((uintptr_t)ctx->precision)};
+                          reinterpret_cast<const void*>(
+                              (uintptr_t)ctx->precision |
+                              ((uintptr_t)ctx->tc_persistent() << 4))};
   for (int i = 0; i < 16; ++i) key.ptr[i] = ptrs[i];
   const int geom[6] = {g.N, g.K, g.Nr, g.Nc, g.row0, g.col0};
   for (int i = 0; i < 6; ++i) key.geom[i] = geom[i];

@@ -165,6 +165,12 @@ struct Context {
     const auto it = tuned_chamfer.find({cols, nimg});
     return it == tuned_chamfer.end() ? 0 : it->second;
   }
+  // Schedule of the split-BF16 tensor-core passes (LITHO_TC_SCHEDULE_*): per-tile CTAs
+  // (tc2.cu) or the persistent pipelines (tc3.cu, the default where supported). A
+  // batched call and a single-image call take the same schedule, so every image's
+  // results are the same alone and in a batch, bit for bit.
+  int tc_schedule = LITHO_TC_SCHEDULE_AUTO;
+  bool tc_persistent() const { return tc_schedule != LITHO_TC_SCHEDULE_PER_TILE; }
 };
 
 // ---------------------------------------------------------------- launch helper
@@ -289,6 +295,29 @@ cudaError_t launch_synth_resist_analysis_tc2(cudaStream_t s, const void* Aimg, c
                                              int nr, float2* part, int* flag, const void* tx_img,
                                              const void* ty_img, int* err, int* nblocks,
                                              int batch = 1);
+// The same passes as persistent, warp-specialised pipelines (tc3.cu): one CTA per SM
+// over a contiguous share of the (image, tile) items. Same arguments and results
+// (image values bit for bit; FP64 partial sums in another order). Supported for tile
+// analyses with 2 Nc rounded to 16 at most 96 and syntheses with kp <= 128; the fused
+// kernel also needs its shared-memory plan to fit.
+bool tc3_analysis_supported(int ncols, int nr);
+bool tc3_synth_supported(int kp);
+bool tc3_fused_supported(int kp, int ncols, int nr);
+cudaError_t launch_analysis_tc3(cudaStream_t s, int mode, const float* in, float* mask_out,
+                                int* flag, int N, int ncols, int nrows_out, int nr, int sym,
+                                float2* part, const void* tx_img, const void* ty_img, int* err,
+                                int batch = 1);
+cudaError_t launch_synth_resist_tc3(cudaStream_t s, const void* Aimg, const void* Bimg, int N,
+                                    int kp, const ResistEpilogue& ep, int* err, int* nblocks,
+                                    int batch = 1);
+cudaError_t launch_synth_grad_tc3(cudaStream_t s, const void* Aimg, const void* Bimg, int N,
+                                  int kp, const GradEpilogue& ep, int* err, int* nblocks,
+                                  int batch = 1);
+cudaError_t launch_synth_resist_analysis_tc3(cudaStream_t s, const void* Aimg, const void* Bimg,
+                                             int N, int kp, const ResistEpilogue& ep, int ncols,
+                                             int nr, float2* part, int* flag, const void* tx_img,
+                                             const void* ty_img, int* err, int* nblocks,
+                                             int batch = 1);
 // The tensor-core path needs kp <= 128 and 2 Nc <= 128 (bands up to 64 x 64).
 inline bool tc2_supported(const BandGeom& g) {
   return g.kp_rows <= 128 && tc2_analysis_supported(g.Nc, g.Nr);
@@ -382,3 +411,8 @@ cudaError_t launch_theta_update(cudaStream_t s, float* theta, const float* grad,
                                 int ts, const int* win, float lr, float* mask);
 
 }  // namespace litho_b200
+
+// The ABI's opaque handles are the library's own objects.
+struct litho_ctx : public litho_b200::Context {};
+struct litho_cache : public litho_b200::Cache {};
+struct litho_field : public litho_b200::Field {};

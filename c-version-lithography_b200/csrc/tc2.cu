@@ -20,6 +20,7 @@
 
 #include "device_common.cuh"
 #include "tc_ptx.cuh"
+#include "tc_split2.cuh"
 
 namespace litho_b200 {
 
@@ -27,45 +28,6 @@ namespace litho_b200 {
 // N * N apart).
 __device__ __forceinline__ size_t img_row(int N, int m) {
   return ((size_t)blockIdx.z * N + m) * N;
-}
-
-__host__ __device__ constexpr uint32_t s2_atoms(int K) { return (uint32_t)(2 * K + 63) / 64; }
-__host__ __device__ constexpr uint32_t s2_tile_bytes(int RB, int K) {
-  return s2_atoms(K) * (uint32_t)RB * 128u;
-}
-
-// Descriptor of the 16-wide K step starting at column k of a split2 tile with RB rows.
-__device__ __forceinline__ uint64_t s2_desc(uint32_t base, int RB, int k) {
-  return tc::desc_sw128(base + (uint32_t)(k / 64) * (uint32_t)RB * 128u +
-                        (uint32_t)((k % 64) / 16) * 32u);
-}
-
-// The three split-BF16 sections of D[M][N] = A[M][K] . B[N][K]^T (K % 16 == 0):
-// 3 K / 16 tcgen05.mma instructions, issued by one thread.
-__device__ __forceinline__ void s2_mma(uint32_t tmem, uint32_t sa, int ra, uint32_t sb, int rb,
-                                       int K, uint32_t idesc) {
-  const int aoff[3] = {0, 0, K}, boff[3] = {0, K, 0};
-  bool first = true;
-  for (int s = 0; s < 3; ++s)
-    for (int k = 0; k < K; k += 16) {
-      tc::mma_bf16(tmem, s2_desc(sa, ra, aoff[s] + k), s2_desc(sb, rb, boff[s] + k), idesc,
-                   first ? 0u : 1u);
-      first = false;
-    }
-}
-
-__device__ __forceinline__ void split_bf16(float v, __nv_bfloat16& hi, __nv_bfloat16& lo) {
-  hi = __float2bfloat16_rn(v);
-  lo = __float2bfloat16_rn(v - __bfloat162float(hi));
-}
-// The same split for two values with packed conversions: hi2 / lo2 hold (a, b)
-// as consecutive bf16 (a at the lower address).
-__device__ __forceinline__ void split_pair(float a, float b, uint32_t& hi2, uint32_t& lo2) {
-  const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
-  const float2 hf = __bfloat1622float2(h);
-  const __nv_bfloat162 l = __floats2bfloat162_rn(a - hf.x, b - hf.y);
-  hi2 = *reinterpret_cast<const uint32_t*>(&h);
-  lo2 = *reinterpret_cast<const uint32_t*>(&l);
 }
 
 // ---------------------------------------------------------------- image packing
@@ -131,30 +93,6 @@ cudaError_t launch_pack_split2(cudaStream_t st, const float* src, int kind, int 
                     RB, K, nkb, reinterpret_cast<uint4*>(dst), n16);
 }
 
-// 16 consecutive FP32 columns of this thread's TMEM lane.
-__device__ __forceinline__ void tmem_ld16x(uint32_t taddr, float (&v)[16]) {
-  uint32_t r[16];
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
-      "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
-        "=r"(r[14]), "=r"(r[15])
-      : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
-}
-
-__device__ __forceinline__ void bulk_tile(uint32_t dst, const uint8_t* src, uint32_t bytes,
-                                          uint32_t bar) {
-  tc::mbar_expect_tx(bar, bytes);
-  for (uint32_t q = 0; q < bytes; q += 16384) {
-    const uint32_t n = bytes - q < 16384u ? bytes - q : 16384u;
-    tc::bulk_g2s(dst + q, src + q, n, bar);
-  }
-}
-
 // ---------------------------------------------------------------- tile analysis
 // For every 128 x 128 tile (rows y0.., columns x0..) of the image A:
 //   stage 1  R[y][f] = sum_x A[y][x] TX[f][x]          (M = 128 y, N = BN f, K = 128 x)
@@ -166,18 +104,8 @@ __device__ __forceinline__ void bulk_tile(uint32_t dst, const uint8_t* src, uint
 // and with sym the conjugate rows -r come from the same Q:
 //   Re = Q[2r][2c] + Q[2r+1][2c+1],  Im = Q[2r][2c+1] - Q[2r+1][2c].
 // Output: part[row][c][tile] (row = r, or r + nr - 1 for +r / nr - 1 - r for -r with sym).
-struct Tc2Analysis {
-  const float* in;
-  float* mask_out;
-  int* flag;
-  int N, mode, vec4;
-  int ncols;           // complex band columns (BN >= 2 ncols)
-  int nrows_out, nr, sym;
-  float2* part;
-};
 
 constexpr int A2_NT = 256;
-constexpr uint32_t A2_A_BYTES = s2_tile_bytes(128, 128);   // 64 KiB
 
 // Stages 1 and 2 of a tile analysis and the tile's partial, for a CTA whose 256
 // threads have written the [hi | lo] image tile into sA (64 KiB) and whose thread

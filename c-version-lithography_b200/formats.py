@@ -4,6 +4,7 @@
   (source/utils/save_txt.cpp:23-105): whitespace-separated text matrices with a
   ``# rows=R cols=C`` header; ``load_txt`` skips blank and ``#`` lines and requires a
   constant column count.
+* :func:`load_target_image` - the demos' target bitmap load (cv::imread grayscale / 255).
 * :func:`binarize`, :func:`binarize_otsu` - ``Imbinarize::binarize`` /
   ``binarize_OTSU`` (source/utils/imbinarize.cpp:12-37): the gray CTM mask scaled to
   8 bits and thresholded with OpenCV's adaptive Gaussian or Otsu threshold, the
@@ -70,6 +71,17 @@ def load_txt(path: str) -> np.ndarray:
     if not rows:
         raise ValueError(f"load_txt: empty matrix in {path}")
     return np.array(rows, dtype=np.float64)
+
+
+def load_target_image(path: str) -> np.ndarray:
+    """A target bitmap as the demos read it (demo/demo_full_chip_ctm.cpp:62-66,
+    demo/demo_full_chip_lsm.cpp:93-97): cv::imread(IMREAD_GRAYSCALE), then each 8-bit
+    pixel / 255 as float64."""
+    import cv2
+    img = cv2.imread(path, cv2.IMREAD_GRAYSCALE)
+    if img is None:
+        raise ValueError(f"load_target_image: cannot read {path}")
+    return img.astype(np.float64) / 255.0
 
 
 def _gray_u8(gray_mask):

@@ -46,6 +46,12 @@ extern "C" {
                                         tensor cores in split BF16 (hi*hi + hi*lo + lo*hi,
                                         FP32 accumulation) */
 
+#define LITHO_TC_SCHEDULE_AUTO 0       /* persistent where the band fits its shared-memory
+                                          plan, else per tile (the default) */
+#define LITHO_TC_SCHEDULE_PER_TILE 1   /* one CTA per 128 x 128 tile, phases in order */
+#define LITHO_TC_SCHEDULE_PERSISTENT 2 /* one CTA per SM over a share of the (image, tile)
+                                          items, warp-specialised and pipelined */
+
 typedef struct litho_ctx litho_ctx;
 typedef struct litho_cache litho_cache;
 typedef struct litho_field litho_field;
@@ -69,6 +75,11 @@ long long litho_ctx_launch_count(const litho_ctx* ctx);
  * when the context's stream is itself being captured by the caller, or under
  * tools that cannot follow a stream capture. */
 int litho_ctx_enable_graphs(litho_ctx* ctx, int on);
+/* Schedule of the split-BF16 tensor-core passes (LITHO_TC_SCHEDULE_*). The schedules
+ * compute the same products per pixel; the loss and norm partial sums are added in
+ * another order, so they may differ in their last bits. This choice has no
+ * counterpart in the reference (whose passes are FFTs on the CPU). */
+int litho_ctx_set_tc_schedule(litho_ctx* ctx, int schedule);
 
 /* Per-stage device timing with CUDA events on the context's stream. Stages:
  * 0 tile analysis of the mask (row DFT + column contraction per 128 x 128 tile),
@@ -80,6 +91,40 @@ int litho_ctx_enable_graphs(litho_ctx* ctx, int on);
 #define LITHO_NUM_STAGES 9
 int litho_ctx_enable_stage_timing(litho_ctx* ctx, int on);
 int litho_ctx_stage_times(const litho_ctx* ctx, double* ms, long long* counts);
+
+/* ------------------------------------------------------------ optical set-up
+ * litho_socs_prepare replaces LithoPrepare's SOCS path (source/litho_model/
+ * litho_prepare.cpp:16-385 with grid.cpp:27,38-48, pupil.cpp:14-46, zernike.cpp:12-56
+ * and source.cpp:114-158): from the optics it builds, in FP64, the annular source map
+ * and its points, the shifted-pupil matrix A = [sqrt(w_s) P(f + f_s)] over the SOCS
+ * support, and the K strongest coherent modes of A (eigenvalues sigma_k^2), then
+ * creates the device cache from them (as litho_cache_create_band). The kernels equal
+ * the reference's up to a phase per kernel (and a basis within each degenerate
+ * eigenvalue), which the image does not depend on when K keeps whole degenerate groups.
+ * info (nullable) receives the sizes; eigenvalues (nullable, K doubles) and
+ * band_kernels (nullable, K x Nr x Nc interleaved complex doubles, band row r at integer
+ * frequency row0 + r) receive the kernels; size them from a first call with info only
+ * and num_socs fixed, or generously (K <= number of source points). */
+typedef struct litho_socs_params {
+  int N;                  /* optical grid (pixels per side) */
+  double pixel_nm;        /* pixel size */
+  double wavelength_nm;
+  double na;
+  double sigma_in, sigma_out; /* annulus, normalised to NA / lambda */
+  double smoothing;       /* source edge width (0: hard edges, the reference's default) */
+  int upsample;           /* source oversampling per axis (<= 0: 10, the reference's) */
+  int num_socs;           /* kernels kept (<= 0: all source points; the reference keeps 36) */
+  int compact;            /* 1: support cropped to the shifted pupils (compact_socs) */
+  const double* zernike;  /* nullable: Fringe coefficients Z1..Z11 (11 doubles, waves) */
+} litho_socs_params;
+typedef struct litho_socs_info {
+  int K, Ns;              /* kernels kept, source points */
+  int Nr, Nc, row0, col0; /* band of the kernels (integer frequencies row0.., col0..) */
+  double ws_sum;          /* sum of the source weights (the image normaliser) */
+  double energy_captured; /* kept eigenvalues / all eigenvalues */
+} litho_socs_info;
+int litho_socs_prepare(litho_ctx* ctx, const litho_socs_params* params, litho_cache** out,
+                       litho_socs_info* info, double* eigenvalues, double* band_kernels);
 
 /* ------------------------------------------------------------ optical cache
  * Replaces ImagingCache (include/litho_model/litho_prepare.h:18-47) as consumed

@@ -58,3 +58,56 @@ def test_no_device_calls_fail_cleanly(pkg):
     h = ctypes.c_void_p()
     assert lib.litho_ctx_create(0, None, ctypes.byref(h)) != 0
     assert not h.value
+
+
+def declared_prototypes():
+    """{name: (return type, [parameter types])} of every function the header declares."""
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    text = re.sub(r"#[^\n]*", "", text)
+    protos = {}
+    for m in re.finditer(r"([A-Za-z_][\w\s\*]*?)\b(litho_[a-z0-9_]+)\s*\(([^)]*)\)\s*;", text):
+        ret = " ".join(m.group(1).split())
+        params = [p.strip() for p in m.group(3).split(",")] if m.group(3).strip() != "void" else []
+        types = []
+        for p in params:
+            p = " ".join(p.split())
+            # drop the parameter name (the last identifier) unless the type is all there is
+            t = re.sub(r"\s*\b[A-Za-z_]\w*$", "", p) if re.search(r"[\w\*]\s+\**[A-Za-z_]\w*$", p) else p
+            types.append(t.replace(" *", "*").strip())
+        protos[m.group(2)] = (ret.replace(" *", "*"), types)
+    return protos
+
+
+def ctypes_class(c_type):
+    """The ctypes argument class a C parameter type must be bound with."""
+    import ctypes as C
+    t = c_type.replace("const ", "").strip()
+    if t.endswith("*"):
+        base = t[:-1].strip()
+        return {"double": C.POINTER(C.c_double), "int": C.POINTER(C.c_int),
+                "long long": C.POINTER(C.c_longlong), "char": C.c_char_p}.get(base, "pointer")
+    return {"int": C.c_int, "double": C.c_double, "long long": C.c_longlong,
+            "size_t": C.c_size_t, "float": C.c_float}[t]
+
+
+def test_binding_signatures_match_the_header(pkg):
+    """Every ctypes binding has the header's parameter count, and each parameter the
+    class its C type needs: int / long long / double by value, double* and int* as typed
+    pointers, any other pointer (handles, float buffers, streams, structs) as a pointer."""
+    import ctypes as C
+    protos = declared_prototypes()
+    assert sorted(protos) == declared_functions()
+    pointer_like = (C.c_void_p, C.c_char_p)
+    for name, (res, args) in pkg.SIGNATURES.items():
+        ret, params = protos[name]
+        assert len(args) == len(params), (name, params, args)
+        want_ret = ctypes_class(ret)
+        assert (res is want_ret) or (want_ret == "pointer" and res in pointer_like), (name, ret, res)
+        for i, (p, a) in enumerate(zip(params, args)):
+            want = ctypes_class(p)
+            if want == "pointer":
+                ok = a in pointer_like or (isinstance(a, type) and issubclass(a, C._Pointer))
+            else:
+                ok = a is want
+            assert ok, (name, i, p, a)
