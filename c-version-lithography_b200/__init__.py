@@ -112,6 +112,10 @@ SIGNATURES = {
     "litho_cache_create_dense": (_I, [_P, _I, _I, _PD, _PD, _D, _PP]),
     "litho_cache_create_band": (_I, [_P, _I, _I, _I, _I, _I, _I, _PD, _PD, _D, _PP]),
     "litho_socs_prepare": (_I, [_P, _P, _PP, _P, _PD, _PD]),
+    "litho_pe_gradient_batch_device": (_I, [_P, _P, _I, _P, _P, _D, _D, _D, _P, _P]),
+    "litho_lsm_rk2_update_batch_device": (_I, [_P, _I, _I, _I, _P, _P, _D, _D, _D, _D, _P, _P, _P]),
+    "litho_lsm_track_batch": (_I, [_P, _I, ctypes.c_longlong, _P, _D, _P, _P, _P, _P, _I, _P]),
+    "litho_ctx_deferred_status": (_I, [_P]),
     "litho_cache_info": (_I, [_P, _PI, _PI, _PI, _PI, _PI, _PI]),
     "litho_cache_destroy": (_I, [_P]),
     "litho_field_create": (_I, [_P, _P, _PP]),

@@ -126,6 +126,18 @@ int Context::ensure_scratch(size_t bytes) {
   return LITHO_OK;
 }
 
+int Context::ensure_deferred() {
+  if (d_deferred) return LITHO_OK;
+  if (cudaMalloc(&d_deferred, 2 * sizeof(int)) != cudaSuccess) {
+    cudaGetLastError();
+    d_deferred = nullptr;
+    return fail(LITHO_ERR_OOM, "deferred status allocation failed");
+  }
+  if (cudaMemsetAsync(d_deferred, 0, 2 * sizeof(int), stream) != cudaSuccess)
+    return fail(LITHO_ERR_CUDA, "deferred status");
+  return LITHO_OK;
+}
+
 int Context::ensure_red(size_t n) {
   if (red_cap >= n) return LITHO_OK;
   if (d_red) {
@@ -215,6 +227,7 @@ int litho_ctx_destroy(litho_ctx* ctx) {
   cudaStreamSynchronize(ctx->stream);
   if (ctx->scratch.base) cudaFree(ctx->scratch.base);
   if (ctx->d_red) cudaFree(ctx->d_red);
+  if (ctx->d_deferred) cudaFree(ctx->d_deferred);
   if (ctx->h_red) cudaFreeHost(ctx->h_red);
   if (ctx->host_stage.base) cudaFree(ctx->host_stage.base);
   if (ctx->eval_graph) cudaGraphExecDestroy(ctx->eval_graph);
@@ -749,6 +762,62 @@ int fetch(Context* ctx, int n) {
   return LITHO_OK;
 }
 
+int* flag_word(const Context* ctx) { return reinterpret_cast<int*>(ctx->d_red + RED_FLAG); }
+
+// deferred[0] |= the call's non-finite flag; deferred[1] keeps the first wait code.
+__global__ void merge_deferred_kernel(const int* __restrict__ flag, int* __restrict__ deferred) {
+  if (threadIdx.x == 0) {
+    if (flag[0]) deferred[0] = 1;
+    if (flag[1] && !deferred[1]) deferred[1] = flag[1];
+  }
+}
+cudaError_t launch_merge_deferred(cudaStream_t s, const int* flag, int* deferred) {
+  merge_deferred_kernel<<<1, 32, 0, s>>>(flag, deferred);
+  return cudaGetLastError();
+}
+
+// dts[i] = the step of image i ((max |Vn|, dt) float pairs).
+__global__ void dt_export_kernel(const float* __restrict__ vd, int batch, double* __restrict__ dts) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < batch) dts[i] = vd[2 * i + 1];
+}
+
+// Per image b: tracked loss l = losses[2b] + pen_weight losses[2b + 1]; history[b][iters[b]]
+// = l when there is a column for it; iters[b] += 1; improved[b] = l < best[b], and then
+// best[b] = l.
+__global__ void track_scalars_kernel(int batch, const double* __restrict__ losses, double pen_weight,
+                                     double* __restrict__ best, double* __restrict__ history,
+                                     int history_cols, int* __restrict__ iters,
+                                     int* __restrict__ improved) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= batch) return;
+  const double l = losses[2 * b] + pen_weight * losses[2 * b + 1];
+  const int it = iters[b];
+  if (history && it >= 0 && it < history_cols) history[(size_t)b * history_cols + it] = l;
+  iters[b] = it + 1;
+  const int up = l < best[b];
+  improved[b] = up;
+  if (up) best[b] = l;
+}
+// best_masks[b] = masks[b] where improved[b]; vec: n % 4 == 0 and both bases 16-byte
+// aligned, so every image's float4 view is aligned.
+__global__ void track_masks_kernel(long long n, int vec, const int* __restrict__ improved,
+                                   const float* __restrict__ masks, float* __restrict__ best_masks) {
+  const int b = blockIdx.y;
+  if (!improved[b]) return;
+  const float* src = masks + (size_t)b * n;
+  float* dst = best_masks + (size_t)b * n;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  const long long i0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (vec) {
+    const float4* s4 = reinterpret_cast<const float4*>(src);
+    float4* d4 = reinterpret_cast<float4*>(dst);
+    for (long long i = i0; i < n / 4; i += stride) d4[i] = s4[i];
+  } else {
+    for (long long i = i0; i < n; i += stride) dst[i] = src[i];
+  }
+}
+
 bool flag_set(const Context* ctx) {
   int v;
   std::memcpy(&v, ctx->h_red + RED_FLAG, sizeof(int));
@@ -1090,9 +1159,14 @@ int litho_ctm_evaluate_batch(litho_ctx* ctx, const litho_cache* cache, int batch
   return LITHO_OK;
 }
 
-int litho_pe_gradient_batch(litho_ctx* ctx, const litho_cache* cache, int batch,
-                            const float* d_masks, const float* d_targets, double threshold,
-                            double alpha, float* d_grad_masks, double* losses) {
+// Batched imaging + PE + dPE/dM. losses (host, nullable): PE per image, after a host
+// round trip. d_losses (device, nullable): {PE, background-penalty term} per image with
+// no host round trip (pen_term also sums that term at threshold pen_thr; a non-finite
+// input goes to the deferred status).
+static int pe_gradient_batch_impl(litho_ctx* ctx, const litho_cache* cache, int batch,
+                                  const float* d_masks, const float* d_targets, double threshold,
+                                  double alpha, float* d_grad_masks, double* losses,
+                                  double* d_losses, bool pen_term, double pen_thr) {
   if (!ctx || !cache || batch < 1 || !d_masks || !d_targets || !d_grad_masks)
     return LITHO_ERR_INVALID_ARGUMENT;
   if (!std::isfinite(threshold) || !std::isfinite(alpha))
@@ -1113,10 +1187,16 @@ int litho_pe_gradient_batch(litho_ctx* ctx, const litho_cache* cache, int batch,
   ep.alpha = (float)alpha;
   ep.pe_weight = 1.f;
   ep.penalty = 0.f;
-  ep.pen_thr = 0.01f;
+  ep.pen_thr = (float)pen_thr;
+  ep.loss_penalty_term = pen_term ? 1 : 0;
   ep.loss_partial = ctx->d_red + RED_PART;
   GradEpilogue gp{};
   cudaStream_t s = ctx->stream;
+  const bool device_out = d_losses != nullptr;
+  if (device_out) {
+    st = ctx->ensure_deferred();
+    if (st) return st;
+  }
   if (tc) {
     // Every image in one pass: the resist synthesis runs the adjoint tile analysis.
     ep.target = d_targets;
@@ -1130,6 +1210,14 @@ int litho_pe_gradient_batch(litho_ctx* ctx, const litho_cache* cache, int batch,
                                                        ctx->d_red + RED_PART, 0, 0, d_sums, batch),
                         "sum");
     ctx->launches += 1;
+    if (device_out) {
+      if (!st)
+        LITHO_CUDA_TRY(ctx, cudaMemcpyAsync(d_losses, d_sums, 2 * (size_t)batch * sizeof(double),
+                                            cudaMemcpyDeviceToDevice, s));
+      if (!st) st = check_launch(ctx, launch_merge_deferred(s, flag_word(ctx), ctx->d_deferred),
+                                 "deferred status");
+      return st;
+    }
     std::vector<double> sums(2 * (size_t)batch);
     if (!st)
       LITHO_CUDA_TRY(ctx, cudaMemcpyAsync(sums.data(), d_sums, sums.size() * sizeof(double),
@@ -1154,12 +1242,40 @@ int litho_pe_gradient_batch(litho_ctx* ctx, const litho_cache* cache, int batch,
                         "sum");
     ctx->launches += 1;
     if (!st) st = run_adjoint(ctx, *cache, f, L, at<float>(ctx, L.dldi), 4.0 * alpha, gp, &nb2);
+    if (device_out) {
+      if (!st)
+        LITHO_CUDA_TRY(ctx, cudaMemcpyAsync(d_losses + 2 * (size_t)b, ctx->d_red + RED_SUM,
+                                            2 * sizeof(double), cudaMemcpyDeviceToDevice, s));
+      if (st) return st;
+      continue;
+    }
     if (!st) st = fetch(ctx, 2);
     if (st) return st;
     if (flag_set(ctx)) return ctx->fail(LITHO_ERR_NONFINITE, "mask must be finite");
     if (losses) losses[b] = ctx->h_red[RED_SUM];
   }
+  if (device_out)
+    return check_launch(ctx, launch_merge_deferred(s, flag_word(ctx), ctx->d_deferred),
+                        "deferred status");
   return LITHO_OK;
+}
+
+int litho_pe_gradient_batch(litho_ctx* ctx, const litho_cache* cache, int batch,
+                            const float* d_masks, const float* d_targets, double threshold,
+                            double alpha, float* d_grad_masks, double* losses) {
+  return pe_gradient_batch_impl(ctx, cache, batch, d_masks, d_targets, threshold, alpha,
+                                d_grad_masks, losses, nullptr, false, 0.01);
+}
+
+int litho_pe_gradient_batch_device(litho_ctx* ctx, const litho_cache* cache, int batch,
+                                   const float* d_masks, const float* d_targets, double threshold,
+                                   double alpha, double penalty_threshold, float* d_grad_masks,
+                                   double* d_losses) {
+  if (!ctx || !d_losses) return LITHO_ERR_INVALID_ARGUMENT;
+  if (!std::isfinite(penalty_threshold))
+    return ctx->fail(LITHO_ERR_NONFINITE, "penalty threshold must be finite");
+  return pe_gradient_batch_impl(ctx, cache, batch, d_masks, d_targets, threshold, alpha,
+                                d_grad_masks, nullptr, d_losses, true, penalty_threshold);
 }
 
 // Host buffers: theta goes up first on the context's stream; the target follows on
@@ -1462,6 +1578,7 @@ int litho_ctx_reserve(litho_ctx* ctx, const litho_cache* cache, int batch) {
   if (st) return st;
   st = ctx->ensure_red(RED_PART + ((size_t)batch * dt_batch_blocks(n, batch) + 1) / 2 + 8 +
                        (size_t)batch + 8);
+  if (!st) st = ctx->ensure_deferred();
   if (st) return st;
   LITHO_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
   return LITHO_OK;
@@ -1647,7 +1764,6 @@ int litho_reinit_sdf_batch(litho_ctx* ctx, int batch, int rows, int cols, const 
                         "mask");
     ctx->launches += d_mask ? 2 : 1;
   }
-  if (!st) LITHO_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
   return st;
 }
 
@@ -1683,12 +1799,14 @@ int litho_lsm_rk2_update(litho_ctx* ctx, int rows, int cols, const float* d_phi,
   return LITHO_OK;
 }
 
-int litho_lsm_rk2_update_batch(litho_ctx* ctx, int batch, int rows, int cols, const float* d_phi,
-                               const float* d_vn, double dx, double dy, double cfl, double b,
-                               float* d_phi_out, float* d_mask, double* dts) {
+static int rk2_update_batch_impl(litho_ctx* ctx, int batch, int rows, int cols,
+                                 const float* d_phi, const float* d_vn, double dx, double dy,
+                                 double cfl, double b, float* d_phi_out, float* d_mask,
+                                 double* dts, bool device_out, double* d_dts) {
   if (!ctx || batch < 1 || !d_phi || !d_vn || !d_phi_out) return LITHO_ERR_INVALID_ARGUMENT;
   if (d_phi_out == d_phi) return ctx->fail(LITHO_ERR_INVALID_ARGUMENT, "phi_out must not alias phi");
   int st = ls_check(ctx, rows, cols, dx, dy, 3);
+  if (!st && device_out) st = ctx->ensure_deferred();
   if (st) return st;
   if (batch > 65535) return ctx->fail(LITHO_ERR_INVALID_ARGUMENT, "at most 65535 images per call");
   const size_t n = (size_t)rows * cols;
@@ -1720,6 +1838,15 @@ int litho_lsm_rk2_update_batch(litho_ctx* ctx, int batch, int rows, int cols, co
                                            batch, nullptr, 2),
                       "rk2 stage 2");
   ctx->launches += 4;
+  if (device_out) {
+    if (!st && d_dts) {
+      dt_export_kernel<<<(batch + 255) / 256, 256, 0, s>>>(vd, batch, d_dts);
+      st = check_launch(ctx, cudaGetLastError(), "dt export");
+      ctx->launches += 1;
+    }
+    if (!st) st = check_launch(ctx, launch_merge_deferred(s, bad, ctx->d_deferred), "deferred status");
+    return st;
+  }
   std::vector<float> h(2 * (size_t)batch);
   if (!st)
     LITHO_CUDA_TRY(ctx, cudaMemcpyAsync(h.data(), vd, h.size() * sizeof(float),
@@ -1728,6 +1855,60 @@ int litho_lsm_rk2_update_batch(litho_ctx* ctx, int batch, int rows, int cols, co
   if (st) return st;
   if (flag_set(ctx)) return ctx->fail(LITHO_ERR_NONFINITE, "normal speed must be finite");
   for (int i = 0; i < batch && dts; ++i) dts[i] = h[2 * (size_t)i + 1];
+  return LITHO_OK;
+}
+
+int litho_lsm_rk2_update_batch(litho_ctx* ctx, int batch, int rows, int cols, const float* d_phi,
+                               const float* d_vn, double dx, double dy, double cfl, double b,
+                               float* d_phi_out, float* d_mask, double* dts) {
+  return rk2_update_batch_impl(ctx, batch, rows, cols, d_phi, d_vn, dx, dy, cfl, b, d_phi_out,
+                               d_mask, dts, false, nullptr);
+}
+
+int litho_lsm_rk2_update_batch_device(litho_ctx* ctx, int batch, int rows, int cols,
+                                      const float* d_phi, const float* d_vn, double dx, double dy,
+                                      double cfl, double b, float* d_phi_out, float* d_mask,
+                                      double* d_dts) {
+  return rk2_update_batch_impl(ctx, batch, rows, cols, d_phi, d_vn, dx, dy, cfl, b, d_phi_out,
+                               d_mask, nullptr, true, d_dts);
+}
+
+int litho_lsm_track_batch(litho_ctx* ctx, int batch, long long n_pixels, const double* d_losses,
+                          double pen_weight, double* d_best, const float* d_masks,
+                          float* d_best_masks, double* d_history, int history_cols, int* d_iters) {
+  if (!ctx || batch < 1 || n_pixels < 1 || !d_losses || !d_best || !d_masks || !d_best_masks ||
+      !d_iters || (d_history && history_cols < 1))
+    return LITHO_ERR_INVALID_ARGUMENT;
+  if (batch > 65535) return ctx->fail(LITHO_ERR_INVALID_ARGUMENT, "at most 65535 images per call");
+  if (cudaSetDevice(ctx->device) != cudaSuccess) return ctx->fail(LITHO_ERR_CUDA, "cudaSetDevice");
+  int st = ctx->ensure_red(RED_PART + (size_t)batch + 8);
+  if (st) return st;
+  int* improved = reinterpret_cast<int*>(ctx->d_red + RED_PART);
+  cudaStream_t s = ctx->stream;
+  track_scalars_kernel<<<(batch + 127) / 128, 128, 0, s>>>(batch, d_losses, pen_weight, d_best,
+                                                            d_history, history_cols, d_iters,
+                                                            improved);
+  const long long blocks = std::min<long long>((n_pixels / 4 + 255) / 256 + 1, 148);
+  const int vec = n_pixels % 4 == 0 && reinterpret_cast<uintptr_t>(d_masks) % 16 == 0 &&
+                  reinterpret_cast<uintptr_t>(d_best_masks) % 16 == 0;
+  track_masks_kernel<<<dim3((unsigned)blocks, batch), 256, 0, s>>>(n_pixels, vec, improved,
+                                                                  d_masks, d_best_masks);
+  ctx->launches += 2;
+  return check_launch(ctx, cudaGetLastError(), "LSM best-state tracking");
+}
+
+int litho_ctx_deferred_status(litho_ctx* ctx) {
+  if (!ctx) return LITHO_ERR_INVALID_ARGUMENT;
+  if (!ctx->d_deferred) return LITHO_OK;
+  int h[2] = {0, 0};
+  LITHO_CUDA_TRY(ctx, cudaMemcpyAsync(h, ctx->d_deferred, sizeof(h), cudaMemcpyDeviceToHost,
+                                      ctx->stream));
+  LITHO_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  LITHO_CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_deferred, 0, sizeof(h), ctx->stream));
+  if (h[1])
+    return ctx->fail(LITHO_ERR_CUDA, "tensor-core pass: a bounded wait expired (code " +
+                                         std::to_string(h[1]) + ")");
+  if (h[0]) return ctx->fail(LITHO_ERR_NONFINITE, "a deferred call saw a non-finite input");
   return LITHO_OK;
 }
 
@@ -1764,6 +1945,8 @@ struct litho_partition {
   // EPs as uploaded (y, x | w) and one tile's candidates (y, x | w), in doubles.
   double* d_ep = nullptr;
   size_t ep_n = 0;
+  void* d_epe_sort = nullptr;   // work of the deterministic dL/dI scatter
+  size_t epe_sort_bytes = 0;
 };
 
 namespace {
@@ -1790,6 +1973,7 @@ void free_partition(litho_partition* p) {
   if (p->d_xpart) cudaFree(p->d_xpart);
   if (p->d_epe_work) cudaFree(p->d_epe_work);
   if (p->d_ep) cudaFree(p->d_ep);
+  if (p->d_epe_sort) cudaFree(p->d_epe_sort);
 }
 
 }  // namespace
@@ -1982,7 +2166,7 @@ int litho_exchange_compute_epe(litho_ctx* ctx, const litho_partition* cp, const 
   const bool guard_region = o.loss_region == LITHO_MICRO_REGION_CORE_GUARD;
   const int periods = guard_region ? 1 : 0;
   const size_t ncand = (size_t)e.n_eps * (2 * periods + 1) * (2 * periods + 1);
-  if (ncand > (size_t)1 << 30)
+  if (ncand > (size_t)1 << 28)   // the sorted scatter takes 4 entries per candidate
     return ctx->fail(LITHO_ERR_INVALID_ARGUMENT, "MicroGradientExchange: too many EPs");
   if (!p->d_work) {
     if (cudaMalloc(&p->d_work, 4 * n * tt * sizeof(float)) != cudaSuccess ||
@@ -2018,6 +2202,17 @@ int litho_exchange_compute_epe(litho_ctx* ctx, const litho_partition* cp, const 
       }
       p->ep_n = ep_n;
     }
+  }
+  const size_t sort_bytes = eval_epe ? epe_scatter_work_bytes((int)ncand) : 0;
+  if (p->epe_sort_bytes < sort_bytes) {
+    LITHO_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    if (p->d_epe_sort) cudaFree(p->d_epe_sort);
+    p->d_epe_sort = nullptr; p->epe_sort_bytes = 0;
+    if (cudaMalloc(&p->d_epe_sort, sort_bytes) != cudaSuccess) {
+      cudaGetLastError();
+      return ctx->fail(LITHO_ERR_OOM, "full-chip EPE scatter allocation failed");
+    }
+    p->epe_sort_bytes = sort_bytes;
   }
   const BandGeom& g = cache->g;
   const size_t fe_n = (size_t)g.K * g.Pr * g.Pc, fm_n = (size_t)g.Nr * g.Nc;
@@ -2120,7 +2315,8 @@ int litho_exchange_compute_epe(litho_ctx* ctx, const litho_partition* cp, const 
       if (!r)
         r = check_launch(ctx, launch_epe(s, aer, ts, ts, cand, cand + 2 * ncand, (int)ncand,
                                          threshold, e.epe_pixel_size, nullptr, part,
-                                         epe_grad ? dl : nullptr, epe_fac, &used),
+                                         epe_grad ? dl : nullptr, epe_fac, &used, p->d_epe_sort,
+                                         p->epe_sort_bytes),
                          "sparse EPE");
       if (!r) r = check_launch(ctx, launch_sum_partials(s, part, used, 3, slot + 2), "sum");
       ctx->launches += 3;
@@ -2545,6 +2741,7 @@ int litho_epe_gradient(litho_ctx* ctx, const litho_field* field, const float* d_
                        float* d_grad) {
   if (!ctx || !field || !d_aerial || !d_grad || n_eps < 0 || (n_eps > 0 && (!eps || !weights)))
     return LITHO_ERR_INVALID_ARGUMENT;
+  if (n_eps > (1 << 28)) return ctx->fail(LITHO_ERR_INVALID_ARGUMENT, "epe_gradient: too many EPs");
   if (!field->valid) return ctx->fail(LITHO_ERR_NOT_READY, "Gradient: field not computed");
   if (!std::isfinite(threshold))
     return ctx->fail(LITHO_ERR_NONFINITE, "epe_gradient: threshold must be finite");
@@ -2556,7 +2753,9 @@ int litho_epe_gradient(litho_ctx* ctx, const litho_field* field, const float* d_
   if (st) return st;
   const int n = n_eps;
   const size_t ep_off = align_up(L.total, 256);
-  st = ctx->ensure_scratch(ep_off + (size_t)(3 * n + 4) * sizeof(double));
+  const size_t sort_off = align_up(ep_off + (size_t)(3 * n + 4) * sizeof(double), 256);
+  const size_t sort_bytes = epe_scatter_work_bytes(n);
+  st = ctx->ensure_scratch(sort_off + sort_bytes);
   if (st) return st;
   const int nb = n == 0 ? 1 : (n + 255) / 256;
   st = ctx->ensure_red(RED_PART + 3 * (size_t)nb + 8);
@@ -2573,9 +2772,10 @@ int litho_epe_gradient(litho_ctx* ctx, const litho_field* field, const float* d_
   }
   int used = 0;
   st = check_launch(ctx, launch_epe(s, d_aerial, N, N, d_eps, d_w, n, threshold, 1.0, nullptr,
-                                    ctx->d_red + RED_PART, dldi, 1.0, &used),
+                                    ctx->d_red + RED_PART, dldi, 1.0, &used,
+                                    at<void>(ctx, sort_off), sort_bytes),
                     "sparse EPE scatter");
-  ctx->launches += 1;
+  ctx->launches += n > 0 ? 3 : 1;   // EPE, sort, per-pixel sums
   if (st) return st;
   // dL/dI already holds the 2 of the squared EPE; |E|^2 gives another 2 (gradient.cpp:225-226).
   GradEpilogue ep{};

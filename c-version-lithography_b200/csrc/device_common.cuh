@@ -102,7 +102,7 @@ struct ResistEpiT {
     const float r = W - T;
     pe += FAST ? (double)(r * r * pw) : (double)r * (double)r * (double)pw;
     float s = p.pe_weight * r * pw;
-    if (p.penalty != 0.f && T < 0.5f) {
+    if ((p.penalty != 0.f || p.loss_penalty_term) && T < 0.5f) {
       const float ex = fmaxf(W - p.pen_thr, 0.f);
       pen += FAST ? (double)(ex * ex * qw) : (double)ex * (double)ex * (double)qw;
       s += p.penalty * ex * qw;
@@ -166,7 +166,8 @@ struct ResistEpiT {
     return g;
   }
   __host__ __device__ bool plain() const {
-    return p.pe_window == nullptr && p.pen_window == nullptr && p.penalty == 0.f;
+    return p.pe_window == nullptr && p.pen_window == nullptr && p.penalty == 0.f &&
+           !p.loss_penalty_term;
   }
   // All EPI_NT threads of the CTA must call finish.
   __device__ __forceinline__ void finish() {

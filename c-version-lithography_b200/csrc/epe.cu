@@ -2,8 +2,13 @@
 // (source/utils/loss.cpp:125-163) and the dL/dI of Gradient::epe_gradient
 // (source/utils/gradient.cpp:198-227). EP selection stays on the host; the points
 // (subpixel (y, x)) and weights arrive per call. One thread per EP, FP64 arithmetic
-// on the FP32 aerial image.
+// on the FP32 aerial image. The dL/dI scatter is deterministic: every EP emits its
+// stencil's (pixel, value) pairs, a stable radix sort groups them by pixel with the EP
+// order kept, and each pixel's contributions are added in FP64 in that order, as the
+// reference's serial loop adds them into its double-precision dL/dI.
 #include <cuda_runtime.h>
+
+#include <cub/cub.cuh>
 
 #include "device_common.cuh"
 
@@ -58,13 +63,15 @@ __device__ __forceinline__ double sample(const Stencil& s, F f) {
 
 // eps: n x 2 (y, x); w: n weights. Per EP: signed EPE (pixels; NaN when inactive) and,
 // per CTA, FP64 partial sums (weighted squared loss, |EPE| nm, active count). With
-// dldi set, scatter_scale x 2 w (I - thr) / G^2 is added onto its stencil (float atomics).
+// keys set, EP i writes its stencil's contributions scatter_scale x 2 w (I - thr) / G^2
+// x weight to keys / vals [4 i .. 4 i + 3] (pixel index, or NO_PIXEL for an empty slot).
 constexpr int EPE_NT = 256;
+constexpr uint32_t NO_PIXEL = 0xFFFFFFFFu;
 __global__ void __launch_bounds__(EPE_NT)
 epe_kernel(const float* __restrict__ I, int rows, int cols, const double* __restrict__ eps,
            const double* __restrict__ w, int n, double thr, double pixel_nm,
-           double* __restrict__ signed_epe, double* __restrict__ partial, float* __restrict__ dldi,
-           double scatter_scale) {
+           double* __restrict__ signed_epe, double* __restrict__ partial,
+           uint32_t* __restrict__ keys, double* __restrict__ vals, double scatter_scale) {
   pdl_trigger();
   pdl_wait();
   __shared__ double sh[EPE_NT / 32];
@@ -73,6 +80,8 @@ epe_kernel(const float* __restrict__ I, int rows, int cols, const double* __rest
   if (i < n) {
     const double wi = w[i];
     double se = nan("");
+    if (keys)
+      for (int c = 0; c < 4; ++c) keys[4 * (size_t)i + c] = NO_PIXEL;
     if (wi > 0.0) {
       const Stencil s = make_stencil(rows, cols, eps[2 * i], eps[2 * i + 1]);
       const double a = sample(s, [&](int y, int x) { return (double)__ldg(I + (size_t)y * cols + x); });
@@ -81,14 +90,19 @@ epe_kernel(const float* __restrict__ I, int rows, int cols, const double* __rest
       loss = wi * se * se;
       absn = fabs(se) * pixel_nm;
       active = 1.0;
-      if (dldi) {
+      if (keys) {
+        // bilinear_scatter (epe_utils.cpp:76-80): the stencil's corners in the reference's
+        // order; a repeated edge pixel appears twice with its partner's weight 0, and
+        // zero-weight slots stay empty
         const double g = scatter_scale * (2.0 * wi * (a - thr) / (m * m));
-        const double wa = (1.0 - s.wy1) * (1.0 - s.wx1), wb = (1.0 - s.wy1) * s.wx1;
-        const double wc = s.wy1 * (1.0 - s.wx1), wd = s.wy1 * s.wx1;
-        if (wa > 0.0) atomicAdd(dldi + (size_t)s.y0 * cols + s.x0, (float)(wa * g));
-        if (wb > 0.0) atomicAdd(dldi + (size_t)s.y0 * cols + s.x1, (float)(wb * g));
-        if (wc > 0.0) atomicAdd(dldi + (size_t)s.y1 * cols + s.x0, (float)(wc * g));
-        if (wd > 0.0) atomicAdd(dldi + (size_t)s.y1 * cols + s.x1, (float)(wd * g));
+        const double wt[4] = {(1.0 - s.wy1) * (1.0 - s.wx1), (1.0 - s.wy1) * s.wx1,
+                              s.wy1 * (1.0 - s.wx1), s.wy1 * s.wx1};
+        const int py[4] = {s.y0, s.y0, s.y1, s.y1}, px[4] = {s.x0, s.x1, s.x0, s.x1};
+        for (int c = 0; c < 4; ++c)
+          if (wt[c] > 0.0) {
+            keys[4 * (size_t)i + c] = (uint32_t)py[c] * (uint32_t)cols + (uint32_t)px[c];
+            vals[4 * (size_t)i + c] = wt[c] * g;
+          }
       }
     }
     if (signed_epe) signed_epe[i] = se;
@@ -103,13 +117,75 @@ epe_kernel(const float* __restrict__ I, int rows, int cols, const double* __rest
   }
 }
 
+// The sorted contributions of pixel keys[t] summed in order by the first entry of its
+// run (each pixel written by one thread) and added to dldi once.
+__global__ void epe_runs_kernel(const uint32_t* __restrict__ keys, const double* __restrict__ vals,
+                                int m, uint32_t npix, float* __restrict__ dldi) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= m) return;
+  const uint32_t k = keys[t];
+  if (k >= npix || (t > 0 && keys[t - 1] == k)) return;
+  double sum = 0.0;
+  for (int u = t; u < m && keys[u] == k; ++u) sum += vals[u];
+  dldi[k] += (float)sum;
+}
+
+namespace {
+struct ScatterWork {
+  uint32_t *k_in, *k_out;
+  double *v_in, *v_out;
+  void* temp;
+  size_t temp_bytes, total;
+};
+size_t align256(size_t v) { return (v + 255) / 256 * 256; }
+ScatterWork scatter_layout(int n, void* base) {
+  ScatterWork w{};
+  const size_t m = 4 * (size_t)(n > 0 ? n : 1);
+  cub::DeviceRadixSort::SortPairs(nullptr, w.temp_bytes, (uint32_t*)nullptr, (uint32_t*)nullptr,
+                                  (double*)nullptr, (double*)nullptr, (int)m);
+  char* p = static_cast<char*>(base);
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    const size_t o = off;
+    off = align256(off + bytes);
+    return p ? p + o : nullptr;
+  };
+  w.k_in = reinterpret_cast<uint32_t*>(take(m * sizeof(uint32_t)));
+  w.k_out = reinterpret_cast<uint32_t*>(take(m * sizeof(uint32_t)));
+  w.v_in = reinterpret_cast<double*>(take(m * sizeof(double)));
+  w.v_out = reinterpret_cast<double*>(take(m * sizeof(double)));
+  w.temp = take(w.temp_bytes);
+  w.total = off;
+  return w;
+}
+}  // namespace
+
+size_t epe_scatter_work_bytes(int n) { return scatter_layout(n, nullptr).total; }
+
 cudaError_t launch_epe(cudaStream_t s, const float* I, int rows, int cols, const double* eps,
                        const double* w, int n, double thr, double pixel_nm, double* signed_epe,
-                       double* partial, float* dldi, double scatter_scale, int* nblocks) {
+                       double* partial, float* dldi, double scatter_scale, int* nblocks,
+                       void* work, size_t work_bytes) {
   *nblocks = (n + EPE_NT - 1) / EPE_NT;
   if (*nblocks == 0) *nblocks = 1;
-  return launch_pdl(epe_kernel, dim3(*nblocks), dim3(EPE_NT), 0, s, I, rows, cols, eps, w, n, thr,
-                    pixel_nm, signed_epe, partial, dldi, scatter_scale);
+  ScatterWork sw{};
+  const bool scatter = dldi && n > 0;
+  if (scatter) {
+    sw = scatter_layout(n, work);
+    if (!work || work_bytes < sw.total) return cudaErrorInvalidValue;
+  }
+  cudaError_t e = launch_pdl(epe_kernel, dim3(*nblocks), dim3(EPE_NT), 0, s, I, rows, cols, eps, w,
+                             n, thr, pixel_nm, signed_epe, partial, scatter ? sw.k_in : nullptr,
+                             scatter ? sw.v_in : nullptr, scatter_scale);
+  if (e != cudaSuccess || !scatter) return e;
+  const int m = 4 * n;
+  size_t tb = sw.temp_bytes;
+  e = cub::DeviceRadixSort::SortPairs(sw.temp, tb, sw.k_in, sw.k_out, sw.v_in, sw.v_out, m, 0,
+                                      32, s);
+  if (e != cudaSuccess) return e;
+  epe_runs_kernel<<<(m + 255) / 256, 256, 0, s>>>(sw.k_out, sw.v_out, m,
+                                                  (uint32_t)rows * (uint32_t)cols, dldi);
+  return cudaGetLastError();
 }
 
 }  // namespace litho_b200

@@ -130,6 +130,10 @@ struct Context {
   bool eval_last_valid = false;
   long long eval_graph_launches = 0;
   double* d_red = nullptr;       // FP64 reduction partials
+  // Deferred status of the device-resident entry points ([0] a non-finite input was
+  // seen, [1] the first tensor-core wait code), read by litho_ctx_deferred_status.
+  int* d_deferred = nullptr;
+  int ensure_deferred();
   size_t red_cap = 0;
   double* h_red = nullptr;       // pinned host mirror for results
   std::string last_error;
@@ -235,6 +239,10 @@ struct ResistEpilogue {
   float pe_weight, penalty, pen_thr;
   float* dldi;              // mode 1
   double* loss_partial;     // mode 1: per-block (pe, penalty) FP64 partial sums
+  // mode 1: sum the background-penalty term (threshold pen_thr) into the loss partials
+  // even when penalty is 0 (it then adds nothing to dL/dI), for the loss the
+  // reference's LSM loop tracks (LSM_Optimizer.cpp:87-90).
+  int loss_penalty_term;
 };
 struct GradEpilogue {
   float* grad_mask;         // nullable
@@ -358,9 +366,16 @@ cudaError_t launch_dt_batch(cudaStream_t s, const float* vn, size_t n, int nimg,
 // device FP64. signed_epe (nullable) per point; partial: 3 FP64 sums per block
 // (weighted squared loss, |EPE| nm, active count); dldi (nullable): scatter of
 // 2 w (I - thr) / G^2 onto each point's bilinear stencil (atomic adds).
+// With dldi set, each EP's dL/dI (scatter_scale x 2 w (I - thr) / G^2) is added onto its
+// bilinear stencil deterministically: the (pixel, weighted value) pairs of all EPs are
+// sorted by pixel with a stable radix sort (EP order kept within a pixel) and each
+// pixel's run is summed in FP64 in that order, then added to dldi once. That needs
+// `work` of at least epe_scatter_work_bytes(n) bytes (device, 256-byte aligned).
+size_t epe_scatter_work_bytes(int n);
 cudaError_t launch_epe(cudaStream_t s, const float* I, int rows, int cols, const double* eps,
                        const double* w, int n, double thr, double pixel_nm, double* signed_epe,
-                       double* partial, float* dldi, double scatter_scale, int* nblocks);
+                       double* partial, float* dldi, double scatter_scale, int* nblocks,
+                       void* work = nullptr, size_t work_bytes = 0);
 
 // Full-chip micro tiles (fullchip.cu). Rects are 4 ints (y0, y1, x0, x1) per tile;
 // origins 2 ints (y, x) per tile; rel holds max_rel entries of FC_REL_INTS ints

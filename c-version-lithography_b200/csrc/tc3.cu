@@ -456,7 +456,7 @@ struct S3Resist {
     const float qw = p.pen_window ? __ldg(p.pen_window + i) : pw;
     pe += r * r * pw;
     float s = p.pe_weight * r * pw;
-    if (p.penalty != 0.f && T < 0.5f) {
+    if ((p.penalty != 0.f || p.loss_penalty_term) && T < 0.5f) {
       const float ex = fmaxf(W - p.pen_thr, 0.f);
       pen += ex * ex * qw;
       s += p.penalty * ex * qw;
@@ -464,7 +464,8 @@ struct S3Resist {
     return s * W * (1.f - W);
   }
   __device__ __forceinline__ bool plain() const {
-    return p.pe_window == nullptr && p.pen_window == nullptr && p.penalty == 0.f;
+    return p.pe_window == nullptr && p.pen_window == nullptr && p.penalty == 0.f &&
+           !p.loss_penalty_term;
   }
 };
 
@@ -553,11 +554,12 @@ synth_tc3_kernel(const uint8_t* __restrict__ Aimg, const uint8_t* __restrict__ B
         if (KIND == 0) {
           const float G = d[e];
           if (in && g.grad_mask) g.grad_mask[i] = G;
-          if (g.theta) {
-            // out of range: theta = 0 and G = 0, so nothing is added
+          if (g.theta && in) {
+            // pixels past the image edge are left out: the band operand's rows there are
+            // not part of the image and may hold anything
             const float gt = -0.5f * G * fast_sin(pre[e]);
             s0 += gt * gt;
-            if (in) g.grad_theta[i] = gt;
+            g.grad_theta[i] = gt;
           }
         } else if (in) {
           const float I = d[e];

@@ -328,7 +328,7 @@ int litho_lbfgs_dots3(litho_ctx* ctx, int k, long long n, const float* d_rows, l
 /* litho_reinit_sdf for `batch` images ([batch][rows][cols]) in one launch, inside =
  * phi > level: level 0.5 on a binary mask gives reinit_sdf(mask - 0.5), the LSM
  * initialisation (LSM_Optimizer.cpp:62), without the shifted copy. d_sdf and d_mask
- * must not alias d_phi. */
+ * must not alias d_phi. It only enqueues work on the context's stream (no wait). */
 int litho_reinit_sdf_batch(litho_ctx* ctx, int batch, int rows, int cols, const float* d_phi,
                            double level, double dx, double dy, float* d_sdf, float* d_mask);
 /* One RK2 level-set update (LSM_Optimizer.cpp:109-115, the second stage reuses
@@ -344,6 +344,40 @@ int litho_lsm_rk2_update(litho_ctx* ctx, int rows, int cols, const float* d_phi,
 int litho_lsm_rk2_update_batch(litho_ctx* ctx, int batch, int rows, int cols, const float* d_phi,
                                const float* d_vn, double dx, double dy, double cfl, double b,
                                float* d_phi_out, float* d_mask, double* dts);
+
+/* ------------------------------------------------------------ device-resident serving
+ * The batched calls above return their per-image scalars to the host and so wait for
+ * the stream. A server that keeps many solves on the GPU uses these forms instead:
+ * they only enqueue work on the context's stream, leave every result on the device and
+ * report a non-finite input (or an expired tensor-core wait) through the context's
+ * deferred status, read with litho_ctx_deferred_status. No counterpart in the
+ * reference (its LSM_Optimizer runs one solve per call).
+ *
+ * litho_pe_gradient_batch_device: litho_pe_gradient_batch with d_losses (device,
+ *   [batch][2] doubles) = {PE, background-penalty term at penalty_threshold}; the
+ *   term adds nothing to dPE/dM (LSM_Optimizer.cpp:87-90 tracks PE + 1.0 x that term
+ *   while its speed is the plain PE gradient).
+ * litho_lsm_rk2_update_batch_device: litho_lsm_rk2_update_batch with d_dts (device,
+ *   nullable, batch doubles).
+ * litho_lsm_track_batch: the best-state bookkeeping of LSM_Optimizer.cpp:93-100 for
+ *   `batch` solves: l_b = d_losses[2b] + pen_weight d_losses[2b + 1];
+ *   d_history[b][d_iters[b]] = l_b (when d_history is set and the column exists),
+ *   d_iters[b] += 1, and when l_b < d_best[b]: d_best[b] = l_b and image b of d_masks
+ *   (n_pixels floats each) is copied to d_best_masks.
+ * litho_ctx_deferred_status: waits for the stream, returns and clears the first
+ *   deferred error (LITHO_OK if none). */
+int litho_pe_gradient_batch_device(litho_ctx* ctx, const litho_cache* cache, int batch,
+                                   const float* d_masks, const float* d_targets, double threshold,
+                                   double alpha, double penalty_threshold, float* d_grad_masks,
+                                   double* d_losses);
+int litho_lsm_rk2_update_batch_device(litho_ctx* ctx, int batch, int rows, int cols,
+                                      const float* d_phi, const float* d_vn, double dx, double dy,
+                                      double cfl, double b, float* d_phi_out, float* d_mask,
+                                      double* d_dts);
+int litho_lsm_track_batch(litho_ctx* ctx, int batch, long long n_pixels, const double* d_losses,
+                          double pen_weight, double* d_best, const float* d_masks,
+                          float* d_best_masks, double* d_history, int history_cols, int* d_iters);
+int litho_ctx_deferred_status(litho_ctx* ctx);
 
 /* ------------------------------------------------------------ full chip
  * Partition (include/utils/partition.h, source/utils/partition.cpp:21-120): the

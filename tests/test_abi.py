@@ -72,9 +72,10 @@ def declared_prototypes():
         types = []
         for p in params:
             p = " ".join(p.split())
-            # drop the parameter name (the last identifier) unless the type is all there is
-            t = re.sub(r"\s*\b[A-Za-z_]\w*$", "", p) if re.search(r"[\w\*]\s+\**[A-Za-z_]\w*$", p) else p
-            types.append(t.replace(" *", "*").strip())
+            # split off the parameter name (the last identifier) unless the type is all there is
+            named = re.search(r"[\w\*]\s+\**([A-Za-z_]\w*)$", p)
+            t = re.sub(r"\s*\b[A-Za-z_]\w*$", "", p) if named else p
+            types.append((t.replace(" *", "*").strip(), named.group(1) if named else ""))
         protos[m.group(2)] = (ret.replace(" *", "*"), types)
     return protos
 
@@ -93,8 +94,9 @@ def ctypes_class(c_type):
 
 def test_binding_signatures_match_the_header(pkg):
     """Every ctypes binding has the header's parameter count, and each parameter the
-    class its C type needs: int / long long / double by value, double* and int* as typed
-    pointers, any other pointer (handles, float buffers, streams, structs) as a pointer."""
+    class its C type needs: int / long long / double by value, host double* and int* as
+    typed pointers, device addresses (d_ names) and any other pointer (handles, float
+    buffers, streams, structs) as a pointer."""
     import ctypes as C
     protos = declared_prototypes()
     assert sorted(protos) == declared_functions()
@@ -104,8 +106,10 @@ def test_binding_signatures_match_the_header(pkg):
         assert len(args) == len(params), (name, params, args)
         want_ret = ctypes_class(ret)
         assert (res is want_ret) or (want_ret == "pointer" and res in pointer_like), (name, ret, res)
-        for i, (p, a) in enumerate(zip(params, args)):
+        for i, ((p, pname), a) in enumerate(zip(params, args)):
             want = ctypes_class(p)
+            if pname.startswith("d_") and p.replace("const ", "").endswith("*"):
+                want = "pointer"    # a device address: passed as a plain pointer
             if want == "pointer":
                 ok = a in pointer_like or (isinstance(a, type) and issubclass(a, C._Pointer))
             else:

@@ -69,7 +69,8 @@ def printed_mismatch(aerial, ref_aerial):
 
 def edge_points(target, n, seed, aerial, min_grad=0.01):
     """n seeded points on the 0.5 contour of a binary target whose nearest pixel has
-    |grad I| >= min_grad in the oracle's image (the EPE divides by |grad I|)."""
+    |grad I| >= min_grad in the oracle's image (the EPE divides by |grad I|), or, where
+    fewer qualify (a smooth image on a fine grid), the n steepest."""
     from oracle.levelset_oracle import gradient_1d
     rng = np.random.default_rng(seed)
     ys, xs = np.nonzero(np.diff(target, axis=0))
@@ -80,7 +81,12 @@ def edge_points(target, n, seed, aerial, min_grad=0.01):
     mag = np.hypot(gradient_1d(aerial, 1.0, 1), gradient_1d(aerial, 1.0, 0))
     iy = np.clip(np.rint(pts[:, 0]).astype(int), 0, aerial.shape[0] - 1)
     ix = np.clip(np.rint(pts[:, 1]).astype(int), 0, aerial.shape[1] - 1)
-    pts = pts[mag[iy, ix] >= min_grad]
+    m = mag[iy, ix]
+    keep = m >= min_grad
+    if keep.sum() < n:
+        keep = np.zeros(len(pts), bool)
+        keep[np.argsort(-m)[:n]] = True
+    pts = pts[keep]
     return pts[rng.choice(len(pts), size=n, replace=False)]
 
 

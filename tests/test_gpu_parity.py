@@ -412,3 +412,29 @@ def test_sparse_epe_and_gradient_match_oracle(L, wl):
     g = L.Gradient(cache, 0.1, 50.0).epe_gradient(aerial, imaging.get_electric_field(), eps, w, 0.1)
     gref = io.epe_gradient(a64, fields, oc, eps, w, 0.1)
     assert rel_l2(cpu(g), gref) < 1e-4
+
+
+def test_epe_gradient_is_bitwise_repeatable(L, wl):
+    """The EPE dL/dI scatter (Gradient::epe_gradient, gradient.cpp:198-227) sums each
+    pixel's contributions in EP order after a stable sort, so repeated calls give the
+    same gradient bit for bit, with many EPs sharing pixels (the reference's serial loop
+    is deterministic too, demo/demo_CTM_parallel_benchmark.cpp:193-196)."""
+    oc = oo.prepare(64, 4.0, 193.0, 1.35, 0.6, 0.9, use_socs=True)
+    cache = device_cache(L, oc)
+    rng = np.random.default_rng(4)
+    target = np.zeros((64, 64))
+    target[14:40, 20:34] = 1.0
+    mask = io.theta_to_mask(io.initialize_theta(target) + 0.2 * rng.standard_normal((64, 64)))
+    imaging = L.Imaging(cache)
+    r = imaging.compute(mask, 0.1, 50.0)
+    eps, w = _edge_points(target, rng, n_extra=200)
+    eps = np.concatenate([eps, eps[::3] + rng.uniform(-0.2, 0.2, eps[::3].shape)])  # shared pixels
+    w = np.concatenate([w, rng.uniform(0.2, 1.0, len(eps) - len(w))])
+    grad = L.Gradient(cache, 0.1, 50.0)
+    g0 = grad.epe_gradient(r.aerial_image, imaging.get_electric_field(), eps, w, 0.1).clone()
+    for _ in range(3):
+        g1 = grad.epe_gradient(r.aerial_image, imaging.get_electric_field(), eps, w, 0.1)
+        assert torch.equal(g0, g1)
+    _, _, fields = io.imaging_compute(mask, oc, 0.1, 50.0, keep_fields=True)
+    gref = io.epe_gradient(cpu(r.aerial_image), fields, oc, eps, w, 0.1)
+    assert rel_l2(cpu(g0), gref) < 1e-4

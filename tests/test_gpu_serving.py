@@ -5,9 +5,10 @@
   split-BF16 tolerance (gradient relative L2 <= 1e-3, PE relative 1e-4); the FP32
   mode (one image after another) matches it within the FP32 tolerance (1e-4, 1e-5).
 * litho_lsm_rk2_update_batch: every image equals its own litho_lsm_rk2_update.
-* TileServer: a solve's results are the same alone and in a mix of other solves of
-  other sizes that arrive while it runs (bit for bit); slot and HBM-budget admission;
-  a seeded Poisson stream reports latency percentiles.
+* TileServer (device-resident, no host round trip per step): a solve's results are the
+  same alone and in a mix of other solves of other sizes that arrive while it runs (bit
+  for bit); its loss history follows LSMOptimizer; a non-finite input is reported;
+  slot and HBM-budget admission; a seeded Poisson stream reports latency percentiles.
 """
 import importlib
 
@@ -128,16 +129,17 @@ def test_server_same_alone_and_in_the_mix(L, S, wl, setup):
 
 
 def test_server_first_iteration_matches_lsm_step(L, S, wl, setup):
-    """The server's first iteration is LSM_Optimizer's: PE of the initial mask and
-    one RK2 update with dPE/dM as the speed (single-image path, same tolerance as
-    the batched gradient)."""
+    """The server's first iteration is LSM_Optimizer's: the tracked loss PE + 1.0 x the
+    background-penalty term at 0.01 of the initial mask (LSM_Optimizer.cpp:87-90) and
+    one RK2 update with dPE/dM as the speed (single-image path, same tolerance as the
+    batched gradient)."""
     ctx, caches, _ = setup
     cache = caches[128]
     tgt, m = tile(wl, 128, 9)
     s = _run_alone(S, caches, tgt, m, 1)
     r = L.Imaging(cache).compute(m, THR, ALPHA)
-    pe = L.Loss.pe_loss(r.wafer_image, tgt, ctx=ctx)
-    assert abs(s.losses[0] - pe) <= 1e-4 * pe
+    pe = L.Loss.pe_loss_with_penalty(r.wafer_image, tgt, 1.0, 0.01, ctx=ctx)
+    assert abs(s.losses[0] - pe) <= 1e-4 * pe and s.best_loss == s.losses[0]
     phi0 = L.LevelSetUtils.reinit_sdf(m - 0.5, 1.0, 1.0, ctx=ctx)
     imaging = L.Imaging(cache)
     r = imaging.compute(m, THR, ALPHA)
@@ -165,6 +167,36 @@ def test_server_slots_and_budget(L, S, wl, setup):
     srv.drain()
     with pytest.raises(L.LithoError):
         srv.submit(torch.zeros((64, 64), device="cuda"), torch.zeros((64, 64), device="cuda"), 2)
+
+
+def test_server_matches_lsm_optimizer(L, S, wl, setup):
+    """A solve of 25 iterations (a re-initialisation after iteration 20) against
+    LSMOptimizer (the single-image LSM_Optimizer loop) on the same cache: the loss
+    history within the split-BF16 tolerance (1e-4 relative per iteration)."""
+    ctx, caches, _ = setup
+    cache = caches[128]
+    tgt, m = tile(wl, 128, 12)
+    srv = S.TileServer(caches, THR, ALPHA, reinit_interval=20)
+    s = srv.submit(tgt, m, 25)
+    srv.drain()
+    lsm = L.LSMOptimizer(cache, tgt, THR, ALPHA, 1.0, 1.0, cfl=0.5, b=0.01, iterations=25)
+    lsm.optimize(m)
+    assert len(s.losses) == 25
+    for a, b in zip(s.losses, lsm.error_history):
+        assert abs(a - b) <= 1e-4 * b
+    assert s.best_loss == min(s.losses)
+
+
+def test_server_reports_a_nonfinite_target(L, S, wl, setup):
+    ctx, caches, _ = setup
+    tgt, m = tile(wl, 128, 13)
+    bad = tgt.clone()
+    bad[3, 3] = float("nan")
+    srv = S.TileServer(caches, THR, ALPHA)
+    srv.submit(bad, m, 2)
+    with pytest.raises(L.LithoError) as e:
+        srv.drain()
+    assert e.value.status == 3
 
 
 def test_server_poisson_stream(L, S, wl, setup):
