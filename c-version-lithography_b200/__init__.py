@@ -41,6 +41,9 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liblitho_b200.so")
 
+# cudaStreamLegacy: the explicit handle of CUDA's legacy default stream.
+CUDA_STREAM_LEGACY = 0x1
+
 # Status codes (include/litho_b200.h).
 LITHO_OK = 0
 STATUS_NAMES = {0: "ok", 1: "invalid argument", 2: "shape mismatch", 3: "non-finite input",
@@ -233,9 +236,13 @@ class Context:
         if stream is None:
             stream = torch.cuda.current_stream(device)
         self.stream = stream
+        # torch's default stream is CUDA's legacy default stream (handle 0), which the
+        # library would read as "create a stream of your own": pass the legacy stream's
+        # explicit handle instead, so that the library's work and the caller's torch
+        # work on that stream stay in one order.
+        raw = stream.cuda_stream if stream.cuda_stream else CUDA_STREAM_LEGACY
         h = ctypes.c_void_p()
-        self._check(self.lib.litho_ctx_create(device, ctypes.c_void_p(stream.cuda_stream),
-                                              ctypes.byref(h)), None)
+        self._check(self.lib.litho_ctx_create(device, ctypes.c_void_p(raw), ctypes.byref(h)), None)
         self.handle = h
 
     def _check(self, status, handle="self"):

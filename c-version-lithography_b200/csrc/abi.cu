@@ -1022,8 +1022,9 @@ static int ctm_evaluate_impl(litho_ctx* ctx, const litho_cache* cache, litho_fie
   for (int i = 0; i < 6; ++i) key.geom[i] = geom[i];
   key.thr = threshold;
   key.alpha = alpha;
-  const bool graphable =
-      ctx->graphs && field != nullptr && target_ready == nullptr && !ctx->timing;
+  const bool graphable = ctx->graphs && field != nullptr && target_ready == nullptr &&
+                         !ctx->timing && ctx->stream != nullptr &&
+                         ctx->stream != cudaStreamLegacy;   // the legacy stream cannot be captured
   if (graphable && ctx->eval_graph && key == ctx->eval_graph_key) {
     LITHO_CUDA_TRY(ctx, cudaGraphLaunch(ctx->eval_graph, ctx->stream));
     ctx->launches += ctx->eval_graph_launches;

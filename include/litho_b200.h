@@ -61,7 +61,10 @@ const char* litho_status_string(int status);
 const char* litho_ctx_last_error(const litho_ctx* ctx);
 
 /* ------------------------------------------------------------ context
- * stream: a cudaStream_t to run on, or NULL for a stream the context creates.
+ * stream: a cudaStream_t to run on (cudaStreamLegacy for the legacy default stream), or
+ * NULL for a stream the context creates. On the legacy default stream the kernels keep
+ * the plain stream order (no programmatic dependent launch) and litho_ctm_evaluate
+ * launches its chain directly (that stream cannot be captured into a graph).
  */
 int litho_ctx_create(int device, void* stream, litho_ctx** out);
 int litho_ctx_destroy(litho_ctx* ctx);

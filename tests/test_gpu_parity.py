@@ -339,13 +339,19 @@ def test_ctm_evaluate_graph_replay(L, wl, precision):
     changes of theta are seen by the replay."""
     N = 256
     band, r0, c0, w, wss = wl.synthetic_socs_band()
-    ctx = L.Context()
+    stream = torch.cuda.Stream()      # a capturable stream (the legacy default is not)
+    ctx = L.Context(stream=stream)
     ctx.set_precision(precision)
     cache = L.ImagingCache.from_band(N, band, r0, c0, w, wss, ctx=ctx)
     rng = np.random.default_rng(11)
     theta0 = (rng.random((N, N)) * 3.0).astype(np.float32)
     theta1 = (rng.random((N, N)) * 3.0).astype(np.float32)
     target = (rng.random((N, N)) > 0.5).astype(np.float32)
+    with torch.cuda.stream(stream):
+        _graph_replay_steps(L, cache, ctx, theta0, theta1, target)
+
+
+def _graph_replay_steps(L, cache, ctx, theta0, theta1, target):
     fresh = L.CTMOptimizer(cache, target, 0.02, 50.0, iterations=1)
     ref0 = fresh.evaluate(torch.from_numpy(theta0).cuda())
     ref0 = (ref0[0], ref0[1].cpu().numpy(), ref0[2])
