@@ -80,6 +80,17 @@ __device__ __forceinline__ Item item_at(int it, int T, int B) {
   r.yt = t / T;
   return r;
 }
+// The item after it (no division: a role walks its items in order).
+__device__ __forceinline__ Item item_next(Item it, int T, int B) {
+  if (++it.z == B) {
+    it.z = 0;
+    if (++it.xt == T) {
+      it.xt = 0;
+      ++it.yt;
+    }
+  }
+  return it;
+}
 
 // Per-item FP64 partial sums of the epilogue warps without a CTA barrier (a warp that
 // leaves its loop on a failed wait must not strand the others): every warp adds its
@@ -126,59 +137,78 @@ __device__ __forceinline__ bool epi_take(const EpiSums<NV>& sh, uint32_t red_bar
 
 // R (tensor memory: lanes y = lane_base + lane, columns f) -> sR, the K-major
 // [hi | lo] operand of stage 2 (rows f, K = y), for the 16-column groups q0, q0 + dq,
-// .. of BN. Lanes y and y ^ 1 share the 4-byte words (f, y & ~1): the even lane
-// stores the hi pair, the odd lane the lo pair. acc: the accumulator's address with
-// this warp's lane base.
+// .. of BN. The words (f, y & ~1) hold the pair of lanes y & ~1 and y | 1: for each
+// pair of columns (f, f + 1) the even lane splits and stores column f (hi and lo
+// word), the odd lane column f + 1, after one exchange of values between the two.
+// acc: the accumulator's address with this warp's lane base.
 template <int BN>
 __device__ __forceinline__ void r_to_operand(uint32_t acc, uint8_t* sR, int lane_base, int q0,
                                              int dq) {
-  const int lane = threadIdx.x & 31;
-  const int y = lane_base + lane;
-  const int ye = y & ~1;
-  const bool odd = lane & 1;
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t ye = ((uint32_t)lane_base + lane) & ~1u;
+  const uint32_t odd = lane & 1u;
+  // sw128_offset(BN, f, k) for f = 16 q + i + odd, k = ye (hi) or 128 + ye (lo): the
+  // part that depends on (f % 8), and the 1024-byte groups of 8 rows f / 8
+  uint32_t off[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const uint32_t f8 = 2u * i + odd;
+    off[i] = (ye >> 6) * (uint32_t)BN * 128u + f8 * 128u + ((((ye & 63u) >> 3) ^ f8) << 4) +
+             (ye & 7u) * 2u;
+  }
+  constexpr uint32_t LO = 2u * (uint32_t)BN * 128u;   // k + 128: two atoms further
 #pragma unroll 1
   for (int q = q0; q < BN / 16; q += dq) {
     float rv[16];
     tmem_ld16x(acc + (uint32_t)(16 * q), rv);
+    uint8_t* sq = sR + (uint32_t)q * 2048u;
 #pragma unroll
-    for (int i = 0; i < 16; ++i) {
-      const float pv = __shfl_xor_sync(0xffffffffu, rv[i], 1);
+    for (int i = 0; i < 16; i += 2) {
+      // the even lane receives its partner's column i, the odd lane column i + 1
+      const float got = __shfl_xor_sync(0xffffffffu, odd ? rv[i] : rv[i + 1], 1);
       uint32_t h2, l2;
-      split_pair(odd ? pv : rv[i], odd ? rv[i] : pv, h2, l2);
-      *reinterpret_cast<uint32_t*>(sR + sw128_offset(BN, 16 * q + i, odd ? 128 + ye : ye)) =
-          odd ? l2 : h2;
+      split_pair(odd ? got : rv[i], odd ? rv[i + 1] : got, h2, l2);
+      uint8_t* w = sq + (uint32_t)(i >> 3) * 1024u + off[(i & 7) >> 1];
+      *reinterpret_cast<uint32_t*>(w) = h2;
+      *reinterpret_cast<uint32_t*>(w + LO) = l2;
     }
   }
 }
 
 // Q (tensor memory: lanes n = 2 r + s, columns f = 2 c + t) -> the tile's partials
 // P[r][c] of the band (see analysis_stages in tc2.cu): Re = Q[2r][2c] - Q[2r+1][2c+1],
-// Im = Q[2r][2c+1] + Q[2r+1][2c]; with sym also the conjugate rows -r.
+// Im = Q[2r][2c+1] + Q[2r+1][2c]; with sym also the conjugate rows -r (from the odd
+// lane of the pair).
 template <int BN>
 __device__ __forceinline__ void q_to_partials(uint32_t acc, float2* out, const Tc2Analysis& a,
                                               int lane_base, int q0, int dq) {
   const int lane = threadIdx.x & 31;
   const int nn = lane_base + lane;
   const int r = nn >> 1, s = nn & 1;
+  // the output row of this lane, or none
+  float2* row = nullptr;
+  if (r < a.nr) {
+    if (!a.sym)
+      row = s == 0 ? out + r * a.ncols : nullptr;
+    else if (s == 0)
+      row = out + (a.nr - 1 + r) * a.ncols;
+    else if (r >= 1)
+      row = out + (a.nr - 1 - r) * a.ncols;
+  }
 #pragma unroll 1
   for (int q = q0; q < BN / 16; q += dq) {
     float qv[16], pv[16];
     tmem_ld16x(acc + (uint32_t)(16 * q), qv);
 #pragma unroll
     for (int i = 0; i < 16; ++i) pv[i] = __shfl_xor_sync(0xffffffffu, qv[i], 1);
-    if (r >= a.nr) continue;
+    if (row == nullptr) continue;
+    float2* rq = row + 8 * q;
+    const int nc = a.ncols - 8 * q;
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
-      const int c = 8 * q + i;
-      if (c >= a.ncols) break;
+      if (i >= nc) break;
       const float o0 = qv[2 * i], o1 = qv[2 * i + 1], p0 = pv[2 * i], p1 = pv[2 * i + 1];
-      if (!a.sym) {
-        if (s == 0) out[r * a.ncols + c] = make_float2(o0 - p1, o1 + p0);
-      } else if (s == 0) {
-        out[(a.nr - 1 + r) * a.ncols + c] = make_float2(o0 - p1, o1 + p0);
-      } else if (r >= 1) {
-        out[(a.nr - 1 - r) * a.ncols + c] = make_float2(p0 + o1, p1 - o0);
-      }
+      rq[i] = s == 0 ? make_float2(o0 - p1, o1 + p0) : make_float2(p0 + o1, p1 - o0);
     }
   }
 }
@@ -260,46 +290,65 @@ analysis_tc3_kernel(Tc2Analysis a, int T, int B, const uint8_t* __restrict__ txI
     // ------------------------------------------------------------ loaders
     pdl_wait();
     const int tid = threadIdx.x;
-    for (int j = 0; j < n; ++j) {
-      const Item it = item_at(lo + j, T, B);
-      const int y0 = it.yt * 128, x0 = it.xt * 128;
-      const float* img = a.in + (size_t)it.z * a.N * a.N;
-      float* mo = a.mask_out ? a.mask_out + (size_t)it.z * a.N * a.N : nullptr;
-      // every load of the tile first (they overlap the previous item's MMAs)
-      float v[8][8];
+    // chunk i of a thread: row (tid >> 4) + 16 i, columns c8 .. c8 + 7 of the tile; its
+    // hi part at so + 2048 i of sA, its lo part 32 KiB further (sw128_offset)
+    const int r0 = tid >> 4, c8 = (tid & 15) * 8;
+    const uint32_t so = sw128_offset(128, r0, c8);
+    float v[8][8];
+    // chunks i0 .. i0 + 3 (rows 16 i0 .. 16 i0 + 63) of item j into v
+    auto load_half = [&](const Item& it, int i0) {
+      const int m0 = it.yt * 128 + r0, x = it.xt * 128 + c8;
+      const float* img = a.in + (size_t)it.z * a.N * a.N + (size_t)m0 * a.N + x;
 #pragma unroll
-      for (int i = 0; i < 8; ++i) {
-        const int jj = tid + i * (A3_LOADW * 32);
-        const int r = jj >> 4, c8 = (jj & 15) * 8;
-        const int m = y0 + r, x = x0 + c8;
+      for (int i = i0; i < i0 + 4; ++i) {
+        const int m = m0 + 16 * i;
+        const float* pi = img + (size_t)(16 * i) * a.N;
         if (a.vec4 && m < a.N && x + 7 < a.N) {
-          const float4 p = __ldg(reinterpret_cast<const float4*>(img + (size_t)m * a.N + x));
-          const float4 q = __ldg(reinterpret_cast<const float4*>(img + (size_t)m * a.N + x + 4));
+          const float4 p = __ldg(reinterpret_cast<const float4*>(pi));
+          const float4 q = __ldg(reinterpret_cast<const float4*>(pi + 4));
           v[i][0] = p.x; v[i][1] = p.y; v[i][2] = p.z; v[i][3] = p.w;
           v[i][4] = q.x; v[i][5] = q.y; v[i][6] = q.z; v[i][7] = q.w;
         } else {
 #pragma unroll
-          for (int e = 0; e < 8; ++e)
-            v[i][e] = (m < a.N && x + e < a.N) ? __ldg(img + (size_t)m * a.N + x + e) : 0.f;
+          for (int e = 0; e < 8; ++e) v[i][e] = (m < a.N && x + e < a.N) ? __ldg(pi + e) : 0.f;
         }
       }
-      // sA is free once stage 1 of the previous item has completed
-      if (j > 0 && !pwait(bar(1 + ((j - 1) & 1)), ((j - 1) >> 1) & 1, vfail, err, 11)) break;
-      bool bad = false;
+    };
+    // chunks i0 .. i0 + 3 of item j: theta -> mask (mode 1), split into sA; the
+    // non-finite inputs flagged in bad
+    auto proc_half = [&](const Item& it, int i0, bool& bad) {
+      const int m0 = it.yt * 128 + r0, x = it.xt * 128 + c8;
+      float* mo = a.mask_out ? a.mask_out + (size_t)it.z * a.N * a.N + (size_t)m0 * a.N + x
+                             : nullptr;
+      const bool full = a.vec4 && it.yt * 128 + 127 < a.N && x + 7 < a.N;
 #pragma unroll
-      for (int i = 0; i < 8; ++i) {
-        const int jj = tid + i * (A3_LOADW * 32);
-        const int r = jj >> 4, c8 = (jj & 15) * 8;
-        const int m = y0 + r, x = x0 + c8;
+      for (int i = i0; i < i0 + 4; ++i) {
+        const int m = m0 + 16 * i;
         float u[8];
+        if (full) {
+          // every input is finite exactly when chk stays 0
+          float chk = 0.f;
 #pragma unroll
-        for (int e = 0; e < 8; ++e) {
-          const bool in_range = m < a.N && x + e < a.N;
-          u[e] = v[i][e];
-          if (in_range) bad |= !isfinite(u[e]);
-          if (a.mode == 1) {
-            u[e] = in_range ? 0.5f * (1.f + fast_cos(u[e])) : 0.f;
-            if (mo && in_range) mo[(size_t)m * a.N + x + e] = u[e];
+          for (int e = 0; e < 8; ++e) {
+            chk = __fmaf_rn(v[i][e], 0.f, chk);
+            u[e] = a.mode == 1 ? 0.5f * (1.f + fast_cos(v[i][e])) : v[i][e];
+          }
+          bad |= chk != 0.f;
+          if (mo) {
+            float* po = mo + (size_t)(16 * i) * a.N;
+            *reinterpret_cast<float4*>(po) = make_float4(u[0], u[1], u[2], u[3]);
+            *reinterpret_cast<float4*>(po + 4) = make_float4(u[4], u[5], u[6], u[7]);
+          }
+        } else {
+#pragma unroll
+          for (int e = 0; e < 8; ++e) {
+            const bool in_range = m < a.N && x + e < a.N;
+            u[e] = v[i][e];
+            if (in_range) bad |= !isfinite(u[e]);
+            if (a.mode == 1) {
+              u[e] = in_range ? 0.5f * (1.f + fast_cos(u[e])) : 0.f;
+              if (mo && in_range) mo[(size_t)(16 * i) * a.N + e] = u[e];
+            }
           }
         }
         uint4 h4, l4;
@@ -307,9 +356,23 @@ analysis_tc3_kernel(Tc2Analysis a, int T, int B, const uint8_t* __restrict__ txI
         split_pair(u[2], u[3], h4.y, l4.y);
         split_pair(u[4], u[5], h4.z, l4.z);
         split_pair(u[6], u[7], h4.w, l4.w);
-        *reinterpret_cast<uint4*>(sA + sw128_offset(128, r, c8)) = h4;
-        *reinterpret_cast<uint4*>(sA + sw128_offset(128, r, 128 + c8)) = l4;
+        *reinterpret_cast<uint4*>(sA + so + 2048u * i) = h4;
+        *reinterpret_cast<uint4*>(sA + so + 32768u + 2048u * i) = l4;
       }
+    };
+    // The loads run half an item ahead of the conversion: the second half of item j
+    // loads while the first half converts, the first half of item j + 1 while the
+    // second half of item j converts.
+    Item cur = item_at(lo, T, B);
+    if (n > 0) load_half(cur, 0);
+    for (int j = 0; j < n; ++j, cur = item_next(cur, T, B)) {
+      load_half(cur, 4);
+      // sA is free once stage 1 of the previous item has completed
+      if (j > 0 && !pwait(bar(1 + ((j - 1) & 1)), ((j - 1) >> 1) & 1, vfail, err, 11)) break;
+      bool bad = false;
+      proc_half(cur, 0, bad);
+      if (j + 1 < n) load_half(item_next(cur, T, B), 0);
+      proc_half(cur, 4, bad);
       if (bad) atomicOr(a.flag, 1);
       fence_async_smem();
       __syncwarp();
@@ -320,7 +383,12 @@ analysis_tc3_kernel(Tc2Analysis a, int T, int B, const uint8_t* __restrict__ txI
     pdl_wait();
     const int lane_base = (warp & 3) * 32;
     const int count = a.nrows_out * a.ncols;
+    Item prv = item_at(lo, T, B), cur = prv;   // items j - 1 and j
     for (int j = 0; j <= n; ++j) {
+      if (j > 0) {
+        prv = cur;
+        cur = item_next(cur, T, B);
+      }
       if (j < n && !pwait(bar(1 + (j & 1)), (j >> 1) & 1, vfail, err, 12)) break;
       // stage 2 of the previous item done: sR is free and its Q is ready
       if (j > 0 && !pwait(bar(4 + ((j - 1) & 1)), ((j - 1) >> 1) & 1, vfail, err, 13)) break;
@@ -336,8 +404,7 @@ analysis_tc3_kernel(Tc2Analysis a, int T, int B, const uint8_t* __restrict__ txI
       if (j > 0) {
         // Q of the previous item -> its partials P[r][c] (see analysis_stages in tc2.cu)
         const int jp = j - 1;
-        const Item it = item_at(lo + jp, T, B);
-        float2* out = a.part + (((size_t)it.z * T + it.yt) * T + it.xt) * count;
+        float2* out = a.part + (((size_t)prv.z * T + prv.yt) * T + prv.xt) * count;
         q_to_partials<BN>(tmem + 256u + (uint32_t)((jp & 1) * 128) + ((uint32_t)lane_base << 16),
                           out, a, lane_base, 0, 1);
         tc::fence_before();
@@ -350,8 +417,8 @@ analysis_tc3_kernel(Tc2Analysis a, int T, int B, const uint8_t* __restrict__ txI
     int pxt = -1, pyt = -1;
     uint32_t ntx = 0, nty = 0;
     int m1 = 0, m2 = 0;
-    for (int j = 0; j < n; ++j) {
-      const Item it = item_at(lo + j, T, B);
+    Item it = item_at(lo, T, B);
+    for (int j = 0; j < n; ++j, it = item_next(it, T, B)) {
       const bool newx = it.xt != pxt;
       if (newx) {
         // the TX tile in use is read by stage 1 of the previous item
@@ -416,7 +483,9 @@ cudaError_t launch_analysis_tc3(cudaStream_t s, int mode, const float* in, float
                                 int* flag, int N, int ncols, int nrows_out, int nr, int sym,
                                 float2* part, const void* tx_img, const void* ty_img, int* err,
                                 int batch) {
-  const int vec4 = (N % 4 == 0) && (reinterpret_cast<uintptr_t>(in) % 16 == 0);
+  // vector loads of the input and vector stores of the mask
+  const int vec4 = (N % 4 == 0) && (reinterpret_cast<uintptr_t>(in) % 16 == 0) &&
+                   (reinterpret_cast<uintptr_t>(mask_out) % 16 == 0);
   Tc2Analysis a{in, mask_out, flag, N, mode, vec4, ncols, nrows_out, nr, sym, part};
   switch (tc2_analysis_rows(ncols)) {
     case 16: return analysis_tc3_t<16>(s, a, tx_img, ty_img, err, batch);
@@ -525,19 +594,33 @@ synth_tc3_kernel(const uint8_t* __restrict__ Aimg, const uint8_t* __restrict__ B
     const uint32_t lane_addr = (uint32_t)(32 * q) << 16;
     const float* src = KIND == 0 ? g.theta : (r.p.mode == 1 ? r.p.target : nullptr);
     const bool plain = KIND == 1 && r.plain();
-    for (int j = 0; j < n; ++j) {
-      const Item it = item_at(lo + j, T, B);
+    // theta chain without the dPE/dM output: the CTM evaluation
+    const bool lean = KIND == 0 && g.theta != nullptr && g.grad_mask == nullptr;
+    // per-pixel input, coalesced along x: rows e0 .. e0 + 15 of item j into pre[]
+    float pre[32];
+    auto load_rows = [&](const Item& it, int e0) {
+      const int x = it.xt * 128 + 32 * q + lane, yb = it.yt * 128 + 32 * h;
+      const float* sp = src + (size_t)it.z * N * N + (size_t)yb * N + x;
+      if (x < N && yb + 31 < N) {
+#pragma unroll
+        for (int e = e0; e < e0 + 16; ++e) pre[e] = __ldg(sp + e * N);
+      } else {
+#pragma unroll
+        for (int e = e0; e < e0 + 16; ++e) pre[e] = (x < N && yb + e < N) ? __ldg(sp + e * N) : 0.f;
+      }
+    };
+    Item it = item_at(lo, T, B);
+    if (src && n > 0) {
+      load_rows(it, 0);
+      load_rows(it, 16);
+    }
+    for (int j = 0; j < n; ++j, it = item_next(it, T, B)) {
+      const Item nxt = item_next(it, T, B);
       const int x = it.xt * 128 + 32 * q + lane;
       const int yb = it.yt * 128 + 32 * h;
       const bool xin = x < N;
+      const bool full = xin && yb + 31 < N;
       const size_t base = (size_t)it.z * N * N;
-      // per-pixel input of the 32 rows, coalesced along x, before the accumulator
-      float pre[32];
-#pragma unroll
-      for (int e = 0; e < 32; ++e) {
-        const int y = yb + e;
-        pre[e] = (src && xin && y < N) ? __ldg(src + base + (size_t)y * N + x) : 0.f;
-      }
       if (!pwait(bar(3 + (j & 1)), (j >> 1) & 1, vfail, err, 21)) break;
       tc::fence_after();
       float d[32];
@@ -546,31 +629,47 @@ synth_tc3_kernel(const uint8_t* __restrict__ Aimg, const uint8_t* __restrict__ B
       __syncwarp();
       if (lane == 0) mbar_arrive(bar(5 + (j & 1)));
       float s0 = 0.f, s1 = 0.f;
+      // rows e0 .. e0 + 15; the inputs of the next item load into the rows just used
+      auto rows = [&](int e0) {
+        if (lean && full) {
+          float* gp = g.grad_theta + base + (size_t)yb * N + x;
 #pragma unroll
-      for (int e = 0; e < 32; ++e) {
-        const int y = yb + e;
-        const bool in = xin && y < N;
-        const size_t i = base + (size_t)y * N + x;
-        if (KIND == 0) {
-          const float G = d[e];
-          if (in && g.grad_mask) g.grad_mask[i] = G;
-          if (g.theta && in) {
-            // pixels past the image edge are left out: the band operand's rows there are
-            // not part of the image and may hold anything
-            const float gt = -0.5f * G * fast_sin(pre[e]);
+          for (int e = e0; e < e0 + 16; ++e) {
+            const float gt = -0.5f * d[e] * fast_sin(pre[e]);
             s0 += gt * gt;
-            g.grad_theta[i] = gt;
+            gp[e * N] = gt;
           }
-        } else if (in) {
-          const float I = d[e];
-          if (r.p.mode == 0) {
-            if (r.p.aerial) r.p.aerial[i] = I;
-            if (r.p.wafer) r.p.wafer[i] = r.sigmoid(I);
-          } else {
-            r.p.dldi[i] = r.dldi(i, I, pre[e], plain, s0, s1);
+        } else {
+#pragma unroll
+          for (int e = e0; e < e0 + 16; ++e) {
+            const int y = yb + e;
+            const bool in = xin && y < N;
+            const size_t i = base + (size_t)y * N + x;
+            if (KIND == 0) {
+              const float G = d[e];
+              if (in && g.grad_mask) g.grad_mask[i] = G;
+              if (g.theta && in) {
+                // pixels past the image edge are left out: the band operand's rows there
+                // are not part of the image and may hold anything
+                const float gt = -0.5f * G * fast_sin(pre[e]);
+                s0 += gt * gt;
+                g.grad_theta[i] = gt;
+              }
+            } else if (in) {
+              const float I = d[e];
+              if (r.p.mode == 0) {
+                if (r.p.aerial) r.p.aerial[i] = I;
+                if (r.p.wafer) r.p.wafer[i] = r.sigmoid(I);
+              } else {
+                r.p.dldi[i] = r.dldi(i, I, pre[e], plain, s0, s1);
+              }
+            }
           }
         }
-      }
+        if (src && j + 1 < n) load_rows(nxt, e0);
+      };
+      rows(0);
+      rows(16);
       const bool sums = KIND == 0 ? g.theta != nullptr : r.p.mode == 1;
       if (sums) {
         const double v[2] = {(double)s0, (double)s1};
@@ -594,19 +693,16 @@ synth_tc3_kernel(const uint8_t* __restrict__ Aimg, const uint8_t* __restrict__ B
     // the band operand image is written by the previous kernel of the stream
     pdl_wait();
     constexpr uint32_t idesc = tc::idesc_bf16(128, 128);
-    auto bt_src = [&](int j) {
-      const Item it = item_at(lo + j, T, B);
-      return Bimg + ((size_t)it.z * T + it.xt) * tb;
-    };
+    auto bt_src = [&](const Item& it) { return Bimg + ((size_t)it.z * T + it.xt) * tb; };
     int pyt = -1;
     uint32_t nay = 0;
     int nb = 0, nm = 0;
+    Item it = item_at(lo, T, B);
     if (n > 0) {
-      bulk_tile(uAY + tb, bt_src(0), tb, bar(0));
+      bulk_tile(uAY + tb, bt_src(it), tb, bar(0));
       nb = 1;
     }
-    for (int j = 0; j < n; ++j) {
-      const Item it = item_at(lo + j, T, B);
+    for (int j = 0; j < n; ++j, it = item_next(it, T, B)) {
       const bool newy = it.yt != pyt;
       if (newy) {
         // the AY tile in use is read by the previous item's MMA
@@ -626,7 +722,8 @@ synth_tc3_kernel(const uint8_t* __restrict__ Aimg, const uint8_t* __restrict__ B
       if (j + 1 < n) {
         // Bt[(j + 1) & 1] is read by the MMA of item j - 1
         if (j >= 1 && !pwait(bar(3 + ((j - 1) & 1)), ((j - 1) >> 1) & 1, vfail, err, 26)) break;
-        bulk_tile(uAY + (uint32_t)(1 + ((j + 1) & 1)) * tb, bt_src(j + 1), tb, bar((j + 1) & 1));
+        bulk_tile(uAY + (uint32_t)(1 + ((j + 1) & 1)) * tb, bt_src(item_next(it, T, B)), tb,
+                  bar((j + 1) & 1));
         ++nb;
       }
     }
@@ -677,8 +774,10 @@ cudaError_t launch_synth_resist_tc3(cudaStream_t s, const void* Aimg, const void
 // (launch_synth_resist_analysis_tc2: same loss partials, same adjoint partials) from a
 // persistent pipeline. Per item j:
 //   SMMA(j)   I^T = Ut . AYD^T into accI[j & 1] (transposed: lanes x);
-//   epi(j)    warps 0-15: resist, loss terms, dL/dI, written as the [hi | lo] operand
-//             sA (rows y, K = x) in region X, while TXD(j) lands behind it;
+//   epi(j)    warps 0-15: resist, loss terms, dL/dI, written as the split operand sA
+//             (M = y, K = x) in region X, while TXD(j) lands behind it. sA is MN-major
+//             (mn_chunk_offset): a thread holds the 32 rows y of its column x and
+//             writes them as 16-byte chunks, with no exchange between lanes;
 //   MMA1(j)   R = sA . TXD^T into accR; once done, X takes the synthesis operands of
 //             item j + 1 (Ut, AYD) and SMMA(j + 1) is issued;
 //   R(j)      warps 0-15: R -> sR;  MMA2(j)  Q = TYD . R^T into accQ;
@@ -749,25 +848,28 @@ fused_tc3_kernel(const uint8_t* __restrict__ Aimg, const uint8_t* __restrict__ B
     const int lane_base = 32 * q;
     const uint32_t lane_addr = (uint32_t)lane_base << 16;
     const int xl = lane_base + lane;
-    const int xe = xl & ~1;
-    const bool odd = lane & 1;
-    const bool plain = r.plain();
+    // no window, no penalty, no aerial / wafer output: the CTM evaluation
+    const bool lean = r.plain() && r.p.aerial == nullptr && r.p.wafer == nullptr;
     const int count = a.nrows_out * a.ncols;
-    float pre[32];
-    auto prefetch = [&](int j) {
-      const Item it = item_at(lo + j, T, B);
-      const int x = it.xt * 128 + xl, yb = it.yt * 128 + 32 * h;
-      const size_t base = (size_t)it.z * N * N;
+    // this thread's four 16-byte chunks of sA (rows y = 32 h + 8 c .. + 7 of column xl)
+    uint32_t aoff[4];
 #pragma unroll
-      for (int e = 0; e < 32; ++e) {
-        const int y = yb + e;
-        pre[e] = (x < N && y < N) ? __ldg(r.p.target + base + (size_t)y * N + x) : 0.f;
+    for (int c = 0; c < 4; ++c) aoff[c] = mn_chunk_offset((uint32_t)(32 * h + 8 * c), (uint32_t)xl);
+    float pre[32];
+    auto prefetch = [&](const Item& it) {
+      const int x = it.xt * 128 + xl, yb = it.yt * 128 + 32 * h;
+      const float* tp = r.p.target + (size_t)it.z * N * N + (size_t)yb * N + x;
+      if (x < N && yb + 31 < N) {
+#pragma unroll
+        for (int e = 0; e < 32; ++e) pre[e] = __ldg(tp + e * N);
+      } else {
+#pragma unroll
+        for (int e = 0; e < 32; ++e) pre[e] = (x < N && yb + e < N) ? __ldg(tp + e * N) : 0.f;
       }
     };
-    bool ok = true;
-    if (n > 0) prefetch(0);
-    for (int j = 0; j < n && ok; ++j) {
-      const Item it = item_at(lo + j, T, B);
+    Item it = item_at(lo, T, B), ip = it;   // items j and j - 1
+    if (n > 0) prefetch(it);
+    for (int j = 0; j < n; ++j, ip = it, it = item_next(it, T, B)) {
       const int x = it.xt * 128 + xl, yb = it.yt * 128 + 32 * h;
       const bool xin = x < N;
       const size_t base = (size_t)it.z * N * N;
@@ -779,21 +881,44 @@ fused_tc3_kernel(const uint8_t* __restrict__ Aimg, const uint8_t* __restrict__ B
       __syncwarp();
       if (lane == 0) mbar_arrive(bar(10 + (j & 1)));
       // sA is free: the MMA thread issues SMMA(j) only after MMA1(j - 1) completed.
+      // d[e] becomes dL/dI at (yb + e, x), 0 outside the image.
       float s0 = 0.f, s1 = 0.f;
-      bool bad = false;
+      bool bad;
+      if (lean && xin && yb + 31 < N) {
+        // Every dL/dI is non-finite exactly when its r is, and then so is r * r in s0 or
+        // the product with 0 in chk (the window-free arithmetic of S3Resist::dldi).
+        float chk = 0.f;
 #pragma unroll
-      for (int e = 0; e < 32; ++e) {
-        const int y = yb + e;
-        float gd = 0.f;
-        if (xin && y < N) gd = r.dldi(base + (size_t)y * N + x, d[e], pre[e], plain, s0, s1);
-        bad |= !isfinite(gd);
-        // lanes x and x ^ 1 share the words (y, x & ~1): hi pair from the even lane,
-        // lo pair from the odd lane
-        const float pv = __shfl_xor_sync(0xffffffffu, gd, 1);
-        uint32_t h2, l2;
-        split_pair(odd ? pv : gd, odd ? gd : pv, h2, l2);
-        *reinterpret_cast<uint32_t*>(sA + sw128_offset(128, 32 * h + e, odd ? 128 + xe : xe)) =
-            odd ? l2 : h2;
+        for (int e = 0; e < 32; ++e) {
+          const float W = r.sigmoid(d[e]);
+          const float rr = W - pre[e];
+          s0 += rr * rr;
+          d[e] = r.p.pe_weight * rr * W * (1.f - W);
+          chk = __fmaf_rn(d[e], 0.f, chk);
+        }
+        bad = chk != 0.f;
+      } else {
+        const bool plain = r.plain();
+        bad = false;
+#pragma unroll
+        for (int e = 0; e < 32; ++e) {
+          const int y = yb + e;
+          float gd = 0.f;
+          if (xin && y < N) gd = r.dldi(base + (size_t)y * N + x, d[e], pre[e], plain, s0, s1);
+          bad |= !isfinite(gd);
+          d[e] = gd;
+        }
+      }
+      // rows 8 c .. 8 c + 7 of column xl: one 16-byte chunk of hi, one of lo
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        uint4 h4, l4;
+        split_pair(d[8 * c + 0], d[8 * c + 1], h4.x, l4.x);
+        split_pair(d[8 * c + 2], d[8 * c + 3], h4.y, l4.y);
+        split_pair(d[8 * c + 4], d[8 * c + 5], h4.z, l4.z);
+        split_pair(d[8 * c + 6], d[8 * c + 7], h4.w, l4.w);
+        *reinterpret_cast<uint4*>(sA + aoff[c]) = h4;
+        *reinterpret_cast<uint4*>(sA + aoff[c] + MN_LO) = l4;
       }
       if (bad) atomicOr(a.flag, 1);
       fence_async_smem();
@@ -811,12 +936,11 @@ fused_tc3_kernel(const uint8_t* __restrict__ Aimg, const uint8_t* __restrict__ B
           r.p.loss_partial[2 * bid + 1] = t[1];
         }
       }
-      if (j + 1 < n) prefetch(j + 1);
+      if (j + 1 < n) prefetch(item_next(it, T, B));
       if (j > 0) {
         // MMA2 of the previous item: its Q is ready and sR is free
         if (!pwait(bar(8), (j - 1) & 1, vfail, err, 32)) break;
         tc::fence_after();
-        const Item ip = item_at(lo + j - 1, T, B);
         q_to_partials<BN>(tmem + 384u + lane_addr,
                           a.part + (((size_t)ip.z * T + ip.yt) * T + ip.xt) * count, a,
                           lane_base, h, 4);
@@ -847,8 +971,7 @@ fused_tc3_kernel(const uint8_t* __restrict__ Aimg, const uint8_t* __restrict__ B
     // the band operand image is written by the previous kernel of the stream
     pdl_wait();
     constexpr uint32_t idI = tc::idesc_bf16(128, 128), idA = tc::idesc_bf16(128, BN);
-    auto load_ops = [&](int j) {
-      const Item it = item_at(lo + j, T, B);
+    auto load_ops = [&](const Item& it) {
       tc::mbar_expect_tx(bar(0), 2 * tb);
       bulk_chunks(uUt, Bimg + ((size_t)it.z * T + it.xt) * tb, tb, bar(0));
       bulk_chunks(uAYD, Aimg + (size_t)it.yt * tb, tb, bar(0));
@@ -864,12 +987,12 @@ fused_tc3_kernel(const uint8_t* __restrict__ Aimg, const uint8_t* __restrict__ B
       last_par = par;
       any = true;
     };
+    Item it = item_at(lo, T, B);
     if (n > 0) {
-      load_ops(0);
+      load_ops(it);
       nops = 1;
     }
-    for (int j = 0; j < n; ++j) {
-      const Item it = item_at(lo + j, T, B);
+    for (int j = 0; j < n; ++j, it = item_next(it, T, B)) {
       if (j == 0) {
         if (!pwait(bar(0), 0, vfail, err, 35)) break;
         tc::fence_after();
@@ -890,13 +1013,13 @@ fused_tc3_kernel(const uint8_t* __restrict__ Aimg, const uint8_t* __restrict__ B
       if (!pwait(bar(3), j & 1, vfail, err, 38)) break;
       if (!pwait(bar(4), j & 1, vfail, err, 39)) break;
       tc::fence_after();
-      s2_mma(tmem + 256u, uX, 128, uTXD, BN, 128, idA);
+      s2_mma_amn(tmem + 256u, uX, uTXD, BN, 128, idA | IDESC_A_MN);
       commit(5, j & 1);
       if (!pwait(bar(5), j & 1, vfail, err, 40)) break;
       if (j + 1 < n) {
         // X is free: the next item's synthesis operands, then its SMMA (accI[(j+1)&1]
         // was read by the epilogue of item j - 1)
-        load_ops(j + 1);
+        load_ops(item_next(it, T, B));
         ++nops;
         if (!pwait(bar(0), (j + 1) & 1, vfail, err, 41)) break;
         if (j >= 1 && !pwait(bar(10 + ((j + 1) & 1)), ((j - 1) >> 1) & 1, vfail, err, 42)) break;

@@ -69,6 +69,48 @@ __device__ __forceinline__ void s2_mma_swapped(uint32_t tmem, uint32_t sa, int r
     }
 }
 
+// MN-major split tile of a 128 (M) x 128 (K) block, 128-byte swizzle: for each k the
+// 128 rows m lie in two 64-row atoms (LBO = 1024 bytes apart), 8 consecutive k form
+// one 1024-byte atom group (SBO = 2048 bytes apart). Element (m, k) of the hi part is
+// at byte
+//   (k / 8) * 2048 + (m / 64) * 1024 + (k % 8) * 128 + ((((m % 64) / 8) ^ (k % 8)) * 16)
+//   + (m % 8) * 2,
+// the lo part MN_LO bytes further; 64 KiB in all, base 1024-byte aligned. A thread
+// that holds 8 consecutive rows m of one column k writes them as one 16-byte chunk.
+constexpr uint32_t MN_LBO = 1024, MN_SBO = 2048, MN_LO = 32768;
+__host__ __device__ constexpr uint32_t mn_chunk_offset(uint32_t m, uint32_t k) {
+  return (k >> 3) * MN_SBO + (m >> 6) * MN_LBO + (k & 7u) * 128u +
+         ((((m & 63u) >> 3) ^ (k & 7u)) << 4);
+}
+// Shared-memory descriptor of the MN-major layout above (sm_100 version bit, SW128).
+__device__ __forceinline__ uint64_t desc_mn_sw128(uint32_t saddr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
+  d |= (uint64_t)(MN_LBO >> 4) << 16;
+  d |= (uint64_t)(MN_SBO >> 4) << 32;
+  d |= (uint64_t)1 << 46;
+  d |= (uint64_t)2 << 61;
+  return d;
+}
+// Instruction-descriptor bit: operand A is MN-major.
+constexpr uint32_t IDESC_A_MN = 1u << 15;
+
+// s2_mma with A (M = 128 rows, K = 128) in the MN-major split layout at sa (hi) and
+// sa + MN_LO (lo): the same three sections and K steps in the same order. idesc must
+// carry IDESC_A_MN.
+__device__ __forceinline__ void s2_mma_amn(uint32_t tmem, uint32_t sa, uint32_t sb, int rb, int K,
+                                           uint32_t idesc) {
+  const uint32_t aoff[3] = {0u, 0u, MN_LO};
+  const int boff[3] = {0, K, 0};
+  bool first = true;
+  for (int s = 0; s < 3; ++s)
+    for (int k = 0; k < K; k += 16) {
+      tc::mma_bf16(tmem, desc_mn_sw128(sa + aoff[s] + (uint32_t)k * 256u),
+                   s2_desc(sb, rb, boff[s] + k), idesc, first ? 0u : 1u);
+      first = false;
+    }
+}
+
 // 16 consecutive FP32 columns of this thread's TMEM lane.
 __device__ __forceinline__ void tmem_ld16x(uint32_t taddr, float (&v)[16]) {
   uint32_t r[16];
