@@ -95,11 +95,13 @@ __device__ __forceinline__ Item item_next(Item it, int T, int B) {
 // Per-item FP64 partial sums of the epilogue warps without a CTA barrier (a warp that
 // leaves its loop on a failed wait must not strand the others): every warp adds its
 // lanes' values in a fixed shuffle order and its lane 0 stores them in slot b = j & 3
-// and arrives on red_bar[b] (count = epilogue warps); thread 0 waits for the slot
-// (bounded), adds the warps in order and writes the partials. No warp runs more than
-// two items ahead of thread 0 (it needs the tensor memory that thread 0's warp frees
-// in its epilogue of item j + 1, after reading slot j), so a slot is read before it is
-// written again four items later.
+// and arrives on red_bar[b] (count = epilogue warps); a collecting thread waits for
+// the slot (bounded), adds the warps in order and writes the partials: thread 0 right
+// after its own part (fused kernel), or, in the syntheses, one warp in turn during its
+// item j + 1 (collect2). Either reads slot b before it reads the accumulator of item
+// j + 2, and no warp reaches item j + 4, which writes slot b again, before every warp
+// has read the accumulator of item j + 2 (the accumulators are double-buffered), so a
+// slot is read before it is written again.
 constexpr int EPI_SLOTS = 4;
 template <int NV>
 struct EpiSums {
@@ -121,7 +123,7 @@ __device__ __forceinline__ void epi_put(EpiSums<NV>& sh, uint32_t red_bar, int b
     mbar_arrive(red_bar);
   }
 }
-// Thread 0: the slot's sums over nw warps (false when the wait gave up).
+// The slot's sums over nw warps, added in warp order (false when the wait gave up).
 template <int NV>
 __device__ __forceinline__ bool epi_take(const EpiSums<NV>& sh, uint32_t red_bar, int b,
                                          uint32_t parity, int nw, volatile int* fail, int* err,
@@ -132,6 +134,30 @@ __device__ __forceinline__ bool epi_take(const EpiSums<NV>& sh, uint32_t red_bar
     out[k] = 0.0;
     for (int w = 0; w < nw; ++w) out[k] += sh.v[b][w][k];
   }
+  return true;
+}
+
+// L2 prefetch of the row segment of this lane for a later item: the line holding row
+// yb + lane, column x0 of image img (N x N floats), when columns x0 .. x0 + 31 lie
+// inside the image and pf (N % 4 == 0, 16-byte aligned image base) holds.
+__device__ __forceinline__ void prefetch_rows(const float* img, int N, int yb, int x0, bool pf) {
+  const int y = yb + (int)(threadIdx.x & 31);
+  if (pf && y < N && x0 + 32 <= N) tc::prefetch_l2_line(img + (size_t)y * N + x0);
+}
+
+// The sums of item j (slot j & 3) over nw warps into out[0 .. nv - 1], by lane 0 of the
+// warp that collects item j (false when the wait gave up). Item j is collected by warp
+// j % nw one item later, when every warp has normally stored its part, so that no warp
+// waits for the others in the common case.
+__device__ __forceinline__ bool collect2(const EpiSums<2>& sh, uint64_t* red_bar, int j, int nw,
+                                         volatile int* fail, int* err, int code, double* out,
+                                         int nv) {
+  double t[2];
+  if (!epi_take<2>(sh, tc::smem_u32(&red_bar[j & 3]), j & 3, (j >> 2) & 1, nw, fail, err, code,
+                   t))
+    return false;
+  out[0] = t[0];
+  if (nv > 1) out[1] = t[1];
   return true;
 }
 
@@ -231,18 +257,20 @@ int sm_count() {
 // =============================================================== tile analysis
 // The partials of launch_analysis_tc2 (same products, same order, same layout
 // part[image][yt][xt][row][c]) from a persistent pipeline:
-//   warps 0-7   load the image tile (theta -> mask for mode 1), split it into the
+//   warps 0-15  load the image tile (theta -> mask for mode 1), split it into the
 //               [hi | lo] operand sA;
-//   warp 12     (one thread) copies the TX tile (per xt) and the TY tile (per yt),
+//   warp 20     (one thread) copies the TX tile (per xt) and the TY tile (per yt),
 //               issues stage 1 R = sA . TX^T into accR[j & 1] and stage 2
 //               Q = TY . R^T into accQ[j & 1];
-//   warps 8-11  turn R into the stage-2 operand sR, and Q into the item's partials.
+//   warps 16-19 turn R into the stage-2 operand sR, and Q into the item's partials.
 // Shared memory: TY 64 KiB | sA 64 KiB | TX | sR (BN x 128 split tiles, BN <= 96).
 // Tensor memory: 512 columns, accR[b] at 128 b, accQ[b] at 256 + 128 b.
-constexpr int A3_LOADW = 8, A3_MMAW = 12;
-constexpr int A3_NT = 13 * 32;
+constexpr int A3_LOADW = 16, A3_MMAW = A3_LOADW + 4;
+constexpr int A3_NT = (A3_MMAW + 1) * 32;
+// chunks of 8 pixels per loader thread, rows between a thread's chunks
+constexpr int A3_CH = 2048 / (32 * A3_LOADW), A3_RS = 2 * A3_LOADW;
 
-template <int BN>
+template <int BN, int MODE>
 __global__ void __launch_bounds__(A3_NT, 1)
 analysis_tc3_kernel(Tc2Analysis a, int T, int B, const uint8_t* __restrict__ txImg,
                     const uint8_t* __restrict__ tyImg, int* __restrict__ err) {
@@ -290,19 +318,20 @@ analysis_tc3_kernel(Tc2Analysis a, int T, int B, const uint8_t* __restrict__ txI
     // ------------------------------------------------------------ loaders
     pdl_wait();
     const int tid = threadIdx.x;
-    // chunk i of a thread: row (tid >> 4) + 16 i, columns c8 .. c8 + 7 of the tile; its
-    // hi part at so + 2048 i of sA, its lo part 32 KiB further (sw128_offset)
+    // chunk i of a thread: row (tid >> 4) + A3_RS i, columns c8 .. c8 + 7 of the tile;
+    // its hi part at so + 128 A3_RS i of sA, its lo part 32 KiB further (sw128_offset)
     const int r0 = tid >> 4, c8 = (tid & 15) * 8;
     const uint32_t so = sw128_offset(128, r0, c8);
-    float v[8][8];
-    // chunks i0 .. i0 + 3 (rows 16 i0 .. 16 i0 + 63) of item j into v
+    constexpr int HALF = A3_CH / 2;
+    float v[A3_CH][8];
+    // chunks i0 .. i0 + HALF - 1 of item it into v
     auto load_half = [&](const Item& it, int i0) {
       const int m0 = it.yt * 128 + r0, x = it.xt * 128 + c8;
       const float* img = a.in + (size_t)it.z * a.N * a.N + (size_t)m0 * a.N + x;
 #pragma unroll
-      for (int i = i0; i < i0 + 4; ++i) {
-        const int m = m0 + 16 * i;
-        const float* pi = img + (size_t)(16 * i) * a.N;
+      for (int i = i0; i < i0 + HALF; ++i) {
+        const int m = m0 + A3_RS * i;
+        const float* pi = img + (size_t)(A3_RS * i) * a.N;
         if (a.vec4 && m < a.N && x + 7 < a.N) {
           const float4 p = __ldg(reinterpret_cast<const float4*>(pi));
           const float4 q = __ldg(reinterpret_cast<const float4*>(pi + 4));
@@ -322,8 +351,8 @@ analysis_tc3_kernel(Tc2Analysis a, int T, int B, const uint8_t* __restrict__ txI
                              : nullptr;
       const bool full = a.vec4 && it.yt * 128 + 127 < a.N && x + 7 < a.N;
 #pragma unroll
-      for (int i = i0; i < i0 + 4; ++i) {
-        const int m = m0 + 16 * i;
+      for (int i = i0; i < i0 + HALF; ++i) {
+        const int m = m0 + A3_RS * i;
         float u[8];
         if (full) {
           // every input is finite exactly when chk stays 0
@@ -331,11 +360,11 @@ analysis_tc3_kernel(Tc2Analysis a, int T, int B, const uint8_t* __restrict__ txI
 #pragma unroll
           for (int e = 0; e < 8; ++e) {
             chk = __fmaf_rn(v[i][e], 0.f, chk);
-            u[e] = a.mode == 1 ? 0.5f * (1.f + fast_cos(v[i][e])) : v[i][e];
+            u[e] = MODE == 1 ? 0.5f * (1.f + fast_cos(v[i][e])) : v[i][e];
           }
           bad |= chk != 0.f;
           if (mo) {
-            float* po = mo + (size_t)(16 * i) * a.N;
+            float* po = mo + (size_t)(A3_RS * i) * a.N;
             *reinterpret_cast<float4*>(po) = make_float4(u[0], u[1], u[2], u[3]);
             *reinterpret_cast<float4*>(po + 4) = make_float4(u[4], u[5], u[6], u[7]);
           }
@@ -345,9 +374,9 @@ analysis_tc3_kernel(Tc2Analysis a, int T, int B, const uint8_t* __restrict__ txI
             const bool in_range = m < a.N && x + e < a.N;
             u[e] = v[i][e];
             if (in_range) bad |= !isfinite(u[e]);
-            if (a.mode == 1) {
+            if (MODE == 1) {
               u[e] = in_range ? 0.5f * (1.f + fast_cos(u[e])) : 0.f;
-              if (mo && in_range) mo[(size_t)(16 * i) * a.N + e] = u[e];
+              if (mo && in_range) mo[(size_t)(A3_RS * i) * a.N + e] = u[e];
             }
           }
         }
@@ -356,23 +385,34 @@ analysis_tc3_kernel(Tc2Analysis a, int T, int B, const uint8_t* __restrict__ txI
         split_pair(u[2], u[3], h4.y, l4.y);
         split_pair(u[4], u[5], h4.z, l4.z);
         split_pair(u[6], u[7], h4.w, l4.w);
-        *reinterpret_cast<uint4*>(sA + so + 2048u * i) = h4;
-        *reinterpret_cast<uint4*>(sA + so + 32768u + 2048u * i) = l4;
+        *reinterpret_cast<uint4*>(sA + so + (uint32_t)(128 * A3_RS) * i) = h4;
+        *reinterpret_cast<uint4*>(sA + so + 32768u + (uint32_t)(128 * A3_RS) * i) = l4;
       }
     };
     // The loads run half an item ahead of the conversion: the second half of item j
     // loads while the first half converts, the first half of item j + 1 while the
     // second half of item j converts.
+    // the input tile of item i + 2 is fetched into L2 during item i: 512 segments of 128
+    // bytes, one per loader thread (row tid / 4, columns 32 (tid % 4) ..)
+    const bool pf = a.N % 4 == 0 && reinterpret_cast<uintptr_t>(a.in) % 16 == 0;
+    auto prefetch_item = [&](const Item& i) {
+      const int y = i.yt * 128 + (tid >> 2), x = i.xt * 128 + 32 * (tid & 3);
+      static_assert(A3_LOADW * 32 == 512, "one 128-byte segment per loader thread");
+      if (pf && y < a.N && x + 32 <= a.N)
+        tc::prefetch_l2_line(a.in + (size_t)i.z * a.N * a.N + (size_t)y * a.N + x);
+    };
     Item cur = item_at(lo, T, B);
     if (n > 0) load_half(cur, 0);
+    if (n > 1) prefetch_item(item_next(cur, T, B));
     for (int j = 0; j < n; ++j, cur = item_next(cur, T, B)) {
-      load_half(cur, 4);
+      if (j + 2 < n) prefetch_item(item_next(item_next(cur, T, B), T, B));
+      load_half(cur, HALF);
       // sA is free once stage 1 of the previous item has completed
       if (j > 0 && !pwait(bar(1 + ((j - 1) & 1)), ((j - 1) >> 1) & 1, vfail, err, 11)) break;
       bool bad = false;
       proc_half(cur, 0, bad);
       if (j + 1 < n) load_half(item_next(cur, T, B), 0);
-      proc_half(cur, 4, bad);
+      proc_half(cur, HALF, bad);
       if (bad) atomicOr(a.flag, 1);
       fence_async_smem();
       __syncwarp();
@@ -461,18 +501,24 @@ analysis_tc3_kernel(Tc2Analysis a, int T, int B, const uint8_t* __restrict__ txI
   if (warp == A3_MMAW) tc::tmem_dealloc(tmem, 512);
 }
 
-template <int BN>
-static cudaError_t analysis_tc3_t(cudaStream_t s, const Tc2Analysis& a, const void* tx,
+template <int BN, int MODE>
+static cudaError_t analysis_tc3_m(cudaStream_t s, const Tc2Analysis& a, const void* tx,
                                   const void* ty, int* err, int batch) {
   const size_t smem = 2 * (size_t)A2_A_BYTES + 2 * (size_t)s2_tile_bytes(BN, 128) + 1024;
-  cudaError_t e = cudaFuncSetAttribute(analysis_tc3_kernel<BN>,
+  cudaError_t e = cudaFuncSetAttribute(analysis_tc3_kernel<BN, MODE>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   const int T = (a.N + 127) / 128;
   const int items = T * T * batch;
   const int grid = items < sm_count() ? items : sm_count();
-  return launch_pdl(analysis_tc3_kernel<BN>, dim3(grid), dim3(A3_NT), smem, s, a, T, batch,
+  return launch_pdl(analysis_tc3_kernel<BN, MODE>, dim3(grid), dim3(A3_NT), smem, s, a, T, batch,
                     static_cast<const uint8_t*>(tx), static_cast<const uint8_t*>(ty), err);
+}
+template <int BN>
+static cudaError_t analysis_tc3_t(cudaStream_t s, const Tc2Analysis& a, const void* tx,
+                                  const void* ty, int* err, int batch) {
+  return a.mode == 1 ? analysis_tc3_m<BN, 1>(s, a, tx, ty, err, batch)
+                     : analysis_tc3_m<BN, 0>(s, a, tx, ty, err, batch);
 }
 
 bool tc3_analysis_supported(int ncols, int nr) {
@@ -610,12 +656,27 @@ synth_tc3_kernel(const uint8_t* __restrict__ Aimg, const uint8_t* __restrict__ B
       }
     };
     Item it = item_at(lo, T, B);
+    // the input rows of item i + 2 are fetched into L2 during item i
+    const bool pf = src && N % 4 == 0 && reinterpret_cast<uintptr_t>(src) % 16 == 0;
+    auto prefetch_item = [&](const Item& i) {
+      prefetch_rows(src + (size_t)i.z * N * N, N, i.yt * 128 + 32 * h, i.xt * 128 + 32 * q, pf);
+    };
     if (src && n > 0) {
       load_rows(it, 0);
       load_rows(it, 16);
     }
-    for (int j = 0; j < n; ++j, it = item_next(it, T, B)) {
+    if (n > 1) prefetch_item(item_next(it, T, B));
+    const bool sums = KIND == 0 ? g.theta != nullptr : r.p.mode == 1;
+    // the partial sums of item i: the squared norm (KIND 0) or the two loss terms
+    auto sums_out = [&](const Item& i) {
+      const size_t bid = ((size_t)i.z * T + i.yt) * T + i.xt;
+      return KIND == 0 ? g.norm_partial + bid : r.p.loss_partial + 2 * bid;
+    };
+    Item ip = it;   // item j - 1
+    int done = 0;   // items finished
+    for (int j = 0; j < n; ++j, ip = it, it = item_next(it, T, B)) {
       const Item nxt = item_next(it, T, B);
+      if (j + 2 < n) prefetch_item(item_next(nxt, T, B));
       const int x = it.xt * 128 + 32 * q + lane;
       const int yb = it.yt * 128 + 32 * h;
       const bool xin = x < N;
@@ -670,24 +731,19 @@ synth_tc3_kernel(const uint8_t* __restrict__ Aimg, const uint8_t* __restrict__ B
       };
       rows(0);
       rows(16);
-      const bool sums = KIND == 0 ? g.theta != nullptr : r.p.mode == 1;
       if (sums) {
         const double v[2] = {(double)s0, (double)s1};
-        const uint32_t rb = tc::smem_u32(&red_bar[j & 3]);
-        epi_put<2>(red, rb, j & 3, v);
-        double t[2];
-        if (threadIdx.x == 0 &&
-            epi_take<2>(red, rb, j & 3, (j >> 2) & 1, S3_EPIW, vfail, err, 27, t)) {
-          const size_t bid = ((size_t)it.z * T + it.yt) * T + it.xt;
-          if (KIND == 0) {
-            g.norm_partial[bid] = t[0];
-          } else {
-            r.p.loss_partial[2 * bid] = t[0];
-            r.p.loss_partial[2 * bid + 1] = t[1];
-          }
-        }
+        epi_put<2>(red, tc::smem_u32(&red_bar[j & 3]), j & 3, v);
+        // the sums of item j - 1, by one warp in turn
+        if (j > 0 && lane == 0 && warp == (j - 1) % S3_EPIW &&
+            !collect2(red, red_bar, j - 1, S3_EPIW, vfail, err, 27, sums_out(ip), KIND == 0 ? 1 : 2))
+          break;
       }
+      done = j + 1;
     }
+    // the sums of the last item
+    if (sums && n > 0 && done == n && lane == 0 && warp == (n - 1) % S3_EPIW)
+      collect2(red, red_bar, n - 1, S3_EPIW, vfail, err, 28, sums_out(ip), KIND == 0 ? 1 : 2);
   } else if (warp == S3_MMAW && lane == 0) {
     // ------------------------------------------------------------ MMA thread
     // the band operand image is written by the previous kernel of the stream
@@ -867,9 +923,16 @@ fused_tc3_kernel(const uint8_t* __restrict__ Aimg, const uint8_t* __restrict__ B
         for (int e = 0; e < 32; ++e) pre[e] = (x < N && yb + e < N) ? __ldg(tp + e * N) : 0.f;
       }
     };
+    // the target rows of item i + 2 are fetched into L2 during item i
+    const bool pf = N % 4 == 0 && reinterpret_cast<uintptr_t>(r.p.target) % 16 == 0;
     Item it = item_at(lo, T, B), ip = it;   // items j and j - 1
     if (n > 0) prefetch(it);
     for (int j = 0; j < n; ++j, ip = it, it = item_next(it, T, B)) {
+      if (j + 2 < n) {
+        const Item i2 = item_next(item_next(it, T, B), T, B);
+        prefetch_rows(r.p.target + (size_t)i2.z * N * N, N, i2.yt * 128 + 32 * h,
+                      i2.xt * 128 + lane_base, pf);
+      }
       const int x = it.xt * 128 + xl, yb = it.yt * 128 + 32 * h;
       const bool xin = x < N;
       const size_t base = (size_t)it.z * N * N;

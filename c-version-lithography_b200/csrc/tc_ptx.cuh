@@ -45,6 +45,11 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
   }
   return true;
 }
+// A hint to fetch the cache line holding src (global memory) into L2: no registers, no
+// scoreboard, nothing cached in L1.
+__device__ __forceinline__ void prefetch_l2_line(const void* src) {
+  asm volatile("prefetch.global.L2 [%0];" ::"l"(src));
+}
 __device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes,
                                          uint32_t bar) {
   asm volatile(
