@@ -727,7 +727,10 @@ def run_ours(args):
                      "traffic": traffic, "algorithmic_bytes": sb[dom], "avg_launch_ms": avg_ms},
         "stages_ms_per_step": {k: v[0] / max(v[1], 1) for k, v in stages.items() if v[1]},
         "latency_ms": {"p50": float(np.percentile(R["times"], 50)),
-                       "p99": float(np.percentile(R["times"], 99))},
+                       "p99": float(np.percentile(R["times"], 99)),
+                       "min": float(min(R["times"])), "max": float(max(R["times"])),
+                       "steps_over_1.5x_median": int(sum(
+                           t > 1.5 * float(np.percentile(R["times"], 50)) for t in R["times"]))},
         "precision_modes": {m: {"value": job_throughput(world, args.steps * runs[m]["tiles"],
                                                         runs[m]["total_ms"]),
                                 "ms_per_step": runs[m]["total_ms"] / args.steps,
@@ -768,9 +771,9 @@ def run_ours(args):
         "basis": "(16K+12) N^2 Nk + (16K+16) N Nk^2 per tile-iteration (per-kernel pruned "
                  "band DFTs, complex MAC = 8 FLOPs); not executed here"}
     out["config"]["launch"] = (
-        "direct kernel launches (PDL), each kernel covering the whole batch" if tiles > 1 else
         "direct kernel launches (PDL)" if args.no_graphs else
-        "CUDA graph replay of the evaluation chain (PDL edges)")
+        "CUDA graph replay of the evaluation chain (PDL edges)") + (
+        ", each kernel covering the whole batch" if tiles > 1 else "")
     if "fp32" in runs and "bf16x3" in runs:
         pm = out["precision_modes"]
         # precision alone: both single-tile chains (CUDA-graph replay)

@@ -231,6 +231,7 @@ int litho_ctx_destroy(litho_ctx* ctx) {
   if (ctx->h_red) cudaFreeHost(ctx->h_red);
   if (ctx->host_stage.base) cudaFree(ctx->host_stage.base);
   if (ctx->eval_graph) cudaGraphExecDestroy(ctx->eval_graph);
+  if (ctx->batch_graph) cudaGraphExecDestroy(ctx->batch_graph);
   for (cudaEvent_t e : ctx->ev_aux)
     if (e) cudaEventDestroy(e);
   if (ctx->aux) cudaStreamDestroy(ctx->aux);
@@ -267,10 +268,13 @@ int litho_ctx_enable_graphs(litho_ctx* ctx, int on) {
   if (!ctx) return LITHO_ERR_INVALID_ARGUMENT;
   ctx->graphs = on != 0;
   ctx->eval_last_valid = false;
-  if (!ctx->graphs && ctx->eval_graph) {
+  ctx->batch_last_valid = false;
+  if (!ctx->graphs && (ctx->eval_graph || ctx->batch_graph)) {
     cudaStreamSynchronize(ctx->stream);
-    cudaGraphExecDestroy(ctx->eval_graph);
+    if (ctx->eval_graph) cudaGraphExecDestroy(ctx->eval_graph);
+    if (ctx->batch_graph) cudaGraphExecDestroy(ctx->batch_graph);
     ctx->eval_graph = nullptr;
+    ctx->batch_graph = nullptr;
   }
   return LITHO_OK;
 }
@@ -1144,8 +1148,61 @@ int litho_ctm_evaluate_batch(litho_ctx* ctx, const litho_cache* cache, int batch
   int st = prepare(ctx, *cache, &L, batch);
   if (st) return st;
   double* d_sums = ctx->d_red + RED_PART + 3 * (size_t)L.tiles * batch;
-  st = ctm_batch_chain(ctx, *cache, L, batch, d_theta, d_target, threshold, alpha, d_grad_theta,
-                       d_sums);
+  auto chain = [&]() {
+    return ctm_batch_chain(ctx, *cache, L, batch, d_theta, d_target, threshold, alpha,
+                           d_grad_theta, d_sums);
+  };
+  // Repeated calls on the same buffers replay a CUDA graph of the chain (captured on
+  // the second consecutive call with the same key), as the single-image evaluation does.
+  EvalKey key;
+  const void* ptrs[16] = {cache, d_theta, d_target, d_grad_theta, ctx->scratch.base, ctx->d_red,
+                          cache->H, cache->AYD_img, cache->TXS_img, cache->TXD_img,
+                          reinterpret_cast<const void*>((uintptr_t)batch),
+                          reinterpret_cast<const void*>(
+                              (uintptr_t)ctx->precision | ((uintptr_t)ctx->tc_persistent() << 4) |
+                              ((uintptr_t)ctx->band_width(g.N, batch) << 8))};
+  for (int i = 0; i < 16; ++i) key.ptr[i] = ptrs[i];
+  const int geom[6] = {g.N, g.K, g.Nr, g.Nc, g.row0, g.col0};
+  for (int i = 0; i < 6; ++i) key.geom[i] = geom[i];
+  key.thr = threshold;
+  key.alpha = alpha;
+  const bool graphable = ctx->graphs && !ctx->timing && ctx->stream != nullptr &&
+                         ctx->stream != cudaStreamLegacy;   // the legacy stream cannot be captured
+  if (graphable && ctx->batch_graph && key == ctx->batch_graph_key) {
+    LITHO_CUDA_TRY(ctx, cudaGraphLaunch(ctx->batch_graph, ctx->stream));
+    ctx->launches += ctx->batch_graph_launches;
+  } else if (graphable && ctx->batch_last_valid && key == ctx->batch_last_key) {
+    if (ctx->batch_graph) {
+      cudaGraphExecDestroy(ctx->batch_graph);
+      ctx->batch_graph = nullptr;
+    }
+    const long long launches0 = ctx->launches;
+    cudaGraph_t graph = nullptr;
+    bool captured = false;
+    if (cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+      st = chain();
+      const cudaError_t e = cudaStreamEndCapture(ctx->stream, &graph);
+      captured = st == LITHO_OK && e == cudaSuccess && graph &&
+                 cudaGraphInstantiate(&ctx->batch_graph, graph, 0) == cudaSuccess;
+      if (graph) cudaGraphDestroy(graph);
+    }
+    cudaGetLastError();
+    if (captured) {
+      ctx->batch_graph_key = key;
+      ctx->batch_graph_launches = ctx->launches - launches0;
+      LITHO_CUDA_TRY(ctx, cudaGraphLaunch(ctx->batch_graph, ctx->stream));
+    } else {
+      // Capture is not available here: launch the chain directly.
+      if (ctx->batch_graph) cudaGraphExecDestroy(ctx->batch_graph);
+      ctx->batch_graph = nullptr;
+      ctx->launches = launches0;
+      st = chain();
+    }
+  } else {
+    st = chain();
+  }
+  ctx->batch_last_key = key;
+  ctx->batch_last_valid = graphable;
   std::vector<double> sums(3 * (size_t)batch);
   if (!st)
     LITHO_CUDA_TRY(ctx, cudaMemcpyAsync(sums.data(), d_sums, sums.size() * sizeof(double),
@@ -1611,8 +1668,9 @@ int litho_ctx_autotune(litho_ctx* ctx, const litho_cache* cache, int batch, int 
   };
   int st = LITHO_OK;
   if (cache) {
-    // Chunk width of the small-grid field and Z kernels (the results do not depend on
-    // it): the forward and adjoint band stages of `batch` images, on zeroed inputs.
+    // Schedule of the small-grid field and Z kernels (8- or 16-column chunks, or the
+    // whole small grid per CTA; the results do not depend on it): the forward and
+    // adjoint band stages of `batch` images, on zeroed inputs.
     Layout L;
     st = prepare(ctx, *cache, &L, batch, true);
     if (!st) LITHO_CUDA_TRY(ctx, cudaMemsetAsync(ctx->scratch.base, 0, L.total, s));
@@ -1623,7 +1681,7 @@ int litho_ctx_autotune(litho_ctx* ctx, const litho_cache* cache, int batch, int 
     f.mband = at<float2>(ctx, L.fm);
     float best = 0.f;
     int bw = 0;
-    for (const int w : {8, 16}) {
+    for (const int w : {8, 16, BW_WHOLE}) {
       if (st) break;
       float ms = 0.f;
       st = timed([&]() -> cudaError_t {

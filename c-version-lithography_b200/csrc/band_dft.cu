@@ -494,6 +494,88 @@ band_fields_kernel(const float2* __restrict__ H, const float2* __restrict__ mban
   }
 }
 
+// C = A B over operands in shared memory: each thread owns an RT x 2 block of C (rows
+// m0 .. m0 + RT - 1, columns 2p and 2p + 1) and adds the terms in k order with cfma,
+// the operand order and summation order of the chunked kernels, so every element is
+// bit-identical to theirs. Work items run pair-fastest: a warp's B loads are adjacent
+// 16-byte words and its A loads mostly one broadcast address. a(m, k) returns A[m][k];
+// B[k][n] is at B + k ldb + n (ldb even, B 16-byte aligned).
+template <int RT, int NT, class ALoad, class Store>
+__device__ __forceinline__ void cgemm_rt2(int M, int npairs, int Kd, ALoad a,
+                                          const float2* __restrict__ B, int ldb, Store store) {
+  const int rblocks = (M + RT - 1) / RT;
+  for (int it = threadIdx.x; it < rblocks * npairs; it += NT) {
+    const int m0 = (it / npairs) * RT, p = it % npairs;
+    float2 acc[RT][2];
+#pragma unroll
+    for (int i = 0; i < RT; ++i) acc[i][0] = acc[i][1] = make_float2(0.f, 0.f);
+    for (int k = 0; k < Kd; ++k) {
+      const float4 b = *reinterpret_cast<const float4*>(B + (size_t)k * ldb + 2 * p);
+      const float2 b0 = make_float2(b.x, b.y), b1 = make_float2(b.z, b.w);
+#pragma unroll
+      for (int i = 0; i < RT; ++i) {
+        const float2 av = a(min(m0 + i, M - 1), k);
+        cfma(acc[i][0], av, b0);
+        cfma(acc[i][1], av, b1);
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < RT; ++i) {
+      if (m0 + i < M) {
+        store(m0 + i, 2 * p, acc[i][0]);
+        store(m0 + i, 2 * p + 1, acc[i][1]);
+      }
+    }
+  }
+}
+
+// Forward 1, whole small grid per CTA: grid (K, 1, batch), CTA (k, b) computes all of
+// e_k = ESr (A ESc^T) (Pr x Pc) and ik = w_k |e_k|^2 for image b, every table staged
+// once per CTA instead of once per column chunk. Same arithmetic as
+// band_fields_kernel (bit-identical results), register-blocked: 5 rows x 2 columns of
+// T and 10 rows x 2 columns of e_k per thread.
+constexpr int BG_NT = 256;
+__global__ void __launch_bounds__(BG_NT)
+band_fields_whole_kernel(const float2* __restrict__ H, const float2* __restrict__ mband,
+                         const float* __restrict__ w, int Nr, int Nc, int Pr, int Pc,
+                         const float2* __restrict__ ESc_t, const float2* __restrict__ ESr_t,
+                         float2* __restrict__ e, float* __restrict__ ik) {
+  extern __shared__ __align__(16) float2 sm2[];
+  const int k = blockIdx.x;
+  {  // image b of a batch
+    const size_t b = blockIdx.z;
+    mband += b * Nr * Nc;
+    e += b * gridDim.x * Pr * Pc;
+    ik += b * gridDim.x * Pr * Pc;
+  }
+  float2* esc = sm2;                    // [Nc][Pc]
+  float2* esr = esc + Nc * Pc;          // [Nr][Pr]
+  float2* T = esr + Nr * Pr;            // [Nr][Pc]
+  float2* A = T + Nr * Pc;              // [Nr][Nc]
+  pdl_trigger();
+  fill_batched<BG_NT>(esc, Nc * Pc, [&](int i) { return ESc_t[i]; });
+  fill_batched<BG_NT>(esr, Nr * Pr, [&](int i) { return ESr_t[i]; });
+  pdl_wait();
+  fill_batched<BG_NT>(A, Nr * Nc, [&](int i) { return cmul(H[(size_t)k * Nr * Nc + i], mband[i]); });
+  __syncthreads();
+  cgemm_rt2<5, BG_NT>(Nr, Pc / 2, Nc, [&](int r, int c) { return A[r * Nc + c]; }, esc, Pc,
+                      [&](int r, int j, float2 v) { T[r * Pc + j] = v; });
+  __syncthreads();
+  const float wk = w[k];
+  float2* ek = e + (size_t)k * Pr * Pc;
+  float* ikk = ik + (size_t)k * Pr * Pc;
+  cgemm_rt2<10, BG_NT>(Pr, Pc / 2, Nr, [&](int jr, int r) { return esr[r * Pr + jr]; }, T, Pc,
+                       [&](int jr, int j, float2 v) {
+                         const size_t o = (size_t)jr * Pc + j;
+                         ek[o] = v;
+                         ikk[o] = wk * (v.x * v.x + v.y * v.y);
+                       });
+}
+
+static size_t fields_whole_smem(const BandGeom& g) {
+  return (size_t)(g.Nc * g.Pc + g.Nr * g.Pr + g.Nr * g.Pc + g.Nr * g.Nc) * sizeof(float2);
+}
+
 template <int W>
 static size_t fields_smem(const BandGeom& g, bool staged) {
   return (size_t)(even_up(g.Nr * g.Nc) + g.Nr * W + g.Nc * W + (staged ? g.Nr * g.Pr : 0)) *
@@ -576,6 +658,96 @@ band_chat_kernel(const float* __restrict__ iP, int Nr, int Nc, int Pr, int Pc,
     a = split_sum<SPLIT>(a);
     if (dc < nd && sub == 0) chat[(size_t)dr * nd + dc] = make_float2(a.x * inv, a.y * inv);
   }
+}
+
+// Four interleaved partial sums added as (0 + 1) + (2 + 3): the order split_sum<4>
+// gives the lane sums of the per-row kernels.
+__device__ __forceinline__ float2 sum4(const float2 (&a)[4]) {
+  return make_float2((a[0].x + a[1].x) + (a[2].x + a[3].x), (a[0].y + a[1].y) + (a[2].y + a[3].y));
+}
+
+// Forward 3 with BC_DR band rows per CTA: grid (ceil(Nr / BC_DR), batch). The tables and
+// the image's small-grid intensity are staged once per BC_DR rows instead of once per
+// row; one thread per pair of outputs keeps the four interleaved partial sums of
+// band_chat_kernel and adds them in its order, so the results are bit-identical.
+constexpr int BC_DR = 5;
+__global__ void __launch_bounds__(256)
+band_chat_rows_kernel(const float* __restrict__ iP, int Nr, int Nc, int Pr, int Pc,
+                      const float2* __restrict__ EDr_t, const float2* __restrict__ EDc, float inv,
+                      float2* __restrict__ chat) {
+  extern __shared__ __align__(16) float2 sb[];
+  const int nd = 2 * Nc - 1, ndE = even_up(nd);
+  const int dr0 = blockIdx.x * BC_DR, nr = min(BC_DR, Nr - dr0);
+  iP += (size_t)blockIdx.y * Pr * Pc;   // image b of a batch
+  chat += (size_t)blockIdx.y * Nr * nd;
+  float2* edc = sb;                                    // [Pc][ndE] (column nd zero)
+  float2* ed = edc + Pc * ndE;                         // [BC_DR][Pr]
+  float2* V = ed + BC_DR * Pr;                         // [BC_DR][Pc]
+  float* ip = reinterpret_cast<float*>(V + BC_DR * Pc);  // [Pr][Pc]
+  pdl_trigger();
+  fill_batched<256>(ed, nr * Pr, [&](int i) {
+    return EDr_t[(size_t)(dr0 + i / Pr + Nr - 1) * Pr + i % Pr];
+  });
+  fill_batched<256>(edc, Pc * ndE, [&](int i) {
+    const int jc = i / ndE, dc = i % ndE;
+    return dc < nd ? EDc[(size_t)jc * nd + dc] : make_float2(0.f, 0.f);
+  });
+  pdl_wait();
+  fill_batched<256>(ip, Pr * Pc, [&](int i) { return iP[i]; });
+  __syncthreads();
+  // V[r][jc] = sum_jr conj(ed[r][jr]) ip[jr][jc], two columns per thread.
+  const int pc2 = Pc / 2;
+  for (int it = threadIdx.x; it < nr * pc2; it += 256) {
+    const int r = it / pc2, jc = 2 * (it % pc2);
+    float2 a0[4], a1[4];
+#pragma unroll
+    for (int s = 0; s < 4; ++s) a0[s] = a1[s] = make_float2(0.f, 0.f);
+    for (int jr0 = 0; jr0 < Pr; jr0 += 4) {
+#pragma unroll
+      for (int s = 0; s < 4; ++s) {
+        const int jr = jr0 + s;
+        if (jr < Pr) {
+          const float2 e = ed[r * Pr + jr];
+          const float2 i2 = *reinterpret_cast<const float2*>(ip + jr * Pc + jc);
+          a0[s].x = fmaf(e.x, i2.x, a0[s].x); a0[s].y = fmaf(-e.y, i2.x, a0[s].y);
+          a1[s].x = fmaf(e.x, i2.y, a1[s].x); a1[s].y = fmaf(-e.y, i2.y, a1[s].y);
+        }
+      }
+    }
+    V[r * Pc + jc] = sum4(a0);
+    V[r * Pc + jc + 1] = sum4(a1);
+  }
+  __syncthreads();
+  // chat[dr][dc] = inv sum_jc V[r][jc] conj(EDc[jc][dc]), two outputs per thread.
+  const int nd2 = ndE / 2;
+  for (int it = threadIdx.x; it < nr * nd2; it += 256) {
+    const int r = it / nd2, dc = 2 * (it % nd2);
+    float2 a0[4], a1[4];
+#pragma unroll
+    for (int s = 0; s < 4; ++s) a0[s] = a1[s] = make_float2(0.f, 0.f);
+    for (int jc0 = 0; jc0 < Pc; jc0 += 4) {
+#pragma unroll
+      for (int s = 0; s < 4; ++s) {
+        const int jc = jc0 + s;
+        if (jc < Pc) {
+          const float2 v = V[r * Pc + jc];
+          const float4 t = *reinterpret_cast<const float4*>(edc + jc * ndE + dc);
+          cfma(a0[s], v, make_float2(t.x, -t.y));
+          cfma(a1[s], v, make_float2(t.z, -t.w));
+        }
+      }
+    }
+    const float2 c0 = sum4(a0), c1 = sum4(a1);
+    float2* out = chat + (size_t)(dr0 + r) * nd;
+    out[dc] = make_float2(c0.x * inv, c0.y * inv);
+    if (dc + 1 < nd) out[dc + 1] = make_float2(c1.x * inv, c1.y * inv);
+  }
+}
+
+static size_t chat_rows_smem(const BandGeom& g) {
+  const int ndE = even_up(2 * g.Nc - 1);
+  return (size_t)(g.Pc * ndE + BC_DR * g.Pr + BC_DR * g.Pc) * sizeof(float2) +
+         (size_t)g.Pr * g.Pc * sizeof(float);
 }
 
 static size_t chat_smem(const BandGeom& g) {
@@ -697,6 +869,124 @@ expand_kernel(const float2* __restrict__ coef, int nrows, int ncoef, int ld,
   expand_store<PAIRS>(cf, ph, nrows, ncoef, N, mode, kp, a0, x0, Ut, img, img_tile_bytes);
 }
 
+// The expansion with every band row of an x strip in one CTA (up to 64 rows): all 256
+// threads stage the tables, then thread (xp, rg), rg < ceil(nrows / 8), computes image
+// rows x0 + 2 xp and x0 + 2 xp + 1 for the eight band rows 8 rg .. 8 rg + 7, so each
+// step over c takes one 16-byte phase load and four 16-byte
+// broadcast coefficient loads for 16 complex FMAs. Coefficients are staged transposed
+// (cfT[c][8 groups]); rows past nrows are zero. Same operands, order and scale as
+// expand_store: bit-identical results.
+constexpr int EXR_X = 64, EXR_NT = 256;
+__global__ void __launch_bounds__(EXR_NT)
+expand_rows_kernel(const float2* __restrict__ coef, int nrows, int ncoef, int ld,
+                   const float2* __restrict__ TX, int N, int mode, int nc, int kp,
+                   float* __restrict__ Ut, uint8_t* __restrict__ img, uint32_t img_tile_bytes) {
+  extern __shared__ __align__(16) float2 sr[];
+  const int groups = (nrows + 7) / 8, R = 8 * groups;
+  float2* ph = sr;                    // [ncoef][EXR_X]
+  float2* cfT = sr + ncoef * EXR_X;   // [ncoef][R]
+  const int x0 = blockIdx.x * EXR_X;
+  {  // image b of a batch
+    const size_t b = blockIdx.z;
+    coef += b * nrows * ld;
+    if (img) img += b * ((N + 127) / 128) * (size_t)img_tile_bytes;
+    else Ut += b * N * kp;
+  }
+  pdl_trigger();
+  fill_batched<EXR_NT>(ph, ncoef * EXR_X, [&](int i) {
+    const int c = i / EXR_X, x = x0 + i % EXR_X;
+    float2 t = make_float2(0.f, 0.f);
+    if (x < N) {
+      if (mode == 0) {
+        t = conjf2(TX[(size_t)c * N + x]);
+      } else {
+        const int d = c - (nc - 1);
+        t = d >= 0 ? conjf2(TX[(size_t)d * N + x]) : TX[(size_t)(-d) * N + x];
+      }
+    }
+    return t;
+  });
+  pdl_wait();
+  // cfT[c][r] = coef[r][c]: a coalesced read of coef, a transposed shared store.
+  for (int base = threadIdx.x; base < R * ncoef; base += EXR_NT * 8) {
+    float2 v[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int i = base + q * EXR_NT, r = i / ncoef;
+      if (i < R * ncoef) v[q] = r < nrows ? coef[(size_t)r * ld + i % ncoef] : make_float2(0.f, 0.f);
+    }
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int i = base + q * EXR_NT;
+      if (i < R * ncoef) cfT[(i % ncoef) * R + i / ncoef] = v[q];
+    }
+  }
+  __syncthreads();
+  const int xp = threadIdx.x % 32, rg = threadIdx.x / 32;
+  if (rg >= groups) return;   // staging helpers only
+  float2 acc[8][2];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) acc[i][0] = acc[i][1] = make_float2(0.f, 0.f);
+  for (int c = 0; c < ncoef; ++c) {
+    const float4 p = *reinterpret_cast<const float4*>(ph + c * EXR_X + 2 * xp);
+    const float2 p0 = make_float2(p.x, p.y), p1 = make_float2(p.z, p.w);
+    const float4* cq = reinterpret_cast<const float4*>(cfT + c * R + 8 * rg);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const float4 a = cq[q];
+      const float2 a0 = make_float2(a.x, a.y), a1 = make_float2(a.z, a.w);
+      cfma(acc[2 * q][0], a0, p0);
+      cfma(acc[2 * q][1], a0, p1);
+      cfma(acc[2 * q + 1][0], a1, p0);
+      cfma(acc[2 * q + 1][1], a1, p1);
+    }
+  }
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int x = x0 + 2 * xp + h;
+    if (x >= N) continue;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int ra = 8 * rg + 2 * q, rb = ra + 1;
+      const float ka = ra < nrows ? ((mode == 1 && ra > 0) ? 2.f : 1.f) : 0.f;
+      const float kb = rb < nrows ? ((mode == 1 && rb > 0) ? 2.f : 1.f) : 0.f;
+      const float4 v = make_float4(ka * acc[2 * q][h].x, ka * acc[2 * q][h].y,
+                                   kb * acc[2 * q + 1][h].x, kb * acc[2 * q + 1][h].y);
+      const int f0 = 2 * ra;
+      if (f0 >= kp) continue;
+      if (img) {
+        uint8_t* tile = img + (size_t)(x / 128) * img_tile_bytes;
+        const __nv_bfloat162 h01 = __floats2bfloat162_rn(v.x, v.y);
+        const __nv_bfloat162 h23 = __floats2bfloat162_rn(v.z, v.w);
+        const float2 f01 = __bfloat1622float2(h01), f23 = __bfloat1622float2(h23);
+        const __nv_bfloat162 l01 = __floats2bfloat162_rn(v.x - f01.x, v.y - f01.y);
+        const __nv_bfloat162 l23 = __floats2bfloat162_rn(v.z - f23.x, v.w - f23.y);
+        uint2 hw, lw;
+        hw.x = *reinterpret_cast<const uint32_t*>(&h01);
+        hw.y = *reinterpret_cast<const uint32_t*>(&h23);
+        lw.x = *reinterpret_cast<const uint32_t*>(&l01);
+        lw.y = *reinterpret_cast<const uint32_t*>(&l23);
+        *reinterpret_cast<uint2*>(tile + sw128_offset(128, x % 128, f0)) = hw;
+        *reinterpret_cast<uint2*>(tile + sw128_offset(128, x % 128, kp + f0)) = lw;
+      } else {
+        *reinterpret_cast<float4*>(Ut + (size_t)x * kp + f0) = v;
+      }
+    }
+    // Columns past the last row group are zero.
+    if (rg == 0) {
+      for (int f = 2 * R; f < kp; f += 4) {
+        if (img) {
+          uint8_t* tile = img + (size_t)(x / 128) * img_tile_bytes;
+          *reinterpret_cast<uint2*>(tile + sw128_offset(128, x % 128, f)) = make_uint2(0u, 0u);
+          *reinterpret_cast<uint2*>(tile + sw128_offset(128, x % 128, kp + f)) = make_uint2(0u, 0u);
+        } else {
+          *reinterpret_cast<float4*>(Ut + (size_t)x * kp + f) = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+      }
+    }
+  }
+}
+
 template <int PAIRS>
 static cudaError_t launch_expand_t(cudaStream_t s, const float2* coef, int nrows, int ncoef,
                                    int ld, const float2* TX, int N, int mode, int nc, int kp,
@@ -718,8 +1008,29 @@ static cudaError_t launch_expand_t(cudaStream_t s, const float2* coef, int nrows
 static cudaError_t launch_expand(cudaStream_t s, const float2* coef, int nrows, int ncoef, int ld,
                                  const float2* TX, int N, int mode, int nc, int kp, float* Ut,
                                  void* img, int batch) {
+  if (batch >= 8 && nrows <= 64) {
+    // Every band row of an x strip in one CTA (enough CTAs from 8 images on).
+    const int R = 8 * ((nrows + 7) / 8);
+    const uint32_t img_tile_bytes = (uint32_t)((2 * kp + 63) / 64) * 128u * 128u;
+    const size_t smem = (size_t)ncoef * (EXR_X + R) * sizeof(float2);
+    cudaError_t e = cudaFuncSetAttribute(expand_rows_kernel,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    return launch_pdl(expand_rows_kernel, dim3((N + EXR_X - 1) / EXR_X, 1, batch),
+                      dim3(EXR_NT), smem, s, coef, nrows, ncoef, ld, TX, N, mode, nc, kp, Ut,
+                      static_cast<uint8_t*>(img), img_tile_bytes);
+  }
   return batch >= 4 ? launch_expand_t<2>(s, coef, nrows, ncoef, ld, TX, N, mode, nc, kp, Ut, img, batch)
                     : launch_expand_t<1>(s, coef, nrows, ncoef, ld, TX, N, mode, nc, kp, Ut, img, batch);
+}
+
+static size_t z_whole_smem(const BandGeom& g);
+
+// Whole small grid per CTA (width BW_WHOLE, or by default from 8 images on) where both
+// whole-grid kernels' tables fit in shared memory.
+static bool band_whole(const BandGeom& g, int batch, int width) {
+  if (fields_whole_smem(g) > SMEM_STAGE || z_whole_smem(g) > SMEM_STAGE) return false;
+  return width > 0 ? width == BW_WHOLE : batch >= 8;
 }
 
 cudaError_t launch_band_forward(cudaStream_t s, const Cache& c, Field& f, float* ik, float* iP,
@@ -736,23 +1047,46 @@ cudaError_t launch_band_forward(cudaStream_t s, const Cache& c, Field& f, float*
                       sm1, s, c.H, static_cast<const float2*>(f.mband), c.w, g.Nr, g.Nc, g.Pr,
                       g.Pc, c.ESc_t, c.ESr_t, (int)staged, f.e, ik);
   };
-  // Chunk width: the autotuned one when set, else wide chunks for batches.
-  const bool wide = width > 0 ? width >= BW_BATCH : batch >= 4;
-  cudaError_t err = wide ? fields(std::integral_constant<int, BW_BATCH>{})
-                         : fields(std::integral_constant<int, BW_ONE>{});
+  // Schedule: the autotuned one when set, else the whole small grid per CTA for large
+  // batches (enough CTAs to fill the GPU) and column chunks otherwise.
+  cudaError_t err;
+  if (band_whole(g, batch, width)) {
+    const size_t smw = fields_whole_smem(g);
+    err = cudaFuncSetAttribute(band_fields_whole_kernel,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smw);
+    if (err == cudaSuccess)
+      err = launch_pdl(band_fields_whole_kernel, dim3(g.K, 1, batch), dim3(BG_NT), smw, s, c.H,
+                       static_cast<const float2*>(f.mband), c.w, g.Nr, g.Nc, g.Pr, g.Pc, c.ESc_t,
+                       c.ESr_t, f.e, ik);
+  } else {
+    const bool wide = width > 0 ? width >= BW_BATCH : batch >= 4;
+    err = wide ? fields(std::integral_constant<int, BW_BATCH>{})
+               : fields(std::integral_constant<int, BW_ONE>{});
+  }
   if (err != cudaSuccess) return err;
   const int n = g.Pr * g.Pc;
   err = launch_pdl(sum_k_kernel, dim3((n + 255) / 256, batch), dim3(256), 0, s,
                    static_cast<const float*>(ik), g.K, n, iP);
   if (err != cudaSuccess) return err;
   const int nd = 2 * g.Nc - 1;
-  const size_t smc = chat_smem(g);
-  err = cudaFuncSetAttribute(band_chat_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smc);
-  if (err != cudaSuccess) return err;
-  err = launch_pdl(band_chat_kernel, dim3(g.Nr, batch), dim3(BI_NT), smc, s,
-                   static_cast<const float*>(iP), g.Nr, g.Nc, g.Pr, g.Pc, c.EDr_t, c.EDc,
-                   1.f / ((float)g.Pr * (float)g.Pc), chat);
+  if (batch >= 4 && chat_rows_smem(g) <= SMEM_STAGE) {
+    // BC_DR band rows per CTA (bit-identical to one row per CTA) once a batch fills the GPU.
+    const size_t smc = chat_rows_smem(g);
+    err = cudaFuncSetAttribute(band_chat_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)smc);
+    if (err != cudaSuccess) return err;
+    err = launch_pdl(band_chat_rows_kernel, dim3((g.Nr + BC_DR - 1) / BC_DR, batch), dim3(256),
+                     smc, s, static_cast<const float*>(iP), g.Nr, g.Nc, g.Pr, g.Pc, c.EDr_t, c.EDc,
+                     1.f / ((float)g.Pr * (float)g.Pc), chat);
+  } else {
+    const size_t smc = chat_smem(g);
+    err = cudaFuncSetAttribute(band_chat_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)smc);
+    if (err != cudaSuccess) return err;
+    err = launch_pdl(band_chat_kernel, dim3(g.Nr, batch), dim3(BI_NT), smc, s,
+                     static_cast<const float*>(iP), g.Nr, g.Nc, g.Pr, g.Pc, c.EDr_t, c.EDc,
+                     1.f / ((float)g.Pr * (float)g.Pc), chat);
+  }
   if (err != cudaSuccess) return err;
   return launch_expand(s, chat, g.Nr, nd, nd, c.TXDc, g.N, 1, g.Nc, g.kp_rows, Ut, img, batch);
 }
@@ -803,6 +1137,78 @@ band_gamma_kernel(const float2* __restrict__ gh, int Nr, int Nc, int Pr, int Pc,
     acc = split_sum<SPLIT>(make_float2(acc, 0.f)).x;
     if (jc < Pc && sub == 0) gam[(size_t)jr * Pc + jc] = acc;
   }
+}
+
+// Adjoint 1 with BG_JR small-grid rows per CTA: grid (ceil(Pr / BG_JR), batch). The
+// tables and the image's g' are staged once per BG_JR rows; one thread per output (wv)
+// or pair of outputs (gamma) keeps the four interleaved partial sums of
+// band_gamma_kernel and adds them in its order, so the results are bit-identical.
+constexpr int BG_JR = 10;
+__global__ void __launch_bounds__(256)
+band_gamma_rows_kernel(const float2* __restrict__ gh, int Nr, int Nc, int Pr, int Pc,
+                       const float2* __restrict__ EDr_t, const float2* __restrict__ EDc_t,
+                       float* __restrict__ gam) {
+  extern __shared__ __align__(16) float2 sg[];
+  const int na = 2 * Nr - 1;
+  const int jr0 = blockIdx.x * BG_JR, nj = min(BG_JR, Pr - jr0);
+  gh += (size_t)blockIdx.y * na * Nc;   // image b of a batch
+  gam += (size_t)blockIdx.y * Pr * Pc;
+  float2* edc = sg;                  // [Nc][Pc] rows Nc-1 .. 2Nc-2 of EDc_t
+  float2* ghs = edc + Nc * Pc;       // [na][Nc]
+  float2* edr = ghs + na * Nc;       // [BG_JR][na]: EDr_t[a][jr0 + j]
+  float2* wv = edr + BG_JR * na;     // [BG_JR][Nc]
+  pdl_trigger();
+  fill_batched<256>(edr, nj * na, [&](int i) {
+    return EDr_t[(size_t)(i % na) * Pr + jr0 + i / na];
+  });
+  fill_batched<256>(edc, Nc * Pc, [&](int i) { return EDc_t[(size_t)(Nc - 1) * Pc + i]; });
+  pdl_wait();
+  fill_batched<256>(ghs, na * Nc, [&](int i) { return gh[i]; });
+  __syncthreads();
+  // wv[j][c] = kappa(c) sum_a EDr_t[a][jr] g'[a][c]
+  for (int it = threadIdx.x; it < nj * Nc; it += 256) {
+    const int j = it / Nc, c = it % Nc;
+    float2 a[4];
+#pragma unroll
+    for (int s = 0; s < 4; ++s) a[s] = make_float2(0.f, 0.f);
+    for (int r0 = 0; r0 < na; r0 += 4) {
+#pragma unroll
+      for (int s = 0; s < 4; ++s) {
+        const int r = r0 + s;
+        if (r < na) cfma(a[s], edr[j * na + r], ghs[r * Nc + c]);
+      }
+    }
+    const float2 v = sum4(a);
+    const float kc = c > 0 ? 2.f : 1.f;
+    wv[j * Nc + c] = make_float2(kc * v.x, kc * v.y);
+  }
+  __syncthreads();
+  // gamma[jr][jc] = Re sum_c wv[j][c] EDc_t[c + Nc - 1][jc], two columns per thread
+  const int pc2 = Pc / 2;
+  for (int it = threadIdx.x; it < nj * pc2; it += 256) {
+    const int j = it / pc2, jc = 2 * (it % pc2);
+    float a0[4] = {0.f, 0.f, 0.f, 0.f}, a1[4] = {0.f, 0.f, 0.f, 0.f};
+    for (int c0 = 0; c0 < Nc; c0 += 4) {
+#pragma unroll
+      for (int s = 0; s < 4; ++s) {
+        const int c = c0 + s;
+        if (c < Nc) {
+          const float2 w = wv[j * Nc + c];
+          const float4 t = *reinterpret_cast<const float4*>(edc + c * Pc + jc);
+          a0[s] = fmaf(w.x, t.x, fmaf(-w.y, t.y, a0[s]));
+          a1[s] = fmaf(w.x, t.z, fmaf(-w.y, t.w, a1[s]));
+        }
+      }
+    }
+    float* out = gam + (size_t)(jr0 + j) * Pc + jc;
+    out[0] = (a0[0] + a0[1]) + (a0[2] + a0[3]);
+    out[1] = (a1[0] + a1[1]) + (a1[2] + a1[3]);
+  }
+}
+
+static size_t gamma_rows_smem(const BandGeom& g) {
+  const int na = 2 * g.Nr - 1;
+  return (size_t)(g.Nc * g.Pc + na * g.Nc + BG_JR * na + BG_JR * g.Nc) * sizeof(float2);
 }
 
 static size_t gamma_smem(const BandGeom& g) {
@@ -899,6 +1305,56 @@ band_z_kernel(const float2* __restrict__ e, const float* __restrict__ gam, int N
   }
 }
 
+// Adjoint 2, whole small grid per CTA: grid (K, 1, batch), CTA (k, b) computes all of
+// Zk for image b, every table staged once. Same arithmetic as band_z_kernel
+// (bit-identical results); the band columns are padded to an even count with zero
+// table columns, whose outputs are not stored.
+__global__ void __launch_bounds__(BG_NT)
+band_z_whole_kernel(const float2* __restrict__ e, const float* __restrict__ gam, int Nr, int Nc,
+                    int Pr, int Pc, const float2* __restrict__ ESc,
+                    const float2* __restrict__ ESr_t, float inv, float2* __restrict__ Zk) {
+  extern __shared__ __align__(16) float2 sz[];
+  const int k = blockIdx.x;
+  const int NcE = even_up(Nc);
+  {  // image b of a batch
+    const size_t b = blockIdx.z;
+    e += b * gridDim.x * Pr * Pc;
+    gam += b * Pr * Pc;
+    Zk += b * gridDim.x * Nr * Nc;
+  }
+  float2* esc = sz;                   // [Pc][NcE]
+  float2* esr = esc + Pc * NcE;       // [Nr][Pr]
+  float2* q = esr + Nr * Pr;          // [Pr][Pc]
+  float2* Z1 = q + Pr * Pc;           // [Pr][NcE]
+  const float2* ek = e + (size_t)k * Pr * Pc;
+  pdl_trigger();
+  fill_batched<BG_NT>(esc, Pc * NcE, [&](int i) {
+    const int jc = i / NcE, u = i % NcE;
+    return u < Nc ? conjf2(ESc[(size_t)jc * Nc + u]) : make_float2(0.f, 0.f);
+  });
+  fill_batched<BG_NT>(esr, Nr * Pr, [&](int i) { return ESr_t[i]; });
+  pdl_wait();
+  fill_batched<BG_NT>(q, Pr * Pc, [&](int i) {
+    const float2 v = ek[i];
+    const float gv = gam[i];
+    return make_float2(v.x * gv, v.y * gv);
+  });
+  __syncthreads();
+  cgemm_rt2<5, BG_NT>(Pr, NcE / 2, Pc, [&](int jr, int jc) { return q[jr * Pc + jc]; }, esc, NcE,
+                      [&](int jr, int u, float2 v) { Z1[jr * NcE + u] = v; });
+  __syncthreads();
+  float2* zk = Zk + (size_t)k * Nr * Nc;
+  cgemm_rt2<3, BG_NT>(Nr, NcE / 2, Pr, [&](int ur, int jr) { return conjf2(esr[ur * Pr + jr]); },
+                      Z1, NcE, [&](int ur, int u, float2 v) {
+                        if (u < Nc) zk[(size_t)ur * Nc + u] = make_float2(v.x * inv, v.y * inv);
+                      });
+}
+
+static size_t z_whole_smem(const BandGeom& g) {
+  const int NcE = even_up(g.Nc);
+  return (size_t)(g.Pc * NcE + g.Nr * g.Pr + g.Pr * g.Pc + g.Pr * NcE) * sizeof(float2);
+}
+
 // Adjoint 3: X[u] = scale sum_k w_k conj(H_k(u)) Z_k(u). Four lanes per u: lane j
 // sums k = j, j + 4, ... in order (the loads of up to 8 of its k issued together),
 // then the four partial sums are added in a fixed order.
@@ -948,12 +1404,23 @@ cudaError_t launch_band_adjoint(cudaStream_t s, const Cache& c, const Field& f, 
                                 double scale, float* gam, float2* Zk, float2* X, float* Vt,
                                 void* img, int batch, int width) {
   const BandGeom& g = c.g;
-  const size_t smg = gamma_smem(g);
-  cudaError_t e0 = cudaFuncSetAttribute(band_gamma_kernel,
-                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smg);
-  if (e0 != cudaSuccess) return e0;
-  e0 = launch_pdl(band_gamma_kernel, dim3(g.Pr, batch), dim3(256), smg, s, gh, g.Nr, g.Nc, g.Pr, g.Pc,
-                  c.EDr_t, c.EDc_t, gam);
+  cudaError_t e0;
+  if (batch >= 4 && gamma_rows_smem(g) <= SMEM_STAGE) {
+    // BG_JR small-grid rows per CTA (bit-identical to one row per CTA) for batches.
+    const size_t smg = gamma_rows_smem(g);
+    e0 = cudaFuncSetAttribute(band_gamma_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)smg);
+    if (e0 != cudaSuccess) return e0;
+    e0 = launch_pdl(band_gamma_rows_kernel, dim3((g.Pr + BG_JR - 1) / BG_JR, batch), dim3(256),
+                    smg, s, gh, g.Nr, g.Nc, g.Pr, g.Pc, c.EDr_t, c.EDc_t, gam);
+  } else {
+    const size_t smg = gamma_smem(g);
+    e0 = cudaFuncSetAttribute(band_gamma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)smg);
+    if (e0 != cudaSuccess) return e0;
+    e0 = launch_pdl(band_gamma_kernel, dim3(g.Pr, batch), dim3(256), smg, s, gh, g.Nr, g.Nc, g.Pr,
+                    g.Pc, c.EDr_t, c.EDc_t, gam);
+  }
   if (e0 != cudaSuccess) return e0;
   auto zk = [&](auto wtag) -> cudaError_t {
     constexpr int W = decltype(wtag)::value;
@@ -968,9 +1435,20 @@ cudaError_t launch_band_adjoint(cudaStream_t s, const Cache& c, const Field& f, 
                       static_cast<const float2*>(f.e), static_cast<const float*>(gam), g.Nr, g.Nc,
                       g.Pr, g.Pc, c.ESc, c.ESr_t, stage, 1.f / ((float)g.Pr * (float)g.Pc), Zk);
   };
-  const bool wide = width > 0 ? width >= BW_BATCH : batch >= 4;
-  cudaError_t err = wide ? zk(std::integral_constant<int, BW_BATCH>{})
-                         : zk(std::integral_constant<int, BW_ONE>{});
+  cudaError_t err;
+  if (band_whole(g, batch, width)) {
+    const size_t smw = z_whole_smem(g);
+    err = cudaFuncSetAttribute(band_z_whole_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)smw);
+    if (err == cudaSuccess)
+      err = launch_pdl(band_z_whole_kernel, dim3(g.K, 1, batch), dim3(BG_NT), smw, s,
+                       static_cast<const float2*>(f.e), static_cast<const float*>(gam), g.Nr,
+                       g.Nc, g.Pr, g.Pc, c.ESc, c.ESr_t, 1.f / ((float)g.Pr * (float)g.Pc), Zk);
+  } else {
+    const bool wide = width > 0 ? width >= BW_BATCH : batch >= 4;
+    err = wide ? zk(std::integral_constant<int, BW_BATCH>{})
+               : zk(std::integral_constant<int, BW_ONE>{});
+  }
   if (err != cudaSuccess) return err;
   const int nb = g.Nr * g.Nc;
   err = launch_pdl(band_x_kernel, dim3((nb * BX_SPLIT + 127) / 128, batch), dim3(128), 0, s,

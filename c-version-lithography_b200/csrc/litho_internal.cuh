@@ -129,6 +129,12 @@ struct Context {
   EvalKey eval_graph_key, eval_last_key;
   bool eval_last_valid = false;
   long long eval_graph_launches = 0;
+  // The same for the batched split-BF16 evaluation (litho_ctm_evaluate_batch), kept
+  // apart so that a loop alternating single-tile and batched calls replays both.
+  cudaGraphExec_t batch_graph = nullptr;
+  EvalKey batch_graph_key, batch_last_key;
+  bool batch_last_valid = false;
+  long long batch_graph_launches = 0;
   double* d_red = nullptr;       // FP64 reduction partials
   // Deferred status of the device-resident entry points ([0] a non-finite input was
   // seen, [1] the first tensor-core wait code), read by litho_ctx_deferred_status.
@@ -217,8 +223,11 @@ cudaError_t launch_reduce_tiles(cudaStream_t s, const float2* part, int tiles, i
 // Shared memory of its per-kernel CTA: band_fields_smem.
 size_t band_fields_smem(const BandGeom& g);
 size_t band_max_smem(const BandGeom& g);
-// width: the chunk width of the small-grid field and Z kernels (8 or 16 columns;
-// 0: 16 for batches of 4 or more images, else 8). The results do not depend on it.
+// width: the schedule of the small-grid field and Z kernels: column chunks of 8 or 16
+// columns per CTA, or BW_WHOLE (the whole small grid per CTA, where its tables fit in
+// shared memory); 0: whole from 8 images on, else 16 for batches of 4 or more images,
+// else 8. The results do not depend on it, bit for bit.
+constexpr int BW_WHOLE = 128;
 cudaError_t launch_band_forward(cudaStream_t s, const Cache& c, Field& f, float* ik, float* iP,
                                 float2* chat, float* Ut, void* img, int batch = 1,
                                 int width = 0);

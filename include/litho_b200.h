@@ -72,9 +72,11 @@ int litho_ctx_synchronize(litho_ctx* ctx);
 int litho_ctx_set_precision(litho_ctx* ctx, int precision);
 /* Kernels this context has launched so far (a counter, for benchmarks). */
 long long litho_ctx_launch_count(const litho_ctx* ctx);
-/* CUDA-graph replay of litho_ctm_evaluate (on by default): the second consecutive
- * call with the same buffers, cache, precision and scalars captures its launch
- * chain into a graph; later identical calls replay it with one launch. Turn it off
+/* CUDA-graph replay of litho_ctm_evaluate and of the split-BF16
+ * litho_ctm_evaluate_batch (on by default, one graph for each): the second
+ * consecutive call with the same buffers, cache, precision, batch and scalars
+ * captures its launch chain into a graph; later identical calls replay it with one
+ * launch. Contexts on the legacy default stream never capture. Turn it off
  * when the context's stream is itself being captured by the caller, or under
  * tools that cannot follow a stream capture. */
 int litho_ctx_enable_graphs(litho_ctx* ctx, int on);
@@ -229,7 +231,8 @@ int litho_ctm_evaluate_host(litho_ctx* ctx, const litho_cache* cache, litho_fiel
  * every kernel covering all images at once, so the per-image latency of the
  * small-grid stages and of each tile's pipeline overlaps across images. losses and
  * norms (host, nullable) receive one value per image, as litho_ctm_evaluate's loss
- * and grad_norm. In LITHO_PRECISION_FP32 the images are evaluated one after another. */
+ * and grad_norm. In LITHO_PRECISION_FP32 the images are evaluated one after another.
+ * Repeated calls on the same buffers replay a CUDA graph (litho_ctx_enable_graphs). */
 int litho_ctm_evaluate_batch(litho_ctx* ctx, const litho_cache* cache, int batch,
                              const float* d_theta, const float* d_target, double threshold,
                              double alpha, float* d_grad_theta, double* losses, double* norms);
@@ -304,9 +307,10 @@ int litho_reinit_sdf(litho_ctx* ctx, int rows, int cols, const float* d_phi, dou
  * serving loop never allocates between its steps. */
 int litho_ctx_reserve(litho_ctx* ctx, const litho_cache* cache, int batch);
 /* Autotuner: times the candidate schedules on this device and keeps the fastest in
- * the context for the calls that follow. With a cache: the chunk width (8 or 16
- * columns) of the small-grid field and Z kernels for `batch` images of that cache,
- * timed on the forward and adjoint band stages (results do not depend on it). With
+ * the context for the calls that follow. With a cache: the schedule of the
+ * small-grid field and Z kernels for `batch` images of that cache (8 or 16 columns
+ * per CTA, or 128: the whole small grid per CTA), timed on the forward and adjoint
+ * band stages (results do not depend on it, bit for bit). With
  * nimg > 0: the CTA size (128, 256, 512 or 1024 threads) of the chamfer transform of
  * reinit_sdf for nimg images of rows x cols (the batched re-initialisations of that
  * many images use it; the result may differ from another CTA size's in the last

@@ -102,11 +102,13 @@ def test_bf16x3_agrees_with_fp32_path(L, wl, tc_ctx):
     assert rel_l2(outs["bf16x3"][1], outs["fp32"][1]) <= 1e-3
 
 
-@pytest.mark.parametrize("N,B", [(300, 3), (2048, 4)])
+@pytest.mark.parametrize("N,B", [(300, 3), (2048, 4), (256, 8)])
 def test_batched_evaluation_equals_single_images(L, wl, tc_ctx, N, B):
     """litho_ctm_evaluate_batch: every image's loss, gradient and norm are the same alone
     and in the batch (same kernels, same summation order: bit for bit), and image 0
-    matches the FP64 oracle within the split-BF16 tolerance."""
+    matches the FP64 oracle within the split-BF16 tolerance. From 8 images on the batch
+    runs the small-grid stage with the whole grid per CTA, the single image with column
+    chunks: the two schedules agree bit for bit."""
     band, r0, c0, w, wss = wl.synthetic_socs_band()
     cache = L.ImagingCache.from_band(N, band, r0, c0, w, wss, ctx=tc_ctx)
     rng = np.random.default_rng(N)
@@ -128,6 +130,45 @@ def test_batched_evaluation_equals_single_images(L, wl, tc_ctx, N, B):
                               0.225, 50.0)
         assert abs(losses[0] - ref["loss"]) <= 1e-4 * ref["loss"]
         assert rel_l2(cpu(grads[0]), ref["grad_theta"]) <= 1e-3
+
+
+def test_batched_graph_replay_equals_direct_launches(L, wl):
+    """Repeated litho_ctm_evaluate_batch calls on the same buffers replay a CUDA graph
+    of the chain from the second call on; every replay gives the directly launched
+    results bit for bit, and new inputs in the same buffers are picked up."""
+    N, B = 256, 3
+    band, r0, c0, w, wss = wl.synthetic_socs_band()
+    targets = np.stack([wl.manhattan_target(N, 12, seed=40 + b) for b in range(B)])
+    thetas = np.stack([wl.theta_init_reference(t) for t in targets])
+    bump = 0.1 * np.random.default_rng(7).standard_normal(thetas.shape)
+    results = {}
+    for graphs in (False, True):
+        stream = torch.cuda.Stream()
+        ctx = L.Context(stream=stream)
+        ctx.set_precision("bf16x3")
+        ctx.enable_graphs(graphs)
+        cache = L.ImagingCache.from_band(N, band, r0, c0, w, wss, ctx=ctx)
+        with torch.cuda.stream(stream):
+            th = torch.tensor(thetas, dtype=torch.float32, device="cuda")
+            tg = torch.tensor(targets, dtype=torch.float32, device="cuda")
+            gr = torch.empty_like(th)
+        stream.synchronize()
+        runs = []
+        for it in range(4):
+            if it == 3:   # new values in the same buffers
+                with torch.cuda.stream(stream):
+                    th.add_(torch.tensor(bump, dtype=torch.float32, device="cuda"))
+            with torch.cuda.stream(stream):
+                losses, grads, norms = L.ctm_evaluate_batch(cache, th, tg, 0.225, 50.0, gr)
+            stream.synchronize()
+            runs.append((losses, norms, grads.clone()))
+        results[graphs] = runs
+        ctx.close()
+    for it in range(4):
+        a, b = results[False][it], results[True][it]
+        assert a[0] == b[0] and a[1] == b[1], it
+        assert torch.equal(a[2], b[2]), it
+    assert results[True][3][0] != results[True][2][0]
 
 
 def test_batched_evaluation_fp32_and_errors(L, wl):
@@ -182,10 +223,11 @@ def test_host_batch_equals_device_batch(L, wl, tc_ctx, N, B, pinned):
 
 
 def test_autotune_keeps_results(L, wl, tc_ctx):
-    """litho_ctx_autotune picks a chunk width for the batched small-grid stage (8 or 16)
-    and a chamfer CTA size; the batched evaluation is bit-identical before and after
-    (the width only distributes the outputs), and the tuned re-initialisation of a
-    batch stays within the OpenCV tolerance."""
+    """litho_ctx_autotune picks a schedule for the batched small-grid stage (8- or
+    16-column chunks, or the whole grid per CTA: 128) and a chamfer CTA size; the
+    batched evaluation is bit-identical before and after (the schedule only distributes
+    the outputs), and the tuned re-initialisation of a batch stays within the OpenCV
+    tolerance."""
     from oracle import levelset_oracle as lo
     band, r0, c0, w, wss = wl.synthetic_socs_band()
     N, B = 256, 5
@@ -197,7 +239,7 @@ def test_autotune_keeps_results(L, wl, tc_ctx):
     before = L.ctm_evaluate_batch(cache, th, tg, 0.225, 50.0)
     g0 = before[1].clone()
     tuned = tc_ctx.autotune(cache, batch=B, shape=(N, N), nimg=B)
-    assert tuned["band_chunk_width"] in (8, 16)
+    assert tuned["band_chunk_width"] in (8, 16, 128)
     assert tuned["chamfer_threads"] in (128, 256, 512, 1024)
     after = L.ctm_evaluate_batch(cache, th, tg, 0.225, 50.0)
     assert list(before[0]) == list(after[0]) and torch.equal(g0, after[1])
