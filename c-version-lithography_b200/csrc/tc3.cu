@@ -275,7 +275,7 @@ __global__ void __launch_bounds__(A3_NT, 1)
 analysis_tc3_kernel(Tc2Analysis a, int T, int B, const uint8_t* __restrict__ txImg,
                     const uint8_t* __restrict__ tyImg, int* __restrict__ err) {
   extern __shared__ __align__(1024) uint8_t smem_raw[];
-  // 0 sA full (8 loader warps), 1-2 stage 1 done [b], 3 sR full (4 TMEM warps),
+  // 0 sA full (16 loader warps), 1-2 stage 1 done [b], 3 sR full (4 TMEM warps),
   // 4-5 stage 2 done [b], 6-7 accQ[b] free (4 TMEM warps), 8 TX landed, 9 TY landed
   __shared__ __align__(8) uint64_t bars[10];
   __shared__ uint32_t tmem_slot;
@@ -457,36 +457,48 @@ analysis_tc3_kernel(Tc2Analysis a, int T, int B, const uint8_t* __restrict__ txI
     int pxt = -1, pyt = -1;
     uint32_t ntx = 0, nty = 0;
     int m1 = 0, m2 = 0;
-    Item it = item_at(lo, T, B);
-    for (int j = 0; j < n; ++j, it = item_next(it, T, B)) {
-      const bool newx = it.xt != pxt;
-      if (newx) {
-        // the TX tile in use is read by stage 1 of the previous item
-        if (j > 0 && !pwait(bar(1 + ((j - 1) & 1)), ((j - 1) >> 1) & 1, vfail, err, 14)) break;
-        bulk_tile(uTX, txImg + (size_t)it.xt * TXB, TXB, bar(8));
-        ++ntx;
-        pxt = it.xt;
+    // Issue order MMA1(0), MMA1(1), MMA2(0), MMA1(2), MMA2(1), ...: stage 1 of item j
+    // is issued as soon as its operand sA is full, before stage 2 of item j - 1 waits
+    // for its operand sR, so the tensor pipe runs stage 1 of the next item while the
+    // TMEM warps build sR.
+    Item it = item_at(lo, T, B), prv = it;
+    for (int j = 0; j <= n; ++j) {
+      if (j < n) {
+        const bool newx = it.xt != pxt;
+        if (newx) {
+          // the TX tile in use is read by stage 1 of the previous item
+          if (j > 0 && !pwait(bar(1 + ((j - 1) & 1)), ((j - 1) >> 1) & 1, vfail, err, 14)) break;
+          bulk_tile(uTX, txImg + (size_t)it.xt * TXB, TXB, bar(8));
+          ++ntx;
+          pxt = it.xt;
+        }
+        if (!pwait(bar(0), j & 1, vfail, err, 15)) break;
+        if (newx && !pwait(bar(8), (ntx - 1) & 1, vfail, err, 16)) break;
+        tc::fence_after();
+        s2_mma(tmem + (uint32_t)((j & 1) * 128), uA, 128, uTX, BN, 128, idesc);
+        tc::mma_commit(bar(1 + (j & 1)));
+        ++m1;
       }
-      if (!pwait(bar(0), j & 1, vfail, err, 15)) break;
-      if (newx && !pwait(bar(8), (ntx - 1) & 1, vfail, err, 16)) break;
-      tc::fence_after();
-      s2_mma(tmem + (uint32_t)((j & 1) * 128), uA, 128, uTX, BN, 128, idesc);
-      tc::mma_commit(bar(1 + (j & 1)));
-      ++m1;
-      const bool newy = it.yt != pyt;
-      if (newy) {
-        if (j > 0 && !pwait(bar(4 + ((j - 1) & 1)), ((j - 1) >> 1) & 1, vfail, err, 17)) break;
-        bulk_tile(uTY, tyImg + (size_t)it.yt * A2_A_BYTES, A2_A_BYTES, bar(9));
-        ++nty;
-        pyt = it.yt;
+      if (j > 0) {
+        // stage 2 of item jj = j - 1
+        const int jj = j - 1;
+        const bool newy = prv.yt != pyt;
+        if (newy) {
+          if (jj > 0 && !pwait(bar(4 + ((jj - 1) & 1)), ((jj - 1) >> 1) & 1, vfail, err, 17)) break;
+          bulk_tile(uTY, tyImg + (size_t)prv.yt * A2_A_BYTES, A2_A_BYTES, bar(9));
+          ++nty;
+          pyt = prv.yt;
+        }
+        if (!pwait(bar(3), jj & 1, vfail, err, 18)) break;
+        if (newy && !pwait(bar(9), (nty - 1) & 1, vfail, err, 19)) break;
+        if (jj >= 2 && !pwait(bar(6 + (jj & 1)), ((jj - 2) >> 1) & 1, vfail, err, 20)) break;
+        tc::fence_after();
+        s2_mma(tmem + 256u + (uint32_t)((jj & 1) * 128), uTY, 128, uR, BN, 128, idesc);
+        tc::mma_commit(bar(4 + (jj & 1)));
+        ++m2;
+        prv = item_next(prv, T, B);
       }
-      if (!pwait(bar(3), j & 1, vfail, err, 18)) break;
-      if (newy && !pwait(bar(9), (nty - 1) & 1, vfail, err, 19)) break;
-      if (j >= 2 && !pwait(bar(6 + (j & 1)), ((j - 2) >> 1) & 1, vfail, err, 20)) break;
-      tc::fence_after();
-      s2_mma(tmem + 256u + (uint32_t)((j & 1) * 128), uTY, 128, uR, BN, 128, idesc);
-      tc::mma_commit(bar(4 + (j & 1)));
-      ++m2;
+      if (j < n) it = item_next(it, T, B);
     }
     if (*vfail) {
       // nothing of this CTA may still be in flight when it exits
