@@ -55,6 +55,9 @@ def parse():
                         "1 reports the single-tile chain")
     p.add_argument("--fullchip-size", type=int, default=16384,
                    help="layout size of the full-chip CTM leg (0: skip it)")
+    p.add_argument("--fullchip-cores", default="256,1024",
+                   help="LO,HI: seeded uneven Core sides in [LO, HI] pixels for the full-chip "
+                        "layout; 'equal' cuts it into --fullchip-grid equal Cores per side")
     p.add_argument("--fullchip-grid", type=int, default=16,
                    help="micro tiles per side of the full-chip layout")
     p.add_argument("--serving-requests", type=int, default=1000,
@@ -477,17 +480,19 @@ def levelset_run(L, torch, stream, N=2048, B=16, steps=10, warmup=3):
             "pixel_updates_per_s": B * N * N / (ms * 1e-3)}
 
 
-def fullchip_run(L, K, size, grid, halo, guard, ctm_steps=3, lsm_steps=20, seed=11):
+def fullchip_run(L, K, size, grid, halo, guard, ctm_steps=3, lsm_steps=20, seed=11, cores=None):
     """The batched full-chip configuration: a size x size layout (2 nm pixels, seeded
-    rectangles at about 34 % density) cut into grid x grid micro tiles (Core size / grid
-    plus a `halo` pixel halo on every side). Two runs per precision mode:
+    rectangles at about 34 % density) cut into micro tiles: seeded uneven Cores with
+    sides in cores = (lo, hi) pixels (rows and columns cut with seeds of their own), or
+    grid x grid equal Cores; every tile is the largest Core plus a `halo` pixel halo
+    on every side (Partition::build's one tile size). Two runs per precision mode:
     FullChipCTMOptimizer for `ctm_steps` steps (each the exchange: imaging, windowed PE
     loss and adjoint of every tile, CEPT and neighbour gradient fusion, then the
     windowed theta step) and FullChipLSMOptimizer for `lsm_steps` WENO5-Godunov steps
     (exchange over Core + Guard with the Core metrics, windowed RK2 per tile, reinit
-    every 20, rendered masks, best-round state). Split-BF16 images the tiles in
-    batched groups, the plain FP32 mode one tile after another. Timed on the wall
-    clock around each run (the exchange returns its losses to the host every step);
+    every 20, rendered masks, best-round state). Split-BF16 images all tiles in one
+    batched pass, the plain FP32 mode one tile after another. Timed on the wall clock
+    around each run (the exchange returns its losses to the host every step);
     tile-iterations count every tile of every exchange (the initial one included)."""
     import torch
     FC = importlib.import_module("c-version-lithography_b200.fullchip")
@@ -495,7 +500,16 @@ def fullchip_run(L, K, size, grid, halo, guard, ctm_steps=3, lsm_steps=20, seed=
     band, r0, c0, w, wss = wl.synthetic_socs_band(K=K)
     layout = torch.from_numpy(wl.cell_layout(size, size, seed)).cuda()
     gopt = FC.MicroGradientOptions(enable_cept=True, enable_grad_fusion=True)
-    out = {"workload": f"{size}^2 layout (2 nm pixels, ~34% density), {grid}x{grid} micro tiles, "
+    if cores:
+        rc = wl.uneven_cuts(size, cores[0], cores[1], seed)
+        cc = wl.uneven_cuts(size, cores[0], cores[1], seed + 1)
+        tiling = (f"{len(rc) - 1}x{len(cc) - 1} micro tiles over seeded uneven Cores of "
+                  f"{cores[0]}-{cores[1]} px")
+    else:
+        rc = [r * size // grid for r in range(grid + 1)]
+        cc = list(rc)
+        tiling = f"{grid}x{grid} micro tiles"
+    out = {"workload": f"{size}^2 layout (2 nm pixels, ~34% density), {tiling}, "
                        f"halo {halo}, guard {guard}, {K} SOCS kernels; CTM: {ctm_steps} steps "
                        f"with CEPT + average gradient fusion; LSM: {lsm_steps} WENO5-Godunov "
                        f"steps, Binary masks, reinit every 20, Core metrics",
@@ -511,12 +525,13 @@ def fullchip_run(L, K, size, grid, halo, guard, ctm_steps=3, lsm_steps=20, seed=
     for mode in ("bf16x3", "fp32"):
         ctx = L.Context()
         ctx.set_precision(mode)
-        part = FC.Partition(size, size, grid, grid, halo, guard, ctx=ctx)
+        part = FC.Partition(size, size, len(rc) - 1, len(cc) - 1, halo, guard, ctx=ctx,
+                            row_cuts=rc, col_cuts=cc)
         cache = L.ImagingCache.from_band(part.tile_size, band, r0, c0, w, wss, ctx=ctx)
-        # schedules of this layout: small-grid stage of the exchange's tile groups,
-        # chamfer re-initialisation of all tiles at once
+        # schedules of this layout: small-grid stage of the exchange's one batched pass
+        # over all tiles, chamfer re-initialisation of all tiles at once
         out.setdefault("autotune", {})[mode] = ctx.autotune(
-            cache, batch=min(16, part.num_tiles), shape=(part.tile_size, part.tile_size),
+            cache, batch=part.num_tiles, shape=(part.tile_size, part.tile_size),
             nimg=part.num_tiles)
         ctm = FC.FullChipCTMOptimizer(part, cache, THRESHOLD, ALPHA)
         ctm.optimize(layout, FC.FullChipCTMOptions(iterations=1, gradient_options=gopt))  # warm-up
@@ -791,7 +806,10 @@ def run_ours(args):
     if world == 1 and args.serving_requests > 0:
         out["serving"] = serving_run(L, K, args.serving_requests)
     if world == 1 and args.fullchip_size > 0:
-        out["fullchip"] = fullchip_run(L, K, args.fullchip_size, args.fullchip_grid, 128, 32)
+        cores = (None if args.fullchip_cores == "equal" else
+                 tuple(int(v) for v in args.fullchip_cores.split(",")))
+        out["fullchip"] = fullchip_run(L, K, args.fullchip_size, args.fullchip_grid, 128, 32,
+                                       cores=cores)
     if world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(N, K, band, r0, c0, w, wss, target, theta,
                                            args.cpu_seconds,

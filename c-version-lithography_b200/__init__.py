@@ -110,6 +110,7 @@ SIGNATURES = {
     "litho_ctx_launch_count": (ctypes.c_longlong, [_P]),
     "litho_ctx_enable_graphs": (_I, [_P, _I]),
     "litho_ctx_set_tc_schedule": (_I, [_P, _I]),
+    "litho_ctx_set_exchange_group": (_I, [_P, _I]),
     "litho_ctx_enable_stage_timing": (_I, [_P, _I]),
     "litho_ctx_stage_times": (_I, [_P, _PD, ctypes.POINTER(ctypes.c_longlong)]),
     "litho_cache_create_dense": (_I, [_P, _I, _I, _PD, _PD, _D, _PP]),
@@ -147,6 +148,7 @@ SIGNATURES = {
                                  _P]),
     "litho_lbfgs_dots3": (_I, [_P, _I, ctypes.c_longlong, _P, ctypes.c_longlong, _P, _P, _P, _PD]),
     "litho_partition_create": (_I, [_P, _I, _I, _I, _I, _I, _I, _PP]),
+    "litho_partition_create_cuts": (_I, [_P, _I, _I, _I, _PI, _I, _PI, _I, _I, _PP]),
     "litho_partition_destroy": (_I, [_P]),
     "litho_partition_info": (_I, [_P, _PI, _PI]),
     "litho_partition_tile_rects": (_I, [_P, _I, _PI]),
@@ -272,6 +274,11 @@ class Context:
     def enable_graphs(self, on: bool = True):
         """CUDA-graph replay of repeated CTM evaluations (on by default)."""
         self._check(self.lib.litho_ctx_enable_graphs(self.handle, 1 if on else 0))
+
+    def set_exchange_group(self, max_tiles: int = 0):
+        """Largest number of micro tiles per batched pass of the split-BF16 exchange
+        (litho_ctx_set_exchange_group); 0: all tiles within the scratch budget."""
+        self._check(self.lib.litho_ctx_set_exchange_group(self.handle, int(max_tiles)))
 
     TC_SCHEDULES = {"auto": 0, "per_tile": 1, "persistent": 2}
 

@@ -279,6 +279,12 @@ int litho_ctx_enable_graphs(litho_ctx* ctx, int on) {
   return LITHO_OK;
 }
 
+int litho_ctx_set_exchange_group(litho_ctx* ctx, int max_tiles) {
+  if (!ctx || max_tiles < 0) return LITHO_ERR_INVALID_ARGUMENT;
+  ctx->exchange_group_max = max_tiles;
+  return LITHO_OK;
+}
+
 int litho_ctx_set_tc_schedule(litho_ctx* ctx, int schedule) {
   if (!ctx) return LITHO_ERR_INVALID_ARGUMENT;
   if (schedule != LITHO_TC_SCHEDULE_AUTO && schedule != LITHO_TC_SCHEDULE_PER_TILE &&
@@ -2037,27 +2043,25 @@ void free_partition(litho_partition* p) {
 
 }  // namespace
 
-extern "C" {
 
-int litho_partition_create(litho_ctx* ctx, int height, int width, int grid_rows, int grid_cols,
-                           int halo, int guard, litho_partition** out) {
-  if (!ctx || !out) return LITHO_ERR_INVALID_ARGUMENT;
-  *out = nullptr;
-  if (height <= 0 || width <= 0 || grid_rows <= 0 || grid_cols <= 0 || grid_rows > height ||
-      grid_cols > width || halo < 0 || guard < 0)
-    return ctx->fail(LITHO_ERR_INVALID_ARGUMENT, "Partition: invalid layout or grid size");
-  if (guard > halo)
-    return ctx->fail(LITHO_ERR_INVALID_ARGUMENT, "Partition: guard must not exceed halo");
+namespace {
+
+// Partition::build (partition.cpp:21-80) over given Core boundaries: row r of the
+// tile grid covers rows [row_cuts[r], row_cuts[r + 1]), column c columns
+// [col_cuts[c], col_cuts[c + 1]); one square tile size = largest Core side + 2 halo,
+// rounded up to even; tiles keyed row-major with their four-neighbour relations.
+int partition_build(litho_ctx* ctx, int height, int width, const std::vector<int>& row_cuts,
+                    const std::vector<int>& col_cuts, int halo, int guard, litho_partition** out) {
+  const int grid_rows = (int)row_cuts.size() - 1, grid_cols = (int)col_cuts.size() - 1;
   auto* p = new (std::nothrow) litho_partition();
   if (!p) return ctx->fail(LITHO_ERR_OOM, "host allocation failed");
   p->device = ctx->device;
   p->height = height; p->width = width; p->grid_rows = grid_rows; p->grid_cols = grid_cols;
   p->halo = halo; p->guard = guard;
-  // Partition::build (partition.cpp:21-80): Core boundaries at i * extent / count, one
-  // square tile size = largest Core side + 2 halo, rounded up to even.
-  const int max_r = (height + grid_rows - 1) / grid_rows;
-  const int max_c = (width + grid_cols - 1) / grid_cols;
-  int ts = std::max(max_r, max_c) + 2 * halo;
+  int max_side = 0;
+  for (int r = 0; r < grid_rows; ++r) max_side = std::max(max_side, row_cuts[r + 1] - row_cuts[r]);
+  for (int c = 0; c < grid_cols; ++c) max_side = std::max(max_side, col_cuts[c + 1] - col_cuts[c]);
+  int ts = max_side + 2 * halo;
   ts += ts % 2;
   p->ts = ts;
   const int n = grid_rows * grid_cols;
@@ -2066,8 +2070,7 @@ int litho_partition_create(litho_ctx* ctx, int height, int width, int grid_rows,
   for (int r = 0; r < grid_rows; ++r)
     for (int c = 0; c < grid_cols; ++c) {
       const int id = r * grid_cols + c;
-      core[id] = {(int)((long long)r * height / grid_rows), (int)((long long)(r + 1) * height / grid_rows),
-                  (int)((long long)c * width / grid_cols), (int)((long long)(c + 1) * width / grid_cols)};
+      core[id] = {row_cuts[r], row_cuts[r + 1], col_cuts[c], col_cuts[c + 1]};
       tile[id] = {core[id].y0 - halo, core[id].y0 - halo + ts, core[id].x0 - halo,
                   core[id].x0 - halo + ts};
     }
@@ -2126,6 +2129,50 @@ int litho_partition_create(litho_ctx* ctx, int height, int width, int grid_rows,
   return LITHO_OK;
 }
 
+}  // namespace
+
+extern "C" {
+
+int litho_partition_create(litho_ctx* ctx, int height, int width, int grid_rows, int grid_cols,
+                           int halo, int guard, litho_partition** out) {
+  if (!ctx || !out) return LITHO_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  if (height <= 0 || width <= 0 || grid_rows <= 0 || grid_cols <= 0 || grid_rows > height ||
+      grid_cols > width || halo < 0 || guard < 0)
+    return ctx->fail(LITHO_ERR_INVALID_ARGUMENT, "Partition: invalid layout or grid size");
+  if (guard > halo)
+    return ctx->fail(LITHO_ERR_INVALID_ARGUMENT, "Partition: guard must not exceed halo");
+  // Core boundaries at i * extent / count (partition.cpp:37-38).
+  std::vector<int> rc(grid_rows + 1), cc(grid_cols + 1);
+  for (int r = 0; r <= grid_rows; ++r) rc[r] = (int)((long long)r * height / grid_rows);
+  for (int c = 0; c <= grid_cols; ++c) cc[c] = (int)((long long)c * width / grid_cols);
+  return partition_build(ctx, height, width, rc, cc, halo, guard, out);
+}
+
+int litho_partition_create_cuts(litho_ctx* ctx, int height, int width, int grid_rows,
+                                const int* row_cuts, int grid_cols, const int* col_cuts, int halo,
+                                int guard, litho_partition** out) {
+  if (!ctx || !out || !row_cuts || !col_cuts) return LITHO_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  if (height <= 0 || width <= 0 || grid_rows <= 0 || grid_cols <= 0 || halo < 0 || guard < 0)
+    return ctx->fail(LITHO_ERR_INVALID_ARGUMENT, "Partition: invalid layout or grid size");
+  if (guard > halo)
+    return ctx->fail(LITHO_ERR_INVALID_ARGUMENT, "Partition: guard must not exceed halo");
+  std::vector<int> rc(row_cuts, row_cuts + grid_rows + 1), cc(col_cuts, col_cuts + grid_cols + 1);
+  auto valid = [&](const std::vector<int>& cuts, int extent) {
+    if (cuts.front() != 0 || cuts.back() != extent) return false;
+    for (size_t i = 0; i + 1 < cuts.size(); ++i)
+      if (cuts[i + 1] - cuts[i] < std::max(1, guard)) return false;
+    return true;
+  };
+  // Every Core at least as wide as the guard: a tile's guard band then reaches only its
+  // four neighbours' Cores, the relations the exchange evaluates.
+  if (!valid(rc, height) || !valid(cc, width))
+    return ctx->fail(LITHO_ERR_INVALID_ARGUMENT,
+                     "Partition: cuts must run from 0 to the extent, each Core at least the guard wide");
+  return partition_build(ctx, height, width, rc, cc, halo, guard, out);
+}
+
 int litho_partition_destroy(litho_partition* p) {
   if (!p) return LITHO_OK;
   free_partition(p);
@@ -2168,9 +2215,18 @@ int litho_partition_assemble(litho_ctx* ctx, const litho_partition* p, const flo
                       "tile assembly");
 }
 
-// Tiles per batched pass of the exchange (tensor-core path): enough to fill the GPU
-// at 1024-2048 pixel tiles, with the group's scratch a few hundred MB at most.
+// Tiles per batched pass of the exchange (tensor-core path): every tile of the
+// partition in one pass while the pass's scratch stays within kExchangeBudget bytes
+// (about 4.6 MB per 1280^2 tile at K = 24: 256 such tiles take 1.2 GB), and at least
+// kExchangeGroup tiles.
 constexpr int kExchangeGroup = 16;
+constexpr size_t kExchangeBudget = (size_t)4 << 30;
+int exchange_group(const Context* ctx, const BandGeom& g, int n) {
+  if (ctx->exchange_group_max > 0) return std::min(n, ctx->exchange_group_max);
+  const size_t per = make_layout(g, 2, true).total - make_layout(g, 1, true).total;
+  const size_t fit = kExchangeBudget / std::max<size_t>(per, 1);
+  return (int)std::min<size_t>((size_t)n, std::max<size_t>(kExchangeGroup, fit));
+}
 
 int litho_exchange_compute_epe(litho_ctx* ctx, const litho_partition* cp, const litho_cache* cache,
                                const float* d_masks, const float* d_global_target, double threshold,
@@ -2213,12 +2269,12 @@ int litho_exchange_compute_epe(litho_ctx* ctx, const litho_partition* cp, const 
   const bool epe_terms = o.loss_type == LITHO_MICRO_LOSS_EPE || o.loss_type == LITHO_MICRO_LOSS_PE_EPE;
   const bool core = e.collect_core_metrics != 0;
   const bool eval_epe = epe_terms || core;   // micro_gradient_exchange.cpp:144-148
-  // Tensor-core path: the tiles go through the imaging + adjoint chain in groups of
-  // kExchangeGroup, one batched pass per group (the EP work stays per tile between
-  // the forward and the adjoint pass).
+  // Tensor-core path: the tiles go through the imaging + adjoint chain in groups
+  // (exchange_group: normally all of them), one batched pass per group (the EP work
+  // stays per tile between the forward and the adjoint pass).
   const bool batched = ctx->precision == LITHO_PRECISION_BF16X3 && cache->TXD_img != nullptr &&
                        n > 1;
-  const int group = batched ? std::min(n, kExchangeGroup) : 1;
+  const int group = batched ? exchange_group(ctx, cache->g, n) : 1;
   Layout L;
   int st = prepare(ctx, *cache, &L, group, batched);
   if (st) return st;

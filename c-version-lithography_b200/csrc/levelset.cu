@@ -23,36 +23,50 @@ constexpr int LS_SH = LS_TY * LS_RPT + 2 * LS_H;
 constexpr int LS_NT = LS_TX * LS_TY;
 static_assert(LS_TX == 32 && LS_SW <= 64, "the tile loader maps one warp to one tile row");
 
-// WENO5-JS one-sided derivative from the five differences v1..v5 (already
-// divided by the spacing), level_set_utils.cpp:45-113. The smoothness
-// indicators are scaled by 1/max(v^2) before forming the weights: the weights
-// are invariant under that scaling (eps = 1e-6 max v^2 scales the same way) and
-// the scaled values stay inside FP32 range.
-__device__ __forceinline__ float weno5(float v1, float v2, float v3, float v4, float v5) {
-  const float d1 = (1.f / 3.f) * v1 - (7.f / 6.f) * v2 + (11.f / 6.f) * v3;
-  const float d2 = -(1.f / 6.f) * v2 + (5.f / 6.f) * v3 + (1.f / 3.f) * v4;
-  const float d3 = (1.f / 3.f) * v3 + (5.f / 6.f) * v4 - (1.f / 6.f) * v5;
-  const float vmax2 = fmaxf(fmaxf(fmaxf(v1 * v1, v2 * v2), fmaxf(v3 * v3, v4 * v4)), v5 * v5);
-  if (!(vmax2 > 0.f)) return 0.f;  // all differences zero: every candidate is zero
-  const float t1 = v1 - 2.f * v2 + v3;
-  const float t2 = v2 - 2.f * v3 + v4;
-  const float t3 = v3 - 2.f * v4 + v5;
-  const float q1 = v1 - 4.f * v2 + 3.f * v3;
-  const float q2 = v2 - v4;
-  const float q3 = 3.f * v3 - 4.f * v4 + v5;
-  // Approximate reciprocal and division (__fdividef, within 2 ulp): vmax2 and the
-  // weight sum below stay far inside the range where they are accurate, and the
-  // weights are a smooth function of both.
-  const float inv = __fdividef(1.f, vmax2);
-  const float S1 = ((13.f / 12.f) * t1 * t1 + 0.25f * q1 * q1) * inv + 1e-6f;
-  const float S2 = ((13.f / 12.f) * t2 * t2 + 0.25f * q2 * q2) * inv + 1e-6f;
-  const float S3 = ((13.f / 12.f) * t3 * t3 + 0.25f * q3 * q3) * inv + 1e-6f;
-  // alpha_i = gamma_i / S_i^2 and the result sum(alpha_i d_i) / sum(alpha_i), both
-  // multiplied by S1^2 S2^2 S3^2: one division instead of four. The scaled S_i lie in
-  // [1e-6, 34], so the products stay well inside FP32 range.
-  const float s1 = S1 * S1, s2 = S2 * S2, s3 = S3 * S3;
-  const float b1 = 0.1f * (s2 * s3), b2 = 0.6f * (s1 * s3), b3 = 0.3f * (s1 * s2);
-  return __fdividef(b1 * d1 + b2 * d2 + b3 * d3, b1 + b2 + b3);
+// WENO5-JS one-sided derivative from the five differences v1..v5 (already divided by
+// the spacing), level_set_utils.cpp:45-113, for two stencils at once: lane x of the
+// result is the derivative of (v1.x .. v5.x), lane y that of (v1.y .. v5.y). The
+// arithmetic is packed FP32x2 (sm_100 FFMA2 / FMUL2 / FADD2: one instruction for both
+// lanes, each lane rounded as the scalar operation), which halves the instructions of
+// this part of an issue-bound stencil. The smoothness indicators are scaled by
+// 1/max(v^2) before forming the weights: the weights are invariant under that scaling
+// (eps = 1e-6 max v^2 scales the same way) and the scaled values stay inside FP32
+// range. alpha_i = gamma_i / S_i^2 and the result sum(alpha_i d_i) / sum(alpha_i) are
+// both multiplied by S1^2 S2^2 S3^2 (one division instead of four; the scaled S_i lie
+// in [1e-6, 34], so the products stay well inside FP32 range). __fdividef (within 2
+// ulp) serves the reciprocal and the division: max v^2 and the weight sum stay far
+// inside the range where it is accurate.
+__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 weno5x2(float2 v1, float2 v2, float2 v3, float2 v4, float2 v5) {
+  const float2 d1 = __ffma2_rn(f2(11.f / 6.f), v3, __ffma2_rn(f2(-7.f / 6.f), v2, __fmul2_rn(f2(1.f / 3.f), v1)));
+  const float2 d2 = __ffma2_rn(f2(1.f / 3.f), v4, __ffma2_rn(f2(5.f / 6.f), v3, __fmul2_rn(f2(-1.f / 6.f), v2)));
+  const float2 d3 = __ffma2_rn(f2(-1.f / 6.f), v5, __ffma2_rn(f2(5.f / 6.f), v4, __fmul2_rn(f2(1.f / 3.f), v3)));
+  const float2 s1 = __fmul2_rn(v1, v1), s2 = __fmul2_rn(v2, v2), s3 = __fmul2_rn(v3, v3);
+  const float2 s4 = __fmul2_rn(v4, v4), s5 = __fmul2_rn(v5, v5);
+  const float mx = fmaxf(fmaxf(fmaxf(s1.x, s2.x), fmaxf(s3.x, s4.x)), s5.x);
+  const float my = fmaxf(fmaxf(fmaxf(s1.y, s2.y), fmaxf(s3.y, s4.y)), s5.y);
+  // all differences of a lane zero: its candidates are zero, and so is its result
+  // (inv = 0 keeps its weights finite)
+  const float2 inv = make_float2(mx > 0.f ? __fdividef(1.f, mx) : 0.f,
+                                 my > 0.f ? __fdividef(1.f, my) : 0.f);
+  const float2 t1 = __fadd2_rn(__ffma2_rn(f2(-2.f), v2, v1), v3);
+  const float2 t2 = __fadd2_rn(__ffma2_rn(f2(-2.f), v3, v2), v4);
+  const float2 t3 = __fadd2_rn(__ffma2_rn(f2(-2.f), v4, v3), v5);
+  const float2 q1 = __ffma2_rn(f2(3.f), v3, __ffma2_rn(f2(-4.f), v2, v1));
+  const float2 q2 = __ffma2_rn(f2(-1.f), v4, v2);
+  const float2 q3 = __fadd2_rn(__ffma2_rn(f2(-4.f), v4, __fmul2_rn(f2(3.f), v3)), v5);
+  auto smooth = [&](float2 t, float2 q) {
+    const float2 a = __fmul2_rn(__fmul2_rn(f2(13.f / 12.f), t), t);
+    return __ffma2_rn(__ffma2_rn(__fmul2_rn(f2(0.25f), q), q, a), inv, f2(1e-6f));
+  };
+  const float2 S1 = smooth(t1, q1), S2 = smooth(t2, q2), S3 = smooth(t3, q3);
+  const float2 w1 = __fmul2_rn(S1, S1), w2 = __fmul2_rn(S2, S2), w3 = __fmul2_rn(S3, S3);
+  const float2 b1 = __fmul2_rn(f2(0.1f), __fmul2_rn(w2, w3));
+  const float2 b2 = __fmul2_rn(f2(0.6f), __fmul2_rn(w1, w3));
+  const float2 b3 = __fmul2_rn(f2(0.3f), __fmul2_rn(w1, w2));
+  const float2 num = __ffma2_rn(b3, d3, __ffma2_rn(b2, d2, __fmul2_rn(b1, d1)));
+  const float2 den = __fadd2_rn(__fadd2_rn(b1, b2), b3);
+  return make_float2(__fdividef(num.x, den.x), __fdividef(num.y, den.y));
 }
 
 // Godunov |grad phi| for the sign of the normal speed (level_set_utils.cpp:180-213).
@@ -91,14 +105,16 @@ __device__ __forceinline__ float weno_delta(const float (*t)[LS_SW], int ly, int
   float d[6];
 #pragma unroll
   for (int q = 0; q < 6; ++q) d[q] = (t[ly][lx - 2 + q] - t[ly][lx - 3 + q]) * idx;
-  // minus: D(j-3..j+1) = d[0..4]; plus: mirrored d[5..1]
-  const float xm = weno5(d[0], d[1], d[2], d[3], d[4]);
-  const float xp = weno5(d[5], d[4], d[3], d[2], d[1]);
+  // minus: D(j-3..j+1) = d[0..4]; plus: mirrored d[5..1]; both in one packed call
+  const float2 xmp = weno5x2(make_float2(d[0], d[5]), make_float2(d[1], d[4]),
+                             make_float2(d[2], d[3]), make_float2(d[3], d[2]),
+                             make_float2(d[4], d[1]));
 #pragma unroll
   for (int q = 0; q < 6; ++q) d[q] = (t[ly - 2 + q][lx] - t[ly - 3 + q][lx]) * idy;
-  const float ym = weno5(d[0], d[1], d[2], d[3], d[4]);
-  const float yp = weno5(d[5], d[4], d[3], d[2], d[1]);
-  return speed * godunov(speed, xm, xp, ym, yp);
+  const float2 ymp = weno5x2(make_float2(d[0], d[5]), make_float2(d[1], d[4]),
+                             make_float2(d[2], d[3]), make_float2(d[3], d[2]),
+                             make_float2(d[4], d[1]));
+  return speed * godunov(speed, xmp.x, xmp.y, ymp.x, ymp.y);
 }
 
 // _gradient_1d along x (level_set_utils.cpp:228-255) at global column x of row ly.

@@ -180,6 +180,9 @@ struct Context {
   // batched call and a single-image call take the same schedule, so every image's
   // results are the same alone and in a batch, bit for bit.
   int tc_schedule = LITHO_TC_SCHEDULE_AUTO;
+  // Largest number of micro tiles per batched pass of the exchange (0: as many as the
+  // scratch budget allows); litho_ctx_set_exchange_group.
+  int exchange_group_max = 0;
   bool tc_persistent() const { return tc_schedule != LITHO_TC_SCHEDULE_PER_TILE; }
 };
 

@@ -107,15 +107,32 @@ class PartitionTile:
 
 
 class Partition:
-    """Partition::build (partition.cpp:21-80) on the device: geometry + tile copies."""
+    """Partition::build (partition.cpp:21-80) on the device: geometry + tile copies.
+
+    By default the Cores are cut at i * extent / count as in the reference; with
+    row_cuts / col_cuts (grid_rows + 1 and grid_cols + 1 boundaries from 0 to the
+    extent) they take the given, possibly uneven boundaries, every tile keeping the
+    one tile size = largest Core side + 2 halo (litho_partition_create_cuts)."""
 
     def __init__(self, height: int, width: int, grid_rows: int, grid_cols: int, halo: int,
-                 guard: int, ctx=None):
+                 guard: int, ctx=None, row_cuts=None, col_cuts=None):
         self.ctx = ctx or default_context()
         lib = self.ctx.lib
         h = ctypes.c_void_p()
-        self.ctx._check(lib.litho_partition_create(self.ctx.handle, height, width, grid_rows,
-                                                   grid_cols, halo, guard, ctypes.byref(h)))
+        if row_cuts is None and col_cuts is None:
+            self.ctx._check(lib.litho_partition_create(self.ctx.handle, height, width, grid_rows,
+                                                       grid_cols, halo, guard, ctypes.byref(h)))
+        else:
+            rc = [int(v) for v in (row_cuts if row_cuts is not None else
+                                   [r * height // grid_rows for r in range(grid_rows + 1)])]
+            cc = [int(v) for v in (col_cuts if col_cuts is not None else
+                                   [c * width // grid_cols for c in range(grid_cols + 1)])]
+            if len(rc) != grid_rows + 1 or len(cc) != grid_cols + 1:
+                raise LithoError(1, "Partition: grid_rows + 1 row cuts and grid_cols + 1 column "
+                                    "cuts are needed")
+            self.ctx._check(lib.litho_partition_create_cuts(
+                self.ctx.handle, height, width, grid_rows, (ctypes.c_int * len(rc))(*rc),
+                grid_cols, (ctypes.c_int * len(cc))(*cc), halo, guard, ctypes.byref(h)))
         self.handle = h
         self.height, self.width = height, width
         self.grid_rows, self.grid_cols = grid_rows, grid_cols

@@ -162,3 +162,22 @@ def theta_init_reference(target: np.ndarray) -> np.ndarray:
     """CTM_Optimizer::_initialize_theta (CTM_Optimizer.cpp:55-64): 0.3 pi / 0.7 pi."""
     pi = 3.14159265358979323846
     return np.where(target > 0.0, 0.3 * pi, 0.7 * pi)
+
+
+def uneven_cuts(extent: int, lo: int, hi: int, seed: int) -> list:
+    """Seeded Core boundaries 0 = c_0 < c_1 < ... < c_n = extent with every Core side
+    c_{i+1} - c_i in [lo, hi] (requires extent >= lo and hi >= 2 lo): sides drawn
+    uniformly from [lo, hi] while the rest exceeds hi, then the rest split into one or
+    two Cores inside the range."""
+    if extent < lo or hi < 2 * lo:
+        raise ValueError("uneven_cuts needs extent >= lo and hi >= 2 lo")
+    rng = np.random.default_rng(seed)
+    cuts = [0]
+    while extent - cuts[-1] > hi:
+        rest = extent - cuts[-1]
+        side = int(rng.integers(lo, hi + 1))
+        if rest - side < lo:          # keep a last Core of at least lo
+            side = rest - lo
+        cuts.append(cuts[-1] + side)
+    cuts.append(extent)
+    return cuts

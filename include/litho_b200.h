@@ -85,6 +85,10 @@ int litho_ctx_enable_graphs(litho_ctx* ctx, int on);
  * another order, so they may differ in their last bits. This choice has no
  * counterpart in the reference (whose passes are FFTs on the CPU). */
 int litho_ctx_set_tc_schedule(litho_ctx* ctx, int schedule);
+/* Largest number of micro tiles the split-BF16 exchange (litho_exchange_compute*)
+ * images in one batched pass; 0 (the default): every tile of the partition while the
+ * pass's scratch stays within 4 GiB, at least 16. Results do not depend on it. */
+int litho_ctx_set_exchange_group(litho_ctx* ctx, int max_tiles);
 
 /* Per-stage device timing with CUDA events on the context's stream. Stages:
  * 0 tile analysis of the mask (row DFT + column contraction per 128 x 128 tile),
@@ -400,6 +404,15 @@ int litho_ctx_deferred_status(litho_ctx* ctx);
 typedef struct litho_partition litho_partition;
 int litho_partition_create(litho_ctx* ctx, int height, int width, int grid_rows, int grid_cols,
                            int halo, int guard, litho_partition** out);
+/* The same geometry over given, possibly uneven Core boundaries (Partition::build,
+ * partition.cpp:21-80, with its i * extent / count cuts replaced by the caller's):
+ * row_cuts[0..grid_rows] and col_cuts[0..grid_cols] run from 0 to height / width,
+ * each Core at least max(1, guard) pixels wide. As in the reference, every tile
+ * takes the one tile_size = largest Core side + 2 halo (rounded up to even), so
+ * smaller Cores carry a wider margin beyond their halo on the bottom / right side. */
+int litho_partition_create_cuts(litho_ctx* ctx, int height, int width, int grid_rows,
+                                const int* row_cuts, int grid_cols, const int* col_cuts, int halo,
+                                int guard, litho_partition** out);
 int litho_partition_destroy(litho_partition* partition);
 int litho_partition_info(const litho_partition* partition, int* num_tiles, int* tile_size);
 /* Rectangles of one tile, each (y0, y1, x0, x1) half-open: rects[0..3]

@@ -85,17 +85,23 @@ class Meta:
     tiles: List[Tile]
 
 
-def build(height, width, grid_rows, grid_cols, halo, guard) -> Meta:
-    """Partition::build (source/utils/partition.cpp:21-80)."""
-    max_r = (height + grid_rows - 1) // grid_rows
-    max_c = (width + grid_cols - 1) // grid_cols
-    ts = max(max_r, max_c) + 2 * halo
+def build(height, width, grid_rows, grid_cols, halo, guard, row_cuts=None,
+          col_cuts=None) -> Meta:
+    """Partition::build (source/utils/partition.cpp:21-80). row_cuts / col_cuts
+    (grid_rows + 1 / grid_cols + 1 boundaries from 0 to the extent) replace the
+    reference's row * height // grid_rows cuts; the tile size stays the largest Core
+    side + 2 halo, rounded up to even (partition.cpp:31-34)."""
+    rc = list(row_cuts) if row_cuts is not None else [r * height // grid_rows
+                                                      for r in range(grid_rows + 1)]
+    cc = list(col_cuts) if col_cuts is not None else [c * width // grid_cols
+                                                      for c in range(grid_cols + 1)]
+    ts = max(max(b - a for a, b in zip(rc, rc[1:])), max(b - a for a, b in zip(cc, cc[1:])))
+    ts += 2 * halo
     ts += ts % 2
     tiles = []
     for row in range(grid_rows):
         for col in range(grid_cols):
-            core = Rect(row * height // grid_rows, (row + 1) * height // grid_rows,
-                        col * width // grid_cols, (col + 1) * width // grid_cols)
+            core = Rect(rc[row], rc[row + 1], cc[col], cc[col + 1])
             oy, ox = core.y0 - halo, core.x0 - halo
             tg = Rect(oy, oy + ts, ox, ox + ts)
             cl = core.shifted(-oy, -ox)

@@ -73,6 +73,106 @@ def test_partition_matches_oracle(L, FC, cfg):
     assert np.array_equal(back, g)
 
 
+UNEVEN = [
+    # (height, width, row_cuts, col_cuts, halo, guard)
+    (300, 260, [0, 40, 96, 150, 200, 300], [0, 33, 100, 181, 260], 14, 6),
+    (97, 120, [0, 12, 97], [0, 50, 51, 120], 5, 1),
+]
+
+
+@pytest.mark.parametrize("cfg", UNEVEN)
+def test_partition_cuts_matches_oracle(L, FC, cfg):
+    """litho_partition_create_cuts: uneven Cores, one tile size = largest Core + 2 halo
+    (even), geometry and neighbour relations as the oracle's Partition::build over the
+    same cuts; tile copies and the Core stitch are exact."""
+    H, W, rc, cc, halo, guard = cfg
+    meta = fc.build(H, W, len(rc) - 1, len(cc) - 1, halo, guard, row_cuts=rc, col_cuts=cc)
+    part = FC.Partition(H, W, len(rc) - 1, len(cc) - 1, halo, guard, row_cuts=rc, col_cuts=cc)
+    assert part.tile_size == meta.tile_size and part.num_tiles == len(meta.tiles)
+    for a, b in zip(part.tiles, meta.tiles):
+        assert (a.row, a.col) == (b.row, b.col)
+        assert rect(a.core_global) == rect(b.core_global)
+        assert rect(a.tile_global) == rect(b.tile_global)
+        assert rect(a.core_local) == rect(b.core_local)
+        assert rect(a.update_local) == rect(b.update_local)
+    g = np.random.default_rng(4).random((H, W)).astype(np.float32)
+    tiles = part.extract_all(torch.from_numpy(g).cuda())
+    assert np.array_equal(tiles.cpu().numpy(), np.stack([fc.extract_local_tile(g, t)
+                                                          for t in meta.tiles]))
+    assert np.array_equal(part.assemble_global(tiles).cpu().numpy(), g)
+    # equal cuts give the default partition
+    eq = FC.Partition(H, W, 2, 3, halo, guard, row_cuts=[0, H // 2, H],
+                      col_cuts=[0, W // 3, 2 * W // 3, W])
+    ref = FC.Partition(H, W, 2, 3, halo, guard)
+    assert [rect(t.tile_global) for t in eq.tiles] == [rect(t.tile_global) for t in ref.tiles]
+    with pytest.raises(L.LithoError):
+        FC.Partition(H, W, 2, 1, halo, guard, row_cuts=[1, 40, H], col_cuts=[0, W])
+    with pytest.raises(L.LithoError):   # a Core narrower than the guard
+        FC.Partition(H, W, 2, 1, halo, 6, row_cuts=[0, 3, H], col_cuts=[0, W])
+
+
+@pytest.mark.parametrize("prec", ["fp32", "bf16x3"])
+def test_uneven_layout_exchange_and_lsm_match_oracle(L, FC, band128, prec):
+    """Micro tiles over uneven Cores (33-100 px, 20 tiles of 128^2): the exchange and
+    three full-chip LSM steps against the FP64 oracle over the same cuts, the stitched
+    Core mask included. Tolerances as the even-layout tests of each precision; the
+    split-BF16 exchange runs all 20 tiles in one batched pass and in passes of at most 8
+    tiles, with the same results bit for bit."""
+    oc, _ = band128
+    H, W, rc, cc, halo, guard = UNEVEN[0]
+    meta = fc.build(H, W, len(rc) - 1, len(cc) - 1, halo, guard, row_cuts=rc, col_cuts=cc)
+    assert meta.tile_size == oc.N
+    ctx = L.Context()
+    ctx.set_precision(prec)
+    part = FC.Partition(H, W, len(rc) - 1, len(cc) - 1, halo, guard, ctx=ctx, row_cuts=rc,
+                        col_cuts=cc)
+    cache = L.ImagingCache.from_kernels(np.stack(oc.kernels), oc.source_ws, oc.eigenvalues, ctx=ctx)
+    target = make_target(H, W, 71)
+    rng = np.random.default_rng(72)
+    theta_g = io.initialize_theta(target) + 0.3 * rng.standard_normal(target.shape)
+    masks32 = [io.theta_to_mask(fc.extract_local_tile(theta_g, t)
+                                + 0.05 * rng.standard_normal((meta.tile_size,) * 2)).astype(np.float32)
+               for t in meta.tiles]
+    opts = OPTION_SETS[1]
+    ev = fc.exchange([m.astype(np.float64) for m in masks32], target, meta, oc, THR, ALPHA,
+                     fc.ExchangeOptions(**opts))
+    ex = FC.MicroGradientExchange(part, cache, THR, ALPHA)
+    gpu_masks = torch.from_numpy(np.stack(masks32)).cuda()
+    gpu_target = torch.from_numpy(target.astype(np.float32)).cuda()
+    res = ex.compute(gpu_masks, gpu_target, FC.MicroGradientOptions(**opts))
+    tol = 1e-4 if prec == "fp32" else 1e-3
+    raw, grad = cpu(res.raw_gradients), cpu(res.mask_gradients)
+    for t in meta.tiles:
+        o = ev["locals"][t.id]
+        assert rel_l2(raw[t.id], o["raw"]) < tol, t.id
+        assert rel_l2(grad[t.id], o["grad"]) < tol, t.id
+    assert abs(res.loss - ev["loss"]) <= 10 * tol * ev["loss"]
+    if prec == "bf16x3":
+        ctx.set_exchange_group(8)
+        res8 = ex.compute(gpu_masks, gpu_target, FC.MicroGradientOptions(**opts))
+        assert np.array_equal(cpu(res8.mask_gradients), grad) and res8.loss == res.loss
+        ctx.set_exchange_group(0)
+    lopts = dict(enable_cept=True, enable_grad_fusion=True)
+    kw = dict(dx=1.0, dy=1.0, cfl=0.7, b=0.01, reinit_interval=2, mask_type="Binary",
+              render_scale=4)
+    ref = fc.full_chip_lsm(target, target, meta, oc, THR, ALPHA, fc.ExchangeOptions(**lopts), 3,
+                           **kw)
+    optz = FC.FullChipLSMOptimizer(part, cache, THR, ALPHA)
+    out = optz.optimize(gpu_target, gpu_target,
+                        FC.FullChipLSMOptions(iterations=3, cfl=0.7, curvature_weight=0.01,
+                                              reinit_interval=2, mask_type="Binary",
+                                              render_scale=4,
+                                              gradient_options=FC.MicroGradientOptions(**lopts)))
+    for a, b in zip(out.history, ref["history"]):
+        assert abs(a.loss - b["loss"]) <= 1e-3 * b["loss"]
+    assert out.best_iteration == ref["best"]["iteration"]
+    gm = cpu(out.global_mask)
+    assert gm.shape == (H, W)
+    assert (np.abs(gm - ref["global_mask"]) > 1e-6).mean() <= 0.005
+    part.close()
+    ctx.close()
+
+
 def make_target(H, W, seed):
     rng = np.random.default_rng(seed)
     t = np.zeros((H, W))
@@ -132,16 +232,18 @@ def test_exchange_matches_oracle(L, FC, band128, oi):
 
 @pytest.mark.parametrize("oi", range(len(OPTION_SETS)))
 def test_exchange_bf16x3_batched_matches_oracle(L, FC, band128, oi):
-    """Split-BF16 mode: the exchange images the tiles in batched passes (groups of 16
-    tiles; 20 tiles here, so two groups, the second partial). Raw and exchanged
-    gradients within the split-BF16 tolerance (relative L2 <= 1e-3 per tile), PE and
-    penalty sums relative 1e-4, CEPT (mask-only) relative 1e-6."""
+    """Split-BF16 mode: the exchange images the tiles in batched passes (20 tiles here:
+    one pass of all of them, or, for the even option sets, passes of at most 16 tiles,
+    the second partial). Raw and exchanged gradients within the split-BF16 tolerance
+    (relative L2 <= 1e-3 per tile), PE and penalty sums relative 1e-4, CEPT (mask-only)
+    relative 1e-6."""
     oc, _ = band128
     cfg = (480, 384, 5, 4, 16, 6)
     meta = fc.build(*cfg)
     assert meta.tile_size == oc.N and len(meta.tiles) == 20
     ctx = L.Context()
     ctx.set_precision("bf16x3")
+    ctx.set_exchange_group(16 if oi % 2 == 0 else 0)
     part = FC.Partition(*cfg, ctx=ctx)
     cache = L.ImagingCache.from_kernels(np.stack(oc.kernels), oc.source_ws, oc.eigenvalues, ctx=ctx)
     target = make_target(cfg[0], cfg[1], 40 + oi)

@@ -139,3 +139,22 @@ def test_region_eps_local_periodic_copies():
     # copies one layout up / left land in the Guard: y 31.5 - 32 = -0.5, x 30.6 - 32 = -1.4
     assert (7.5, 12.0) in got and (10.0, 6.6) in got and (24.0, 11.0) in got
     assert len(le) == len(lw) == 5
+
+
+def test_partition_geometry_with_cuts():
+    """Partition::build over caller-given Core boundaries: the reference's own cuts
+    reproduce the default partition; uneven cuts keep one tile size (largest Core +
+    2 halo, rounded even), Core + halo origins, and a Core stitch that is exact."""
+    a = fc.build(25, 31, 2, 3, 3, 1)
+    b = fc.build(25, 31, 2, 3, 3, 1, row_cuts=[0, 12, 25], col_cuts=[0, 10, 20, 31])
+    assert a == b
+    meta = fc.build(60, 50, 3, 2, 4, 2, row_cuts=[0, 5, 45, 60], col_cuts=[0, 17, 50])
+    assert meta.tile_size == 40 + 8
+    t = meta.tiles[1 * 2 + 1]
+    assert t.core_global == fc.Rect(5, 45, 17, 50)
+    assert t.tile_global == fc.Rect(1, 49, 13, 61)
+    top = [n for n in t.neighbors if n.direction == fc.TOP][0]
+    assert top.guard_global == fc.Rect(3, 5, 17, 50)
+    g = np.random.default_rng(1).random((60, 50))
+    locs = [fc.extract_local_tile(g, tt) for tt in meta.tiles]
+    assert np.array_equal(fc.assemble_global(locs, meta), g)
