@@ -614,7 +614,9 @@ int run_forward(Context* ctx, const Cache& c, Field& f, const Layout& L, int inp
   ctx->stage_begin(0);
   const bool tc = ctx->precision == LITHO_PRECISION_BF16X3 && c.TXS_img;
   const bool pers = tc && ctx->tc_persistent();
-  if (tc && pers && tc3_analysis_supported(g.Nc, g.Nr))
+  const bool fwd_tc3 = tc && pers && tc3_analysis_supported(g.Nc, g.Nr);
+  ctx->fwd_part_trows = fwd_tc3 ? g.Nr : 0;   // the persistent analysis stores [c][row]
+  if (fwd_tc3)
     st = check_launch(ctx, launch_analysis_tc3(s, input_mode, input, mask_out, flag, g.N, g.Nc,
                                                g.Nr, g.Nr, 0, at<float2>(ctx, L.part), c.TXS_img,
                                                c.TYS_img, flag + 1, batch),
@@ -632,7 +634,8 @@ int run_forward(Context* ctx, const Cache& c, Field& f, const Layout& L, int inp
   if (st) return st;
   ctx->stage_begin(1);
   st = check_launch(ctx, launch_reduce_tiles(s, at<float2>(ctx, L.part), L.tiles, g.Nr * g.Nc,
-                                             1.f / ((float)g.N * g.N), f.mband, batch),
+                                             1.f / ((float)g.N * g.N), f.mband, batch,
+                                             ctx->fwd_part_trows),
                     "tile reduction");
   ctx->stage_end(1);
   if (st) return st;
@@ -649,7 +652,9 @@ int run_forward(Context* ctx, const Cache& c, Field& f, const Layout& L, int inp
   ctx->stage_begin(3);
   if (tc) {
     int* err = reinterpret_cast<int*>(ctx->d_red + RED_FLAG) + 1;
-    if (fuse_adjoint && pers && tc3_fused_supported(g.kp_rows, g.Nc, g.Nr))
+    const bool fused_tc3 = fuse_adjoint && pers && tc3_fused_supported(g.kp_rows, g.Nc, g.Nr);
+    if (fuse_adjoint) ctx->adj_part_trows = fused_tc3 ? 2 * g.Nr - 1 : 0;
+    if (fused_tc3)
       st = check_launch(ctx, launch_synth_resist_analysis_tc3(
                                  s, c.AYD_img, at<void>(ctx, L.img), g.N, g.kp_rows, ep, g.Nc,
                                  g.Nr, at<float2>(ctx, L.part), flag, c.TXD_img, c.TYD_img, err,
@@ -691,6 +696,7 @@ int run_adjoint(Context* ctx, const Cache& c, const Field& f, const Layout& L, c
   ctx->stage_begin(4);
   const bool tc = ctx->precision == LITHO_PRECISION_BF16X3 && c.TXD_img;
   const bool pers = tc && ctx->tc_persistent();
+  if (!analysed) ctx->adj_part_trows = tc && pers && tc3_analysis_supported(g.Nc, g.Nr) ? na : 0;
   if (analysed)
     st = LITHO_OK;  // the partials are already in L.part
   else if (tc && pers && tc3_analysis_supported(g.Nc, g.Nr))
@@ -711,7 +717,8 @@ int run_adjoint(Context* ctx, const Cache& c, const Field& f, const Layout& L, c
   if (st) return st;
   ctx->stage_begin(5);
   st = check_launch(ctx, launch_reduce_tiles(s, at<float2>(ctx, L.part), L.tiles, na * g.Nc,
-                                             1.f / ((float)g.N * g.N), at<float2>(ctx, L.gh), batch),
+                                             1.f / ((float)g.N * g.N), at<float2>(ctx, L.gh), batch,
+                                             ctx->adj_part_trows),
                     "adjoint tile reduction");
   ctx->stage_end(5);
   if (st) return st;

@@ -259,8 +259,8 @@ cudaError_t launch_analysis(cudaStream_t s, int mode, const float* in, float* ma
 // RT_E consecutive entries, so each group's loads are coalesced.
 constexpr int RT_E = 16, RT_G = 32;
 __global__ void __launch_bounds__(RT_E * RT_G)
-reduce_tiles_kernel(const float2* __restrict__ part, int tiles, int count, float scale,
-                    float2* __restrict__ out) {
+reduce_tiles_kernel(const float2* __restrict__ part, int tiles, int count, int trows,
+                    float scale, float2* __restrict__ out) {
   pdl_trigger();
   pdl_wait();
   part += (size_t)blockIdx.y * tiles * count;   // image b of a batch: [b][tile][entry]
@@ -287,13 +287,16 @@ reduce_tiles_kernel(const float2* __restrict__ part, int tiles, int count, float
     }
     __syncthreads();
   }
-  if (g == 0 && o < count) out[o] = make_float2(sh[0][e].x * scale, sh[0][e].y * scale);
+  // Entry o of a tile block is (row, c) = (o / ncols, o % ncols), or with trows > 0
+  // (column-major blocks of trows rows) (o % trows, o / trows); out is row-major.
+  const int oo = trows > 0 ? (o % trows) * (count / trows) + o / trows : o;
+  if (g == 0 && o < count) out[oo] = make_float2(sh[0][e].x * scale, sh[0][e].y * scale);
 }
 
 cudaError_t launch_reduce_tiles(cudaStream_t s, const float2* part, int tiles, int count,
-                                float scale, float2* out, int batch) {
+                                float scale, float2* out, int batch, int trows) {
   return launch_pdl(reduce_tiles_kernel, dim3((count + RT_E - 1) / RT_E, batch),
-                    dim3(RT_E * RT_G), 0, s, part, tiles, count, scale, out);
+                    dim3(RT_E * RT_G), 0, s, part, tiles, count, trows, scale, out);
 }
 
 // ---------------------------------------------------------------- row synthesis

@@ -183,6 +183,10 @@ struct Context {
   // Largest number of micro tiles per batched pass of the exchange (0: as many as the
   // scratch budget allows); litho_ctx_set_exchange_group.
   int exchange_group_max = 0;
+  // Layout of the tile partials the last analysis launch left in the scratch, for
+  // the reduction that follows it: 0 row-major, else column-major with this many rows
+  // (forward and adjoint analyses; the adjoint's may come from the fused synthesis).
+  int fwd_part_trows = 0, adj_part_trows = 0;
   bool tc_persistent() const { return tc_schedule != LITHO_TC_SCHEDULE_PER_TILE; }
 };
 
@@ -217,9 +221,11 @@ int analysis_tiles(int N);
 cudaError_t launch_analysis(cudaStream_t s, int mode, const float* in, float* mask_out,
                             int* flag, const float* tw, int N, int ncols, const float2* TY,
                             int nrows_out, int nr, int sym, float2* part);
-// out[o] = scale * sum_t part[o][t] (fixed order).
+// out[o] = scale * sum_t part[o][t] (fixed order). Tile blocks are row-major [row][c],
+// or column-major [c][row] with trows rows when trows > 0 (the persistent tensor-core
+// analyses); out is row-major either way.
 cudaError_t launch_reduce_tiles(cudaStream_t s, const float2* part, int tiles, int count,
-                                float scale, float2* out, int batch = 1);
+                                float scale, float2* out, int batch = 1, int trows = 0);
 // Small-grid stage of the forward: f.mband -> f.e, ik, iP and Ut (the row
 // synthesis operand), or, with img set, Ut's split-BF16 operand image for the
 // tensor-core synthesis (launch_pack_tc2_rows layout) instead of Ut.

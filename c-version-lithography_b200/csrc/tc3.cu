@@ -204,7 +204,10 @@ __device__ __forceinline__ void r_to_operand(uint32_t acc, uint8_t* sR, int lane
 // Q (tensor memory: lanes n = 2 r + s, columns f = 2 c + t) -> the tile's partials
 // P[r][c] of the band (see analysis_stages in tc2.cu): Re = Q[2r][2c] - Q[2r+1][2c+1],
 // Im = Q[2r][2c+1] + Q[2r+1][2c]; with sym also the conjugate rows -r (from the odd
-// lane of the pair).
+// lane of the pair). The tile's block is stored column-major, P[c][row] at
+// out + c nrows_out + row, so that a warp's store of one column touches two runs of
+// consecutive rows instead of 32 rows ncols apart (reduce_tiles_kernel with trows =
+// nrows_out reads this layout).
 template <int BN>
 __device__ __forceinline__ void q_to_partials(uint32_t acc, float2* out, const Tc2Analysis& a,
                                               int lane_base, int q0, int dq) {
@@ -215,11 +218,11 @@ __device__ __forceinline__ void q_to_partials(uint32_t acc, float2* out, const T
   float2* row = nullptr;
   if (r < a.nr) {
     if (!a.sym)
-      row = s == 0 ? out + r * a.ncols : nullptr;
+      row = s == 0 ? out + r : nullptr;
     else if (s == 0)
-      row = out + (a.nr - 1 + r) * a.ncols;
+      row = out + (a.nr - 1 + r);
     else if (r >= 1)
-      row = out + (a.nr - 1 - r) * a.ncols;
+      row = out + (a.nr - 1 - r);
   }
 #pragma unroll 1
   for (int q = q0; q < BN / 16; q += dq) {
@@ -228,13 +231,14 @@ __device__ __forceinline__ void q_to_partials(uint32_t acc, float2* out, const T
 #pragma unroll
     for (int i = 0; i < 16; ++i) pv[i] = __shfl_xor_sync(0xffffffffu, qv[i], 1);
     if (row == nullptr) continue;
-    float2* rq = row + 8 * q;
+    float2* rq = row + (size_t)(8 * q) * a.nrows_out;
     const int nc = a.ncols - 8 * q;
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
       if (i >= nc) break;
       const float o0 = qv[2 * i], o1 = qv[2 * i + 1], p0 = pv[2 * i], p1 = pv[2 * i + 1];
-      rq[i] = s == 0 ? make_float2(o0 - p1, o1 + p0) : make_float2(p0 + o1, p1 - o0);
+      rq[(size_t)i * a.nrows_out] = s == 0 ? make_float2(o0 - p1, o1 + p0)
+                                           : make_float2(p0 + o1, p1 - o0);
     }
   }
 }
