@@ -60,6 +60,10 @@ def parse():
                         "layout; 'equal' cuts it into --fullchip-grid equal Cores per side")
     p.add_argument("--fullchip-grid", type=int, default=16,
                    help="micro tiles per side of the full-chip layout")
+    p.add_argument("--profile", default="", choices=["", "ctm", "levelset"],
+                   help="for profilers: run only --steps untimed calls of the batched split-BF16 "
+                        "CTM evaluation (--batch tiles of --size^2, graphs off) or of the batched "
+                        "RK2 level-set update (--batch images of --size^2), print nothing else")
     p.add_argument("--serving-requests", type=int, default=1000,
                    help="LSM tile solves of the serving stream reported beside the headline "
                         "(0 skips it)")
@@ -861,9 +865,42 @@ def _ncu_traffic(stage, N, precision):
         return None
 
 
+def profile_run(args):
+    """The bench's batched workloads alone, without timing, for a profiler's capture
+    (ncu -k <kernel> -s <skipped launches> -c <captured launches>): `steps` batched
+    split-BF16 CTM evaluations of the headline workload with graphs off (every kernel
+    launched directly), or `steps` batched RK2 level-set updates."""
+    import torch
+    L = importlib.import_module("c-version-lithography_b200")
+    N, K, B = args.size, args.kernels, max(1, args.batch)
+    if args.profile == "ctm":
+        band, r0, c0, w, wss, _, _ = workload(N, K, seed=1)
+        tiles = [workload(N, K, seed=1 + b)[5:] for b in range(B)]
+        ctx = L.Context(0, stream=torch.cuda.Stream())
+        ctx.set_precision("bf16x3")
+        ctx.enable_graphs(False)
+        cache = L.ImagingCache.from_band(N, band, r0, c0, w, wss, ctx=ctx)
+        th = torch.tensor(np.stack([t[1] for t in tiles]), dtype=torch.float32, device="cuda")
+        tg = torch.tensor(np.stack([t[0] for t in tiles]), dtype=torch.float32, device="cuda")
+        gr = torch.empty_like(th)
+        for _ in range(args.steps):
+            L.ctm_evaluate_batch(cache, th, tg, THRESHOLD, ALPHA, gr)
+    else:
+        yy, xx = np.mgrid[0:N, 0:N].astype(np.float32)
+        phi = torch.tensor(np.stack([N / 6 + 20 * b - np.hypot(yy - N / 2, xx - N / 2 + 8 * b)
+                                     for b in range(B)]), dtype=torch.float32, device="cuda")
+        vn = 0.01 * torch.randn(B, N, N, device="cuda")
+        out, mask = torch.empty_like(phi), torch.empty_like(phi)
+        for _ in range(args.steps):
+            L.LevelSetUtils.rk2_update_batch(phi, vn, 2.0, 2.0, 0.5, 0.01, out, mask)
+    torch.cuda.synchronize()
+
+
 def main():
     args = parse()
-    if args.impl == "reference":
+    if args.profile:
+        profile_run(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)
