@@ -964,18 +964,30 @@ fused_tc3_kernel(const uint8_t* __restrict__ Aimg, const uint8_t* __restrict__ B
       float s0 = 0.f, s1 = 0.f;
       bool bad;
       if (lean && xin && yb + 31 < N) {
-        // Every dL/dI is non-finite exactly when its r is, and then so is r * r in s0 or
-        // the product with 0 in chk (the window-free arithmetic of S3Resist::dldi).
-        float chk = 0.f;
+        // The window-free arithmetic of S3Resist::dldi on pixel pairs in packed FP32x2
+        // (each lane rounded as the scalar operation, in the scalar order, so dL/dI is
+        // the per-tile kernels' bit for bit; __expf and the reciprocal stay per lane).
+        // Every dL/dI is non-finite exactly when its r is, and then so is the product
+        // with 0 in chk. The loss terms are summed in two interleaved FP32 chains.
+        float2 chk = make_float2(0.f, 0.f), se = chk;
+        const float2 na = make_float2(-r.p.alpha, -r.p.alpha);
+        const float2 nt = make_float2(-r.p.thr, -r.p.thr);
+        const float2 one = make_float2(1.f, 1.f), pw = make_float2(r.p.pe_weight, r.p.pe_weight);
 #pragma unroll
-        for (int e = 0; e < 32; ++e) {
-          const float W = r.sigmoid(d[e]);
-          const float rr = W - pre[e];
-          s0 += rr * rr;
-          d[e] = r.p.pe_weight * rr * W * (1.f - W);
-          chk = __fmaf_rn(d[e], 0.f, chk);
+        for (int e = 0; e < 32; e += 2) {
+          const float2 z = __fmul2_rn(na, __fadd2_rn(make_float2(d[e], d[e + 1]), nt));
+          const float2 den = __fadd2_rn(one, make_float2(__expf(z.x), __expf(z.y)));
+          const float2 W = make_float2(__fdividef(1.f, den.x), __fdividef(1.f, den.y));
+          const float2 rr = __fadd2_rn(W, make_float2(-pre[e], -pre[e + 1]));
+          se = __ffma2_rn(rr, rr, se);
+          const float2 g = __fmul2_rn(__fmul2_rn(__fmul2_rn(pw, rr), W),
+                                      __fadd2_rn(one, make_float2(-W.x, -W.y)));
+          chk = __ffma2_rn(g, make_float2(0.f, 0.f), chk);
+          d[e] = g.x;
+          d[e + 1] = g.y;
         }
-        bad = chk != 0.f;
+        s0 = se.x + se.y;
+        bad = chk.x + chk.y != 0.f;
       } else {
         const bool plain = r.plain();
         bad = false;
