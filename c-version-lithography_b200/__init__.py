@@ -110,6 +110,7 @@ SIGNATURES = {
     "litho_ctx_launch_count": (ctypes.c_longlong, [_P]),
     "litho_ctx_enable_graphs": (_I, [_P, _I]),
     "litho_ctx_set_tc_schedule": (_I, [_P, _I]),
+    "litho_ctx_tuned_schedule": (_I, [_P, _I, _I, _PI, _PI]),
     "litho_ctx_set_exchange_group": (_I, [_P, _I]),
     "litho_ctx_enable_stage_timing": (_I, [_P, _I]),
     "litho_ctx_stage_times": (_I, [_P, _PD, ctypes.POINTER(ctypes.c_longlong)]),
@@ -305,15 +306,22 @@ class Context:
 
     def autotune(self, cache=None, batch: int = 1, shape=None, nimg: int = 0):
         """Time the candidate schedules on this GPU and keep the fastest for the calls
-        that follow (litho_ctx_autotune): with `cache`, the small-grid chunk width for
-        `batch` images of it; with `shape` (rows, cols) and nimg > 0, the chamfer CTA
-        size of reinit_sdf for nimg such images. Returns the choices."""
+        that follow (litho_ctx_autotune): with `cache`, the small-grid schedule and (split
+        BF16, schedule 'auto') the tensor-core schedule for `batch` images of it; with
+        `shape` (rows, cols) and nimg > 0, the chamfer CTA size of reinit_sdf for nimg
+        such images. Returns the choices."""
         bw, ct = ctypes.c_int(), ctypes.c_int()
         rows, cols = shape if shape is not None else (0, 0)
         self._check(self.lib.litho_ctx_autotune(self.handle, cache.handle if cache else None,
                                                 int(batch), int(rows), int(cols), int(nimg),
                                                 ctypes.byref(bw), ctypes.byref(ct)))
-        return {"band_chunk_width": bw.value, "chamfer_threads": ct.value}
+        out = {"band_chunk_width": bw.value, "chamfer_threads": ct.value}
+        if cache is not None:
+            tw, ts = ctypes.c_int(), ctypes.c_int()
+            self._check(self.lib.litho_ctx_tuned_schedule(self.handle, cache.N, int(batch),
+                                                          ctypes.byref(tw), ctypes.byref(ts)))
+            out["tc_schedule"] = {0: None, 1: "per_tile", 2: "persistent"}.get(ts.value)
+        return out
 
     def close(self):
         if getattr(self, "handle", None):

@@ -279,6 +279,17 @@ int litho_ctx_enable_graphs(litho_ctx* ctx, int on) {
   return LITHO_OK;
 }
 
+int litho_ctx_tuned_schedule(const litho_ctx* ctx, int N, int batch, int* band_width,
+                             int* tc_schedule) {
+  if (!ctx) return LITHO_ERR_INVALID_ARGUMENT;
+  if (band_width) *band_width = ctx->band_width(N, batch);
+  if (tc_schedule) {
+    const auto it = ctx->tuned_tc.find({N, batch});
+    *tc_schedule = it == ctx->tuned_tc.end() ? 0 : it->second;
+  }
+  return LITHO_OK;
+}
+
 int litho_ctx_set_exchange_group(litho_ctx* ctx, int max_tiles) {
   if (!ctx || max_tiles < 0) return LITHO_ERR_INVALID_ARGUMENT;
   ctx->exchange_group_max = max_tiles;
@@ -613,7 +624,7 @@ int run_forward(Context* ctx, const Cache& c, Field& f, const Layout& L, int inp
   int st;
   ctx->stage_begin(0);
   const bool tc = ctx->precision == LITHO_PRECISION_BF16X3 && c.TXS_img;
-  const bool pers = tc && ctx->tc_persistent();
+  const bool pers = tc && ctx->tc_persistent(g.N, batch);
   const bool fwd_tc3 = tc && pers && tc3_analysis_supported(g.Nc, g.Nr);
   ctx->fwd_part_trows = fwd_tc3 ? g.Nr : 0;   // the persistent analysis stores [c][row]
   if (fwd_tc3)
@@ -695,7 +706,7 @@ int run_adjoint(Context* ctx, const Cache& c, const Field& f, const Layout& L, c
   int st;
   ctx->stage_begin(4);
   const bool tc = ctx->precision == LITHO_PRECISION_BF16X3 && c.TXD_img;
-  const bool pers = tc && ctx->tc_persistent();
+  const bool pers = tc && ctx->tc_persistent(g.N, batch);
   if (!analysed) ctx->adj_part_trows = tc && pers && tc3_analysis_supported(g.Nc, g.Nr) ? na : 0;
   if (analysed)
     st = LITHO_OK;  // the partials are already in L.part
@@ -1033,7 +1044,7 @@ static int ctm_evaluate_impl(litho_ctx* ctx, const litho_cache* cache, litho_fie
                           cache->H,    cache->AYD_img, cache->TXS,
                           reinterpret_cast<const void*>(
                               (uintptr_t)ctx->precision |
-                              ((uintptr_t)ctx->tc_persistent() << 4))};
+                              ((uintptr_t)ctx->tc_persistent(cache->g.N, 1) << 4))};
   for (int i = 0; i < 16; ++i) key.ptr[i] = ptrs[i];
   const int geom[6] = {g.N, g.K, g.Nr, g.Nc, g.row0, g.col0};
   for (int i = 0; i < 6; ++i) key.geom[i] = geom[i];
@@ -1172,7 +1183,7 @@ int litho_ctm_evaluate_batch(litho_ctx* ctx, const litho_cache* cache, int batch
                           cache->H, cache->AYD_img, cache->TXS_img, cache->TXD_img,
                           reinterpret_cast<const void*>((uintptr_t)batch),
                           reinterpret_cast<const void*>(
-                              (uintptr_t)ctx->precision | ((uintptr_t)ctx->tc_persistent() << 4) |
+                              (uintptr_t)ctx->precision | ((uintptr_t)ctx->tc_persistent(g.N, batch) << 4) |
                               ((uintptr_t)ctx->band_width(g.N, batch) << 8))};
   for (int i = 0; i < 16; ++i) key.ptr[i] = ptrs[i];
   const int geom[6] = {g.N, g.K, g.Nr, g.Nc, g.row0, g.col0};
@@ -1712,6 +1723,38 @@ int litho_ctx_autotune(litho_ctx* ctx, const litho_cache* cache, int batch, int 
     if (!st) {
       ctx->tuned_band[{cache->g.N, batch}] = bw;
       if (band_width) *band_width = bw;
+    }
+    // Schedule of the split-BF16 tensor-core passes (per-tile CTAs or the persistent
+    // pipelines) for `batch` images, when the context leaves it to the tuner: the
+    // whole batched CTM chain timed with each, on zero theta and target images.
+    if (!st && tc && ctx->tc_schedule == LITHO_TC_SCHEDULE_AUTO) {
+      const size_t px = (size_t)cache->g.N * cache->g.N * batch;
+      float* buf = nullptr;
+      if (cudaMalloc(&buf, 3 * px * sizeof(float)) != cudaSuccess) {
+        cudaGetLastError();
+        st = ctx->fail(LITHO_ERR_OOM, "autotune buffers");
+      }
+      if (!st) LITHO_CUDA_TRY(ctx, cudaMemsetAsync(buf, 0, 3 * px * sizeof(float), s));
+      double* d_sums = ctx->d_red + RED_PART + 3 * (size_t)L.tiles * batch;
+      float best_tc = 0.f;
+      int pick = LITHO_TC_SCHEDULE_PERSISTENT;
+      for (const int sched : {LITHO_TC_SCHEDULE_PERSISTENT, LITHO_TC_SCHEDULE_PER_TILE}) {
+        if (st) break;
+        ctx->tuned_tc[{cache->g.N, batch}] = sched;
+        float ms = 0.f;
+        int cst = LITHO_OK;
+        st = timed([&]() -> cudaError_t {
+          cst = ctm_batch_chain(ctx, *cache, L, batch, buf, buf + px, 0.225, 50.0, buf + 2 * px,
+                                d_sums);
+          return cst ? cudaErrorUnknown : cudaSuccess;
+        }, &ms);
+        if (!st && ms > 0.f && (best_tc == 0.f || ms < best_tc)) { best_tc = ms; pick = sched; }
+      }
+      if (buf) {
+        cudaStreamSynchronize(s);
+        cudaFree(buf);
+      }
+      ctx->tuned_tc[{cache->g.N, batch}] = pick;
     }
   }
   if (!st && nimg > 0) {

@@ -187,7 +187,15 @@ struct Context {
   // the reduction that follows it: 0 row-major, else column-major with this many rows
   // (forward and adjoint analyses; the adjoint's may come from the fused synthesis).
   int fwd_part_trows = 0, adj_part_trows = 0;
-  bool tc_persistent() const { return tc_schedule != LITHO_TC_SCHEDULE_PER_TILE; }
+  // The schedule used for `batch` images of size N: the set one, or under
+  // LITHO_TC_SCHEDULE_AUTO the one litho_ctx_autotune chose for (N, batch), else the
+  // persistent pipelines.
+  std::map<std::pair<int, int>, int> tuned_tc;
+  bool tc_persistent(int N, int batch) const {
+    if (tc_schedule != LITHO_TC_SCHEDULE_AUTO) return tc_schedule == LITHO_TC_SCHEDULE_PERSISTENT;
+    const auto it = tuned_tc.find({N, batch});
+    return it == tuned_tc.end() || it->second == LITHO_TC_SCHEDULE_PERSISTENT;
+  }
 };
 
 // ---------------------------------------------------------------- launch helper

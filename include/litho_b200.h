@@ -46,8 +46,10 @@ extern "C" {
                                         tensor cores in split BF16 (hi*hi + hi*lo + lo*hi,
                                         FP32 accumulation) */
 
-#define LITHO_TC_SCHEDULE_AUTO 0       /* persistent where the band fits its shared-memory
-                                          plan, else per tile (the default) */
+#define LITHO_TC_SCHEDULE_AUTO 0       /* the one litho_ctx_autotune chose for the size
+                                          and batch, else persistent; per tile where the
+                                          band does not fit the persistent kernels'
+                                          shared-memory plan (the default) */
 #define LITHO_TC_SCHEDULE_PER_TILE 1   /* one CTA per 128 x 128 tile, phases in order */
 #define LITHO_TC_SCHEDULE_PERSISTENT 2 /* one CTA per SM over a share of the (image, tile)
                                           items, warp-specialised and pipelined */
@@ -314,13 +316,21 @@ int litho_ctx_reserve(litho_ctx* ctx, const litho_cache* cache, int batch);
  * the context for the calls that follow. With a cache: the schedule of the
  * small-grid field and Z kernels for `batch` images of that cache (8 or 16 columns
  * per CTA, or 128: the whole small grid per CTA), timed on the forward and adjoint
- * band stages (results do not depend on it, bit for bit). With
+ * band stages (results do not depend on it, bit for bit); in
+ * LITHO_PRECISION_BF16X3 under LITHO_TC_SCHEDULE_AUTO also the schedule of the
+ * tensor-core passes for that batch (per-tile CTAs or the persistent pipelines), timed
+ * on the whole batched CTM chain (images agree bit for bit between the schedules; the
+ * loss sums may differ in their last bits). With
  * nimg > 0: the CTA size (128, 256, 512 or 1024 threads) of the chamfer transform of
  * reinit_sdf for nimg images of rows x cols (the batched re-initialisations of that
  * many images use it; the result may differ from another CTA size's in the last
  * bit). Writes the choices (0: not tuned) to band_width / chamfer_threads (nullable). */
 int litho_ctx_autotune(litho_ctx* ctx, const litho_cache* cache, int batch, int rows, int cols,
                        int nimg, int* band_width, int* chamfer_threads);
+/* The schedules the autotuner chose for `batch` images of size N (0: not tuned):
+ * band_width as litho_ctx_autotune reports it, tc_schedule a LITHO_TC_SCHEDULE_* value. */
+int litho_ctx_tuned_schedule(const litho_ctx* ctx, int N, int batch, int* band_width,
+                             int* tc_schedule);
 /* Vector kernels of the CTM L-BFGS driver (CTM_Optimizer.cpp:189-227, LBFGS++'s
  * two-loop recursion evaluated on FP64 Gram matrices of the stored pairs).
  * litho_lbfgs_dots: out[j] = sum_i rows[j][i] v[i] accumulated in FP64 for the k
