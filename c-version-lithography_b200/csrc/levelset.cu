@@ -200,6 +200,9 @@ struct LsArgs {
   int dt_stride;
 };
 
+// WHAT (the mode, LsArgs::what) is a template parameter so that the per-pixel loop
+// carries no mode tests.
+template <int WHAT>
 __global__ void __launch_bounds__(LS_NT) levelset_kernel(LsArgs a) {
   const size_t img = (size_t)blockIdx.z * a.rows * a.cols;
   const float* phi = a.phi + img;
@@ -209,20 +212,20 @@ __global__ void __launch_bounds__(LS_NT) levelset_kernel(LsArgs a) {
     const int* w = a.wins + 4 * (size_t)blockIdx.z;
     wy0 = w[0]; wy1 = w[1]; wx0 = w[2]; wx1 = w[3];
   }
-  if (a.what >= 5) {  // elementwise modes
+  if (WHAT >= 5) {  // elementwise modes
     const int x = blockIdx.x * LS_TX + threadIdx.x % LS_TX;
     for (int r = 0; r < LS_RPT; ++r) {
       const int y = blockIdx.y * LS_TY * LS_RPT + threadIdx.x / LS_TX + r * LS_TY;
       if (y < a.rows && x < a.cols) {
         const size_t i = (size_t)y * a.cols + x;
         const bool in = y >= wy0 && y < wy1 && x >= wx0 && x < wx1;
-        if (a.what == 5)         // printed mask: phi >= 0 (LSM_Optimizer.cpp:128)
+        if (WHAT == 5)         // printed mask: phi >= 0 (LSM_Optimizer.cpp:128)
           out[i] = phi[i] >= 0.f ? 1.f : 0.f;
-        else if (a.what == 6)    // speed restricted to the update window
+        else if (WHAT == 6)    // speed restricted to the update window
           out[i] = in ? a.vn[img + i] : 0.f;
-        else if (a.what == 7)    // +-0.5 sign image of phi >= 0 (full_chip_lsm.cpp:229-230)
+        else if (WHAT == 7)    // +-0.5 sign image of phi >= 0 (full_chip_lsm.cpp:229-230)
           out[i] = phi[i] >= 0.f ? 0.5f : -0.5f;
-        else if (a.what == 9)    // mask - 0.5 (full_chip_lsm.cpp:143)
+        else if (WHAT == 9)    // mask - 0.5 (full_chip_lsm.cpp:143)
           out[i] = phi[i] - 0.5f;
         else                     // commit phi inside the window over phi0 (out may be phi0)
           out[i] = in ? phi[i] : a.phi0[img + i];
@@ -236,7 +239,7 @@ __global__ void __launch_bounds__(LS_NT) levelset_kernel(LsArgs a) {
   load_tile(t, phi, a.rows, a.cols, y0, x0);
   __syncthreads();
   const float idx = 1.f / a.dx, idy = 1.f / a.dy;
-  const float dt = (a.what >= 3) ? a.dt[(size_t)blockIdx.z * a.dt_stride] : 0.f;
+  const float dt = (WHAT >= 3) ? a.dt[(size_t)blockIdx.z * a.dt_stride] : 0.f;
   const float* phi0 = a.phi0 ? a.phi0 + img : nullptr;
   const float* vn = a.vn ? a.vn + img : nullptr;
   float* out2 = a.out2 ? a.out2 + img : nullptr;
@@ -246,26 +249,26 @@ __global__ void __launch_bounds__(LS_NT) levelset_kernel(LsArgs a) {
     const int y = y0 + ly, x = x0 + lx;
     if (y >= a.rows || x >= a.cols) continue;
     const size_t i = (size_t)y * a.cols + x;
-    if (a.what >= 3 && !(y >= wy0 && y < wy1 && x >= wx0 && x < wx1)) {
+    if (WHAT >= 3 && !(y >= wy0 && y < wy1 && x >= wx0 && x < wx1)) {
       // Outside the update window the step keeps phi (stage 1) / the starting phi (stage 2).
-      const float keep = a.what == 3 ? t[ly + LS_H][lx + LS_H] : __ldg(phi0 + i);
-      if (a.what == 4 && out2) out2[i] = keep >= 0.f ? 1.f : 0.f;
+      const float keep = WHAT == 3 ? t[ly + LS_H][lx + LS_H] : __ldg(phi0 + i);
+      if (WHAT == 4 && out2) out2[i] = keep >= 0.f ? 1.f : 0.f;
       out[i] = keep;
       continue;
     }
-    const float speed = a.what == 1 ? 0.f : __ldg(vn + i);
+    const float speed = WHAT == 1 ? 0.f : __ldg(vn + i);
     float v;
-    if (a.what == 0) {
+    if (WHAT == 0) {
       v = weno_delta(t, ly + LS_H, lx + LS_H, speed, idx, idy);
       if (out2) out2[i] = fabsf(speed);
-    } else if (a.what == 1) {
+    } else if (WHAT == 1) {
       v = kappa_term(t, ly + LS_H, lx + LS_H, y, x, a.rows, a.cols, a.dx, a.dy, a.b);
     } else {
       const float n = kappa_term(t, ly + LS_H, lx + LS_H, y, x, a.rows, a.cols, a.dx, a.dy, a.b) -
                       weno_delta(t, ly + LS_H, lx + LS_H, speed, idx, idy);
-      if (a.what == 2) {
+      if (WHAT == 2) {
         v = n;
-      } else if (a.what == 3) {
+      } else if (WHAT == 3) {
         v = t[ly + LS_H][lx + LS_H] + dt * n;
       } else {
         v = 0.5f * __ldg(phi0 + i) + 0.5f * (t[ly + LS_H][lx + LS_H] + dt * n);
@@ -292,7 +295,19 @@ cudaError_t launch_levelset(cudaStream_t s, int what, int rows, int cols, const 
   }
   dim3 g = ls_grid(rows, cols);
   g.z = nimg;
-  levelset_kernel<<<g, LS_NT, 0, s>>>(a);
+  switch (what) {
+    case 0: levelset_kernel<0><<<g, LS_NT, 0, s>>>(a); break;
+    case 1: levelset_kernel<1><<<g, LS_NT, 0, s>>>(a); break;
+    case 2: levelset_kernel<2><<<g, LS_NT, 0, s>>>(a); break;
+    case 3: levelset_kernel<3><<<g, LS_NT, 0, s>>>(a); break;
+    case 4: levelset_kernel<4><<<g, LS_NT, 0, s>>>(a); break;
+    case 5: levelset_kernel<5><<<g, LS_NT, 0, s>>>(a); break;
+    case 6: levelset_kernel<6><<<g, LS_NT, 0, s>>>(a); break;
+    case 7: levelset_kernel<7><<<g, LS_NT, 0, s>>>(a); break;
+    case 8: levelset_kernel<8><<<g, LS_NT, 0, s>>>(a); break;
+    case 9: levelset_kernel<9><<<g, LS_NT, 0, s>>>(a); break;
+    default: return cudaErrorInvalidValue;
+  }
   return cudaGetLastError();
 }
 
