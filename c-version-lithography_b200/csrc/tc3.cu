@@ -263,13 +263,16 @@ int sm_count() {
 // part[image][yt][xt][row][c]) from a persistent pipeline:
 //   warps 0-15  load the image tile (theta -> mask for mode 1), split it into the
 //               [hi | lo] operand sA;
-//   warp 20     (one thread) copies the TX tile (per xt) and the TY tile (per yt),
+//   warp 24     (one thread) copies the TX tile (per xt) and the TY tile (per yt),
 //               issues stage 1 R = sA . TX^T into accR[j & 1] and stage 2
 //               Q = TY . R^T into accQ[j & 1];
-//   warps 16-19 turn R into the stage-2 operand sR, and Q into the item's partials.
+//   warps 16-23 turn R into the stage-2 operand sR, and Q into the item's partials
+//               (two warps per lane quarter, each taking every other 16-column group).
 // Shared memory: TY 64 KiB | sA 64 KiB | TX | sR (BN x 128 split tiles, BN <= 96).
 // Tensor memory: 512 columns, accR[b] at 128 b, accQ[b] at 256 + 128 b.
-constexpr int A3_LOADW = 16, A3_MMAW = A3_LOADW + 4;
+// A3_TMW TMEM warps: warps A3_LOADW + i and A3_LOADW + i + 4 share the lane quarter i
+// of the accumulators and split its 16-column groups (even / odd).
+constexpr int A3_LOADW = 16, A3_TMW = 8, A3_MMAW = A3_LOADW + A3_TMW;
 constexpr int A3_NT = (A3_MMAW + 1) * 32;
 // chunks of 8 pixels per loader thread, rows between a thread's chunks
 constexpr int A3_CH = 2048 / (32 * A3_LOADW), A3_RS = 2 * A3_LOADW;
@@ -279,8 +282,8 @@ __global__ void __launch_bounds__(A3_NT, 1)
 analysis_tc3_kernel(Tc2Analysis a, int T, int B, const uint8_t* __restrict__ txImg,
                     const uint8_t* __restrict__ tyImg, int* __restrict__ err) {
   extern __shared__ __align__(1024) uint8_t smem_raw[];
-  // 0 sA full (16 loader warps), 1-2 stage 1 done [b], 3 sR full (4 TMEM warps),
-  // 4-5 stage 2 done [b], 6-7 accQ[b] free (4 TMEM warps), 8 TX landed, 9 TY landed
+  // 0 sA full (16 loader warps), 1-2 stage 1 done [b], 3 sR full (8 TMEM warps),
+  // 4-5 stage 2 done [b], 6-7 accQ[b] free (8 TMEM warps), 8 TX landed, 9 TY landed
   __shared__ __align__(8) uint64_t bars[10];
   __shared__ uint32_t tmem_slot;
   __shared__ int fail;
@@ -300,11 +303,11 @@ analysis_tc3_kernel(Tc2Analysis a, int T, int B, const uint8_t* __restrict__ txI
     tc::mbar_init(bar(0), A3_LOADW);
     tc::mbar_init(bar(1), 1);
     tc::mbar_init(bar(2), 1);
-    tc::mbar_init(bar(3), 4);
+    tc::mbar_init(bar(3), A3_TMW);
     tc::mbar_init(bar(4), 1);
     tc::mbar_init(bar(5), 1);
-    tc::mbar_init(bar(6), 4);
-    tc::mbar_init(bar(7), 4);
+    tc::mbar_init(bar(6), A3_TMW);
+    tc::mbar_init(bar(7), A3_TMW);
     tc::mbar_init(bar(8), 1);
     tc::mbar_init(bar(9), 1);
     fail = 0;
@@ -347,9 +350,10 @@ analysis_tc3_kernel(Tc2Analysis a, int T, int B, const uint8_t* __restrict__ txI
         }
       }
     };
-    // chunks i0 .. i0 + 3 of item j: theta -> mask (mode 1), split into sA; the
-    // non-finite inputs flagged in bad
-    auto proc_half = [&](const Item& it, int i0, bool& bad) {
+    // chunks i0 .. i0 + HALF - 1 of item j: theta -> mask (mode 1), split into the hi /
+    // lo words hw / lw of sA (stored by store_half); the non-finite inputs flagged in bad
+    uint4 hw[HALF], lw[HALF];
+    auto conv_half = [&](const Item& it, int i0, bool& bad) {
       const int m0 = it.yt * 128 + r0, x = it.xt * 128 + c8;
       float* mo = a.mask_out ? a.mask_out + (size_t)it.z * a.N * a.N + (size_t)m0 * a.N + x
                              : nullptr;
@@ -384,18 +388,23 @@ analysis_tc3_kernel(Tc2Analysis a, int T, int B, const uint8_t* __restrict__ txI
             }
           }
         }
-        uint4 h4, l4;
-        split_pair(u[0], u[1], h4.x, l4.x);
-        split_pair(u[2], u[3], h4.y, l4.y);
-        split_pair(u[4], u[5], h4.z, l4.z);
-        split_pair(u[6], u[7], h4.w, l4.w);
-        *reinterpret_cast<uint4*>(sA + so + (uint32_t)(128 * A3_RS) * i) = h4;
-        *reinterpret_cast<uint4*>(sA + so + 32768u + (uint32_t)(128 * A3_RS) * i) = l4;
+        split_pair(u[0], u[1], hw[i - i0].x, lw[i - i0].x);
+        split_pair(u[2], u[3], hw[i - i0].y, lw[i - i0].y);
+        split_pair(u[4], u[5], hw[i - i0].z, lw[i - i0].z);
+        split_pair(u[6], u[7], hw[i - i0].w, lw[i - i0].w);
+      }
+    };
+    auto store_half = [&](int i0) {
+#pragma unroll
+      for (int i = i0; i < i0 + HALF; ++i) {
+        *reinterpret_cast<uint4*>(sA + so + (uint32_t)(128 * A3_RS) * i) = hw[i - i0];
+        *reinterpret_cast<uint4*>(sA + so + 32768u + (uint32_t)(128 * A3_RS) * i) = lw[i - i0];
       }
     };
     // The loads run half an item ahead of the conversion: the second half of item j
     // loads while the first half converts, the first half of item j + 1 while the
-    // second half of item j converts.
+    // second half of item j converts. The first half is converted before the wait for
+    // sA to become free, so that only its stores follow stage 1 of the previous item.
     // the input tile of item i + 2 is fetched into L2 during item i: 512 segments of 128
     // bytes, one per loader thread (row tid / 4, columns 32 (tid % 4) ..)
     const bool pf = a.N % 4 == 0 && reinterpret_cast<uintptr_t>(a.in) % 16 == 0;
@@ -411,12 +420,14 @@ analysis_tc3_kernel(Tc2Analysis a, int T, int B, const uint8_t* __restrict__ txI
     for (int j = 0; j < n; ++j, cur = item_next(cur, T, B)) {
       if (j + 2 < n) prefetch_item(item_next(item_next(cur, T, B), T, B));
       load_half(cur, HALF);
+      bool bad = false;
+      conv_half(cur, 0, bad);
       // sA is free once stage 1 of the previous item has completed
       if (j > 0 && !pwait(bar(1 + ((j - 1) & 1)), ((j - 1) >> 1) & 1, vfail, err, 11)) break;
-      bool bad = false;
-      proc_half(cur, 0, bad);
+      store_half(0);
       if (j + 1 < n) load_half(item_next(cur, T, B), 0);
-      proc_half(cur, HALF, bad);
+      conv_half(cur, HALF, bad);
+      store_half(HALF);
       if (bad) atomicOr(a.flag, 1);
       fence_async_smem();
       __syncwarp();
@@ -426,6 +437,8 @@ analysis_tc3_kernel(Tc2Analysis a, int T, int B, const uint8_t* __restrict__ txI
     // ------------------------------------------------------------ TMEM warps
     pdl_wait();
     const int lane_base = (warp & 3) * 32;
+    constexpr int DQ = A3_TMW / 4;
+    const int q0 = (warp - A3_LOADW) / 4;   // first 16-column group of this warp
     const int count = a.nrows_out * a.ncols;
     Item prv = item_at(lo, T, B), cur = prv;   // items j - 1 and j
     for (int j = 0; j <= n; ++j) {
@@ -439,7 +452,7 @@ analysis_tc3_kernel(Tc2Analysis a, int T, int B, const uint8_t* __restrict__ txI
       tc::fence_after();
       if (j < n) {
         r_to_operand<BN>(tmem + (uint32_t)((j & 1) * 128) + ((uint32_t)lane_base << 16), sR,
-                         lane_base, 0, 1);
+                         lane_base, q0, DQ);
         fence_async_smem();
         tc::fence_before();
         __syncwarp();
@@ -450,7 +463,7 @@ analysis_tc3_kernel(Tc2Analysis a, int T, int B, const uint8_t* __restrict__ txI
         const int jp = j - 1;
         float2* out = a.part + (((size_t)prv.z * T + prv.yt) * T + prv.xt) * count;
         q_to_partials<BN>(tmem + 256u + (uint32_t)((jp & 1) * 128) + ((uint32_t)lane_base << 16),
-                          out, a, lane_base, 0, 1);
+                          out, a, lane_base, q0, DQ);
         tc::fence_before();
         __syncwarp();
         if (lane == 0) mbar_arrive(bar(6 + (jp & 1)));
