@@ -64,6 +64,9 @@ def parse():
                    help="for profilers: run only --steps untimed calls of the batched split-BF16 "
                         "CTM evaluation (--batch tiles of --size^2, graphs off) or of the batched "
                         "RK2 level-set update (--batch images of --size^2), print nothing else")
+    p.add_argument("--serving-slots", type=int, default=16,
+                   help="solves per size class batched in one step of the split-BF16 server "
+                        "(16 measured best: 64 and 128 lengthen each step more than they add)")
     p.add_argument("--serving-requests", type=int, default=1000,
                    help="LSM tile solves of the serving stream reported beside the headline "
                         "(0 skips it)")
@@ -339,11 +342,11 @@ def run_reference(args):
     print(json.dumps(out), flush=True)
 
 
-def serving_run(L, K, requests, seed=7):
+def serving_run(L, K, requests, seed=7, slots=16):
     """The serving configuration: a seeded Poisson stream (mean 400 requests/s) of LSM
     tile solves of 20 iterations, tile sizes 256^2 / 512^2 / 1024^2 / 2048^2 in
     proportions 4:3:2:1, through the continuous-batching TileServer in split-BF16 (up
-    to 16 solves per size batched, one stream per size class, 120 GB HBM budget), and
+    to `slots` solves per size batched, one stream per size class, 120 GB HBM budget), and
     the same stream through the plain FP32 one-tile-at-a-time loop (max_batch 1, one
     stream). Each server first serves the first 50 requests of the stream unmeasured
     (start-up: kernels loaded, memory sized), then a fresh server on the same contexts
@@ -366,7 +369,8 @@ def serving_run(L, K, requests, seed=7):
                        f"sizes {sizes} in proportions 4:3:2:1, {K} SOCS kernels",
            "initial_mask": "the target (binary)",
            "offered_tile_iterations_per_s": rate * its}
-    for mode, max_batch in (("bf16x3", 16), ("fp32", 1)):
+    out["bf16x3_slots_per_size"] = slots
+    for mode, max_batch in (("bf16x3", slots), ("fp32", 1)):
         if mode == "bf16x3":
             ctxs = {N: L.Context(stream=torch.cuda.Stream()) for N in sizes}
         else:
@@ -825,7 +829,7 @@ def run_ours(args):
         out["ctm_full_run"] = ctm_full_run(L, torch, stream, N, band, r0, c0, w, wss, target,
                                            graphs=not args.no_graphs)
     if world == 1 and args.serving_requests > 0:
-        out["serving"] = serving_run(L, K, args.serving_requests)
+        out["serving"] = serving_run(L, K, args.serving_requests, slots=args.serving_slots)
     if world == 1 and args.fullchip_size > 0:
         cores = (None if args.fullchip_cores == "equal" else
                  tuple(int(v) for v in args.fullchip_cores.split(",")))
