@@ -768,13 +768,42 @@ static size_t chat_smem(const BandGeom& g) {
 // straight into the split-BF16 operand image of the row synthesis instead of Ut:
 // x tile x / 128 at img + (x / 128) * img_tile_bytes, hi of column f at
 // sw128_offset(128, x % 128, f) and lo at sw128_offset(128, x % 128, kp + f).
+//
+// Both modes are summed over the nph = nc phase rows T_j = TX[j][x] = (t, u) as
+// sum_j S_j t + D_j u. For a coefficient A of phase conj(T_j) and B of phase T_j,
+// A conj(T_j) + B T_j = (A + B) t + (A.y - B.y, B.x - A.x) u, so
+//   S_j = A + B, D_j = (A.y - B.y, B.x - A.x),
+// with A = coef[a][j], B = 0 in mode 0 and A = coef[a][nc-1+j], B = coef[a][nc-1-j]
+// (B = 0 for j = 0) in mode 1: each conjugate pair of the difference set costs one
+// complex-by-real product pair instead of two complex products. Every output adds
+// its terms in j order as fma(D, u, fma(S, t, acc)) per component, in every kernel
+// below, so the batched and per-image expansions give bit-identical results.
 constexpr int EX_X = 64, EX_NT = 256;
+
+// S_j and D_j of band row coef_row for phase row j, as (S.x, S.y, D.x, D.y).
+__device__ __forceinline__ float4 expand_sd(const float2* __restrict__ coef_row, int mode, int nc,
+                                            int j) {
+  const float2 A = coef_row[mode ? nc - 1 + j : j];
+  const float2 B = (mode && j > 0) ? coef_row[nc - 1 - j] : make_float2(0.f, 0.f);
+  return make_float4(A.x + B.x, A.y + B.y, A.y - B.y, B.x - A.x);
+}
+// acc + S t + D u, lane by lane fma(D, u, fma(S, t, acc)) (packed FP32x2, the
+// rounding of two scalar fmaf per lane).
+__device__ __forceinline__ float2 sd_fma(float2 acc, float4 sd, float t, float u) {
+  return __ffma2_rn(make_float2(sd.z, sd.w), make_float2(u, u),
+                    __ffma2_rn(make_float2(sd.x, sd.y), make_float2(t, t), acc));
+}
+// Phase rows of an expansion: nc for the difference set, ncoef for the band S.
+__host__ __device__ __forceinline__ int expand_nph(int mode, int ncoef, int nc) {
+  return mode ? nc : ncoef;
+}
+
 // The accumulation and store of the expansion for one CTA of 8 PAIRS band rows, from
-// its staged coefficients cf [8 PAIRS][ncoef] and phases ph [ncoef][EX_X]. Each output
-// is summed over c in order whatever PAIRS is.
+// its staged coefficient pairs sd [8 PAIRS][nph] and phases ph [nph][EX_X]. Each
+// output is summed over j in order whatever PAIRS is.
 template <int PAIRS>
-__device__ __forceinline__ void expand_store(const float2* cf, const float2* ph, int nrows,
-                                             int ncoef, int N, int mode, int kp, int a0, int x0,
+__device__ __forceinline__ void expand_store(const float4* sd, const float2* ph, int nrows,
+                                             int nph, int N, int mode, int kp, int a0, int x0,
                                              float* __restrict__ Ut, uint8_t* __restrict__ img,
                                              uint32_t img_tile_bytes) {
   // Thread (xx, rq): row pairs p of rows a0 + 2 (PAIRS rq + p) + {0, 1}, each pair the
@@ -786,10 +815,10 @@ __device__ __forceinline__ void expand_store(const float2* cf, const float2* ph,
   float2 acc[2 * PAIRS];
 #pragma unroll
   for (int i = 0; i < 2 * PAIRS; ++i) acc[i] = make_float2(0.f, 0.f);
-  for (int c = 0; c < ncoef; ++c) {
-    const float2 p = ph[c * EX_X + xx];
+  for (int j = 0; j < nph; ++j) {
+    const float2 p = ph[j * EX_X + xx];
 #pragma unroll
-    for (int i = 0; i < 2 * PAIRS; ++i) cfma(acc[i], cf[(2 * PAIRS * rq + i) * ncoef + c], p);
+    for (int i = 0; i < 2 * PAIRS; ++i) acc[i] = sd_fma(acc[i], sd[(2 * PAIRS * rq + i) * nph + j], p.x, p.y);
   }
   if (x >= N) return;
 #pragma unroll
@@ -839,9 +868,10 @@ expand_kernel(const float2* __restrict__ coef, int nrows, int ncoef, int ld,
               const float2* __restrict__ TX, int N, int mode, int nc, int kp,
               float* __restrict__ Ut, uint8_t* __restrict__ img, uint32_t img_tile_bytes) {
   constexpr int R = 8 * PAIRS;
-  extern __shared__ float2 se[];
-  float2* cf = se;                    // [R][ncoef]
-  float2* ph = se + R * ncoef;        // [ncoef][EX_X]
+  extern __shared__ __align__(16) float4 se[];
+  const int nph = expand_nph(mode, ncoef, nc);
+  float4* sd = se;                                         // [R][nph]
+  float2* ph = reinterpret_cast<float2*>(se + R * nph);    // [nph][EX_X]
   const int x0 = blockIdx.x * EX_X, a0 = blockIdx.y * R;
   {  // image b of a batch
     const size_t b = blockIdx.z;
@@ -850,44 +880,37 @@ expand_kernel(const float2* __restrict__ coef, int nrows, int ncoef, int ld,
     else Ut += b * N * kp;
   }
   pdl_trigger();
-  fill_batched<EX_NT>(ph, ncoef * EX_X, [&](int i) {
-    const int c = i / EX_X, xx = i % EX_X, x = x0 + xx;
-    float2 t = make_float2(0.f, 0.f);
-    if (x < N) {
-      if (mode == 0) {
-        t = conjf2(TX[(size_t)c * N + x]);
-      } else {
-        const int d = c - (nc - 1);
-        t = d >= 0 ? conjf2(TX[(size_t)d * N + x]) : TX[(size_t)(-d) * N + x];
-      }
-    }
-    return t;
+  fill_batched<EX_NT>(ph, nph * EX_X, [&](int i) {
+    const int j = i / EX_X, x = x0 + i % EX_X;
+    return x < N ? TX[(size_t)j * N + x] : make_float2(0.f, 0.f);
   });
   pdl_wait();
-  fill_batched<EX_NT>(cf, R * ncoef, [&](int i) {
-    const int r = i / ncoef, c = i % ncoef;
-    return (a0 + r < nrows) ? coef[(size_t)(a0 + r) * ld + c] : make_float2(0.f, 0.f);
+  fill_batched<EX_NT>(sd, R * nph, [&](int i) {
+    const int r = i / nph, j = i % nph;
+    return (a0 + r < nrows) ? expand_sd(coef + (size_t)(a0 + r) * ld, mode, nc, j)
+                            : make_float4(0.f, 0.f, 0.f, 0.f);
   });
   __syncthreads();
-  expand_store<PAIRS>(cf, ph, nrows, ncoef, N, mode, kp, a0, x0, Ut, img, img_tile_bytes);
+  expand_store<PAIRS>(sd, ph, nrows, nph, N, mode, kp, a0, x0, Ut, img, img_tile_bytes);
 }
 
 // The expansion with every band row of an x strip in one CTA (up to 64 rows): all 256
 // threads stage the tables, then thread (xp, rg), rg < ceil(nrows / 8), computes image
 // rows x0 + 2 xp and x0 + 2 xp + 1 for the eight band rows 8 rg .. 8 rg + 7, so each
-// step over c takes one 16-byte phase load and four 16-byte
-// broadcast coefficient loads for 16 complex FMAs. Coefficients are staged transposed
-// (cfT[c][8 groups]); rows past nrows are zero. Same operands, order and scale as
+// step over j takes one 16-byte phase load and eight 16-byte broadcast loads of
+// coefficient pairs for 32 packed FMAs. The pairs are staged transposed
+// (sdT[j][8 groups]); rows past nrows are zero. Same operands, order and scale as
 // expand_store: bit-identical results.
 constexpr int EXR_X = 64, EXR_NT = 256;
 __global__ void __launch_bounds__(EXR_NT)
 expand_rows_kernel(const float2* __restrict__ coef, int nrows, int ncoef, int ld,
                    const float2* __restrict__ TX, int N, int mode, int nc, int kp,
                    float* __restrict__ Ut, uint8_t* __restrict__ img, uint32_t img_tile_bytes) {
-  extern __shared__ __align__(16) float2 sr[];
+  extern __shared__ __align__(16) float4 sr4[];
   const int groups = (nrows + 7) / 8, R = 8 * groups;
-  float2* ph = sr;                    // [ncoef][EXR_X]
-  float2* cfT = sr + ncoef * EXR_X;   // [ncoef][R]
+  const int nph = expand_nph(mode, ncoef, nc);
+  float4* sdT = sr4;                                             // [nph][R]
+  float2* ph = reinterpret_cast<float2*>(sr4 + nph * R);         // [nph][EXR_X]
   const int x0 = blockIdx.x * EXR_X;
   {  // image b of a batch
     const size_t b = blockIdx.z;
@@ -896,32 +919,25 @@ expand_rows_kernel(const float2* __restrict__ coef, int nrows, int ncoef, int ld
     else Ut += b * N * kp;
   }
   pdl_trigger();
-  fill_batched<EXR_NT>(ph, ncoef * EXR_X, [&](int i) {
-    const int c = i / EXR_X, x = x0 + i % EXR_X;
-    float2 t = make_float2(0.f, 0.f);
-    if (x < N) {
-      if (mode == 0) {
-        t = conjf2(TX[(size_t)c * N + x]);
-      } else {
-        const int d = c - (nc - 1);
-        t = d >= 0 ? conjf2(TX[(size_t)d * N + x]) : TX[(size_t)(-d) * N + x];
-      }
-    }
-    return t;
+  fill_batched<EXR_NT>(ph, nph * EXR_X, [&](int i) {
+    const int j = i / EXR_X, x = x0 + i % EXR_X;
+    return x < N ? TX[(size_t)j * N + x] : make_float2(0.f, 0.f);
   });
   pdl_wait();
-  // cfT[c][r] = coef[r][c]: a coalesced read of coef, a transposed shared store.
-  for (int base = threadIdx.x; base < R * ncoef; base += EXR_NT * 8) {
-    float2 v[8];
+  // sdT[j][r] = the pair of band row r: coalesced reads of coef, a transposed store.
+  for (int base = threadIdx.x; base < R * nph; base += EXR_NT * 4) {
+    float4 v[4];
 #pragma unroll
-    for (int q = 0; q < 8; ++q) {
-      const int i = base + q * EXR_NT, r = i / ncoef;
-      if (i < R * ncoef) v[q] = r < nrows ? coef[(size_t)r * ld + i % ncoef] : make_float2(0.f, 0.f);
+    for (int q = 0; q < 4; ++q) {
+      const int i = base + q * EXR_NT, r = i / nph;
+      if (i < R * nph)
+        v[q] = r < nrows ? expand_sd(coef + (size_t)r * ld, mode, nc, i % nph)
+                         : make_float4(0.f, 0.f, 0.f, 0.f);
     }
 #pragma unroll
-    for (int q = 0; q < 8; ++q) {
+    for (int q = 0; q < 4; ++q) {
       const int i = base + q * EXR_NT;
-      if (i < R * ncoef) cfT[(i % ncoef) * R + i / ncoef] = v[q];
+      if (i < R * nph) sdT[(i % nph) * R + i / nph] = v[q];
     }
   }
   __syncthreads();
@@ -930,18 +946,14 @@ expand_rows_kernel(const float2* __restrict__ coef, int nrows, int ncoef, int ld
   float2 acc[8][2];
 #pragma unroll
   for (int i = 0; i < 8; ++i) acc[i][0] = acc[i][1] = make_float2(0.f, 0.f);
-  for (int c = 0; c < ncoef; ++c) {
-    const float4 p = *reinterpret_cast<const float4*>(ph + c * EXR_X + 2 * xp);
-    const float2 p0 = make_float2(p.x, p.y), p1 = make_float2(p.z, p.w);
-    const float4* cq = reinterpret_cast<const float4*>(cfT + c * R + 8 * rg);
+  for (int j = 0; j < nph; ++j) {
+    const float4 p = *reinterpret_cast<const float4*>(ph + j * EXR_X + 2 * xp);
+    const float4* cq = sdT + j * R + 8 * rg;
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const float4 a = cq[q];
-      const float2 a0 = make_float2(a.x, a.y), a1 = make_float2(a.z, a.w);
-      cfma(acc[2 * q][0], a0, p0);
-      cfma(acc[2 * q][1], a0, p1);
-      cfma(acc[2 * q + 1][0], a1, p0);
-      cfma(acc[2 * q + 1][1], a1, p1);
+    for (int i = 0; i < 8; ++i) {
+      const float4 sd = cq[i];
+      acc[i][0] = sd_fma(acc[i][0], sd, p.x, p.y);
+      acc[i][1] = sd_fma(acc[i][1], sd, p.z, p.w);
     }
   }
 #pragma unroll
@@ -997,7 +1009,8 @@ static cudaError_t launch_expand_t(cudaStream_t s, const float2* coef, int nrows
   constexpr int R = 8 * PAIRS;
   // Split-BF16 image tile: 128 rows x [hi | lo] of kp columns, in 64-column atoms.
   const uint32_t img_tile_bytes = (uint32_t)((2 * kp + 63) / 64) * 128u * 128u;
-  const size_t smem = (size_t)(R * ncoef + ncoef * EX_X) * sizeof(float2);
+  const int nph = expand_nph(mode, ncoef, nc);
+  const size_t smem = (size_t)R * nph * sizeof(float4) + (size_t)nph * EX_X * sizeof(float2);
   cudaError_t e = cudaFuncSetAttribute(expand_kernel<PAIRS>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
@@ -1015,7 +1028,8 @@ static cudaError_t launch_expand(cudaStream_t s, const float2* coef, int nrows, 
     // Every band row of an x strip in one CTA (enough CTAs from 8 images on).
     const int R = 8 * ((nrows + 7) / 8);
     const uint32_t img_tile_bytes = (uint32_t)((2 * kp + 63) / 64) * 128u * 128u;
-    const size_t smem = (size_t)ncoef * (EXR_X + R) * sizeof(float2);
+    const int nph = expand_nph(mode, ncoef, nc);
+    const size_t smem = (size_t)nph * R * sizeof(float4) + (size_t)nph * EXR_X * sizeof(float2);
     cudaError_t e = cudaFuncSetAttribute(expand_rows_kernel,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
