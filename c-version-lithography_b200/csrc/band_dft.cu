@@ -438,10 +438,20 @@ __device__ __forceinline__ void cfma4(float2 (&acc)[4], float2 a, const float2* 
   cfma(acc[3], a, make_float2(b23.z, b23.w));
 }
 
+// The small-grid tables are zero-padded DFTs of even length P = 2 n: for band frequency
+// f, ES[f][j + n] = (-1)^f ES[f][j]. A transform over the P outputs folds into n:
+// out[j] = Ev[j] + Od[j] and out[j + n] = Ev[j] - Od[j], Ev and Od the sums over the
+// frequencies of even and odd f (each in increasing order), and a transform over the
+// P inputs into n: out = sum_{j < n} ES[f][j] (in[j] + (-1)^f in[j + n]). Every kernel
+// of a stage folds the same way with the same operation order, so chunked, whole-grid,
+// batched and single-image launches stay bit-identical.
+__device__ __forceinline__ float2 fold_sum(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 fold_diff(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+
 template <int W>
 __global__ void __launch_bounds__(BF_NT)
 band_fields_kernel(const float2* __restrict__ H, const float2* __restrict__ mband,
-                   const float* __restrict__ w, int Nr, int Nc, int Pr, int Pc,
+                   const float* __restrict__ w, int Nr, int Nc, int Pr, int Pc, int row0,
                    const float2* __restrict__ ESc_t, const float2* __restrict__ ESr_t,
                    int stage_tables, float2* __restrict__ e, float* __restrict__ ik) {
   static_assert(W % 4 == 0, "four columns per thread");
@@ -483,16 +493,23 @@ band_fields_kernel(const float2* __restrict__ H, const float2* __restrict__ mban
   }
   __syncthreads();
   const float wk = w[k];
-  for (int it = threadIdx.x; it < Pr * JB; it += BF_NT) {
+  // e_k rows jr and jr + Nr from the two parity classes of the band rows (fold_rows).
+  const int r_even = row0 & 1;   // first r with row0 + r even
+  for (int it = threadIdx.x; it < Nr * JB; it += BF_NT) {
     const int jr = it / JB, jb = 4 * (it % JB);
-    float2 acc[4] = {};
-    for (int r = 0; r < Nr; ++r) cfma4(acc, ESR[r * Pr + jr], T + r * W + jb);
+    float2 ev[4] = {}, od[4] = {};
+    for (int r = r_even; r < Nr; r += 2) cfma4(ev, ESR[r * Pr + jr], T + r * W + jb);
+    for (int r = 1 - r_even; r < Nr; r += 2) cfma4(od, ESR[r * Pr + jr], T + r * W + jb);
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
       if (jb + q >= cw) break;
-      const size_t o = ((size_t)k * Pr + jr) * Pc + j0 + jb + q;
-      e[o] = acc[q];
-      ik[o] = wk * (acc[q].x * acc[q].x + acc[q].y * acc[q].y);
+      const float2 v[2] = {fold_sum(ev[q], od[q]), fold_diff(ev[q], od[q])};
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const size_t o = ((size_t)k * Pr + jr + h * Nr) * Pc + j0 + jb + q;
+        e[o] = v[h];
+        ik[o] = wk * (v[h].x * v[h].x + v[h].y * v[h].y);
+      }
     }
   }
 }
@@ -532,15 +549,62 @@ __device__ __forceinline__ void cgemm_rt2(int M, int npairs, int Kd, ALoad a,
   }
 }
 
+// C = A B folded over the output rows (the transform over P = 2 M outputs): output rows
+// m and m + M of each column pair from Ev = sum over k of the parity class k0, k0 + 2,
+// ... and Od = sum over the other class, each in increasing k with cfma, stored as
+// Ev + Od (row m) and Ev - Od (row m + M). Each thread owns RT rows x 2 columns.
+template <int RT, int NT, class ALoad, class Store>
+__device__ __forceinline__ void fold_rows(int M, int npairs, int Kd, int k0, ALoad a,
+                                          const float2* __restrict__ B, int ldb, Store store) {
+  const int rblocks = (M + RT - 1) / RT;
+  for (int it = threadIdx.x; it < rblocks * npairs; it += NT) {
+    const int m0 = (it / npairs) * RT, p = it % npairs;
+    float2 ev[RT][2], od[RT][2];
+#pragma unroll
+    for (int i = 0; i < RT; ++i) ev[i][0] = ev[i][1] = od[i][0] = od[i][1] = make_float2(0.f, 0.f);
+    for (int k = k0; k < Kd; k += 2) {
+      const float4 b = *reinterpret_cast<const float4*>(B + (size_t)k * ldb + 2 * p);
+      const float2 b0 = make_float2(b.x, b.y), b1 = make_float2(b.z, b.w);
+#pragma unroll
+      for (int i = 0; i < RT; ++i) {
+        const float2 av = a(min(m0 + i, M - 1), k);
+        cfma(ev[i][0], av, b0);
+        cfma(ev[i][1], av, b1);
+      }
+    }
+    for (int k = 1 - k0; k < Kd; k += 2) {
+      const float4 b = *reinterpret_cast<const float4*>(B + (size_t)k * ldb + 2 * p);
+      const float2 b0 = make_float2(b.x, b.y), b1 = make_float2(b.z, b.w);
+#pragma unroll
+      for (int i = 0; i < RT; ++i) {
+        const float2 av = a(min(m0 + i, M - 1), k);
+        cfma(od[i][0], av, b0);
+        cfma(od[i][1], av, b1);
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < RT; ++i) {
+      if (m0 + i < M) {
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          store(m0 + i, 2 * p + h, fold_sum(ev[i][h], od[i][h]));
+          store(m0 + i + M, 2 * p + h, fold_diff(ev[i][h], od[i][h]));
+        }
+      }
+    }
+  }
+}
+
 // Forward 1, whole small grid per CTA: grid (K, 1, batch), CTA (k, b) computes all of
 // e_k = ESr (A ESc^T) (Pr x Pc) and ik = w_k |e_k|^2 for image b, every table staged
 // once per CTA instead of once per column chunk. Same arithmetic as
 // band_fields_kernel (bit-identical results), register-blocked: 5 rows x 2 columns of
-// T and 10 rows x 2 columns of e_k per thread.
+// T and, folded over the row parity classes, 5 row pairs (jr, jr + Nr) x 2 columns of
+// e_k per thread.
 constexpr int BG_NT = 256;
 __global__ void __launch_bounds__(BG_NT)
 band_fields_whole_kernel(const float2* __restrict__ H, const float2* __restrict__ mband,
-                         const float* __restrict__ w, int Nr, int Nc, int Pr, int Pc,
+                         const float* __restrict__ w, int Nr, int Nc, int Pr, int Pc, int row0,
                          const float2* __restrict__ ESc_t, const float2* __restrict__ ESr_t,
                          float2* __restrict__ e, float* __restrict__ ik) {
   extern __shared__ __align__(16) float2 sm2[];
@@ -567,12 +631,12 @@ band_fields_whole_kernel(const float2* __restrict__ H, const float2* __restrict_
   const float wk = w[k];
   float2* ek = e + (size_t)k * Pr * Pc;
   float* ikk = ik + (size_t)k * Pr * Pc;
-  cgemm_rt2<10, BG_NT>(Pr, Pc / 2, Nr, [&](int jr, int r) { return esr[r * Pr + jr]; }, T, Pc,
-                       [&](int jr, int j, float2 v) {
-                         const size_t o = (size_t)jr * Pc + j;
-                         ek[o] = v;
-                         ikk[o] = wk * (v.x * v.x + v.y * v.y);
-                       });
+  fold_rows<5, BG_NT>(Nr, Pc / 2, Nr, row0 & 1, [&](int jr, int r) { return esr[r * Pr + jr]; }, T,
+                      Pc, [&](int jr, int j, float2 v) {
+                        const size_t o = (size_t)jr * Pc + j;
+                        ek[o] = v;
+                        ikk[o] = wk * (v.x * v.x + v.y * v.y);
+                      });
 }
 
 static size_t fields_whole_smem(const BandGeom& g) {
@@ -1062,7 +1126,7 @@ cudaError_t launch_band_forward(cudaStream_t s, const Cache& c, Field& f, float*
     if (e1 != cudaSuccess) return e1;
     return launch_pdl(band_fields_kernel<W>, dim3(g.K, (g.Pc + W - 1) / W, batch), dim3(BF_NT),
                       sm1, s, c.H, static_cast<const float2*>(f.mband), c.w, g.Nr, g.Nc, g.Pr,
-                      g.Pc, c.ESc_t, c.ESr_t, (int)staged, f.e, ik);
+                      g.Pc, g.row0, c.ESc_t, c.ESr_t, (int)staged, f.e, ik);
   };
   // Schedule: the autotuned one when set, else the whole small grid per CTA for large
   // batches (enough CTAs to fill the GPU) and column chunks otherwise.
@@ -1073,8 +1137,8 @@ cudaError_t launch_band_forward(cudaStream_t s, const Cache& c, Field& f, float*
                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smw);
     if (err == cudaSuccess)
       err = launch_pdl(band_fields_whole_kernel, dim3(g.K, 1, batch), dim3(BG_NT), smw, s, c.H,
-                       static_cast<const float2*>(f.mband), c.w, g.Nr, g.Nc, g.Pr, g.Pc, c.ESc_t,
-                       c.ESr_t, f.e, ik);
+                       static_cast<const float2*>(f.mband), c.w, g.Nr, g.Nc, g.Pr, g.Pc, g.row0,
+                       c.ESc_t, c.ESr_t, f.e, ik);
   } else {
     const bool wide = width > 0 ? width >= BW_BATCH : batch >= 4;
     err = wide ? fields(std::integral_constant<int, BW_BATCH>{})
@@ -1245,6 +1309,71 @@ size_t band_max_smem(const BandGeom& g) {
   return m;
 }
 
+// The folded input of the Z transform over the small-grid columns: entry i = jr Pc + jc
+// of [Pr][Pc] holds, for jc < Nc, q(jr, jc) + q(jr, jc + Nc) and, for jc >= Nc,
+// q(jr, jc - Nc) - q(jr, jc), where q = e_k gamma (products rounded on their own).
+__device__ __forceinline__ float2 z_fold_q(const float2* __restrict__ ek,
+                                           const float* __restrict__ gam, int Nc, int Pc, int i) {
+  const int jr = i / Pc, jc = i % Pc, j = jc < Nc ? jc : jc - Nc;
+  const size_t o0 = (size_t)jr * Pc + j, o1 = o0 + Nc;
+  const float2 t0 = ek[o0], t1 = ek[o1];
+  const float g0 = gam[o0], g1 = gam[o1];
+  const float2 a = make_float2(__fmul_rn(t0.x, g0), __fmul_rn(t0.y, g0));
+  const float2 b = make_float2(__fmul_rn(t1.x, g1), __fmul_rn(t1.y, g1));
+  return jc < Nc ? fold_sum(a, b) : fold_diff(a, b);
+}
+
+// The staged product q = e_k gamma ([Pr][Pc], products by __fmul_rn) folded in place into
+// the layout of z_fold_q, with the same operations; one thread per (jr, jc < Nc) pair.
+__device__ __forceinline__ float2 z_product(const float2* __restrict__ ek,
+                                            const float* __restrict__ gam, int i) {
+  const float2 t = ek[i];
+  const float g = gam[i];
+  return make_float2(__fmul_rn(t.x, g), __fmul_rn(t.y, g));
+}
+template <int NT>
+__device__ __forceinline__ void z_fold_inplace(float2* q, int Pr, int Nc, int Pc) {
+  for (int i = threadIdx.x; i < Pr * Nc; i += NT) {
+    const int jr = i / Nc, jc = i - jr * Nc;
+    float2* row = q + jr * Pc;
+    const float2 a = row[jc], b = row[jc + Nc];
+    row[jc] = fold_sum(a, b);
+    row[jc + Nc] = fold_diff(a, b);
+  }
+}
+
+// C = A B with a separate A operand per column of each pair (the transform over P = 2 n
+// inputs, folded: column 2p reads a0, column 2p + 1 reads a1), K = Kd in increasing
+// order with cfma; each thread owns RT rows x 2 columns.
+template <int RT, int NT, class ALoad0, class ALoad1, class Store>
+__device__ __forceinline__ void fold_cols_in(int M, int npairs, int Kd, ALoad0 a0, ALoad1 a1,
+                                             const float2* __restrict__ B, int ldb, Store store) {
+  const int rblocks = (M + RT - 1) / RT;
+  for (int it = threadIdx.x; it < rblocks * npairs; it += NT) {
+    const int m0 = (it / npairs) * RT, p = it % npairs;
+    float2 acc[RT][2];
+#pragma unroll
+    for (int i = 0; i < RT; ++i) acc[i][0] = acc[i][1] = make_float2(0.f, 0.f);
+    for (int k = 0; k < Kd; ++k) {
+      const float4 b = *reinterpret_cast<const float4*>(B + (size_t)k * ldb + 2 * p);
+      const float2 b0 = make_float2(b.x, b.y), b1 = make_float2(b.z, b.w);
+#pragma unroll
+      for (int i = 0; i < RT; ++i) {
+        const int m = min(m0 + i, M - 1);
+        cfma(acc[i][0], a0(m, k), b0);
+        cfma(acc[i][1], a1(m, k), b1);
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < RT; ++i) {
+      if (m0 + i < M) {
+        store(m0 + i, 2 * p, acc[i][0]);
+        store(m0 + i, 2 * p + 1, acc[i][1]);
+      }
+    }
+  }
+}
+
 // Adjoint 2: grid (K, band column chunks of W, batch). CTA (k, q) owns band columns
 // uc in [q W, q W + W): q_k = e_k gamma (Pr x Pc, staged), Z1 = q_k conj(ESc)
 // restricted to those columns (Pr x W), Zk = conj(ESr_t) Z1 / (Pr Pc) (Nr x W); four
@@ -1252,7 +1381,7 @@ size_t band_max_smem(const BandGeom& g) {
 template <int W>
 __global__ void __launch_bounds__(BF_NT)
 band_z_kernel(const float2* __restrict__ e, const float* __restrict__ gam, int Nr, int Nc, int Pr,
-              int Pc, const float2* __restrict__ ESc, const float2* __restrict__ ESr_t,
+              int Pc, int col0, const float2* __restrict__ ESc, const float2* __restrict__ ESr_t,
               int stage_tables, float inv, float2* __restrict__ Zk) {
   static_assert(W % 4 == 0, "four columns per thread");
   constexpr int JB = W / 4;
@@ -1267,12 +1396,12 @@ band_z_kernel(const float2* __restrict__ e, const float* __restrict__ gam, int N
     Zk += b * gridDim.x * Nr * Nc;
   }
   float2* Z1 = sz;                  // [Pr][W]
-  float2* esc = Z1 + Pr * W;        // [Pc][W] (columns past uw are zero)
-  float2* q = esc + Pc * W;         // [Pr][Pc]   (staged)
+  float2* esc = Z1 + Pr * W;        // [Pc][W] (rows jc < Nc used; columns past uw are zero)
+  float2* q = esc + Pc * W;         // [Pr][Pc]   (staged: folded, z_fold_q)
   float2* esr = q + Pr * Pc;        // [Nr][Pr]   (staged)
   const float2* ek = e + (size_t)k * Pr * Pc;
   pdl_trigger();
-  fill_batched<BF_NT>(esc, Pc * W, [&](int i) {
+  fill_batched<BF_NT>(esc, Nc * W, [&](int i) {
     const int jc = i / W, uu = i % W;
     return uu < uw ? conjf2(ESc[(size_t)jc * Nc + u0 + uu]) : make_float2(0.f, 0.f);
   });
@@ -1283,26 +1412,34 @@ band_z_kernel(const float2* __restrict__ e, const float* __restrict__ gam, int N
   }
   pdl_wait();
   if (stage_tables) {
-    fill_batched<BF_NT>(q, Pr * Pc, [&](int i) {
-      const float2 v = ek[i];
-      const float gv = gam[i];
-      return make_float2(v.x * gv, v.y * gv);
-    });
+    fill_batched<BF_NT>(q, Pr * Pc, [&](int i) { return z_product(ek, gam, i); });
+    __syncthreads();
+    z_fold_inplace<BF_NT>(q, Pr, Nc, Pc);
   }
   __syncthreads();
+  // Columns u0 + jb + {0, 2} have the parity of col0, {1, 3} the other (u0, jb multiples
+  // of 4): the even class takes the folded sums, the odd class the differences.
+  const int cpar = col0 & 1;
   for (int it = threadIdx.x; it < Pr * JB; it += BF_NT) {
     const int jr = it / JB, jb = 4 * (it % JB);
     float2 acc[4] = {};
-    for (int jc = 0; jc < Pc; ++jc) {
-      float2 v;
+    for (int jc = 0; jc < Nc; ++jc) {
+      float2 va, vb;
       if (stage_tables) {
-        v = q[jr * Pc + jc];
+        va = q[jr * Pc + (cpar ? Nc : 0) + jc];
+        vb = q[jr * Pc + (cpar ? 0 : Nc) + jc];
       } else {
-        const float2 t = ek[(size_t)jr * Pc + jc];
-        const float gv = gam[(size_t)jr * Pc + jc];
-        v = make_float2(t.x * gv, t.y * gv);
+        const float2 vs = z_fold_q(ek, gam, Nc, Pc, jr * Pc + jc);
+        const float2 vd = z_fold_q(ek, gam, Nc, Pc, jr * Pc + Nc + jc);
+        va = cpar ? vd : vs;
+        vb = cpar ? vs : vd;
       }
-      cfma4(acc, v, esc + jc * W + jb);
+      const float4 b01 = *reinterpret_cast<const float4*>(esc + jc * W + jb);
+      const float4 b23 = *reinterpret_cast<const float4*>(esc + jc * W + jb + 2);
+      cfma(acc[0], va, make_float2(b01.x, b01.y));
+      cfma(acc[1], vb, make_float2(b01.z, b01.w));
+      cfma(acc[2], va, make_float2(b23.x, b23.y));
+      cfma(acc[3], vb, make_float2(b23.z, b23.w));
     }
     *reinterpret_cast<float4*>(Z1 + jr * W + jb) = make_float4(acc[0].x, acc[0].y, acc[1].x, acc[1].y);
     *reinterpret_cast<float4*>(Z1 + jr * W + jb + 2) =
@@ -1328,7 +1465,7 @@ band_z_kernel(const float2* __restrict__ e, const float* __restrict__ gam, int N
 // table columns, whose outputs are not stored.
 __global__ void __launch_bounds__(BG_NT)
 band_z_whole_kernel(const float2* __restrict__ e, const float* __restrict__ gam, int Nr, int Nc,
-                    int Pr, int Pc, const float2* __restrict__ ESc,
+                    int Pr, int Pc, int col0, const float2* __restrict__ ESc,
                     const float2* __restrict__ ESr_t, float inv, float2* __restrict__ Zk) {
   extern __shared__ __align__(16) float2 sz[];
   const int k = blockIdx.x;
@@ -1345,20 +1482,21 @@ band_z_whole_kernel(const float2* __restrict__ e, const float* __restrict__ gam,
   float2* Z1 = q + Pr * Pc;           // [Pr][NcE]
   const float2* ek = e + (size_t)k * Pr * Pc;
   pdl_trigger();
-  fill_batched<BG_NT>(esc, Pc * NcE, [&](int i) {
+  fill_batched<BG_NT>(esc, Nc * NcE, [&](int i) {
     const int jc = i / NcE, u = i % NcE;
     return u < Nc ? conjf2(ESc[(size_t)jc * Nc + u]) : make_float2(0.f, 0.f);
   });
   fill_batched<BG_NT>(esr, Nr * Pr, [&](int i) { return ESr_t[i]; });
   pdl_wait();
-  fill_batched<BG_NT>(q, Pr * Pc, [&](int i) {
-    const float2 v = ek[i];
-    const float gv = gam[i];
-    return make_float2(v.x * gv, v.y * gv);
-  });
+  fill_batched<BG_NT>(q, Pr * Pc, [&](int i) { return z_product(ek, gam, i); });
   __syncthreads();
-  cgemm_rt2<5, BG_NT>(Pr, NcE / 2, Pc, [&](int jr, int jc) { return q[jr * Pc + jc]; }, esc, NcE,
-                      [&](int jr, int u, float2 v) { Z1[jr * NcE + u] = v; });
+  z_fold_inplace<BG_NT>(q, Pr, Nc, Pc);
+  __syncthreads();
+  // Column 2p has the parity of col0: sums for an even class, differences for an odd one.
+  const int off0 = (col0 & 1) ? Nc : 0, off1 = Nc - off0;
+  fold_cols_in<5, BG_NT>(Pr, NcE / 2, Nc, [&](int jr, int jc) { return q[jr * Pc + off0 + jc]; },
+                         [&](int jr, int jc) { return q[jr * Pc + off1 + jc]; }, esc, NcE,
+                         [&](int jr, int u, float2 v) { Z1[jr * NcE + u] = v; });
   __syncthreads();
   float2* zk = Zk + (size_t)k * Nr * Nc;
   cgemm_rt2<3, BG_NT>(Nr, NcE / 2, Pr, [&](int ur, int jr) { return conjf2(esr[ur * Pr + jr]); },
@@ -1450,7 +1588,8 @@ cudaError_t launch_band_adjoint(cudaStream_t s, const Cache& c, const Field& f, 
     if (e1 != cudaSuccess) return e1;
     return launch_pdl(band_z_kernel<W>, dim3(g.K, (g.Nc + W - 1) / W, batch), dim3(BF_NT), smz, s,
                       static_cast<const float2*>(f.e), static_cast<const float*>(gam), g.Nr, g.Nc,
-                      g.Pr, g.Pc, c.ESc, c.ESr_t, stage, 1.f / ((float)g.Pr * (float)g.Pc), Zk);
+                      g.Pr, g.Pc, g.col0, c.ESc, c.ESr_t, stage, 1.f / ((float)g.Pr * (float)g.Pc),
+                      Zk);
   };
   cudaError_t err;
   if (band_whole(g, batch, width)) {
@@ -1460,7 +1599,8 @@ cudaError_t launch_band_adjoint(cudaStream_t s, const Cache& c, const Field& f, 
     if (err == cudaSuccess)
       err = launch_pdl(band_z_whole_kernel, dim3(g.K, 1, batch), dim3(BG_NT), smw, s,
                        static_cast<const float2*>(f.e), static_cast<const float*>(gam), g.Nr,
-                       g.Nc, g.Pr, g.Pc, c.ESc, c.ESr_t, 1.f / ((float)g.Pr * (float)g.Pc), Zk);
+                       g.Nc, g.Pr, g.Pc, g.col0, c.ESc, c.ESr_t, 1.f / ((float)g.Pr * (float)g.Pc),
+                       Zk);
   } else {
     const bool wide = width > 0 ? width >= BW_BATCH : batch >= 4;
     err = wide ? zk(std::integral_constant<int, BW_BATCH>{})
